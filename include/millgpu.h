@@ -1,0 +1,284 @@
+/*
+ * millgpu.h -- C ABI of the B200 implementation of MillDynamics3's per-sub-step hot path
+ * (PBF slurry + XPBD ball discs + two-way coupling), the drop-in for the Rust functions it names.
+ *
+ * Conventions (mirroring the reference's Rust API, crates/mill-core):
+ *   - Every function returns an int status: MG_OK (0) on success, otherwise an MG_ERR_* code;
+ *     mg_last_error(sim) / mg_global_last_error() give a message owned by the library.
+ *   - Params are SI, field for field the reference's `Params` (params.rs:535-541) with the same
+ *     names, units and defaults; enums are plain uint32 codes listed below.
+ *   - State arrays are caller-owned, SoA, FP32, world coordinates with the drum centre at the
+ *     origin (geometry.rs:112-114). Vec2 arrays are interleaved (x0, y0, x1, y1, ...).
+ *   - The step is infallible in the reference (it sanitises NaN instead of failing); here a step
+ *     fails only on device errors or on exceeding a buffer capacity, reported by status code.
+ *   - Threading: one CUDA stream per handle; a handle is not thread-safe; distinct handles may be
+ *     driven from distinct host threads.
+ */
+#ifndef MILLGPU_H
+#define MILLGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  MG_OK = 0,
+  MG_ERR_INVALID_PARAMS = 1, /* Params::validate failed (params.rs:545-552) */
+  MG_ERR_ARG = 2,            /* null pointer, size mismatch, unknown preset */
+  MG_ERR_CUDA = 3,           /* a CUDA runtime call failed */
+  MG_ERR_CAPACITY = 4,       /* a device buffer bound was exceeded (see mg_last_error) */
+  MG_ERR_NO_DEVICE = 5,      /* no CUDA device / extension built without one */
+  MG_ERR_STATE = 6           /* the handle is in an unusable state */
+};
+
+/* enum codes */
+enum { MG_SPEED_RPM = 0, MG_SPEED_PERCENT_CRITICAL = 1 };
+enum { MG_DIR_CCW = 0, MG_DIR_CW = 1 };
+enum { MG_CG_AUTO = 0, MG_CG_OFF = 1, MG_CG_MANUAL = 2 };
+enum { MG_RHEOLOGY_NEWTONIAN = 0, MG_RHEOLOGY_BINGHAM = 1 };
+enum { MG_DYE_LEFT_RIGHT = 0, MG_DYE_TOP_BOTTOM = 1, MG_DYE_NONE = 2 };
+enum { MG_IMPACT_BALL_BALL = 0, MG_IMPACT_BALL_WALL = 1 };
+#define MG_WALL_PARTNER 0xFFFFFFFFu
+#define MG_WALL_IMPULSE_BINS 32
+#define MG_IMPACT_BINS 12
+#define MG_SE_BINS 28
+
+/* params.rs:53-60 MillParams */
+typedef struct MgMillParams {
+  float diameter_m;
+  uint32_t speed_mode;
+  float speed_value;
+  uint32_t direction;
+} MgMillParams;
+
+/* params.rs:125-185 MediaParams */
+typedef struct MgMediaParams {
+  float ball_diameter_m, fill_fraction, packing_fraction_2d, density_kg_m3;
+  float restitution_ball_ball, restitution_ball_wall, friction_ball_ball, friction_ball_wall;
+  float friction_ball_ball_static, friction_ball_wall_static, friction_velocity_scale_m_s;
+  float rolling_friction;
+} MgMediaParams;
+
+/* params.rs:297-345 SlurryParams */
+typedef struct MgSlurryParams {
+  uint32_t enabled;
+  float fill_fraction, density_kg_m3, viscosity_pa_s;
+  uint32_t rheology;
+  float yield_stress_pa, wall_no_slip, ball_no_slip, wettability, surface_tension_n_m;
+  uint32_t dye_pattern;
+} MgSlurryParams;
+
+/* params.rs:409-417 LiftersParams */
+typedef struct MgLiftersParams {
+  uint32_t count;
+  float height_m, base_width_m, top_width_m, phase_deg;
+} MgLiftersParams;
+
+/* params.rs:452-491 SimulationParams */
+typedef struct MgSimulationParams {
+  uint32_t resolution, substeps, pbf_iterations, dem_iterations;
+  float time_scale, frame_budget_ms;
+  uint32_t max_balls, reserved0;
+  uint64_t seed;
+  uint32_t coarse_graining_mode;
+  float coarse_graining_k;
+} MgSimulationParams;
+
+/* params.rs:535-541 Params */
+typedef struct MgParams {
+  MgMillParams mill;
+  MgMediaParams media;
+  MgSlurryParams slurry;
+  MgLiftersParams lifters;
+  MgSimulationParams simulation;
+} MgParams;
+
+/* Quantities derived from Params (params.rs:80-113, 558-726). */
+typedef struct MgDerived {
+  float critical_speed_rpm, rpm, percent_critical, omega, radius_m;
+  float true_ball_count;
+  float eff_true_diameter_m, eff_diameter_m, eff_density_kg_m3;
+  uint32_t eff_ball_count;
+  float eff_scale_factor;
+  uint32_t effective_fluid_resolution, effective_substeps;
+  float fixed_sub_dt;
+} MgDerived;
+
+/* geometry.rs:18-31 Drum */
+typedef struct MgDrum {
+  float radius_m, omega;
+  MgLiftersParams lifters;
+} MgDrum;
+
+/* pbf.rs:874-917 FluidStepStats */
+typedef struct MgFluidStepStats {
+  uint32_t viscosity_iterations;
+  float mean_shear_rate_per_s;
+  uint32_t coupling_clamp_hits;
+  float wall_work_j;
+  float wall_impulse[2];
+  float wall_angular_impulse;
+  float wall_normal_impulse_by_angle[MG_WALL_IMPULSE_BINS];
+  float ke_delta_noslip_j, ke_delta_drag_j, ke_delta_buoyancy_j, ke_delta_viscosity_j, ke_delta_clamp_j;
+} MgFluidStepStats;
+
+/* dem.rs:176-221 DemStepStats */
+typedef struct MgDemStepStats {
+  float wall_work_j;
+  uint32_t collision_count;
+  uint32_t impact_energy_histogram[MG_IMPACT_BINS];
+  float dissipated_energy_j;
+  float max_substep_displacement_over_diameter;
+  float coupling_work_j;
+} MgDemStepStats;
+
+/* dem.rs:142-169 ImpactRecord (partner == MG_WALL_PARTNER for a wall impact) */
+typedef struct MgImpactRecord {
+  uint32_t kind, ball, partner;
+  float normal_speed, slip_speed, restitution;
+} MgImpactRecord;
+
+/* Counters of the last sub-step (stage_timing.rs Counters semantics). */
+typedef struct MgStepCounters {
+  uint32_t density_iters, cg_iters, n_groups, n_links, links_in_range;
+  uint32_t n_ball_pairs, n_fluid_edges, n_active_contacts;
+} MgStepCounters;
+
+/* dem.rs:277-309 Balls' uniform material fields */
+typedef struct MgBallMaterial {
+  float radius, mass, inertia, true_radius;
+} MgBallMaterial;
+
+/* pbf.rs:1018-1028 FluidParticles' uniform material fields */
+typedef struct MgFluidMaterial {
+  float particle_mass, h, rest_density;
+} MgFluidMaterial;
+
+/* lib.rs:61-78 EnergyBudget */
+typedef struct MgEnergyBudget {
+  double elapsed_s, shaft_work_j, dem_wall_work_j, fluid_wall_work_j, ball_contact_dissipation_j;
+  double fluid_wall_slip_j, fluid_viscous_j, fluid_clamp_removed_j, interface_created_j;
+  double delta_mechanical_j, unattributed_j, fluid_wall_angular_impulse;
+} MgEnergyBudget;
+
+/* lib.rs:82-119 Simulation's scalar outputs */
+typedef struct MgScalars {
+  float drum_angle, power_draw_w, torque_nm, collision_rate_per_s, dissipated_power_w;
+  float max_substep_displacement_over_diameter;
+  uint32_t coupling_clamp_hits, viscosity_iterations;
+  float mean_shear_rate_per_s, reserved0;
+  double sim_time;
+} MgScalars;
+
+/* Device-path options. cg_fp64: 0 = the reference's sequential f32 inner products in the
+ * viscosity solve, 1 = f64 inner products and residual norms. block_threads: 0 = default. */
+typedef struct MgOptions {
+  uint32_t cg_fp64;
+  uint32_t block_threads;
+  uint32_t reserved[6];
+} MgOptions;
+
+typedef struct MgSim MgSim;
+
+/* ---- sizes (layout checks for FFI bindings) ---- */
+size_t mg_sizeof_params(void);
+size_t mg_sizeof_fluid_stats(void);
+size_t mg_sizeof_dem_stats(void);
+
+/* ---- params.rs / presets.ts ---- */
+/* Params::default() (params.rs:62-77,210-227,351-375,419-428,505-518) */
+int mg_params_default(MgParams* out);
+/* Params::validate() (params.rs:545-552); err receives the reference's message. */
+int mg_params_validate(const MgParams* p, char* err, size_t err_len);
+/* web/src/params/presets.ts:91-123 QUALITY_PRESETS by id ("realtime", "balanced", ...) */
+int mg_preset_apply(MgParams* p, const char* id);
+/* MillParams::{critical_speed_rpm,rpm,omega}, Params::{true_ball_count, effective_media,
+ * effective_fluid_resolution, effective_substeps}, Simulation::fixed_sub_dt */
+int mg_params_derived(const MgParams* p, MgDerived* out);
+
+/* ---- lib.rs Simulation ---- */
+/* Simulation::new (lib.rs:126-128) */
+int mg_sim_create(const MgParams* p, MgSim** out);
+/* Simulation::with_initial_balls (lib.rs:134-136); xy holds n interleaved positions */
+int mg_sim_create_with_balls(const MgParams* p, const float* xy, uint32_t n, MgSim** out);
+void mg_sim_destroy(MgSim* sim);
+const char* mg_last_error(const MgSim* sim);
+const char* mg_global_last_error(void);
+int mg_sim_set_options(MgSim* sim, const MgOptions* opt);
+/* Simulation::step (lib.rs:456-464): effective_substeps() sub-steps of dt/n each */
+int mg_sim_step(MgSim* sim, float dt);
+/* Simulation::step_fixed (lib.rs:438-441) */
+int mg_sim_step_fixed(MgSim* sim);
+/* Simulation::reset_frame_stats (lib.rs:449-452) */
+int mg_sim_reset_frame_stats(MgSim* sim);
+/* Simulation::set_params (lib.rs:270-274) */
+int mg_sim_set_params(MgSim* sim, const MgParams* p);
+/* Simulation::fixed_sub_dt (lib.rs:426-428) */
+float mg_sim_fixed_sub_dt(const MgSim* sim);
+/* Simulation::reset_energy_budget (lib.rs:211-214) */
+int mg_sim_reset_energy_budget(MgSim* sim);
+
+/* ---- the path itself: coupling.rs:71-96 step_recorded ----
+ * Runs one coupled sub-step (fluid first, then the balls with the fluid's impulses) on the
+ * handle's state, in place. Impact records are written to `out` (up to `cap`); *n_out receives
+ * the full count (a count above cap means records were dropped). Any stats pointer may be NULL. */
+int mg_coupling_step_recorded(MgSim* sim, const MgDrum* drum, float drum_angle, const MgMediaParams* media,
+                              const MgSlurryParams* slurry, uint32_t dem_iterations, uint32_t pbf_iterations,
+                              float dt, MgFluidStepStats* fluid_stats, MgDemStepStats* dem_stats,
+                              MgImpactRecord* out, uint32_t cap, uint32_t* n_out);
+/* FluidParticles::step_coupled (pbf.rs:1174-2365): the fluid half alone; impulses (2*n_balls),
+ * angular (n_balls), clamp_hits and fluid_momentum (2) receive CouplingImpulses (coupling.rs:37-63). */
+int mg_fluid_step_coupled(MgSim* sim, const MgDrum* drum, float drum_angle, const MgSlurryParams* slurry,
+                          uint32_t iterations, float dt, MgFluidStepStats* stats, float* impulses, float* angular,
+                          uint32_t* clamp_hits, float* fluid_momentum);
+/* DemState::step_recorded (dem.rs:530-1066): the ball half alone; impulses/angular may be NULL
+ * (no external impulses, DemState::step). */
+int mg_dem_step_recorded(MgSim* sim, const MgDrum* drum, float drum_angle, const MgMediaParams* media,
+                         uint32_t iterations, float dt, const float* impulses, const float* angular,
+                         MgDemStepStats* stats, MgImpactRecord* out, uint32_t cap, uint32_t* n_out);
+
+/* ---- state I/O ---- */
+int mg_get_counts(const MgSim* sim, uint32_t* n_balls, uint32_t* n_fluid);
+int mg_get_balls(MgSim* sim, float* x, float* v, float* theta, float* omega);
+int mg_set_balls(MgSim* sim, uint32_t n, const float* x, const float* v, const float* theta, const float* omega);
+int mg_get_ball_material(const MgSim* sim, MgBallMaterial* out);
+int mg_set_ball_material(MgSim* sim, const MgBallMaterial* m);
+/* guess may be NULL; *guess_len receives the viscous warm-start length (0 or n_fluid). */
+int mg_get_fluid(MgSim* sim, float* x, float* v, float* dye, float* guess, uint32_t* guess_len);
+/* guess may be NULL (empty warm start, as after FluidParticles::seed_lattice). */
+int mg_set_fluid(MgSim* sim, uint32_t n, const float* x, const float* v, const float* dye, const float* guess);
+int mg_get_fluid_material(const MgSim* sim, MgFluidMaterial* out);
+int mg_set_fluid_material(MgSim* sim, const MgFluidMaterial* m);
+
+/* ---- outputs ---- */
+int mg_get_scalars(MgSim* sim, MgScalars* out);
+/* Simulation::energy_budget (lib.rs:218-229) */
+int mg_energy_budget(MgSim* sim, MgEnergyBudget* out);
+/* FNV-1a over the f32 bits of the state (examples/perf_probe.rs:230-262) */
+int mg_state_hash(MgSim* sim, int extended, uint64_t* out);
+/* metrics::mixing_index (metrics.rs:506-576); *valid = 0 for None */
+int mg_mixing_index(MgSim* sim, float* out, int* valid);
+/* StressAccum::histogram_rate (stress.rs:174-176), 28 bins per second */
+int mg_stress_histogram_rate(MgSim* sim, double* out28);
+/* stats of the last sub-step taken by any step call */
+int mg_last_step_stats(MgSim* sim, MgFluidStepStats* fluid, MgDemStepStats* dem, MgStepCounters* ctr);
+
+/* ---- parity probes of the grid stage (grid.rs, pbf.rs:262-288) ----
+ * Run the device grid build / candidate-pair / neighbour-list code on caller points. */
+int mg_probe_grid(const float* xy, uint32_t n, float cell, int32_t* min_cxy, int64_t* wh, uint32_t* cell_start,
+                  uint32_t cell_cap, uint32_t* indices, uint32_t* n_cells_out, int* dense_out);
+int mg_probe_candidate_pairs(const float* xy, uint32_t n, float cell, uint32_t* pairs, uint32_t cap, uint32_t* n_out);
+int mg_probe_neighbor_lists(const float* xy, uint32_t n, float h, uint32_t* offsets, uint32_t* nbrs, uint32_t cap,
+                            uint32_t* n_edges);
+/* neighbour CSR / ball pair list of the last fluid / ball sub-step taken on this handle */
+int mg_last_neighbor_lists(MgSim* sim, uint32_t* offsets, uint32_t* nbrs, uint32_t cap, uint32_t* n_edges);
+int mg_last_ball_pairs(MgSim* sim, uint32_t* pairs, uint32_t cap, uint32_t* n_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MILLGPU_H */

@@ -1,0 +1,224 @@
+"""ctypes mirror of include/millgpu.h.
+
+`Lib(path, prefix)` binds every entry point of the header from a shared library under a name
+prefix ("mg_" for the CUDA library). The structs below are field-for-field copies of the header,
+which in turn mirrors the reference's Rust types (params.rs, pbf.rs, dem.rs, lib.rs).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+MG_OK = 0
+MG_ERR_INVALID_PARAMS = 1
+MG_ERR_ARG = 2
+MG_ERR_CUDA = 3
+MG_ERR_CAPACITY = 4
+MG_ERR_NO_DEVICE = 5
+MG_ERR_STATE = 6
+
+SPEED_RPM, SPEED_PERCENT_CRITICAL = 0, 1
+DIR_CCW, DIR_CW = 0, 1
+CG_AUTO, CG_OFF, CG_MANUAL = 0, 1, 2
+RHEOLOGY_NEWTONIAN, RHEOLOGY_BINGHAM = 0, 1
+DYE_LEFT_RIGHT, DYE_TOP_BOTTOM, DYE_NONE = 0, 1, 2
+WALL_PARTNER = 0xFFFFFFFF
+WALL_IMPULSE_BINS = 32
+IMPACT_BINS = 12
+SE_BINS = 28
+
+
+class _S(C.Structure):
+    def to_dict(self):
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            if isinstance(v, C.Structure):
+                v = v.to_dict()
+            elif isinstance(v, C.Array):
+                v = list(v)
+            out[name] = v
+        return out
+
+    def copy(self):
+        c = type(self)()
+        C.memmove(C.byref(c), C.byref(self), C.sizeof(self))
+        return c
+
+
+class MillParams(_S):
+    _fields_ = [("diameter_m", C.c_float), ("speed_mode", C.c_uint32), ("speed_value", C.c_float),
+                ("direction", C.c_uint32)]
+
+
+class MediaParams(_S):
+    _fields_ = [(n, C.c_float) for n in (
+        "ball_diameter_m", "fill_fraction", "packing_fraction_2d", "density_kg_m3",
+        "restitution_ball_ball", "restitution_ball_wall", "friction_ball_ball", "friction_ball_wall",
+        "friction_ball_ball_static", "friction_ball_wall_static", "friction_velocity_scale_m_s",
+        "rolling_friction")]
+
+
+class SlurryParams(_S):
+    _fields_ = [("enabled", C.c_uint32), ("fill_fraction", C.c_float), ("density_kg_m3", C.c_float),
+                ("viscosity_pa_s", C.c_float), ("rheology", C.c_uint32), ("yield_stress_pa", C.c_float),
+                ("wall_no_slip", C.c_float), ("ball_no_slip", C.c_float), ("wettability", C.c_float),
+                ("surface_tension_n_m", C.c_float), ("dye_pattern", C.c_uint32)]
+
+
+class LiftersParams(_S):
+    _fields_ = [("count", C.c_uint32), ("height_m", C.c_float), ("base_width_m", C.c_float),
+                ("top_width_m", C.c_float), ("phase_deg", C.c_float)]
+
+
+class SimulationParams(_S):
+    _fields_ = [("resolution", C.c_uint32), ("substeps", C.c_uint32), ("pbf_iterations", C.c_uint32),
+                ("dem_iterations", C.c_uint32), ("time_scale", C.c_float), ("frame_budget_ms", C.c_float),
+                ("max_balls", C.c_uint32), ("reserved0", C.c_uint32), ("seed", C.c_uint64),
+                ("coarse_graining_mode", C.c_uint32), ("coarse_graining_k", C.c_float)]
+
+
+class Params(_S):
+    _fields_ = [("mill", MillParams), ("media", MediaParams), ("slurry", SlurryParams),
+                ("lifters", LiftersParams), ("simulation", SimulationParams)]
+
+
+class Derived(_S):
+    _fields_ = [("critical_speed_rpm", C.c_float), ("rpm", C.c_float), ("percent_critical", C.c_float),
+                ("omega", C.c_float), ("radius_m", C.c_float), ("true_ball_count", C.c_float),
+                ("eff_true_diameter_m", C.c_float), ("eff_diameter_m", C.c_float),
+                ("eff_density_kg_m3", C.c_float), ("eff_ball_count", C.c_uint32),
+                ("eff_scale_factor", C.c_float), ("effective_fluid_resolution", C.c_uint32),
+                ("effective_substeps", C.c_uint32), ("fixed_sub_dt", C.c_float)]
+
+
+class Drum(_S):
+    _fields_ = [("radius_m", C.c_float), ("omega", C.c_float), ("lifters", LiftersParams)]
+
+
+class FluidStepStats(_S):
+    _fields_ = [("viscosity_iterations", C.c_uint32), ("mean_shear_rate_per_s", C.c_float),
+                ("coupling_clamp_hits", C.c_uint32), ("wall_work_j", C.c_float),
+                ("wall_impulse", C.c_float * 2), ("wall_angular_impulse", C.c_float),
+                ("wall_normal_impulse_by_angle", C.c_float * WALL_IMPULSE_BINS),
+                ("ke_delta_noslip_j", C.c_float), ("ke_delta_drag_j", C.c_float),
+                ("ke_delta_buoyancy_j", C.c_float), ("ke_delta_viscosity_j", C.c_float),
+                ("ke_delta_clamp_j", C.c_float)]
+
+
+class DemStepStats(_S):
+    _fields_ = [("wall_work_j", C.c_float), ("collision_count", C.c_uint32),
+                ("impact_energy_histogram", C.c_uint32 * IMPACT_BINS), ("dissipated_energy_j", C.c_float),
+                ("max_substep_displacement_over_diameter", C.c_float), ("coupling_work_j", C.c_float)]
+
+
+class ImpactRecord(_S):
+    _fields_ = [("kind", C.c_uint32), ("ball", C.c_uint32), ("partner", C.c_uint32),
+                ("normal_speed", C.c_float), ("slip_speed", C.c_float), ("restitution", C.c_float)]
+
+
+class StepCounters(_S):
+    _fields_ = [(n, C.c_uint32) for n in (
+        "density_iters", "cg_iters", "n_groups", "n_links", "links_in_range", "n_ball_pairs",
+        "n_fluid_edges", "n_active_contacts")]
+
+
+class BallMaterial(_S):
+    _fields_ = [(n, C.c_float) for n in ("radius", "mass", "inertia", "true_radius")]
+
+
+class FluidMaterial(_S):
+    _fields_ = [(n, C.c_float) for n in ("particle_mass", "h", "rest_density")]
+
+
+class EnergyBudget(_S):
+    _fields_ = [(n, C.c_double) for n in (
+        "elapsed_s", "shaft_work_j", "dem_wall_work_j", "fluid_wall_work_j", "ball_contact_dissipation_j",
+        "fluid_wall_slip_j", "fluid_viscous_j", "fluid_clamp_removed_j", "interface_created_j",
+        "delta_mechanical_j", "unattributed_j", "fluid_wall_angular_impulse")]
+
+
+class Scalars(_S):
+    _fields_ = [("drum_angle", C.c_float), ("power_draw_w", C.c_float), ("torque_nm", C.c_float),
+                ("collision_rate_per_s", C.c_float), ("dissipated_power_w", C.c_float),
+                ("max_substep_displacement_over_diameter", C.c_float), ("coupling_clamp_hits", C.c_uint32),
+                ("viscosity_iterations", C.c_uint32), ("mean_shear_rate_per_s", C.c_float),
+                ("reserved0", C.c_float), ("sim_time", C.c_double)]
+
+
+class Options(_S):
+    _fields_ = [("cg_fp64", C.c_uint32), ("block_threads", C.c_uint32), ("reserved", C.c_uint32 * 6)]
+
+
+P = C.POINTER
+f32p = P(C.c_float)
+u32p = P(C.c_uint32)
+vp = C.c_void_p
+
+# (name, restype, argtypes) of every entry point in include/millgpu.h
+SIGNATURES = [
+    ("sizeof_params", C.c_size_t, []),
+    ("sizeof_fluid_stats", C.c_size_t, []),
+    ("sizeof_dem_stats", C.c_size_t, []),
+    ("params_default", C.c_int, [P(Params)]),
+    ("params_validate", C.c_int, [P(Params), C.c_char_p, C.c_size_t]),
+    ("preset_apply", C.c_int, [P(Params), C.c_char_p]),
+    ("params_derived", C.c_int, [P(Params), P(Derived)]),
+    ("sim_create", C.c_int, [P(Params), P(vp)]),
+    ("sim_create_with_balls", C.c_int, [P(Params), f32p, C.c_uint32, P(vp)]),
+    ("sim_destroy", None, [vp]),
+    ("global_last_error", C.c_char_p, []),
+    ("sim_step", C.c_int, [vp, C.c_float]),
+    ("sim_step_fixed", C.c_int, [vp]),
+    ("sim_reset_frame_stats", C.c_int, [vp]),
+    ("sim_set_params", C.c_int, [vp, P(Params)]),
+    ("sim_fixed_sub_dt", C.c_float, [vp]),
+    ("sim_reset_energy_budget", C.c_int, [vp]),
+    ("coupling_step_recorded", C.c_int, [vp, P(Drum), C.c_float, P(MediaParams), P(SlurryParams), C.c_uint32,
+                                         C.c_uint32, C.c_float, P(FluidStepStats), P(DemStepStats),
+                                         P(ImpactRecord), C.c_uint32, u32p]),
+    ("fluid_step_coupled", C.c_int, [vp, P(Drum), C.c_float, P(SlurryParams), C.c_uint32, C.c_float,
+                                     P(FluidStepStats), f32p, f32p, u32p, f32p]),
+    ("dem_step_recorded", C.c_int, [vp, P(Drum), C.c_float, P(MediaParams), C.c_uint32, C.c_float, f32p, f32p,
+                                    P(DemStepStats), P(ImpactRecord), C.c_uint32, u32p]),
+    ("get_counts", C.c_int, [vp, u32p, u32p]),
+    ("get_balls", C.c_int, [vp, f32p, f32p, f32p, f32p]),
+    ("set_balls", C.c_int, [vp, C.c_uint32, f32p, f32p, f32p, f32p]),
+    ("get_ball_material", C.c_int, [vp, P(BallMaterial)]),
+    ("set_ball_material", C.c_int, [vp, P(BallMaterial)]),
+    ("get_fluid", C.c_int, [vp, f32p, f32p, f32p, f32p, u32p]),
+    ("set_fluid", C.c_int, [vp, C.c_uint32, f32p, f32p, f32p, f32p]),
+    ("get_fluid_material", C.c_int, [vp, P(FluidMaterial)]),
+    ("set_fluid_material", C.c_int, [vp, P(FluidMaterial)]),
+    ("get_scalars", C.c_int, [vp, P(Scalars)]),
+    ("energy_budget", C.c_int, [vp, P(EnergyBudget)]),
+    ("state_hash", C.c_int, [vp, C.c_int, P(C.c_uint64)]),
+    ("mixing_index", C.c_int, [vp, f32p, P(C.c_int)]),
+    ("stress_histogram_rate", C.c_int, [vp, P(C.c_double)]),
+    ("last_step_stats", C.c_int, [vp, P(FluidStepStats), P(DemStepStats), P(StepCounters)]),
+    ("probe_grid", C.c_int, [f32p, C.c_uint32, C.c_float, P(C.c_int32), P(C.c_int64), u32p, C.c_uint32, u32p,
+                             u32p, P(C.c_int)]),
+    ("probe_candidate_pairs", C.c_int, [f32p, C.c_uint32, C.c_float, u32p, C.c_uint32, u32p]),
+    ("probe_neighbor_lists", C.c_int, [f32p, C.c_uint32, C.c_float, u32p, u32p, C.c_uint32, u32p]),
+    ("last_neighbor_lists", C.c_int, [vp, u32p, u32p, C.c_uint32, u32p]),
+    ("last_ball_pairs", C.c_int, [vp, u32p, C.c_uint32, u32p]),
+]
+
+# entry points only the device library exports
+DEVICE_ONLY = [
+    ("last_error", C.c_char_p, [vp]),
+    ("sim_set_options", C.c_int, [vp, P(Options)]),
+]
+
+
+class Lib:
+    """Binds the header's entry points of one shared library under `prefix`."""
+
+    def __init__(self, path: str, prefix: str, extra=()):
+        self.path = path
+        self.prefix = prefix
+        self.dll = C.CDLL(path)
+        for name, res, args in list(SIGNATURES) + list(extra):
+            fn = getattr(self.dll, prefix + name)
+            fn.restype = res
+            fn.argtypes = args
+            setattr(self, name, fn)

@@ -1,0 +1,1349 @@
+// Oracle (test infrastructure only): pbf.rs step_coupled and helpers, mac/lubrication.rs subset,
+// dem.rs step_recorded. Each function cites the reference lines it restates.
+#include <algorithm>
+#include <cstring>
+
+#include "oracle_core.hpp"
+
+namespace orc {
+
+static const float GRAVITY = -9.81f;
+
+// ------------------------------------------------------------------ pbf.rs:45-116 constants
+static const float EPSILON_RELAX = 200.0f;
+static const uint32_t ADAPTIVE_MAX_EXTRA_ITERATIONS = 6;
+static const float COMPRESSION_CONVERGENCE_TOLERANCE = 0.02f;
+static const float OVERLAP_PUSH_MARGIN = 0.05f;
+static const float REFERENCE_SURFACE_TENSION_N_M = 0.072f;
+static const float COHESION_ACCEL_FACTOR = 2.0f;
+static const float ADHESION_ACCEL_FACTOR = 2.0f;
+static const float VISCOSITY_CG_TOLERANCE = 1e-3f;
+static const uint32_t VISCOSITY_CG_MAX_ITERS = 50;
+static const float VISCOSITY_ETA_FACTOR = 0.01f;
+static const float BALL_FORM_DRAG_COEFFICIENT = 1.0f;
+static const float CENTRAL_VISCOSITY_FACTOR = 4.0f;
+static const float BALL_BC_GAIN = 0.5f;
+static const float BINGHAM_PLASTIC_RATIO = 100.0f;
+static const float SQUEEZE_GAIN = 1.0f;
+static const float SQUEEZE_STIFFNESS_CAP = 8.0f;
+static const double MIN_FILM_GAP_RATIO = 0.02;
+static const float F_CLAMP_G_MULTIPLE = 60.0f;
+static const float FLUID_SPEED_SAFETY_FACTOR = 5.0f;
+
+// pbf.rs:119-181 kernels
+static float poly6(float r2, float h) {
+  if (r2 >= h * h || r2 < 0.0f) return 0.0f;
+  float h2 = h * h;
+  float term = h2 - r2;
+  return 4.0f / (PI_F * powi8(h)) * term * term * term;
+}
+static Vec2 spiky_grad(Vec2 delta, float r, float h) {
+  if (r <= 1e-9f || r >= h) return Vec2();
+  float coeff = -30.0f / (PI_F * powi5(h)) * (h - r) * (h - r);
+  return (delta / r) * coeff;
+}
+static float cohesion_kernel(float r, float h) {
+  if (r <= 0.0f || r >= h) return 0.0f;
+  float coeff = 35840.0f / (209.0f * PI_F * powi8(h));
+  float term = powi3(h - r) * powi3(r);
+  if (r <= 0.5f * h) return coeff * (2.0f * term - powi6(h) / 64.0f);
+  return coeff * term;
+}
+static float adhesion_kernel(float r, float h) {
+  if (r <= 0.5f * h || r >= h) return 0.0f;
+  float coeff = 35840.0f / (163.0f * PI_F * powi8(h));
+  return coeff * powi3(h - r) * powi3(r);
+}
+
+// pbf.rs:190-219
+static uint32_t boundary_points_per_ball(float ball_radius, float dx) {
+  float circumference = TAU_F * ball_radius;
+  return std::max(f2u_sat(std::round(circumference / dx)), 6u);
+}
+static std::vector<Vec2> ball_boundary_particles(const Balls& b, float dx) {
+  std::vector<Vec2> out;
+  if (b.len() == 0 || b.radius <= 0.0f || dx <= 0.0f) return out;
+  uint32_t count = boundary_points_per_ball(b.radius, dx);
+  std::vector<Vec2> offsets(count);
+  for (uint32_t k = 0; k < count; ++k) {
+    float angle = TAU_F * (float)k / (float)count;
+    offsets[k] = Vec2(std::cos(angle), std::sin(angle)) * b.radius;
+  }
+  out.reserve(b.len() * count);
+  for (size_t i = 0; i < b.len(); ++i)
+    for (uint32_t k = 0; k < count; ++k) out.push_back(b.x[i] + offsets[k]);
+  return out;
+}
+
+// pbf.rs:262-288
+void neighbor_lists(const std::vector<Vec2>& x, float h, std::vector<uint32_t>* offsets,
+                    std::vector<uint32_t>* nbrs) {
+  UniformGrid g = UniformGrid::build(x, h);
+  size_t n = x.size();
+  std::vector<std::pair<uint32_t, uint32_t>> edges;
+  g.for_each_candidate_pair([&](uint32_t i, uint32_t j) {
+    if ((x[i] - x[j]).length_squared() <= h * h) {
+      edges.push_back({i, j});
+      edges.push_back({j, i});
+    }
+  });
+  offsets->assign(n + 1, 0);
+  for (auto& e : edges) (*offsets)[e.first + 1] += 1;
+  for (size_t k = 1; k < offsets->size(); ++k) (*offsets)[k] += (*offsets)[k - 1];
+  std::vector<uint32_t> cursor = *offsets;
+  nbrs->assign(edges.size(), 0);
+  for (auto& e : edges) { (*nbrs)[cursor[e.first]] = e.second; cursor[e.first] += 1; }
+}
+
+struct Nbr {
+  std::vector<uint32_t> off, idx;
+  size_t b(size_t i) const { return off[i]; }
+  size_t e(size_t i) const { return off[i + 1]; }
+};
+
+// pbf.rs:292-294 (sequential f32 sum) and its f64 counterpart
+static float dot_f32(const std::vector<Vec2>& a, const std::vector<Vec2>& b) {
+  float s = 0.0f;
+  for (size_t i = 0; i < a.size(); ++i) s += a[i].dot(b[i]);
+  return s;
+}
+static double dot_f64(const std::vector<Vec2>& a, const std::vector<Vec2>& b) {
+  double s = 0.0;
+  for (size_t i = 0; i < a.size(); ++i) s += (double)a[i].x * (double)b[i].x + (double)a[i].y * (double)b[i].y;
+  return s;
+}
+
+// pbf.rs:312-351
+struct ViscWeights { std::vector<float> w; std::vector<Vec2> dir; };
+static ViscWeights morris_weights(const std::vector<Vec2>& x, const Nbr& nb, const std::vector<float>& density,
+                                  float mass, const std::vector<float>& mu, float h) {
+  float eta2 = VISCOSITY_ETA_FACTOR * h * h;
+  ViscWeights vw;
+  vw.w.assign(nb.idx.size(), 0.0f);
+  vw.dir.assign(nb.idx.size(), Vec2());
+  for (size_t i = 0; i < x.size(); ++i) {
+    float rho_i = fmax_r(density[i], 1e-6f);
+    for (size_t k = nb.b(i); k < nb.e(i); ++k) {
+      size_t ju = nb.idx[k];
+      float rho_j = fmax_r(density[ju], 1e-6f);
+      Vec2 delta = x[i] - x[ju];
+      float r = delta.length();
+      Vec2 grad = spiky_grad(delta, r, h);
+      float numerator = (mass * (mu[i] + mu[ju]) / (rho_i * rho_j)) * std::fabs(delta.dot(grad));
+      vw.w[k] = numerator / (delta.length_squared() + eta2);
+      vw.dir[k] = r > 1e-9f ? delta / r : Vec2(1.0f, 0.0f);
+    }
+  }
+  return vw;
+}
+
+// pbf.rs:359-377
+static void laplacian_apply_into(const Nbr& nb, const ViscWeights& w, const Vec2* v, size_t n, Vec2* out) {
+  for (size_t i = 0; i < n; ++i) {
+    Vec2 sum;
+    for (size_t k = nb.b(i); k < nb.e(i); ++k) {
+      size_t j = nb.idx[k];
+      Vec2 e = w.dir[k];
+      sum += (CENTRAL_VISCOSITY_FACTOR * w.w[k] * e.dot(v[i] - v[j])) * e;
+    }
+    out[i] = sum;
+  }
+}
+static float viscosity_diag(float sum_w) { return 0.5f * CENTRAL_VISCOSITY_FACTOR * sum_w; }
+
+// pbf.rs:423-480 (fluid-only CG); `fp64` selects f64 inner products and norms.
+static uint32_t solve_implicit_viscosity(const Nbr& nb, const ViscWeights& w, std::vector<Vec2>* vp, float dt,
+                                         bool fp64) {
+  std::vector<Vec2>& v = *vp;
+  size_t n = v.size();
+  double b_norm = fp64 ? std::sqrt(dot_f64(v, v)) : (double)std::sqrt(dot_f32(v, v));
+  if (b_norm <= 0.0 || !std::isfinite(b_norm)) return 0;
+  float target_f = VISCOSITY_CG_TOLERANCE * (float)b_norm;
+  double target_d = (double)VISCOSITY_CG_TOLERANCE * b_norm;
+  std::vector<Vec2> lv(n), ax(n), r(n), p, ap(n);
+  auto apply = [&](const std::vector<Vec2>& in, std::vector<Vec2>& out) {
+    laplacian_apply_into(nb, w, in.data(), n, lv.data());
+    for (size_t i = 0; i < n; ++i) out[i] = in[i] + dt * lv[i];
+  };
+  apply(v, ax);
+  for (size_t i = 0; i < n; ++i) r[i] = v[i] - ax[i];
+  p = r;
+  if (!fp64) {
+    float rs_old = dot_f32(r, r);
+    if (std::sqrt(rs_old) <= target_f) return 0;
+    for (uint32_t iter = 1; iter <= VISCOSITY_CG_MAX_ITERS; ++iter) {
+      apply(p, ap);
+      float p_ap = dot_f32(p, ap);
+      if (p_ap <= 0.0f || !std::isfinite(p_ap)) return iter;
+      float alpha = rs_old / p_ap;
+      for (size_t i = 0; i < n; ++i) { v[i] += alpha * p[i]; r[i] -= alpha * ap[i]; }
+      float rs_new = dot_f32(r, r);
+      if (std::sqrt(rs_new) <= target_f) return iter;
+      float beta = rs_new / rs_old;
+      for (size_t i = 0; i < n; ++i) p[i] = r[i] + beta * p[i];
+      rs_old = rs_new;
+    }
+  } else {
+    double rs_old = dot_f64(r, r);
+    if (std::sqrt(rs_old) <= target_d) return 0;
+    for (uint32_t iter = 1; iter <= VISCOSITY_CG_MAX_ITERS; ++iter) {
+      apply(p, ap);
+      double p_ap = dot_f64(p, ap);
+      if (p_ap <= 0.0 || !std::isfinite(p_ap)) return iter;
+      float alpha = (float)(rs_old / p_ap);
+      for (size_t i = 0; i < n; ++i) { v[i] += alpha * p[i]; r[i] -= alpha * ap[i]; }
+      double rs_new = dot_f64(r, r);
+      if (std::sqrt(rs_new) <= target_d) return iter;
+      float beta = (float)(rs_new / rs_old);
+      for (size_t i = 0; i < n; ++i) p[i] = r[i] + beta * p[i];
+      rs_old = rs_new;
+    }
+  }
+  return VISCOSITY_CG_MAX_ITERS;
+}
+
+struct BoundaryGroup { uint32_t fluid, ball; float c; Vec2 lever_c; float lever2_c; };
+struct SqueezeLink { uint32_t ball, other; Vec2 n; float c; };
+
+// mac/lubrication.rs:19-115 (the subset pbf.rs:544-625 uses)
+static const double H_START = 8.0;
+struct SqueezeFilm {
+  double r, c1, c2, prefactor;
+  SqueezeFilm(double k1, double k2, double nu) {
+    r = 1.0 / (k1 + k2);
+    double r3 = r * (r * r);
+    double q = r3 * (k1 * (k1 * k1) + k2 * (k2 * k2));
+    c1 = 0.788 + 0.265 * q;
+    c2 = dmax_r(0.006 + 0.057 * (q - 0.25), 0.0);
+    prefactor = 3.0 * std::sqrt(2.0) * M_PI * nu * std::pow(r, 1.5);
+  }
+  double coefficient(double h) const {
+    double eps = h / r;
+    return prefactor / (h * std::sqrt(h)) * (1.0 + c1 * eps + c2 * eps * eps);
+  }
+};
+static double resolved_ratio(double h_cells) {
+  static const double T[6][2] = {{0.0, 0.0}, {0.5, 0.06}, {1.0, 0.25}, {2.0, 0.90}, {4.0, 0.99}, {8.0, 1.0}};
+  if (h_cells >= 8.0) return 1.0;
+  double h = dmax_r(h_cells, 0.0);
+  for (int k = 0; k < 5; ++k) {
+    if (h <= T[k + 1][0]) {
+      double t = (h - T[k][0]) / (T[k + 1][0] - T[k][0]);
+      return T[k][1] + t * (T[k + 1][1] - T[k][1]);
+    }
+  }
+  return 1.0;
+}
+
+// pbf.rs:544-625
+static std::vector<SqueezeLink> squeeze_links(const Balls& balls, float drum_radius, float dx, float mu, float dt,
+                                              const std::vector<Vec2>* closing, size_t* in_range_out) {
+  std::vector<SqueezeLink> out;
+  size_t in_range = 0;
+  float r = balls.radius;
+  *in_range_out = 0;
+  if (balls.len() == 0 || r <= 0.0f || mu <= 0.0f) return out;
+  double a = (double)r, b = (double)drum_radius, dxd = (double)dx, mud = (double)mu;
+  float gain = SQUEEZE_GAIN;
+  float reach = (float)(H_START * dxd);
+  float c_max = SQUEEZE_STIFFNESS_CAP * balls.mass / fmax_r(dt, 1e-12f);
+  UniformGrid grid = UniformGrid::build(balls.x, 2.0f * r + reach);
+  float range2 = (2.0f * r + reach) * (2.0f * r + reach) * (1.0f + 1e-4f);
+  SqueezeFilm pair_film(1.0 / a, 1.0 / a, mud);
+  SqueezeFilm wall_film(1.0 / a, -1.0 / b, mud);
+  for (size_t i = 0; i < balls.len(); ++i) {
+    Vec2 xi = balls.x[i];
+    if (!xi.is_finite()) continue;
+    grid.for_each_near(xi, [&](uint32_t j) {
+      if ((size_t)j <= i) return;
+      Vec2 e = balls.x[j] - xi;
+      if (e.length_squared() >= range2 || !e.is_finite()) return;
+      float dist = e.length();
+      float gap = dist - 2.0f * r;
+      if (gap >= reach || dist < 1e-9f) return;
+      in_range += 1;
+      Vec2 n = e / dist;
+      if (closing && n.dot((*closing)[i] - (*closing)[j]) <= 0.0f) return;
+      double weight = 1.0 - resolved_ratio((double)gap / dxd);
+      double hh = dmax_r((double)gap, MIN_FILM_GAP_RATIO * a);
+      double c = weight * pair_film.coefficient(hh);
+      out.push_back({(uint32_t)i, j, n, fmin_r(gain * (float)c, c_max)});
+    });
+    float dist = xi.length();
+    float gap = drum_radius - r - dist;
+    if (gap < reach && dist > 1e-9f) {
+      in_range += 1;
+      Vec2 n = xi / dist;
+      if (closing && n.dot((*closing)[i]) <= 0.0f) continue;
+      double weight = 1.0 - resolved_ratio((double)gap / dxd);
+      double hh = dmax_r((double)gap, MIN_FILM_GAP_RATIO * a);
+      double c = weight * wall_film.coefficient(hh);
+      out.push_back({(uint32_t)i, WALL_ID, n, fmin_r(gain * (float)c, c_max)});
+    }
+  }
+  *in_range_out = in_range;
+  return out;
+}
+
+// pbf.rs:641-791 (joint fluid + ball Jacobi-PCG); `fp64` selects f64 inner products and norms.
+static uint32_t solve_viscosity_with_balls(const Nbr& nb, const ViscWeights& weights,
+                                           const std::vector<BoundaryGroup>& groups,
+                                           const std::vector<SqueezeLink>& links, float mass, float ball_mass_,
+                                           float ball_inertia_, float dt, const std::vector<Vec2>& guess,
+                                           std::vector<Vec2>* vp, std::vector<Vec2>* ball_vp,
+                                           std::vector<float>* ball_wp, bool fp64) {
+  std::vector<Vec2>& v = *vp;
+  std::vector<Vec2>& ball_v = *ball_vp;
+  std::vector<float>& ball_w = *ball_wp;
+  size_t n = v.size(), nbn = ball_v.size(), len = n + 2 * nbn;
+  auto perp = [](Vec2 l) { return Vec2(-l.y, l.x); };
+  std::vector<Vec2> x;
+  x.reserve(len);
+  if (guess.size() == n) {
+    for (size_t i = 0; i < n; ++i) x.push_back(v[i] + guess[i]);
+  } else {
+    for (size_t i = 0; i < n; ++i) x.push_back(v[i]);
+  }
+  for (size_t i = 0; i < nbn; ++i) x.push_back(ball_v[i]);
+  for (size_t i = 0; i < nbn; ++i) x.push_back(Vec2(ball_w[i], 0.0f));
+  std::vector<Vec2> b;
+  b.reserve(len);
+  for (size_t i = 0; i < n; ++i) b.push_back(mass * v[i]);
+  for (size_t i = 0; i < nbn; ++i) b.push_back(ball_mass_ * ball_v[i]);
+  for (size_t i = 0; i < nbn; ++i) b.push_back(Vec2(ball_inertia_ * ball_w[i], 0.0f));
+  std::vector<float> diag(len, 0.0f);
+  for (size_t i = 0; i < n; ++i) {
+    float sw = 0.0f;
+    for (size_t k = nb.b(i); k < nb.e(i); ++k) sw += weights.w[k];
+    diag[i] = mass * (1.0f + dt * viscosity_diag(sw));
+  }
+  for (size_t bi = 0; bi < nbn; ++bi) { diag[n + bi] = ball_mass_; diag[n + nbn + bi] = ball_inertia_; }
+  for (const auto& g : groups) {
+    float d = dt * mass * g.c;
+    diag[g.fluid] += d;
+    diag[n + g.ball] += d;
+    diag[n + nbn + g.ball] += dt * mass * g.lever2_c;
+  }
+  for (const auto& l : links) {
+    float d = dt * l.c;
+    diag[n + l.ball] += d;
+    if (l.other != WALL_ID) diag[n + l.other] += d;
+  }
+  std::vector<float> inv_diag(len);
+  for (size_t i = 0; i < len; ++i) inv_diag[i] = 1.0f / fmax_r(diag[i], 1e-20f);
+  std::vector<Vec2> lv(n);
+  auto apply = [&](const std::vector<Vec2>& xx, std::vector<Vec2>& out) {
+    laplacian_apply_into(nb, weights, xx.data(), n, lv.data());
+    for (size_t i = 0; i < n; ++i) out[i] = mass * (xx[i] + dt * lv[i]);
+    for (size_t bi = 0; bi < nbn; ++bi) {
+      out[n + bi] = ball_mass_ * xx[n + bi];
+      out[n + nbn + bi] = Vec2(ball_inertia_ * xx[n + nbn + bi].x, 0.0f);
+    }
+    for (const auto& g : groups) {
+      size_t i = g.fluid, bi = g.ball;
+      Vec2 vb = xx[n + bi];
+      float w = xx[n + nbn + bi].x;
+      Vec2 rel = xx[i] - vb;
+      float k = dt * mass;
+      Vec2 d = k * (g.c * rel - w * perp(g.lever_c));
+      out[i] += d;
+      out[n + bi] -= d;
+      out[n + nbn + bi].x -= k * (cross2(g.lever_c, rel) - w * g.lever2_c);
+    }
+    for (const auto& l : links) {
+      size_t i = l.ball;
+      Vec2 rel = xx[n + l.ball];
+      if (l.other != WALL_ID) rel = rel - xx[n + l.other];
+      Vec2 d = (dt * l.c * l.n.dot(rel)) * l.n;
+      out[n + i] += d;
+      if (l.other != WALL_ID) out[n + l.other] -= d;
+    }
+  };
+  auto res_norm_f = [&](const std::vector<Vec2>& r) {
+    float s = 0.0f;
+    for (size_t i = 0; i < r.size(); ++i) s += inv_diag[i] * r[i].length_squared();
+    return std::sqrt(s);
+  };
+  auto res_norm_d = [&](const std::vector<Vec2>& r) {
+    double s = 0.0;
+    for (size_t i = 0; i < r.size(); ++i)
+      s += (double)inv_diag[i] * ((double)r[i].x * (double)r[i].x + (double)r[i].y * (double)r[i].y);
+    return std::sqrt(s);
+  };
+  std::vector<Vec2> ax(len);
+  apply(x, ax);
+  std::vector<Vec2> r(len), z(len);
+  for (size_t i = 0; i < len; ++i) r[i] = b[i] - ax[i];
+  for (size_t i = 0; i < len; ++i) z[i] = r[i] * inv_diag[i];
+  uint32_t iters = 0;
+  if (!fp64) {
+    float b_norm = res_norm_f(b);
+    if (b_norm > 0.0f && std::isfinite(b_norm) && res_norm_f(r) > VISCOSITY_CG_TOLERANCE * b_norm) {
+      float target = VISCOSITY_CG_TOLERANCE * b_norm;
+      std::vector<Vec2> p = z, ap(len);
+      float rz_old = dot_f32(r, z);
+      for (uint32_t iter = 1; iter <= 4 * VISCOSITY_CG_MAX_ITERS; ++iter) {
+        iters = iter;
+        apply(p, ap);
+        float p_ap = dot_f32(p, ap);
+        if (p_ap <= 0.0f || !std::isfinite(p_ap)) break;
+        float alpha = rz_old / p_ap;
+        for (size_t i = 0; i < len; ++i) { x[i] += alpha * p[i]; r[i] -= alpha * ap[i]; }
+        if (res_norm_f(r) <= target) break;
+        for (size_t i = 0; i < len; ++i) z[i] = r[i] * inv_diag[i];
+        float rz_new = dot_f32(r, z);
+        float beta = rz_new / rz_old;
+        for (size_t i = 0; i < len; ++i) p[i] = z[i] + beta * p[i];
+        rz_old = rz_new;
+      }
+    }
+  } else {
+    double b_norm = res_norm_d(b);
+    if (b_norm > 0.0 && std::isfinite(b_norm) && res_norm_d(r) > (double)VISCOSITY_CG_TOLERANCE * b_norm) {
+      double target = (double)VISCOSITY_CG_TOLERANCE * b_norm;
+      std::vector<Vec2> p = z, ap(len);
+      double rz_old = dot_f64(r, z);
+      for (uint32_t iter = 1; iter <= 4 * VISCOSITY_CG_MAX_ITERS; ++iter) {
+        iters = iter;
+        apply(p, ap);
+        double p_ap = dot_f64(p, ap);
+        if (p_ap <= 0.0 || !std::isfinite(p_ap)) break;
+        float alpha = (float)(rz_old / p_ap);
+        for (size_t i = 0; i < len; ++i) { x[i] += alpha * p[i]; r[i] -= alpha * ap[i]; }
+        if (res_norm_d(r) <= target) break;
+        for (size_t i = 0; i < len; ++i) z[i] = r[i] * inv_diag[i];
+        double rz_new = dot_f64(r, z);
+        float beta = (float)(rz_new / rz_old);
+        for (size_t i = 0; i < len; ++i) p[i] = z[i] + beta * p[i];
+        rz_old = rz_new;
+      }
+    }
+  }
+  for (size_t i = 0; i < n; ++i) v[i] = x[i];
+  for (size_t i = 0; i < nbn; ++i) ball_v[i] = x[n + i];
+  for (size_t i = 0; i < nbn; ++i) ball_w[i] = x[n + nbn + i].x;
+  return iters;
+}
+
+// pbf.rs:800-868
+static std::vector<float> shear_rates(const std::vector<Vec2>& x, const std::vector<Vec2>& v, const Nbr& nb,
+                                      const std::vector<float>& density, float mass, float h) {
+  size_t n = x.size();
+  std::vector<float> out(n, 0.0f);
+  for (size_t i = 0; i < n; ++i) {
+    float gxx = 0.0f, gxy = 0.0f, gyx = 0.0f, gyy = 0.0f;
+    for (size_t k = nb.b(i); k < nb.e(i); ++k) {
+      size_t ju = nb.idx[k];
+      Vec2 delta = x[i] - x[ju];
+      float r = delta.length();
+      Vec2 grad = spiky_grad(delta, r, h);
+      float coeff = mass / fmax_r(density[ju], 1e-6f);
+      Vec2 dv = v[ju] - v[i];
+      gxx += coeff * dv.x * grad.x;
+      gxy += coeff * dv.x * grad.y;
+      gyx += coeff * dv.y * grad.x;
+      gyy += coeff * dv.y * grad.y;
+    }
+    float dxy = 0.5f * (gxy + gyx);
+    out[i] = std::sqrt(2.0f * (gxx * gxx + gyy * gyy + 2.0f * dxy * dxy));
+  }
+  return out;
+}
+static float mean_shear_rate(const std::vector<Vec2>& x, const std::vector<Vec2>& v, const Nbr& nb,
+                             const std::vector<float>& density, float mass, float h) {
+  std::vector<float> rates = shear_rates(x, v, nb, density, mass, h);
+  float sum = 0.0f;
+  uint32_t count = 0;
+  for (float g : rates)
+    if (std::isfinite(g)) { sum += g; count += 1; }
+  return count == 0 ? 0.0f : sum / (float)count;
+}
+static std::vector<float> bingham_viscosity(const std::vector<float>& rates, float mu, float tau_y) {
+  float gamma0 = tau_y / (BINGHAM_PLASTIC_RATIO * mu);
+  std::vector<float> out(rates.size());
+  for (size_t i = 0; i < rates.size(); ++i) {
+    float g = std::isfinite(rates[i]) ? rates[i] : 0.0f;
+    float extra = g < 1e-4f * gamma0 ? tau_y / gamma0 : tau_y * (1.0f - std::exp(-g / gamma0)) / g;
+    out[i] = mu + extra;
+  }
+  return out;
+}
+
+// pbf.rs:924-926, 957-996
+static double kinetic_energy_f64(const std::vector<Vec2>& v, float mass) {
+  double s = 0.0;
+  for (const Vec2& q : v) s += (double)q.length_squared();
+  return 0.5 * (double)mass * s;
+}
+static float impulse_clamp(float ball_mass_, float dt) { return F_CLAMP_G_MULTIPLE * ball_mass_ * 9.81f * dt; }
+static float fluid_speed_clamp_v_max(const Drum& d) {
+  return FLUID_SPEED_SAFETY_FACTOR * (std::fabs(d.omega) * d.radius_m + std::sqrt(4.0f * std::fabs(GRAVITY) * d.radius_m));
+}
+static void clamp_fluid_speed(std::vector<Vec2>* v, float v_max) {
+  for (Vec2& q : *v) {
+    float speed = q.length();
+    if (!std::isfinite(speed)) q = Vec2();
+    else if (speed > v_max) q *= v_max / speed;
+  }
+}
+
+// pbf.rs:1124-1150
+std::vector<float> fluid_densities(const Fluid& f) {
+  size_t n = f.len();
+  std::vector<float> density(n, 0.0f);
+  if (n == 0) return density;
+  UniformGrid g = UniformGrid::build(f.x, f.h);
+  float self_c = f.particle_mass * poly6(0.0f, f.h);
+  std::fill(density.begin(), density.end(), self_c);
+  g.for_each_candidate_pair([&](uint32_t i, uint32_t j) {
+    float r2 = (f.x[i] - f.x[j]).length_squared();
+    float w = poly6(r2, f.h);
+    density[i] += f.particle_mass * w;
+    density[j] += f.particle_mass * w;
+  });
+  return density;
+}
+double fluid_mechanical_energy(const Fluid& f) {
+  double py = 0.0;
+  for (const Vec2& p : f.x) py += (double)p.y;
+  double potential = py * (double)f.particle_mass * (double)std::fabs(GRAVITY);
+  return kinetic_energy_f64(f.v, f.particle_mass) + potential;
+}
+
+// pbf.rs:1174-2365
+void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const SlurryParams& slurry,
+                        uint32_t iterations, float dt, const Balls& balls, CouplingImpulses* coupling,
+                        FluidStepStats* stats_out, StepCounters* ctr, Debug* dbg, const SolveOptions& opt) {
+  size_t n = fl->len();
+  coupling->zeros(balls.len());
+  *stats_out = FluidStepStats();
+  if (n == 0 || dt <= 0.0f) return;
+  std::vector<Vec2>& X = fl->x;
+  std::vector<Vec2>& V = fl->v;
+  // step 0: sanitize
+  for (size_t i = 0; i < n; ++i)
+    if (!X[i].is_finite() || !V[i].is_finite()) { X[i] = Vec2(); V[i] = Vec2(); }
+  float h = fl->h, rest_density = fl->rest_density, mass = fl->particle_mass;
+  bool have_ball_grid = balls.len() > 0;
+  UniformGrid ball_grid;
+  if (have_ball_grid) {
+    float contact_radius = balls.radius + OVERLAP_PUSH_MARGIN * h;
+    ball_grid = UniformGrid::build(balls.x, fmax_r(fmax_r(2.0f * balls.radius, contact_radius), 1e-6f));
+  }
+  // step 1: predict
+  std::vector<Vec2> x0 = X;
+  for (size_t i = 0; i < n; ++i) {
+    V[i].y += GRAVITY * dt;
+    X[i] += V[i] * dt;
+  }
+  float drum_angle_next = drum_angle + drum.omega * dt;
+  // step 2: grid + neighbour lists
+  UniformGrid grid = UniformGrid::build(X, h);
+  Nbr nb;
+  {
+    std::vector<std::pair<uint32_t, uint32_t>> edges;
+    grid.for_each_candidate_pair([&](uint32_t i, uint32_t j) {
+      if ((X[i] - X[j]).length_squared() <= h * h) { edges.push_back({i, j}); edges.push_back({j, i}); }
+    });
+    nb.off.assign(n + 1, 0);
+    for (auto& e : edges) nb.off[e.first + 1] += 1;
+    for (size_t k = 1; k < nb.off.size(); ++k) nb.off[k] += nb.off[k - 1];
+    std::vector<uint32_t> cursor = nb.off;
+    nb.idx.assign(edges.size(), 0);
+    for (auto& e : edges) { nb.idx[cursor[e.first]] = e.second; cursor[e.first] += 1; }
+  }
+  if (ctr) ctr->n_fluid_edges = (uint32_t)nb.idx.size();
+  if (dbg) { dbg->nbr_offsets = nb.off; dbg->nbrs = nb.idx; }
+  // step 3: density constraint iterations
+  std::vector<float> density(n, 0.0f), lambda(n, 0.0f);
+  std::vector<Vec2> delta_p(n), grad_cache(nb.idx.size());
+  uint32_t base_iterations = std::max(iterations, 1u);
+  uint32_t iter_count = 0;
+  for (;;) {
+    float max_c = 0.0f;
+    for (size_t i = 0; i < n; ++i) {
+      float rho = mass * poly6(0.0f, h);
+      Vec2 grad_self;
+      float sum_grad_sq = 0.0f;
+      for (size_t k = nb.b(i); k < nb.e(i); ++k) {
+        size_t ju = nb.idx[k];
+        Vec2 delta = X[i] - X[ju];
+        float r2 = delta.length_squared();
+        rho += mass * poly6(r2, h);
+        float r = delta.length();
+        Vec2 raw_grad = spiky_grad(delta, r, h);
+        grad_cache[k] = raw_grad;
+        Vec2 grad = raw_grad * (mass / rest_density);
+        grad_self += grad;
+        sum_grad_sq += grad.length_squared();
+      }
+      density[i] = rho;
+      float c_i = fmax_r(density[i] / rest_density - 1.0f, 0.0f);
+      max_c = fmax_r(max_c, c_i);
+      sum_grad_sq += grad_self.length_squared();
+      lambda[i] = -c_i / (sum_grad_sq + EPSILON_RELAX);
+    }
+    for (size_t i = 0; i < n; ++i) {
+      Vec2 sum;
+      for (size_t k = nb.b(i); k < nb.e(i); ++k) {
+        size_t ju = nb.idx[k];
+        sum += (lambda[i] + lambda[ju]) * grad_cache[k];
+      }
+      delta_p[i] = sum * (mass / rest_density);
+    }
+    for (size_t i = 0; i < n; ++i) X[i] += delta_p[i];
+    iter_count += 1;
+    bool converged = max_c <= COMPRESSION_CONVERGENCE_TOLERANCE;
+    if ((iter_count >= base_iterations && converged) || iter_count >= base_iterations + ADAPTIVE_MAX_EXTRA_ITERATIONS)
+      break;
+  }
+  if (ctr) ctr->density_iters = iter_count;
+  // step 3.5: ball overlap push
+  std::vector<Vec2> push_velocity_excess(n);
+  if (have_ball_grid) {
+    float contact_radius = balls.radius + OVERLAP_PUSH_MARGIN * h;
+    std::vector<uint32_t> nearby;
+    for (size_t i = 0; i < n; ++i) {
+      nearby.clear();
+      ball_grid.for_each_near(X[i], [&](uint32_t b) { nearby.push_back(b); });
+      for (uint32_t bb : nearby) {
+        size_t b = bb;
+        Vec2 delta = X[i] - balls.x[b];
+        float dist = delta.length();
+        if (std::isnan(dist) || dist >= contact_radius) continue;
+        Vec2 n_hat = dist > 1e-9f ? delta / dist : Vec2(1.0f, 0.0f);
+        float push_mag = fmin_r(contact_radius - dist, 0.5f * balls.radius);
+        Vec2 push = push_mag * n_hat;
+        X[i] += push;
+        Vec2 lever = n_hat * balls.radius;
+        Vec2 v_surface = balls.v[b] + balls.omega[b] * Vec2(-lever.y, lever.x);
+        float arrest_speed = fmax_r(-(V[i] - v_surface).dot(n_hat), 0.0f);
+        float full_impulse_mag = mass * push_mag / dt;
+        float reduced_mass = balls.mass > 0.0f ? (mass * balls.mass) / (mass + balls.mass) : mass;
+        float impulse_mag = fmin_r(full_impulse_mag, reduced_mass * arrest_speed);
+        push_velocity_excess[i] += ((full_impulse_mag - impulse_mag) / mass) * n_hat;
+        Vec2 reaction = -impulse_mag * n_hat;
+        coupling->impulses[b] += reaction;
+        coupling->fluid_momentum_change += impulse_mag * n_hat;
+        coupling->angular_impulses[b] += cross2(lever, reaction);
+      }
+    }
+  }
+  // step 3.6a: cohesion
+  std::vector<Vec2> cohesion_dv(n);
+  float cohesion_accel = (fmax_r(slurry.surface_tension_n_m, 0.0f) / REFERENCE_SURFACE_TENSION_N_M) *
+                         COHESION_ACCEL_FACTOR * std::fabs(GRAVITY);
+  if (cohesion_accel > 0.0f) {
+    for (size_t i = 0; i < n; ++i) {
+      Vec2 pull;
+      for (size_t k = nb.b(i); k < nb.e(i); ++k) {
+        size_t ju = nb.idx[k];
+        Vec2 delta = X[i] - X[ju];
+        float r = delta.length();
+        if (r <= 1e-9f) continue;
+        float w = mass * cohesion_kernel(r, h) / rest_density;
+        pull -= w * (delta / r);
+      }
+      cohesion_dv[i] = cohesion_accel * pull * dt;
+    }
+  }
+  // step 3.6b: adhesion (queries the stale step-2 grid)
+  std::vector<Vec2> adhesion_dv(n);
+  float wettability = clamp_r(slurry.wettability, 0.0f, 1.0f);
+  if (wettability > 0.0f && balls.len() > 0 && balls.radius > 0.0f) {
+    float dx = 0.5f * h;
+    float h_adh = fmin_r(h, 2.0f * balls.radius);
+    std::vector<Vec2> bpos = ball_boundary_particles(balls, dx);
+    size_t count_per_ball = boundary_points_per_ball(balls.radius, dx);
+    if (!bpos.empty() && h_adh > 0.0f) {
+      float adhesion_accel = wettability * ADHESION_ACCEL_FACTOR * std::fabs(GRAVITY);
+      struct Item { size_t j; Vec2 dir; float w; };
+      std::vector<Item> items;
+      std::vector<uint32_t> slot(n, UINT32_MAX);
+      std::vector<uint32_t> nearby;
+      float range2 = h_adh * h_adh * (1.0f + 1e-4f);
+      float inner2 = 0.25f * h_adh * h_adh * (1.0f - 1e-4f);
+      for (size_t b = 0; b < balls.len(); ++b) {
+        if (!balls.x[b].is_finite()) continue;
+        size_t start = b * count_per_ball;
+        size_t end = std::min(start + count_per_ball, bpos.size());
+        items.clear();
+        for (size_t q = start; q < end; ++q) {
+          Vec2 bp = bpos[q];
+          nearby.clear();
+          grid.for_each_near(bp, [&](uint32_t j) { nearby.push_back(j); });
+          for (uint32_t jj : nearby) {
+            size_t ju = jj;
+            Vec2 delta = bp - X[ju];
+            float r2 = delta.length_squared();
+            if (r2 >= range2 || r2 <= inner2) continue;
+            float r = std::sqrt(r2);
+            if (!std::isfinite(r) || r <= 0.5f * h_adh || r >= h_adh) continue;
+            float w = mass * adhesion_kernel(r, h_adh) / rest_density;
+            if (w <= 0.0f) continue;
+            Vec2 n_hat = delta / r;
+            if (slot[ju] == UINT32_MAX) {
+              slot[ju] = (uint32_t)items.size();
+              items.push_back({ju, w * n_hat, w});
+            } else {
+              Item& it = items[slot[ju]];
+              it.dir += w * n_hat;
+              it.w += w;
+            }
+          }
+        }
+        for (auto& it : items) slot[it.j] = UINT32_MAX;
+        if (items.empty()) continue;
+        float weight_sum = 0.0f;
+        Vec2 dir_sum;
+        for (auto& it : items) { dir_sum += it.dir; weight_sum += it.w; }
+        if (weight_sum <= 1e-9f) continue;
+        float pull_len = dir_sum.length();
+        if (pull_len <= 1e-9f) continue;
+        Vec2 ball_pull_dir = -dir_sum / pull_len;
+        float coverage = fmin_r(weight_sum, 1.0f);
+        float m_contrib = mass * weight_sum;
+        float attach = m_contrib / (balls.mass + m_contrib);
+        Vec2 dv_b = ball_pull_dir * (adhesion_accel * coverage * dt * attach);
+        coupling->impulses[b] += balls.mass * dv_b;
+        Vec2 lever = ball_pull_dir * balls.radius;
+        coupling->angular_impulses[b] += balls.mass * cross2(lever, dv_b);
+        for (auto& it : items) {
+          float frac = it.w / weight_sum;
+          Vec2 dv_i = -(balls.mass * frac / mass) * dv_b;
+          adhesion_dv[it.j] += dv_i;
+          coupling->fluid_momentum_change += mass * dv_i;
+        }
+      }
+    }
+  }
+  // step 4: wall projection
+  std::vector<uint8_t> touched(n, 0);
+  double acct_wall_impulse[2] = {0.0, 0.0};
+  double acct_wall_angular = 0.0;
+  float acct_wall_bins[WALL_IMPULSE_BINS] = {};
+  for (size_t i = 0; i < n; ++i) {
+    float d;
+    Vec2 normal;
+    drum.sdf_world(X[i], drum_angle_next, &d, &normal);
+    if (d < 0.0f) {
+      X[i] += -d * normal;
+      touched[i] = 1;
+      Vec2 push = mass * (-d * normal) / dt;
+      acct_wall_impulse[0] += (double)push.x;
+      acct_wall_impulse[1] += (double)push.y;
+      acct_wall_angular += (double)cross2(X[i], push);
+      float angle = std::atan2(X[i].y, X[i].x);
+      size_t bin = f2u_sat(((angle + PI_F) / TAU_F) * (float)WALL_IMPULSE_BINS);
+      acct_wall_bins[std::min(bin, (size_t)WALL_IMPULSE_BINS - 1)] += mass * -d / dt;
+    }
+  }
+  // step 5: velocity reconstruction
+  for (size_t i = 0; i < n; ++i) V[i] = (X[i] - x0[i]) / dt;
+  for (size_t i = 0; i < n; ++i) V[i] -= push_velocity_excess[i];
+  for (size_t i = 0; i < n; ++i) V[i] += cohesion_dv[i];
+  for (size_t i = 0; i < n; ++i) V[i] += adhesion_dv[i];
+  // step 6: wall no-slip
+  float beta = clamp_r(slurry.wall_no_slip, 0.0f, 1.0f);
+  float wall_work_j = 0.0f;
+  double ke_before_noslip = kinetic_energy_f64(V, mass);
+  if (beta > 0.0f) {
+    for (size_t i = 0; i < n; ++i) {
+      if (!touched[i]) continue;
+      Vec2 v_wall = drum.wall_velocity(X[i]);
+      Vec2 v_old = V[i];
+      V[i] = (1.0f - beta) * v_old + beta * v_wall;
+      Vec2 dv = V[i] - v_old;
+      wall_work_j += mass * dv.dot(v_wall);
+      acct_wall_impulse[0] += (double)(mass * dv.x);
+      acct_wall_impulse[1] += (double)(mass * dv.y);
+      acct_wall_angular += (double)cross2(X[i], mass * dv);
+    }
+  }
+  double ke_mark = kinetic_energy_f64(V, mass);
+  double ke_delta_noslip = ke_mark - ke_before_noslip;
+  // step 6.5: ball drag (Gauss-Seidel over balls)
+  float mu = fmax_r(slurry.viscosity_pa_s, 0.0f);
+  if (balls.len() > 0 && balls.radius > 0.0f && balls.true_radius > 0.0f && mu > 1e-6f) {
+    float beta_b = clamp_r(slurry.ball_no_slip, 0.0f, 1.0f);
+    float rot_cap = 0.2f * fluid_speed_clamp_v_max(drum);
+    float rho_ball = balls.mass / (PI_F * balls.radius * balls.radius);
+    float mass_true = rho_ball * PI_F * balls.true_radius * balls.true_radius;
+    float inv_tau_stokes = 0.0f;
+    if (beta_b > 0.0f) {
+      float h_c = balls.radius + h;
+      float w_hc0 = fmax_r(poly6(0.0f, h_c), 1e-12f);
+      UniformGrid cgrid = UniformGrid::build(X, fmax_r(h_c, 1e-6f));
+      float i_b = balls.inertia;
+      std::vector<uint32_t> nearby;
+      struct Item { size_t j; Vec2 r_i; float phi; };
+      std::vector<Item> items;
+      for (size_t b = 0; b < balls.len(); ++b) {
+        if (!balls.x[b].is_finite()) continue;
+        nearby.clear();
+        cgrid.for_each_near(balls.x[b], [&](uint32_t j) { nearby.push_back(j); });
+        if (nearby.empty()) continue;
+        items.clear();
+        float m_ent = 0.0f, i_ent = 0.0f, l_sum = 0.0f;
+        Vec2 r_sum, v_sum;
+        for (uint32_t jj : nearby) {
+          size_t ju = jj;
+          Vec2 r_i = X[ju] - balls.x[b];
+          float r2 = r_i.length_squared();
+          if (!std::isfinite(r2) || r2 >= h_c * h_c) continue;
+          float phi = poly6(r2, h_c) / w_hc0;
+          if (phi <= 0.0f) continue;
+          float w = mass * phi;
+          m_ent += w;
+          r_sum += w * r_i;
+          v_sum += w * V[ju];
+          i_ent += w * r2;
+          l_sum += w * cross2(r_i, V[ju]);
+          items.push_back({ju, r_i, phi});
+        }
+        if (m_ent <= 1e-12f || items.empty()) continue;
+        Vec2 r_bar = r_sum / m_ent;
+        Vec2 v_bar = v_sum / m_ent;
+        Vec2 v_rel = v_bar - balls.v[b];
+        float speed_rel = v_rel.length();
+        float inv_tau_form = (speed_rel > 1e-6f && rest_density > 0.0f)
+                                 ? 0.5f * rest_density * BALL_FORM_DRAG_COEFFICIENT * (2.0f * balls.true_radius) *
+                                       speed_rel / mass_true
+                                 : 0.0f;
+        float bt = beta_b * (1.0f - std::exp(-dt * (inv_tau_stokes + inv_tau_form)));
+        float a_lin = bt * m_ent / (balls.mass + m_ent);
+        Vec2 dv_b = a_lin * v_rel;
+        float dw_b = 0.0f, c_rot = 0.0f;
+        Vec2 p_bar;
+        if (i_ent > 1e-12f) {
+          float omega_bar = l_sum / i_ent;
+          float a_rot = bt * i_ent / (i_b + i_ent);
+          float candidate_dw = a_rot * (omega_bar - balls.omega[b]);
+          p_bar = Vec2(-r_bar.y, r_bar.x);
+          float s = 0.0f, s_scale = 0.0f;
+          for (auto& it : items) {
+            Vec2 perp_i(-it.r_i.y, it.r_i.x);
+            float phi2 = it.phi * it.phi;
+            s += mass * phi2 * cross2(it.r_i, perp_i - p_bar);
+            s_scale += mass * phi2 * it.r_i.length_squared();
+          }
+          if (std::fabs(s) > 0.1f * s_scale) {
+            float raw_c_rot = -i_b * candidate_dw / s;
+            float max_lever = 2.0f * h_c;
+            float c_rot_cap = max_lever > 1e-9f ? rot_cap / max_lever : 0.0f;
+            c_rot = clamp_r(raw_c_rot, -c_rot_cap, c_rot_cap);
+            dw_b = -c_rot * s / i_b;
+          }
+        }
+        for (auto& it : items) {
+          Vec2 dv_i = -(balls.mass / m_ent) * dv_b * it.phi;
+          if (c_rot != 0.0f) {
+            Vec2 perp_i(-it.r_i.y, it.r_i.x);
+            dv_i += c_rot * it.phi * (perp_i - p_bar);
+          }
+          V[it.j] += dv_i;
+          coupling->fluid_momentum_change += mass * dv_i;
+        }
+        coupling->impulses[b] += balls.mass * dv_b;
+        coupling->angular_impulses[b] += i_b * dw_b + balls.mass * cross2(r_bar, dv_b);
+      }
+    }
+  }
+  double ke_after_drag = kinetic_energy_f64(V, mass);
+  double ke_delta_drag = ke_after_drag - ke_mark;
+  ke_mark = ke_after_drag;
+  // step 6.6: buoyancy (Gauss-Seidel over balls on the stale step-2 grid)
+  if (balls.len() > 0 && balls.radius > 0.0f) {
+    float area = PI_F * balls.radius * balls.radius;
+    std::vector<uint32_t> nearby;
+    std::vector<std::pair<size_t, float>> weights;
+    for (size_t b = 0; b < balls.len(); ++b) {
+      if (!balls.x[b].is_finite()) continue;
+      nearby.clear();
+      grid.for_each_near(balls.x[b], [&](uint32_t j) { nearby.push_back(j); });
+      if (nearby.empty()) continue;
+      float rho_local = 0.0f;
+      weights.clear();
+      for (uint32_t jj : nearby) {
+        size_t ju = jj;
+        float r2 = (balls.x[b] - X[ju]).length_squared();
+        float w = mass * poly6(r2, h);
+        if (w > 0.0f) { rho_local += w; weights.push_back({ju, w}); }
+      }
+      if (rho_local <= 0.0f) continue;
+      float rho_eff = fmin_r(rho_local, rest_density);
+      float omega_num = 0.0f, omega_den = 0.0f;
+      for (auto& jw : weights) {
+        Vec2 d = X[jw.first];
+        float d2 = d.length_squared();
+        if (d2 <= 1e-12f) continue;
+        omega_num += jw.second * cross2(d, V[jw.first]) / d2;
+        omega_den += jw.second;
+      }
+      float omega_local = omega_den > 0.0f
+                              ? clamp_r(omega_num / omega_den, -std::fabs(drum.omega), std::fabs(drum.omega))
+                              : 0.0f;
+      Vec2 g_vec(0.0f, GRAVITY);
+      Vec2 centripetal = omega_local * omega_local * balls.x[b];
+      Vec2 g_eff = g_vec + centripetal;
+      Vec2 impulse_on_ball = -rho_eff * area * g_eff * dt;
+      coupling->impulses[b] += impulse_on_ball;
+      for (auto& jw : weights) {
+        float frac = jw.second / rho_local;
+        Vec2 dv = -(impulse_on_ball * frac) / mass;
+        V[jw.first] += dv;
+        coupling->fluid_momentum_change += mass * dv;
+      }
+    }
+  }
+  double ke_after_buoy = kinetic_energy_f64(V, mass);
+  double ke_delta_buoy = ke_after_buoy - ke_mark;
+  ke_mark = ke_after_buoy;
+  // density recompute at final x over the step-2 neighbour lists
+  uint32_t viscosity_iterations = 0;
+  for (size_t i = 0; i < n; ++i) {
+    float rho = mass * poly6(0.0f, h);
+    for (size_t k = nb.b(i); k < nb.e(i); ++k) {
+      float r2 = (X[i] - X[nb.idx[k]]).length_squared();
+      rho += mass * poly6(r2, h);
+    }
+    density[i] = rho;
+  }
+  // step 7: implicit viscosity
+  if (mu > 0.0f) {
+    std::vector<float> mu_eff;
+    if (slurry.rheology == RHEO_BINGHAM && slurry.yield_stress_pa > 0.0f) {
+      mu_eff = bingham_viscosity(shear_rates(X, V, nb, density, mass, h), mu, slurry.yield_stress_pa);
+    } else {
+      mu_eff.assign(n, mu);
+    }
+    ViscWeights weights = morris_weights(X, nb, density, mass, mu_eff, h);
+    std::vector<BoundaryGroup> groups;
+    if (balls.len() > 0 && balls.radius > 0.0f) {
+      float dx = 0.5f * h;
+      size_t count = boundary_points_per_ball(balls.radius, dx);
+      std::vector<Vec2> pts = ball_boundary_particles(balls, dx);
+      UniformGrid grid_now = UniformGrid::build(X, h);
+      float eta2 = VISCOSITY_ETA_FACTOR * h * h;
+      float spiky_norm = -30.0f / (PI_F * powi5(h));
+      float range2 = h * h * (1.0f + 1e-4f);
+      std::vector<float> fluid_factor(n);
+      for (size_t j = 0; j < n; ++j)
+        fluid_factor[j] = BALL_BC_GAIN * (mass * 2.0f * mu_eff[j] / (fmax_r(density[j], 1e-6f) * rest_density));
+      std::vector<uint32_t> slot(n, UINT32_MAX);
+      size_t group_start = 0, current_ball = SIZE_MAX;
+      for (size_t k = 0; k < pts.size(); ++k) {
+        Vec2 bp = pts[k];
+        size_t bi = k / count;
+        if (bi != current_ball) {
+          for (size_t g = group_start; g < groups.size(); ++g) slot[groups[g].fluid] = UINT32_MAX;
+          group_start = groups.size();
+          current_ball = bi;
+        }
+        if (!balls.x[bi].is_finite()) continue;
+        grid_now.for_each_near(bp, [&](uint32_t j) {
+          Vec2 delta = X[j] - bp;
+          float r2 = delta.length_squared();
+          if (r2 >= range2) return;
+          float r = std::sqrt(r2);
+          if (!std::isfinite(r) || r >= h || r <= 1e-9f) return;
+          float dot_abs = std::fabs(spiky_norm * (h - r) * (h - r) * r);
+          float c = fluid_factor[j] * dot_abs / (r2 + eta2);
+          if (c > 0.0f) {
+            Vec2 lever = bp - balls.x[bi];
+            Vec2 lever_c = c * lever;
+            float lever2_c = c * lever.length_squared();
+            uint32_t s = slot[j];
+            if (s == UINT32_MAX) {
+              slot[j] = (uint32_t)groups.size();
+              groups.push_back({j, (uint32_t)bi, c, lever_c, lever2_c});
+            } else {
+              BoundaryGroup& g = groups[s];
+              g.c += c;
+              g.lever_c += lever_c;
+              g.lever2_c += lever2_c;
+            }
+          }
+        });
+      }
+    }
+    std::vector<Vec2> ball_v0(balls.len());
+    for (size_t bi = 0; bi < balls.len(); ++bi) ball_v0[bi] = balls.v[bi] + coupling->impulses[bi] / balls.mass;
+    size_t links_in_range = 0;
+    std::vector<SqueezeLink> links = squeeze_links(balls, drum.radius_m, 0.5f * h, mu, dt, &ball_v0, &links_in_range);
+    if (ctr) {
+      ctr->n_groups = (uint32_t)groups.size();
+      ctr->n_links = (uint32_t)links.size();
+      ctr->links_in_range = (uint32_t)links_in_range;
+    }
+    if (groups.empty() && links_in_range == 0) {
+      viscosity_iterations = solve_implicit_viscosity(nb, weights, &V, dt, opt.cg_fp64 != 0);
+    } else {
+      std::vector<Vec2> ball_v = ball_v0;
+      std::vector<float> ball_w(balls.len());
+      for (size_t bi = 0; bi < balls.len(); ++bi)
+        ball_w[bi] = balls.omega[bi] + coupling->angular_impulses[bi] / balls.inertia;
+      std::vector<float> ball_w0 = ball_w;
+      std::vector<Vec2> guess;
+      guess.swap(fl->viscous_guess);
+      std::vector<Vec2> v_in = V;
+      viscosity_iterations = solve_viscosity_with_balls(nb, weights, groups, links, mass, balls.mass, balls.inertia,
+                                                        dt, guess, &V, &ball_v, &ball_w, opt.cg_fp64 != 0);
+      fl->viscous_guess.resize(n);
+      for (size_t i = 0; i < n; ++i) {
+        Vec2 d = V[i] - v_in[i];
+        fl->viscous_guess[i] = d.is_finite() ? d : Vec2();
+      }
+      for (size_t bi = 0; bi < balls.len(); ++bi) {
+        Vec2 dv = ball_v[bi] - ball_v0[bi];
+        float dw = ball_w[bi] - ball_w0[bi];
+        if (dv.is_finite() && std::isfinite(dw)) {
+          coupling->impulses[bi] += balls.mass * dv;
+          coupling->angular_impulses[bi] += balls.inertia * dw;
+          coupling->fluid_momentum_change -= balls.mass * dv;
+        }
+      }
+    }
+  }
+  if (ctr) ctr->cg_iters = viscosity_iterations;
+  float mean_shear = mean_shear_rate(X, V, nb, density, mass, h);
+  double ke_after_visc = kinetic_energy_f64(V, mass);
+  double ke_delta_visc = ke_after_visc - ke_mark;
+  clamp_fluid_speed(&V, fluid_speed_clamp_v_max(drum));
+  double ke_delta_clamp = kinetic_energy_f64(V, mass) - ke_after_visc;
+  // step 8: impulse clamp
+  if (balls.len() > 0) {
+    float clamp = impulse_clamp(balls.mass, dt);
+    float angular_clamp = clamp * balls.radius;
+    for (size_t b = 0; b < balls.len(); ++b) {
+      float mag = coupling->impulses[b].length();
+      if (mag > clamp && mag > 1e-9f) {
+        coupling->impulses[b] *= clamp / mag;
+        coupling->clamp_hits += 1;
+      }
+      coupling->angular_impulses[b] = clamp_r(coupling->angular_impulses[b], -angular_clamp, angular_clamp);
+    }
+  }
+  FluidStepStats& st = *stats_out;
+  st.viscosity_iterations = viscosity_iterations;
+  st.mean_shear_rate_per_s = mean_shear;
+  st.coupling_clamp_hits = coupling->clamp_hits;
+  st.wall_work_j = wall_work_j;
+  st.wall_impulse[0] = (float)acct_wall_impulse[0];
+  st.wall_impulse[1] = (float)acct_wall_impulse[1];
+  st.wall_angular_impulse = (float)acct_wall_angular;
+  for (int k = 0; k < WALL_IMPULSE_BINS; ++k) st.wall_normal_impulse_by_angle[k] = acct_wall_bins[k];
+  st.ke_delta_noslip_j = (float)ke_delta_noslip;
+  st.ke_delta_drag_j = (float)ke_delta_drag;
+  st.ke_delta_buoyancy_j = (float)ke_delta_buoy;
+  st.ke_delta_viscosity_j = (float)ke_delta_visc;
+  st.ke_delta_clamp_j = (float)ke_delta_clamp;
+}
+
+// ------------------------------------------------------------------ dem.rs
+static const float RESTITUTION_VELOCITY_THRESHOLD = 0.02f;
+static const float RESTITUTION_THRESHOLD_FROUDE = 0.1428f;
+static const float MAX_RECOVERY_FRACTION = 0.2f;
+static const float CCD_CONTACT_SKIN_FRACTION = 1e-2f;
+static const float IMPACT_ENERGY_MIN_J = 1e-6f;
+static const float IMPACT_ENERGY_MAX_J = 1.0f;
+
+// dem.rs:43-46
+float restitution_velocity_threshold(float r) {
+  return RESTITUTION_THRESHOLD_FROUDE * std::sqrt(-GRAVITY * 2.0f * r);
+}
+// dem.rs:99-109
+int impact_energy_bin(float e) {
+  if (!std::isfinite(e) || e <= 0.0f) return -1;
+  float ec = clamp_r(e, IMPACT_ENERGY_MIN_J, IMPACT_ENERGY_MAX_J);
+  float log_min = std::log10(IMPACT_ENERGY_MIN_J);
+  float log_max = std::log10(IMPACT_ENERGY_MAX_J);
+  float t = (std::log10(ec) - log_min) / (log_max - log_min);
+  uint32_t idx = f2u_sat(t * (float)IMPACT_BINS);
+  return (int)std::min(idx, (uint32_t)IMPACT_BINS - 1);
+}
+// dem.rs:127-138
+float effective_friction(float mu_k, float mu_s, float v_t, float vs) {
+  if (mu_s <= mu_k) return mu_k;
+  float ratio = v_t / vs;
+  float weight = std::exp(-(ratio * ratio));
+  return mu_k + (mu_s - mu_k) * weight;
+}
+// dem.rs:253-273
+static float mechanical_energy_j(const Balls& b) {
+  float e = 0.0f;
+  for (size_t i = 0; i < b.len(); ++i) {
+    e += 0.5f * b.mass * b.v[i].length_squared();
+    e += 0.5f * b.inertia * b.omega[i] * b.omega[i];
+    e += b.mass * std::fabs(GRAVITY) * b.x[i].y;
+  }
+  return e;
+}
+double dem_mechanical_energy_f64(const Balls& b) {
+  double e = 0.0;
+  for (size_t i = 0; i < b.len(); ++i) {
+    e += 0.5 * (double)b.mass * (double)b.v[i].length_squared();
+    e += 0.5 * (double)b.inertia * (double)(b.omega[i] * b.omega[i]);
+    e += (double)b.mass * (double)std::fabs(GRAVITY) * (double)b.x[i].y;
+  }
+  return e;
+}
+// dem.rs:1071-1080
+static float angle_diff(float a, float b) {
+  float d = a - b;
+  while (d > PI_F) d -= 2.0f * PI_F;
+  while (d < -PI_F) d += 2.0f * PI_F;
+  return d;
+}
+
+// dem.rs:530-1066
+DemStepStats dem_step_recorded(Balls* bp, const Drum& drum, float drum_angle, const MediaParams& media,
+                               uint32_t iterations, float dt, const CouplingImpulses* ext,
+                               std::vector<ImpactRecord>* impacts, StepCounters* ctr, Debug* dbg) {
+  Balls& B = *bp;
+  DemStepStats out;
+  if (B.len() == 0 || dt <= 0.0f) return out;
+  size_t n = B.len();
+  float w = B.mass > 0.0f ? 1.0f / B.mass : 0.0f;
+  float w_rot = B.inertia > 0.0f ? 1.0f / B.inertia : 0.0f;
+  float r = B.radius;
+  float impact_threshold = restitution_velocity_threshold(r);
+  for (size_t i = 0; i < n; ++i)
+    if (!B.x[i].is_finite() || !B.v[i].is_finite()) { B.x[i] = Vec2(); B.v[i] = Vec2(); }
+  std::vector<Vec2> x0 = B.x;
+  std::vector<float> theta0 = B.theta;
+  std::vector<Vec2> v_pre = B.v;
+  std::vector<float> omega_pre = B.omega;
+  double coupling_work = 0.0;
+  for (size_t i = 0; i < n; ++i) {
+    B.v[i].y += GRAVITY * dt;
+    if (ext) {
+      double ke_before = 0.5 * (double)B.mass * (double)B.v[i].length_squared() +
+                         0.5 * (double)B.inertia * (double)(B.omega[i] * B.omega[i]);
+      B.v[i] += ext->impulses[i] * w;
+      B.omega[i] += ext->angular_impulses[i] * w_rot;
+      double ke_after = 0.5 * (double)B.mass * (double)B.v[i].length_squared() +
+                        0.5 * (double)B.inertia * (double)(B.omega[i] * B.omega[i]);
+      coupling_work += ke_after - ke_before;
+    }
+    B.x[i] += B.v[i] * dt;
+    B.theta[i] += B.omega[i] * dt;
+  }
+  float e_after_predict = mechanical_energy_j(B);
+  float max_disp = 0.0f;
+  for (size_t i = 0; i < n; ++i) max_disp = fmax_r(max_disp, B.v[i].length() * dt / fmax_r(2.0f * r, 1e-12f));
+  float max_speed = 0.0f;
+  for (size_t i = 0; i < n; ++i) max_speed = fmax_r(max_speed, B.v[i].length());
+  float solve_margin = (float)std::max(iterations, 1u) * MAX_RECOVERY_FRACTION * 2.0f * r;
+  float cell_size = fmax_r(fmax_r(2.0f * r * 1.05f, 2.0f * r + max_speed * dt + solve_margin), 1e-6f);
+  UniformGrid grid = UniformGrid::build(B.x, cell_size);
+  std::vector<std::pair<uint32_t, uint32_t>> pairs;
+  grid.for_each_candidate_pair([&](uint32_t i, uint32_t j) { pairs.push_back({i, j}); });
+  if (ctr) ctr->n_ball_pairs = (uint32_t)pairs.size();
+  if (dbg) dbg->ball_pairs = pairs;
+  // step 2.5: wall CCD
+  float drum_angle_next = drum_angle + drum.omega * dt;
+  std::vector<float> toi(n, 1.0f);
+  for (size_t i = 0; i < n; ++i) {
+    float d_end;
+    Vec2 nn;
+    drum.sdf_world(B.x[i], drum_angle_next, &d_end, &nn);
+    float c_end = d_end - r;
+    if (c_end >= -MAX_RECOVERY_FRACTION * 2.0f * r) continue;
+    float t;
+    if (drum.toi_swept(x0[i], B.x[i], drum_angle, drum_angle_next, r, &t)) toi[i] = fmin_r(toi[i], t);
+  }
+  for (size_t i = 0; i < n; ++i) {
+    if (toi[i] < 1.0f) {
+      float path_len = (B.x[i] - x0[i]).length();
+      float skin = CCD_CONTACT_SKIN_FRACTION * r;
+      float t_skin = path_len > 1e-9f ? skin / path_len : 1.0f;
+      float t_cl = fmin_r(toi[i] + t_skin, 1.0f);
+      B.x[i] = x0[i] + (B.x[i] - x0[i]) * t_cl;
+    }
+  }
+  std::vector<float> lam_bb(pairs.size(), 0.0f), lam_bw(n, 0.0f);
+  // step 3: projection
+  for (uint32_t it = 0; it < std::max(iterations, 1u); ++it) {
+    for (size_t k = 0; k < pairs.size(); ++k) {
+      size_t i = pairs[k].first, j = pairs[k].second;
+      Vec2 delta = B.x[i] - B.x[j];
+      float dist = delta.length();
+      float c = dist - 2.0f * r;
+      if (c >= 0.0f) continue;
+      Vec2 n_hat = dist > 1e-9f ? delta / dist : Vec2(1.0f, 0.0f);
+      float w_sum = w + w;
+      if (w_sum <= 0.0f) continue;
+      float c_eff = fmax_r(c, -MAX_RECOVERY_FRACTION * 2.0f * r);
+      float d_lambda = -c_eff / w_sum;
+      B.x[i] += w * d_lambda * n_hat;
+      B.x[j] -= w * d_lambda * n_hat;
+      lam_bb[k] += d_lambda;
+    }
+    for (size_t i = 0; i < n; ++i) {
+      float d;
+      Vec2 n_hat;
+      drum.sdf_world(B.x[i], drum_angle_next, &d, &n_hat);
+      float c = d - r;
+      if (c >= 0.0f) continue;
+      if (w <= 0.0f) continue;
+      float c_eff = fmax_r(c, -MAX_RECOVERY_FRACTION * 2.0f * r);
+      float d_lambda = -c_eff / w;
+      B.x[i] += w * d_lambda * n_hat;
+      lam_bw[i] += d_lambda;
+    }
+  }
+  // step 4: velocity reconstruction
+  for (size_t i = 0; i < n; ++i) {
+    B.v[i] = (B.x[i] - x0[i]) / dt;
+    B.omega[i] = angle_diff(B.theta[i], theta0[i]) / dt;
+  }
+  struct C3 { uint32_t i, j; float l; };
+  std::vector<C3> bb(pairs.size());
+  for (size_t k = 0; k < pairs.size(); ++k) bb[k] = {pairs[k].first, pairs[k].second, lam_bb[k]};
+  std::sort(bb.begin(), bb.end(), [](const C3& a, const C3& b) { return a.i != b.i ? a.i < b.i : a.j < b.j; });
+  if (ctr) {
+    uint32_t act = 0;
+    for (auto& c : bb) act += c.l > 0.0f;
+    ctr->n_active_contacts = act;
+  }
+  // step 5: friction
+  for (const C3& c : bb) {
+    if (c.l <= 0.0f) continue;
+    size_t iu = c.i, ju = c.j;
+    Vec2 delta = B.x[iu] - B.x[ju];
+    float dist = delta.length();
+    Vec2 n_hat = dist > 1e-9f ? delta / dist : Vec2(1.0f, 0.0f);
+    Vec2 t_hat(-n_hat.y, n_hat.x);
+    float v_t = (B.v[iu] - B.v[ju]).dot(t_hat) - r * B.omega[iu] - r * B.omega[ju];
+    float w_sum_t = w + w + r * r * w_rot + r * r * w_rot;
+    if (w_sum_t <= 0.0f) continue;
+    float raw = -v_t * dt / w_sum_t;
+    float mu = effective_friction(media.friction_ball_ball, media.friction_ball_ball_static, v_t,
+                                  media.friction_velocity_scale_m_s);
+    float max_mag = mu * c.l;
+    float dlt = clamp_r(raw, -max_mag, max_mag);
+    B.x[iu] += w * dlt * t_hat;
+    B.x[ju] -= w * dlt * t_hat;
+    B.theta[iu] -= r * w_rot * dlt;
+    B.theta[ju] -= r * w_rot * dlt;
+    Vec2 dv = w * dlt * t_hat / dt;
+    float domega = -r * w_rot * dlt / dt;
+    B.v[iu] += dv;
+    B.v[ju] -= dv;
+    B.omega[iu] += domega;
+    B.omega[ju] += domega;
+  }
+  float wall_work_j = 0.0f;
+  for (size_t i = 0; i < n; ++i) {
+    float lambda_n = lam_bw[i];
+    if (lambda_n <= 0.0f) continue;
+    float dd;
+    Vec2 n_hat;
+    drum.sdf_world(B.x[i], drum_angle_next, &dd, &n_hat);
+    Vec2 t_hat(-n_hat.y, n_hat.x);
+    Vec2 v_wall = drum.wall_velocity(B.x[i] - r * n_hat);
+    float v_t = (B.v[i] - v_wall).dot(t_hat) - r * B.omega[i];
+    float w_sum_t = w + r * r * w_rot;
+    if (w_sum_t <= 0.0f) continue;
+    float raw = -v_t * dt / w_sum_t;
+    float mu = effective_friction(media.friction_ball_wall, media.friction_ball_wall_static, v_t,
+                                  media.friction_velocity_scale_m_s);
+    float max_mag = mu * lambda_n;
+    float dlt = clamp_r(raw, -max_mag, max_mag);
+    B.x[i] += w * dlt * t_hat;
+    B.theta[i] -= r * w_rot * dlt;
+    B.v[i] += w * dlt * t_hat / dt;
+    B.omega[i] += -r * w_rot * dlt / dt;
+    wall_work_j += (dlt / dt) * t_hat.dot(v_wall);
+    wall_work_j += (lambda_n / dt) * n_hat.dot(v_wall);
+  }
+  // resync
+  for (size_t i = 0; i < n; ++i) {
+    B.v[i] = (B.x[i] - x0[i]) / dt;
+    B.omega[i] = angle_diff(B.theta[i], theta0[i]) / dt;
+  }
+  // step 6: restitution
+  uint32_t collision_count = 0;
+  uint32_t hist[IMPACT_BINS] = {};
+  for (const C3& c : bb) {
+    if (c.l <= 0.0f) continue;
+    size_t iu = c.i, ju = c.j;
+    Vec2 delta = B.x[iu] - B.x[ju];
+    float dist = delta.length();
+    Vec2 n_hat = dist > 1e-9f ? delta / dist : Vec2(1.0f, 0.0f);
+    float v_n_pre = (v_pre[iu] - v_pre[ju]).dot(n_hat);
+    bool fresh = v_n_pre < -RESTITUTION_VELOCITY_THRESHOLD;
+    if (fresh) {
+      collision_count += 1;
+      float e_imp = 0.5f * (B.mass * 0.5f) * v_n_pre * v_n_pre;
+      int bin = impact_energy_bin(e_imp);
+      if (bin >= 0) hist[bin] += 1;
+    }
+    float e = fresh ? media.restitution_ball_ball : 0.0f;
+    if (-v_n_pre > impact_threshold && impacts) {
+      Vec2 t_hat(-n_hat.y, n_hat.x);
+      float slip = (v_pre[iu] - v_pre[ju]).dot(t_hat) - r * omega_pre[iu] - r * omega_pre[ju];
+      impacts->push_back({0u, c.i, c.j, -v_n_pre, std::fabs(slip), e});
+    }
+    float target = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
+    float v_n_now = (B.v[iu] - B.v[ju]).dot(n_hat);
+    float delta_v_n = target - v_n_now;
+    float w_sum = w + w;
+    if (w_sum <= 0.0f) continue;
+    float impulse = delta_v_n / w_sum;
+    B.v[iu] += w * impulse * n_hat;
+    B.v[ju] -= w * impulse * n_hat;
+  }
+  for (size_t i = 0; i < n; ++i) {
+    float lambda_n = lam_bw[i];
+    if (lambda_n <= 0.0f) continue;
+    float dd;
+    Vec2 n_hat;
+    drum.sdf_world(B.x[i], drum_angle_next, &dd, &n_hat);
+    Vec2 v_wall = drum.wall_velocity(B.x[i] - r * n_hat);
+    float v_n_pre = (v_pre[i] - v_wall).dot(n_hat);
+    bool fresh = v_n_pre < -RESTITUTION_VELOCITY_THRESHOLD;
+    if (fresh) {
+      collision_count += 1;
+      float e_imp = 0.5f * B.mass * v_n_pre * v_n_pre;
+      int bin = impact_energy_bin(e_imp);
+      if (bin >= 0) hist[bin] += 1;
+    }
+    float e = fresh ? media.restitution_ball_wall : 0.0f;
+    if (-v_n_pre > impact_threshold && impacts) {
+      Vec2 t_hat(-n_hat.y, n_hat.x);
+      float slip = (v_pre[i] - v_wall).dot(t_hat) - r * omega_pre[i];
+      impacts->push_back({1u, (uint32_t)i, WALL_ID, -v_n_pre, std::fabs(slip), e});
+    }
+    float target = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
+    float v_n_now = (B.v[i] - v_wall).dot(n_hat);
+    float delta_v_n = target - v_n_now;
+    if (w <= 0.0f) continue;
+    B.v[i] += delta_v_n * n_hat;
+  }
+  // step 7: rolling resistance
+  if (media.rolling_friction > 0.0f && B.inertia > 0.0f) {
+    std::vector<float> total(n, 0.0f);
+    for (const C3& c : bb) { total[c.i] += fmax_r(c.l, 0.0f); total[c.j] += fmax_r(c.l, 0.0f); }
+    for (size_t i = 0; i < n; ++i) total[i] += fmax_r(lam_bw[i], 0.0f);
+    for (size_t i = 0; i < n; ++i) {
+      float ln = total[i];
+      if (ln <= 0.0f || B.omega[i] == 0.0f) continue;
+      float normal_force = ln / dt;
+      float max_dw = media.rolling_friction * normal_force * r / B.inertia * dt;
+      float dw = fmin_r(max_dw, std::fabs(B.omega[i]));
+      B.omega[i] -= signum_r(B.omega[i]) * dw;
+    }
+  }
+  float e_final = mechanical_energy_j(B);
+  out.wall_work_j = wall_work_j;
+  out.collision_count = collision_count;
+  for (int k = 0; k < IMPACT_BINS; ++k) out.impact_energy_histogram[k] = hist[k];
+  out.dissipated_energy_j = e_after_predict + wall_work_j - e_final;
+  out.max_substep_displacement_over_diameter = max_disp;
+  out.coupling_work_j = (float)coupling_work;
+  return out;
+}
+
+}  // namespace orc
