@@ -145,6 +145,8 @@ typedef struct MgImpactRecord {
 typedef struct MgStepCounters {
   uint32_t density_iters, cg_iters, n_groups, n_links, links_in_range;
   uint32_t n_ball_pairs, n_fluid_edges, n_active_contacts;
+  uint32_t n_coupling_items; /* entrained (ball, fluid) items of drag plus buoyancy */
+  uint32_t reserved0;
 } MgStepCounters;
 
 /* dem.rs:277-309 Balls' uniform material fields */
@@ -265,6 +267,15 @@ int mg_mixing_index(MgSim* sim, float* out, int* valid);
 int mg_stress_histogram_rate(MgSim* sim, double* out28);
 /* stats of the last sub-step taken by any step call */
 int mg_last_step_stats(MgSim* sim, MgFluidStepStats* fluid, MgDemStepStats* dem, MgStepCounters* ctr);
+
+/* ---- measurement ----
+ * The CUDA stream the handle launches on (a cudaStream_t), for event timing by the caller. */
+int mg_sim_stream(MgSim* sim, void** stream);
+/* Device duration (CUDA events) of the last kernel launch, and the number of launches so far. */
+int mg_sim_last_kernel_ms(MgSim* sim, float* ms, uint64_t* launches);
+/* Sums of every MgStepCounters field over all sub-steps since creation (or the last reset),
+ * in field order, and the number of sub-steps summed. */
+int mg_counter_totals(MgSim* sim, uint64_t* totals10, uint64_t* n_substeps, int reset);
 
 /* ---- parity probes of the grid stage (grid.rs, pbf.rs:262-288) ----
  * Run the device grid build / candidate-pair / neighbour-list code on caller points. */

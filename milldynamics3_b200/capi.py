@@ -119,7 +119,7 @@ class ImpactRecord(_S):
 class StepCounters(_S):
     _fields_ = [(n, C.c_uint32) for n in (
         "density_iters", "cg_iters", "n_groups", "n_links", "links_in_range", "n_ball_pairs",
-        "n_fluid_edges", "n_active_contacts")]
+        "n_fluid_edges", "n_active_contacts", "n_coupling_items", "reserved0")]
 
 
 class BallMaterial(_S):
@@ -207,6 +207,9 @@ SIGNATURES = [
 DEVICE_ONLY = [
     ("last_error", C.c_char_p, [vp]),
     ("sim_set_options", C.c_int, [vp, P(Options)]),
+    ("sim_stream", C.c_int, [vp, P(vp)]),
+    ("sim_last_kernel_ms", C.c_int, [vp, P(C.c_float), P(C.c_uint64)]),
+    ("counter_totals", C.c_int, [vp, P(C.c_uint64), P(C.c_uint64), C.c_int]),
 ]
 
 

@@ -1,0 +1,166 @@
+// Block-level building blocks for the one-CTA-per-mill kernels: deterministic reductions, an
+// in-place exclusive scan over global memory, and a stable bucket sort (records grouped by key,
+// ascending record index inside a bucket). Every routine is called by all threads of the block.
+#pragma once
+
+#include "mill_common.cuh"
+
+namespace mg {
+
+__device__ __forceinline__ uint32_t tid() { return threadIdx.x; }
+__device__ __forceinline__ uint32_t nthr() { return blockDim.x; }
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic f64 sum: fixed xor-tree inside warps, then a fixed tree over the warp sums.
+__device__ double block_sum_d(double v) {
+  __shared__ double sh[32];
+  __shared__ double res;
+  v = warp_sum(v);
+  int w = tid() >> 5, l = tid() & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    int nw = (nthr() + 31) >> 5;
+    double x = l < nw ? sh[l] : 0.0;
+    x = warp_sum(x);
+    if (l == 0) res = x;
+  }
+  __syncthreads();
+  double r = res;
+  __syncthreads();
+  return r;
+}
+
+__device__ uint32_t block_sum_u(uint32_t v) {
+  __shared__ uint32_t sh[32];
+  __shared__ uint32_t res;
+  v = warp_sum(v);
+  int w = tid() >> 5, l = tid() & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    int nw = (nthr() + 31) >> 5;
+    uint32_t x = l < nw ? sh[l] : 0u;
+    x = warp_sum(x);
+    if (l == 0) res = x;
+  }
+  __syncthreads();
+  uint32_t r = res;
+  __syncthreads();
+  return r;
+}
+
+// f32::max fold (order-independent: max is exact).
+__device__ float block_max_f(float v) {
+  __shared__ float sh[32];
+  __shared__ float res;
+  for (int o = 16; o > 0; o >>= 1) v = fmax_r(v, __shfl_xor_sync(0xffffffffu, v, o));
+  int w = tid() >> 5, l = tid() & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    int nw = (nthr() + 31) >> 5;
+    float x = l < nw ? sh[l] : 0.0f;
+    for (int o = 16; o > 0; o >>= 1) x = fmax_r(x, __shfl_xor_sync(0xffffffffu, x, o));
+    if (l == 0) res = x;
+  }
+  __syncthreads();
+  float r = res;
+  __syncthreads();
+  return r;
+}
+
+__device__ void block_minmax_i(int32_t& mn0, int32_t& mx0, int32_t& mn1, int32_t& mx1) {
+  __shared__ int32_t sh[4][32];
+  int w = tid() >> 5, l = tid() & 31;
+  for (int o = 16; o > 0; o >>= 1) {
+    mn0 = min(mn0, __shfl_xor_sync(0xffffffffu, mn0, o));
+    mx0 = max(mx0, __shfl_xor_sync(0xffffffffu, mx0, o));
+    mn1 = min(mn1, __shfl_xor_sync(0xffffffffu, mn1, o));
+    mx1 = max(mx1, __shfl_xor_sync(0xffffffffu, mx1, o));
+  }
+  if (l == 0) { sh[0][w] = mn0; sh[1][w] = mx0; sh[2][w] = mn1; sh[3][w] = mx1; }
+  __syncthreads();
+  int nw = (nthr() + 31) >> 5;
+  mn0 = INT32_MAX; mx0 = INT32_MIN; mn1 = INT32_MAX; mx1 = INT32_MIN;
+  for (int k = 0; k < nw; ++k) {
+    mn0 = min(mn0, sh[0][k]); mx0 = max(mx0, sh[1][k]);
+    mn1 = min(mn1, sh[2][k]); mx1 = max(mx1, sh[3][k]);
+  }
+  __syncthreads();
+}
+
+// In-place exclusive scan of a[0..m); returns the total. All threads call it.
+__device__ uint32_t block_exclusive_scan(uint32_t* a, uint32_t m) {
+  __shared__ uint32_t wsum[32];
+  __shared__ uint32_t carry;
+  if (tid() == 0) carry = 0;
+  __syncthreads();
+  int w = tid() >> 5, l = tid() & 31;
+  int nw = (nthr() + 31) >> 5;
+  for (uint32_t base = 0; base < m; base += nthr()) {
+    uint32_t idx = base + tid();
+    uint32_t v = idx < m ? a[idx] : 0u;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (l >= o) x += y;
+    }
+    if (l == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      uint32_t s = l < nw ? wsum[l] : 0u;
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+        if (l >= o) s += y;
+      }
+      if (l < nw) wsum[l] = s;  // inclusive warp prefix
+    }
+    __syncthreads();
+    uint32_t before = carry + (w > 0 ? wsum[w - 1] : 0u) + (x - v);
+    if (idx < m) a[idx] = before;
+    __syncthreads();
+    if (tid() == 0) carry += wsum[nw - 1];
+    __syncthreads();
+  }
+  uint32_t total = carry;
+  __syncthreads();
+  return total;
+}
+
+// Insertion sort of a short segment (ascending).
+__device__ __forceinline__ void small_sort_u32(uint32_t* a, uint32_t n) {
+  for (uint32_t i = 1; i < n; ++i) {
+    uint32_t v = a[i];
+    uint32_t j = i;
+    while (j > 0 && a[j - 1] > v) { a[j] = a[j - 1]; --j; }
+    a[j] = v;
+  }
+}
+
+// Stable bucket sort: start[0..nbk] receives bucket offsets, order[] the record indices grouped by
+// key in ascending record order; cur[0..nbk) is scratch. Buckets are expected to be short.
+__device__ void block_bucket_sort(const uint32_t* keys, uint32_t nrec, uint32_t nbk, uint32_t* start, uint32_t* cur,
+                                  uint32_t* order) {
+  for (uint32_t k = tid(); k <= nbk; k += nthr()) start[k] = 0;
+  __syncthreads();
+  for (uint32_t r = tid(); r < nrec; r += nthr()) atomicAdd(&start[keys[r]], 1u);
+  __syncthreads();
+  block_exclusive_scan(start, nbk + 1);
+  for (uint32_t k = tid(); k < nbk; k += nthr()) cur[k] = start[k];
+  __syncthreads();
+  for (uint32_t r = tid(); r < nrec; r += nthr()) {
+    uint32_t slot = atomicAdd(&cur[keys[r]], 1u);
+    order[slot] = r;
+  }
+  __syncthreads();
+  for (uint32_t k = tid(); k < nbk; k += nthr()) small_sort_u32(order + start[k], start[k + 1] - start[k]);
+  __syncthreads();
+}
+
+}  // namespace mg

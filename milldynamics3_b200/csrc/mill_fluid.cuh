@@ -1,0 +1,1137 @@
+// The fluid half of the sub-step (FluidParticles::step_coupled, pbf.rs:1174-2365) for one mill,
+// executed by one thread block. Per-particle and per-ball stages are block-stride loops in
+// gather form (no atomics on positions); the reference's order-dependent reductions and its
+// Gauss-Seidel sweeps (drag, buoyancy) are replayed in the reference order, so the results match
+// the sequential Rust arithmetic bit for bit.
+#pragma once
+
+#include "mill_geom.cuh"
+#include "mill_grid.cuh"
+
+namespace mg {
+
+constexpr float EPSILON_RELAX = 200.0f;
+constexpr uint32_t ADAPTIVE_MAX_EXTRA = 6;
+constexpr float COMPRESSION_TOL = 0.02f;
+constexpr float OVERLAP_PUSH_MARGIN = 0.05f;
+constexpr float VISC_CG_TOL = 1e-3f;
+constexpr uint32_t VISC_CG_MAX = 50;
+constexpr float VISC_ETA = 0.01f;
+constexpr float CENTRAL_VISC = 4.0f;
+constexpr float BALL_BC_GAIN = 0.5f;
+
+struct FluidShared {
+  GridHdr hA, hB, hBall;
+  uint32_t n_edges, n_recs, n_groups, n_links, links_in_range;
+  float fscal[8];
+  double dscal[8];
+  uint32_t uscal[8];
+};
+
+__device__ __forceinline__ float fluid_vmax(const StepUniform& U) {
+  return 5.0f * (fabsf(U.drum_omega) * U.drum_radius + sqrtf(4.0f * fabsf(GRAVITY) * U.drum_radius));
+}
+
+// pbf.rs:924-926: 0.5 m sum |v|^2 in f64, summed in particle order.
+__device__ double kinetic_energy_seq(const float2* v, uint32_t n, float mass, FluidShared& S) {
+  if (tid() == 0) {
+    double s = 0.0;
+    for (uint32_t i = 0; i < n; ++i) s += (double)V2(v[i]).len2();
+    S.dscal[7] = 0.5 * (double)mass * s;
+  }
+  __syncthreads();
+  double r = S.dscal[7];
+  __syncthreads();
+  return r;
+}
+
+// pbf.rs:292-294 dot in the reference's sequential f32 order, or in f64 (deterministic tree).
+__device__ double block_dot(const float2* a, const float2* b, uint32_t len, bool fp64, FluidShared& S) {
+  if (fp64) {
+    double acc = 0.0;
+    for (uint32_t e = tid(); e < len; e += nthr())
+      acc += (double)a[e].x * (double)b[e].x + (double)a[e].y * (double)b[e].y;
+    return block_sum_d(acc);
+  }
+  if (tid() == 0) {
+    float s = 0.0f;
+    for (uint32_t e = 0; e < len; ++e) s += V2(a[e]).dot(V2(b[e]));
+    S.fscal[7] = s;
+  }
+  __syncthreads();
+  double r = (double)S.fscal[7];
+  __syncthreads();
+  return r;
+}
+
+// pbf.rs:738-744 residual norm sqrt(sum inv_diag |r|^2), sequential f32 or f64.
+__device__ double block_res_norm(const float2* r, const float* inv, uint32_t len, bool fp64, FluidShared& S) {
+  if (fp64) {
+    double acc = 0.0;
+    for (uint32_t e = tid(); e < len; e += nthr())
+      acc += (double)inv[e] * ((double)r[e].x * (double)r[e].x + (double)r[e].y * (double)r[e].y);
+    return sqrt(block_sum_d(acc));
+  }
+  if (tid() == 0) {
+    float s = 0.0f;
+    for (uint32_t e = 0; e < len; ++e) s += inv[e] * V2(r[e]).len2();
+    S.fscal[6] = sqrtf(s);
+  }
+  __syncthreads();
+  double v = (double)S.fscal[6];
+  __syncthreads();
+  return v;
+}
+
+// pbf.rs:359-377 laplacian row i.
+__device__ __forceinline__ V2 laplacian_row(const MillDev& m, const float2* v, uint32_t i) {
+  V2 sum;
+  V2 vi(v[i]);
+  for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
+    uint32_t j = m.nbrs[k];
+    V2 e(m.visc_dir[k]);
+    sum += (CENTRAL_VISC * m.visc_w[k] * e.dot(vi - V2(v[j]))) * e;
+  }
+  return sum;
+}
+
+// pbf.rs:544-625 squeeze-film coefficient pieces (f64, mac/lubrication.rs:49-115)
+__device__ __forceinline__ double film_coefficient(const FilmConsts& f, double h) {
+  double eps = h / f.r;
+  return f.prefactor / (h * sqrt(h)) * (1.0 + f.c1 * eps + f.c2 * eps * eps);
+}
+__device__ __forceinline__ double resolved_ratio(double hc) {
+  const double T0[6] = {0.0, 0.5, 1.0, 2.0, 4.0, 8.0};
+  const double T1[6] = {0.0, 0.06, 0.25, 0.90, 0.99, 1.0};
+  if (hc >= 8.0) return 1.0;
+  double h = hc < 0.0 ? 0.0 : hc;
+  if (hc != hc) h = 0.0;
+  for (int k = 0; k < 5; ++k) {
+    if (h <= T0[k + 1]) {
+      double t = (h - T0[k]) / (T0[k + 1] - T0[k]);
+      return T1[k] + t * (T1[k + 1] - T1[k]);
+    }
+  }
+  return 1.0;
+}
+
+// One squeeze link candidate (ball i, partner j or wall); returns false when not in range.
+struct LinkEval { bool in_range, emit; V2 n; float c; };
+
+__device__ __forceinline__ LinkEval link_pair(const MillDev& m, const StepUniform& U, uint32_t i, uint32_t j,
+                                              float reach, float range2, double dxd, float c_max) {
+  LinkEval L{false, false, V2(), 0.0f};
+  float r = m.b_r;
+  V2 xi(m.bx[i]);
+  V2 e = V2(m.bx[j]) - xi;
+  if (e.len2() >= range2 || !e.finite()) return L;
+  float dist = e.len();
+  float gap = dist - 2.0f * r;
+  if (gap >= reach || dist < 1e-9f) return L;
+  L.in_range = true;
+  L.n = e / dist;
+  if (L.n.dot(V2(m.ball_v0[i]) - V2(m.ball_v0[j])) <= 0.0f) return L;
+  double weight = 1.0 - resolved_ratio((double)gap / dxd);
+  double hh = (double)gap > 0.02 * (double)r ? (double)gap : 0.02 * (double)r;
+  double c = weight * film_coefficient(U.pair_film, hh);
+  L.emit = true;
+  L.c = fmin_r(1.0f * (float)c, c_max);
+  return L;
+}
+__device__ __forceinline__ LinkEval link_wall(const MillDev& m, const StepUniform& U, uint32_t i, float reach,
+                                              double dxd, float c_max) {
+  LinkEval L{false, false, V2(), 0.0f};
+  float r = m.b_r;
+  V2 xi(m.bx[i]);
+  float dist = xi.len();
+  float gap = U.drum_radius - r - dist;
+  if (!(gap < reach && dist > 1e-9f)) return L;
+  L.in_range = true;
+  L.n = xi / dist;
+  if (L.n.dot(V2(m.ball_v0[i])) <= 0.0f) return L;
+  double weight = 1.0 - resolved_ratio((double)gap / dxd);
+  double hh = (double)gap > 0.02 * (double)r ? (double)gap : 0.02 * (double)r;
+  double c = weight * film_coefficient(U.wall_film, hh);
+  L.emit = true;
+  L.c = fmin_r(1.0f * (float)c, c_max);
+  return L;
+}
+
+// Joint-system operator of pbf.rs:703-737 applied to xx, written to out (all rows).
+__device__ void joint_apply(const MillDev& m, float dt, const float2* xx, float2* out) {
+  uint32_t n = m.nf, nb = m.nb;
+  float mass = m.f_mass;
+  float k = dt * mass;
+  for (uint32_t i = tid(); i < n; i += nthr()) m.cg_lv[i] = laplacian_row(m, xx, i).f2();
+  __syncthreads();
+  for (uint32_t i = tid(); i < n; i += nthr()) {
+    V2 o = mass * (V2(xx[i]) + dt * V2(m.cg_lv[i]));
+    for (uint32_t q = m.fg_start[i]; q < m.fg_start[i + 1]; ++q) {
+      uint32_t g = m.fg_list[q];
+      uint32_t bi = m.g_ball[g];
+      V2 vb(xx[n + bi]);
+      float w = xx[n + nb + bi].x;
+      V2 rel = V2(xx[i]) - vb;
+      V2 lc(m.g_lc[g]);
+      V2 d = k * (m.g_c[g] * rel - w * V2(-lc.y, lc.x));
+      o += d;
+    }
+    out[i] = o.f2();
+  }
+  for (uint32_t bi = tid(); bi < nb; bi += nthr()) {
+    V2 vb(xx[n + bi]);
+    float w = xx[n + nb + bi].x;
+    V2 o = m.b_m * vb;
+    float oa = m.b_I * w;
+    for (uint32_t g = m.g_off[bi]; g < m.g_off[bi + 1]; ++g) {
+      uint32_t i = m.g_fluid[g];
+      V2 rel = V2(xx[i]) - vb;
+      V2 lc(m.g_lc[g]);
+      V2 d = k * (m.g_c[g] * rel - w * V2(-lc.y, lc.x));
+      o -= d;
+      oa -= k * (cross2(lc, rel) - w * m.g_l2[g]);
+    }
+    for (uint32_t q = m.lo_start[bi]; q < m.lo_start[bi + 1]; ++q) {
+      uint32_t l = m.lo_list[q];
+      V2 rel = V2(xx[n + m.l_ball[l]]) - vb;
+      V2 ln(m.l_n[l]);
+      V2 d = (dt * m.l_c[l] * ln.dot(rel)) * ln;
+      o -= d;
+    }
+    for (uint32_t l = m.l_off[bi]; l < m.l_off[bi + 1]; ++l) {
+      uint32_t other = m.l_other[l];
+      V2 rel = vb;
+      if (other != NONE) rel = rel - V2(xx[n + other]);
+      V2 ln(m.l_n[l]);
+      V2 d = (dt * m.l_c[l] * ln.dot(rel)) * ln;
+      o += d;
+    }
+    out[n + bi] = o.f2();
+    out[n + nb + bi] = make_float2(oa, 0.0f);
+  }
+  __syncthreads();
+}
+
+__device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err, FluidShared& S) {
+  const uint32_t n = m.nf, nb = m.nb;
+  const float dt = U.dt;
+  for (uint32_t b = tid(); b < nb; b += nthr()) { m.imp[b] = make_float2(0.0f, 0.0f); m.ang[b] = 0.0f; }
+  if (tid() == 0) { memset(&out.fs, 0, sizeof(out.fs)); out.clamp_hits = 0; out.fluid_momentum[0] = out.fluid_momentum[1] = 0.0f; }
+  __syncthreads();
+  if (n == 0 || dt <= 0.0f) return;
+  const float h = m.f_h, rho0 = m.f_rho0, mass = m.f_mass;
+  float2* X = m.fx;
+  float2* V = m.fv;
+  // ---- step 0: sanitize (pbf.rs:1200-1205)
+  for (uint32_t i = tid(); i < n; i += nthr())
+    if (!V2(X[i]).finite() || !V2(V[i]).finite()) { X[i] = make_float2(0.0f, 0.0f); V[i] = make_float2(0.0f, 0.0f); }
+  __syncthreads();
+  // ball grid for the overlap push (pbf.rs:1214-1222)
+  const float contact_radius = m.b_r + OVERLAP_PUSH_MARGIN * h;
+  if (nb > 0) grid_build(m.bx, nb, fmax_r(fmax_r(2.0f * m.b_r, contact_radius), 1e-6f), m.gBall, S.hBall, err);
+  // ---- step 1: predict (pbf.rs:1225-1235)
+  for (uint32_t i = tid(); i < n; i += nthr()) {
+    V2 x(X[i]), v(V[i]);
+    m.x0[i] = X[i];
+    v.y += GRAVITY * dt;
+    x += v * dt;
+    X[i] = x.f2();
+    V[i] = v.f2();
+  }
+  __syncthreads();
+  // ---- step 2: grid + neighbour lists (pbf.rs:1238-1239)
+  grid_build(X, n, h, m.gA, S.hA, err);
+  build_neighbor_lists(X, n, h, S.hA, m.gA, m.nbr_off, m.nbrs, m.cap_edges, err, &S.n_edges);
+  if (tid() == 0) out.ctr.n_fluid_edges = S.n_edges;
+  if (*err) return;
+  // ---- step 3: density constraint (pbf.rs:1257-1334)
+  const uint32_t base_it = U.pbf_iterations > 1 ? U.pbf_iterations : 1u;
+  const float m_rho = mass / rho0;
+  const float self_rho = mass * poly6(0.0f, h);
+  uint32_t iter_count = 0;
+  for (;;) {
+    float max_c = 0.0f;
+    for (uint32_t i = tid(); i < n; i += nthr()) {
+      V2 xi(X[i]);
+      float rho = self_rho;
+      V2 grad_self;
+      float sum_grad_sq = 0.0f;
+      for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
+        V2 delta = xi - V2(X[m.nbrs[k]]);
+        float r2 = delta.len2();
+        rho += mass * poly6(r2, h);
+        float r = delta.len();
+        V2 grad = spiky_grad(delta, r, h) * m_rho;
+        grad_self += grad;
+        sum_grad_sq += grad.len2();
+      }
+      m.density[i] = rho;
+      float c_i = fmax_r(rho / rho0 - 1.0f, 0.0f);
+      max_c = fmax_r(max_c, c_i);
+      sum_grad_sq += grad_self.len2();
+      m.lambda[i] = -c_i / (sum_grad_sq + EPSILON_RELAX);
+    }
+    max_c = block_max_f(max_c);
+    for (uint32_t i = tid(); i < n; i += nthr()) {
+      V2 xi(X[i]);
+      float li = m.lambda[i];
+      V2 sum;
+      for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
+        uint32_t j = m.nbrs[k];
+        V2 delta = xi - V2(X[j]);
+        float r = delta.len();
+        sum += (li + m.lambda[j]) * spiky_grad(delta, r, h);
+      }
+      m.dp[i] = (sum * m_rho).f2();
+    }
+    __syncthreads();
+    for (uint32_t i = tid(); i < n; i += nthr()) X[i] = (V2(X[i]) + V2(m.dp[i])).f2();
+    __syncthreads();
+    iter_count += 1;
+    bool converged = max_c <= COMPRESSION_TOL;
+    if ((iter_count >= base_it && converged) || iter_count >= base_it + ADAPTIVE_MAX_EXTRA) break;
+  }
+  if (tid() == 0) out.ctr.density_iters = iter_count;
+  // ---- step 3.5: ball overlap push (pbf.rs:1361-1444); two passes (count, fill), then the
+  // per-ball reaction sums replayed in the reference's (fluid index, near order) order.
+  for (uint32_t i = tid(); i < n; i += nthr()) m.push_ex[i] = make_float2(0.0f, 0.0f);
+  if (nb > 0) {
+    const float reduced_mass = m.b_m > 0.0f ? (mass * m.b_m) / (mass + m.b_m) : mass;
+    for (int pass = 0; pass < 2; ++pass) {
+      for (uint32_t i = tid(); i < n; i += nthr()) {
+        V2 xi(X[i]);
+        V2 vi(V[i]);
+        V2 ex;
+        uint32_t c = 0, o = pass ? m.rec_cnt[i] : 0;
+        V2 xq = xi;
+        for_each_near(S.hBall, m.gBall, xq, [&](uint32_t b) {
+          V2 delta = xi - V2(m.bx[b]);
+          float dist = delta.len();
+          if (isnan_f(dist) || dist >= contact_radius) return;
+          V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
+          float push_mag = fmin_r(contact_radius - dist, 0.5f * m.b_r);
+          xi += push_mag * n_hat;
+          V2 lever = n_hat * m.b_r;
+          V2 v_surface = V2(m.bv[b]) + m.bom[b] * V2(-lever.y, lever.x);
+          float arrest = fmax_r(-(vi - v_surface).dot(n_hat), 0.0f);
+          float full = mass * push_mag / dt;
+          float imag = fmin_r(full, reduced_mass * arrest);
+          ex += ((full - imag) / mass) * n_hat;
+          if (pass) {
+            V2 reaction = -imag * n_hat;
+            if (o < m.cap_recs) {
+              m.rec_i[o] = i;
+              m.rec_b[o] = b;
+              m.rec_J[o] = reaction.f2();
+              m.rec_L[o] = cross2(lever, reaction);
+              m.rec_M[o] = (imag * n_hat).f2();
+            }
+            ++o;
+          }
+          ++c;
+        });
+        if (!pass) {
+          m.rec_cnt[i] = c;
+        } else {
+          X[i] = xi.f2();
+          m.push_ex[i] = ex.f2();
+        }
+      }
+      __syncthreads();
+      if (!pass) {
+        if (tid() == 0) m.rec_cnt[n] = 0;
+        __syncthreads();
+        S.n_recs = 0;
+        uint32_t tot = block_exclusive_scan(m.rec_cnt, n + 1);
+        if (tot > m.cap_recs) { if (tid() == 0) atomicOr(err, ERR_RECORDS); __syncthreads(); return; }
+        if (tid() == 0) S.n_recs = tot;
+        __syncthreads();
+      }
+    }
+    if (tid() == 0) {
+      V2 mom;
+      for (uint32_t q = 0; q < S.n_recs; ++q) {
+        uint32_t b = m.rec_b[q];
+        m.imp[b] = (V2(m.imp[b]) + V2(m.rec_J[q])).f2();
+        mom += V2(m.rec_M[q]);
+        m.ang[b] += m.rec_L[q];
+      }
+      S.fscal[0] = mom.x;
+      S.fscal[1] = mom.y;
+    }
+  } else if (tid() == 0) {
+    S.fscal[0] = S.fscal[1] = 0.0f;
+  }
+  __syncthreads();
+  // ---- step 3.6a: cohesion (pbf.rs:1464-1491)
+  const float cohesion_accel = (fmax_r(U.slurry.surface_tension_n_m, 0.0f) / 0.072f) * 2.0f * fabsf(GRAVITY);
+  for (uint32_t i = tid(); i < n; i += nthr()) {
+    V2 pull;
+    if (cohesion_accel > 0.0f) {
+      V2 xi(X[i]);
+      for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
+        V2 delta = xi - V2(X[m.nbrs[k]]);
+        float r = delta.len();
+        if (r <= 1e-9f) continue;
+        float w = mass * cohesion_kernel(r, h) / rho0;
+        pull -= w * (delta / r);
+      }
+      m.coh_dv[i] = (cohesion_accel * pull * dt).f2();
+    } else {
+      m.coh_dv[i] = make_float2(0.0f, 0.0f);
+    }
+    m.adh_dv[i] = make_float2(0.0f, 0.0f);
+  }
+  __syncthreads();
+  // ---- step 3.6b: adhesion (pbf.rs:1515-1631) on the stale step-2 grid
+  const float wett = clamp_r(U.slurry.wettability, 0.0f, 1.0f);
+  const uint32_t count_pb = U.boundary_count;
+  if (wett > 0.0f && nb > 0 && m.b_r > 0.0f && count_pb > 0) {
+    const float h_adh = fmin_r(h, 2.0f * m.b_r);
+    if (h_adh > 0.0f) {
+      const float adhesion_accel = wett * 2.0f * fabsf(GRAVITY);
+      const float range2 = h_adh * h_adh * (1.0f + 1e-4f);
+      const float inner2 = 0.25f * h_adh * h_adh * (1.0f - 1e-4f);
+      for (uint32_t b = tid(); b < nb; b += nthr()) {
+        uint32_t base = b * m.cap_items, cnt = 0;
+        bool overflow = false;
+        V2 xb(m.bx[b]);
+        if (xb.finite()) {
+          for (uint32_t q = 0; q < count_pb; ++q) {
+            V2 bp = xb + U.boundary_offset[q];
+            for_each_near(S.hA, m.gA, bp, [&](uint32_t j) {
+              V2 delta = bp - V2(X[j]);
+              float r2 = delta.len2();
+              if (r2 >= range2 || r2 <= inner2) return;
+              float r = sqrtf(r2);
+              if (!finite_f(r) || r <= 0.5f * h_adh || r >= h_adh) return;
+              float w = mass * adhesion_kernel(r, h_adh) / rho0;
+              if (w <= 0.0f) return;
+              V2 n_hat = delta / r;
+              uint32_t s = 0;
+              while (s < cnt && m.item_j[base + s] != j) ++s;
+              if (s == cnt) {
+                if (cnt >= m.cap_items) { overflow = true; return; }
+                m.item_j[base + s] = j;
+                m.item_v[base + s] = (w * n_hat).f2();
+                m.item_w[base + s] = w;
+                ++cnt;
+              } else {
+                m.item_v[base + s] = (V2(m.item_v[base + s]) + w * n_hat).f2();
+                m.item_w[base + s] += w;
+              }
+            });
+          }
+        }
+        if (overflow) atomicOr(err, ERR_ITEMS);
+        uint32_t used = 0;
+        if (cnt > 0) {
+          float weight_sum = 0.0f;
+          V2 dir_sum;
+          for (uint32_t s = 0; s < cnt; ++s) { dir_sum += V2(m.item_v[base + s]); weight_sum += m.item_w[base + s]; }
+          float pull_len = dir_sum.len();
+          if (weight_sum > 1e-9f && pull_len > 1e-9f) {
+            V2 ball_pull_dir = -dir_sum / pull_len;
+            float coverage = fmin_r(weight_sum, 1.0f);
+            float m_contrib = mass * weight_sum;
+            float attach = m_contrib / (m.b_m + m_contrib);
+            V2 dv_b = ball_pull_dir * (adhesion_accel * coverage * dt * attach);
+            m.imp[b] = (V2(m.imp[b]) + m.b_m * dv_b).f2();
+            V2 lever = ball_pull_dir * m.b_r;
+            m.ang[b] += m.b_m * cross2(lever, dv_b);
+            for (uint32_t s = 0; s < cnt; ++s) {
+              float frac = m.item_w[base + s] / weight_sum;
+              V2 dv_i = -(m.b_m * frac / mass) * dv_b;
+              m.item_v[base + s] = dv_i.f2();
+            }
+            used = cnt;
+          }
+        }
+        m.item_n[b] = used;
+      }
+      __syncthreads();
+      if (*err) return;
+      if (tid() == 0) {
+        V2 mom(S.fscal[0], S.fscal[1]);
+        for (uint32_t b = 0; b < nb; ++b) {
+          uint32_t base = b * m.cap_items;
+          for (uint32_t s = 0; s < m.item_n[b]; ++s) {
+            uint32_t j = m.item_j[base + s];
+            V2 dv_i(m.item_v[base + s]);
+            m.adh_dv[j] = (V2(m.adh_dv[j]) + dv_i).f2();
+            mom += mass * dv_i;
+          }
+        }
+        S.fscal[0] = mom.x;
+        S.fscal[1] = mom.y;
+      }
+      __syncthreads();
+    }
+  }
+  // ---- step 4: wall projection (pbf.rs:1635-1653)
+  for (uint32_t i = tid(); i < n; i += nthr()) {
+    V2 x(X[i]);
+    float d;
+    V2 normal;
+    drum_sdf_world(U, x, U.to_local_next, U.to_world_next, d, normal);
+    if (d < 0.0f) {
+      x += -d * normal;
+      X[i] = x.f2();
+      V2 push = mass * (-d * normal) / dt;
+      m.dv_tmp[i] = push.f2();
+      m.f_tmp[i] = cross2(x, push);
+      float angle = atan2f_r(x.y, x.x);
+      uint32_t bin = f2u_sat(((angle + PI_F) / TAU_F) * 32.0f);
+      m.wall_bin[i] = (int32_t)(bin < 31u ? bin : 31u);
+      m.wall_val[i] = mass * -d / dt;
+    } else {
+      m.wall_bin[i] = -1;
+    }
+  }
+  __syncthreads();
+  if (tid() == 0) {
+    double ix = 0.0, iy = 0.0, ia = 0.0;
+    float bins[32];
+    for (int k = 0; k < 32; ++k) bins[k] = 0.0f;
+    for (uint32_t i = 0; i < n; ++i) {
+      int32_t bin = m.wall_bin[i];
+      if (bin < 0) continue;
+      V2 push(m.dv_tmp[i]);
+      ix += (double)push.x;
+      iy += (double)push.y;
+      ia += (double)m.f_tmp[i];
+      bins[bin] += m.wall_val[i];
+    }
+    S.dscal[0] = ix;
+    S.dscal[1] = iy;
+    S.dscal[2] = ia;
+    for (int k = 0; k < 32; ++k) out.fs.wall_normal_impulse_by_angle[k] = bins[k];
+  }
+  __syncthreads();
+  // ---- step 5: velocity reconstruction (pbf.rs:1656-1674)
+  for (uint32_t i = tid(); i < n; i += nthr()) {
+    V2 v = (V2(X[i]) - V2(m.x0[i])) / dt;
+    v -= V2(m.push_ex[i]);
+    v += V2(m.coh_dv[i]);
+    v += V2(m.adh_dv[i]);
+    V[i] = v.f2();
+  }
+  __syncthreads();
+  // ---- step 6: wall no-slip (pbf.rs:1677-1700)
+  const float beta = clamp_r(U.slurry.wall_no_slip, 0.0f, 1.0f);
+  double ke_before_noslip = kinetic_energy_seq(V, n, mass, S);
+  if (beta > 0.0f) {
+    for (uint32_t i = tid(); i < n; i += nthr()) {
+      if (m.wall_bin[i] < 0) continue;
+      V2 x(X[i]);
+      V2 v_wall = wall_velocity(U.drum_omega, x);
+      V2 v_old(V[i]);
+      V2 v = (1.0f - beta) * v_old + beta * v_wall;
+      V[i] = v.f2();
+      m.dv_tmp[i] = (v - v_old).f2();
+    }
+    __syncthreads();
+    if (tid() == 0) {
+      float work = 0.0f;
+      double ix = S.dscal[0], iy = S.dscal[1], ia = S.dscal[2];
+      for (uint32_t i = 0; i < n; ++i) {
+        if (m.wall_bin[i] < 0) continue;
+        V2 x(X[i]);
+        V2 v_wall = wall_velocity(U.drum_omega, x);
+        V2 dv(m.dv_tmp[i]);
+        work += mass * dv.dot(v_wall);
+        ix += (double)(mass * dv.x);
+        iy += (double)(mass * dv.y);
+        ia += (double)cross2(x, mass * dv);
+      }
+      S.dscal[0] = ix;
+      S.dscal[1] = iy;
+      S.dscal[2] = ia;
+      out.fs.wall_work_j = work;
+    }
+    __syncthreads();
+  }
+  double ke_mark = kinetic_energy_seq(V, n, mass, S);
+  const double ke_delta_noslip = ke_mark - ke_before_noslip;
+  // ---- step 6.5: ball drag, Gauss-Seidel over balls (pbf.rs:1777-2013)
+  const float mu = fmax_r(U.slurry.viscosity_pa_s, 0.0f);
+  if (nb > 0 && m.b_r > 0.0f && m.b_rtrue > 0.0f && mu > 1e-6f) {
+    const float beta_b = clamp_r(U.slurry.ball_no_slip, 0.0f, 1.0f);
+    const float rot_cap = 0.2f * fluid_vmax(U);
+    const float rho_ball = m.b_m / (PI_F * m.b_r * m.b_r);
+    const float mass_true = rho_ball * PI_F * m.b_rtrue * m.b_rtrue;
+    if (beta_b > 0.0f) {
+      const float h_c = m.b_r + h;
+      const float w_hc0 = fmax_r(poly6(0.0f, h_c), 1e-12f);
+      grid_build(X, n, fmax_r(h_c, 1e-6f), m.gB, S.hB, err);
+      // item lists per ball (positions do not change during the sweep)
+      for (uint32_t b = tid(); b < nb; b += nthr()) {
+        uint32_t base = b * m.cap_items, cnt = 0;
+        bool overflow = false;
+        V2 xb(m.bx[b]);
+        if (xb.finite()) {
+          for_each_near(S.hB, m.gB, xb, [&](uint32_t j) {
+            V2 r_i = V2(X[j]) - xb;
+            float r2 = r_i.len2();
+            if (!finite_f(r2) || r2 >= h_c * h_c) return;
+            float phi = poly6(r2, h_c) / w_hc0;
+            if (phi <= 0.0f) return;
+            if (cnt >= m.cap_items) { overflow = true; return; }
+            m.item_j[base + cnt] = j;
+            m.item_v[base + cnt] = r_i.f2();
+            m.item_w[base + cnt] = phi;
+            ++cnt;
+          });
+        }
+        if (overflow) atomicOr(err, ERR_ITEMS);
+        m.item_n[b] = cnt;
+        atomicAdd(&out.ctr.n_coupling_items, cnt);
+      }
+      __syncthreads();
+      if (*err) return;
+      if (tid() == 0) {
+        const float i_b = m.b_I;
+        V2 mom(S.fscal[0], S.fscal[1]);
+        for (uint32_t b = 0; b < nb; ++b) {
+          uint32_t base = b * m.cap_items, cnt = m.item_n[b];
+          if (cnt == 0) continue;
+          float m_ent = 0.0f, i_ent = 0.0f, l_sum = 0.0f;
+          V2 r_sum, v_sum;
+          for (uint32_t s = 0; s < cnt; ++s) {
+            uint32_t j = m.item_j[base + s];
+            V2 r_i(m.item_v[base + s]);
+            float phi = m.item_w[base + s];
+            float r2 = r_i.len2();
+            float w = mass * phi;
+            V2 vj(V[j]);
+            m_ent += w;
+            r_sum += w * r_i;
+            v_sum += w * vj;
+            i_ent += w * r2;
+            l_sum += w * cross2(r_i, vj);
+          }
+          if (m_ent <= 1e-12f) continue;
+          V2 r_bar = r_sum / m_ent;
+          V2 v_bar = v_sum / m_ent;
+          V2 v_rel = v_bar - V2(m.bv[b]);
+          float speed_rel = v_rel.len();
+          float inv_tau_form = (speed_rel > 1e-6f && rho0 > 0.0f)
+                                   ? 0.5f * rho0 * 1.0f * (2.0f * m.b_rtrue) * speed_rel / mass_true
+                                   : 0.0f;
+          float bt = beta_b * (1.0f - expf_r(-dt * (0.0f + inv_tau_form)));
+          float a_lin = bt * m_ent / (m.b_m + m_ent);
+          V2 dv_b = a_lin * v_rel;
+          float dw_b = 0.0f, c_rot = 0.0f;
+          V2 p_bar;
+          if (i_ent > 1e-12f) {
+            float omega_bar = l_sum / i_ent;
+            float a_rot = bt * i_ent / (i_b + i_ent);
+            float candidate_dw = a_rot * (omega_bar - m.bom[b]);
+            p_bar = V2(-r_bar.y, r_bar.x);
+            float s = 0.0f, s_scale = 0.0f;
+            for (uint32_t q = 0; q < cnt; ++q) {
+              V2 r_i(m.item_v[base + q]);
+              float phi = m.item_w[base + q];
+              V2 perp_i(-r_i.y, r_i.x);
+              float phi2 = phi * phi;
+              s += mass * phi2 * cross2(r_i, perp_i - p_bar);
+              s_scale += mass * phi2 * r_i.len2();
+            }
+            if (fabsf(s) > 0.1f * s_scale) {
+              float raw_c_rot = -i_b * candidate_dw / s;
+              float max_lever = 2.0f * h_c;
+              float cap = max_lever > 1e-9f ? rot_cap / max_lever : 0.0f;
+              c_rot = clamp_r(raw_c_rot, -cap, cap);
+              dw_b = -c_rot * s / i_b;
+            }
+          }
+          for (uint32_t q = 0; q < cnt; ++q) {
+            uint32_t j = m.item_j[base + q];
+            V2 r_i(m.item_v[base + q]);
+            float phi = m.item_w[base + q];
+            V2 dv_i = -(m.b_m / m_ent) * dv_b * phi;
+            if (c_rot != 0.0f) {
+              V2 perp_i(-r_i.y, r_i.x);
+              dv_i += c_rot * phi * (perp_i - p_bar);
+            }
+            V[j] = (V2(V[j]) + dv_i).f2();
+            mom += mass * dv_i;
+          }
+          m.imp[b] = (V2(m.imp[b]) + m.b_m * dv_b).f2();
+          m.ang[b] += i_b * dw_b + m.b_m * cross2(r_bar, dv_b);
+        }
+        S.fscal[0] = mom.x;
+        S.fscal[1] = mom.y;
+      }
+      __syncthreads();
+    }
+  }
+  double ke_after_drag = kinetic_energy_seq(V, n, mass, S);
+  const double ke_delta_drag = ke_after_drag - ke_mark;
+  ke_mark = ke_after_drag;
+  // ---- step 6.6: buoyancy, Gauss-Seidel over balls on the stale step-2 grid (pbf.rs:2035-2122)
+  if (nb > 0 && m.b_r > 0.0f) {
+    const float area = PI_F * m.b_r * m.b_r;
+    for (uint32_t b = tid(); b < nb; b += nthr()) {
+      uint32_t base = b * m.cap_items, cnt = 0;
+      bool overflow = false;
+      V2 xb(m.bx[b]);
+      float rho_local = 0.0f;
+      if (xb.finite()) {
+        for_each_near(S.hA, m.gA, xb, [&](uint32_t j) {
+          float r2 = (xb - V2(X[j])).len2();
+          float w = mass * poly6(r2, h);
+          if (w > 0.0f) {
+            rho_local += w;
+            if (cnt >= m.cap_items) { overflow = true; return; }
+            m.item_j[base + cnt] = j;
+            m.item_w[base + cnt] = w;
+            ++cnt;
+          }
+        });
+      }
+      if (overflow) atomicOr(err, ERR_ITEMS);
+      m.item_n[b] = rho_local > 0.0f ? cnt : 0u;
+      if (rho_local > 0.0f) atomicAdd(&out.ctr.n_coupling_items, cnt);
+      m.item_v[base] = make_float2(rho_local, 0.0f);
+    }
+    __syncthreads();
+    if (*err) return;
+    if (tid() == 0) {
+      V2 mom(S.fscal[0], S.fscal[1]);
+      const float om_abs = fabsf(U.drum_omega);
+      for (uint32_t b = 0; b < nb; ++b) {
+        uint32_t base = b * m.cap_items, cnt = m.item_n[b];
+        if (cnt == 0) continue;
+        float rho_local = m.item_v[base].x;
+        float rho_eff = fmin_r(rho_local, rho0);
+        float num = 0.0f, den = 0.0f;
+        for (uint32_t s = 0; s < cnt; ++s) {
+          uint32_t j = m.item_j[base + s];
+          V2 d(X[j]);
+          float d2 = d.len2();
+          if (d2 <= 1e-12f) continue;
+          float w = m.item_w[base + s];
+          num += w * cross2(d, V2(V[j])) / d2;
+          den += w;
+        }
+        float omega_local = den > 0.0f ? clamp_r(num / den, -om_abs, om_abs) : 0.0f;
+        V2 xb(m.bx[b]);
+        V2 g_eff = V2(0.0f, GRAVITY) + omega_local * omega_local * xb;
+        V2 impulse = -rho_eff * area * g_eff * dt;
+        m.imp[b] = (V2(m.imp[b]) + impulse).f2();
+        for (uint32_t s = 0; s < cnt; ++s) {
+          uint32_t j = m.item_j[base + s];
+          float frac = m.item_w[base + s] / rho_local;
+          V2 dv = -(impulse * frac) / mass;
+          V[j] = (V2(V[j]) + dv).f2();
+          mom += mass * dv;
+        }
+      }
+      S.fscal[0] = mom.x;
+      S.fscal[1] = mom.y;
+    }
+    __syncthreads();
+  }
+  double ke_after_buoy = kinetic_energy_seq(V, n, mass, S);
+  const double ke_delta_buoy = ke_after_buoy - ke_mark;
+  ke_mark = ke_after_buoy;
+  // ---- density recompute at final x over the step-2 lists (pbf.rs:2137-2144)
+  for (uint32_t i = tid(); i < n; i += nthr()) {
+    V2 xi(X[i]);
+    float rho = self_rho;
+    for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) rho += mass * poly6((xi - V2(X[m.nbrs[k]])).len2(), h);
+    m.density[i] = rho;
+  }
+  __syncthreads();
+  // ---- step 7: implicit viscosity (pbf.rs:2146-2300)
+  uint32_t visc_iters = 0;
+  const bool fp64 = U.cg_fp64 != 0;
+  if (mu > 0.0f) {
+    const bool bingham = U.slurry.rheology == MG_RHEOLOGY_BINGHAM && U.slurry.yield_stress_pa > 0.0f;
+    const float tau_y = U.slurry.yield_stress_pa;
+    for (uint32_t i = tid(); i < n; i += nthr()) {
+      float mu_i = mu;
+      if (bingham) {
+        // pbf.rs:821-868 shear rate then Papanastasiou viscosity
+        V2 xi(X[i]), vi(V[i]);
+        float gxx = 0.0f, gxy = 0.0f, gyx = 0.0f, gyy = 0.0f;
+        for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
+          uint32_t j = m.nbrs[k];
+          V2 delta = xi - V2(X[j]);
+          float r = delta.len();
+          V2 grad = spiky_grad(delta, r, h);
+          float coeff = mass / fmax_r(m.density[j], 1e-6f);
+          V2 dv = V2(V[j]) - vi;
+          gxx += coeff * dv.x * grad.x;
+          gxy += coeff * dv.x * grad.y;
+          gyx += coeff * dv.y * grad.x;
+          gyy += coeff * dv.y * grad.y;
+        }
+        float dxy = 0.5f * (gxy + gyx);
+        float g = sqrtf(2.0f * (gxx * gxx + gyy * gyy + 2.0f * dxy * dxy));
+        float gamma0 = tau_y / (100.0f * mu);
+        g = finite_f(g) ? g : 0.0f;
+        float extra = g < 1e-4f * gamma0 ? tau_y / gamma0 : tau_y * (1.0f - expf_r(-g / gamma0)) / g;
+        mu_i = mu + extra;
+      }
+      m.mu_eff[i] = mu_i;
+    }
+    __syncthreads();
+    const float eta2 = VISC_ETA * h * h;
+    for (uint32_t i = tid(); i < n; i += nthr()) {
+      V2 xi(X[i]);
+      float rho_i = fmax_r(m.density[i], 1e-6f);
+      float mu_i = m.mu_eff[i];
+      for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
+        uint32_t j = m.nbrs[k];
+        float rho_j = fmax_r(m.density[j], 1e-6f);
+        V2 delta = xi - V2(X[j]);
+        float r = delta.len();
+        V2 grad = spiky_grad(delta, r, h);
+        float numerator = (mass * (mu_i + m.mu_eff[j]) / (rho_i * rho_j)) * fabsf(delta.dot(grad));
+        m.visc_w[k] = numerator / (delta.len2() + eta2);
+        m.visc_dir[k] = (r > 1e-9f ? delta / r : V2(1.0f, 0.0f)).f2();
+      }
+    }
+    __syncthreads();
+    // boundary groups (pbf.rs:2159-2232) on a fresh h-grid, one ball per thread, merged per fluid
+    if (tid() == 0) { S.n_groups = 0; S.n_links = 0; S.links_in_range = 0; }
+    __syncthreads();
+    if (nb > 0 && m.b_r > 0.0f) {
+      grid_build(X, n, h, m.gB, S.hB, err);
+      const float spiky_norm = -30.0f / (PI_F * powi5(h));
+      const float range2 = h * h * (1.0f + 1e-4f);
+      for (uint32_t j = tid(); j < n; j += nthr())
+        m.f_tmp[j] = BALL_BC_GAIN * (mass * 2.0f * m.mu_eff[j] / (fmax_r(m.density[j], 1e-6f) * rho0));
+      __syncthreads();
+      for (uint32_t b = tid(); b < nb; b += nthr()) {
+        uint32_t base = b * m.cap_items, cnt = 0;
+        bool overflow = false;
+        V2 xb(m.bx[b]);
+        if (xb.finite()) {
+          for (uint32_t q = 0; q < count_pb; ++q) {
+            V2 bp = xb + U.boundary_offset[q];
+            for_each_near(S.hB, m.gB, bp, [&](uint32_t j) {
+              V2 delta = V2(X[j]) - bp;
+              float r2 = delta.len2();
+              if (r2 >= range2) return;
+              float r = sqrtf(r2);
+              if (!finite_f(r) || r >= h || r <= 1e-9f) return;
+              float dot_abs = fabsf(spiky_norm * (h - r) * (h - r) * r);
+              float c = m.f_tmp[j] * dot_abs / (r2 + eta2);
+              if (!(c > 0.0f)) return;
+              V2 lever = bp - xb;
+              V2 lever_c = c * lever;
+              float lever2_c = c * lever.len2();
+              uint32_t s = 0;
+              while (s < cnt && m.item_j[base + s] != j) ++s;
+              if (s == cnt) {
+                if (cnt >= m.cap_items) { overflow = true; return; }
+                m.item_j[base + s] = j;
+                m.item_w[base + s] = c;
+                m.item_v[base + s] = lever_c.f2();
+                m.item_w2[base + s] = lever2_c;
+                ++cnt;
+              } else {
+                m.item_w[base + s] += c;
+                m.item_v[base + s] = (V2(m.item_v[base + s]) + lever_c).f2();
+                m.item_w2[base + s] += lever2_c;
+              }
+            });
+          }
+        }
+        if (overflow) atomicOr(err, ERR_ITEMS);
+        m.g_off[b] = cnt;
+      }
+      if (tid() == 0) m.g_off[nb] = 0;
+      __syncthreads();
+      if (*err) return;
+      uint32_t ng = block_exclusive_scan(m.g_off, nb + 1);
+      if (ng > m.cap_groups) { if (tid() == 0) atomicOr(err, ERR_GROUPS); __syncthreads(); return; }
+      for (uint32_t b = tid(); b < nb; b += nthr()) {
+        uint32_t base = b * m.cap_items, o = m.g_off[b], cnt = m.g_off[b + 1] - o;
+        for (uint32_t s = 0; s < cnt; ++s) {
+          m.g_fluid[o + s] = m.item_j[base + s];
+          m.g_ball[o + s] = b;
+          m.g_c[o + s] = m.item_w[base + s];
+          m.g_lc[o + s] = m.item_v[base + s];
+          m.g_l2[o + s] = m.item_w2[base + s];
+        }
+      }
+      if (tid() == 0) S.n_groups = ng;
+      __syncthreads();
+    }
+    // ball_v0 (pbf.rs:2237-2239) and squeeze links (pbf.rs:544-625)
+    for (uint32_t b = tid(); b < nb; b += nthr()) {
+      m.ball_v0[b] = (V2(m.bv[b]) + V2(m.imp[b]) / m.b_m).f2();
+      m.ball_w0[b] = m.bom[b] + m.ang[b] / m.b_I;
+    }
+    __syncthreads();
+    if (nb > 0 && m.b_r > 0.0f) {
+      const float r = m.b_r;
+      const double dxd = (double)(0.5f * h);
+      const float reach = (float)(8.0 * dxd);
+      const float c_max = 8.0f * m.b_m / fmax_r(dt, 1e-12f);
+      const float range2 = (2.0f * r + reach) * (2.0f * r + reach) * (1.0f + 1e-4f);
+      grid_build(m.bx, nb, 2.0f * r + reach, m.gBall, S.hBall, err);
+      uint32_t in_range = 0;
+      for (int pass = 0; pass < 2; ++pass) {
+        for (uint32_t i = tid(); i < nb; i += nthr()) {
+          V2 xi(m.bx[i]);
+          uint32_t c = 0, o = pass ? m.l_off[i] : 0u;
+          if (xi.finite()) {
+            for_each_near(S.hBall, m.gBall, xi, [&](uint32_t j) {
+              if (j <= i) return;
+              LinkEval L = link_pair(m, U, i, j, reach, range2, dxd, c_max);
+              if (!pass && L.in_range) in_range += 1;
+              if (!L.emit) return;
+              if (pass) { m.l_ball[o] = i; m.l_other[o] = j; m.l_n[o] = L.n.f2(); m.l_c[o] = L.c; ++o; }
+              ++c;
+            });
+            LinkEval W = link_wall(m, U, i, reach, dxd, c_max);
+            if (!pass && W.in_range) in_range += 1;
+            if (W.emit) {
+              if (pass) { m.l_ball[o] = i; m.l_other[o] = NONE; m.l_n[o] = W.n.f2(); m.l_c[o] = W.c; ++o; }
+              ++c;
+            }
+          }
+          if (!pass) m.l_off[i] = c;
+        }
+        if (!pass) {
+          if (tid() == 0) m.l_off[nb] = 0;
+          __syncthreads();
+          uint32_t tot_in = block_sum_u(in_range);
+          uint32_t nl = block_exclusive_scan(m.l_off, nb + 1);
+          if (nl > m.cap_links) { if (tid() == 0) atomicOr(err, ERR_LINKS); __syncthreads(); return; }
+          if (tid() == 0) { S.n_links = nl; S.links_in_range = tot_in; }
+        }
+        __syncthreads();
+      }
+    }
+    if (tid() == 0) {
+      out.ctr.n_groups = S.n_groups;
+      out.ctr.n_links = S.n_links;
+      out.ctr.links_in_range = S.links_in_range;
+    }
+    __syncthreads();
+    if (S.n_groups == 0 && S.links_in_range == 0) {
+      // ---- fluid-only CG (pbf.rs:423-480), solution in place in V
+      float2 *r = m.cg_r, *p = m.cg_p, *ap = m.cg_ap;
+      double bn2 = block_dot(V, V, n, fp64, S);
+      double b_norm = fp64 ? sqrt(bn2) : (double)sqrtf((float)bn2);
+      if (b_norm > 0.0 && isfinite(b_norm)) {
+        const float target_f = VISC_CG_TOL * (float)b_norm;
+        const double target_d = (double)VISC_CG_TOL * b_norm;
+        auto apply = [&](const float2* in, float2* o) {
+          for (uint32_t i = tid(); i < n; i += nthr()) o[i] = (V2(in[i]) + dt * laplacian_row(m, in, i)).f2();
+          __syncthreads();
+        };
+        apply(V, m.cg_ap);
+        for (uint32_t i = tid(); i < n; i += nthr()) { r[i] = (V2(V[i]) - V2(ap[i])).f2(); p[i] = r[i]; }
+        __syncthreads();
+        double rs_old = block_dot(r, r, n, fp64, S);
+        bool done = fp64 ? sqrt(rs_old) <= target_d : sqrtf((float)rs_old) <= target_f;
+        if (!done) {
+          visc_iters = VISC_CG_MAX;
+          for (uint32_t it = 1; it <= VISC_CG_MAX; ++it) {
+            apply(p, ap);
+            double p_ap = block_dot(p, ap, n, fp64, S);
+            if (p_ap <= 0.0 || !isfinite(p_ap)) { visc_iters = it; break; }
+            float alpha = fp64 ? (float)(rs_old / p_ap) : (float)rs_old / (float)p_ap;
+            for (uint32_t i = tid(); i < n; i += nthr()) {
+              V[i] = (V2(V[i]) + alpha * V2(p[i])).f2();
+              r[i] = (V2(r[i]) - alpha * V2(ap[i])).f2();
+            }
+            __syncthreads();
+            double rs_new = block_dot(r, r, n, fp64, S);
+            bool conv = fp64 ? sqrt(rs_new) <= target_d : sqrtf((float)rs_new) <= target_f;
+            if (conv) { visc_iters = it; break; }
+            float bt = fp64 ? (float)(rs_new / rs_old) : (float)rs_new / (float)rs_old;
+            for (uint32_t i = tid(); i < n; i += nthr()) p[i] = (V2(r[i]) + bt * V2(p[i])).f2();
+            __syncthreads();
+            rs_old = rs_new;
+          }
+        }
+      }
+    } else {
+      // ---- joint fluid + ball Jacobi-PCG (pbf.rs:641-791)
+      const uint32_t len = n + 2 * nb;
+      // per-fluid group lists and per-ball "other" link lists (stable, in group / link order)
+      for (uint32_t g = tid(); g < S.n_groups; g += nthr()) m.rec_i[g] = m.g_fluid[g];
+      __syncthreads();
+      block_bucket_sort(m.rec_i, S.n_groups, n, m.fg_start, m.bk_start, m.fg_list);
+      for (uint32_t l = tid(); l < S.n_links; l += nthr()) m.rec_b[l] = m.l_other[l] == NONE ? nb : m.l_other[l];
+      __syncthreads();
+      block_bucket_sort(m.rec_b, S.n_links, nb + 1, m.lo_start, m.bk_start, m.lo_list);
+      float2 *x = m.cg_x, *bvec = m.cg_b, *r = m.cg_r, *z = m.cg_z, *p = m.cg_p, *ap = m.cg_ap;
+      float *diag = m.cg_diag, *inv = m.cg_inv;
+      const bool use_guess = *m.guess_valid_dev != 0;
+      for (uint32_t i = tid(); i < n; i += nthr()) {
+        V2 v(V[i]);
+        x[i] = (use_guess ? v + V2(m.fguess[i]) : v).f2();
+        bvec[i] = (mass * v).f2();
+        float sw = 0.0f;
+        for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) sw += m.visc_w[k];
+        float d = mass * (1.0f + dt * (0.5f * CENTRAL_VISC * sw));
+        for (uint32_t q = m.fg_start[i]; q < m.fg_start[i + 1]; ++q) d += dt * mass * m.g_c[m.fg_list[q]];
+        diag[i] = d;
+        m.dv_tmp[i] = V[i];  // v_in for the warm start of the next sub-step
+      }
+      for (uint32_t b = tid(); b < nb; b += nthr()) {
+        V2 v0(m.ball_v0[b]);
+        float w0 = m.ball_w0[b];
+        x[n + b] = v0.f2();
+        x[n + nb + b] = make_float2(w0, 0.0f);
+        bvec[n + b] = (m.b_m * v0).f2();
+        bvec[n + nb + b] = make_float2(m.b_I * w0, 0.0f);
+        float dl = m.b_m, da = m.b_I;
+        for (uint32_t g = m.g_off[b]; g < m.g_off[b + 1]; ++g) {
+          dl += dt * mass * m.g_c[g];
+          da += dt * mass * m.g_l2[g];
+        }
+        for (uint32_t q = m.lo_start[b]; q < m.lo_start[b + 1]; ++q) dl += dt * m.l_c[m.lo_list[q]];
+        for (uint32_t l = m.l_off[b]; l < m.l_off[b + 1]; ++l) dl += dt * m.l_c[l];
+        diag[n + b] = dl;
+        diag[n + nb + b] = da;
+      }
+      __syncthreads();
+      for (uint32_t e = tid(); e < len; e += nthr()) inv[e] = 1.0f / fmax_r(diag[e], 1e-20f);
+      __syncthreads();
+      joint_apply(m, dt, x, ap);
+      for (uint32_t e = tid(); e < len; e += nthr()) {
+        V2 re = V2(bvec[e]) - V2(ap[e]);
+        r[e] = re.f2();
+        z[e] = (re * inv[e]).f2();
+      }
+      __syncthreads();
+      double b_norm = block_res_norm(bvec, inv, len, fp64, S);
+      double r_norm = block_res_norm(r, inv, len, fp64, S);
+      double tol_b = fp64 ? (double)VISC_CG_TOL * b_norm : (double)(VISC_CG_TOL * (float)b_norm);
+      if (b_norm > 0.0 && isfinite(b_norm) && r_norm > tol_b) {
+        for (uint32_t e = tid(); e < len; e += nthr()) p[e] = z[e];
+        __syncthreads();
+        double rz_old = block_dot(r, z, len, fp64, S);
+        for (uint32_t it = 1; it <= 4 * VISC_CG_MAX; ++it) {
+          visc_iters = it;
+          joint_apply(m, dt, p, ap);
+          double p_ap = block_dot(p, ap, len, fp64, S);
+          if (p_ap <= 0.0 || !isfinite(p_ap)) break;
+          float alpha = fp64 ? (float)(rz_old / p_ap) : (float)rz_old / (float)p_ap;
+          for (uint32_t e = tid(); e < len; e += nthr()) {
+            x[e] = (V2(x[e]) + alpha * V2(p[e])).f2();
+            r[e] = (V2(r[e]) - alpha * V2(ap[e])).f2();
+          }
+          __syncthreads();
+          if (block_res_norm(r, inv, len, fp64, S) <= tol_b) break;
+          for (uint32_t e = tid(); e < len; e += nthr()) z[e] = (V2(r[e]) * inv[e]).f2();
+          __syncthreads();
+          double rz_new = block_dot(r, z, len, fp64, S);
+          float bt = fp64 ? (float)(rz_new / rz_old) : (float)rz_new / (float)rz_old;
+          for (uint32_t e = tid(); e < len; e += nthr()) p[e] = (V2(z[e]) + bt * V2(p[e])).f2();
+          __syncthreads();
+          rz_old = rz_new;
+        }
+      }
+      for (uint32_t i = tid(); i < n; i += nthr()) {
+        V2 vn(x[i]);
+        V[i] = vn.f2();
+        V2 d = vn - V2(m.dv_tmp[i]);
+        m.fguess[i] = (d.finite() ? d : V2()).f2();
+      }
+      __syncthreads();
+      if (tid() == 0) {
+        m.guess_valid_dev[0] = 1u;
+        V2 mom(S.fscal[0], S.fscal[1]);
+        for (uint32_t b = 0; b < nb; ++b) {
+          V2 dv = V2(x[n + b]) - V2(m.ball_v0[b]);
+          float dw = x[n + nb + b].x - m.ball_w0[b];
+          if (dv.finite() && finite_f(dw)) {
+            m.imp[b] = (V2(m.imp[b]) + m.b_m * dv).f2();
+            m.ang[b] += m.b_I * dw;
+            mom -= m.b_m * dv;
+          }
+        }
+        S.fscal[0] = mom.x;
+        S.fscal[1] = mom.y;
+      }
+      __syncthreads();
+    }
+  }
+  // ---- mean shear rate (pbf.rs:800-849) on the final velocities
+  for (uint32_t i = tid(); i < n; i += nthr()) {
+    V2 xi(X[i]), vi(V[i]);
+    float gxx = 0.0f, gxy = 0.0f, gyx = 0.0f, gyy = 0.0f;
+    for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
+      uint32_t j = m.nbrs[k];
+      V2 delta = xi - V2(X[j]);
+      float r = delta.len();
+      V2 grad = spiky_grad(delta, r, h);
+      float coeff = mass / fmax_r(m.density[j], 1e-6f);
+      V2 dv = V2(V[j]) - vi;
+      gxx += coeff * dv.x * grad.x;
+      gxy += coeff * dv.x * grad.y;
+      gyx += coeff * dv.y * grad.x;
+      gyy += coeff * dv.y * grad.y;
+    }
+    float dxy = 0.5f * (gxy + gyx);
+    m.f_tmp[i] = sqrtf(2.0f * (gxx * gxx + gyy * gyy + 2.0f * dxy * dxy));
+  }
+  __syncthreads();
+  if (tid() == 0) {
+    float s = 0.0f;
+    uint32_t c = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      float g = m.f_tmp[i];
+      if (finite_f(g)) { s += g; c += 1; }
+    }
+    out.fs.mean_shear_rate_per_s = c == 0 ? 0.0f : s / (float)c;
+  }
+  __syncthreads();
+  double ke_after_visc = kinetic_energy_seq(V, n, mass, S);
+  const double ke_delta_visc = ke_after_visc - ke_mark;
+  // ---- step 7.5: speed clamp (pbf.rs:979-996, 2321)
+  const float v_max = fluid_vmax(U);
+  for (uint32_t i = tid(); i < n; i += nthr()) {
+    V2 v(V[i]);
+    float speed = v.len();
+    if (!finite_f(speed)) v = V2();
+    else if (speed > v_max) v *= v_max / speed;
+    V[i] = v.f2();
+  }
+  __syncthreads();
+  double ke_after_clamp = kinetic_energy_seq(V, n, mass, S);
+  // ---- step 8: impulse clamp (pbf.rs:2330-2345)
+  uint32_t hits = 0;
+  if (nb > 0) {
+    const float clamp = 60.0f * m.b_m * 9.81f * dt;
+    const float angular_clamp = clamp * m.b_r;
+    for (uint32_t b = tid(); b < nb; b += nthr()) {
+      V2 J(m.imp[b]);
+      float mag = J.len();
+      if (mag > clamp && mag > 1e-9f) { J *= clamp / mag; hits += 1; }
+      m.imp[b] = J.f2();
+      m.ang[b] = clamp_r(m.ang[b], -angular_clamp, angular_clamp);
+    }
+  }
+  hits = block_sum_u(hits);
+  if (tid() == 0) {
+    out.ctr.cg_iters = visc_iters;
+    out.fs.viscosity_iterations = visc_iters;
+    out.fs.coupling_clamp_hits = hits;
+    out.clamp_hits = hits;
+    out.fs.wall_impulse[0] = (float)S.dscal[0];
+    out.fs.wall_impulse[1] = (float)S.dscal[1];
+    out.fs.wall_angular_impulse = (float)S.dscal[2];
+    out.fs.ke_delta_noslip_j = (float)ke_delta_noslip;
+    out.fs.ke_delta_drag_j = (float)ke_delta_drag;
+    out.fs.ke_delta_buoyancy_j = (float)ke_delta_buoy;
+    out.fs.ke_delta_viscosity_j = (float)ke_delta_visc;
+    out.fs.ke_delta_clamp_j = (float)(ke_after_clamp - ke_after_visc);
+    out.fluid_momentum[0] = S.fscal[0];
+    out.fluid_momentum[1] = S.fscal[1];
+  }
+  __syncthreads();
+}
+
+}  // namespace mg

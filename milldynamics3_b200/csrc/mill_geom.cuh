@@ -1,0 +1,93 @@
+// Drum geometry on the device (geometry.rs:37-275): circle plus trapezoid-lifter SDF in the drum
+// frame, the world-space query with its central-difference normal (EPS = 1e-4), the wall
+// velocity and the swept time of impact. Lifter frames and the drum-angle rotations arrive
+// precomputed in the StepUniform (host trig), so the per-query work is pure f32 arithmetic.
+#pragma once
+
+#include "mill_common.cuh"
+
+namespace mg {
+
+// geometry.rs:258-275 convex_polygon_sdf over the 4 CCW vertices of one lifter.
+__device__ __forceinline__ float convex_quad_sdf(V2 p, const V2* verts) {
+  float min_dist_sq = 3.40282347e38f;
+  bool inside = true;
+  for (int i = 0; i < 4; ++i) {
+    V2 a = verts[i];
+    V2 b = verts[(i + 1) & 3];
+    V2 edge = b - a;
+    V2 to_p = p - a;
+    float len_sq = edge.len2();
+    if (len_sq < 1e-12f) continue;
+    float t = clamp_r(to_p.dot(edge) / len_sq, 0.0f, 1.0f);
+    V2 closest = a + edge * t;
+    min_dist_sq = fmin_r(min_dist_sq, (p - closest).len2());
+    float cross = edge.x * to_p.y - edge.y * to_p.x;
+    if (cross < 0.0f) inside = false;
+  }
+  float dist = sqrtf(min_dist_sq);
+  return inside ? dist : -dist;
+}
+
+// geometry.rs:37-72 Drum::sdf (local frame)
+__device__ __forceinline__ float drum_sdf(const StepUniform& U, V2 p) {
+  float d = U.drum_radius - p.len();
+  if (U.lifter_count == 0) return d;
+  float r = U.drum_radius;
+  float r_top = r - U.lifter_height;
+  V2 verts[4] = {V2(r, -U.lifter_base_half), V2(r, U.lifter_base_half), V2(r_top, U.lifter_top_half),
+                 V2(r_top, -U.lifter_top_half)};
+  float max_inside = -INFINITY;
+  for (uint32_t k = 0; k < U.lifter_count; ++k) {
+    float s = U.lifter_sin[k], c = U.lifter_cos[k];
+    float pr = p.x * c + p.y * s;
+    float pt = -p.x * s + p.y * c;
+    max_inside = fmax_r(max_inside, convex_quad_sdf(V2(pr, pt), verts));
+  }
+  return fmin_r(d, -max_inside);
+}
+
+// geometry.rs:87-109 Drum::sdf_world with the rotations from_angle(-angle) / from_angle(angle).
+__device__ __forceinline__ void drum_sdf_world(const StepUniform& U, V2 pw, V2 to_local, V2 to_world, float& d,
+                                               V2& normal) {
+  if (!pw.finite()) { d = 0.0f; normal = V2(); return; }
+  V2 pl = rotate(pw, to_local);
+  const float EPS = 1e-4f;
+  float dd = drum_sdf(U, pl);
+  float gx = drum_sdf(U, pl + V2(EPS, 0.0f)) - drum_sdf(U, pl - V2(EPS, 0.0f));
+  float gy = drum_sdf(U, pl + V2(0.0f, EPS)) - drum_sdf(U, pl - V2(0.0f, EPS));
+  V2 grad = V2(gx, gy) / (2.0f * EPS);
+  V2 nl = grad.len2() > 1e-12f ? grad.normalize() : -pl.normalize_or_zero();
+  d = dd;
+  normal = rotate(nl, to_world);
+}
+
+__device__ __forceinline__ V2 wall_velocity(float omega, V2 p) { return omega * V2(-p.y, p.x); }
+
+// geometry.rs:146-194 Drum::toi_swept; returns false for None.
+__device__ bool drum_toi_swept(const StepUniform& U, V2 x0, V2 x1, float a0, float a1, float radius, float& t_out) {
+  V2 local0 = rotate(x0, U.to_local0);
+  if (drum_sdf(U, local0) - radius <= 0.0f) return false;
+  V2 path = x1 - x0;
+  float path_len = path.len();
+  float dangle = a1 - a0;
+  float pos_bound = x0.len() + path_len;
+  float bound = path_len + fabsf(dangle) * pos_bound;
+  if (bound < 1e-9f) return false;
+  float t = 0.0f;
+  for (int it = 0; it < 32; ++it) {
+    float angle_t = a0 + dangle * t;
+    V2 x_t = x0 + path * t;
+    float na = -angle_t;
+    V2 local = rotate(x_t, V2(cosf_r(na), sinf_r(na)));
+    float d = drum_sdf(U, local) - radius;
+    if (d <= 0.0f) { t_out = t; return true; }
+    float step_t = fmax_r(d / bound, 1e-6f);
+    t += step_t;
+    if (t >= 1.0f) return false;
+  }
+  t_out = fmin_r(t, 1.0f);
+  return true;
+}
+
+}  // namespace mg

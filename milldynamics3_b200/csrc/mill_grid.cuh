@@ -1,0 +1,286 @@
+// Device uniform grid (grid.rs:101-399 semantics): floor(p / cell) keys, a dense counting-sort CSR
+// (cell-key histogram, block prefix scan, scatter, per-cell index sort) when the bounding box
+// holds at most 2n + 512 cells, otherwise a sparse layout of sorted occupied keys. Both give the
+// reference's iteration order: cells ascending by (cx, cy), points ascending by index in a cell.
+#pragma once
+
+#include "mill_block.cuh"
+
+namespace mg {
+
+__device__ __forceinline__ int2 cell_key(V2 p, float cell) {
+  return make_int2(f2i_sat(floorf(p.x / cell)), f2i_sat(floorf(p.y / cell)));
+}
+__device__ __forceinline__ bool key_lt(int2 a, int2 b) { return a.x < b.x || (a.x == b.x && a.y < b.y); }
+__device__ __forceinline__ bool key_eq(int2 a, int2 b) { return a.x == b.x && a.y == b.y; }
+
+// Builds the grid of points[0..n) into gb; hdr (shared memory) receives the layout.
+// Sets ERR_CELLS in *err if a key saturates the i32 range (coordinates beyond 2^31 cells).
+__device__ void grid_build(const float2* pts, uint32_t n, float cell, const GridBuf& gb, GridHdr& hdr, uint32_t* err) {
+  int32_t mnx = INT32_MAX, mxx = INT32_MIN, mny = INT32_MAX, mxy = INT32_MIN;
+  uint32_t cnt = 0;
+  bool sat = false;
+  for (uint32_t i = tid(); i < n; i += nthr()) {
+    V2 p(pts[i]);
+    if (!p.finite()) continue;
+    int2 k = cell_key(p, cell);
+    gb.pkey[i] = k;
+    mnx = min(mnx, k.x); mxx = max(mxx, k.x); mny = min(mny, k.y); mxy = max(mxy, k.y);
+    cnt += 1;
+    sat = sat || k.x <= INT32_MIN + 1 || k.x >= INT32_MAX - 1 || k.y <= INT32_MIN + 1 || k.y >= INT32_MAX - 1;
+  }
+  if (sat) atomicOr(err, ERR_CELLS);
+  block_minmax_i(mnx, mxx, mny, mxy);
+  uint32_t nvalid = block_sum_u(cnt);
+  if (tid() == 0) {
+    hdr.cell = cell;
+    hdr.npoints = nvalid;
+    hdr.min_cx = mnx;
+    hdr.min_cy = mny;
+    hdr.dense = 0;
+    hdr.width = hdr.height = 0;
+    hdr.ncells = 0;
+    if (nvalid > 0) {
+      int64_t w = (int64_t)mxx - (int64_t)mnx + 1, h = (int64_t)mxy - (int64_t)mny + 1;
+      uint64_t total = (uint64_t)w * (uint64_t)h;
+      uint64_t budget = 2ull * nvalid + 512ull;
+      if (total <= budget) {
+        hdr.dense = 1;
+        hdr.width = (int32_t)w;
+        hdr.height = (int32_t)h;
+        hdr.ncells = (uint32_t)total;
+      }
+    }
+    if (hdr.ncells > gb.cap_cells) { atomicOr(err, ERR_CELLS); hdr.ncells = 0; hdr.dense = 1; hdr.npoints = 0; }
+  }
+  __syncthreads();
+  if (hdr.npoints == 0) {
+    if (tid() == 0) { gb.cell_start[0] = 0; hdr.ncells = 0; hdr.dense = 0; }
+    __syncthreads();
+    return;
+  }
+  if (hdr.dense) {
+    uint32_t total = hdr.ncells;
+    for (uint32_t k = tid(); k <= total; k += nthr()) gb.cell_start[k] = 0;
+    __syncthreads();
+    for (uint32_t i = tid(); i < n; i += nthr()) {
+      if (!V2(pts[i]).finite()) continue;
+      int2 k = gb.pkey[i];
+      uint32_t c = (uint32_t)((k.x - hdr.min_cx) * hdr.height + (k.y - hdr.min_cy));
+      atomicAdd(&gb.cell_start[c], 1u);
+    }
+    __syncthreads();
+    block_exclusive_scan(gb.cell_start, total + 1);
+    for (uint32_t k = tid(); k < total; k += nthr()) gb.cursor[k] = gb.cell_start[k];
+    __syncthreads();
+    for (uint32_t i = tid(); i < n; i += nthr()) {
+      if (!V2(pts[i]).finite()) continue;
+      int2 k = gb.pkey[i];
+      uint32_t c = (uint32_t)((k.x - hdr.min_cx) * hdr.height + (k.y - hdr.min_cy));
+      uint32_t slot = atomicAdd(&gb.cursor[c], 1u);
+      gb.indices[slot] = i;
+    }
+    __syncthreads();
+    for (uint32_t k = tid(); k < total; k += nthr())
+      small_sort_u32(gb.indices + gb.cell_start[k], gb.cell_start[k + 1] - gb.cell_start[k]);
+    __syncthreads();
+  } else {
+    // Sparse: rank every valid point by (key, index); O(n^2 / threads), used only for a
+    // pathologically large bounding box (a diverged point far from the rest).
+    for (uint32_t i = tid(); i < n; i += nthr()) {
+      if (!V2(pts[i]).finite()) continue;
+      int2 ki = gb.pkey[i];
+      uint32_t rank = 0;
+      for (uint32_t j = 0; j < n; ++j) {
+        if (j == i || !V2(pts[j]).finite()) continue;
+        int2 kj = gb.pkey[j];
+        if (key_lt(kj, ki) || (key_eq(kj, ki) && j < i)) rank += 1;
+      }
+      gb.indices[rank] = i;
+    }
+    __syncthreads();
+    uint32_t nv = hdr.npoints;
+    for (uint32_t q = tid(); q < nv; q += nthr()) {
+      bool start = q == 0 || !key_eq(gb.pkey[gb.indices[q]], gb.pkey[gb.indices[q - 1]]);
+      gb.cursor[q] = start ? 1u : 0u;
+    }
+    __syncthreads();
+    uint32_t ncell = block_exclusive_scan(gb.cursor, nv);
+    for (uint32_t q = tid(); q < nv; q += nthr()) {
+      bool start = q == 0 || !key_eq(gb.pkey[gb.indices[q]], gb.pkey[gb.indices[q - 1]]);
+      if (start) {
+        uint32_t c = gb.cursor[q];
+        gb.keys[c] = gb.pkey[gb.indices[q]];
+        gb.cell_start[c] = q;
+      }
+    }
+    if (tid() == 0) { gb.cell_start[ncell] = nv; hdr.ncells = ncell; }
+    __syncthreads();
+  }
+}
+
+// grid.rs:242-270 cell_range
+__device__ __forceinline__ bool cell_range(const GridHdr& hdr, const GridBuf& gb, int2 key, uint32_t& s, uint32_t& e) {
+  if (hdr.npoints == 0) return false;
+  if (hdr.dense) {
+    int64_t dcx = (int64_t)key.x - hdr.min_cx, dcy = (int64_t)key.y - hdr.min_cy;
+    if (dcx < 0 || dcy < 0 || dcx >= hdr.width || dcy >= hdr.height) return false;
+    uint32_t k = (uint32_t)(dcx * hdr.height + dcy);
+    s = gb.cell_start[k];
+    e = gb.cell_start[k + 1];
+    return s != e;
+  }
+  uint32_t lo = 0, hi = hdr.ncells;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (key_lt(gb.keys[mid], key)) lo = mid + 1;
+    else hi = mid;
+  }
+  if (lo >= hdr.ncells || !key_eq(gb.keys[lo], key)) return false;
+  s = gb.cell_start[lo];
+  e = gb.cell_start[lo + 1];
+  return true;
+}
+
+// grid.rs:371-399 for_each_near: up to 9 distinct cells, dy outer (-1..1), dx inner (-1..1).
+template <class F>
+__device__ __forceinline__ void for_each_near(const GridHdr& hdr, const GridBuf& gb, V2 p, F f) {
+  if (!p.finite() || hdr.npoints == 0) return;
+  int2 c = cell_key(p, hdr.cell);
+  int2 ks[9];
+  int nk = 0;
+  for (int dy = -1; dy <= 1; ++dy)
+    for (int dx = -1; dx <= 1; ++dx) {
+      int2 k = make_int2(sat_add(c.x, dx), sat_add(c.y, dy));
+      bool seen = false;
+      for (int q = 0; q < nk; ++q) seen = seen || key_eq(ks[q], k);
+      if (!seen) ks[nk++] = k;
+    }
+  for (int q = 0; q < nk; ++q) {
+    uint32_t s, e;
+    if (!cell_range(hdr, gb, ks[q], s, e)) continue;
+    for (uint32_t a = s; a < e; ++a) f(gb.indices[a]);
+  }
+}
+
+// The cells a point's neighbour list visits, in the order build_neighbor_lists (pbf.rs:262-288)
+// produces: the forward-offset sweep of for_each_candidate_pair (grid.rs:291-362) reaches a point
+// in cell C from (-1,-1), (-1,0), (0,-1) before C's own pairs, then C's targets (+1,0), (+1,+1),
+// (0,+1), (-1,+1), and finally from (+1,-1). Keys never saturate here (grid_build flags that).
+__constant__ int STENCIL_DX[9] = {-1, -1, 0, 0, 1, 1, 0, -1, 1};
+__constant__ int STENCIL_DY[9] = {-1, 0, -1, 0, 0, 1, 1, 1, -1};
+
+template <class F>
+__device__ __forceinline__ void for_each_stencil_neighbor(const GridHdr& hdr, const GridBuf& gb, uint32_t self,
+                                                          int2 c, F f) {
+  for (int q = 0; q < 9; ++q) {
+    uint32_t s, e;
+    if (!cell_range(hdr, gb, make_int2(c.x + STENCIL_DX[q], c.y + STENCIL_DY[q]), s, e)) continue;
+    for (uint32_t a = s; a < e; ++a) {
+      uint32_t j = gb.indices[a];
+      if (j != self) f(j);
+    }
+  }
+}
+
+// Neighbour CSR in the reference's per-particle order (r^2 <= h^2). Two passes: count, scan, fill.
+__device__ void build_neighbor_lists(const float2* x, uint32_t n, float h, const GridHdr& hdr, const GridBuf& gb,
+                                     uint32_t* off, uint32_t* nbrs, uint32_t cap, uint32_t* err, uint32_t* n_edges) {
+  float h2 = h * h;
+  for (uint32_t i = tid(); i < n; i += nthr()) {
+    V2 xi(x[i]);
+    uint32_t c = 0;
+    if (xi.finite()) {
+      int2 k = cell_key(xi, hdr.cell);
+      for_each_stencil_neighbor(hdr, gb, i, k, [&](uint32_t j) {
+        if ((xi - V2(x[j])).len2() <= h2) c += 1;
+      });
+    }
+    off[i] = c;
+  }
+  if (tid() == 0) off[n] = 0;
+  __syncthreads();
+  uint32_t total = block_exclusive_scan(off, n + 1);
+  if (total > cap) {
+    if (tid() == 0) atomicOr(err, ERR_EDGES);
+    __syncthreads();
+    *n_edges = 0;
+    return;
+  }
+  for (uint32_t i = tid(); i < n; i += nthr()) {
+    V2 xi(x[i]);
+    if (!xi.finite()) continue;
+    uint32_t o = off[i];
+    int2 k = cell_key(xi, hdr.cell);
+    for_each_stencil_neighbor(hdr, gb, i, k, [&](uint32_t j) {
+      if ((xi - V2(x[j])).len2() <= h2) nbrs[o++] = j;
+    });
+  }
+  __syncthreads();
+  *n_edges = total;
+}
+
+// for_each_candidate_pair (grid.rs:291-362) materialised in its visiting order: per occupied cell,
+// the in-cell pairs (a < b) then the forward targets (1,0), (1,1), (0,1), (-1,1); each as (min, max).
+__constant__ int FWD_DX[4] = {1, 1, 0, -1};
+__constant__ int FWD_DY[4] = {0, 1, 1, 1};
+
+__device__ __forceinline__ int2 cell_of(const GridHdr& hdr, const GridBuf& gb, uint32_t k) {
+  if (hdr.dense) return make_int2(hdr.min_cx + (int32_t)(k / (uint32_t)hdr.height),
+                                  hdr.min_cy + (int32_t)(k % (uint32_t)hdr.height));
+  return gb.keys[k];
+}
+
+__device__ uint32_t build_candidate_pairs(const GridHdr& hdr, const GridBuf& gb, uint32_t* cnt, uint32_t* pi,
+                                          uint32_t* pj, uint32_t cap, uint32_t* err) {
+  uint32_t nc = hdr.ncells;
+  for (uint32_t k = tid(); k < nc; k += nthr()) {
+    uint32_t s = gb.cell_start[k], e = gb.cell_start[k + 1];
+    uint32_t m = e - s, c = 0;
+    if (m > 0) {
+      c = m * (m - 1) / 2;
+      int2 key = cell_of(hdr, gb, k);
+      for (int q = 0; q < 4; ++q) {
+        int2 t = make_int2(sat_add(key.x, FWD_DX[q]), sat_add(key.y, FWD_DY[q]));
+        if (key_eq(t, key)) continue;
+        uint32_t os, oe;
+        if (cell_range(hdr, gb, t, os, oe)) c += m * (oe - os);
+      }
+    }
+    cnt[k] = c;
+  }
+  if (tid() == 0) cnt[nc] = 0;
+  __syncthreads();
+  uint32_t total = block_exclusive_scan(cnt, nc + 1);
+  if (total > cap) {
+    if (tid() == 0) atomicOr(err, ERR_PAIRS);
+    __syncthreads();
+    return 0;
+  }
+  for (uint32_t k = tid(); k < nc; k += nthr()) {
+    uint32_t s = gb.cell_start[k], e = gb.cell_start[k + 1];
+    if (s == e) continue;
+    uint32_t o = cnt[k];
+    for (uint32_t a = s; a < e; ++a)
+      for (uint32_t b = a + 1; b < e; ++b) {
+        uint32_t i = gb.indices[a], j = gb.indices[b];
+        pi[o] = min(i, j); pj[o] = max(i, j); ++o;
+      }
+    int2 key = cell_of(hdr, gb, k);
+    for (int q = 0; q < 4; ++q) {
+      int2 t = make_int2(sat_add(key.x, FWD_DX[q]), sat_add(key.y, FWD_DY[q]));
+      if (key_eq(t, key)) continue;
+      uint32_t os, oe;
+      if (!cell_range(hdr, gb, t, os, oe)) continue;
+      for (uint32_t a = s; a < e; ++a)
+        for (uint32_t b = os; b < oe; ++b) {
+          uint32_t i = gb.indices[a], j = gb.indices[b];
+          pi[o] = min(i, j); pj[o] = max(i, j); ++o;
+        }
+    }
+  }
+  __syncthreads();
+  return total;
+}
+
+}  // namespace mg

@@ -1,0 +1,1081 @@
+// C ABI of the library (include/millgpu.h): simulation handles over device-resident mill state.
+// The host prepares the mill-uniform inputs (drum rotations, lifter frames, boundary offsets,
+// squeeze-film constants) and folds the per-sub-step outputs the device writes into the
+// Simulation bookkeeping of lib.rs:470-565 (EMA power and torque, f64 energy budget, the stress
+// accumulator of stress.rs with its debounce table), exactly in sub-step order.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "mill_kernels.h"
+#include "mill_params.h"
+
+using namespace mg;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail_global(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+// ------------------------------------------------------------------ stress.rs:28-171 on the host
+struct Stress {
+  double count_rate[4] = {}, se_hat_rate[4] = {}, hist_rate[MG_SE_BINS] = {}, above_rate_j[6] = {};
+  double cum_wall_j = 0.0, cum_above_j[6] = {};
+  std::map<std::pair<uint32_t, uint32_t>, double> last_counted;
+  bool has_factor = false;
+  double factor = 0.25;
+  uint64_t updates = 0;
+
+  static int se_bin(double e_hat) {
+    if (std::isnan(e_hat) || e_hat <= 0.0) return 0;
+    double t = (std::log10(e_hat) + 3.0) * 4.0;
+    if (!(t > 0.0)) t = 0.0;
+    if (t >= 27.0) return 27;
+    return (int)t;
+  }
+  void update(const MgImpactRecord* recs, uint32_t n, double m3, double scale_j, double d, double now_s,
+              double sub_dt, double alpha, double wall_work_j) {
+    static const double THR[6] = {0.03, 0.1, 0.3, 1.0, 3.0, 10.0};
+    double window = (has_factor ? factor : 0.25) * std::sqrt(d / 9.81);
+    updates += 1;
+    if (updates % 4096 == 0) {
+      for (auto it = last_counted.begin(); it != last_counted.end();) {
+        if (!(now_s - it->second < 4.0 * window)) it = last_counted.erase(it);
+        else ++it;
+      }
+    }
+    double count[4] = {}, se_hat[4] = {}, hist[MG_SE_BINS] = {}, above[6] = {};
+    for (uint32_t k = 0; k < n; ++k) {
+      const MgImpactRecord& r = recs[k];
+      if (window > 0.0) {
+        std::pair<uint32_t, uint32_t> key = {std::min(r.ball, r.partner), std::max(r.ball, r.partner)};
+        if (r.partner == MG_WALL_PARTNER) key = {r.ball, MG_WALL_PARTNER};
+        auto it = last_counted.find(key);
+        if (it != last_counted.end() && now_s - it->second < window) continue;
+        last_counted[key] = now_s;
+      }
+      bool bb = r.kind == MG_IMPACT_BALL_BALL;
+      double vn = r.normal_speed, vs = r.slip_speed;
+      int cls = bb ? (vs > vn ? 1 : 0) : (vs > vn ? 3 : 2);
+      double m_red = bb ? 0.5 * m3 : m3;
+      double se = 0.5 * m_red * (vn * vn + vs * vs);
+      double e_hat = se / scale_j;
+      count[cls] += 1.0;
+      se_hat[cls] += e_hat;
+      hist[se_bin(e_hat)] += 1.0;
+      for (int q = 0; q < 6; ++q)
+        if (e_hat >= THR[q]) above[q] += se;
+    }
+    cum_wall_j += wall_work_j;
+    for (int q = 0; q < 6; ++q) cum_above_j[q] += above[q];
+    auto ema = [&](double* s, double inst) { *s += alpha * (inst / sub_dt - *s); };
+    for (int c = 0; c < 4; ++c) { ema(&count_rate[c], count[c]); ema(&se_hat_rate[c], se_hat[c]); }
+    for (int b = 0; b < MG_SE_BINS; ++b) ema(&hist_rate[b], hist[b]);
+    for (int q = 0; q < 6; ++q) ema(&above_rate_j[q], above[q]);
+  }
+  double total_rate() const { return count_rate[0] + count_rate[1] + count_rate[2] + count_rate[3]; }
+};
+
+// ------------------------------------------------------------------ device arena
+struct Arena {
+  size_t off = 0;
+  char* base = nullptr;
+  template <class T>
+  T* take(size_t n) {
+    off = (off + 255) & ~size_t(255);
+    T* p = reinterpret_cast<T*>(base + off);
+    off += std::max<size_t>(n, 1) * sizeof(T);
+    return p;
+  }
+};
+
+constexpr uint32_t MAX_SUB = 64;
+
+}  // namespace
+
+struct MgSim {
+  MgParams params;
+  MgOptions opt{};
+  std::string err;
+  // Simulation scalars (lib.rs:82-119)
+  float drum_angle = 0.0f;
+  double sim_time = 0.0;
+  float power = 0.0f, torque = 0.0f, collision_rate = 0.0f, dissipated_power = 0.0f, max_disp = 0.0f;
+  uint32_t clamp_hits_frame = 0;
+  MgFluidStepStats last_fluid{};
+  MgDemStepStats last_dem{};
+  MgStepCounters last_ctr{};
+  MgEnergyBudget budget{};
+  double e0 = 0.0;
+  Stress stress;
+  // device state
+  cudaStream_t stream = nullptr;
+  uint32_t nf = 0, nb = 0, cap_nf = 0, cap_nb = 0;
+  MgBallMaterial bmat{};
+  MgFluidMaterial fmat{};
+  void* dmem = nullptr;
+  size_t dbytes = 0;
+  MillDev md{};
+  MillDev* d_md = nullptr;
+  StepUniform* h_uni = nullptr;
+  StepUniform* d_uni = nullptr;
+  SubAngles* h_ang = nullptr;
+  SubAngles* d_ang = nullptr;
+  StepOut* h_out = nullptr;
+  MgImpactRecord* h_imp = nullptr;
+  uint32_t guess_valid_host = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_kernel_ms = 0.0f;
+  uint64_t launches = 0;
+  uint64_t ctr_tot[10] = {};
+  uint64_t ctr_n = 0;
+};
+
+namespace {
+
+int fail(MgSim* s, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (s) s->err = buf;
+  g_err = buf;
+  return code;
+}
+
+#define CK(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) return fail(s, MG_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+uint32_t cap_items_for() { return 256; }
+
+// Sizes the device arena for nf fluid particles and nb balls (capacities documented in DESIGN.md).
+int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
+  if (s->dmem && nf <= s->cap_nf && nb <= s->cap_nb) {
+    s->nf = nf;
+    s->nb = nb;
+    s->md.nf = nf;
+    s->md.nb = nb;
+    return MG_OK;
+  }
+  if (s->dmem) { cudaFree(s->dmem); s->dmem = nullptr; }
+  uint32_t cf = std::max(nf, 1u), cb = std::max(nb, 1u);
+  MillDev m{};
+  m.cap_nf = cf;
+  m.cap_nb = cb;
+  m.cap_edges = 64u * cf + 1024u;
+  m.cap_pairs = 64u * cb + 1024u;
+  m.cap_items = cap_items_for();
+  m.cap_groups = cb * m.cap_items;
+  // squeeze links: every pair of balls within 2r + 8 dx plus the wall, bounded by nb per ball
+  m.cap_links = cb * std::min<uint32_t>(cb + 1u, 512u) + 1024u;
+  m.cap_recs = std::max({8u * cf + 1024u, m.cap_groups, m.cap_links});
+  m.cap_impacts = 4u * cb + 256u;
+  const uint32_t fcells = 2u * cf + 513u, bcells = 2u * cb + 513u;
+  const uint32_t nbig = std::max(cf, cb) + 2u;
+  // pass 1: measure, pass 2: carve
+  for (int pass = 0; pass < 2; ++pass) {
+    Arena a;
+    a.base = pass ? (char*)s->dmem : nullptr;
+    m.guess_valid_dev = a.take<uint32_t>(1);
+    m.err = a.take<uint32_t>(1);
+    m.fx = a.take<float2>(cf); m.fv = a.take<float2>(cf); m.fguess = a.take<float2>(cf); m.fdye = a.take<float>(cf);
+    m.bx = a.take<float2>(cb); m.bv = a.take<float2>(cb); m.bth = a.take<float>(cb); m.bom = a.take<float>(cb);
+    m.imp = a.take<float2>(cb); m.ang = a.take<float>(cb);
+    m.x0 = a.take<float2>(cf); m.dp = a.take<float2>(cf); m.push_ex = a.take<float2>(cf);
+    m.coh_dv = a.take<float2>(cf); m.adh_dv = a.take<float2>(cf); m.dv_tmp = a.take<float2>(cf);
+    m.density = a.take<float>(cf); m.lambda = a.take<float>(cf); m.wall_val = a.take<float>(cf);
+    m.f_tmp = a.take<float>(cf); m.mu_eff = a.take<float>(cf); m.wall_bin = a.take<int32_t>(cf);
+    m.nbr_off = a.take<uint32_t>(cf + 1); m.nbrs = a.take<uint32_t>(m.cap_edges);
+    m.visc_w = a.take<float>(m.cap_edges); m.visc_dir = a.take<float2>(m.cap_edges);
+    GridBuf* gs[3] = {&m.gA, &m.gB, &m.gBall};
+    for (int g = 0; g < 3; ++g) {
+      uint32_t pts = g < 2 ? cf : cb, cells = g < 2 ? fcells : bcells;
+      gs[g]->cap_points = pts;
+      gs[g]->cap_cells = cells;
+      gs[g]->pkey = a.take<int2>(pts);
+      gs[g]->cell_start = a.take<uint32_t>(cells + 1);
+      gs[g]->cursor = a.take<uint32_t>(cells + 1);
+      gs[g]->indices = a.take<uint32_t>(pts);
+      gs[g]->keys = a.take<int2>(pts);
+    }
+    m.rec_i = a.take<uint32_t>(m.cap_recs); m.rec_b = a.take<uint32_t>(m.cap_recs);
+    m.rec_J = a.take<float2>(m.cap_recs); m.rec_M = a.take<float2>(m.cap_recs);
+    m.rec_L = a.take<float>(m.cap_recs);
+    m.rec_cnt = a.take<uint32_t>(cf + 1);
+    size_t items = (size_t)cb * m.cap_items;
+    m.item_j = a.take<uint32_t>(items); m.item_v = a.take<float2>(items);
+    m.item_w = a.take<float>(items); m.item_w2 = a.take<float>(items);
+    m.item_n = a.take<uint32_t>(cb + 1);
+    m.bk_start = a.take<uint32_t>(nbig); m.bk_cur = a.take<uint32_t>(nbig);
+    m.bk_order = a.take<uint32_t>(m.cap_pairs);
+    m.g_fluid = a.take<uint32_t>(m.cap_groups); m.g_ball = a.take<uint32_t>(m.cap_groups);
+    m.g_c = a.take<float>(m.cap_groups); m.g_l2 = a.take<float>(m.cap_groups); m.g_lc = a.take<float2>(m.cap_groups);
+    m.g_off = a.take<uint32_t>(cb + 1);
+    m.fg_start = a.take<uint32_t>(cf + 1); m.fg_list = a.take<uint32_t>(m.cap_groups);
+    m.l_ball = a.take<uint32_t>(m.cap_links); m.l_other = a.take<uint32_t>(m.cap_links);
+    m.l_n = a.take<float2>(m.cap_links); m.l_c = a.take<float>(m.cap_links);
+    m.l_off = a.take<uint32_t>(cb + 1);
+    m.lo_start = a.take<uint32_t>(cb + 2); m.lo_list = a.take<uint32_t>(m.cap_links);
+    size_t len = (size_t)cf + 2u * cb;
+    m.cg_x = a.take<float2>(len); m.cg_b = a.take<float2>(len); m.cg_r = a.take<float2>(len);
+    m.cg_z = a.take<float2>(len); m.cg_p = a.take<float2>(len); m.cg_ap = a.take<float2>(len);
+    m.cg_lv = a.take<float2>(cf); m.cg_diag = a.take<float>(len); m.cg_inv = a.take<float>(len);
+    m.ball_v0 = a.take<float2>(cb); m.ball_w0 = a.take<float>(cb);
+    m.bx0 = a.take<float2>(cb); m.bvpre = a.take<float2>(cb);
+    m.bth0 = a.take<float>(cb); m.bompre = a.take<float>(cb); m.lam_bw = a.take<float>(cb);
+    m.lam_tot = a.take<float>(cb); m.f_cw = a.take<double>(cb);
+    m.pair_i = a.take<uint32_t>(m.cap_pairs); m.pair_j = a.take<uint32_t>(m.cap_pairs);
+    m.lam_bb = a.take<float>(m.cap_pairs);
+    m.cs_i = a.take<uint32_t>(m.cap_pairs); m.cs_j = a.take<uint32_t>(m.cap_pairs); m.cs_l = a.take<float>(m.cap_pairs);
+    m.pair_cnt = a.take<uint32_t>(bcells + 1);
+    m.out = a.take<StepOut>(MAX_SUB);
+    m.impacts = a.take<MgImpactRecord>((size_t)MAX_SUB * m.cap_impacts);
+    if (!pass) {
+      s->dbytes = a.off + 256;
+      cudaError_t e = cudaMalloc(&s->dmem, s->dbytes);
+      if (e != cudaSuccess) return fail(s, MG_ERR_CUDA, "cudaMalloc(%zu): %s", s->dbytes, cudaGetErrorString(e));
+      cudaMemsetAsync(s->dmem, 0, s->dbytes, s->stream);
+    }
+  }
+  m.nf = nf;
+  m.nb = nb;
+  s->md = m;
+  s->cap_nf = cf;
+  s->cap_nb = cb;
+  s->nf = nf;
+  s->nb = nb;
+  delete[] s->h_imp;
+  s->h_imp = new MgImpactRecord[(size_t)MAX_SUB * m.cap_impacts];
+  return MG_OK;
+}
+
+int push_desc(MgSim* s) {
+  s->md.nf = s->nf;
+  s->md.nb = s->nb;
+  s->md.f_mass = s->fmat.particle_mass;
+  s->md.f_h = s->fmat.h;
+  s->md.f_rho0 = s->fmat.rest_density;
+  s->md.b_r = s->bmat.radius;
+  s->md.b_m = s->bmat.mass;
+  s->md.b_I = s->bmat.inertia;
+  s->md.b_rtrue = s->bmat.true_radius;
+  CK(cudaMemcpyAsync(s->d_md, &s->md, sizeof(MillDev), cudaMemcpyHostToDevice, s->stream));
+  return MG_OK;
+}
+
+// Fills the mill-uniform block for one call (geometry trig, boundary offsets, films).
+int fill_uniform(MgSim* s, const MgDrum& drum, const MgMediaParams& media, const MgSlurryParams& slurry,
+                 uint32_t pbf_it, uint32_t dem_it, int run_fluid, int run_dem, int ext) {
+  StepUniform& U = *s->h_uni;
+  std::memset(&U, 0, sizeof(U));
+  U.drum_radius = drum.radius_m;
+  U.drum_omega = drum.omega;
+  if (drum.lifters.count > (uint32_t)MAX_LIFTERS) return fail(s, MG_ERR_ARG, "lifters.count above %d", MAX_LIFTERS);
+  U.lifter_count = drum.lifters.count;
+  U.lifter_height = drum.lifters.height_m;
+  U.lifter_base_half = drum.lifters.base_width_m * 0.5f;
+  U.lifter_top_half = drum.lifters.top_width_m * 0.5f;
+  const float rads_per_deg = mgh::PI_F / 180.0f;
+  float phase = drum.lifters.phase_deg * rads_per_deg;
+  for (uint32_t k = 0; k < U.lifter_count; ++k) {
+    float th = phase + (float)k * mgh::TAU_F / (float)U.lifter_count;  // geometry.rs:55
+    U.lifter_sin[k] = mgh::sinf_r(th);
+    U.lifter_cos[k] = mgh::cosf_r(th);
+  }
+  U.pbf_iterations = pbf_it;
+  U.dem_iterations = dem_it;
+  U.run_fluid = run_fluid;
+  U.run_dem = run_dem;
+  U.dem_external = ext;
+  U.media = media;
+  U.slurry = slurry;
+  U.cg_fp64 = s->opt.cg_fp64;
+  // pbf.rs:190-219: boundary points at dx = h / 2 (adhesion and viscosity groups)
+  U.boundary_count = 0;
+  float br = s->bmat.radius, dx = 0.5f * s->fmat.h;
+  if (s->nb > 0 && br > 0.0f && dx > 0.0f) {
+    float circumference = mgh::TAU_F * br;
+    uint32_t count = std::max(mgh::f2u_sat(std::round(circumference / dx)), 6u);
+    if (count > (uint32_t)MAX_BOUNDARY_POINTS)
+      return fail(s, MG_ERR_CAPACITY, "%u boundary points per ball exceed %d", count, MAX_BOUNDARY_POINTS);
+    U.boundary_count = count;
+    for (uint32_t k = 0; k < count; ++k) {
+      float angle = mgh::TAU_F * (float)k / (float)count;
+      U.boundary_offset[k] = V2(mgh::cosf_r(angle) * br, mgh::sinf_r(angle) * br);
+    }
+  }
+  // mac/lubrication.rs:49-73 SqueezeFilm::new for the pair (1/a, 1/a) and wall (1/a, -1/b) films
+  auto film = [](double k1, double k2, double nu) {
+    FilmConsts f;
+    f.r = 1.0 / (k1 + k2);
+    double q = (f.r * (f.r * f.r)) * (k1 * (k1 * k1) + k2 * (k2 * k2));
+    f.c1 = 0.788 + 0.265 * q;
+    double c2 = 0.006 + 0.057 * (q - 0.25);
+    f.c2 = c2 > 0.0 ? c2 : 0.0;
+    f.prefactor = 3.0 * std::sqrt(2.0) * M_PI * nu * std::pow(f.r, 1.5);
+    return f;
+  };
+  double a = (double)br, bd = (double)drum.radius_m, mud = (double)mgh::fmax_r(slurry.viscosity_pa_s, 0.0f);
+  if (a > 0.0) {
+    U.pair_film = film(1.0 / a, 1.0 / a, mud);
+    U.wall_film = film(1.0 / a, -1.0 / bd, mud);
+  }
+  return MG_OK;
+}
+
+void fill_angle(SubAngles& A, float angle, float omega, float dt) {
+  A.drum_angle = angle;
+  A.drum_angle_next = angle + omega * dt;
+  A.dt = dt;
+  A.pad = 0.0f;
+  float an = A.drum_angle_next;
+  A.to_local_next = V2(mgh::cosf_r(-an), mgh::sinf_r(-an));
+  A.to_world_next = V2(mgh::cosf_r(an), mgh::sinf_r(an));
+  A.to_local0 = V2(mgh::cosf_r(-angle), mgh::sinf_r(-angle));
+}
+
+// Launches n_sub sub-steps (angles already in h_ang) and waits; outputs land in h_out / h_imp.
+int run(MgSim* s, uint32_t n_sub) {
+  if (n_sub > MAX_SUB) return fail(s, MG_ERR_ARG, "at most %u sub-steps per launch", MAX_SUB);
+  int rc = push_desc(s);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(s->d_uni, s->h_uni, sizeof(StepUniform), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->d_ang, s->h_ang, sizeof(SubAngles) * n_sub, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemsetAsync(s->md.err, 0, sizeof(uint32_t), s->stream));
+  CK(cudaEventRecord(s->ev0, s->stream));
+  CK(launch_substeps(s->d_md, 1, s->d_uni, s->d_ang, n_sub, s->opt.block_threads, s->stream));
+  CK(cudaEventRecord(s->ev1, s->stream));
+  CK(cudaMemcpyAsync(s->h_out, s->md.out, sizeof(StepOut) * n_sub, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaEventElapsedTime(&s->last_kernel_ms, s->ev0, s->ev1));
+  s->launches += 1;
+  for (uint32_t k = 0; k < n_sub; ++k) {
+    const uint32_t* c = reinterpret_cast<const uint32_t*>(&s->h_out[k].ctr);
+    for (int q = 0; q < 10; ++q) s->ctr_tot[q] += c[q];
+    s->ctr_n += 1;
+  }
+  uint32_t e = 0;
+  for (uint32_t k = 0; k < n_sub; ++k) e |= s->h_out[k].err;
+  if (e) return fail(s, MG_ERR_CAPACITY, "device capacity exceeded (error bits 0x%x)", e);
+  size_t total_imp = 0;
+  for (uint32_t k = 0; k < n_sub; ++k) total_imp += s->h_out[k].n_impacts;
+  if (total_imp) {
+    for (uint32_t k = 0; k < n_sub; ++k) {
+      uint32_t ni = std::min(s->h_out[k].n_impacts, s->md.cap_impacts);
+      if (ni)
+        CK(cudaMemcpyAsync(s->h_imp + (size_t)k * s->md.cap_impacts, s->md.impacts + (size_t)k * s->md.cap_impacts,
+                           sizeof(MgImpactRecord) * ni, cudaMemcpyDeviceToHost, s->stream));
+    }
+    CK(cudaStreamSynchronize(s->stream));
+  }
+  s->last_fluid = s->h_out[n_sub - 1].fs;
+  s->last_dem = s->h_out[n_sub - 1].ds;
+  s->last_ctr = s->h_out[n_sub - 1].ctr;
+  return MG_OK;
+}
+
+MgDrum sim_drum(const MgSim* s) {
+  MgDrum d;
+  d.radius_m = mgh::mill_radius(s->params.mill);
+  d.omega = mgh::mill_omega(s->params.mill);
+  d.lifters = s->params.lifters;
+  return d;
+}
+
+// lib.rs:491-565 for sub-step k of the last launch
+void fold_substep(MgSim* s, uint32_t k, float sub_dt, float omega) {
+  const MgFluidStepStats& fs = s->h_out[k].fs;
+  const MgDemStepStats& ds = s->h_out[k].ds;
+  s->clamp_hits_frame += fs.coupling_clamp_hits;
+  MgEnergyBudget& b = s->budget;
+  b.elapsed_s += (double)sub_dt;
+  b.dem_wall_work_j += (double)ds.wall_work_j;
+  b.fluid_wall_work_j += (double)fs.wall_work_j;
+  b.shaft_work_j += (double)(ds.wall_work_j + fs.wall_work_j);
+  b.ball_contact_dissipation_j += (double)ds.dissipated_energy_j;
+  b.fluid_wall_slip_j += (double)(fs.wall_work_j - fs.ke_delta_noslip_j);
+  b.fluid_viscous_j -= (double)fs.ke_delta_viscosity_j;
+  b.fluid_clamp_removed_j -= (double)fs.ke_delta_clamp_j;
+  b.interface_created_j += (double)(ds.coupling_work_j + fs.ke_delta_drag_j + fs.ke_delta_buoyancy_j);
+  b.fluid_wall_angular_impulse += (double)fs.wall_angular_impulse;
+  // update_grinding_stats
+  float alpha = 1.0f - mgh::expf_r(-sub_dt / 1.0f);
+  float p_inst = (ds.wall_work_j + fs.wall_work_j) / sub_dt;
+  s->power += alpha * (p_inst - s->power);
+  float t_inst = std::fabs(omega) > 1e-6f ? p_inst / omega : 0.0f;
+  s->torque += alpha * (t_inst - s->torque);
+  double r = (double)s->bmat.radius;
+  double m3 = (double)s->bmat.mass * 4.0 / 3.0 * r;
+  double d = 2.0 * r;
+  double scale_j = m3 * 9.81 * d;
+  uint32_t ni = std::min(s->h_out[k].n_impacts, s->md.cap_impacts);
+  s->stress.update(s->h_imp + (size_t)k * s->md.cap_impacts, ni, m3, scale_j, d, s->sim_time, (double)sub_dt,
+                   (double)alpha, (double)(ds.wall_work_j + fs.wall_work_j));
+  s->collision_rate = (float)s->stress.total_rate();
+  float diss = mgh::fmax_r(ds.dissipated_energy_j, 0.0f) / sub_dt;
+  s->dissipated_power += alpha * (diss - s->dissipated_power);
+  s->max_disp = mgh::fmax_r(s->max_disp, ds.max_substep_displacement_over_diameter);
+  s->drum_angle = mgh::rem_euclid_r(s->drum_angle + omega * sub_dt, mgh::TAU_F);
+  s->sim_time += (double)sub_dt;
+}
+
+// Simulation::step / step_fixed: n sub-steps of sub_dt in one launch, then the bookkeeping.
+int advance(MgSim* s, uint32_t n, float sub_dt) {
+  MgDrum drum = sim_drum(s);
+  float omega = drum.omega;
+  const MgSimulationParams& q = s->params.simulation;
+  int rc = fill_uniform(s, drum, s->params.media, s->params.slurry, q.pbf_iterations, q.dem_iterations, 1, 1, 1);
+  if (rc) return rc;
+  uint32_t done = 0;
+  while (done < n) {
+    uint32_t chunk = std::min(n - done, MAX_SUB);
+    float angle = s->drum_angle;
+    for (uint32_t k = 0; k < chunk; ++k) {
+      fill_angle(s->h_ang[k], angle, omega, sub_dt);
+      angle = mgh::rem_euclid_r(angle + omega * sub_dt, mgh::TAU_F);
+    }
+    rc = run(s, chunk);
+    if (rc) return rc;
+    for (uint32_t k = 0; k < chunk; ++k) fold_substep(s, k, sub_dt, omega);
+    done += chunk;
+  }
+  return MG_OK;
+}
+
+int init_handle(MgSim* s) {
+  CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  CK(cudaMalloc(&s->d_md, sizeof(MillDev)));
+  CK(cudaMalloc(&s->d_uni, sizeof(StepUniform)));
+  CK(cudaMalloc(&s->d_ang, sizeof(SubAngles) * MAX_SUB));
+  CK(cudaMallocHost(&s->h_uni, sizeof(StepUniform)));
+  CK(cudaMallocHost(&s->h_ang, sizeof(SubAngles) * MAX_SUB));
+  CK(cudaMallocHost(&s->h_out, sizeof(StepOut) * MAX_SUB));
+  CK(cudaEventCreate(&s->ev0));
+  CK(cudaEventCreate(&s->ev1));
+  return MG_OK;
+}
+
+int upload_balls(MgSim* s, const float* x, const float* v, const float* th, const float* om) {
+  size_t n = s->nb;
+  if (!n) return MG_OK;
+  CK(cudaMemcpyAsync(s->md.bx, x, 8 * n, cudaMemcpyHostToDevice, s->stream));
+  if (v) CK(cudaMemcpyAsync(s->md.bv, v, 8 * n, cudaMemcpyHostToDevice, s->stream));
+  else CK(cudaMemsetAsync(s->md.bv, 0, 8 * n, s->stream));
+  if (th) CK(cudaMemcpyAsync(s->md.bth, th, 4 * n, cudaMemcpyHostToDevice, s->stream));
+  else CK(cudaMemsetAsync(s->md.bth, 0, 4 * n, s->stream));
+  if (om) CK(cudaMemcpyAsync(s->md.bom, om, 4 * n, cudaMemcpyHostToDevice, s->stream));
+  else CK(cudaMemsetAsync(s->md.bom, 0, 4 * n, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return MG_OK;
+}
+
+int upload_fluid(MgSim* s, const float* x, const float* v, const float* dye, const float* guess) {
+  size_t n = s->nf;
+  uint32_t gv = guess ? 1u : 0u;
+  if (n) {
+    CK(cudaMemcpyAsync(s->md.fx, x, 8 * n, cudaMemcpyHostToDevice, s->stream));
+    if (v) CK(cudaMemcpyAsync(s->md.fv, v, 8 * n, cudaMemcpyHostToDevice, s->stream));
+    else CK(cudaMemsetAsync(s->md.fv, 0, 8 * n, s->stream));
+    if (dye) CK(cudaMemcpyAsync(s->md.fdye, dye, 4 * n, cudaMemcpyHostToDevice, s->stream));
+    else CK(cudaMemsetAsync(s->md.fdye, 0, 4 * n, s->stream));
+    if (guess) CK(cudaMemcpyAsync(s->md.fguess, guess, 8 * n, cudaMemcpyHostToDevice, s->stream));
+  }
+  CK(cudaMemcpyAsync(s->md.guess_valid_dev, &gv, 4, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return MG_OK;
+}
+
+int create_sim(const MgParams* p, const float* xy, uint32_t n_init, MgSim** out) {
+  if (!p || !out) return fail_global(MG_ERR_ARG, "null argument");
+  std::string e;
+  if (!mgh::params_validate(*p, &e)) return fail_global(MG_ERR_INVALID_PARAMS, "%s", e.c_str());
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail_global(MG_ERR_NO_DEVICE, "no CUDA device visible");
+  MgSim* s = new MgSim();
+  s->params = *p;
+  int rc = init_handle(s);
+  if (rc) { g_err = s->err; mg_sim_destroy(s); return rc; }
+  float radius = mgh::mill_radius(p->mill);
+  mgh::Effective eff = mgh::effective_media(*p);
+  mgh::Balls balls;
+  mgh::seed_balls(&balls, eff, radius, p->simulation.seed);
+  if (xy) {
+    balls.x.assign(xy, xy + 2 * (size_t)n_init);
+    balls.v.assign(2 * (size_t)n_init, 0.0f);
+    balls.theta.assign(n_init, 0.0f);
+    balls.omega.assign(n_init, 0.0f);
+  }
+  uint32_t res = mgh::effective_fluid_resolution(*p);
+  mgh::Fluid fluid;
+  if (p->slurry.enabled) {
+    mgh::seed_fluid(&fluid, p->slurry, radius, res, balls.x, balls.radius);
+  } else {
+    MgSlurryParams sp = p->slurry;
+    sp.fill_fraction = 0.0f;
+    mgh::seed_fluid(&fluid, sp, radius, res, std::vector<float>(), 0.0f);
+  }
+  if (xy) {
+    float w = mgh::mill_omega(p->mill);
+    for (size_t i = 0; i < balls.len(); ++i) {
+      balls.v[2 * i] = w * -balls.x[2 * i + 1];
+      balls.v[2 * i + 1] = w * balls.x[2 * i];
+      balls.omega[i] = w;
+    }
+    for (size_t i = 0; i < fluid.len(); ++i) {
+      fluid.v[2 * i] = w * -fluid.x[2 * i + 1];
+      fluid.v[2 * i + 1] = w * fluid.x[2 * i];
+    }
+  }
+  s->bmat = {balls.radius, balls.mass, balls.inertia, balls.true_radius};
+  s->fmat = {fluid.particle_mass, fluid.h, fluid.rest_density};
+  s->e0 = mgh::balls_energy_f64(balls) + mgh::fluid_energy_f64(fluid);
+  rc = alloc_state(s, (uint32_t)fluid.len(), (uint32_t)balls.len());
+  if (!rc) rc = upload_balls(s, balls.x.data(), balls.v.data(), balls.theta.data(), balls.omega.data());
+  if (!rc) rc = upload_fluid(s, fluid.x.data(), fluid.v.data(), fluid.dye.data(), nullptr);
+  if (rc) { g_err = s->err; mg_sim_destroy(s); return rc; }
+  *out = s;
+  return MG_OK;
+}
+
+int download(MgSim* s, mgh::Balls* b, mgh::Fluid* f) {
+  if (b) {
+    b->x.resize(2 * s->nb); b->v.resize(2 * s->nb); b->theta.resize(s->nb); b->omega.resize(s->nb);
+    if (s->nb) {
+      CK(cudaMemcpyAsync(b->x.data(), s->md.bx, 8 * s->nb, cudaMemcpyDeviceToHost, s->stream));
+      CK(cudaMemcpyAsync(b->v.data(), s->md.bv, 8 * s->nb, cudaMemcpyDeviceToHost, s->stream));
+      CK(cudaMemcpyAsync(b->theta.data(), s->md.bth, 4 * s->nb, cudaMemcpyDeviceToHost, s->stream));
+      CK(cudaMemcpyAsync(b->omega.data(), s->md.bom, 4 * s->nb, cudaMemcpyDeviceToHost, s->stream));
+    }
+    b->radius = s->bmat.radius; b->mass = s->bmat.mass; b->inertia = s->bmat.inertia; b->true_radius = s->bmat.true_radius;
+  }
+  if (f) {
+    f->x.resize(2 * s->nf); f->v.resize(2 * s->nf); f->dye.resize(s->nf);
+    if (s->nf) {
+      CK(cudaMemcpyAsync(f->x.data(), s->md.fx, 8 * s->nf, cudaMemcpyDeviceToHost, s->stream));
+      CK(cudaMemcpyAsync(f->v.data(), s->md.fv, 8 * s->nf, cudaMemcpyDeviceToHost, s->stream));
+      CK(cudaMemcpyAsync(f->dye.data(), s->md.fdye, 4 * s->nf, cudaMemcpyDeviceToHost, s->stream));
+    }
+    f->particle_mass = s->fmat.particle_mass; f->h = s->fmat.h; f->rest_density = s->fmat.rest_density;
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  return MG_OK;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+size_t mg_sizeof_params(void) { return sizeof(MgParams); }
+size_t mg_sizeof_fluid_stats(void) { return sizeof(MgFluidStepStats); }
+size_t mg_sizeof_dem_stats(void) { return sizeof(MgDemStepStats); }
+
+int mg_params_default(MgParams* out) {
+  if (!out) return fail_global(MG_ERR_ARG, "null argument");
+  *out = mgh::params_default();
+  return MG_OK;
+}
+int mg_params_validate(const MgParams* p, char* err, size_t n) {
+  if (!p) return fail_global(MG_ERR_ARG, "null argument");
+  std::string e;
+  if (mgh::params_validate(*p, &e)) return MG_OK;
+  if (err && n) { std::strncpy(err, e.c_str(), n - 1); err[n - 1] = 0; }
+  return fail_global(MG_ERR_INVALID_PARAMS, "%s", e.c_str());
+}
+int mg_preset_apply(MgParams* p, const char* id) {
+  if (!p) return fail_global(MG_ERR_ARG, "null argument");
+  return mgh::preset_apply(p, id) ? MG_OK : fail_global(MG_ERR_ARG, "unknown preset '%s'", id ? id : "");
+}
+int mg_params_derived(const MgParams* pp, MgDerived* o) {
+  if (!pp || !o) return fail_global(MG_ERR_ARG, "null argument");
+  const MgParams& p = *pp;
+  mgh::Effective e = mgh::effective_media(p);
+  o->critical_speed_rpm = mgh::critical_speed_rpm(p.mill);
+  o->rpm = mgh::mill_rpm(p.mill);
+  o->percent_critical = mgh::mill_percent_critical(p.mill);
+  o->omega = mgh::mill_omega(p.mill);
+  o->radius_m = mgh::mill_radius(p.mill);
+  o->true_ball_count = mgh::true_ball_count(p);
+  o->eff_true_diameter_m = e.true_diameter_m;
+  o->eff_diameter_m = e.diameter_m;
+  o->eff_density_kg_m3 = e.density_kg_m3;
+  o->eff_ball_count = e.ball_count;
+  o->eff_scale_factor = e.scale_factor;
+  o->effective_fluid_resolution = mgh::effective_fluid_resolution(p);
+  o->effective_substeps = mgh::effective_substeps(p);
+  o->fixed_sub_dt = 1.0f / (60.0f * (float)std::max(o->effective_substeps, 1u));
+  return MG_OK;
+}
+
+int mg_sim_create(const MgParams* p, MgSim** out) { return create_sim(p, nullptr, 0, out); }
+int mg_sim_create_with_balls(const MgParams* p, const float* xy, uint32_t n, MgSim** out) {
+  if (!xy && n) return fail_global(MG_ERR_ARG, "null positions");
+  static const float dummy[2] = {0.0f, 0.0f};
+  return create_sim(p, xy ? xy : dummy, n, out);
+}
+void mg_sim_destroy(MgSim* s) {
+  if (!s) return;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->dmem) cudaFree(s->dmem);
+  if (s->d_md) cudaFree(s->d_md);
+  if (s->d_uni) cudaFree(s->d_uni);
+  if (s->d_ang) cudaFree(s->d_ang);
+  if (s->h_uni) cudaFreeHost(s->h_uni);
+  if (s->h_ang) cudaFreeHost(s->h_ang);
+  if (s->h_out) cudaFreeHost(s->h_out);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete[] s->h_imp;
+  delete s;
+}
+const char* mg_last_error(const MgSim* s) { return s ? s->err.c_str() : g_err.c_str(); }
+const char* mg_global_last_error(void) { return g_err.c_str(); }
+int mg_sim_set_options(MgSim* s, const MgOptions* o) {
+  if (!s || !o) return fail(s, MG_ERR_ARG, "null argument");
+  if (o->block_threads != 0 && (o->block_threads % 32 != 0 || o->block_threads > 512))
+    return fail(s, MG_ERR_ARG, "block_threads must be a multiple of 32 in [32, 512]");
+  s->opt = *o;
+  return MG_OK;
+}
+int mg_sim_step(MgSim* s, float dt) {
+  if (!s) return fail_global(MG_ERR_ARG, "null handle");
+  uint32_t n = std::max(mgh::effective_substeps(s->params), 1u);
+  float sub_dt = dt / (float)n;
+  s->max_disp = 0.0f;
+  s->clamp_hits_frame = 0;
+  return advance(s, n, sub_dt);
+}
+int mg_sim_step_fixed(MgSim* s) {
+  if (!s) return fail_global(MG_ERR_ARG, "null handle");
+  return advance(s, 1, mg_sim_fixed_sub_dt(s));
+}
+int mg_sim_reset_frame_stats(MgSim* s) {
+  if (!s) return fail_global(MG_ERR_ARG, "null handle");
+  s->max_disp = 0.0f;
+  s->clamp_hits_frame = 0;
+  return MG_OK;
+}
+int mg_sim_set_params(MgSim* s, const MgParams* p) {
+  if (!s || !p) return fail(s, MG_ERR_ARG, "null argument");
+  std::string e;
+  if (!mgh::params_validate(*p, &e)) return fail(s, MG_ERR_INVALID_PARAMS, "%s", e.c_str());
+  s->params = *p;
+  return MG_OK;
+}
+float mg_sim_fixed_sub_dt(const MgSim* s) {
+  return 1.0f / (60.0f * (float)std::max(mgh::effective_substeps(s->params), 1u));
+}
+int mg_sim_reset_energy_budget(MgSim* s) {
+  if (!s) return fail_global(MG_ERR_ARG, "null handle");
+  mgh::Balls b;
+  mgh::Fluid f;
+  int rc = download(s, &b, &f);
+  if (rc) return rc;
+  std::memset(&s->budget, 0, sizeof(s->budget));
+  s->e0 = mgh::balls_energy_f64(b) + mgh::fluid_energy_f64(f);
+  return MG_OK;
+}
+
+int mg_coupling_step_recorded(MgSim* s, const MgDrum* drum, float drum_angle, const MgMediaParams* media,
+                              const MgSlurryParams* slurry, uint32_t dem_it, uint32_t pbf_it, float dt,
+                              MgFluidStepStats* fstats, MgDemStepStats* dstats, MgImpactRecord* out, uint32_t cap,
+                              uint32_t* n_out) {
+  if (!s || !drum || !media || !slurry) return fail(s, MG_ERR_ARG, "null argument");
+  int rc = fill_uniform(s, *drum, *media, *slurry, pbf_it, dem_it, 1, 1, 1);
+  if (rc) return rc;
+  fill_angle(s->h_ang[0], drum_angle, drum->omega, dt);
+  rc = run(s, 1);
+  if (rc) return rc;
+  if (fstats) *fstats = s->h_out[0].fs;
+  if (dstats) *dstats = s->h_out[0].ds;
+  uint32_t ni = std::min(s->h_out[0].n_impacts, s->md.cap_impacts);
+  if (n_out) *n_out = s->h_out[0].n_impacts;
+  if (out) std::memcpy(out, s->h_imp, sizeof(MgImpactRecord) * std::min(ni, cap));
+  return MG_OK;
+}
+
+int mg_fluid_step_coupled(MgSim* s, const MgDrum* drum, float drum_angle, const MgSlurryParams* slurry,
+                          uint32_t it, float dt, MgFluidStepStats* fstats, float* impulses, float* angular,
+                          uint32_t* clamp_hits, float* fluid_momentum) {
+  if (!s || !drum || !slurry) return fail(s, MG_ERR_ARG, "null argument");
+  int rc = fill_uniform(s, *drum, s->params.media, *slurry, it, 1, 1, 0, 1);
+  if (rc) return rc;
+  fill_angle(s->h_ang[0], drum_angle, drum->omega, dt);
+  rc = run(s, 1);
+  if (rc) return rc;
+  if (fstats) *fstats = s->h_out[0].fs;
+  if (clamp_hits) *clamp_hits = s->h_out[0].clamp_hits;
+  if (fluid_momentum) { fluid_momentum[0] = s->h_out[0].fluid_momentum[0]; fluid_momentum[1] = s->h_out[0].fluid_momentum[1]; }
+  if (s->nb) {
+    if (impulses) CK(cudaMemcpyAsync(impulses, s->md.imp, 8 * s->nb, cudaMemcpyDeviceToHost, s->stream));
+    if (angular) CK(cudaMemcpyAsync(angular, s->md.ang, 4 * s->nb, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+  }
+  return MG_OK;
+}
+
+int mg_dem_step_recorded(MgSim* s, const MgDrum* drum, float drum_angle, const MgMediaParams* media, uint32_t it,
+                         float dt, const float* impulses, const float* angular, MgDemStepStats* dstats,
+                         MgImpactRecord* out, uint32_t cap, uint32_t* n_out) {
+  if (!s || !drum || !media) return fail(s, MG_ERR_ARG, "null argument");
+  int ext = (impulses || angular) ? 1 : 0;
+  int rc = fill_uniform(s, *drum, *media, s->params.slurry, 1, it, 0, 1, ext);
+  if (rc) return rc;
+  if (s->nb) {
+    if (impulses) CK(cudaMemcpyAsync(s->md.imp, impulses, 8 * s->nb, cudaMemcpyHostToDevice, s->stream));
+    else CK(cudaMemsetAsync(s->md.imp, 0, 8 * s->nb, s->stream));
+    if (angular) CK(cudaMemcpyAsync(s->md.ang, angular, 4 * s->nb, cudaMemcpyHostToDevice, s->stream));
+    else CK(cudaMemsetAsync(s->md.ang, 0, 4 * s->nb, s->stream));
+  }
+  fill_angle(s->h_ang[0], drum_angle, drum->omega, dt);
+  rc = run(s, 1);
+  if (rc) return rc;
+  if (dstats) *dstats = s->h_out[0].ds;
+  uint32_t ni = std::min(s->h_out[0].n_impacts, s->md.cap_impacts);
+  if (n_out) *n_out = s->h_out[0].n_impacts;
+  if (out) std::memcpy(out, s->h_imp, sizeof(MgImpactRecord) * std::min(ni, cap));
+  return MG_OK;
+}
+
+int mg_get_counts(const MgSim* s, uint32_t* nb, uint32_t* nf) {
+  if (!s) return fail_global(MG_ERR_ARG, "null handle");
+  if (nb) *nb = s->nb;
+  if (nf) *nf = s->nf;
+  return MG_OK;
+}
+int mg_get_balls(MgSim* s, float* x, float* v, float* theta, float* omega) {
+  if (!s) return fail_global(MG_ERR_ARG, "null handle");
+  size_t n = s->nb;
+  if (!n) return MG_OK;
+  if (x) CK(cudaMemcpyAsync(x, s->md.bx, 8 * n, cudaMemcpyDeviceToHost, s->stream));
+  if (v) CK(cudaMemcpyAsync(v, s->md.bv, 8 * n, cudaMemcpyDeviceToHost, s->stream));
+  if (theta) CK(cudaMemcpyAsync(theta, s->md.bth, 4 * n, cudaMemcpyDeviceToHost, s->stream));
+  if (omega) CK(cudaMemcpyAsync(omega, s->md.bom, 4 * n, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return MG_OK;
+}
+int mg_set_balls(MgSim* s, uint32_t n, const float* x, const float* v, const float* theta, const float* omega) {
+  if (!s || (!x && n)) return fail(s, MG_ERR_ARG, "null argument");
+  if (n > s->cap_nb) {
+    // grow: keep the fluid state across the reallocation
+    mgh::Fluid f;
+    int rc = download(s, nullptr, &f);
+    std::vector<float> guess(2 * (size_t)s->nf);
+    uint32_t gv = 0;
+    if (!rc && s->nf) {
+      CK(cudaMemcpy(guess.data(), s->md.fguess, 8 * (size_t)s->nf, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(&gv, s->md.guess_valid_dev, 4, cudaMemcpyDeviceToHost));
+    }
+    uint32_t nf = s->nf;
+    if (!rc) rc = alloc_state(s, nf, n);
+    if (!rc) rc = upload_fluid(s, f.x.data(), f.v.data(), f.dye.data(), gv ? guess.data() : nullptr);
+    if (rc) return rc;
+  }
+  s->nb = n;
+  s->md.nb = n;
+  return upload_balls(s, x, v, theta, omega);
+}
+int mg_get_ball_material(const MgSim* s, MgBallMaterial* o) {
+  if (!s || !o) return fail_global(MG_ERR_ARG, "null argument");
+  *o = s->bmat;
+  return MG_OK;
+}
+int mg_set_ball_material(MgSim* s, const MgBallMaterial* m) {
+  if (!s || !m) return fail(s, MG_ERR_ARG, "null argument");
+  s->bmat = *m;
+  return MG_OK;
+}
+int mg_get_fluid(MgSim* s, float* x, float* v, float* dye, float* guess, uint32_t* guess_len) {
+  if (!s) return fail_global(MG_ERR_ARG, "null handle");
+  size_t n = s->nf;
+  uint32_t gv = 0;
+  CK(cudaMemcpy(&gv, s->md.guess_valid_dev, 4, cudaMemcpyDeviceToHost));
+  if (guess_len) *guess_len = gv ? (uint32_t)n : 0u;
+  if (!n) return MG_OK;
+  if (x) CK(cudaMemcpyAsync(x, s->md.fx, 8 * n, cudaMemcpyDeviceToHost, s->stream));
+  if (v) CK(cudaMemcpyAsync(v, s->md.fv, 8 * n, cudaMemcpyDeviceToHost, s->stream));
+  if (dye) CK(cudaMemcpyAsync(dye, s->md.fdye, 4 * n, cudaMemcpyDeviceToHost, s->stream));
+  if (guess && gv) CK(cudaMemcpyAsync(guess, s->md.fguess, 8 * n, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return MG_OK;
+}
+int mg_set_fluid(MgSim* s, uint32_t n, const float* x, const float* v, const float* dye, const float* guess) {
+  if (!s || (!x && n)) return fail(s, MG_ERR_ARG, "null argument");
+  if (n > s->cap_nf) {
+    mgh::Balls b;
+    int rc = download(s, &b, nullptr);
+    uint32_t nb = s->nb;
+    if (!rc) rc = alloc_state(s, n, nb);
+    if (!rc) rc = upload_balls(s, b.x.data(), b.v.data(), b.theta.data(), b.omega.data());
+    if (rc) return rc;
+  }
+  s->nf = n;
+  s->md.nf = n;
+  return upload_fluid(s, x, v, dye, guess);
+}
+int mg_get_fluid_material(const MgSim* s, MgFluidMaterial* o) {
+  if (!s || !o) return fail_global(MG_ERR_ARG, "null argument");
+  *o = s->fmat;
+  return MG_OK;
+}
+int mg_set_fluid_material(MgSim* s, const MgFluidMaterial* m) {
+  if (!s || !m) return fail(s, MG_ERR_ARG, "null argument");
+  s->fmat = *m;
+  return MG_OK;
+}
+
+int mg_get_scalars(MgSim* s, MgScalars* o) {
+  if (!s || !o) return fail_global(MG_ERR_ARG, "null argument");
+  std::memset(o, 0, sizeof(*o));
+  o->drum_angle = s->drum_angle;
+  o->power_draw_w = s->power;
+  o->torque_nm = s->torque;
+  o->collision_rate_per_s = s->collision_rate;
+  o->dissipated_power_w = s->dissipated_power;
+  o->max_substep_displacement_over_diameter = s->max_disp;
+  o->coupling_clamp_hits = s->clamp_hits_frame;
+  o->viscosity_iterations = s->last_fluid.viscosity_iterations;
+  o->mean_shear_rate_per_s = s->last_fluid.mean_shear_rate_per_s;
+  o->sim_time = s->sim_time;
+  return MG_OK;
+}
+int mg_energy_budget(MgSim* s, MgEnergyBudget* o) {
+  if (!s || !o) return fail_global(MG_ERR_ARG, "null argument");
+  mgh::Balls b;
+  mgh::Fluid f;
+  int rc = download(s, &b, &f);
+  if (rc) return rc;
+  MgEnergyBudget e = s->budget;
+  e.delta_mechanical_j = mgh::balls_energy_f64(b) + mgh::fluid_energy_f64(f) - s->e0;
+  double explained = e.shaft_work_j - e.ball_contact_dissipation_j - e.fluid_wall_slip_j - e.fluid_viscous_j -
+                     e.fluid_clamp_removed_j + e.interface_created_j;
+  e.unattributed_j = e.delta_mechanical_j - explained;
+  *o = e;
+  return MG_OK;
+}
+int mg_state_hash(MgSim* s, int extended, uint64_t* out) {
+  if (!s || !out) return fail_global(MG_ERR_ARG, "null argument");
+  mgh::Balls b;
+  mgh::Fluid f;
+  int rc = download(s, &b, &f);
+  if (rc) return rc;
+  uint64_t h = 0xcbf29ce484222325ull;
+  auto mix = [&](float v) {
+    uint32_t bits;
+    std::memcpy(&bits, &v, 4);
+    for (int k = 0; k < 4; ++k) { h ^= (uint64_t)((bits >> (8 * k)) & 0xFFu); h *= 0x100000001b3ull; }
+  };
+  for (size_t i = 0; i < b.len(); ++i) {
+    mix(b.x[2 * i]); mix(b.x[2 * i + 1]); mix(b.v[2 * i]); mix(b.v[2 * i + 1]); mix(b.omega[i]);
+    if (extended) mix(b.theta[i]);
+  }
+  for (size_t i = 0; i < f.len(); ++i) {
+    mix(f.x[2 * i]); mix(f.x[2 * i + 1]); mix(f.v[2 * i]); mix(f.v[2 * i + 1]);
+    if (extended) mix(f.dye[i]);
+  }
+  *out = h;
+  return MG_OK;
+}
+int mg_mixing_index(MgSim* s, float* out, int* valid) {
+  if (!s || !out || !valid) return fail_global(MG_ERR_ARG, "null argument");
+  mgh::Fluid f;
+  int rc = download(s, nullptr, &f);
+  if (rc) return rc;
+  // metrics.rs:506-576 (16 x 16 dye grid, count-weighted Lacey index)
+  const int G = 16;
+  *valid = 0;
+  *out = 0.0f;
+  size_t n = f.len();
+  float r = mgh::mill_radius(s->params.mill);
+  if (n == 0 || r <= 0.0f) return MG_OK;
+  float cell = 2.0f * r / (float)G;
+  float dye_sum[G * G] = {};
+  uint32_t count[G * G] = {};
+  float total = 0.0f;
+  for (size_t i = 0; i < n; ++i) {
+    int32_t gi = std::min(std::max(mgh::f2i_sat(std::floor((f.x[2 * i] + r) / cell)), 0), G - 1);
+    int32_t gj = std::min(std::max(mgh::f2i_sat(std::floor((f.x[2 * i + 1] + r) / cell)), 0), G - 1);
+    dye_sum[gj * G + gi] += f.dye[i];
+    count[gj * G + gi] += 1;
+    total += f.dye[i];
+  }
+  float p_mean = total / (float)n;
+  std::vector<float> means;
+  std::vector<uint32_t> counts;
+  for (int k = 0; k < G * G; ++k)
+    if (count[k]) { means.push_back(dye_sum[k] / (float)count[k]); counts.push_back(count[k]); }
+  if (means.size() < 2) return MG_OK;
+  uint32_t ws = 0;
+  for (uint32_t c : counts) ws += c;
+  float wsum = (float)ws, ov = 0.0f, wa = 0.0f;
+  for (size_t q = 0; q < means.size(); ++q) { float dm = means[q] - p_mean; ov += (float)counts[q] * (dm * dm); }
+  float observed = ov / wsum;
+  float s0 = p_mean * (1.0f - p_mean);
+  for (uint32_t c : counts) wa += (float)c * (float)c;
+  float sr = s0 / mgh::fmax_r(wa / wsum, 1.0f);
+  if (s0 < 1e-9f) return MG_OK;
+  float denom = s0 - sr;
+  *valid = 1;
+  if (std::fabs(denom) < 1e-9f) { *out = 1.0f; return MG_OK; }
+  *out = mgh::clamp_r((s0 - observed) / denom, 0.0f, 1.0f);
+  return MG_OK;
+}
+int mg_stress_histogram_rate(MgSim* s, double* out28) {
+  if (!s || !out28) return fail_global(MG_ERR_ARG, "null argument");
+  std::memcpy(out28, s->stress.hist_rate, sizeof(double) * MG_SE_BINS);
+  return MG_OK;
+}
+int mg_last_step_stats(MgSim* s, MgFluidStepStats* f, MgDemStepStats* d, MgStepCounters* c) {
+  if (!s) return fail_global(MG_ERR_ARG, "null handle");
+  if (f) *f = s->last_fluid;
+  if (d) *d = s->last_dem;
+  if (c) *c = s->last_ctr;
+  return MG_OK;
+}
+
+int mg_sim_stream(MgSim* s, void** stream) {
+  if (!s || !stream) return fail_global(MG_ERR_ARG, "null argument");
+  *stream = (void*)s->stream;
+  return MG_OK;
+}
+int mg_sim_last_kernel_ms(MgSim* s, float* ms, uint64_t* launches) {
+  if (!s) return fail_global(MG_ERR_ARG, "null handle");
+  if (ms) *ms = s->last_kernel_ms;
+  if (launches) *launches = s->launches;
+  return MG_OK;
+}
+int mg_counter_totals(MgSim* s, uint64_t* totals10, uint64_t* n_substeps, int reset) {
+  if (!s) return fail_global(MG_ERR_ARG, "null handle");
+  if (totals10) std::memcpy(totals10, s->ctr_tot, sizeof(s->ctr_tot));
+  if (n_substeps) *n_substeps = s->ctr_n;
+  if (reset) { std::memset(s->ctr_tot, 0, sizeof(s->ctr_tot)); s->ctr_n = 0; }
+  return MG_OK;
+}
+
+int mg_last_neighbor_lists(MgSim* s, uint32_t* offsets, uint32_t* nbrs, uint32_t cap, uint32_t* n_edges) {
+  if (!s || !offsets || !n_edges) return fail_global(MG_ERR_ARG, "null argument");
+  CK(cudaMemcpy(offsets, s->md.nbr_off, 4 * ((size_t)s->nf + 1), cudaMemcpyDeviceToHost));
+  uint32_t ne = s->nf ? offsets[s->nf] : 0;
+  *n_edges = ne;
+  if (ne > cap) return fail(s, MG_ERR_CAPACITY, "neighbour buffer too small");
+  if (ne && nbrs) CK(cudaMemcpy(nbrs, s->md.nbrs, 4 * (size_t)ne, cudaMemcpyDeviceToHost));
+  return MG_OK;
+}
+int mg_last_ball_pairs(MgSim* s, uint32_t* pairs, uint32_t cap, uint32_t* n_out) {
+  if (!s || !n_out) return fail_global(MG_ERR_ARG, "null argument");
+  uint32_t np = s->last_ctr.n_ball_pairs;
+  *n_out = np;
+  if (np > cap) return fail(s, MG_ERR_CAPACITY, "pair buffer too small");
+  std::vector<uint32_t> pi(np), pj(np);
+  if (np) {
+    CK(cudaMemcpy(pi.data(), s->md.pair_i, 4 * (size_t)np, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(pj.data(), s->md.pair_j, 4 * (size_t)np, cudaMemcpyDeviceToHost));
+  }
+  for (uint32_t k = 0; k < np; ++k) { pairs[2 * k] = pi[k]; pairs[2 * k + 1] = pj[k]; }
+  return MG_OK;
+}
+
+// ---- grid-stage probes: a scratch mill holding only the caller's points
+static int probe(const float* xy, uint32_t n, float cell, int mode, MgSim** out_s, uint32_t res[9]) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail_global(MG_ERR_NO_DEVICE, "no CUDA device visible");
+  if (!(cell > 0.0f) || !std::isfinite(cell)) return fail_global(MG_ERR_ARG, "cell_size must be positive");
+  MgSim* s = new MgSim();
+  s->params = mgh::params_default();
+  int rc = init_handle(s);
+  // the probe grid lives in the fluid-side buffers; the pair buffers are sized by the ball count
+  if (!rc) rc = alloc_state(s, n, std::max(n, 1u));
+  if (!rc && n) {
+    cudaError_t e = cudaMemcpy(s->md.fx, xy, 8 * (size_t)n, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) rc = fail(s, MG_ERR_CUDA, "%s", cudaGetErrorString(e));
+  }
+  s->nb = 0;
+  if (!rc) rc = push_desc(s);
+  uint32_t* d_res = nullptr;
+  if (!rc && cudaMalloc(&d_res, 9 * sizeof(uint32_t)) != cudaSuccess) rc = fail(s, MG_ERR_CUDA, "cudaMalloc");
+  if (!rc) {
+    cudaMemsetAsync(s->md.err, 0, 4, s->stream);
+    cudaError_t e = launch_probe(s->d_md, cell, mode, d_res, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(res, d_res, 9 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) rc = fail(s, MG_ERR_CUDA, "%s", cudaGetErrorString(e));
+  }
+  if (d_res) cudaFree(d_res);
+  if (rc) { g_err = s->err; mg_sim_destroy(s); return rc; }
+  *out_s = s;
+  return MG_OK;
+}
+
+int mg_probe_grid(const float* xy, uint32_t n, float cell, int32_t* min_cxy, int64_t* wh, uint32_t* cell_start,
+                  uint32_t cell_cap, uint32_t* indices, uint32_t* n_cells_out, int* dense_out) {
+  MgSim* s = nullptr;
+  uint32_t res[9] = {};
+  int rc = probe(xy, n, cell, 0, &s, res);
+  if (rc) return rc;
+  *dense_out = (int)res[0];
+  min_cxy[0] = (int32_t)res[1];
+  min_cxy[1] = (int32_t)res[2];
+  wh[0] = res[0] ? (int64_t)(int32_t)res[3] : 0;
+  wh[1] = res[0] ? (int64_t)(int32_t)res[4] : 0;
+  uint32_t nc = res[6] ? res[5] : 0;
+  *n_cells_out = nc + 1;
+  if (nc + 1 > cell_cap) { mg_sim_destroy(s); return fail_global(MG_ERR_CAPACITY, "cell buffer too small"); }
+  cudaMemcpy(cell_start, s->md.gA.cell_start, 4 * ((size_t)nc + 1), cudaMemcpyDeviceToHost);
+  if (n) cudaMemcpy(indices, s->md.gA.indices, 4 * (size_t)res[6], cudaMemcpyDeviceToHost);
+  mg_sim_destroy(s);
+  return MG_OK;
+}
+int mg_probe_candidate_pairs(const float* xy, uint32_t n, float cell, uint32_t* pairs, uint32_t cap, uint32_t* n_out) {
+  MgSim* s = nullptr;
+  uint32_t res[9] = {};
+  int rc = probe(xy, n, cell, 1, &s, res);
+  if (rc) return rc;
+  uint32_t np = res[8];
+  *n_out = np;
+  if (res[7]) { mg_sim_destroy(s); return fail_global(MG_ERR_CAPACITY, "probe error bits 0x%x", res[7]); }
+  if (np > cap) { mg_sim_destroy(s); return fail_global(MG_ERR_CAPACITY, "pair buffer too small"); }
+  std::vector<uint32_t> pi(np), pj(np);
+  if (np) {
+    cudaMemcpy(pi.data(), s->md.pair_i, 4 * (size_t)np, cudaMemcpyDeviceToHost);
+    cudaMemcpy(pj.data(), s->md.pair_j, 4 * (size_t)np, cudaMemcpyDeviceToHost);
+  }
+  for (uint32_t k = 0; k < np; ++k) { pairs[2 * k] = pi[k]; pairs[2 * k + 1] = pj[k]; }
+  mg_sim_destroy(s);
+  return MG_OK;
+}
+int mg_probe_neighbor_lists(const float* xy, uint32_t n, float h, uint32_t* offsets, uint32_t* nbrs, uint32_t cap,
+                            uint32_t* n_edges) {
+  MgSim* s = nullptr;
+  uint32_t res[9] = {};
+  int rc = probe(xy, n, h, 2, &s, res);
+  if (rc) return rc;
+  uint32_t ne = res[8];
+  *n_edges = ne;
+  if (res[7]) { mg_sim_destroy(s); return fail_global(MG_ERR_CAPACITY, "probe error bits 0x%x", res[7]); }
+  cudaMemcpy(offsets, s->md.nbr_off, 4 * ((size_t)n + 1), cudaMemcpyDeviceToHost);
+  if (ne > cap) { mg_sim_destroy(s); return fail_global(MG_ERR_CAPACITY, "neighbour buffer too small"); }
+  if (ne) cudaMemcpy(nbrs, s->md.nbrs, 4 * (size_t)ne, cudaMemcpyDeviceToHost);
+  mg_sim_destroy(s);
+  return MG_OK;
+}
+
+}  // extern "C"

@@ -16,6 +16,7 @@ static_assert(sizeof(MgSlurryParams) == sizeof(SlurryParams), "slurry layout");
 static_assert(sizeof(MgFluidStepStats) == sizeof(FluidStepStats), "fluid stats layout");
 static_assert(sizeof(MgDemStepStats) == sizeof(DemStepStats), "dem stats layout");
 static_assert(sizeof(MgImpactRecord) == sizeof(ImpactRecord), "impact layout");
+static_assert(sizeof(MgStepCounters) == sizeof(StepCounters), "counter layout");
 
 struct OrSim {
   Simulation sim;

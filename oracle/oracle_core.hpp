@@ -29,6 +29,16 @@ namespace orc {
 constexpr float PI_F = 3.14159265358979323846f;
 constexpr float TAU_F = 6.28318530717958647692f;
 
+// Transcendentals. Every f32 exp/sin/cos/atan2/log10 of the reference is evaluated here as the
+// f32 rounding of the f64 function (error <= 0.5 ulp + 2^-29, against <= ~0.502 ulp for the
+// platform's f32 functions the Rust build calls), so that the device path, which evaluates them
+// the same way, can agree bit for bit.
+inline float expf_r(float x) { return (float)std::exp((double)x); }
+inline float sinf_r(float x) { return (float)std::sin((double)x); }
+inline float cosf_r(float x) { return (float)std::cos((double)x); }
+inline float atan2f_r(float y, float x) { return (float)std::atan2((double)y, (double)x); }
+inline float log10f_r(float x) { return (float)std::log10((double)x); }
+
 // f32::max / f32::min (IEEE maxNum/minNum: a NaN operand yields the other operand).
 inline float fmax_r(float a, float b) {
   if (std::isnan(a)) return b;
@@ -118,7 +128,7 @@ struct Vec2 {
     if (std::isfinite(rcp) && rcp > 0.0f) return *this * rcp;
     return Vec2();
   }
-  static Vec2 from_angle(float a) { return Vec2(std::cos(a), std::sin(a)); }
+  static Vec2 from_angle(float a) { return Vec2(cosf_r(a), sinf_r(a)); }
 };
 inline Vec2 operator*(float s, Vec2 v) { return Vec2(s * v.x, s * v.y); }
 inline float cross2(Vec2 a, Vec2 b) { return a.x * b.y - a.y * b.x; }
@@ -341,6 +351,7 @@ struct ImpactRecord {
 struct StepCounters {
   uint32_t density_iters = 0, cg_iters = 0, n_groups = 0, n_links = 0, links_in_range = 0;
   uint32_t n_ball_pairs = 0, n_fluid_edges = 0, n_active_contacts = 0;
+  uint32_t n_coupling_items = 0, reserved0 = 0;
 };
 
 // Last sub-step's internal structures, kept for parity checks of the device path.

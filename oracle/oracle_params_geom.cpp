@@ -378,7 +378,7 @@ float Drum::sdf_lifters(Vec2 p) const {
   float max_inside = -INFINITY;
   for (uint32_t k = 0; k < n; ++k) {
     float theta_i = phase + (float)k * TAU_F / (float)n;
-    float s = std::sin(theta_i), c = std::cos(theta_i);
+    float s = sinf_r(theta_i), c = cosf_r(theta_i);
     float pr = p.x * c + p.y * s;
     float pt = -p.x * s + p.y * c;
     float inside = lifter_cross_section_sdf(pr, pt, radius_m, lifters.height_m, lifters.base_width_m * 0.5f,

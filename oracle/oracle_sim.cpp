@@ -178,7 +178,7 @@ void Simulation::advance_one_sub_step(float sub_dt) {
 
 // lib.rs:516-565
 void Simulation::update_grinding_stats(const DemStepStats& s, float fluid_wall_work, float sub_dt, float omega) {
-  float alpha = 1.0f - std::exp(-sub_dt / 1.0f);
+  float alpha = 1.0f - expf_r(-sub_dt / 1.0f);
   float power_instant = (s.wall_work_j + fluid_wall_work) / sub_dt;
   power_draw_w += alpha * (power_instant - power_draw_w);
   float torque_instant = std::fabs(omega) > 1e-6f ? power_instant / omega : 0.0f;

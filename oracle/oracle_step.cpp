@@ -67,7 +67,7 @@ static std::vector<Vec2> ball_boundary_particles(const Balls& b, float dx) {
   std::vector<Vec2> offsets(count);
   for (uint32_t k = 0; k < count; ++k) {
     float angle = TAU_F * (float)k / (float)count;
-    offsets[k] = Vec2(std::cos(angle), std::sin(angle)) * b.radius;
+    offsets[k] = Vec2(cosf_r(angle), sinf_r(angle)) * b.radius;
   }
   out.reserve(b.len() * count);
   for (size_t i = 0; i < b.len(); ++i)
@@ -463,7 +463,7 @@ static std::vector<float> bingham_viscosity(const std::vector<float>& rates, flo
   std::vector<float> out(rates.size());
   for (size_t i = 0; i < rates.size(); ++i) {
     float g = std::isfinite(rates[i]) ? rates[i] : 0.0f;
-    float extra = g < 1e-4f * gamma0 ? tau_y / gamma0 : tau_y * (1.0f - std::exp(-g / gamma0)) / g;
+    float extra = g < 1e-4f * gamma0 ? tau_y / gamma0 : tau_y * (1.0f - expf_r(-g / gamma0)) / g;
     out[i] = mu + extra;
   }
   return out;
@@ -733,7 +733,7 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
       acct_wall_impulse[0] += (double)push.x;
       acct_wall_impulse[1] += (double)push.y;
       acct_wall_angular += (double)cross2(X[i], push);
-      float angle = std::atan2(X[i].y, X[i].x);
+      float angle = atan2f_r(X[i].y, X[i].x);
       size_t bin = f2u_sat(((angle + PI_F) / TAU_F) * (float)WALL_IMPULSE_BINS);
       acct_wall_bins[std::min(bin, (size_t)WALL_IMPULSE_BINS - 1)] += mass * -d / dt;
     }
@@ -801,6 +801,7 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
           l_sum += w * cross2(r_i, V[ju]);
           items.push_back({ju, r_i, phi});
         }
+        if (ctr) ctr->n_coupling_items += (uint32_t)items.size();
         if (m_ent <= 1e-12f || items.empty()) continue;
         Vec2 r_bar = r_sum / m_ent;
         Vec2 v_bar = v_sum / m_ent;
@@ -810,7 +811,7 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
                                  ? 0.5f * rest_density * BALL_FORM_DRAG_COEFFICIENT * (2.0f * balls.true_radius) *
                                        speed_rel / mass_true
                                  : 0.0f;
-        float bt = beta_b * (1.0f - std::exp(-dt * (inv_tau_stokes + inv_tau_form)));
+        float bt = beta_b * (1.0f - expf_r(-dt * (inv_tau_stokes + inv_tau_form)));
         float a_lin = bt * m_ent / (balls.mass + m_ent);
         Vec2 dv_b = a_lin * v_rel;
         float dw_b = 0.0f, c_rot = 0.0f;
@@ -870,6 +871,7 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
         float w = mass * poly6(r2, h);
         if (w > 0.0f) { rho_local += w; weights.push_back({ju, w}); }
       }
+      if (ctr && rho_local > 0.0f) ctr->n_coupling_items += (uint32_t)weights.size();
       if (rho_local <= 0.0f) continue;
       float rho_eff = fmin_r(rho_local, rest_density);
       float omega_num = 0.0f, omega_den = 0.0f;
@@ -1056,9 +1058,9 @@ float restitution_velocity_threshold(float r) {
 int impact_energy_bin(float e) {
   if (!std::isfinite(e) || e <= 0.0f) return -1;
   float ec = clamp_r(e, IMPACT_ENERGY_MIN_J, IMPACT_ENERGY_MAX_J);
-  float log_min = std::log10(IMPACT_ENERGY_MIN_J);
-  float log_max = std::log10(IMPACT_ENERGY_MAX_J);
-  float t = (std::log10(ec) - log_min) / (log_max - log_min);
+  float log_min = log10f_r(IMPACT_ENERGY_MIN_J);
+  float log_max = log10f_r(IMPACT_ENERGY_MAX_J);
+  float t = (log10f_r(ec) - log_min) / (log_max - log_min);
   uint32_t idx = f2u_sat(t * (float)IMPACT_BINS);
   return (int)std::min(idx, (uint32_t)IMPACT_BINS - 1);
 }
@@ -1066,7 +1068,7 @@ int impact_energy_bin(float e) {
 float effective_friction(float mu_k, float mu_s, float v_t, float vs) {
   if (mu_s <= mu_k) return mu_k;
   float ratio = v_t / vs;
-  float weight = std::exp(-(ratio * ratio));
+  float weight = expf_r(-(ratio * ratio));
   return mu_k + (mu_s - mu_k) * weight;
 }
 // dem.rs:253-273
