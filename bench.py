@@ -212,6 +212,10 @@ def run_device(args):
     nsum = C.c_uint64()
     lib.counter_totals(sim.h, tot, C.byref(nsum), 0)
     per_launch_bytes = bytes_model(list(tot), nsum.value, nf, nb, p.simulation.dem_iterations) / max(args.steps, 1)
+    cyc = (C.c_uint64 * 40)()
+    lib.stage_cycles(sim.h, cyc, 1)
+    mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    stages = {capi.STAGE_NAMES[q]: round(cyc[q] / max(nsum.value, 1) / mhz, 2) for q in range(40) if cyc[q]}
     k_ms = sum(kernel_ms) / len(kernel_ms)
     hbm, peak_kind = peaks()
     achieved = per_launch_bytes / (k_ms / 1e3) / 1e9
@@ -252,7 +256,7 @@ def run_device(args):
                              "kernel": "mill_substeps_kernel (one launch per frame)",
                              "kernel_ms_per_launch": k_ms, "algorithmic_bytes_per_launch": per_launch_bytes},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
-                "gpu_launches": args.steps, "clocks": clocks}
+                "gpu_launches": args.steps, "clocks": clocks, "stage_us_per_substep": stages}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
         print(json.dumps(line), flush=True)

@@ -176,11 +176,16 @@ typedef struct MgScalars {
 } MgScalars;
 
 /* Device-path options. cg_fp64: 0 = the reference's sequential f32 inner products in the
- * viscosity solve, 1 = f64 inner products and residual norms. block_threads: 0 = default. */
+ * viscosity solve, 1 = f64 inner products and residual norms. block_threads: 0 = default.
+ * sweep_warps: warps that take balls in the per-ball drag and buoyancy sweeps (0 = default).
+ * spin_ns: poll interval of a ball waiting for an earlier ball in those sweeps (0 = default).
+ * None of them changes results. */
 typedef struct MgOptions {
   uint32_t cg_fp64;
   uint32_t block_threads;
-  uint32_t reserved[6];
+  uint32_t sweep_warps;
+  uint32_t spin_ns;
+  uint32_t reserved[4];
 } MgOptions;
 
 typedef struct MgSim MgSim;
@@ -276,6 +281,16 @@ int mg_sim_last_kernel_ms(MgSim* sim, float* ms, uint64_t* launches);
 /* Sums of every MgStepCounters field over all sub-steps since creation (or the last reset),
  * in field order, and the number of sub-steps summed. */
 int mg_counter_totals(MgSim* sim, uint64_t* totals10, uint64_t* n_substeps, int reset);
+/* Device cycles per stage summed over all sub-steps since creation (or the last reset): slots
+ * 0-14 are the reference's stage_timing.rs stages (predict + grid, density, push, cohesion,
+ * adhesion, wall 4-6, drag + buoyancy, density recompute, Morris weights, ball boundary pairs,
+ * squeeze links, CG, mean shear rate, clamps, DEM), 15-18 split the DEM step (predict + broad
+ * phase, projection, friction, restitution + rolling), 19 is drag alone and 20-31 split the
+ * sweeps further (DEM predecessors, levels, level bucketing, contact ordering; drag and
+ * buoyancy item lists, predecessors and sweeps). 32-37 are not wall-clock slots: they sum over
+ * balls the cycles the drag (32-34) and buoyancy (35-37) sweeps spent prefetching each ball,
+ * waiting for earlier balls and running the ball's dependent part. 40 slots in all. */
+int mg_stage_cycles(MgSim* sim, uint64_t* cycles40, int reset);
 
 /* ---- parity probes of the grid stage (grid.rs, pbf.rs:262-288) ----
  * Run the device grid build / candidate-pair / neighbour-list code on caller points. */

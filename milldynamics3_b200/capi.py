@@ -146,7 +146,8 @@ class Scalars(_S):
 
 
 class Options(_S):
-    _fields_ = [("cg_fp64", C.c_uint32), ("block_threads", C.c_uint32), ("reserved", C.c_uint32 * 6)]
+    _fields_ = [("cg_fp64", C.c_uint32), ("block_threads", C.c_uint32), ("sweep_warps", C.c_uint32),
+                ("spin_ns", C.c_uint32), ("reserved", C.c_uint32 * 4)]
 
 
 P = C.POINTER
@@ -210,7 +211,22 @@ DEVICE_ONLY = [
     ("sim_stream", C.c_int, [vp, P(vp)]),
     ("sim_last_kernel_ms", C.c_int, [vp, P(C.c_float), P(C.c_uint64)]),
     ("counter_totals", C.c_int, [vp, P(C.c_uint64), P(C.c_uint64), C.c_int]),
+    ("stage_cycles", C.c_int, [vp, P(C.c_uint64), C.c_int]),
 ]
+
+STAGE_NAMES = [
+    "PBF predict + grid build", "density iterations", "ball overlap push (3.5)", "fluid cohesion (3.6a)",
+    "ball adhesion (3.6b)", "wall projection (4-6)", "ball drag + buoyancy (6.5-6.6)", "density recompute",
+    "viscosity: Morris weights (+ Bingham rates)", "viscosity: ball boundary pairs", "viscosity: squeeze links",
+    "viscosity: CG solve (+ ball bookkeeping)", "mean_shear_rate", "fluid clamps/other (7.5-8)", "DEM step",
+    "DEM: predict + broad phase + CCD", "DEM: projection sweeps", "DEM: friction", "DEM: restitution + rolling",
+    "drag alone (6.5)", "DEM: projection predecessors", "DEM: projection levels", "DEM: level bucketing",
+    "unused (23)", "drag: item lists", "drag: predecessors", "drag: sweep", "buoyancy: item lists",
+    "buoyancy: predecessors", "buoyancy: sweep", "DEM: contact ordering", "unused (31)",
+    "drag sweep: ball prefetch (sum)", "drag sweep: ball waits (sum)", "drag sweep: ball chain work (sum)",
+    "buoyancy sweep: ball prefetch (sum)", "buoyancy sweep: ball waits (sum)",
+    "buoyancy sweep: ball chain work (sum)", "unused (38)", "unused (39)"]
+assert len(STAGE_NAMES) == 40
 
 
 class Lib:

@@ -8,6 +8,17 @@
 namespace mg {
 
 __device__ __forceinline__ uint32_t tid() { return threadIdx.x; }
+
+// Stage timing: thread 0 adds the cycles since the previous mark to out_stage[slot]. Called right
+// after a block barrier, so the interval covers the whole block's work on the stage.
+__shared__ long long g_stage_last;
+__device__ __forceinline__ void stage_mark(unsigned long long* out_stage, int slot) {
+  if (threadIdx.x == 0) {
+    long long t = clock64();
+    out_stage[slot] += (unsigned long long)(t - g_stage_last);
+    g_stage_last = t;
+  }
+}
 __device__ __forceinline__ uint32_t nthr() { return blockDim.x; }
 
 template <class T>

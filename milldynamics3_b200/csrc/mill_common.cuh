@@ -18,7 +18,10 @@ constexpr float TAU_F = 6.28318530717958647692f;
 constexpr float GRAVITY = -9.81f;
 constexpr uint32_t NONE = 0xFFFFFFFFu;
 constexpr int MAX_LIFTERS = 64;
-constexpr int MAX_BOUNDARY_POINTS = 256;
+// Per-ball sweeps (drag, buoyancy): warps taking balls and the poll interval of a waiting ball.
+constexpr uint32_t DEFAULT_SWEEP_WARPS = 16;
+constexpr uint32_t DEFAULT_SPIN_NS = 64;
+constexpr int MAX_BOUNDARY_POINTS = 1024;
 
 // ---------------------------------------------------------------- scalar helpers (f32::max etc.)
 MG_HD float fmax_r(float a, float b) {
@@ -147,6 +150,9 @@ struct StepUniform {
   // squeeze films (mac/lubrication.rs; pbf.rs:544-625)
   FilmConsts pair_film, wall_film;
   uint32_t cg_fp64;
+  uint32_t want_momentum;  // accumulate CouplingImpulses::fluid_momentum_change (coupling.rs:49-51)
+  uint32_t sweep_warps;    // warps taking balls in the per-ball sweeps
+  uint32_t spin_ns;        // poll interval of a waiting ball
 };
 
 // The per-sub-step part of the uniform block (drum angle and its rotations, dt), one per sub-step
@@ -166,6 +172,10 @@ struct StepOut {
   uint32_t n_impacts;
   uint32_t err;
   uint32_t pad;
+  // per-stage device cycles (clock64 deltas at the stage barriers); slots 0-14 follow the
+  // reference's stage_timing.rs STAGE_NAMES, 15-18 split the DEM step, 19 is drag alone, 20-31
+  // split the sweeps further (see capi.STAGE_NAMES)
+  unsigned long long stage[40];
 };
 
 enum : uint32_t {
@@ -257,11 +267,21 @@ struct MillDev {
   float2 *bx0, *bvpre;
   float *bth0, *bompre, *lam_bw, *lam_tot;
   double* f_cw;  // per-ball coupling work of the predict step
+  uint32_t *rec_off, *rec_pred, *ball_done;  // per-ball sweep records (cap_nb + 1, cap_recs, cap_nb)
+  uint32_t* slot;  // per-warp fluid -> item maps of the in-order merges (16 x cap_nf, all NONE at rest)
   uint32_t *pair_i, *pair_j;
   float* lam_bb;
   uint32_t *cs_i, *cs_j;  // contacts sorted by (i, j)
   float* cs_l;
   uint32_t* pair_cnt;  // per cell pair counts (cap cells + 1)
+  // sweep replay (mill_replay.cuh): predecessors, levels, active contacts of the contact sweeps
+  uint32_t *dm_pa, *dm_pb, *dm_lvl, *lev_start, *lev_cur, *lev_items;
+  uint32_t *act_i, *act_j, *act_flag;
+  float *act_l, *act_w1, *act_w2;
+  int32_t* act_bin;
+  MgImpactRecord* act_rec;
+  uint32_t smem_balls;  // balls whose state fits the launch's dynamic shared memory (0: global)
+  uint32_t smem_bytes;  // the launch's dynamic shared memory (staged ball state, then sweep scratch)
   // outputs
   StepOut* out;             // one per sub-step of the launch
   MgImpactRecord* impacts;  // cap_impacts per sub-step of the launch

@@ -1,11 +1,13 @@
 // The ball half of the sub-step (DemState::step_recorded, dem.rs:530-1066) for one mill, executed
-// by one thread block: per-ball stages in parallel; the broad phase materialises the candidate
-// pairs in the grid's visiting order; the Gauss-Seidel projection, friction and restitution
-// sweeps are replayed in the reference's order (bit-exact results).
+// by one thread block. Per-ball stages run in parallel; the broad phase materialises the candidate
+// pairs in the grid's visiting order; the Gauss-Seidel projection, friction and restitution sweeps
+// are replayed exactly (mill_replay.cuh): the projection by dependency levels, the contact sweeps
+// in 32-item chunks. Ball state lives in shared memory during the sweeps when it fits.
 #pragma once
 
 #include "mill_geom.cuh"
 #include "mill_grid.cuh"
+#include "mill_replay.cuh"
 
 namespace mg {
 
@@ -15,7 +17,8 @@ constexpr float CCD_SKIN_FRACTION = 1e-2f;
 
 struct DemShared {
   GridHdr hg;
-  uint32_t npairs;
+  uint32_t npairs, nact, nrec_imp, collisions;
+  uint32_t hist[MG_IMPACT_BINS];
   float fscal[4];
   double dscal[4];
 };
@@ -49,19 +52,31 @@ __device__ __forceinline__ int impact_energy_bin(float e) {
   return (int)(idx < 11u ? idx : 11u);
 }
 
-// dem.rs:253-261 f32 mechanical energy, summed in ball order
-__device__ float mech_energy_seq(const MillDev& m) {
+// dem.rs:253-261 f32 mechanical energy, summed in ball order (three adds per ball); called by
+// warp 0, result in every lane
+__device__ float mech_energy_seq(const MillDev& m, const float2* X, const float2* V, const float* OM) {
+  const uint32_t lane = threadIdx.x & 31u;
   float e = 0.0f;
-  for (uint32_t i = 0; i < m.nb; ++i) {
-    e += 0.5f * m.b_m * V2(m.bv[i]).len2();
-    e += 0.5f * m.b_I * m.bom[i] * m.bom[i];
-    e += m.b_m * fabsf(GRAVITY) * m.bx[i].y;
+  for (uint32_t c = 0; c < m.nb; c += 32) {
+    float a = 0.0f, b = 0.0f, g = 0.0f;
+    uint32_t i = c + lane;
+    if (i < m.nb) {
+      a = 0.5f * m.b_m * V2(V[i]).len2();
+      b = 0.5f * m.b_I * OM[i] * OM[i];
+      g = m.b_m * fabsf(GRAVITY) * X[i].y;
+    }
+    uint32_t lim = min(32u, m.nb - c);
+    for (uint32_t t = 0; t < lim; ++t) {
+      e += __shfl_sync(FULL, a, t);
+      e += __shfl_sync(FULL, b, t);
+      e += __shfl_sync(FULL, g, t);
+    }
   }
   return e;
 }
 
 __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, MgImpactRecord* impacts,
-                         uint32_t* err, DemShared& S) {
+                         uint32_t* err, DemShared& S, unsigned char* dsm) {
   const uint32_t n = m.nb;
   const float dt = U.dt;
   if (tid() == 0) { memset(&out.ds, 0, sizeof(out.ds)); out.n_impacts = 0; }
@@ -72,17 +87,25 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
   const float r = m.b_r;
   const float impact_threshold = 0.1428f * sqrtf(-GRAVITY * 2.0f * r);
   const bool ext = U.dem_external != 0;
+  // ball state: shared memory when it fits, global otherwise
+  const bool staged = n <= m.smem_balls;
   float2 *X = m.bx, *V = m.bv;
   float *TH = m.bth, *OM = m.bom;
+  if (staged) {
+    X = reinterpret_cast<float2*>(dsm);
+    V = X + n;
+    TH = reinterpret_cast<float*>(V + n);
+    OM = TH + n;
+  }
   // step 0 sanitize, snapshots; step 1 predict (dem.rs:558-595)
   float max_disp = 0.0f, max_speed = 0.0f;
   for (uint32_t i = tid(); i < n; i += nthr()) {
-    V2 x(X[i]), v(V[i]);
+    V2 x(m.bx[i]), v(m.bv[i]);
     if (!x.finite() || !v.finite()) { x = V2(); v = V2(); }
+    float th = m.bth[i], om = m.bom[i];
     m.bx0[i] = x.f2();
-    m.bth0[i] = TH[i];
+    m.bth0[i] = th;
     m.bvpre[i] = v.f2();
-    float om = OM[i];
     m.bompre[i] = om;
     v.y += GRAVITY * dt;
     double cw = 0.0;
@@ -97,18 +120,17 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
     X[i] = x.f2();
     V[i] = v.f2();
     OM[i] = om;
-    TH[i] = TH[i] + om * dt;
+    TH[i] = th + om * dt;
     m.f_cw[i] = cw;
     max_disp = fmax_r(max_disp, v.len() * dt / fmax_r(2.0f * r, 1e-12f));
     max_speed = fmax_r(max_speed, v.len());
   }
   max_disp = block_max_f(max_disp);
   max_speed = block_max_f(max_speed);
-  if (tid() == 0) {
-    double cw = 0.0;
-    for (uint32_t i = 0; i < n; ++i) cw += m.f_cw[i];
-    S.dscal[0] = cw;
-    S.fscal[0] = mech_energy_seq(m);
+  if (tid() < 32) {
+    double cw = warp_ordered_sum(0.0, n, [&](uint32_t i, double& t) { t = m.f_cw[i]; return true; });
+    float e = mech_energy_seq(m, X, V, OM);
+    if (tid() == 0) { S.dscal[0] = cw; S.fscal[0] = e; }
   }
   __syncthreads();
   // step 2 broad phase (dem.rs:626-633)
@@ -144,43 +166,85 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
     }
     m.lam_bw[i] = 0.0f;
   }
+  const uint32_t nitems = np + n;
   for (uint32_t k = tid(); k < np; k += nthr()) m.lam_bb[k] = 0.0f;
+  for (uint32_t k = tid(); k < nitems; k += nthr()) { m.dm_pa[k] = NONE; m.dm_pb[k] = NONE; }
+  // occurrence records of the projection sweep: pair k -> (i, 2k), (j, 2k+1); wall of ball b -> 2np+b
+  for (uint32_t q = tid(); q < 2 * np + n; q += nthr())
+    m.rec_i[q] = q < 2 * np ? ((q & 1u) ? m.pair_j[q >> 1] : m.pair_i[q >> 1]) : q - 2 * np;
   __syncthreads();
-  // step 3 projection: Gauss-Seidel over pairs in grid order, then walls (dem.rs:711-750)
-  if (tid() == 0) {
-    for (uint32_t it = 0; it < iters; ++it) {
-      for (uint32_t k = 0; k < np; ++k) {
-        uint32_t i = m.pair_i[k], j = m.pair_j[k];
+  stage_mark(out.stage, 15);
+  preds_from_records(m.rec_i, 2 * np + n, n, n, m.bk_start, m.bk_cur, m.bk_order, m.dm_pa, m.dm_pb,
+                     [&](uint32_t q) { return q < 2 * np ? q >> 1 : np + (q - 2 * np); },
+                     [&](uint32_t q) { return q < 2 * np ? (q & 1u) : 0u; });
+  stage_mark(out.stage, 20);
+  // sweep scratch (levels, level-ordered descriptors, multipliers): shared memory after the ball
+  // state when the items fit, global otherwise
+  uint32_t *lvl = m.dm_lvl, *di = m.act_i, *dj = m.act_j;
+  float* dl = m.act_l;
+  if (staged) {
+    const uint32_t used = (24u * n + 15u) & ~15u;
+    const uint32_t fit = m.smem_bytes > used ? (m.smem_bytes - used) / 16u : 0u;
+    if (nitems <= fit) {
+      lvl = reinterpret_cast<uint32_t*>(dsm + used);
+      di = lvl + nitems;
+      dj = di + nitems;
+      dl = reinterpret_cast<float*>(dj + nitems);
+    }
+  }
+  const uint32_t nlev = compute_levels(nitems, m.dm_pa, m.dm_pb, lvl);
+  stage_mark(out.stage, 21);
+  bucket_levels(nitems, lvl, nlev, m.lev_start, m.lev_cur, m.lev_items);
+  // level-ordered sweep descriptors: balls (j = NONE for a wall) and a lambda accumulator
+  for (uint32_t q = tid(); q < nitems; q += nthr()) {
+    uint32_t k = m.lev_items[q];
+    di[q] = k < np ? m.pair_i[k] : k - np;
+    dj[q] = k < np ? m.pair_j[k] : NONE;
+    dl[q] = 0.0f;
+  }
+  __syncthreads();
+  stage_mark(out.stage, 22);
+  // step 3 projection: pairs in grid order, then walls, `iters` times (dem.rs:711-750)
+  for (uint32_t it = 0; it < iters; ++it) {
+    run_levels(nlev, m.lev_start, [&](uint32_t q) {
+      const uint32_t i = di[q], j = dj[q];
+      if (j != NONE) {
         V2 xi(X[i]), xj(X[j]);
         V2 delta = xi - xj;
         float dist = delta.len();
         float c = dist - 2.0f * r;
-        if (c >= 0.0f) continue;
+        if (c >= 0.0f) return;
         V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
         float w_sum = w + w;
-        if (w_sum <= 0.0f) continue;
+        if (w_sum <= 0.0f) return;
         float c_eff = fmax_r(c, cap_depth);
         float d_lambda = -c_eff / w_sum;
         X[i] = (xi + w * d_lambda * n_hat).f2();
         X[j] = (xj - w * d_lambda * n_hat).f2();
-        m.lam_bb[k] += d_lambda;
-      }
-      for (uint32_t i = 0; i < n; ++i) {
+        dl[q] += d_lambda;
+      } else {
         V2 x(X[i]);
         float d;
         V2 n_hat;
         drum_sdf_world(U, x, U.to_local_next, U.to_world_next, d, n_hat);
         float c = d - r;
-        if (c >= 0.0f) continue;
-        if (w <= 0.0f) continue;
+        if (c >= 0.0f) return;
+        if (w <= 0.0f) return;
         float c_eff = fmax_r(c, cap_depth);
         float d_lambda = -c_eff / w;
         X[i] = (x + w * d_lambda * n_hat).f2();
-        m.lam_bw[i] += d_lambda;
+        dl[q] += d_lambda;
       }
-    }
+    });
+  }
+  // the accumulated multipliers back to pair / ball order (ContactBook, dem.rs:437-454)
+  for (uint32_t q = tid(); q < nitems; q += nthr()) {
+    uint32_t k = m.lev_items[q];
+    if (k < np) m.lam_bb[k] = dl[q];
+    else m.lam_bw[k - np] = dl[q];
   }
   __syncthreads();
+  stage_mark(out.stage, 16);
   // step 4 velocity reconstruction (dem.rs:753-756)
   for (uint32_t i = tid(); i < n; i += nthr()) {
     V[i] = ((V2(X[i]) - V2(m.bx0[i])) / dt).f2();
@@ -200,29 +264,53 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
     }
   }
   __syncthreads();
-  for (uint32_t q = tid(); q < np; q += nthr()) {
-    uint32_t k = m.bk_order[q];
-    m.cs_i[q] = m.pair_i[k];
-    m.cs_j[q] = m.pair_j[k];
-    m.cs_l[q] = m.lam_bb[k];
+  // the contact sweeps visit only contacts with lambda_n > 0: sorted pairs, then walls
+  for (uint32_t q = tid(); q < nitems; q += nthr()) {
+    float l = q < np ? m.lam_bb[m.bk_order[q]] : m.lam_bw[q - np];
+    m.act_flag[q] = l > 0.0f ? 1u : 0u;
+  }
+  if (tid() == 0) m.act_flag[nitems] = 0;
+  __syncthreads();
+  const uint32_t na = block_exclusive_scan(m.act_flag, nitems + 1);
+  for (uint32_t q = tid(); q < nitems; q += nthr()) {
+    uint32_t o = m.act_flag[q];
+    if (m.act_flag[q + 1] == o) continue;
+    if (q < np) {
+      uint32_t k = m.bk_order[q];
+      m.act_i[o] = m.pair_i[k];
+      m.act_j[o] = m.pair_j[k];
+      m.act_l[o] = m.lam_bb[k];
+    } else {
+      m.act_i[o] = q - np;
+      m.act_j[o] = NONE;
+      m.act_l[o] = m.lam_bw[q - np];
+    }
   }
   __syncthreads();
-  // step 5 friction: sorted pairs, then walls (dem.rs:782-882)
+  for (uint32_t k = tid(); k < na; k += nthr()) { m.dm_pa[k] = NONE; m.dm_pb[k] = NONE; }
+  for (uint32_t q = tid(); q < 2 * na; q += nthr()) {
+    uint32_t j = m.act_j[q >> 1];
+    m.rec_i[q] = (q & 1u) ? (j == NONE ? n : j) : m.act_i[q >> 1];
+  }
+  __syncthreads();
+  // buckets 0..n-1 are balls; bucket n collects the absent second ball of wall contacts
+  preds_from_records(m.rec_i, 2 * na, n + 1, n, m.bk_start, m.bk_cur, m.bk_order, m.dm_pa, m.dm_pb,
+                     [&](uint32_t q) { return q >> 1; }, [&](uint32_t q) { return q & 1u; });
+  stage_mark(out.stage, 30);
+  // step 5 friction (dem.rs:782-882)
   const MgMediaParams& md = U.media;
-  if (tid() == 0) {
-    uint32_t act = 0;
-    for (uint32_t q = 0; q < np; ++q) {
-      float lambda_n = m.cs_l[q];
-      if (lambda_n <= 0.0f) continue;
-      ++act;
-      uint32_t i = m.cs_i[q], j = m.cs_j[q];
+  auto load_contact = [&](uint32_t k) { return make_uint3(m.act_i[k], m.act_j[k], __float_as_uint(m.act_l[k])); };
+  run_chunked(na, m.dm_pa, m.dm_pb, load_contact, [&](uint32_t k, uint3 d) {
+    const uint32_t i = d.x, j = d.y;
+    const float lambda_n = __uint_as_float(d.z);
+    if (j != NONE) {
       V2 delta = V2(X[i]) - V2(X[j]);
       float dist = delta.len();
       V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
       V2 t_hat(-n_hat.y, n_hat.x);
       float v_t = (V2(V[i]) - V2(V[j])).dot(t_hat) - r * OM[i] - r * OM[j];
       float w_sum_t = w + w + r * r * w_rot + r * r * w_rot;
-      if (w_sum_t <= 0.0f) continue;
+      if (w_sum_t <= 0.0f) return;
       float raw = -v_t * dt / w_sum_t;
       float mu = effective_friction(md.friction_ball_ball, md.friction_ball_ball_static, v_t, md.friction_velocity_scale_m_s);
       float max_mag = mu * lambda_n;
@@ -237,12 +325,8 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
       V[j] = (V2(V[j]) - dv).f2();
       OM[i] += domega;
       OM[j] += domega;
-    }
-    out.ctr.n_active_contacts = act;
-    float wall_work = 0.0f;
-    for (uint32_t i = 0; i < n; ++i) {
-      float lambda_n = m.lam_bw[i];
-      if (lambda_n <= 0.0f) continue;
+    } else {
+      m.act_bin[k] = -2;  // no work terms unless the contact completes below
       float dd;
       V2 n_hat;
       drum_sdf_world(U, V2(X[i]), U.to_local_next, U.to_world_next, dd, n_hat);
@@ -250,7 +334,7 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
       V2 v_wall = wall_velocity(U.drum_omega, V2(X[i]) - r * n_hat);
       float v_t = (V2(V[i]) - v_wall).dot(t_hat) - r * OM[i];
       float w_sum_t = w + r * r * w_rot;
-      if (w_sum_t <= 0.0f) continue;
+      if (w_sum_t <= 0.0f) return;
       float raw = -v_t * dt / w_sum_t;
       float mu = effective_friction(md.friction_ball_wall, md.friction_ball_wall_static, v_t, md.friction_velocity_scale_m_s);
       float max_mag = mu * lambda_n;
@@ -259,57 +343,77 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
       TH[i] -= r * w_rot * dlt;
       V[i] = (V2(V[i]) + w * dlt * t_hat / dt).f2();
       OM[i] += -r * w_rot * dlt / dt;
-      wall_work += (dlt / dt) * t_hat.dot(v_wall);
-      wall_work += (lambda_n / dt) * n_hat.dot(v_wall);
+      m.act_w1[k] = (dlt / dt) * t_hat.dot(v_wall);
+      m.act_w2[k] = (lambda_n / dt) * n_hat.dot(v_wall);
+      m.act_bin[k] = 0;
     }
-    S.fscal[1] = wall_work;
+  });
+  if (tid() < 32) {
+    // wall work summed in wall-contact order, two adds per contact (dem.rs:870, 881)
+    const uint32_t lane = tid();
+    float wall_work = 0.0f;
+    uint32_t act = 0;
+    for (uint32_t c = 0; c < na; c += 32) {
+      uint32_t k = c + lane;
+      bool wall = k < na && m.act_j[k] == NONE && m.act_bin[k] != -2;
+      act += (k < na && m.act_j[k] != NONE) ? 1u : 0u;
+      float a = wall ? m.act_w1[k] : 0.0f, b = wall ? m.act_w2[k] : 0.0f;
+      uint32_t mask = __ballot_sync(FULL, wall);
+      while (mask) {
+        int t = __ffs(mask) - 1;
+        mask &= mask - 1;
+        wall_work += __shfl_sync(FULL, a, t);
+        wall_work += __shfl_sync(FULL, b, t);
+      }
+    }
+    act = warp_sum(act);
+    if (lane == 0) {
+      S.fscal[1] = wall_work;
+      out.ctr.n_active_contacts = act;
+      S.collisions = 0;
+      for (int q = 0; q < MG_IMPACT_BINS; ++q) S.hist[q] = 0;
+    }
   }
   __syncthreads();
+  stage_mark(out.stage, 17);
   // resync (dem.rs:887-890)
   for (uint32_t i = tid(); i < n; i += nthr()) {
     V[i] = ((V2(X[i]) - V2(m.bx0[i])) / dt).f2();
     OM[i] = angle_diff(TH[i], m.bth0[i], err) / dt;
   }
   __syncthreads();
-  // step 6 restitution with impact accounting (dem.rs:909-1019)
-  if (tid() == 0) {
-    uint32_t collisions = 0, nrec = 0;
-    uint32_t hist[MG_IMPACT_BINS];
-    for (int k = 0; k < MG_IMPACT_BINS; ++k) hist[k] = 0;
-    for (uint32_t q = 0; q < np; ++q) {
-      if (m.cs_l[q] <= 0.0f) continue;
-      uint32_t i = m.cs_i[q], j = m.cs_j[q];
+  // step 6 restitution with impact accounting (dem.rs:909-1019); per-item records are compacted
+  // in sweep order afterwards
+  run_chunked(na, m.dm_pa, m.dm_pb, load_contact, [&](uint32_t k, uint3 d) {
+    const uint32_t i = d.x, j = d.y;
+    m.act_flag[k] = 0;
+    if (j != NONE) {
       V2 delta = V2(X[i]) - V2(X[j]);
       float dist = delta.len();
       V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
       float v_n_pre = (V2(m.bvpre[i]) - V2(m.bvpre[j])).dot(n_hat);
       bool fresh = v_n_pre < -RESTITUTION_VELOCITY_THRESHOLD;
       if (fresh) {
-        collisions += 1;
+        atomicAdd(&S.collisions, 1u);
         int bin = impact_energy_bin(0.5f * (m.b_m * 0.5f) * v_n_pre * v_n_pre);
-        if (bin >= 0) hist[bin] += 1;
+        if (bin >= 0) atomicAdd(&S.hist[bin], 1u);
       }
       float e = fresh ? md.restitution_ball_ball : 0.0f;
       if (-v_n_pre > impact_threshold) {
-        if (nrec < m.cap_impacts) {
-          V2 t_hat(-n_hat.y, n_hat.x);
-          float slip = (V2(m.bvpre[i]) - V2(m.bvpre[j])).dot(t_hat) - r * m.bompre[i] - r * m.bompre[j];
-          impacts[nrec] = MgImpactRecord{MG_IMPACT_BALL_BALL, i, j, -v_n_pre, fabsf(slip), e};
-        }
-        ++nrec;
+        V2 t_hat(-n_hat.y, n_hat.x);
+        float slip = (V2(m.bvpre[i]) - V2(m.bvpre[j])).dot(t_hat) - r * m.bompre[i] - r * m.bompre[j];
+        m.act_rec[k] = MgImpactRecord{MG_IMPACT_BALL_BALL, i, j, -v_n_pre, fabsf(slip), e};
+        m.act_flag[k] = 1;
       }
       float target = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
       float v_n_now = (V2(V[i]) - V2(V[j])).dot(n_hat);
       float dvn = target - v_n_now;
       float w_sum = w + w;
-      if (w_sum <= 0.0f) continue;
+      if (w_sum <= 0.0f) return;
       float impulse = dvn / w_sum;
       V[i] = (V2(V[i]) + w * impulse * n_hat).f2();
       V[j] = (V2(V[j]) - w * impulse * n_hat).f2();
-    }
-    for (uint32_t i = 0; i < n; ++i) {
-      float lambda_n = m.lam_bw[i];
-      if (lambda_n <= 0.0f) continue;
+    } else {
       float dd;
       V2 n_hat;
       drum_sdf_world(U, V2(X[i]), U.to_local_next, U.to_world_next, dd, n_hat);
@@ -317,61 +421,70 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
       float v_n_pre = (V2(m.bvpre[i]) - v_wall).dot(n_hat);
       bool fresh = v_n_pre < -RESTITUTION_VELOCITY_THRESHOLD;
       if (fresh) {
-        collisions += 1;
+        atomicAdd(&S.collisions, 1u);
         int bin = impact_energy_bin(0.5f * m.b_m * v_n_pre * v_n_pre);
-        if (bin >= 0) hist[bin] += 1;
+        if (bin >= 0) atomicAdd(&S.hist[bin], 1u);
       }
       float e = fresh ? md.restitution_ball_wall : 0.0f;
       if (-v_n_pre > impact_threshold) {
-        if (nrec < m.cap_impacts) {
-          V2 t_hat(-n_hat.y, n_hat.x);
-          float slip = (V2(m.bvpre[i]) - v_wall).dot(t_hat) - r * m.bompre[i];
-          impacts[nrec] = MgImpactRecord{MG_IMPACT_BALL_WALL, i, MG_WALL_PARTNER, -v_n_pre, fabsf(slip), e};
-        }
-        ++nrec;
+        V2 t_hat(-n_hat.y, n_hat.x);
+        float slip = (V2(m.bvpre[i]) - v_wall).dot(t_hat) - r * m.bompre[i];
+        m.act_rec[k] = MgImpactRecord{MG_IMPACT_BALL_WALL, i, MG_WALL_PARTNER, -v_n_pre, fabsf(slip), e};
+        m.act_flag[k] = 1;
       }
       float target = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
       float v_n_now = (V2(V[i]) - v_wall).dot(n_hat);
       float dvn = target - v_n_now;
-      if (w <= 0.0f) continue;
+      if (w <= 0.0f) return;
       V[i] = (V2(V[i]) + dvn * n_hat).f2();
     }
-    out.ds.collision_count = collisions;
-    for (int k = 0; k < MG_IMPACT_BINS; ++k) out.ds.impact_energy_histogram[k] = hist[k];
+  });
+  if (tid() == 0) m.act_flag[na] = 0;
+  __syncthreads();
+  const uint32_t nrec = block_exclusive_scan(m.act_flag, na + 1);
+  for (uint32_t k = tid(); k < na; k += nthr()) {
+    uint32_t o = m.act_flag[k];
+    if (m.act_flag[k + 1] != o && o < m.cap_impacts) impacts[o] = m.act_rec[k];
+  }
+  if (tid() == 0) {
+    out.ds.collision_count = S.collisions;
+    for (int q = 0; q < MG_IMPACT_BINS; ++q) out.ds.impact_energy_histogram[q] = S.hist[q];
     out.n_impacts = nrec;
     if (nrec > m.cap_impacts) atomicOr(err, ERR_IMPACTS);
-    // step 7 rolling resistance sums, in sorted-contact order then walls (dem.rs:1036-1044)
-    if (md.rolling_friction > 0.0f && m.b_I > 0.0f) {
-      for (uint32_t i = 0; i < n; ++i) m.lam_tot[i] = 0.0f;
-      for (uint32_t q = 0; q < np; ++q) {
-        float l = fmax_r(m.cs_l[q], 0.0f);
-        m.lam_tot[m.cs_i[q]] += l;
-        m.lam_tot[m.cs_j[q]] += l;
-      }
-      for (uint32_t i = 0; i < n; ++i) m.lam_tot[i] += fmax_r(m.lam_bw[i], 0.0f);
-    }
   }
-  __syncthreads();
+  // step 7 rolling resistance (dem.rs:1036-1055): per ball, sum lambda_n over its contacts in
+  // sweep order (sorted pairs, then the wall); contacts with lambda_n <= 0 add +0 and are skipped
   if (md.rolling_friction > 0.0f && m.b_I > 0.0f) {
-    for (uint32_t i = tid(); i < n; i += nthr()) {
-      float ln = m.lam_tot[i];
-      float om = OM[i];
-      if (ln <= 0.0f || om == 0.0f) continue;
-      float normal_force = ln / dt;
+    for (uint32_t b = tid(); b < n; b += nthr()) {
+      float tot = 0.0f;
+      for (uint32_t q = m.bk_start[b]; q < m.bk_start[b + 1]; ++q) tot += fmax_r(m.act_l[m.bk_order[q] >> 1], 0.0f);
+      float om = OM[b];
+      if (tot <= 0.0f || om == 0.0f) continue;
+      float normal_force = tot / dt;
       float max_dw = md.rolling_friction * normal_force * r / m.b_I * dt;
       float dw = fmin_r(max_dw, fabsf(om));
-      OM[i] = om - (om < 0.0f ? -1.0f : 1.0f) * dw;
+      OM[b] = om - (om < 0.0f ? -1.0f : 1.0f) * dw;
     }
   }
   __syncthreads();
+  float e_final = 0.0f;
+  if (tid() < 32) e_final = mech_energy_seq(m, X, V, OM);
   if (tid() == 0) {
-    float e_final = mech_energy_seq(m);
     out.ds.wall_work_j = S.fscal[1];
     out.ds.dissipated_energy_j = S.fscal[0] + S.fscal[1] - e_final;
     out.ds.max_substep_displacement_over_diameter = max_disp;
     out.ds.coupling_work_j = (float)S.dscal[0];
   }
+  if (staged) {
+    for (uint32_t i = tid(); i < n; i += nthr()) {
+      m.bx[i] = X[i];
+      m.bv[i] = V[i];
+      m.bth[i] = TH[i];
+      m.bom[i] = OM[i];
+    }
+  }
   __syncthreads();
+  stage_mark(out.stage, 18);
 }
 
 }  // namespace mg

@@ -7,6 +7,7 @@
 
 #include "mill_geom.cuh"
 #include "mill_grid.cuh"
+#include "mill_replay.cuh"
 
 namespace mg {
 
@@ -34,10 +35,9 @@ __device__ __forceinline__ float fluid_vmax(const StepUniform& U) {
 
 // pbf.rs:924-926: 0.5 m sum |v|^2 in f64, summed in particle order.
 __device__ double kinetic_energy_seq(const float2* v, uint32_t n, float mass, FluidShared& S) {
-  if (tid() == 0) {
-    double s = 0.0;
-    for (uint32_t i = 0; i < n; ++i) s += (double)V2(v[i]).len2();
-    S.dscal[7] = 0.5 * (double)mass * s;
+  if (tid() < 32) {
+    double s = warp_ordered_sum(0.0, n, [&](uint32_t i, double& t) { t = (double)V2(v[i]).len2(); return true; });
+    if (tid() == 0) S.dscal[7] = 0.5 * (double)mass * s;
   }
   __syncthreads();
   double r = S.dscal[7];
@@ -53,10 +53,9 @@ __device__ double block_dot(const float2* a, const float2* b, uint32_t len, bool
       acc += (double)a[e].x * (double)b[e].x + (double)a[e].y * (double)b[e].y;
     return block_sum_d(acc);
   }
-  if (tid() == 0) {
-    float s = 0.0f;
-    for (uint32_t e = 0; e < len; ++e) s += V2(a[e]).dot(V2(b[e]));
-    S.fscal[7] = s;
+  if (tid() < 32) {
+    float s = warp_ordered_sum(0.0f, len, [&](uint32_t e, float& t) { t = V2(a[e]).dot(V2(b[e])); return true; });
+    if (tid() == 0) S.fscal[7] = s;
   }
   __syncthreads();
   double r = (double)S.fscal[7];
@@ -72,10 +71,9 @@ __device__ double block_res_norm(const float2* r, const float* inv, uint32_t len
       acc += (double)inv[e] * ((double)r[e].x * (double)r[e].x + (double)r[e].y * (double)r[e].y);
     return sqrt(block_sum_d(acc));
   }
-  if (tid() == 0) {
-    float s = 0.0f;
-    for (uint32_t e = 0; e < len; ++e) s += inv[e] * V2(r[e]).len2();
-    S.fscal[6] = sqrtf(s);
+  if (tid() < 32) {
+    float s = warp_ordered_sum(0.0f, len, [&](uint32_t e, float& t) { t = inv[e] * V2(r[e]).len2(); return true; });
+    if (tid() == 0) S.fscal[6] = sqrtf(s);
   }
   __syncthreads();
   double v = (double)S.fscal[6];
@@ -119,7 +117,7 @@ __device__ __forceinline__ double resolved_ratio(double hc) {
 struct LinkEval { bool in_range, emit; V2 n; float c; };
 
 __device__ __forceinline__ LinkEval link_pair(const MillDev& m, const StepUniform& U, uint32_t i, uint32_t j,
-                                              float reach, float range2, double dxd, float c_max) {
+                                              float reach, float range2, double dxd, float c_max, bool need_c = true) {
   LinkEval L{false, false, V2(), 0.0f};
   float r = m.b_r;
   V2 xi(m.bx[i]);
@@ -131,6 +129,8 @@ __device__ __forceinline__ LinkEval link_pair(const MillDev& m, const StepUnifor
   L.in_range = true;
   L.n = e / dist;
   if (L.n.dot(V2(m.ball_v0[i]) - V2(m.ball_v0[j])) <= 0.0f) return L;
+  L.emit = true;
+  if (!need_c) return L;
   double weight = 1.0 - resolved_ratio((double)gap / dxd);
   double hh = (double)gap > 0.02 * (double)r ? (double)gap : 0.02 * (double)r;
   double c = weight * film_coefficient(U.pair_film, hh);
@@ -212,7 +212,9 @@ __device__ void joint_apply(const MillDev& m, float dt, const float2* xx, float2
   __syncthreads();
 }
 
-__device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err, FluidShared& S) {
+__device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err, FluidShared& S,
+                           unsigned char* dsm) {
+  uint32_t* done = m.ball_done;  // completion flags of the per-ball sweeps (moved to shared below)
   const uint32_t n = m.nf, nb = m.nb;
   const float dt = U.dt;
   for (uint32_t b = tid(); b < nb; b += nthr()) { m.imp[b] = make_float2(0.0f, 0.0f); m.ang[b] = 0.0f; }
@@ -243,6 +245,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
   grid_build(X, n, h, m.gA, S.hA, err);
   build_neighbor_lists(X, n, h, S.hA, m.gA, m.nbr_off, m.nbrs, m.cap_edges, err, &S.n_edges);
   if (tid() == 0) out.ctr.n_fluid_edges = S.n_edges;
+  stage_mark(out.stage, 0);
   if (*err) return;
   // ---- step 3: density constraint (pbf.rs:1257-1334)
   const uint32_t base_it = U.pbf_iterations > 1 ? U.pbf_iterations : 1u;
@@ -292,6 +295,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
     if ((iter_count >= base_it && converged) || iter_count >= base_it + ADAPTIVE_MAX_EXTRA) break;
   }
   if (tid() == 0) out.ctr.density_iters = iter_count;
+  stage_mark(out.stage, 1);
   // ---- step 3.5: ball overlap push (pbf.rs:1361-1444); two passes (count, fill), then the
   // per-ball reaction sums replayed in the reference's (fluid index, near order) order.
   for (uint32_t i = tid(); i < n; i += nthr()) m.push_ex[i] = make_float2(0.0f, 0.0f);
@@ -348,14 +352,24 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
         __syncthreads();
       }
     }
+    // per-ball reaction sums in record order (fluid index ascending, near order): a stable
+    // bucket sort of the records by ball, then one thread per ball
+    block_bucket_sort(m.rec_b, S.n_recs, nb, m.bk_start, m.bk_cur, m.bk_order);
+    for (uint32_t b = tid(); b < nb; b += nthr()) {
+      V2 J;
+      float L = 0.0f;
+      for (uint32_t q = m.bk_start[b]; q < m.bk_start[b + 1]; ++q) {
+        uint32_t r = m.bk_order[q];
+        J += V2(m.rec_J[r]);
+        L += m.rec_L[r];
+      }
+      m.imp[b] = J.f2();
+      m.ang[b] = L;
+    }
     if (tid() == 0) {
       V2 mom;
-      for (uint32_t q = 0; q < S.n_recs; ++q) {
-        uint32_t b = m.rec_b[q];
-        m.imp[b] = (V2(m.imp[b]) + V2(m.rec_J[q])).f2();
-        mom += V2(m.rec_M[q]);
-        m.ang[b] += m.rec_L[q];
-      }
+      if (U.want_momentum)
+        for (uint32_t q = 0; q < S.n_recs; ++q) mom += V2(m.rec_M[q]);
       S.fscal[0] = mom.x;
       S.fscal[1] = mom.y;
     }
@@ -363,6 +377,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
     S.fscal[0] = S.fscal[1] = 0.0f;
   }
   __syncthreads();
+  stage_mark(out.stage, 2);
   // ---- step 3.6a: cohesion (pbf.rs:1464-1491)
   const float cohesion_accel = (fmax_r(U.slurry.surface_tension_n_m, 0.0f) / 0.072f) * 2.0f * fabsf(GRAVITY);
   for (uint32_t i = tid(); i < n; i += nthr()) {
@@ -383,6 +398,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
     m.adh_dv[i] = make_float2(0.0f, 0.0f);
   }
   __syncthreads();
+  stage_mark(out.stage, 3);
   // ---- step 3.6b: adhesion (pbf.rs:1515-1631) on the stale step-2 grid
   const float wett = clamp_r(U.slurry.wettability, 0.0f, 1.0f);
   const uint32_t count_pb = U.boundary_count;
@@ -392,43 +408,57 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       const float adhesion_accel = wett * 2.0f * fabsf(GRAVITY);
       const float range2 = h_adh * h_adh * (1.0f + 1e-4f);
       const float inner2 = 0.25f * h_adh * h_adh * (1.0f - 1e-4f);
-      for (uint32_t b = tid(); b < nb; b += nthr()) {
-        uint32_t base = b * m.cap_items, cnt = 0;
+      // one warp per ball: candidates of each boundary point in for_each_near order, 32 at a time,
+      // merged per fluid particle in first-seen order
+      const uint32_t lane = tid() & 31u, nwarps = nthr() >> 5;
+      uint32_t* slot = m.slot + (size_t)(tid() >> 5) * m.cap_nf;
+      for (uint32_t b = tid() >> 5; b < nb; b += nwarps) {
+        const uint32_t base = b * m.cap_items;
+        const MergeList L{m.item_j + base, m.item_w + base, m.item_v + base, nullptr, m.cap_items};
+        uint32_t cnt = 0;
         bool overflow = false;
-        V2 xb(m.bx[b]);
+        const V2 xb(m.bx[b]);
         if (xb.finite()) {
           for (uint32_t q = 0; q < count_pb; ++q) {
-            V2 bp = xb + U.boundary_offset[q];
-            for_each_near(S.hA, m.gA, bp, [&](uint32_t j) {
-              V2 delta = bp - V2(X[j]);
-              float r2 = delta.len2();
-              if (r2 >= range2 || r2 <= inner2) return;
-              float r = sqrtf(r2);
-              if (!finite_f(r) || r <= 0.5f * h_adh || r >= h_adh) return;
-              float w = mass * adhesion_kernel(r, h_adh) / rho0;
-              if (w <= 0.0f) return;
-              V2 n_hat = delta / r;
-              uint32_t s = 0;
-              while (s < cnt && m.item_j[base + s] != j) ++s;
-              if (s == cnt) {
-                if (cnt >= m.cap_items) { overflow = true; return; }
-                m.item_j[base + s] = j;
-                m.item_v[base + s] = (w * n_hat).f2();
-                m.item_w[base + s] = w;
-                ++cnt;
-              } else {
-                m.item_v[base + s] = (V2(m.item_v[base + s]) + w * n_hat).f2();
-                m.item_w[base + s] += w;
+            const V2 bp = xb + U.boundary_offset[q];
+            warp_near_chunks(S.hA, m.gA, bp, [&](uint32_t j, uint32_t, bool valid) {
+              bool acc = false;
+              float w = 0.0f;
+              V2 dir;
+              if (valid) {
+                V2 delta = bp - V2(X[j]);
+                float r2 = delta.len2();
+                if (!(r2 >= range2 || r2 <= inner2)) {
+                  float r = sqrtf(r2);
+                  if (!(!finite_f(r) || r <= 0.5f * h_adh || r >= h_adh)) {
+                    w = mass * adhesion_kernel(r, h_adh) / rho0;
+                    if (w > 0.0f) { acc = true; dir = w * (delta / r); }
+                  }
+                }
               }
+              warp_merge(acc, j, w, dir, 0.0f, slot, L, cnt, overflow);
             });
           }
         }
-        if (overflow) atomicOr(err, ERR_ITEMS);
+        for (uint32_t s = lane; s < min(cnt, m.cap_items); s += 32) slot[L.j[s]] = NONE;
+        __syncwarp();
+        if (__any_sync(FULL, overflow)) { if (lane == 0) atomicOr(err, ERR_ITEMS); cnt = 0; }
         uint32_t used = 0;
         if (cnt > 0) {
-          float weight_sum = 0.0f;
-          V2 dir_sum;
-          for (uint32_t s = 0; s < cnt; ++s) { dir_sum += V2(m.item_v[base + s]); weight_sum += m.item_w[base + s]; }
+          // dir_sum and weight_sum in item order (pbf.rs:1586-1594)
+          float weight_sum = 0.0f, dsx = 0.0f, dsy = 0.0f;
+          for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+            const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
+            float ww = 0.0f;
+            V2 dd;
+            if (s < cnt) { ww = L.v0[s]; dd = V2(L.v1[s]); }
+            for (uint32_t t = 0; t < lim; ++t) {
+              dsx += __shfl_sync(FULL, dd.x, t);
+              dsy += __shfl_sync(FULL, dd.y, t);
+              weight_sum += __shfl_sync(FULL, ww, t);
+            }
+          }
+          V2 dir_sum(dsx, dsy);
           float pull_len = dir_sum.len();
           if (weight_sum > 1e-9f && pull_len > 1e-9f) {
             V2 ball_pull_dir = -dir_sum / pull_len;
@@ -436,38 +466,47 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
             float m_contrib = mass * weight_sum;
             float attach = m_contrib / (m.b_m + m_contrib);
             V2 dv_b = ball_pull_dir * (adhesion_accel * coverage * dt * attach);
-            m.imp[b] = (V2(m.imp[b]) + m.b_m * dv_b).f2();
-            V2 lever = ball_pull_dir * m.b_r;
-            m.ang[b] += m.b_m * cross2(lever, dv_b);
-            for (uint32_t s = 0; s < cnt; ++s) {
-              float frac = m.item_w[base + s] / weight_sum;
+            if (lane == 0) {
+              m.imp[b] = (V2(m.imp[b]) + m.b_m * dv_b).f2();
+              V2 lever = ball_pull_dir * m.b_r;
+              m.ang[b] += m.b_m * cross2(lever, dv_b);
+            }
+            for (uint32_t s = lane; s < cnt; s += 32) {
+              float frac = L.v0[s] / weight_sum;
               V2 dv_i = -(m.b_m * frac / mass) * dv_b;
-              m.item_v[base + s] = dv_i.f2();
+              L.v1[s] = dv_i.f2();
             }
             used = cnt;
           }
         }
-        m.item_n[b] = used;
+        if (lane == 0) m.item_n[b] = used;
+        __syncwarp();
       }
       __syncthreads();
       if (*err) return;
-      if (tid() == 0) {
+      // per-fluid sums of the balls' contributions in ball order (stable bucket sort by fluid)
+      uint32_t nrec = pack_ball_items(m.item_j, m.item_n, m.cap_items, nb, m.rec_off, m.rec_i, m.rec_b);
+      for (uint32_t b = tid(); b < nb; b += nthr()) {
+        uint32_t o = m.rec_off[b], base = b * m.cap_items;
+        for (uint32_t s = 0; s < m.item_n[b]; ++s) m.rec_J[o + s] = m.item_v[base + s];
+      }
+      __syncthreads();
+      block_bucket_sort(m.rec_i, nrec, n, m.bk_start, m.bk_cur, m.bk_order);
+      for (uint32_t j = tid(); j < n; j += nthr()) {
+        V2 acc;
+        for (uint32_t q = m.bk_start[j]; q < m.bk_start[j + 1]; ++q) acc += V2(m.rec_J[m.bk_order[q]]);
+        if (m.bk_start[j + 1] > m.bk_start[j]) m.adh_dv[j] = acc.f2();
+      }
+      if (tid() == 0 && U.want_momentum) {
         V2 mom(S.fscal[0], S.fscal[1]);
-        for (uint32_t b = 0; b < nb; ++b) {
-          uint32_t base = b * m.cap_items;
-          for (uint32_t s = 0; s < m.item_n[b]; ++s) {
-            uint32_t j = m.item_j[base + s];
-            V2 dv_i(m.item_v[base + s]);
-            m.adh_dv[j] = (V2(m.adh_dv[j]) + dv_i).f2();
-            mom += mass * dv_i;
-          }
-        }
+        for (uint32_t r = 0; r < nrec; ++r) mom += mass * V2(m.rec_J[r]);
         S.fscal[0] = mom.x;
         S.fscal[1] = mom.y;
       }
       __syncthreads();
     }
   }
+  stage_mark(out.stage, 4);
   // ---- step 4: wall projection (pbf.rs:1635-1653)
   for (uint32_t i = tid(); i < n; i += nthr()) {
     V2 x(X[i]);
@@ -489,23 +528,33 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
     }
   }
   __syncthreads();
-  if (tid() == 0) {
+  // accumulations in particle order by warp 0: each lane keeps one angle bin; every lane carries
+  // the three f64 sums (identical chains)
+  if (tid() < 32) {
+    const int lane = tid();
+    float bin_acc = 0.0f;
     double ix = 0.0, iy = 0.0, ia = 0.0;
-    float bins[32];
-    for (int k = 0; k < 32; ++k) bins[k] = 0.0f;
-    for (uint32_t i = 0; i < n; ++i) {
-      int32_t bin = m.wall_bin[i];
-      if (bin < 0) continue;
-      V2 push(m.dv_tmp[i]);
-      ix += (double)push.x;
-      iy += (double)push.y;
-      ia += (double)m.f_tmp[i];
-      bins[bin] += m.wall_val[i];
+    for (uint32_t c = 0; c < n; c += 32) {
+      int32_t bin = -1;
+      float val = 0.0f, px = 0.0f, py = 0.0f, pa = 0.0f;
+      if (c + lane < n) {
+        bin = m.wall_bin[c + lane];
+        if (bin >= 0) { val = m.wall_val[c + lane]; px = m.dv_tmp[c + lane].x; py = m.dv_tmp[c + lane].y; pa = m.f_tmp[c + lane]; }
+      }
+      uint32_t mask = __ballot_sync(FULL, bin >= 0);
+      while (mask) {
+        int t = __ffs(mask) - 1;
+        mask &= mask - 1;
+        int bt = __shfl_sync(FULL, bin, t);
+        float vt = __shfl_sync(FULL, val, t);
+        ix += (double)__shfl_sync(FULL, px, t);
+        iy += (double)__shfl_sync(FULL, py, t);
+        ia += (double)__shfl_sync(FULL, pa, t);
+        if (bt == lane) bin_acc += vt;
+      }
     }
-    S.dscal[0] = ix;
-    S.dscal[1] = iy;
-    S.dscal[2] = ia;
-    for (int k = 0; k < 32; ++k) out.fs.wall_normal_impulse_by_angle[k] = bins[k];
+    out.fs.wall_normal_impulse_by_angle[lane] = bin_acc;
+    if (lane == 0) { S.dscal[0] = ix; S.dscal[1] = iy; S.dscal[2] = ia; }
   }
   __syncthreads();
   // ---- step 5: velocity reconstruction (pbf.rs:1656-1674)
@@ -531,28 +580,56 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       m.dv_tmp[i] = (v - v_old).f2();
     }
     __syncthreads();
-    if (tid() == 0) {
+    // accumulations in particle order, continuing the step-4 sums (warp 0, identical chains)
+    if (tid() < 32) {
+      const int lane = tid();
       float work = 0.0f;
       double ix = S.dscal[0], iy = S.dscal[1], ia = S.dscal[2];
-      for (uint32_t i = 0; i < n; ++i) {
-        if (m.wall_bin[i] < 0) continue;
-        V2 x(X[i]);
-        V2 v_wall = wall_velocity(U.drum_omega, x);
-        V2 dv(m.dv_tmp[i]);
-        work += mass * dv.dot(v_wall);
-        ix += (double)(mass * dv.x);
-        iy += (double)(mass * dv.y);
-        ia += (double)cross2(x, mass * dv);
+      for (uint32_t c = 0; c < n; c += 32) {
+        bool touched = c + lane < n && m.wall_bin[c + lane] >= 0;
+        float wk = 0.0f, jx = 0.0f, jy = 0.0f, ja = 0.0f;
+        if (touched) {
+          V2 x(X[c + lane]);
+          V2 dv(m.dv_tmp[c + lane]);
+          wk = mass * dv.dot(wall_velocity(U.drum_omega, x));
+          jx = mass * dv.x;
+          jy = mass * dv.y;
+          ja = cross2(x, mass * dv);
+        }
+        uint32_t mask = __ballot_sync(FULL, touched);
+        while (mask) {
+          int t = __ffs(mask) - 1;
+          mask &= mask - 1;
+          work += __shfl_sync(FULL, wk, t);
+          ix += (double)__shfl_sync(FULL, jx, t);
+          iy += (double)__shfl_sync(FULL, jy, t);
+          ia += (double)__shfl_sync(FULL, ja, t);
+        }
       }
-      S.dscal[0] = ix;
-      S.dscal[1] = iy;
-      S.dscal[2] = ia;
-      out.fs.wall_work_j = work;
+      __syncwarp();
+      if (lane == 0) { S.dscal[0] = ix; S.dscal[1] = iy; S.dscal[2] = ia; out.fs.wall_work_j = work; }
     }
     __syncthreads();
   }
   double ke_mark = kinetic_energy_seq(V, n, mass, S);
   const double ke_delta_noslip = ke_mark - ke_before_noslip;
+  stage_mark(out.stage, 5);
+  // The drag and buoyancy sweeps (steps 6.5 / 6.6) run on copies of X and V in the dynamic shared
+  // region when they fit, with the per-ball completion flags after them; V is written back after
+  // step 6.6. X does not change in between.
+  float2* Vg = V;
+  float2* Xg = X;
+  if (16u * n + 4u * nb + 64u <= m.smem_bytes) {
+    float2* sX = reinterpret_cast<float2*>(dsm);
+    float2* sV = sX + n;
+    for (uint32_t i = tid(); i < n; i += nthr()) { sX[i] = Xg[i]; sV[i] = Vg[i]; }
+    done = reinterpret_cast<uint32_t*>(sV + n);
+    X = sX;
+    V = sV;
+    __syncthreads();
+  } else {
+    done = m.ball_done;
+  }
   // ---- step 6.5: ball drag, Gauss-Seidel over balls (pbf.rs:1777-2013)
   const float mu = fmax_r(U.slurry.viscosity_pa_s, 0.0f);
   if (nb > 0 && m.b_r > 0.0f && m.b_rtrue > 0.0f && mu > 1e-6f) {
@@ -564,178 +641,387 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       const float h_c = m.b_r + h;
       const float w_hc0 = fmax_r(poly6(0.0f, h_c), 1e-12f);
       grid_build(X, n, fmax_r(h_c, 1e-6f), m.gB, S.hB, err);
-      // item lists per ball (positions do not change during the sweep)
-      for (uint32_t b = tid(); b < nb; b += nthr()) {
-        uint32_t base = b * m.cap_items, cnt = 0;
-        bool overflow = false;
-        V2 xb(m.bx[b]);
+      // item lists per ball in for_each_near order (positions do not change during the sweep):
+      // one warp per ball, an ordered compaction of each 32-candidate chunk
+      for (uint32_t b = tid() >> 5; b < nb; b += nthr() >> 5) {
+        const uint32_t lane = tid() & 31u, base = b * m.cap_items;
+        uint32_t cnt = 0;
+        const V2 xb(m.bx[b]);
         if (xb.finite()) {
-          for_each_near(S.hB, m.gB, xb, [&](uint32_t j) {
-            V2 r_i = V2(X[j]) - xb;
-            float r2 = r_i.len2();
-            if (!finite_f(r2) || r2 >= h_c * h_c) return;
-            float phi = poly6(r2, h_c) / w_hc0;
-            if (phi <= 0.0f) return;
-            if (cnt >= m.cap_items) { overflow = true; return; }
-            m.item_j[base + cnt] = j;
-            m.item_v[base + cnt] = r_i.f2();
-            m.item_w[base + cnt] = phi;
-            ++cnt;
+          warp_near_chunks(S.hB, m.gB, xb, [&](uint32_t j, uint32_t, bool valid) {
+            bool keep = false;
+            V2 r_i;
+            float phi = 0.0f;
+            if (valid) {
+              r_i = V2(X[j]) - xb;
+              float r2 = r_i.len2();
+              if (!(!finite_f(r2) || r2 >= h_c * h_c)) {
+                phi = poly6(r2, h_c) / w_hc0;
+                keep = phi > 0.0f;
+              }
+            }
+            const uint32_t bal = __ballot_sync(FULL, keep);
+            const uint32_t pos = cnt + __popc(bal & ((1u << lane) - 1u));
+            if (keep && pos < m.cap_items) {
+              m.item_j[base + pos] = j;
+              m.item_v[base + pos] = r_i.f2();
+              m.item_w[base + pos] = phi;
+            }
+            cnt += __popc(bal);
           });
         }
-        if (overflow) atomicOr(err, ERR_ITEMS);
-        m.item_n[b] = cnt;
-        atomicAdd(&out.ctr.n_coupling_items, cnt);
+        if (cnt > m.cap_items) { if (lane == 0) atomicOr(err, ERR_ITEMS); cnt = 0; }
+        if (lane == 0) { m.item_n[b] = cnt; atomicAdd(&out.ctr.n_coupling_items, cnt); }
+        __syncwarp();
       }
       __syncthreads();
       if (*err) return;
-      if (tid() == 0) {
-        const float i_b = m.b_I;
+      stage_mark(out.stage, 24);
+      const uint32_t nrec = pack_ball_items(m.item_j, m.item_n, m.cap_items, nb, m.rec_off, m.rec_i, m.rec_b);
+      ball_item_preds(m.rec_i, m.rec_b, nrec, n, m.bk_start, m.bk_cur, m.bk_order, m.rec_pred);
+      stage_mark(out.stage, 25);
+      const float i_b = m.b_I;
+      const bool want_mom = U.want_momentum != 0;
+      // Lane l holds item l of the ball (items from 32 on are read from the lists when needed).
+      struct DragBall {
+        uint32_t cnt, j;
+        V2 r_i;
+        float phi, m_ent, i_ent, s_acc, s_scale;
+        V2 r_bar, p_bar, vb;
+        float omb;
+        V2 dv_b, dv_i;
+        float dw_b;
+        bool live;
+      };
+      auto item_r = [&](const DragBall& q, uint32_t base, uint32_t s) { return s < 32 ? q.r_i : V2(m.item_v[base + s]); };
+      auto item_phi = [&](const DragBall& q, uint32_t base, uint32_t s) { return s < 32 ? q.phi : m.item_w[base + s]; };
+      auto item_j = [&](const DragBall& q, uint32_t base, uint32_t s) { return s < 32 ? q.j : m.item_j[base + s]; };
+      ball_dataflow(
+          nb, m.rec_off, m.rec_pred, done, U.sweep_warps, U.spin_ns, err, &out.stage[32],
+          // before the wait: entrained mass, centroid, inertia and the s-gate sums (pbf.rs:1845-1905)
+          // read only the item geometry, which the sweep does not change
+          [&](uint32_t b, int lane) {
+            DragBall q;
+            q.cnt = m.item_n[b];
+            q.live = false;
+            q.j = 0;
+            q.phi = 0.0f;
+            if (q.cnt == 0) return q;
+            const uint32_t base = b * m.cap_items, cnt = q.cnt;
+            if ((uint32_t)lane < cnt) {
+              q.j = m.item_j[base + lane];
+              q.r_i = V2(m.item_v[base + lane]);
+              q.phi = m.item_w[base + lane];
+            }
+            q.vb = V2(m.bv[b]);
+            q.omb = m.bom[b];
+            float m_ent = 0.0f, i_ent = 0.0f, rsx = 0.0f, rsy = 0.0f;
+            for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+              const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
+              float w = 0.0f, r2w = 0.0f;
+              V2 rw;
+              if (s < cnt) {
+                V2 r_i = item_r(q, base, s);
+                w = mass * item_phi(q, base, s);
+                rw = w * r_i;
+                r2w = w * r_i.len2();
+              }
+#pragma unroll
+              for (uint32_t t = 0; t < 32; ++t) {
+                if (t < lim) {
+                  m_ent += __shfl_sync(FULL, w, t);
+                  rsx += __shfl_sync(FULL, rw.x, t);
+                  rsy += __shfl_sync(FULL, rw.y, t);
+                  i_ent += __shfl_sync(FULL, r2w, t);
+                }
+              }
+            }
+            q.m_ent = m_ent;
+            q.i_ent = i_ent;
+            if (m_ent <= 1e-12f) return q;
+            q.live = true;
+            q.r_bar = V2(rsx, rsy) / m_ent;
+            q.s_acc = 0.0f;
+            q.s_scale = 0.0f;
+            if (i_ent > 1e-12f) {
+              q.p_bar = V2(-q.r_bar.y, q.r_bar.x);
+              float s_acc = 0.0f, s_scale = 0.0f;
+              for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+                const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
+                float sv = 0.0f, ss = 0.0f;
+                if (s < cnt) {
+                  V2 r_i = item_r(q, base, s);
+                  float phi = item_phi(q, base, s);
+                  V2 perp_i(-r_i.y, r_i.x);
+                  float phi2 = phi * phi;
+                  sv = mass * phi2 * cross2(r_i, perp_i - q.p_bar);
+                  ss = mass * phi2 * r_i.len2();
+                }
+#pragma unroll
+                for (uint32_t t = 0; t < 32; ++t) {
+                  if (t < lim) {
+                    s_acc += __shfl_sync(FULL, sv, t);
+                    s_scale += __shfl_sync(FULL, ss, t);
+                  }
+                }
+              }
+              q.s_acc = s_acc;
+              q.s_scale = s_scale;
+            }
+            return q;
+          },
+          // on the chain: entrained velocity and angular momentum, the relaxation, the fluid updates
+          [&](uint32_t b, int lane, DragBall& q) {
+            if (!q.live) return;
+            const uint32_t base = b * m.cap_items, cnt = q.cnt;
+            float l_sum = 0.0f, vsx = 0.0f, vsy = 0.0f;
+            for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+              const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
+              float lw = 0.0f;
+              V2 vw;
+              if (s < cnt) {
+                V2 r_i = item_r(q, base, s);
+                V2 vj(V[item_j(q, base, s)]);
+                float w = mass * item_phi(q, base, s);
+                vw = w * vj;
+                lw = w * cross2(r_i, vj);
+              }
+#pragma unroll
+              for (uint32_t t = 0; t < 32; ++t) {
+                if (t < lim) {
+                  vsx += __shfl_sync(FULL, vw.x, t);
+                  vsy += __shfl_sync(FULL, vw.y, t);
+                  l_sum += __shfl_sync(FULL, lw, t);
+                }
+              }
+            }
+            const float m_ent = q.m_ent, i_ent = q.i_ent;
+            V2 v_bar = V2(vsx, vsy) / m_ent;
+            V2 v_rel = v_bar - q.vb;
+            float speed_rel = v_rel.len();
+            float inv_tau_form = (speed_rel > 1e-6f && rho0 > 0.0f)
+                                     ? 0.5f * rho0 * 1.0f * (2.0f * m.b_rtrue) * speed_rel / mass_true
+                                     : 0.0f;
+            float bt = beta_b * (1.0f - expf_r(-dt * (0.0f + inv_tau_form)));
+            float a_lin = bt * m_ent / (m.b_m + m_ent);
+            V2 dv_b = a_lin * v_rel;
+            float dw_b = 0.0f, c_rot = 0.0f;
+            if (i_ent > 1e-12f) {
+              float omega_bar = l_sum / i_ent;
+              float a_rot = bt * i_ent / (i_b + i_ent);
+              float candidate_dw = a_rot * (omega_bar - q.omb);
+              if (fabsf(q.s_acc) > 0.1f * q.s_scale) {
+                float raw_c_rot = -i_b * candidate_dw / q.s_acc;
+                float max_lever = 2.0f * h_c;
+                float cap = max_lever > 1e-9f ? rot_cap / max_lever : 0.0f;
+                c_rot = clamp_r(raw_c_rot, -cap, cap);
+                dw_b = -c_rot * q.s_acc / i_b;
+              }
+            }
+            for (uint32_t s = lane; s < cnt; s += 32) {
+              const uint32_t j = item_j(q, base, s);
+              V2 r_i = item_r(q, base, s);
+              float phi = item_phi(q, base, s);
+              V2 dv_i = -(m.b_m / m_ent) * dv_b * phi;
+              if (c_rot != 0.0f) {
+                V2 perp_i(-r_i.y, r_i.x);
+                dv_i += c_rot * phi * (perp_i - q.p_bar);
+              }
+              V[j] = (V2(V[j]) + dv_i).f2();
+              if (s < 32) q.dv_i = dv_i;
+              else if (want_mom) m.rec_M[m.rec_off[b] + s] = (mass * dv_i).f2();
+            }
+            q.dv_b = dv_b;
+            q.dw_b = dw_b;
+          },
+          // after the flag: the ball's impulse and angular impulse, the momentum records
+          [&](uint32_t b, int lane, DragBall& q) {
+            if (!q.live) return;
+            if (want_mom && (uint32_t)lane < q.cnt) m.rec_M[m.rec_off[b] + lane] = (mass * q.dv_i).f2();
+            if (lane == 0) {
+              m.imp[b] = (V2(m.imp[b]) + m.b_m * q.dv_b).f2();
+              m.ang[b] += i_b * q.dw_b + m.b_m * cross2(q.r_bar, q.dv_b);
+              m.item_n[b] = q.cnt | 0x80000000u;  // mark: contributed fluid momentum records
+            }
+          });
+      if (tid() == 0 && U.want_momentum) {
         V2 mom(S.fscal[0], S.fscal[1]);
         for (uint32_t b = 0; b < nb; ++b) {
-          uint32_t base = b * m.cap_items, cnt = m.item_n[b];
-          if (cnt == 0) continue;
-          float m_ent = 0.0f, i_ent = 0.0f, l_sum = 0.0f;
-          V2 r_sum, v_sum;
-          for (uint32_t s = 0; s < cnt; ++s) {
-            uint32_t j = m.item_j[base + s];
-            V2 r_i(m.item_v[base + s]);
-            float phi = m.item_w[base + s];
-            float r2 = r_i.len2();
-            float w = mass * phi;
-            V2 vj(V[j]);
-            m_ent += w;
-            r_sum += w * r_i;
-            v_sum += w * vj;
-            i_ent += w * r2;
-            l_sum += w * cross2(r_i, vj);
-          }
-          if (m_ent <= 1e-12f) continue;
-          V2 r_bar = r_sum / m_ent;
-          V2 v_bar = v_sum / m_ent;
-          V2 v_rel = v_bar - V2(m.bv[b]);
-          float speed_rel = v_rel.len();
-          float inv_tau_form = (speed_rel > 1e-6f && rho0 > 0.0f)
-                                   ? 0.5f * rho0 * 1.0f * (2.0f * m.b_rtrue) * speed_rel / mass_true
-                                   : 0.0f;
-          float bt = beta_b * (1.0f - expf_r(-dt * (0.0f + inv_tau_form)));
-          float a_lin = bt * m_ent / (m.b_m + m_ent);
-          V2 dv_b = a_lin * v_rel;
-          float dw_b = 0.0f, c_rot = 0.0f;
-          V2 p_bar;
-          if (i_ent > 1e-12f) {
-            float omega_bar = l_sum / i_ent;
-            float a_rot = bt * i_ent / (i_b + i_ent);
-            float candidate_dw = a_rot * (omega_bar - m.bom[b]);
-            p_bar = V2(-r_bar.y, r_bar.x);
-            float s = 0.0f, s_scale = 0.0f;
-            for (uint32_t q = 0; q < cnt; ++q) {
-              V2 r_i(m.item_v[base + q]);
-              float phi = m.item_w[base + q];
-              V2 perp_i(-r_i.y, r_i.x);
-              float phi2 = phi * phi;
-              s += mass * phi2 * cross2(r_i, perp_i - p_bar);
-              s_scale += mass * phi2 * r_i.len2();
-            }
-            if (fabsf(s) > 0.1f * s_scale) {
-              float raw_c_rot = -i_b * candidate_dw / s;
-              float max_lever = 2.0f * h_c;
-              float cap = max_lever > 1e-9f ? rot_cap / max_lever : 0.0f;
-              c_rot = clamp_r(raw_c_rot, -cap, cap);
-              dw_b = -c_rot * s / i_b;
-            }
-          }
-          for (uint32_t q = 0; q < cnt; ++q) {
-            uint32_t j = m.item_j[base + q];
-            V2 r_i(m.item_v[base + q]);
-            float phi = m.item_w[base + q];
-            V2 dv_i = -(m.b_m / m_ent) * dv_b * phi;
-            if (c_rot != 0.0f) {
-              V2 perp_i(-r_i.y, r_i.x);
-              dv_i += c_rot * phi * (perp_i - p_bar);
-            }
-            V[j] = (V2(V[j]) + dv_i).f2();
-            mom += mass * dv_i;
-          }
-          m.imp[b] = (V2(m.imp[b]) + m.b_m * dv_b).f2();
-          m.ang[b] += i_b * dw_b + m.b_m * cross2(r_bar, dv_b);
+          if (!(m.item_n[b] & 0x80000000u)) continue;
+          for (uint32_t r = m.rec_off[b]; r < m.rec_off[b + 1]; ++r) mom += V2(m.rec_M[r]);
         }
         S.fscal[0] = mom.x;
         S.fscal[1] = mom.y;
       }
       __syncthreads();
+      stage_mark(out.stage, 26);
     }
   }
+  stage_mark(out.stage, 19);
   double ke_after_drag = kinetic_energy_seq(V, n, mass, S);
   const double ke_delta_drag = ke_after_drag - ke_mark;
   ke_mark = ke_after_drag;
   // ---- step 6.6: buoyancy, Gauss-Seidel over balls on the stale step-2 grid (pbf.rs:2035-2122)
   if (nb > 0 && m.b_r > 0.0f) {
     const float area = PI_F * m.b_r * m.b_r;
-    for (uint32_t b = tid(); b < nb; b += nthr()) {
-      uint32_t base = b * m.cap_items, cnt = 0;
-      bool overflow = false;
-      V2 xb(m.bx[b]);
+    for (uint32_t b = tid() >> 5; b < nb; b += nthr() >> 5) {
+      const uint32_t lane = tid() & 31u, base = b * m.cap_items;
+      uint32_t cnt = 0;
+      const V2 xb(m.bx[b]);
       float rho_local = 0.0f;
       if (xb.finite()) {
-        for_each_near(S.hA, m.gA, xb, [&](uint32_t j) {
-          float r2 = (xb - V2(X[j])).len2();
-          float w = mass * poly6(r2, h);
-          if (w > 0.0f) {
-            rho_local += w;
-            if (cnt >= m.cap_items) { overflow = true; return; }
-            m.item_j[base + cnt] = j;
-            m.item_w[base + cnt] = w;
-            ++cnt;
-          }
+        warp_near_chunks(S.hA, m.gA, xb, [&](uint32_t j, uint32_t, bool valid) {
+          float w = 0.0f;
+          if (valid) w = mass * poly6((xb - V2(X[j])).len2(), h);
+          const bool keep = w > 0.0f;
+          const uint32_t bal = __ballot_sync(FULL, keep);
+          const uint32_t pos = cnt + __popc(bal & ((1u << lane) - 1u));
+          if (keep && pos < m.cap_items) { m.item_j[base + pos] = j; m.item_w[base + pos] = w; }
+          for (uint32_t mk = bal; mk; mk &= mk - 1u) rho_local += __shfl_sync(FULL, w, __ffs(mk) - 1);
+          cnt += __popc(bal);
         });
       }
-      if (overflow) atomicOr(err, ERR_ITEMS);
-      m.item_n[b] = rho_local > 0.0f ? cnt : 0u;
-      if (rho_local > 0.0f) atomicAdd(&out.ctr.n_coupling_items, cnt);
-      m.item_v[base] = make_float2(rho_local, 0.0f);
+      if (cnt > m.cap_items) { if (lane == 0) atomicOr(err, ERR_ITEMS); cnt = 0; }
+      if (lane == 0) {
+        m.item_n[b] = rho_local > 0.0f ? cnt : 0u;
+        if (rho_local > 0.0f) atomicAdd(&out.ctr.n_coupling_items, cnt);
+        m.item_v[base] = make_float2(rho_local, 0.0f);
+      }
+      __syncwarp();
     }
     __syncthreads();
     if (*err) return;
-    if (tid() == 0) {
+    stage_mark(out.stage, 27);
+    const uint32_t nrec = pack_ball_items(m.item_j, m.item_n, m.cap_items, nb, m.rec_off, m.rec_i, m.rec_b);
+    ball_item_preds(m.rec_i, m.rec_b, nrec, n, m.bk_start, m.bk_cur, m.bk_order, m.rec_pred);
+    stage_mark(out.stage, 28);
+    const float om_abs = fabsf(U.drum_omega);
+    const bool want_mom = U.want_momentum != 0;
+    // Lane l holds item l of the ball (items from 32 on are read from the lists when needed).
+    struct BuoyBall {
+      uint32_t cnt, j;
+      float w, rho_local, d2, den;
+      V2 d, xb, impulse, dv;
+      bool valid;
+    };
+    ball_dataflow(
+        nb, m.rec_off, m.rec_pred, done, U.sweep_warps, U.spin_ns, err, &out.stage[35],
+        // before the wait: item geometry and the weight sum, which the sweep does not change
+        [&](uint32_t b, int lane) {
+          BuoyBall q;
+          q.cnt = m.item_n[b];
+          q.j = 0;
+          q.w = 0.0f;
+          q.valid = false;
+          if (q.cnt == 0) return q;
+          const uint32_t base = b * m.cap_items, cnt = q.cnt;
+          q.rho_local = m.item_v[base].x;
+          q.xb = V2(m.bx[b]);
+          if ((uint32_t)lane < cnt) {
+            q.j = m.item_j[base + lane];
+            q.w = m.item_w[base + lane];
+            q.d = V2(X[q.j]);
+            q.d2 = q.d.len2();
+            q.valid = !(q.d2 <= 1e-12f);
+          }
+          float den = 0.0f;
+          for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+            const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
+            bool valid = false;
+            float dvw = 0.0f;
+            if (s < cnt) {
+              if (s < 32) {
+                valid = q.valid;
+                dvw = q.w;
+              } else {
+                float d2 = V2(X[m.item_j[base + s]]).len2();
+                valid = !(d2 <= 1e-12f);
+                dvw = m.item_w[base + s];
+              }
+            }
+            const uint32_t vmask = __ballot_sync(FULL, valid);
+#pragma unroll
+            for (uint32_t t = 0; t < 32; ++t) {
+              if (t < lim) {
+                float c = __shfl_sync(FULL, dvw, t);
+                if ((vmask >> t) & 1u) den += c;
+              }
+            }
+          }
+          q.den = den;
+          return q;
+        },
+        // on the chain: the local rotation rate from the current velocities, the fluid updates
+        [&](uint32_t b, int lane, BuoyBall& q) {
+          if (q.cnt == 0) return;
+          const uint32_t base = b * m.cap_items, cnt = q.cnt;
+          const float rho_local = q.rho_local;
+          const float rho_eff = fmin_r(rho_local, rho0);
+          float num = 0.0f;
+          for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+            const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
+            float nv = 0.0f;
+            bool valid = false;
+            if (s < cnt) {
+              if (s < 32) {
+                valid = q.valid;
+                nv = q.w * cross2(q.d, V2(V[q.j])) / q.d2;
+              } else {
+                uint32_t j = m.item_j[base + s];
+                V2 d(X[j]);
+                float d2 = d.len2();
+                valid = !(d2 <= 1e-12f);
+                nv = m.item_w[base + s] * cross2(d, V2(V[j])) / d2;
+              }
+            }
+            const uint32_t vmask = __ballot_sync(FULL, valid);
+#pragma unroll
+            for (uint32_t t = 0; t < 32; ++t) {
+              if (t < lim) {
+                float a = __shfl_sync(FULL, nv, t);
+                if ((vmask >> t) & 1u) num += a;
+              }
+            }
+          }
+          const float den = q.den;
+          float omega_local = den > 0.0f ? clamp_r(num / den, -om_abs, om_abs) : 0.0f;
+          V2 g_eff = V2(0.0f, GRAVITY) + omega_local * omega_local * q.xb;
+          V2 impulse = -rho_eff * area * g_eff * dt;
+          for (uint32_t s = lane; s < cnt; s += 32) {
+            const uint32_t j = s < 32 ? q.j : m.item_j[base + s];
+            float frac = (s < 32 ? q.w : m.item_w[base + s]) / rho_local;
+            V2 dv = -(impulse * frac) / mass;
+            V[j] = (V2(V[j]) + dv).f2();
+            if (s < 32) q.dv = dv;
+            else if (want_mom) m.rec_M[m.rec_off[b] + s] = (mass * dv).f2();
+          }
+          q.impulse = impulse;
+        },
+        // after the flag: the ball's impulse, the momentum records
+        [&](uint32_t b, int lane, BuoyBall& q) {
+          if (q.cnt == 0) return;
+          if (want_mom && (uint32_t)lane < q.cnt) m.rec_M[m.rec_off[b] + lane] = (mass * q.dv).f2();
+          if (lane == 0) m.imp[b] = (V2(m.imp[b]) + q.impulse).f2();
+        });
+    if (tid() == 0 && U.want_momentum) {
       V2 mom(S.fscal[0], S.fscal[1]);
-      const float om_abs = fabsf(U.drum_omega);
-      for (uint32_t b = 0; b < nb; ++b) {
-        uint32_t base = b * m.cap_items, cnt = m.item_n[b];
-        if (cnt == 0) continue;
-        float rho_local = m.item_v[base].x;
-        float rho_eff = fmin_r(rho_local, rho0);
-        float num = 0.0f, den = 0.0f;
-        for (uint32_t s = 0; s < cnt; ++s) {
-          uint32_t j = m.item_j[base + s];
-          V2 d(X[j]);
-          float d2 = d.len2();
-          if (d2 <= 1e-12f) continue;
-          float w = m.item_w[base + s];
-          num += w * cross2(d, V2(V[j])) / d2;
-          den += w;
-        }
-        float omega_local = den > 0.0f ? clamp_r(num / den, -om_abs, om_abs) : 0.0f;
-        V2 xb(m.bx[b]);
-        V2 g_eff = V2(0.0f, GRAVITY) + omega_local * omega_local * xb;
-        V2 impulse = -rho_eff * area * g_eff * dt;
-        m.imp[b] = (V2(m.imp[b]) + impulse).f2();
-        for (uint32_t s = 0; s < cnt; ++s) {
-          uint32_t j = m.item_j[base + s];
-          float frac = m.item_w[base + s] / rho_local;
-          V2 dv = -(impulse * frac) / mass;
-          V[j] = (V2(V[j]) + dv).f2();
-          mom += mass * dv;
-        }
-      }
+      for (uint32_t r = 0; r < nrec; ++r) mom += V2(m.rec_M[r]);
       S.fscal[0] = mom.x;
       S.fscal[1] = mom.y;
     }
     __syncthreads();
+    stage_mark(out.stage, 29);
   }
   double ke_after_buoy = kinetic_energy_seq(V, n, mass, S);
   const double ke_delta_buoy = ke_after_buoy - ke_mark;
   ke_mark = ke_after_buoy;
+  if (V != Vg) {
+    for (uint32_t i = tid(); i < n; i += nthr()) Vg[i] = V[i];
+    V = Vg;
+    X = Xg;
+    __syncthreads();
+  }
+  stage_mark(out.stage, 6);
   // ---- density recompute at final x over the step-2 lists (pbf.rs:2137-2144)
   for (uint32_t i = tid(); i < n; i += nthr()) {
     V2 xi(X[i]);
@@ -744,6 +1030,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
     m.density[i] = rho;
   }
   __syncthreads();
+  stage_mark(out.stage, 7);
   // ---- step 7: implicit viscosity (pbf.rs:2146-2300)
   uint32_t visc_iters = 0;
   const bool fp64 = U.cg_fp64 != 0;
@@ -795,6 +1082,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       }
     }
     __syncthreads();
+    stage_mark(out.stage, 8);
     // boundary groups (pbf.rs:2159-2232) on a fresh h-grid, one ball per thread, merged per fluid
     if (tid() == 0) { S.n_groups = 0; S.n_links = 0; S.links_in_range = 0; }
     __syncthreads();
@@ -805,44 +1093,47 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       for (uint32_t j = tid(); j < n; j += nthr())
         m.f_tmp[j] = BALL_BC_GAIN * (mass * 2.0f * m.mu_eff[j] / (fmax_r(m.density[j], 1e-6f) * rho0));
       __syncthreads();
-      for (uint32_t b = tid(); b < nb; b += nthr()) {
-        uint32_t base = b * m.cap_items, cnt = 0;
+      // one warp per ball, candidates merged per fluid particle in first-seen order
+      uint32_t* slot = m.slot + (size_t)(tid() >> 5) * m.cap_nf;
+      for (uint32_t b = tid() >> 5; b < nb; b += nthr() >> 5) {
+        const uint32_t lane = tid() & 31u, base = b * m.cap_items;
+        const MergeList L{m.item_j + base, m.item_w + base, m.item_v + base, m.item_w2 + base, m.cap_items};
+        uint32_t cnt = 0;
         bool overflow = false;
-        V2 xb(m.bx[b]);
+        const V2 xb(m.bx[b]);
         if (xb.finite()) {
           for (uint32_t q = 0; q < count_pb; ++q) {
-            V2 bp = xb + U.boundary_offset[q];
-            for_each_near(S.hB, m.gB, bp, [&](uint32_t j) {
-              V2 delta = V2(X[j]) - bp;
-              float r2 = delta.len2();
-              if (r2 >= range2) return;
-              float r = sqrtf(r2);
-              if (!finite_f(r) || r >= h || r <= 1e-9f) return;
-              float dot_abs = fabsf(spiky_norm * (h - r) * (h - r) * r);
-              float c = m.f_tmp[j] * dot_abs / (r2 + eta2);
-              if (!(c > 0.0f)) return;
-              V2 lever = bp - xb;
-              V2 lever_c = c * lever;
-              float lever2_c = c * lever.len2();
-              uint32_t s = 0;
-              while (s < cnt && m.item_j[base + s] != j) ++s;
-              if (s == cnt) {
-                if (cnt >= m.cap_items) { overflow = true; return; }
-                m.item_j[base + s] = j;
-                m.item_w[base + s] = c;
-                m.item_v[base + s] = lever_c.f2();
-                m.item_w2[base + s] = lever2_c;
-                ++cnt;
-              } else {
-                m.item_w[base + s] += c;
-                m.item_v[base + s] = (V2(m.item_v[base + s]) + lever_c).f2();
-                m.item_w2[base + s] += lever2_c;
+            const V2 bp = xb + U.boundary_offset[q];
+            warp_near_chunks(S.hB, m.gB, bp, [&](uint32_t j, uint32_t, bool valid) {
+              bool acc = false;
+              float c = 0.0f, lever2_c = 0.0f;
+              V2 lever_c;
+              if (valid) {
+                V2 delta = V2(X[j]) - bp;
+                float r2 = delta.len2();
+                if (!(r2 >= range2)) {
+                  float r = sqrtf(r2);
+                  if (!(!finite_f(r) || r >= h || r <= 1e-9f)) {
+                    float dot_abs = fabsf(spiky_norm * (h - r) * (h - r) * r);
+                    c = m.f_tmp[j] * dot_abs / (r2 + eta2);
+                    if (c > 0.0f) {
+                      acc = true;
+                      V2 lever = bp - xb;
+                      lever_c = c * lever;
+                      lever2_c = c * lever.len2();
+                    }
+                  }
+                }
               }
+              warp_merge(acc, j, c, lever_c, lever2_c, slot, L, cnt, overflow);
             });
           }
         }
-        if (overflow) atomicOr(err, ERR_ITEMS);
-        m.g_off[b] = cnt;
+        for (uint32_t s = lane; s < min(cnt, m.cap_items); s += 32) slot[L.j[s]] = NONE;
+        __syncwarp();
+        if (__any_sync(FULL, overflow)) { if (lane == 0) atomicOr(err, ERR_ITEMS); cnt = 0; }
+        if (lane == 0) m.g_off[b] = cnt;
+        __syncwarp();
       }
       if (tid() == 0) m.g_off[nb] = 0;
       __syncthreads();
@@ -862,6 +1153,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       if (tid() == 0) S.n_groups = ng;
       __syncthreads();
     }
+    stage_mark(out.stage, 9);
     // ball_v0 (pbf.rs:2237-2239) and squeeze links (pbf.rs:544-625)
     for (uint32_t b = tid(); b < nb; b += nthr()) {
       m.ball_v0[b] = (V2(m.bv[b]) + V2(m.imp[b]) / m.b_m).f2();
@@ -876,27 +1168,41 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       const float range2 = (2.0f * r + reach) * (2.0f * r + reach) * (1.0f + 1e-4f);
       grid_build(m.bx, nb, 2.0f * r + reach, m.gBall, S.hBall, err);
       uint32_t in_range = 0;
+      // one warp per ball: candidates j > i in for_each_near order, ordered compaction, then the
+      // wall link; pass 0 counts, pass 1 evaluates the films and writes
       for (int pass = 0; pass < 2; ++pass) {
-        for (uint32_t i = tid(); i < nb; i += nthr()) {
-          V2 xi(m.bx[i]);
-          uint32_t c = 0, o = pass ? m.l_off[i] : 0u;
+        for (uint32_t i = tid() >> 5; i < nb; i += nthr() >> 5) {
+          const uint32_t lane = tid() & 31u;
+          const V2 xi(m.bx[i]);
+          uint32_t c = 0, inr = 0;
+          const uint32_t o = pass ? m.l_off[i] : 0u;
           if (xi.finite()) {
-            for_each_near(S.hBall, m.gBall, xi, [&](uint32_t j) {
-              if (j <= i) return;
-              LinkEval L = link_pair(m, U, i, j, reach, range2, dxd, c_max);
-              if (!pass && L.in_range) in_range += 1;
-              if (!L.emit) return;
-              if (pass) { m.l_ball[o] = i; m.l_other[o] = j; m.l_n[o] = L.n.f2(); m.l_c[o] = L.c; ++o; }
-              ++c;
+            warp_near_chunks(S.hBall, m.gBall, xi, [&](uint32_t j, uint32_t, bool valid) {
+              const bool cand = valid && j > i;
+              LinkEval L{false, false, V2(), 0.0f};
+              if (cand) L = link_pair(m, U, i, j, reach, range2, dxd, c_max, pass == 1);
+              inr += __popc(__ballot_sync(FULL, cand && L.in_range));
+              const uint32_t bal = __ballot_sync(FULL, cand && L.emit);
+              if (pass && cand && L.emit) {
+                const uint32_t q = o + c + __popc(bal & ((1u << lane) - 1u));
+                m.l_ball[q] = i; m.l_other[q] = j; m.l_n[q] = L.n.f2(); m.l_c[q] = L.c;
+              }
+              c += __popc(bal);
             });
-            LinkEval W = link_wall(m, U, i, reach, dxd, c_max);
-            if (!pass && W.in_range) in_range += 1;
-            if (W.emit) {
-              if (pass) { m.l_ball[o] = i; m.l_other[o] = NONE; m.l_n[o] = W.n.f2(); m.l_c[o] = W.c; ++o; }
-              ++c;
+            if (lane == 0) {
+              LinkEval W = link_wall(m, U, i, reach, dxd, c_max);
+              if (W.in_range) inr += 1;
+              if (W.emit) {
+                if (pass) { m.l_ball[o + c] = i; m.l_other[o + c] = NONE; m.l_n[o + c] = W.n.f2(); m.l_c[o + c] = W.c; }
+                ++c;
+              }
             }
           }
-          if (!pass) m.l_off[i] = c;
+          if (lane == 0 && !pass) {
+            m.l_off[i] = c;
+            in_range += inr;
+          }
+          __syncwarp();
         }
         if (!pass) {
           if (tid() == 0) m.l_off[nb] = 0;
@@ -915,6 +1221,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       out.ctr.links_in_range = S.links_in_range;
     }
     __syncthreads();
+    stage_mark(out.stage, 10);
     if (S.n_groups == 0 && S.links_in_range == 0) {
       // ---- fluid-only CG (pbf.rs:423-480), solution in place in V
       float2 *r = m.cg_r, *p = m.cg_p, *ap = m.cg_ap;
@@ -1058,6 +1365,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       __syncthreads();
     }
   }
+  stage_mark(out.stage, 11);
   // ---- mean shear rate (pbf.rs:800-849) on the final velocities
   for (uint32_t i = tid(); i < n; i += nthr()) {
     V2 xi(X[i]), vi(V[i]);
@@ -1078,16 +1386,18 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
     m.f_tmp[i] = sqrtf(2.0f * (gxx * gxx + gyy * gyy + 2.0f * dxy * dxy));
   }
   __syncthreads();
-  if (tid() == 0) {
-    float s = 0.0f;
+  if (tid() < 32) {
     uint32_t c = 0;
-    for (uint32_t i = 0; i < n; ++i) {
-      float g = m.f_tmp[i];
-      if (finite_f(g)) { s += g; c += 1; }
-    }
-    out.fs.mean_shear_rate_per_s = c == 0 ? 0.0f : s / (float)c;
+    float s = warp_ordered_sum(0.0f, n, [&](uint32_t i, float& t) {
+      t = m.f_tmp[i];
+      return finite_f(t);
+    });
+    for (uint32_t i = tid(); i < n; i += 32) c += finite_f(m.f_tmp[i]) ? 1u : 0u;
+    c = warp_sum(c);
+    if (tid() == 0) out.fs.mean_shear_rate_per_s = c == 0 ? 0.0f : s / (float)c;
   }
   __syncthreads();
+  stage_mark(out.stage, 12);
   double ke_after_visc = kinetic_energy_seq(V, n, mass, S);
   const double ke_delta_visc = ke_after_visc - ke_mark;
   // ---- step 7.5: speed clamp (pbf.rs:979-996, 2321)
@@ -1132,6 +1442,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
     out.fluid_momentum[1] = S.fscal[1];
   }
   __syncthreads();
+  stage_mark(out.stage, 13);
 }
 
 }  // namespace mg

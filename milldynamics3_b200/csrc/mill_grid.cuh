@@ -163,6 +163,49 @@ __device__ __forceinline__ void for_each_near(const GridHdr& hdr, const GridBuf&
   }
 }
 
+// Warp-cooperative for_each_near: the candidates of query point p, in for_each_near order, handed
+// out 32 at a time. f(j, pos, valid) is called by every lane of the warp for each chunk, with
+// lane l holding candidate pos = chunk start + l (valid = pos < total); f may use warp collectives.
+template <class F>
+__device__ __forceinline__ void warp_near_chunks(const GridHdr& hdr, const GridBuf& gb, V2 p, F f) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t s = 0, cnt = 0;
+  if (p.finite() && hdr.npoints > 0 && lane < 9) {
+    int2 c = cell_key(p, hdr.cell);
+    int dy = (int)(lane / 3) - 1, dx = (int)(lane % 3) - 1;
+    int2 k = make_int2(sat_add(c.x, dx), sat_add(c.y, dy));
+    bool dup = false;
+    for (uint32_t q = 0; q < lane; ++q) {
+      int qy = (int)(q / 3) - 1, qx = (int)(q % 3) - 1;
+      dup = dup || key_eq(k, make_int2(sat_add(c.x, qx), sat_add(c.y, qy)));
+    }
+    uint32_t e;
+    if (!dup && cell_range(hdr, gb, k, s, e)) cnt = e - s;
+  }
+  // inclusive prefix of the 9 cell sizes
+  uint32_t incl = cnt;
+  for (int o = 1; o < 16; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if ((int)lane >= o) incl += y;
+  }
+  const uint32_t total = __shfl_sync(0xffffffffu, incl, 8);
+  for (uint32_t c0 = 0; c0 < total; c0 += 32) {
+    const uint32_t pos = c0 + lane;
+    uint32_t j = NONE;
+    // cell of position pos: the first cell whose inclusive prefix exceeds pos
+    uint32_t cell = 0, base_prefix = 0, cell_s = 0;
+    for (uint32_t q = 0; q < 9; ++q) {
+      uint32_t inc_q = __shfl_sync(0xffffffffu, incl, q);
+      uint32_t cnt_q = __shfl_sync(0xffffffffu, cnt, q);
+      uint32_t s_q = __shfl_sync(0xffffffffu, s, q);
+      if (pos < inc_q && pos >= inc_q - cnt_q) { cell = q; base_prefix = inc_q - cnt_q; cell_s = s_q; }
+    }
+    (void)cell;
+    if (pos < total) j = gb.indices[cell_s + (pos - base_prefix)];
+    f(j, pos, pos < total);
+  }
+}
+
 // The cells a point's neighbour list visits, in the order build_neighbor_lists (pbf.rs:262-288)
 // produces: the forward-offset sweep of for_each_candidate_pair (grid.rs:291-362) reaches a point
 // in cell C from (-1,-1), (-1,0), (0,-1) before C's own pairs, then C's targets (+1,0), (+1,+1),

@@ -142,6 +142,7 @@ struct MgSim {
   uint64_t launches = 0;
   uint64_t ctr_tot[10] = {};
   uint64_t ctr_n = 0;
+  uint64_t stage_tot[40] = {};
 };
 
 namespace {
@@ -185,7 +186,7 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
   m.cap_groups = cb * m.cap_items;
   // squeeze links: every pair of balls within 2r + 8 dx plus the wall, bounded by nb per ball
   m.cap_links = cb * std::min<uint32_t>(cb + 1u, 512u) + 1024u;
-  m.cap_recs = std::max({8u * cf + 1024u, m.cap_groups, m.cap_links});
+  m.cap_recs = std::max({8u * cf + 1024u, m.cap_groups, m.cap_links, 2u * m.cap_pairs + cb + 64u});
   m.cap_impacts = 4u * cb + 256u;
   const uint32_t fcells = 2u * cf + 513u, bcells = 2u * cb + 513u;
   const uint32_t nbig = std::max(cf, cb) + 2u;
@@ -224,7 +225,15 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
     m.item_w = a.take<float>(items); m.item_w2 = a.take<float>(items);
     m.item_n = a.take<uint32_t>(cb + 1);
     m.bk_start = a.take<uint32_t>(nbig); m.bk_cur = a.take<uint32_t>(nbig);
-    m.bk_order = a.take<uint32_t>(m.cap_pairs);
+    m.bk_order = a.take<uint32_t>(m.cap_recs);
+    const size_t nit = (size_t)m.cap_pairs + cb + 1;
+    m.dm_pa = a.take<uint32_t>(nit); m.dm_pb = a.take<uint32_t>(nit); m.dm_lvl = a.take<uint32_t>(nit);
+    m.lev_start = a.take<uint32_t>(nit + 1); m.lev_cur = a.take<uint32_t>(nit + 1);
+    m.lev_items = a.take<uint32_t>(nit);
+    m.act_i = a.take<uint32_t>(nit); m.act_j = a.take<uint32_t>(nit); m.act_flag = a.take<uint32_t>(nit + 1);
+    m.act_l = a.take<float>(nit); m.act_w1 = a.take<float>(nit); m.act_w2 = a.take<float>(nit);
+    m.act_bin = a.take<int32_t>(nit);
+    m.act_rec = a.take<MgImpactRecord>(nit);
     m.g_fluid = a.take<uint32_t>(m.cap_groups); m.g_ball = a.take<uint32_t>(m.cap_groups);
     m.g_c = a.take<float>(m.cap_groups); m.g_l2 = a.take<float>(m.cap_groups); m.g_lc = a.take<float2>(m.cap_groups);
     m.g_off = a.take<uint32_t>(cb + 1);
@@ -241,6 +250,9 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
     m.bx0 = a.take<float2>(cb); m.bvpre = a.take<float2>(cb);
     m.bth0 = a.take<float>(cb); m.bompre = a.take<float>(cb); m.lam_bw = a.take<float>(cb);
     m.lam_tot = a.take<float>(cb); m.f_cw = a.take<double>(cb);
+    m.rec_off = a.take<uint32_t>(cb + 1); m.rec_pred = a.take<uint32_t>(m.cap_recs);
+    m.ball_done = a.take<uint32_t>(cb);
+    m.slot = a.take<uint32_t>((size_t)16 * cf);
     m.pair_i = a.take<uint32_t>(m.cap_pairs); m.pair_j = a.take<uint32_t>(m.cap_pairs);
     m.lam_bb = a.take<float>(m.cap_pairs);
     m.cs_i = a.take<uint32_t>(m.cap_pairs); m.cs_j = a.take<uint32_t>(m.cap_pairs); m.cs_l = a.take<float>(m.cap_pairs);
@@ -254,6 +266,8 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
       cudaMemsetAsync(s->dmem, 0, s->dbytes, s->stream);
     }
   }
+  // the merge slot maps are kept all-NONE between uses
+  cudaMemsetAsync(m.slot, 0xFF, sizeof(uint32_t) * (size_t)16 * cf, s->stream);
   m.nf = nf;
   m.nb = nb;
   s->md = m;
@@ -276,6 +290,8 @@ int push_desc(MgSim* s) {
   s->md.b_m = s->bmat.mass;
   s->md.b_I = s->bmat.inertia;
   s->md.b_rtrue = s->bmat.true_radius;
+  s->md.smem_bytes = (uint32_t)stage_smem_bytes(s->nf, s->nb);
+  s->md.smem_balls = (size_t)s->nb * 24 <= s->md.smem_bytes ? s->nb : 0u;
   CK(cudaMemcpyAsync(s->d_md, &s->md, sizeof(MillDev), cudaMemcpyHostToDevice, s->stream));
   return MG_OK;
 }
@@ -307,10 +323,12 @@ int fill_uniform(MgSim* s, const MgDrum& drum, const MgMediaParams& media, const
   U.media = media;
   U.slurry = slurry;
   U.cg_fp64 = s->opt.cg_fp64;
+  U.sweep_warps = s->opt.sweep_warps ? s->opt.sweep_warps : DEFAULT_SWEEP_WARPS;
+  U.spin_ns = s->opt.spin_ns ? s->opt.spin_ns : DEFAULT_SPIN_NS;
   // pbf.rs:190-219: boundary points at dx = h / 2 (adhesion and viscosity groups)
   U.boundary_count = 0;
   float br = s->bmat.radius, dx = 0.5f * s->fmat.h;
-  if (s->nb > 0 && br > 0.0f && dx > 0.0f) {
+  if (s->nb > 0 && s->nf > 0 && br > 0.0f && dx > 0.0f) {
     float circumference = mgh::TAU_F * br;
     uint32_t count = std::max(mgh::f2u_sat(std::round(circumference / dx)), 6u);
     if (count > (uint32_t)MAX_BOUNDARY_POINTS)
@@ -360,7 +378,7 @@ int run(MgSim* s, uint32_t n_sub) {
   CK(cudaMemcpyAsync(s->d_ang, s->h_ang, sizeof(SubAngles) * n_sub, cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemsetAsync(s->md.err, 0, sizeof(uint32_t), s->stream));
   CK(cudaEventRecord(s->ev0, s->stream));
-  CK(launch_substeps(s->d_md, 1, s->d_uni, s->d_ang, n_sub, s->opt.block_threads, s->stream));
+  CK(launch_substeps(s->d_md, 1, s->d_uni, s->d_ang, n_sub, s->opt.block_threads, s->md.smem_bytes, s->stream));
   CK(cudaEventRecord(s->ev1, s->stream));
   CK(cudaMemcpyAsync(s->h_out, s->md.out, sizeof(StepOut) * n_sub, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
@@ -369,6 +387,7 @@ int run(MgSim* s, uint32_t n_sub) {
   for (uint32_t k = 0; k < n_sub; ++k) {
     const uint32_t* c = reinterpret_cast<const uint32_t*>(&s->h_out[k].ctr);
     for (int q = 0; q < 10; ++q) s->ctr_tot[q] += c[q];
+    for (int q = 0; q < 40; ++q) s->stage_tot[q] += s->h_out[k].stage[q];
     s->ctr_n += 1;
   }
   uint32_t e = 0;
@@ -653,6 +672,8 @@ int mg_sim_set_options(MgSim* s, const MgOptions* o) {
   if (!s || !o) return fail(s, MG_ERR_ARG, "null argument");
   if (o->block_threads != 0 && (o->block_threads % 32 != 0 || o->block_threads > 512))
     return fail(s, MG_ERR_ARG, "block_threads must be a multiple of 32 in [32, 512]");
+  if (o->sweep_warps > 16) return fail(s, MG_ERR_ARG, "sweep_warps must be in [0, 16]");
+  if (o->spin_ns > 100000) return fail(s, MG_ERR_ARG, "spin_ns must be at most 100000");
   s->opt = *o;
   return MG_OK;
 }
@@ -719,6 +740,7 @@ int mg_fluid_step_coupled(MgSim* s, const MgDrum* drum, float drum_angle, const 
   if (!s || !drum || !slurry) return fail(s, MG_ERR_ARG, "null argument");
   int rc = fill_uniform(s, *drum, s->params.media, *slurry, it, 1, 1, 0, 1);
   if (rc) return rc;
+  s->h_uni->want_momentum = 1;  // CouplingImpulses::fluid_momentum_change is returned here only
   fill_angle(s->h_ang[0], drum_angle, drum->omega, dt);
   rc = run(s, 1);
   if (rc) return rc;
@@ -968,6 +990,13 @@ int mg_counter_totals(MgSim* s, uint64_t* totals10, uint64_t* n_substeps, int re
   if (totals10) std::memcpy(totals10, s->ctr_tot, sizeof(s->ctr_tot));
   if (n_substeps) *n_substeps = s->ctr_n;
   if (reset) { std::memset(s->ctr_tot, 0, sizeof(s->ctr_tot)); s->ctr_n = 0; }
+  return MG_OK;
+}
+
+int mg_stage_cycles(MgSim* s, uint64_t* cycles40, int reset) {
+  if (!s) return fail_global(MG_ERR_ARG, "null handle");
+  if (cycles40) std::memcpy(cycles40, s->stage_tot, sizeof(s->stage_tot));
+  if (reset) std::memset(s->stage_tot, 0, sizeof(s->stage_tot));
   return MG_OK;
 }
 

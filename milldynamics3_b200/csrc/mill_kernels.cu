@@ -13,6 +13,7 @@ __global__ void __launch_bounds__(512) mill_substeps_kernel(const MillDev* __res
   __shared__ MillDev m;
   __shared__ FluidShared fs;
   __shared__ DemShared ds;
+  extern __shared__ __align__(16) unsigned char dsm[];  // staged ball state (24 bytes per ball)
   const uint32_t mill = blockIdx.x;
   if (threadIdx.x == 0) m = mills[mill];
   __syncthreads();
@@ -28,15 +29,18 @@ __global__ void __launch_bounds__(512) mill_substeps_kernel(const MillDev* __res
       U.to_world_next = a.to_world_next;
       U.to_local0 = a.to_local0;
       memset(&out.ctr, 0, sizeof(out.ctr));
+      memset(out.stage, 0, sizeof(out.stage));
+      g_stage_last = clock64();
     }
     __syncthreads();
     if (*m.err) break;
     // Without the fluid half, imp/ang hold the caller's external impulses (DEM-only entry point).
-    if (U.run_fluid) fluid_step(m, U, out, m.err, fs);
+    if (U.run_fluid) fluid_step(m, U, out, m.err, fs, dsm);
     __syncthreads();
     if (*m.err) break;
-    if (U.run_dem) dem_step(m, U, out, m.impacts + (size_t)s * m.cap_impacts, m.err, ds);
+    if (U.run_dem) dem_step(m, U, out, m.impacts + (size_t)s * m.cap_impacts, m.err, ds, dsm);
     __syncthreads();
+    if (threadIdx.x == 0) out.stage[14] = out.stage[15] + out.stage[16] + out.stage[17] + out.stage[18] + out.stage[20] + out.stage[21] + out.stage[22] + out.stage[30];
     if (threadIdx.x == 0) out.err = *m.err;
     __syncthreads();
   }
@@ -72,9 +76,14 @@ __global__ void __launch_bounds__(512) probe_kernel(const MillDev* __restrict__ 
 }
 
 cudaError_t launch_substeps(const MillDev* mills, uint32_t n_mills, StepUniform* uni, const SubAngles* angles,
-                            uint32_t n_sub, uint32_t threads, cudaStream_t stream) {
+                            uint32_t n_sub, uint32_t threads, size_t smem_bytes, cudaStream_t stream) {
   if (threads == 0 || threads > 512) threads = 512;
-  mill_substeps_kernel<<<n_mills, threads, 0, stream>>>(mills, uni, angles, n_sub);
+  if (smem_bytes > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(mill_substeps_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem_bytes);
+    if (e != cudaSuccess) return e;
+  }
+  mill_substeps_kernel<<<n_mills, threads, smem_bytes, stream>>>(mills, uni, angles, n_sub);
   return cudaGetLastError();
 }
 

@@ -7,8 +7,20 @@ namespace mg {
 
 // Runs n_sub coupled sub-steps on each of n_mills mills (one block per mill). uni holds one
 // StepUniform per mill; angles holds n_mills * n_sub SubAngles, mill-major.
+// smem_bytes of dynamic shared memory hold the staged ball state (MillDev::smem_balls * 24 bytes).
 cudaError_t launch_substeps(const MillDev* mills, uint32_t n_mills, StepUniform* uni, const SubAngles* angles,
-                            uint32_t n_sub, uint32_t threads, cudaStream_t stream);
+                            uint32_t n_sub, uint32_t threads, size_t smem_bytes, cudaStream_t stream);
+// Largest dynamic shared-memory allotment of a launch. The region holds, one phase at a time,
+// the fluid positions and velocities plus completion flags of the drag / buoyancy sweeps
+// (16 nf + 4 nb bytes) and the ball state of the DEM sweeps (24 nb bytes); it is sized to the
+// larger of the two so that the rest of the SM's L1 / shared storage stays L1 cache.
+constexpr size_t MAX_STAGE_SMEM = 200 * 1024;
+inline size_t stage_smem_bytes(uint32_t nf, uint32_t nb) {
+  size_t fluid = 16 * (size_t)nf + 4 * (size_t)nb + 64, balls = 24 * (size_t)nb;
+  size_t need = ((fluid > balls ? fluid : balls) + 255) & ~size_t(255);
+  if (need <= MAX_STAGE_SMEM) return need;
+  return balls <= MAX_STAGE_SMEM ? ((balls + 255) & ~size_t(255)) : 0;
+}
 // Grid-stage probe over the descriptor's fx[0..nf): mode 0 grid, 1 candidate pairs, 2 neighbours.
 cudaError_t launch_probe(const MillDev* mill, float cell, int mode, uint32_t* result, cudaStream_t stream);
 

@@ -1,0 +1,344 @@
+// Exact parallel replay of the reference's Gauss-Seidel sweeps.
+//
+// A sweep is a sequence of items; each item touches at most two balls (a ball-ball contact or a
+// ball-wall contact). Executing any two items that share no ball in either order gives the same
+// floating-point results, so the sequential result is reproduced exactly by any schedule that
+// keeps, for every ball, the items touching it in sequence order. pred_a[k] / pred_b[k] name the
+// previous item touching each of item k's balls (NONE when there is none).
+//
+//   * level replay: level(k) = 1 + max(level(preds)); all items of one level are independent and
+//     run in parallel, levels in increasing order (used for the long projection sweeps);
+//   * chunked replay: one warp walks the sequence 32 items at a time and runs, round by round,
+//     the items whose in-chunk predecessors are done (used for the short contact sweeps).
+#pragma once
+
+#include "mill_block.cuh"
+
+namespace mg {
+
+constexpr uint32_t FULL = 0xffffffffu;
+
+// Records r in [0, nrec) name a (ball key[r], item item_of(r)) occurrence, numbered so that
+// records of earlier items come first. Bucket-sorts them by key into nbk buckets (stable) and,
+// for the first nballs buckets, stores for each record the item of the previous record of the
+// same ball into pred_a / pred_b (per slot_of(r)). Buckets from nballs on collect placeholders.
+template <class ItemOf, class SlotOf>
+__device__ void preds_from_records(const uint32_t* key, uint32_t nrec, uint32_t nbk, uint32_t nballs, uint32_t* start,
+                                   uint32_t* cur, uint32_t* order, uint32_t* pred_a, uint32_t* pred_b, ItemOf item_of,
+                                   SlotOf slot_of) {
+  block_bucket_sort(key, nrec, nbk, start, cur, order);
+  for (uint32_t b = tid(); b < nballs; b += nthr()) {
+    uint32_t prev = NONE;
+    for (uint32_t q = start[b]; q < start[b + 1]; ++q) {
+      uint32_t r = order[q];
+      uint32_t it = item_of(r);
+      if (slot_of(r)) pred_b[it] = prev;
+      else pred_a[it] = prev;
+      prev = it;
+    }
+  }
+  __syncthreads();
+}
+
+// Levels of items [0, n) (warp 0; chunks of 32 items, in-chunk propagation by shuffles).
+// Returns the number of levels (block-uniform).
+__device__ uint32_t compute_levels(uint32_t n, const uint32_t* pred_a, const uint32_t* pred_b, uint32_t* lvl) {
+  __shared__ uint32_t nlev;
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    uint32_t maxl = 0;
+    for (uint32_t c = 0; c < n; c += 32) {
+      uint32_t k = c + lane;
+      int base = 0, la = -1, lb = -1;
+      if (k < n) {
+        uint32_t a = pred_a[k], b = pred_b[k];
+        if (a != NONE) { if (a >= c) la = (int)(a - c); else base = max(base, (int)lvl[a] + 1); }
+        if (b != NONE) { if (b >= c) lb = (int)(b - c); else base = max(base, (int)lvl[b] + 1); }
+      }
+      int L = base;
+      for (int round = 0; round < 33; ++round) {
+        int A = __shfl_sync(FULL, L, la < 0 ? lane : la) + 1;
+        int Bv = __shfl_sync(FULL, L, lb < 0 ? lane : lb) + 1;
+        int nl = base;
+        if (la >= 0) nl = max(nl, A);
+        if (lb >= 0) nl = max(nl, Bv);
+        bool changed = nl != L;
+        L = nl;
+        if (!__any_sync(FULL, changed)) break;
+      }
+      if (k < n) { lvl[k] = (uint32_t)L; maxl = max(maxl, (uint32_t)L + 1); }
+      __syncwarp();
+    }
+    for (int o = 16; o > 0; o >>= 1) maxl = max(maxl, __shfl_xor_sync(FULL, maxl, o));
+    if (lane == 0) nlev = maxl;
+  }
+  __syncthreads();
+  uint32_t r = nlev;
+  __syncthreads();
+  return r;
+}
+
+// Groups items by level: lev_start[0..nlev], lev_items[] (order inside a level is irrelevant).
+__device__ void bucket_levels(uint32_t n, const uint32_t* lvl, uint32_t nlev, uint32_t* lev_start, uint32_t* lev_cur,
+                              uint32_t* lev_items) {
+  for (uint32_t l = tid(); l <= nlev; l += nthr()) lev_start[l] = 0;
+  __syncthreads();
+  for (uint32_t k = tid(); k < n; k += nthr()) atomicAdd(&lev_start[lvl[k]], 1u);
+  __syncthreads();
+  block_exclusive_scan(lev_start, nlev + 1);
+  for (uint32_t l = tid(); l < nlev; l += nthr()) lev_cur[l] = lev_start[l];
+  __syncthreads();
+  for (uint32_t k = tid(); k < n; k += nthr()) lev_items[atomicAdd(&lev_cur[lvl[k]], 1u)] = k;
+  __syncthreads();
+}
+
+// Runs exec(q) for every level-ordered position q, level by level, in warp 0; the block waits at
+// the end. Positions [lev_start[l], lev_start[l+1]) form level l.
+template <class Exec>
+__device__ void run_levels(uint32_t nlev, const uint32_t* lev_start, Exec exec) {
+  if (threadIdx.x < 32) {
+    uint32_t s = lev_start[0];
+    for (uint32_t l = 0; l < nlev; ++l) {
+      uint32_t e = lev_start[l + 1];
+      for (uint32_t q = s + threadIdx.x; q < e; q += 32) exec(q);
+      s = e;
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+}
+
+// Chunked in-order replay in warp 0: in each chunk of 32 items, rounds run the items whose
+// in-chunk predecessors are done (earlier chunks are complete). At most 32 rounds per chunk.
+// load(k) fetches item k's descriptor once per chunk (all lanes together); exec(k, desc) runs it.
+template <class Load, class Exec>
+__device__ void run_chunked(uint32_t n, const uint32_t* pred_a, const uint32_t* pred_b, Load load, Exec exec) {
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    for (uint32_t c = 0; c < n; c += 32) {
+      uint32_t k = c + lane;
+      bool active = k < n;
+      int la = -1, lb = -1;
+      decltype(load(0u)) desc{};
+      if (active) {
+        uint32_t a = pred_a[k], b = pred_b[k];
+        if (a != NONE && a >= c) la = (int)(a - c);
+        if (b != NONE && b >= c) lb = (int)(b - c);
+        desc = load(k);
+      }
+      uint32_t done = __ballot_sync(FULL, !active);
+      for (int round = 0; round < 33 && done != FULL; ++round) {
+        bool ready = active && !((done >> lane) & 1u) && (la < 0 || ((done >> la) & 1u)) && (lb < 0 || ((done >> lb) & 1u));
+        if (ready) exec(k, desc);
+        __syncwarp();
+        done |= __ballot_sync(FULL, ready);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------- per-ball sweeps over fluid
+// The drag and buoyancy sweeps (pbf.rs:1824-2011, 2042-2121) visit balls in index order; ball b
+// reads and writes the velocities of its items (fluid particles), so it depends on the earlier
+// balls that share an item. Balls are claimed in index order by the warps of the block, and a
+// warp starts ball b once every earlier ball sharing one of b's items is done.
+
+__shared__ uint32_t g_ticket;
+
+// Packs the per-ball item lists (item_j[b * cap + s], s < cnt[b]) into records in ball order:
+// rec_off[0..nb], rec_key[r] = fluid index, rec_ball[r] = ball. Returns the record count.
+__device__ uint32_t pack_ball_items(const uint32_t* item_j, const uint32_t* cnt, uint32_t cap, uint32_t nb,
+                                    uint32_t* rec_off, uint32_t* rec_key, uint32_t* rec_ball) {
+  for (uint32_t b = tid(); b < nb; b += nthr()) rec_off[b] = cnt[b];
+  if (tid() == 0) rec_off[nb] = 0;
+  __syncthreads();
+  uint32_t total = block_exclusive_scan(rec_off, nb + 1);
+  for (uint32_t b = tid(); b < nb; b += nthr()) {
+    uint32_t o = rec_off[b], c = cnt[b];
+    for (uint32_t s = 0; s < c; ++s) { rec_key[o + s] = item_j[(size_t)b * cap + s]; rec_ball[o + s] = b; }
+  }
+  __syncthreads();
+  return total;
+}
+
+// rec_pred[r] = the ball of the previous record with the same fluid index (NONE if first).
+__device__ void ball_item_preds(const uint32_t* rec_key, const uint32_t* rec_ball, uint32_t nrec, uint32_t nf,
+                                uint32_t* start, uint32_t* cur, uint32_t* order, uint32_t* rec_pred) {
+  block_bucket_sort(rec_key, nrec, nf, start, cur, order);
+  for (uint32_t j = tid(); j < nf; j += nthr()) {
+    uint32_t prev = NONE;
+    for (uint32_t q = start[j]; q < start[j + 1]; ++q) {
+      uint32_t r = order[q];
+      rec_pred[r] = prev;
+      prev = rec_ball[r];
+    }
+  }
+  __syncthreads();
+}
+
+constexpr uint32_t SPIN_LIMIT = 1u << 24;
+
+// Runs fn(b, lane) once per ball, one warp per ball, in a dependency-respecting order. done[] is
+// nb words of scratch (shared or global). Waits are bounded: a wait that runs out sets
+// ERR_BUDGET in *err and lets the ball proceed.
+// Each ball runs in three parts: st = pre(b, lane) before the wait (loads and everything that
+// does not read what the sweep writes), run(b, lane, st) once the earlier balls sharing an item
+// are done (the part that reads and writes the swept velocities), then, after b is flagged done,
+// post(b, lane, st) (per-ball outputs that no other ball reads during the sweep). Only run() lies
+// on the dependency chain.
+// acct (optional, 3 counters): clock cycles summed over balls spent in pre, waiting, and in
+// run + post.
+// Warp-uniform wait until every lane's ball p (NONE: no wait) is flagged done: the lanes poll
+// together and sleep together, so the warp never diverges here (lanes that spun on their own
+// were measured to leave the shuffle-heavy code after the wait several times slower).
+__device__ __forceinline__ void wait_ball_done(volatile uint32_t* vdone, uint32_t p, uint32_t spin_ns,
+                                               uint32_t* err) {
+  for (uint32_t spins = 0;; ++spins) {
+    const bool ok = p == NONE || vdone[p] != 0u;
+    if (__all_sync(FULL, ok)) break;
+    if (spins > SPIN_LIMIT) {
+      if ((threadIdx.x & 31u) == 0) atomicOr(err, ERR_BUDGET);
+      break;
+    }
+    __nanosleep(spin_ns);  // yield issue slots to the warps on the critical path
+  }
+}
+
+// Warps from `warps` on sit the sweep out (they wait at the closing barrier).
+template <class Pre, class Run, class Post>
+__device__ void ball_dataflow(uint32_t nb, const uint32_t* rec_off, const uint32_t* rec_pred, uint32_t* done,
+                              uint32_t warps, uint32_t spin_ns, uint32_t* err, unsigned long long* acct, Pre pre,
+                              Run run, Post post) {
+  for (uint32_t b = tid(); b < nb; b += nthr()) done[b] = 0u;
+  if (tid() == 0) g_ticket = 0;
+  __syncthreads();
+  volatile uint32_t* vdone = done;
+  const int lane = threadIdx.x & 31;
+  unsigned long long t_pre = 0, t_wait = 0, t_run = 0;
+  for (;;) {
+    if ((threadIdx.x >> 5) >= warps) break;
+    uint32_t b = 0;
+    if (lane == 0) b = atomicAdd(&g_ticket, 1u);
+    b = __shfl_sync(FULL, b, 0);
+    if (b >= nb) break;
+    const long long t0 = clock64();
+    const uint32_t r0 = rec_off[b], r1 = rec_off[b + 1];
+    const uint32_t p0 = r0 + lane < r1 ? rec_pred[r0 + lane] : NONE;
+    auto st = pre(b, lane);
+    const long long t1 = clock64();
+    wait_ball_done(vdone, p0, spin_ns, err);
+    for (uint32_t c = r0 + 32; c < r1; c += 32) wait_ball_done(vdone, c + lane < r1 ? rec_pred[c + lane] : NONE, spin_ns, err);
+    __syncwarp();
+    __threadfence_block();
+    const long long t2 = clock64();
+    run(b, lane, st);
+    __threadfence_block();
+    __syncwarp();
+    if (lane == 0) vdone[b] = 1u;
+    post(b, lane, st);
+    t_pre += (unsigned long long)(t1 - t0);
+    t_wait += (unsigned long long)(t2 - t1);
+    t_run += (unsigned long long)(clock64() - t2);
+  }
+  if (acct && lane == 0 && (t_pre | t_wait | t_run)) {
+    atomicAdd(&acct[0], t_pre);
+    atomicAdd(&acct[1], t_wait);
+    atomicAdd(&acct[2], t_run);
+  }
+  __syncthreads();
+}
+
+// In-order sum over the lanes' values t = 0..lim-1 (every lane computes the same chain).
+__device__ __forceinline__ float lane_seq_sum(float acc, float v, uint32_t lim) {
+  for (uint32_t t = 0; t < lim; ++t) acc += __shfl_sync(FULL, v, t);
+  return acc;
+}
+__device__ __forceinline__ double lane_seq_sum(double acc, double v, uint32_t lim) {
+  for (uint32_t t = 0; t < lim; ++t) acc += __shfl_sync(FULL, v, t);
+  return acc;
+}
+
+// In-order merge of one 32-candidate chunk into a per-ball item list (the slot-map merge of
+// pbf.rs:1570-1577 and 2213-2228): candidates with acc = true, taken in lane order, either open a
+// new item (appended in first-seen order, initialised with their values) or add their values to
+// the existing item of the same fluid index j. slot[] maps j to its item index (NONE when absent)
+// and is private to the calling warp. Values: v0 (scalar), v1 (Vec2), v2 (scalar).
+struct MergeList {
+  uint32_t* j;
+  float* v0;
+  float2* v1;
+  float* v2;  // may be null
+  uint32_t cap;
+};
+__device__ __forceinline__ void warp_merge(bool acc, uint32_t j, float v0, V2 v1, float v2, uint32_t* slot,
+                                           const MergeList& L, uint32_t& cnt, bool& overflow) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t key = acc ? j : (0x80000000u | lane);
+  const uint32_t peers = __match_any_sync(FULL, key);
+  const uint32_t leader = __ffs(peers) - 1;
+  uint32_t g = NONE;
+  if (acc && lane == leader) g = slot[j];
+  const bool is_new = acc && lane == leader && g == NONE;
+  const uint32_t newmask = __ballot_sync(FULL, is_new);
+  if (is_new) {
+    g = cnt + __popc(newmask & ((1u << lane) - 1u));
+    if (g < L.cap) { slot[j] = g; L.j[g] = j; } else { overflow = true; }
+  }
+  cnt += __popc(newmask);
+  // the leader of each j accumulates its peers' values in lane order
+  float a0 = 0.0f, a2 = 0.0f;
+  V2 a1;
+  if (acc && lane == leader && !is_new && g < L.cap) {
+    a0 = L.v0[g];
+    a1 = V2(L.v1[g]);
+    if (L.v2) a2 = L.v2[g];
+  }
+  uint32_t vmask = __ballot_sync(FULL, acc);
+  while (vmask) {
+    const int t = __ffs(vmask) - 1;
+    vmask &= vmask - 1u;
+    const float t0 = __shfl_sync(FULL, v0, t), t1x = __shfl_sync(FULL, v1.x, t), t1y = __shfl_sync(FULL, v1.y, t);
+    const float t2 = __shfl_sync(FULL, v2, t);
+    const uint32_t lt = __shfl_sync(FULL, leader, t);
+    if (lane == lt) {
+      if (is_new && t == (int)lane) { a0 = t0; a1 = V2(t1x, t1y); a2 = t2; }
+      else { a0 += t0; a1.x += t1x; a1.y += t1y; a2 += t2; }
+    }
+  }
+  if (acc && lane == leader && g < L.cap) {
+    L.v0[g] = a0;
+    L.v1[g] = a1.f2();
+    if (L.v2) L.v2[g] = a2;
+  }
+  __syncwarp();
+}
+
+// Sequential-order reduction acc = (((init + f(0)) + f(1)) + ...) + f(n-1), with the exact
+// rounding of a one-thread loop, computed by one warp: the lanes evaluate 32 consecutive terms in
+// parallel (coalesced loads), then every lane adds them in index order by shuffles. Terms for
+// which f returns false are skipped (not added). Returns the result to all lanes of the warp.
+template <class T, class F>
+__device__ __forceinline__ T warp_ordered_sum(T init, uint32_t n, F f) {
+  const uint32_t lane = threadIdx.x & 31u;
+  T acc = init;
+  // software pipeline: the next chunk's terms are evaluated (loads in flight) before the current
+  // chunk is folded
+  T v = T(0);
+  bool use = lane < n ? f(lane, v) : false;
+  for (uint32_t c = 0; c < n; c += 32) {
+    T vn = T(0);
+    bool usen = c + 32 + lane < n ? f(c + 32 + lane, vn) : false;
+    uint32_t mask = __ballot_sync(FULL, use);
+    while (mask) {
+      int t = __ffs(mask) - 1;
+      acc += __shfl_sync(FULL, v, t);
+      mask &= mask - 1;
+    }
+    v = vn;
+    use = usen;
+  }
+  return acc;
+}
+
+}  // namespace mg

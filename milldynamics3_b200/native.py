@@ -19,7 +19,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["mill_kernels.cu", "mill_host.cu", "mill_params.cpp"]
 HEADERS = ["mill_common.cuh", "mill_block.cuh", "mill_grid.cuh", "mill_geom.cuh", "mill_fluid.cuh",
-           "mill_dem.cuh", "mill_kernels.h", "mill_params.h"]
+           "mill_dem.cuh", "mill_replay.cuh", "mill_kernels.h", "mill_params.h"]
 
 # Arithmetic contract: IEEE f32 division and square root, no fused multiply-add contraction in
 # device code (-fmad=false) or host code (-ffp-contract=off), no fast-math.
