@@ -299,6 +299,19 @@ int mg_probe_grid(const float* xy, uint32_t n, float cell, int32_t* min_cxy, int
 int mg_probe_candidate_pairs(const float* xy, uint32_t n, float cell, uint32_t* pairs, uint32_t cap, uint32_t* n_out);
 int mg_probe_neighbor_lists(const float* xy, uint32_t n, float h, uint32_t* offsets, uint32_t* nbrs, uint32_t cap,
                             uint32_t* n_edges);
+/* The neighbour CSR of mg_probe_neighbor_lists without allocating anything. No reference
+ * counterpart: it exists for callers that cannot allocate device memory per call (a loop held to
+ * a fixed memory budget, or one that must not synchronise the device). All pointers are DEVICE
+ * pointers the caller owns: xy_dev (2n floats), offsets_dev (n + 1), nbrs_dev (cap),
+ * n_edges_dev (1; the full edge count, also when it exceeds cap) and status_dev (1; 0 or error
+ * bits: 1 = cap too small, nothing written to nbrs_dev; 4 = a cell key saturated). Runs
+ * asynchronously on `stream` (a cudaStream_t; NULL = the legacy default stream); the grid scratch
+ * is one fixed static device array (at most 16384 points per call; a larger n returns
+ * MG_ERR_CAPACITY). Calls on one device share that scratch and must not overlap (issue them on
+ * one stream). The first call on a device resolves the scratch address; make it before capturing
+ * a stream. */
+int mg_neighbor_lists_noalloc(const float* xy_dev, uint32_t n, float h, uint32_t* offsets_dev, uint32_t* nbrs_dev,
+                              uint32_t cap, uint32_t* n_edges_dev, uint32_t* status_dev, void* stream);
 /* neighbour CSR / ball pair list of the last fluid / ball sub-step taken on this handle */
 int mg_last_neighbor_lists(MgSim* sim, uint32_t* offsets, uint32_t* nbrs, uint32_t cap, uint32_t* n_edges);
 int mg_last_ball_pairs(MgSim* sim, uint32_t* pairs, uint32_t cap, uint32_t* n_out);

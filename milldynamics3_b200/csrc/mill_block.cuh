@@ -28,7 +28,7 @@ __device__ __forceinline__ T warp_sum(T v) {
 }
 
 // Deterministic f64 sum: fixed xor-tree inside warps, then a fixed tree over the warp sums.
-__device__ double block_sum_d(double v) {
+__device__ inline double block_sum_d(double v) {
   __shared__ double sh[32];
   __shared__ double res;
   v = warp_sum(v);
@@ -47,7 +47,7 @@ __device__ double block_sum_d(double v) {
   return r;
 }
 
-__device__ uint32_t block_sum_u(uint32_t v) {
+__device__ inline uint32_t block_sum_u(uint32_t v) {
   __shared__ uint32_t sh[32];
   __shared__ uint32_t res;
   v = warp_sum(v);
@@ -67,7 +67,7 @@ __device__ uint32_t block_sum_u(uint32_t v) {
 }
 
 // f32::max fold (order-independent: max is exact).
-__device__ float block_max_f(float v) {
+__device__ inline float block_max_f(float v) {
   __shared__ float sh[32];
   __shared__ float res;
   for (int o = 16; o > 0; o >>= 1) v = fmax_r(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -86,7 +86,7 @@ __device__ float block_max_f(float v) {
   return r;
 }
 
-__device__ void block_minmax_i(int32_t& mn0, int32_t& mx0, int32_t& mn1, int32_t& mx1) {
+__device__ inline void block_minmax_i(int32_t& mn0, int32_t& mx0, int32_t& mn1, int32_t& mx1) {
   __shared__ int32_t sh[4][32];
   int w = tid() >> 5, l = tid() & 31;
   for (int o = 16; o > 0; o >>= 1) {
@@ -107,7 +107,7 @@ __device__ void block_minmax_i(int32_t& mn0, int32_t& mx0, int32_t& mn1, int32_t
 }
 
 // In-place exclusive scan of a[0..m); returns the total. All threads call it.
-__device__ uint32_t block_exclusive_scan(uint32_t* a, uint32_t m) {
+__device__ inline uint32_t block_exclusive_scan(uint32_t* a, uint32_t m) {
   __shared__ uint32_t wsum[32];
   __shared__ uint32_t carry;
   if (tid() == 0) carry = 0;
@@ -156,7 +156,7 @@ __device__ __forceinline__ void small_sort_u32(uint32_t* a, uint32_t n) {
 
 // Stable bucket sort: start[0..nbk] receives bucket offsets, order[] the record indices grouped by
 // key in ascending record order; cur[0..nbk) is scratch. Buckets are expected to be short.
-__device__ void block_bucket_sort(const uint32_t* keys, uint32_t nrec, uint32_t nbk, uint32_t* start, uint32_t* cur,
+__device__ inline void block_bucket_sort(const uint32_t* keys, uint32_t nrec, uint32_t nbk, uint32_t* start, uint32_t* cur,
                                   uint32_t* order) {
   for (uint32_t k = tid(); k <= nbk; k += nthr()) start[k] = 0;
   __syncthreads();

@@ -65,7 +65,7 @@ __device__ __forceinline__ void drum_sdf_world(const StepUniform& U, V2 pw, V2 t
 __device__ __forceinline__ V2 wall_velocity(float omega, V2 p) { return omega * V2(-p.y, p.x); }
 
 // geometry.rs:146-194 Drum::toi_swept; returns false for None.
-__device__ bool drum_toi_swept(const StepUniform& U, V2 x0, V2 x1, float a0, float a1, float radius, float& t_out) {
+__device__ inline bool drum_toi_swept(const StepUniform& U, V2 x0, V2 x1, float a0, float a1, float radius, float& t_out) {
   V2 local0 = rotate(x0, U.to_local0);
   if (drum_sdf(U, local0) - radius <= 0.0f) return false;
   V2 path = x1 - x0;

@@ -16,7 +16,7 @@ __device__ __forceinline__ bool key_eq(int2 a, int2 b) { return a.x == b.x && a.
 
 // Builds the grid of points[0..n) into gb; hdr (shared memory) receives the layout.
 // Sets ERR_CELLS in *err if a key saturates the i32 range (coordinates beyond 2^31 cells).
-__device__ void grid_build(const float2* pts, uint32_t n, float cell, const GridBuf& gb, GridHdr& hdr, uint32_t* err) {
+__device__ inline void grid_build(const float2* pts, uint32_t n, float cell, const GridBuf& gb, GridHdr& hdr, uint32_t* err) {
   int32_t mnx = INT32_MAX, mxx = INT32_MIN, mny = INT32_MAX, mxy = INT32_MIN;
   uint32_t cnt = 0;
   bool sat = false;
@@ -227,7 +227,7 @@ __device__ __forceinline__ void for_each_stencil_neighbor(const GridHdr& hdr, co
 }
 
 // Neighbour CSR in the reference's per-particle order (r^2 <= h^2). Two passes: count, scan, fill.
-__device__ void build_neighbor_lists(const float2* x, uint32_t n, float h, const GridHdr& hdr, const GridBuf& gb,
+__device__ inline void build_neighbor_lists(const float2* x, uint32_t n, float h, const GridHdr& hdr, const GridBuf& gb,
                                      uint32_t* off, uint32_t* nbrs, uint32_t cap, uint32_t* err, uint32_t* n_edges) {
   float h2 = h * h;
   for (uint32_t i = tid(); i < n; i += nthr()) {
@@ -274,7 +274,7 @@ __device__ __forceinline__ int2 cell_of(const GridHdr& hdr, const GridBuf& gb, u
   return gb.keys[k];
 }
 
-__device__ uint32_t build_candidate_pairs(const GridHdr& hdr, const GridBuf& gb, uint32_t* cnt, uint32_t* pi,
+__device__ inline uint32_t build_candidate_pairs(const GridHdr& hdr, const GridBuf& gb, uint32_t* cnt, uint32_t* pi,
                                           uint32_t* pj, uint32_t cap, uint32_t* err) {
   uint32_t nc = hdr.ncells;
   for (uint32_t k = tid(); k < nc; k += nthr()) {

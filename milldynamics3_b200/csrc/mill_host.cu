@@ -600,6 +600,10 @@ int download(MgSim* s, mgh::Balls* b, mgh::Fluid* f) {
 
 }  // namespace
 
+namespace mg {
+int set_global_error(int code, const char* msg) { return fail_global(code, "%s", msg); }
+}  // namespace mg
+
 // ====================================================================== C ABI
 extern "C" {
 

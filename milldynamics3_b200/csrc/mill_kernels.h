@@ -21,6 +21,8 @@ inline size_t stage_smem_bytes(uint32_t nf, uint32_t nb) {
   if (need <= MAX_STAGE_SMEM) return need;
   return balls <= MAX_STAGE_SMEM ? ((balls + 255) & ~size_t(255)) : 0;
 }
+// Sets the message mg_global_last_error() returns on this host thread; returns code.
+int set_global_error(int code, const char* msg);
 // Grid-stage probe over the descriptor's fx[0..nf): mode 0 grid, 1 candidate pairs, 2 neighbours.
 cudaError_t launch_probe(const MillDev* mill, float cell, int mode, uint32_t* result, cudaStream_t stream);
 

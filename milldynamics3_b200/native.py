@@ -17,7 +17,7 @@ LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libmillgpu.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["mill_kernels.cu", "mill_host.cu", "mill_params.cpp"]
+SOURCES = ["mill_kernels.cu", "mill_host.cu", "mill_params.cpp", "mill_noalloc.cu"]
 HEADERS = ["mill_common.cuh", "mill_block.cuh", "mill_grid.cuh", "mill_geom.cuh", "mill_fluid.cuh",
            "mill_dem.cuh", "mill_replay.cuh", "mill_kernels.h", "mill_params.h"]
 
