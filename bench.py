@@ -164,6 +164,71 @@ def cpu_baseline(seconds=10.0):
                       % (frames, dt)}
 
 
+def run_batched(lib, backend, args):
+    """The 512-mill mix in one launch per frame (mg_batch_*), against the plain path (each mill
+    stepped alone, one after another) sampled on the same mix. Returns the 'batched' object."""
+    import numpy as np
+    import torch
+    from milldynamics3_b200.batch import Batch, mix_params
+    from milldynamics3_b200.sim import Simulation
+    ps, info = mix_params(backend, args.batch_mills, seed=1)
+    d = [backend.derived(p) for p in ps]
+    batch = Batch(backend, ps)
+    foot = C.c_uint64()
+    total_bytes = 0
+    for i in range(len(ps)):
+        lib.sim_footprint(batch.mill(i).h, C.byref(foot))
+        total_bytes += foot.value
+    stream = torch.cuda.ExternalStream(batch.stream())
+    for _ in range(max(args.warmup, 3)):
+        batch.step_frames(1)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lat = []
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.batch_frames):
+        t0 = time.perf_counter()
+        batch.step_frames(1)
+        lat.append(time.perf_counter() - t0)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t = ev0.elapsed_time(ev1) / 1e3
+    kernel_ms, _ = batch.last_kernel_ms()
+    batch.close()
+    mfps = args.batch_frames * len(ps) / t
+    # plain path on a sample of the same mix: each mill alone, one frame after one warm-up frame
+    rng = np.random.default_rng(2)
+    sample = sorted(rng.choice(len(ps), size=min(args.plain_sample, len(ps)), replace=False).tolist())
+    plain_t = []
+    for i in sample:
+        s = Simulation(backend, ps[i])
+        s.step(1.0 / 60.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.step(1.0 / 60.0)
+        torch.cuda.synchronize()
+        plain_t.append(time.perf_counter() - t0)
+        s.close()
+    plain_mfps = 1.0 / (sum(plain_t) / len(plain_t))
+    nb = np.array([x.eff_ball_count for x in d])
+    ns = np.array([x.effective_substeps for x in d])
+    res = np.array([x.effective_fluid_resolution for x in d])
+    lat_ms = sorted(1e3 * x for x in lat)
+    return {"mills": len(ps), "mill_frames_per_s": mfps, "ms_per_batch_frame": 1e3 * t / args.batch_frames,
+            "kernel_ms_per_batch_frame": kernel_ms, "frames_timed": args.batch_frames,
+            "frame_latency_ms": {"p50": lat_ms[len(lat_ms) // 2], "max": lat_ms[-1]},
+            "plain_mill_frames_per_s": plain_mfps, "plain_sample_mills": len(sample),
+            "ratio_vs_plain": mfps / plain_mfps, "device_bytes": total_bytes,
+            "mix": {"balls_min_mean_max": [int(nb.min()), float(nb.mean()), int(nb.max())],
+                    "substeps_min_mean_max": [int(ns.min()), float(ns.mean()), int(ns.max())],
+                    "resolution_min_mean_max": [int(res.min()), float(res.mean()), int(res.max())],
+                    "diameter_mm_min_max": [1e3 * min(x["diameter_m"] for x in info),
+                                            1e3 * max(x["diameter_m"] for x in info)],
+                    "sampling": "ball count log-uniform 100-3000 and fill U[0.2,0.4] with D = 2r sqrt(N/(J phi)) "
+                                "redrawn until D in [40,120] mm; resolution U[15,60]; speed U[50,90]% critical; "
+                                "2 mm discs; seed per mill"}}
+
+
 def run_device(args):
     import numpy as np
     import torch
@@ -257,6 +322,8 @@ def run_device(args):
                              "kernel_ms_per_launch": k_ms, "algorithmic_bytes_per_launch": per_launch_bytes},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
                 "gpu_launches": args.steps, "clocks": clocks, "stage_us_per_substep": stages}
+        if args.batch_mills > 0:
+            line["batched"] = run_batched(lib, b, args)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
         print(json.dumps(line), flush=True)
@@ -273,6 +340,9 @@ def main():
     ap.add_argument("--impl", default="device", choices=["device", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-mills", type=int, default=512, help="mills of the batched leg (0: skip it)")
+    ap.add_argument("--batch-frames", type=int, default=5)
+    ap.add_argument("--plain-sample", type=int, default=16, help="mills of the mix timed on the plain path")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

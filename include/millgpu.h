@@ -316,6 +316,29 @@ int mg_neighbor_lists_noalloc(const float* xy_dev, uint32_t n, float h, uint32_t
 int mg_last_neighbor_lists(MgSim* sim, uint32_t* offsets, uint32_t* nbrs, uint32_t cap, uint32_t* n_edges);
 int mg_last_ball_pairs(MgSim* sim, uint32_t* pairs, uint32_t cap, uint32_t* n_out);
 
+/* ---- batches: many independent mills per launch (batch::run_seed's unit of work, batch.rs:40-191,
+ * run many at a time). No single reference counterpart: the reference steps one Simulation at a
+ * time. Each mill is an ordinary Simulation (params[i], its own seed) whose sub-steps run as one
+ * thread block of a shared launch; a mill's results are identical alone or in a batch. */
+typedef struct MgBatch MgBatch;
+int mg_batch_create(const MgParams* params, uint32_t n_mills, MgBatch** out);
+void mg_batch_destroy(MgBatch* batch);
+const char* mg_batch_last_error(const MgBatch* batch);
+uint32_t mg_batch_size(const MgBatch* batch);
+int mg_batch_set_options(MgBatch* batch, const MgOptions* opt);
+/* Simulation::step(frame_dt) on every mill, `frames` times (each mill its own effective_substeps). */
+int mg_batch_step_frames(MgBatch* batch, uint32_t frames, float frame_dt);
+/* Simulation scalars of every mill (n_mills entries). */
+int mg_batch_scalars(MgBatch* batch, MgScalars* out);
+/* Borrows mill i's handle for the per-mill accessors (mg_get_balls, mg_energy_budget,
+ * mg_stress_histogram_rate, mg_state_hash ...). Owned by the batch: do not destroy it. */
+int mg_batch_mill(MgBatch* batch, uint32_t i, MgSim** out);
+int mg_batch_stream(MgBatch* batch, void** stream);
+/* Device duration of the last frame launch and the number of frame launches so far. */
+int mg_batch_last_kernel_ms(MgBatch* batch, float* ms, uint64_t* launches);
+/* Device memory a handle holds (its arena plus launch blocks), for admission by footprint. */
+int mg_sim_footprint(const MgSim* sim, uint64_t* device_bytes);
+
 #ifdef __cplusplus
 }
 #endif

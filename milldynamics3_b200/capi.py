@@ -212,6 +212,17 @@ DEVICE_ONLY = [
     ("sim_last_kernel_ms", C.c_int, [vp, P(C.c_float), P(C.c_uint64)]),
     ("counter_totals", C.c_int, [vp, P(C.c_uint64), P(C.c_uint64), C.c_int]),
     ("stage_cycles", C.c_int, [vp, P(C.c_uint64), C.c_int]),
+    ("batch_create", C.c_int, [P(Params), C.c_uint32, P(vp)]),
+    ("batch_destroy", None, [vp]),
+    ("batch_last_error", C.c_char_p, [vp]),
+    ("batch_size", C.c_uint32, [vp]),
+    ("batch_set_options", C.c_int, [vp, P(Options)]),
+    ("batch_step_frames", C.c_int, [vp, C.c_uint32, C.c_float]),
+    ("batch_scalars", C.c_int, [vp, P(Scalars)]),
+    ("batch_mill", C.c_int, [vp, C.c_uint32, P(vp)]),
+    ("batch_stream", C.c_int, [vp, P(vp)]),
+    ("batch_last_kernel_ms", C.c_int, [vp, P(C.c_float), P(C.c_uint64)]),
+    ("sim_footprint", C.c_int, [vp, P(C.c_uint64)]),
 ]
 
 STAGE_NAMES = [

@@ -280,7 +280,8 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
   return MG_OK;
 }
 
-int push_desc(MgSim* s) {
+// The descriptor's per-mill scalars: counts, materials, shared-memory sizing.
+void fill_desc(MgSim* s) {
   s->md.nf = s->nf;
   s->md.nb = s->nb;
   s->md.f_mass = s->fmat.particle_mass;
@@ -292,7 +293,24 @@ int push_desc(MgSim* s) {
   s->md.b_rtrue = s->bmat.true_radius;
   s->md.smem_bytes = (uint32_t)stage_smem_bytes(s->nf, s->nb);
   s->md.smem_balls = (size_t)s->nb * 24 <= s->md.smem_bytes ? s->nb : 0u;
+}
+
+int push_desc(MgSim* s) {
+  fill_desc(s);
   CK(cudaMemcpyAsync(s->d_md, &s->md, sizeof(MillDev), cudaMemcpyHostToDevice, s->stream));
+  return MG_OK;
+}
+
+// The sub-step kernel is only launched on materials it is written for: positive, finite fluid
+// smoothing length, particle mass and rest density (when there is fluid) and ball radius, mass,
+// inertia and true radius (when there are balls).
+bool pos_finite(float v) { return v > 0.0f && std::isfinite(v); }
+int check_materials(MgSim* s) {
+  if (s->nf > 0 && !(pos_finite(s->fmat.h) && pos_finite(s->fmat.particle_mass) && pos_finite(s->fmat.rest_density)))
+    return fail(s, MG_ERR_STATE, "fluid material (h, particle mass, rest density) must be positive and finite");
+  if (s->nb > 0 && !(pos_finite(s->bmat.radius) && pos_finite(s->bmat.mass) && pos_finite(s->bmat.inertia) &&
+                     pos_finite(s->bmat.true_radius)))
+    return fail(s, MG_ERR_STATE, "ball material (radius, mass, inertia, true radius) must be positive and finite");
   return MG_OK;
 }
 
@@ -372,13 +390,15 @@ void fill_angle(SubAngles& A, float angle, float omega, float dt) {
 // Launches n_sub sub-steps (angles already in h_ang) and waits; outputs land in h_out / h_imp.
 int run(MgSim* s, uint32_t n_sub) {
   if (n_sub > MAX_SUB) return fail(s, MG_ERR_ARG, "at most %u sub-steps per launch", MAX_SUB);
-  int rc = push_desc(s);
+  int rc = check_materials(s);
+  if (!rc) rc = push_desc(s);
   if (rc) return rc;
   CK(cudaMemcpyAsync(s->d_uni, s->h_uni, sizeof(StepUniform), cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemcpyAsync(s->d_ang, s->h_ang, sizeof(SubAngles) * n_sub, cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemsetAsync(s->md.err, 0, sizeof(uint32_t), s->stream));
   CK(cudaEventRecord(s->ev0, s->stream));
-  CK(launch_substeps(s->d_md, 1, s->d_uni, s->d_ang, n_sub, s->opt.block_threads, s->md.smem_bytes, s->stream));
+  CK(launch_substeps(s->d_md, 1, s->d_uni, s->d_ang, n_sub, nullptr, s->opt.block_threads, s->md.smem_bytes,
+                     s->stream));
   CK(cudaEventRecord(s->ev1, s->stream));
   CK(cudaMemcpyAsync(s->h_out, s->md.out, sizeof(StepOut) * n_sub, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
@@ -1108,6 +1128,283 @@ int mg_probe_neighbor_lists(const float* xy, uint32_t n, float h, uint32_t* offs
   if (ne > cap) { mg_sim_destroy(s); return fail_global(MG_ERR_CAPACITY, "neighbour buffer too small"); }
   if (ne) cudaMemcpy(nbrs, s->md.nbrs, 4 * (size_t)ne, cudaMemcpyDeviceToHost);
   mg_sim_destroy(s);
+  return MG_OK;
+}
+
+}  // extern "C"
+
+// ====================================================================== batches of mills
+// Many independent mills advanced together: one launch per frame with one thread block per mill
+// (each mill its own sub-step count), then one packing launch for the impact records. Every mill
+// keeps the arena, uniforms and host bookkeeping of an ordinary handle (EMA power and torque,
+// energy budget, stress accumulators), so a mill's results are the same alone or in a batch.
+struct MgBatch {
+  std::vector<MgSim*> mills;
+  std::vector<uint32_t> n_sub;  // effective_substeps per mill
+  uint32_t stride = 0;          // sub-step stride of the angle and output blocks (max n_sub)
+  cudaStream_t stream = nullptr;
+  MillDev* d_md = nullptr;      // descriptors (out -> the batch's output block)
+  StepUniform* d_uni = nullptr;
+  SubAngles* d_ang = nullptr;
+  SubAngles* h_ang = nullptr;
+  uint32_t* d_nsub = nullptr;
+  StepOut* d_out = nullptr;
+  StepOut* h_out = nullptr;
+  MgImpactRecord* d_packed = nullptr;
+  MgImpactRecord* h_packed = nullptr;
+  uint32_t packed_cap = 0;
+  uint32_t* d_cursor = nullptr;
+  uint2* d_table = nullptr;
+  uint2* h_table = nullptr;
+  size_t smem = 0;
+  uint32_t threads = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_kernel_ms = 0.0f;
+  uint64_t launches = 0;
+  std::string err;
+};
+
+namespace {
+
+int bfail(MgBatch* b, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (b) b->err = buf;
+  g_err = buf;
+  return code;
+}
+#define BCK(call)                                                                   \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess) return bfail(b, MG_ERR_CUDA, "%s", cudaGetErrorString(e_)); \
+  } while (0)
+
+// Uploads the descriptors and mill-uniform blocks of every mill (at creation and after options
+// change).
+int batch_upload(MgBatch* b) {
+  const uint32_t n = (uint32_t)b->mills.size();
+  std::vector<MillDev> md(n);
+  std::vector<StepUniform> uni(n);
+  b->smem = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    MgSim* s = b->mills[i];
+    const MgSimulationParams& q = s->params.simulation;
+    int rc = fill_uniform(s, sim_drum(s), s->params.media, s->params.slurry, q.pbf_iterations, q.dem_iterations, 1,
+                          1, 1);
+    if (rc) return bfail(b, rc, "mill %u: %s", i, s->err.c_str());
+    fill_desc(s);
+    md[i] = s->md;
+    md[i].out = b->d_out + (size_t)i * b->stride;
+    uni[i] = *s->h_uni;
+    b->smem = std::max(b->smem, (size_t)s->md.smem_bytes);
+  }
+  BCK(cudaMemcpyAsync(b->d_md, md.data(), sizeof(MillDev) * n, cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaMemcpyAsync(b->d_uni, uni.data(), sizeof(StepUniform) * n, cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  return MG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mg_batch_create(const MgParams* params, uint32_t n_mills, MgBatch** out) {
+  if (!params || !out || n_mills == 0) return fail_global(MG_ERR_ARG, "null argument or empty batch");
+  MgBatch* b = new MgBatch();
+  int rc = MG_OK;
+  for (uint32_t i = 0; i < n_mills && !rc; ++i) {
+    MgSim* s = nullptr;
+    rc = create_sim(&params[i], nullptr, 0, &s);
+    if (rc) { bfail(b, rc, "mill %u: %s", i, g_err.c_str()); break; }
+    b->mills.push_back(s);
+    uint32_t ns = std::max(mgh::effective_substeps(s->params), 1u);
+    if (ns > MAX_SUB) { rc = bfail(b, MG_ERR_ARG, "mill %u: %u sub-steps per frame, at most %u", i, ns, MAX_SUB); break; }
+    b->n_sub.push_back(ns);
+    b->stride = std::max(b->stride, ns);
+  }
+  auto setup = [&]() -> int {
+    BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    BCK(cudaMalloc(&b->d_md, sizeof(MillDev) * n_mills));
+    BCK(cudaMalloc(&b->d_uni, sizeof(StepUniform) * n_mills));
+    BCK(cudaMalloc(&b->d_ang, sizeof(SubAngles) * n_mills * b->stride));
+    BCK(cudaMallocHost(&b->h_ang, sizeof(SubAngles) * n_mills * b->stride));
+    BCK(cudaMalloc(&b->d_nsub, sizeof(uint32_t) * n_mills));
+    BCK(cudaMalloc(&b->d_out, sizeof(StepOut) * n_mills * b->stride));
+    BCK(cudaMallocHost(&b->h_out, sizeof(StepOut) * n_mills * b->stride));
+    uint64_t cap = 0;
+    for (MgSim* s : b->mills) cap += (uint64_t)s->md.cap_impacts * b->stride;
+    b->packed_cap = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFF0ull);
+    BCK(cudaMalloc(&b->d_packed, sizeof(MgImpactRecord) * (size_t)b->packed_cap));
+    BCK(cudaMallocHost(&b->h_packed, sizeof(MgImpactRecord) * (size_t)b->packed_cap));
+    BCK(cudaMalloc(&b->d_cursor, sizeof(uint32_t)));
+    BCK(cudaMalloc(&b->d_table, sizeof(uint2) * n_mills));
+    BCK(cudaMallocHost(&b->h_table, sizeof(uint2) * n_mills));
+    BCK(cudaEventCreate(&b->ev0));
+    BCK(cudaEventCreate(&b->ev1));
+    BCK(cudaMemcpyAsync(b->d_nsub, b->n_sub.data(), sizeof(uint32_t) * n_mills, cudaMemcpyHostToDevice, b->stream));
+    return batch_upload(b);
+  };
+  if (!rc) rc = setup();
+  if (rc) {
+    std::string e = b->err;
+    mg_batch_destroy(b);
+    g_err = e;
+    return rc;
+  }
+  *out = b;
+  return MG_OK;
+}
+
+void mg_batch_destroy(MgBatch* b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (MgSim* s : b->mills) mg_sim_destroy(s);
+  if (b->d_md) cudaFree(b->d_md);
+  if (b->d_uni) cudaFree(b->d_uni);
+  if (b->d_ang) cudaFree(b->d_ang);
+  if (b->h_ang) cudaFreeHost(b->h_ang);
+  if (b->d_nsub) cudaFree(b->d_nsub);
+  if (b->d_out) cudaFree(b->d_out);
+  if (b->h_out) cudaFreeHost(b->h_out);
+  if (b->d_packed) cudaFree(b->d_packed);
+  if (b->h_packed) cudaFreeHost(b->h_packed);
+  if (b->d_cursor) cudaFree(b->d_cursor);
+  if (b->d_table) cudaFree(b->d_table);
+  if (b->h_table) cudaFreeHost(b->h_table);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+const char* mg_batch_last_error(const MgBatch* b) { return b ? b->err.c_str() : g_err.c_str(); }
+
+uint32_t mg_batch_size(const MgBatch* b) { return b ? (uint32_t)b->mills.size() : 0u; }
+
+int mg_batch_set_options(MgBatch* b, const MgOptions* opt) {
+  if (!b || !opt) return fail_global(MG_ERR_ARG, "null argument");
+  for (MgSim* s : b->mills) {
+    int rc = mg_sim_set_options(s, opt);
+    if (rc) return bfail(b, rc, "%s", s->err.c_str());
+  }
+  b->threads = opt->block_threads;
+  return batch_upload(b);
+}
+
+int mg_batch_mill(MgBatch* b, uint32_t i, MgSim** out) {
+  if (!b || !out) return fail_global(MG_ERR_ARG, "null argument");
+  if (i >= b->mills.size()) return bfail(b, MG_ERR_ARG, "mill %u out of range (%zu mills)", i, b->mills.size());
+  *out = b->mills[i];
+  return MG_OK;
+}
+
+int mg_batch_step_frames(MgBatch* b, uint32_t frames, float frame_dt) {
+  if (!b) return fail_global(MG_ERR_ARG, "null handle");
+  const uint32_t n = (uint32_t)b->mills.size();
+  // descriptors follow the members' current counts and materials (the per-mill setters may change
+  // them between calls)
+  std::vector<MillDev> md(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    MgSim* s = b->mills[i];
+    int rc = check_materials(s);
+    if (rc) return bfail(b, rc, "mill %u: %s", i, s->err.c_str());
+    fill_desc(s);
+    md[i] = s->md;
+    md[i].out = b->d_out + (size_t)i * b->stride;
+    b->smem = std::max(b->smem, (size_t)s->md.smem_bytes);
+  }
+  BCK(cudaMemcpyAsync(b->d_md, md.data(), sizeof(MillDev) * n, cudaMemcpyHostToDevice, b->stream));
+  for (uint32_t f = 0; f < frames; ++f) {
+    // Simulation::step(frame_dt) for every mill: n_sub[i] sub-steps of frame_dt / n_sub[i]
+    for (uint32_t i = 0; i < n; ++i) {
+      MgSim* s = b->mills[i];
+      const uint32_t ns = b->n_sub[i];
+      const float sub_dt = frame_dt / (float)ns;
+      const float omega = mgh::mill_omega(s->params.mill);
+      float angle = s->drum_angle;
+      for (uint32_t k = 0; k < ns; ++k) {
+        fill_angle(b->h_ang[(size_t)i * b->stride + k], angle, omega, sub_dt);
+        angle = mgh::rem_euclid_r(angle + omega * sub_dt, mgh::TAU_F);
+      }
+    }
+    BCK(cudaMemcpyAsync(b->d_ang, b->h_ang, sizeof(SubAngles) * n * b->stride, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaEventRecord(b->ev0, b->stream));
+    BCK(launch_substeps(b->d_md, n, b->d_uni, b->d_ang, b->stride, b->d_nsub, b->threads, b->smem, b->stream));
+    BCK(cudaEventRecord(b->ev1, b->stream));
+    BCK(cudaMemsetAsync(b->d_cursor, 0, sizeof(uint32_t), b->stream));
+    BCK(launch_pack_impacts(b->d_md, n, b->d_nsub, b->d_packed, b->packed_cap, b->d_cursor, b->d_table, b->stream));
+    BCK(cudaMemcpyAsync(b->h_out, b->d_out, sizeof(StepOut) * n * b->stride, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaMemcpyAsync(b->h_table, b->d_table, sizeof(uint2) * n, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    BCK(cudaEventElapsedTime(&b->last_kernel_ms, b->ev0, b->ev1));
+    b->launches += 1;
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < n; ++i) total = std::max<uint64_t>(total, (uint64_t)b->h_table[i].x + b->h_table[i].y);
+    if (total > b->packed_cap) return bfail(b, MG_ERR_CAPACITY, "impact records exceed the batch buffer");
+    if (total)
+      BCK(cudaMemcpyAsync(b->h_packed, b->d_packed, sizeof(MgImpactRecord) * total, cudaMemcpyDeviceToHost,
+                          b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    for (uint32_t i = 0; i < n; ++i) {
+      MgSim* s = b->mills[i];
+      const uint32_t ns = b->n_sub[i];
+      const StepOut* o = b->h_out + (size_t)i * b->stride;
+      uint32_t e = 0;
+      for (uint32_t k = 0; k < ns; ++k) e |= o[k].err;
+      if (e) return bfail(b, MG_ERR_CAPACITY, "mill %u: device capacity exceeded (error bits 0x%x)", i, e);
+      std::memcpy(s->h_out, o, sizeof(StepOut) * ns);
+      const MgImpactRecord* rec = b->h_packed + b->h_table[i].x;
+      for (uint32_t k = 0; k < ns; ++k) {
+        const uint32_t ni = std::min(o[k].n_impacts, s->md.cap_impacts);
+        if (ni) std::memcpy(s->h_imp + (size_t)k * s->md.cap_impacts, rec, sizeof(MgImpactRecord) * ni);
+        rec += ni;
+        const uint32_t* c = reinterpret_cast<const uint32_t*>(&o[k].ctr);
+        for (int q = 0; q < 10; ++q) s->ctr_tot[q] += c[q];
+        for (int q = 0; q < 40; ++q) s->stage_tot[q] += o[k].stage[q];
+        s->ctr_n += 1;
+      }
+      s->max_disp = 0.0f;
+      s->clamp_hits_frame = 0;
+      const float sub_dt = frame_dt / (float)ns;
+      const float omega = mgh::mill_omega(s->params.mill);
+      for (uint32_t k = 0; k < ns; ++k) fold_substep(s, k, sub_dt, omega);
+      s->last_fluid = o[ns - 1].fs;
+      s->last_dem = o[ns - 1].ds;
+      s->last_ctr = o[ns - 1].ctr;
+      s->launches += 1;
+    }
+  }
+  return MG_OK;
+}
+
+int mg_batch_scalars(MgBatch* b, MgScalars* out) {
+  if (!b || !out) return fail_global(MG_ERR_ARG, "null argument");
+  for (size_t i = 0; i < b->mills.size(); ++i) {
+    int rc = mg_get_scalars(b->mills[i], &out[i]);
+    if (rc) return bfail(b, rc, "mill %zu: %s", i, b->mills[i]->err.c_str());
+  }
+  return MG_OK;
+}
+
+int mg_batch_stream(MgBatch* b, void** stream) {
+  if (!b || !stream) return fail_global(MG_ERR_ARG, "null argument");
+  *stream = b->stream;
+  return MG_OK;
+}
+
+int mg_batch_last_kernel_ms(MgBatch* b, float* ms, uint64_t* launches) {
+  if (!b) return fail_global(MG_ERR_ARG, "null handle");
+  if (ms) *ms = b->last_kernel_ms;
+  if (launches) *launches = b->launches;
+  return MG_OK;
+}
+
+int mg_sim_footprint(const MgSim* s, uint64_t* device_bytes) {
+  if (!s || !device_bytes) return fail_global(MG_ERR_ARG, "null argument");
+  *device_bytes = (uint64_t)s->dbytes + sizeof(MillDev) + sizeof(StepUniform) + sizeof(SubAngles) * MAX_SUB;
   return MG_OK;
 }
 

@@ -8,16 +8,23 @@
 
 namespace mg {
 
+// n_sub is the sub-step stride of `angles`; mill b runs n_sub_of[b] sub-steps when n_sub_of is
+// given (a batch of mills with different sub-step counts), else n_sub.
 __global__ void __launch_bounds__(512) mill_substeps_kernel(const MillDev* __restrict__ mills, StepUniform* uni,
-                                                            const SubAngles* __restrict__ angles, uint32_t n_sub) {
+                                                            const SubAngles* __restrict__ angles, uint32_t n_sub,
+                                                            const uint32_t* __restrict__ n_sub_of) {
   __shared__ MillDev m;
   __shared__ FluidShared fs;
   __shared__ DemShared ds;
   extern __shared__ __align__(16) unsigned char dsm[];  // staged ball state (24 bytes per ball)
   const uint32_t mill = blockIdx.x;
-  if (threadIdx.x == 0) m = mills[mill];
+  if (threadIdx.x == 0) {
+    m = mills[mill];
+    *m.err = 0;
+  }
   __syncthreads();
-  for (uint32_t s = 0; s < n_sub; ++s) {
+  const uint32_t my_sub = n_sub_of ? n_sub_of[mill] : n_sub;
+  for (uint32_t s = 0; s < my_sub; ++s) {
     StepUniform& U = uni[mill];
     StepOut& out = m.out[s];
     if (threadIdx.x == 0) {
@@ -76,14 +83,49 @@ __global__ void __launch_bounds__(512) probe_kernel(const MillDev* __restrict__ 
 }
 
 cudaError_t launch_substeps(const MillDev* mills, uint32_t n_mills, StepUniform* uni, const SubAngles* angles,
-                            uint32_t n_sub, uint32_t threads, size_t smem_bytes, cudaStream_t stream) {
+                            uint32_t n_sub, const uint32_t* n_sub_of, uint32_t threads, size_t smem_bytes,
+                            cudaStream_t stream) {
   if (threads == 0 || threads > 512) threads = 512;
   if (smem_bytes > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(mill_substeps_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem_bytes);
     if (e != cudaSuccess) return e;
   }
-  mill_substeps_kernel<<<n_mills, threads, smem_bytes, stream>>>(mills, uni, angles, n_sub);
+  mill_substeps_kernel<<<n_mills, threads, smem_bytes, stream>>>(mills, uni, angles, n_sub, n_sub_of);
+  return cudaGetLastError();
+}
+
+// One block per mill: appends the mill's impact records (sub-step order) to the packed buffer.
+__global__ void __launch_bounds__(256) pack_impacts_kernel(const MillDev* __restrict__ mills,
+                                                           const uint32_t* __restrict__ n_sub_of,
+                                                           MgImpactRecord* packed, uint32_t cap, uint32_t* cursor,
+                                                           uint2* table) {
+  __shared__ uint32_t base, total;
+  const uint32_t mill = blockIdx.x;
+  const MillDev& m = mills[mill];
+  const uint32_t ns = n_sub_of[mill];
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (uint32_t s = 0; s < ns; ++s) t += min(m.out[s].n_impacts, m.cap_impacts);
+    total = t;
+    base = atomicAdd(cursor, t);
+    table[mill] = make_uint2(base, t);
+  }
+  __syncthreads();
+  uint32_t o = base;
+  for (uint32_t s = 0; s < ns; ++s) {
+    const uint32_t ni = min(m.out[s].n_impacts, m.cap_impacts);
+    const MgImpactRecord* src = m.impacts + (size_t)s * m.cap_impacts;
+    for (uint32_t r = threadIdx.x; r < ni; r += blockDim.x)
+      if (o + r < cap) packed[o + r] = src[r];
+    o += ni;
+  }
+}
+
+cudaError_t launch_pack_impacts(const MillDev* mills, uint32_t n_mills, const uint32_t* n_sub_of,
+                                MgImpactRecord* packed, uint32_t cap, uint32_t* cursor, uint2* table,
+                                cudaStream_t stream) {
+  pack_impacts_kernel<<<n_mills, 256, 0, stream>>>(mills, n_sub_of, packed, cap, cursor, table);
   return cudaGetLastError();
 }
 

@@ -5,11 +5,21 @@
 
 namespace mg {
 
-// Runs n_sub coupled sub-steps on each of n_mills mills (one block per mill). uni holds one
-// StepUniform per mill; angles holds n_mills * n_sub SubAngles, mill-major.
-// smem_bytes of dynamic shared memory hold the staged ball state (MillDev::smem_balls * 24 bytes).
+// Runs coupled sub-steps on each of n_mills mills (one block per mill): n_sub_of[b] of them on
+// mill b when n_sub_of is given, else n_sub. uni holds one StepUniform per mill; angles holds
+// n_mills * n_sub SubAngles, mill-major (n_sub is the stride). Each mill's sticky error word is
+// cleared at the start of the launch. smem_bytes of dynamic shared memory must be at least every
+// mill's MillDev::smem_bytes.
 cudaError_t launch_substeps(const MillDev* mills, uint32_t n_mills, StepUniform* uni, const SubAngles* angles,
-                            uint32_t n_sub, uint32_t threads, size_t smem_bytes, cudaStream_t stream);
+                            uint32_t n_sub, const uint32_t* n_sub_of, uint32_t threads, size_t smem_bytes,
+                            cudaStream_t stream);
+// Packs the impact records of n_mills mills after a launch: mill b's records of its sub-steps
+// 0..n_sub_of[b]-1 (StepOut::n_impacts each, at most cap_impacts) are appended in sub-step order
+// at an offset taken from *cursor (one atomic per mill); table[b] = {offset, count}. Records that
+// would pass `cap` are not written (the count still is).
+cudaError_t launch_pack_impacts(const MillDev* mills, uint32_t n_mills, const uint32_t* n_sub_of,
+                                MgImpactRecord* packed, uint32_t cap, uint32_t* cursor, uint2* table,
+                                cudaStream_t stream);
 // Largest dynamic shared-memory allotment of a launch. The region holds, one phase at a time,
 // the fluid positions and velocities plus completion flags of the drag / buoyancy sweeps
 // (16 nf + 4 nb bytes) and the ball state of the DEM sweeps (24 nb bytes); it is sized to the

@@ -101,7 +101,8 @@ class Simulation:
 
     def close(self):
         if getattr(self, "h", None):
-            self.lib.sim_destroy(self.h)
+            if getattr(self, "_owned", True):
+                self.lib.sim_destroy(self.h)
             self.h = None
 
     def __del__(self):
