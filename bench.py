@@ -321,7 +321,9 @@ def run_device(args):
                              "kernel": "mill_substeps_kernel (one launch per frame)",
                              "kernel_ms_per_launch": k_ms, "algorithmic_bytes_per_launch": per_launch_bytes},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
-                "gpu_launches": args.steps, "clocks": clocks, "stage_us_per_substep": stages}
+                "gpu_launches": args.steps, "clocks": clocks, "stage_us_per_substep": stages,
+                "counters_per_substep": {f: round(tot[q] / max(nsum.value, 1), 2) for q, (f, _) in
+                                         enumerate(capi.StepCounters._fields_) if f != "reserved0"}}
         if args.batch_mills > 0:
             line["batched"] = run_batched(lib, b, args)
         if not args.no_cpu_baseline:

@@ -232,8 +232,8 @@ STAGE_NAMES = [
     "viscosity: CG solve (+ ball bookkeeping)", "mean_shear_rate", "fluid clamps/other (7.5-8)", "DEM step",
     "DEM: predict + broad phase + CCD", "DEM: projection sweeps", "DEM: friction", "DEM: restitution + rolling",
     "drag alone (6.5)", "DEM: projection predecessors", "DEM: projection levels", "DEM: level bucketing",
-    "unused (23)", "drag: item lists", "drag: predecessors", "drag: sweep", "buoyancy: item lists",
-    "buoyancy: predecessors", "buoyancy: sweep", "DEM: contact ordering", "unused (31)",
+    "viscosity: CG setup (joint)", "drag: item lists", "drag: predecessors", "drag: sweep", "buoyancy: item lists",
+    "buoyancy: predecessors", "buoyancy: sweep", "DEM: contact ordering", "viscosity: CG iterations (joint)",
     "drag sweep: ball prefetch (sum)", "drag sweep: ball waits (sum)", "drag sweep: ball chain work (sum)",
     "buoyancy sweep: ball prefetch (sum)", "buoyancy sweep: ball waits (sum)",
     "buoyancy sweep: ball chain work (sum)", "unused (38)", "unused (39)"]

@@ -144,8 +144,41 @@ __device__ inline uint32_t block_exclusive_scan(uint32_t* a, uint32_t m) {
   return total;
 }
 
-// Insertion sort of a short segment (ascending).
+// Sorts a[0..n), n <= N, in registers: one batch of loads, a bitonic network (the tail padded
+// with the largest value), one batch of stores.
+template <int N>
+__device__ __forceinline__ void reg_sort_u32(uint32_t* a, uint32_t n) {
+  uint32_t v[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) v[k] = (uint32_t)k < n ? a[k] : 0xFFFFFFFFu;
+#pragma unroll
+  for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        const int l = i ^ j;
+        if (l > i) {
+          const bool up = (i & k) == 0;
+          const uint32_t x = v[i], y = v[l];
+          if ((x > y) == up) {
+            v[i] = y;
+            v[l] = x;
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+    if ((uint32_t)k < n) a[k] = v[k];
+}
+
+// Sort of a short segment (ascending): in registers up to 32 entries, else insertion sort.
 __device__ __forceinline__ void small_sort_u32(uint32_t* a, uint32_t n) {
+  if (n <= 1) return;
+  if (n <= 8) { reg_sort_u32<8>(a, n); return; }
+  if (n <= 32) { reg_sort_u32<32>(a, n); return; }
   for (uint32_t i = 1; i < n; ++i) {
     uint32_t v = a[i];
     uint32_t j = i;

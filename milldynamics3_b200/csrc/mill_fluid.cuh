@@ -116,19 +116,19 @@ __device__ __forceinline__ double resolved_ratio(double hc) {
 // One squeeze link candidate (ball i, partner j or wall); returns false when not in range.
 struct LinkEval { bool in_range, emit; V2 n; float c; };
 
-__device__ __forceinline__ LinkEval link_pair(const MillDev& m, const StepUniform& U, uint32_t i, uint32_t j,
+// Ball i at xi with viscous start velocity v0i against ball j (xj, v0j).
+__device__ __forceinline__ LinkEval link_pair(const MillDev& m, const StepUniform& U, V2 xi, V2 v0i, V2 xj, V2 v0j,
                                               float reach, float range2, double dxd, float c_max, bool need_c = true) {
   LinkEval L{false, false, V2(), 0.0f};
   float r = m.b_r;
-  V2 xi(m.bx[i]);
-  V2 e = V2(m.bx[j]) - xi;
+  V2 e = xj - xi;
   if (e.len2() >= range2 || !e.finite()) return L;
   float dist = e.len();
   float gap = dist - 2.0f * r;
   if (gap >= reach || dist < 1e-9f) return L;
   L.in_range = true;
   L.n = e / dist;
-  if (L.n.dot(V2(m.ball_v0[i]) - V2(m.ball_v0[j])) <= 0.0f) return L;
+  if (L.n.dot(v0i - v0j) <= 0.0f) return L;
   L.emit = true;
   if (!need_c) return L;
   double weight = 1.0 - resolved_ratio((double)gap / dxd);
@@ -419,26 +419,27 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
         bool overflow = false;
         const V2 xb(m.bx[b]);
         if (xb.finite()) {
-          for (uint32_t q = 0; q < count_pb; ++q) {
-            const V2 bp = xb + U.boundary_offset[q];
-            warp_near_chunks(S.hA, m.gA, bp, [&](uint32_t j, uint32_t, bool valid) {
-              bool acc = false;
-              float w = 0.0f;
-              V2 dir;
-              if (valid) {
-                V2 delta = bp - V2(X[j]);
-                float r2 = delta.len2();
-                if (!(r2 >= range2 || r2 <= inner2)) {
-                  float r = sqrtf(r2);
-                  if (!(!finite_f(r) || r <= 0.5f * h_adh || r >= h_adh)) {
-                    w = mass * adhesion_kernel(r, h_adh) / rho0;
-                    if (w > 0.0f) { acc = true; dir = w * (delta / r); }
+          warp_near_multi(
+              S.hA, m.gA, count_pb, [&](uint32_t q) { return xb + U.boundary_offset[q]; },
+              [&](uint32_t j, bool valid) { return valid ? V2(X[j]) : V2(); },
+              [&](uint32_t j, uint32_t q, V2 xj, bool valid) {
+                bool acc = false;
+                float w = 0.0f;
+                V2 dir;
+                if (valid) {
+                  const V2 bp = xb + U.boundary_offset[q];
+                  V2 delta = bp - xj;
+                  float r2 = delta.len2();
+                  if (!(r2 >= range2 || r2 <= inner2)) {
+                    float r = sqrtf(r2);
+                    if (!(!finite_f(r) || r <= 0.5f * h_adh || r >= h_adh)) {
+                      w = mass * adhesion_kernel(r, h_adh) / rho0;
+                      if (w > 0.0f) { acc = true; dir = w * (delta / r); }
+                    }
                   }
                 }
-              }
-              warp_merge(acc, j, w, dir, 0.0f, slot, L, cnt, overflow);
-            });
-          }
+                warp_merge(acc, j, w, dir, 0.0f, slot, L, cnt, overflow);
+              });
         }
         for (uint32_t s = lane; s < min(cnt, m.cap_items); s += 32) slot[L.j[s]] = NONE;
         __syncwarp();
@@ -648,12 +649,15 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
         uint32_t cnt = 0;
         const V2 xb(m.bx[b]);
         if (xb.finite()) {
-          warp_near_chunks(S.hB, m.gB, xb, [&](uint32_t j, uint32_t, bool valid) {
+          warp_near_multi(
+              S.hB, m.gB, 1u, [&](uint32_t) { return xb; },
+              [&](uint32_t j, bool valid) { return valid ? V2(X[j]) : V2(); },
+              [&](uint32_t j, uint32_t, V2 xj, bool valid) {
             bool keep = false;
             V2 r_i;
             float phi = 0.0f;
             if (valid) {
-              r_i = V2(X[j]) - xb;
+              r_i = xj - xb;
               float r2 = r_i.len2();
               if (!(!finite_f(r2) || r2 >= h_c * h_c)) {
                 phi = poly6(r2, h_c) / w_hc0;
@@ -870,9 +874,12 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       const V2 xb(m.bx[b]);
       float rho_local = 0.0f;
       if (xb.finite()) {
-        warp_near_chunks(S.hA, m.gA, xb, [&](uint32_t j, uint32_t, bool valid) {
+        warp_near_multi(
+            S.hA, m.gA, 1u, [&](uint32_t) { return xb; },
+            [&](uint32_t j, bool valid) { return valid ? V2(X[j]) : V2(); },
+            [&](uint32_t j, uint32_t, V2 xj, bool valid) {
           float w = 0.0f;
-          if (valid) w = mass * poly6((xb - V2(X[j])).len2(), h);
+          if (valid) w = mass * poly6((xb - xj).len2(), h);
           const bool keep = w > 0.0f;
           const uint32_t bal = __ballot_sync(FULL, keep);
           const uint32_t pos = cnt + __popc(bal & ((1u << lane) - 1u));
@@ -1102,32 +1109,44 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
         bool overflow = false;
         const V2 xb(m.bx[b]);
         if (xb.finite()) {
-          for (uint32_t q = 0; q < count_pb; ++q) {
-            const V2 bp = xb + U.boundary_offset[q];
-            warp_near_chunks(S.hB, m.gB, bp, [&](uint32_t j, uint32_t, bool valid) {
-              bool acc = false;
-              float c = 0.0f, lever2_c = 0.0f;
-              V2 lever_c;
-              if (valid) {
-                V2 delta = V2(X[j]) - bp;
-                float r2 = delta.len2();
-                if (!(r2 >= range2)) {
-                  float r = sqrtf(r2);
-                  if (!(!finite_f(r) || r >= h || r <= 1e-9f)) {
-                    float dot_abs = fabsf(spiky_norm * (h - r) * (h - r) * r);
-                    c = m.f_tmp[j] * dot_abs / (r2 + eta2);
-                    if (c > 0.0f) {
-                      acc = true;
-                      V2 lever = bp - xb;
-                      lever_c = c * lever;
-                      lever2_c = c * lever.len2();
+          struct XF {
+            V2 x;
+            float f;
+          };
+          warp_near_multi(
+              S.hB, m.gB, count_pb, [&](uint32_t q) { return xb + U.boundary_offset[q]; },
+              [&](uint32_t j, bool valid) {
+                XF d{V2(), 0.0f};
+                if (valid) {
+                  d.x = V2(X[j]);
+                  d.f = m.f_tmp[j];
+                }
+                return d;
+              },
+              [&](uint32_t j, uint32_t q, XF d, bool valid) {
+                bool acc = false;
+                float c = 0.0f, lever2_c = 0.0f;
+                V2 lever_c;
+                if (valid) {
+                  const V2 bp = xb + U.boundary_offset[q];
+                  V2 delta = d.x - bp;
+                  float r2 = delta.len2();
+                  if (!(r2 >= range2)) {
+                    float r = sqrtf(r2);
+                    if (!(!finite_f(r) || r >= h || r <= 1e-9f)) {
+                      float dot_abs = fabsf(spiky_norm * (h - r) * (h - r) * r);
+                      c = d.f * dot_abs / (r2 + eta2);
+                      if (c > 0.0f) {
+                        acc = true;
+                        V2 lever = bp - xb;
+                        lever_c = c * lever;
+                        lever2_c = c * lever.len2();
+                      }
                     }
                   }
                 }
-              }
-              warp_merge(acc, j, c, lever_c, lever2_c, slot, L, cnt, overflow);
-            });
-          }
+                warp_merge(acc, j, c, lever_c, lever2_c, slot, L, cnt, overflow);
+              });
         }
         for (uint32_t s = lane; s < min(cnt, m.cap_items); s += 32) slot[L.j[s]] = NONE;
         __syncwarp();
@@ -1173,14 +1192,27 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       for (int pass = 0; pass < 2; ++pass) {
         for (uint32_t i = tid() >> 5; i < nb; i += nthr() >> 5) {
           const uint32_t lane = tid() & 31u;
-          const V2 xi(m.bx[i]);
+          const V2 xi(m.bx[i]), v0i(m.ball_v0[i]);
           uint32_t c = 0, inr = 0;
           const uint32_t o = pass ? m.l_off[i] : 0u;
           if (xi.finite()) {
-            warp_near_chunks(S.hBall, m.gBall, xi, [&](uint32_t j, uint32_t, bool valid) {
+            struct XV {
+              V2 x, v0;
+            };
+            warp_near_multi(
+                S.hBall, m.gBall, 1u, [&](uint32_t) { return xi; },
+                [&](uint32_t j, bool valid) {
+                  XV d{V2(), V2()};
+                  if (valid && j > i) {
+                    d.x = V2(m.bx[j]);
+                    d.v0 = V2(m.ball_v0[j]);
+                  }
+                  return d;
+                },
+                [&](uint32_t j, uint32_t, XV d, bool valid) {
               const bool cand = valid && j > i;
               LinkEval L{false, false, V2(), 0.0f};
-              if (cand) L = link_pair(m, U, i, j, reach, range2, dxd, c_max, pass == 1);
+              if (cand) L = link_pair(m, U, xi, v0i, d.x, d.v0, reach, range2, dxd, c_max, pass == 1);
               inr += __popc(__ballot_sync(FULL, cand && L.in_range));
               const uint32_t bal = __ballot_sync(FULL, cand && L.emit);
               if (pass && cand && L.emit) {
@@ -1314,6 +1346,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       __syncthreads();
       double b_norm = block_res_norm(bvec, inv, len, fp64, S);
       double r_norm = block_res_norm(r, inv, len, fp64, S);
+      stage_mark(out.stage, 23);
       double tol_b = fp64 ? (double)VISC_CG_TOL * b_norm : (double)(VISC_CG_TOL * (float)b_norm);
       if (b_norm > 0.0 && isfinite(b_norm) && r_norm > tol_b) {
         for (uint32_t e = tid(); e < len; e += nthr()) p[e] = z[e];
@@ -1340,6 +1373,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
           rz_old = rz_new;
         }
       }
+      stage_mark(out.stage, 31);
       for (uint32_t i = tid(); i < n; i += nthr()) {
         V2 vn(x[i]);
         V[i] = vn.f2();
@@ -1347,20 +1381,32 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
         m.fguess[i] = (d.finite() ? d : V2()).f2();
       }
       __syncthreads();
-      if (tid() == 0) {
-        m.guess_valid_dev[0] = 1u;
-        V2 mom(S.fscal[0], S.fscal[1]);
-        for (uint32_t b = 0; b < nb; ++b) {
+      // ball impulses from the solved velocities (pbf.rs:2237-2298), one thread per ball
+      for (uint32_t b = tid(); b < nb; b += nthr()) {
+        V2 dv = V2(x[n + b]) - V2(m.ball_v0[b]);
+        float dw = x[n + nb + b].x - m.ball_w0[b];
+        if (dv.finite() && finite_f(dw)) {
+          m.imp[b] = (V2(m.imp[b]) + m.b_m * dv).f2();
+          m.ang[b] += m.b_I * dw;
+        }
+      }
+      if (tid() == 0) m.guess_valid_dev[0] = 1u;
+      if (U.want_momentum && tid() < 32) {
+        // the fluid's momentum change loses b_m * dv per ball, in ball order (a - t == a + (-t))
+        auto term = [&](uint32_t b, float& t, int c) {
           V2 dv = V2(x[n + b]) - V2(m.ball_v0[b]);
           float dw = x[n + nb + b].x - m.ball_w0[b];
-          if (dv.finite() && finite_f(dw)) {
-            m.imp[b] = (V2(m.imp[b]) + m.b_m * dv).f2();
-            m.ang[b] += m.b_I * dw;
-            mom -= m.b_m * dv;
-          }
+          if (!(dv.finite() && finite_f(dw))) return false;
+          V2 p = m.b_m * dv;
+          t = -(c ? p.y : p.x);
+          return true;
+        };
+        const float mx = warp_ordered_sum(S.fscal[0], nb, [&](uint32_t b, float& t) { return term(b, t, 0); });
+        const float my = warp_ordered_sum(S.fscal[1], nb, [&](uint32_t b, float& t) { return term(b, t, 1); });
+        if (tid() == 0) {
+          S.fscal[0] = mx;
+          S.fscal[1] = my;
         }
-        S.fscal[0] = mom.x;
-        S.fscal[1] = mom.y;
       }
       __syncthreads();
     }

@@ -206,6 +206,69 @@ __device__ __forceinline__ void warp_near_chunks(const GridHdr& hdr, const GridB
   }
 }
 
+// for_each_near over several query points in turn (point 0's candidates, then point 1's, ...), as
+// the per-ball boundary-point loops of pbf.rs:1540-1577 and 2166-2228 visit them, three points
+// (27 cell ranges, one per lane) at a time. Lane l of a chunk holds candidate pos = chunk start + l,
+// located by a shuffle binary search over the ranges' inclusive prefix. fetch(j, valid) loads
+// what f needs of candidate j; it runs one chunk ahead of f, so the next chunk's loads are in
+// flight while f works. f(j, q, data, valid) gets the point index q; f may use warp collectives.
+template <class PointOf, class Fetch, class F>
+__device__ __forceinline__ void warp_near_multi(const GridHdr& hdr, const GridBuf& gb, uint32_t npts, PointOf point_of,
+                                                Fetch fetch, F f) {
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t q0 = 0; q0 < npts; q0 += 3) {
+    const uint32_t nq = min(3u, npts - q0);
+    uint32_t s = 0, cnt = 0;
+    if (lane < 9u * nq && hdr.npoints > 0) {
+      const uint32_t c9 = lane % 9u;
+      const V2 p = point_of(q0 + lane / 9u);
+      if (p.finite()) {
+        const int2 c = cell_key(p, hdr.cell);
+        const int2 k = make_int2(sat_add(c.x, (int)(c9 % 3u) - 1), sat_add(c.y, (int)(c9 / 3u) - 1));
+        bool dup = false;
+        for (uint32_t u = 0; u < c9; ++u)
+          dup = dup || key_eq(k, make_int2(sat_add(c.x, (int)(u % 3u) - 1), sat_add(c.y, (int)(u / 3u) - 1)));
+        uint32_t e;
+        if (!dup && cell_range(hdr, gb, k, s, e)) cnt = e - s;
+      }
+    }
+    uint32_t incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if ((int)lane >= o) incl += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    // range r of position pos: the number of ranges whose inclusive prefix is <= pos
+    auto locate = [&](uint32_t pos, uint32_t& j, uint32_t& q) {
+      uint32_t r = 0;
+      for (uint32_t step = 16; step > 0; step >>= 1) {
+        const uint32_t v = __shfl_sync(0xffffffffu, incl, (int)(r + step - 1u));
+        if (v <= pos) r += step;
+      }
+      const uint32_t rs = __shfl_sync(0xffffffffu, s, (int)r), ri = __shfl_sync(0xffffffffu, incl, (int)r);
+      const uint32_t rc = __shfl_sync(0xffffffffu, cnt, (int)r);
+      q = q0 + r / 9u;
+      j = pos < total ? gb.indices[rs + (pos - (ri - rc))] : NONE;
+    };
+    uint32_t j, q;
+    locate(lane, j, q);
+    auto d = fetch(j, lane < total);
+    for (uint32_t c0 = 0; c0 < total; c0 += 32) {
+      const uint32_t nxt = c0 + 32u;
+      uint32_t jn = NONE, qn = q0;
+      decltype(d) dn{};
+      if (nxt < total) {
+        locate(nxt + lane, jn, qn);
+        dn = fetch(jn, nxt + lane < total);
+      }
+      f(j, q, d, c0 + lane < total);
+      j = jn;
+      q = qn;
+      d = dn;
+    }
+  }
+}
+
 // The cells a point's neighbour list visits, in the order build_neighbor_lists (pbf.rs:262-288)
 // produces: the forward-offset sweep of for_each_candidate_pair (grid.rs:291-362) reaches a point
 // in cell C from (-1,-1), (-1,0), (0,-1) before C's own pairs, then C's targets (+1,0), (+1,+1),

@@ -268,6 +268,8 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
   }
   // the merge slot maps are kept all-NONE between uses
   cudaMemsetAsync(m.slot, 0xFF, sizeof(uint32_t) * (size_t)16 * cf, s->stream);
+  // the clears must land before anything else touches the arena, whichever stream it uses
+  CK(cudaStreamSynchronize(s->stream));
   m.nf = nf;
   m.nb = nb;
   s->md = m;
@@ -828,8 +830,9 @@ int mg_set_balls(MgSim* s, uint32_t n, const float* x, const float* v, const flo
     std::vector<float> guess(2 * (size_t)s->nf);
     uint32_t gv = 0;
     if (!rc && s->nf) {
-      CK(cudaMemcpy(guess.data(), s->md.fguess, 8 * (size_t)s->nf, cudaMemcpyDeviceToHost));
-      CK(cudaMemcpy(&gv, s->md.guess_valid_dev, 4, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpyAsync(guess.data(), s->md.fguess, 8 * (size_t)s->nf, cudaMemcpyDeviceToHost, s->stream));
+      CK(cudaMemcpyAsync(&gv, s->md.guess_valid_dev, 4, cudaMemcpyDeviceToHost, s->stream));
+      CK(cudaStreamSynchronize(s->stream));
     }
     uint32_t nf = s->nf;
     if (!rc) rc = alloc_state(s, nf, n);
@@ -854,7 +857,8 @@ int mg_get_fluid(MgSim* s, float* x, float* v, float* dye, float* guess, uint32_
   if (!s) return fail_global(MG_ERR_ARG, "null handle");
   size_t n = s->nf;
   uint32_t gv = 0;
-  CK(cudaMemcpy(&gv, s->md.guess_valid_dev, 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpyAsync(&gv, s->md.guess_valid_dev, 4, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
   if (guess_len) *guess_len = gv ? (uint32_t)n : 0u;
   if (!n) return MG_OK;
   if (x) CK(cudaMemcpyAsync(x, s->md.fx, 8 * n, cudaMemcpyDeviceToHost, s->stream));
@@ -1058,7 +1062,7 @@ static int probe(const float* xy, uint32_t n, float cell, int mode, MgSim** out_
   // the probe grid lives in the fluid-side buffers; the pair buffers are sized by the ball count
   if (!rc) rc = alloc_state(s, n, std::max(n, 1u));
   if (!rc && n) {
-    cudaError_t e = cudaMemcpy(s->md.fx, xy, 8 * (size_t)n, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpyAsync(s->md.fx, xy, 8 * (size_t)n, cudaMemcpyHostToDevice, s->stream);
     if (e != cudaSuccess) rc = fail(s, MG_ERR_CUDA, "%s", cudaGetErrorString(e));
   }
   s->nb = 0;

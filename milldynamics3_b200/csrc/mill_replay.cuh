@@ -286,24 +286,36 @@ __device__ __forceinline__ void warp_merge(bool acc, uint32_t j, float v0, V2 v1
     if (g < L.cap) { slot[j] = g; L.j[g] = j; } else { overflow = true; }
   }
   cnt += __popc(newmask);
-  // the leader of each j accumulates its peers' values in lane order
+  // the leader of each j (its lowest lane) takes its own value (a new item) or adds it to the
+  // stored one, then adds its peers' values in lane order; the rounds run over the largest peer
+  // group of the chunk, each round one shuffle per value for all leaders at once
   float a0 = 0.0f, a2 = 0.0f;
   V2 a1;
-  if (acc && lane == leader && !is_new && g < L.cap) {
-    a0 = L.v0[g];
-    a1 = V2(L.v1[g]);
-    if (L.v2) a2 = L.v2[g];
+  const bool lead = acc && lane == leader;
+  if (lead) {
+    if (is_new) {
+      a0 = v0;
+      a1 = v1;
+      a2 = v2;
+    } else if (g < L.cap) {
+      a0 = L.v0[g] + v0;
+      const V2 s1(L.v1[g]);
+      a1 = V2(s1.x + v1.x, s1.y + v1.y);
+      a2 = (L.v2 ? L.v2[g] : 0.0f) + v2;
+    }
   }
-  uint32_t vmask = __ballot_sync(FULL, acc);
-  while (vmask) {
-    const int t = __ffs(vmask) - 1;
-    vmask &= vmask - 1u;
+  uint32_t rest = lead ? (peers & (peers - 1u)) : 0u;
+  const uint32_t rounds = __reduce_max_sync(FULL, (uint32_t)__popc(rest));
+  for (uint32_t k = 0; k < rounds; ++k) {
+    const int t = rest ? __ffs(rest) - 1 : (int)lane;
     const float t0 = __shfl_sync(FULL, v0, t), t1x = __shfl_sync(FULL, v1.x, t), t1y = __shfl_sync(FULL, v1.y, t);
     const float t2 = __shfl_sync(FULL, v2, t);
-    const uint32_t lt = __shfl_sync(FULL, leader, t);
-    if (lane == lt) {
-      if (is_new && t == (int)lane) { a0 = t0; a1 = V2(t1x, t1y); a2 = t2; }
-      else { a0 += t0; a1.x += t1x; a1.y += t1y; a2 += t2; }
+    if (rest) {
+      a0 += t0;
+      a1.x += t1x;
+      a1.y += t1y;
+      a2 += t2;
+      rest &= rest - 1u;
     }
   }
   if (acc && lane == leader && g < L.cap) {
