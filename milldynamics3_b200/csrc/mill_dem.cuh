@@ -66,10 +66,14 @@ __device__ float mech_energy_seq(const MillDev& m, const float2* X, const float2
       g = m.b_m * fabsf(GRAVITY) * X[i].y;
     }
     uint32_t lim = min(32u, m.nb - c);
-    for (uint32_t t = 0; t < lim; ++t) {
-      e += __shfl_sync(FULL, a, t);
-      e += __shfl_sync(FULL, b, t);
-      e += __shfl_sync(FULL, g, t);
+#pragma unroll
+    for (uint32_t t = 0; t < 32; ++t) {
+      const float at = __shfl_sync(FULL, a, t), bt = __shfl_sync(FULL, b, t), gt = __shfl_sync(FULL, g, t);
+      if (t < lim) {
+        e += at;
+        e += bt;
+        e += gt;
+      }
     }
   }
   return e;
@@ -358,12 +362,14 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
       bool wall = k < na && m.act_j[k] == NONE && m.act_bin[k] != -2;
       act += (k < na && m.act_j[k] != NONE) ? 1u : 0u;
       float a = wall ? m.act_w1[k] : 0.0f, b = wall ? m.act_w2[k] : 0.0f;
-      uint32_t mask = __ballot_sync(FULL, wall);
-      while (mask) {
-        int t = __ffs(mask) - 1;
-        mask &= mask - 1;
-        wall_work += __shfl_sync(FULL, a, t);
-        wall_work += __shfl_sync(FULL, b, t);
+      const uint32_t mask = __ballot_sync(FULL, wall);
+#pragma unroll
+      for (int t = 0; t < 32; ++t) {
+        const float at = __shfl_sync(FULL, a, t), bt = __shfl_sync(FULL, b, t);
+        if ((mask >> t) & 1u) {
+          wall_work += at;
+          wall_work += bt;
+        }
       }
     }
     act = warp_sum(act);

@@ -85,7 +85,9 @@ __device__ double block_res_norm(const float2* r, const float* inv, uint32_t len
 __device__ __forceinline__ V2 laplacian_row(const MillDev& m, const float2* v, uint32_t i) {
   V2 sum;
   V2 vi(v[i]);
-  for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
+  const uint32_t k0 = m.nbr_off[i], k1 = m.nbr_off[i + 1];
+#pragma unroll 4
+  for (uint32_t k = k0; k < k1; ++k) {
     uint32_t j = m.nbrs[k];
     V2 e(m.visc_dir[k]);
     sum += (CENTRAL_VISC * m.visc_w[k] * e.dot(vi - V2(v[j]))) * e;
@@ -164,9 +166,13 @@ __device__ void joint_apply(const MillDev& m, float dt, const float2* xx, float2
   float k = dt * mass;
   for (uint32_t i = tid(); i < n; i += nthr()) m.cg_lv[i] = laplacian_row(m, xx, i).f2();
   __syncthreads();
+  // (the loops are unrolled so that the independent loads of consecutive terms overlap; the
+  // additions keep their order)
   for (uint32_t i = tid(); i < n; i += nthr()) {
     V2 o = mass * (V2(xx[i]) + dt * V2(m.cg_lv[i]));
-    for (uint32_t q = m.fg_start[i]; q < m.fg_start[i + 1]; ++q) {
+    const uint32_t q0 = m.fg_start[i], q1 = m.fg_start[i + 1];
+#pragma unroll 4
+    for (uint32_t q = q0; q < q1; ++q) {
       uint32_t g = m.fg_list[q];
       uint32_t bi = m.g_ball[g];
       V2 vb(xx[n + bi]);
@@ -183,7 +189,9 @@ __device__ void joint_apply(const MillDev& m, float dt, const float2* xx, float2
     float w = xx[n + nb + bi].x;
     V2 o = m.b_m * vb;
     float oa = m.b_I * w;
-    for (uint32_t g = m.g_off[bi]; g < m.g_off[bi + 1]; ++g) {
+    const uint32_t g0 = m.g_off[bi], g1 = m.g_off[bi + 1];
+#pragma unroll 4
+    for (uint32_t g = g0; g < g1; ++g) {
       uint32_t i = m.g_fluid[g];
       V2 rel = V2(xx[i]) - vb;
       V2 lc(m.g_lc[g]);
@@ -191,14 +199,18 @@ __device__ void joint_apply(const MillDev& m, float dt, const float2* xx, float2
       o -= d;
       oa -= k * (cross2(lc, rel) - w * m.g_l2[g]);
     }
-    for (uint32_t q = m.lo_start[bi]; q < m.lo_start[bi + 1]; ++q) {
+    const uint32_t lq0 = m.lo_start[bi], lq1 = m.lo_start[bi + 1];
+#pragma unroll 4
+    for (uint32_t q = lq0; q < lq1; ++q) {
       uint32_t l = m.lo_list[q];
       V2 rel = V2(xx[n + m.l_ball[l]]) - vb;
       V2 ln(m.l_n[l]);
       V2 d = (dt * m.l_c[l] * ln.dot(rel)) * ln;
       o -= d;
     }
-    for (uint32_t l = m.l_off[bi]; l < m.l_off[bi + 1]; ++l) {
+    const uint32_t l0 = m.l_off[bi], l1 = m.l_off[bi + 1];
+#pragma unroll 4
+    for (uint32_t l = l0; l < l1; ++l) {
       uint32_t other = m.l_other[l];
       V2 rel = vb;
       if (other != NONE) rel = rel - V2(xx[n + other]);
@@ -453,10 +465,15 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
             float ww = 0.0f;
             V2 dd;
             if (s < cnt) { ww = L.v0[s]; dd = V2(L.v1[s]); }
-            for (uint32_t t = 0; t < lim; ++t) {
-              dsx += __shfl_sync(FULL, dd.x, t);
-              dsy += __shfl_sync(FULL, dd.y, t);
-              weight_sum += __shfl_sync(FULL, ww, t);
+#pragma unroll
+            for (uint32_t t = 0; t < 32; ++t) {
+              const float xt = __shfl_sync(FULL, dd.x, t), yt = __shfl_sync(FULL, dd.y, t);
+              const float wt = __shfl_sync(FULL, ww, t);
+              if (t < lim) {
+                dsx += xt;
+                dsy += yt;
+                weight_sum += wt;
+              }
             }
           }
           V2 dir_sum(dsx, dsy);
@@ -542,16 +559,18 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
         bin = m.wall_bin[c + lane];
         if (bin >= 0) { val = m.wall_val[c + lane]; px = m.dv_tmp[c + lane].x; py = m.dv_tmp[c + lane].y; pa = m.f_tmp[c + lane]; }
       }
-      uint32_t mask = __ballot_sync(FULL, bin >= 0);
-      while (mask) {
-        int t = __ffs(mask) - 1;
-        mask &= mask - 1;
-        int bt = __shfl_sync(FULL, bin, t);
-        float vt = __shfl_sync(FULL, val, t);
-        ix += (double)__shfl_sync(FULL, px, t);
-        iy += (double)__shfl_sync(FULL, py, t);
-        ia += (double)__shfl_sync(FULL, pa, t);
-        if (bt == lane) bin_acc += vt;
+      const uint32_t mask = __ballot_sync(FULL, bin >= 0);
+#pragma unroll
+      for (int t = 0; t < 32; ++t) {
+        const int bt = __shfl_sync(FULL, bin, t);
+        const float vt = __shfl_sync(FULL, val, t), xt = __shfl_sync(FULL, px, t), yt = __shfl_sync(FULL, py, t);
+        const float at = __shfl_sync(FULL, pa, t);
+        if ((mask >> t) & 1u) {
+          ix += (double)xt;
+          iy += (double)yt;
+          ia += (double)at;
+          if (bt == lane) bin_acc += vt;
+        }
       }
     }
     out.fs.wall_normal_impulse_by_angle[lane] = bin_acc;
@@ -597,14 +616,17 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
           jy = mass * dv.y;
           ja = cross2(x, mass * dv);
         }
-        uint32_t mask = __ballot_sync(FULL, touched);
-        while (mask) {
-          int t = __ffs(mask) - 1;
-          mask &= mask - 1;
-          work += __shfl_sync(FULL, wk, t);
-          ix += (double)__shfl_sync(FULL, jx, t);
-          iy += (double)__shfl_sync(FULL, jy, t);
-          ia += (double)__shfl_sync(FULL, ja, t);
+        const uint32_t mask = __ballot_sync(FULL, touched);
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+          const float wt = __shfl_sync(FULL, wk, t), xt = __shfl_sync(FULL, jx, t), yt = __shfl_sync(FULL, jy, t);
+          const float at = __shfl_sync(FULL, ja, t);
+          if ((mask >> t) & 1u) {
+            work += wt;
+            ix += (double)xt;
+            iy += (double)yt;
+            ia += (double)at;
+          }
         }
       }
       __syncwarp();
@@ -884,7 +906,11 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
           const uint32_t bal = __ballot_sync(FULL, keep);
           const uint32_t pos = cnt + __popc(bal & ((1u << lane) - 1u));
           if (keep && pos < m.cap_items) { m.item_j[base + pos] = j; m.item_w[base + pos] = w; }
-          for (uint32_t mk = bal; mk; mk &= mk - 1u) rho_local += __shfl_sync(FULL, w, __ffs(mk) - 1);
+#pragma unroll
+          for (int t = 0; t < 32; ++t) {
+            const float wt = __shfl_sync(FULL, w, t);
+            if ((bal >> t) & 1u) rho_local += wt;
+          }
           cnt += __popc(bal);
         });
       }

@@ -47,11 +47,16 @@ __device__ uint32_t compute_levels(uint32_t n, const uint32_t* pred_a, const uin
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
     uint32_t maxl = 0;
+    // the next chunk's predecessors are loaded while this chunk propagates
+    uint32_t a_next = (uint32_t)lane < n ? pred_a[lane] : NONE, b_next = (uint32_t)lane < n ? pred_b[lane] : NONE;
     for (uint32_t c = 0; c < n; c += 32) {
       uint32_t k = c + lane;
+      const uint32_t a = a_next, b = b_next;
+      const uint32_t kn = k + 32;
+      a_next = kn < n ? pred_a[kn] : NONE;
+      b_next = kn < n ? pred_b[kn] : NONE;
       int base = 0, la = -1, lb = -1;
       if (k < n) {
-        uint32_t a = pred_a[k], b = pred_b[k];
         if (a != NONE) { if (a >= c) la = (int)(a - c); else base = max(base, (int)lvl[a] + 1); }
         if (b != NONE) { if (b >= c) lb = (int)(b - c); else base = max(base, (int)lvl[b] + 1); }
       }
@@ -97,12 +102,19 @@ __device__ void bucket_levels(uint32_t n, const uint32_t* lvl, uint32_t nlev, ui
 template <class Exec>
 __device__ void run_levels(uint32_t nlev, const uint32_t* lev_start, Exec exec) {
   if (threadIdx.x < 32) {
+    const uint32_t lane = threadIdx.x;
     uint32_t s = lev_start[0];
-    for (uint32_t l = 0; l < nlev; ++l) {
-      uint32_t e = lev_start[l + 1];
-      for (uint32_t q = s + threadIdx.x; q < e; q += 32) exec(q);
-      s = e;
-      __syncwarp();
+    // the level ends are loaded 32 at a time (one per lane) and handed out by shuffles, so no
+    // memory round trip sits between two levels
+    for (uint32_t b = 0; b < nlev; b += 32) {
+      const uint32_t ends = b + lane < nlev ? lev_start[b + lane + 1] : 0u;
+      const uint32_t cnt = min(32u, nlev - b);
+      for (uint32_t t = 0; t < cnt; ++t) {
+        const uint32_t e = __shfl_sync(FULL, ends, t);
+        for (uint32_t q = s + lane; q < e; q += 32) exec(q);
+        s = e;
+        __syncwarp();
+      }
     }
   }
   __syncthreads();
@@ -251,11 +263,19 @@ __device__ void ball_dataflow(uint32_t nb, const uint32_t* rec_off, const uint32
 
 // In-order sum over the lanes' values t = 0..lim-1 (every lane computes the same chain).
 __device__ __forceinline__ float lane_seq_sum(float acc, float v, uint32_t lim) {
-  for (uint32_t t = 0; t < lim; ++t) acc += __shfl_sync(FULL, v, t);
+#pragma unroll
+  for (uint32_t t = 0; t < 32; ++t) {
+    const float x = __shfl_sync(FULL, v, t);
+    if (t < lim) acc += x;
+  }
   return acc;
 }
 __device__ __forceinline__ double lane_seq_sum(double acc, double v, uint32_t lim) {
-  for (uint32_t t = 0; t < lim; ++t) acc += __shfl_sync(FULL, v, t);
+#pragma unroll
+  for (uint32_t t = 0; t < 32; ++t) {
+    const double x = __shfl_sync(FULL, v, t);
+    if (t < lim) acc += x;
+  }
   return acc;
 }
 
@@ -341,11 +361,13 @@ __device__ __forceinline__ T warp_ordered_sum(T init, uint32_t n, F f) {
   for (uint32_t c = 0; c < n; c += 32) {
     T vn = T(0);
     bool usen = c + 32 + lane < n ? f(c + 32 + lane, vn) : false;
-    uint32_t mask = __ballot_sync(FULL, use);
-    while (mask) {
-      int t = __ffs(mask) - 1;
-      acc += __shfl_sync(FULL, v, t);
-      mask &= mask - 1;
+    const uint32_t mask = __ballot_sync(FULL, use);
+    // the 32 shuffles are independent of one another; only the additions form a chain, in lane
+    // order, skipping the unused lanes
+#pragma unroll
+    for (int t = 0; t < 32; ++t) {
+      const T x = __shfl_sync(FULL, v, t);
+      if ((mask >> t) & 1u) acc += x;
     }
     v = vn;
     use = usen;
