@@ -27,6 +27,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "sub-steps/s (1 mill) & batched mill-frames/s on 1 B200; p50/p99 frame latency"
 UNIT = "sub-steps/s"
+# DRAM bytes (read + write) of one realtime frame launch, from an ncu capture (see profiles/)
+REALTIME_LAUNCH_DRAM_BYTES = 1.392e6 + 0.232e6
 
 
 def dist_env():
@@ -317,7 +319,9 @@ def run_device(args):
                            % (per_launch_bytes / n_sub / 1e6),
                            "ms_per_frame": 1e3 * t / args.steps, "parallelism": "replicas" if world > 1 else "1 mill"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                             "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                             "frac": achieved / hbm, "traffic": REALTIME_LAUNCH_DRAM_BYTES, "peak_kind": peak_kind,
+                             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one realtime "
+                                               "frame launch (profiles/mill_substeps_kernel_realtime.md)",
                              "kernel": "mill_substeps_kernel (one launch per frame)",
                              "kernel_ms_per_launch": k_ms, "algorithmic_bytes_per_launch": per_launch_bytes},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},

@@ -754,11 +754,13 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
               }
 #pragma unroll
               for (uint32_t t = 0; t < 32; ++t) {
+                const float wt = __shfl_sync(FULL, w, t), xt = __shfl_sync(FULL, rw.x, t);
+                const float yt = __shfl_sync(FULL, rw.y, t), it = __shfl_sync(FULL, r2w, t);
                 if (t < lim) {
-                  m_ent += __shfl_sync(FULL, w, t);
-                  rsx += __shfl_sync(FULL, rw.x, t);
-                  rsy += __shfl_sync(FULL, rw.y, t);
-                  i_ent += __shfl_sync(FULL, r2w, t);
+                  m_ent += wt;
+                  rsx += xt;
+                  rsy += yt;
+                  i_ent += it;
                 }
               }
             }
@@ -785,9 +787,10 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
                 }
 #pragma unroll
                 for (uint32_t t = 0; t < 32; ++t) {
+                  const float at = __shfl_sync(FULL, sv, t), st = __shfl_sync(FULL, ss, t);
                   if (t < lim) {
-                    s_acc += __shfl_sync(FULL, sv, t);
-                    s_scale += __shfl_sync(FULL, ss, t);
+                    s_acc += at;
+                    s_scale += st;
                   }
                 }
               }
@@ -814,10 +817,12 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
               }
 #pragma unroll
               for (uint32_t t = 0; t < 32; ++t) {
+                const float xt = __shfl_sync(FULL, vw.x, t), yt = __shfl_sync(FULL, vw.y, t);
+                const float lt = __shfl_sync(FULL, lw, t);
                 if (t < lim) {
-                  vsx += __shfl_sync(FULL, vw.x, t);
-                  vsy += __shfl_sync(FULL, vw.y, t);
-                  l_sum += __shfl_sync(FULL, lw, t);
+                  vsx += xt;
+                  vsy += yt;
+                  l_sum += lt;
                 }
               }
             }
@@ -975,10 +980,9 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
             const uint32_t vmask = __ballot_sync(FULL, valid);
 #pragma unroll
             for (uint32_t t = 0; t < 32; ++t) {
-              if (t < lim) {
-                float c = __shfl_sync(FULL, dvw, t);
-                if ((vmask >> t) & 1u) den += c;
-              }
+              // vmask has no bits from lim on
+              const float c = __shfl_sync(FULL, dvw, t);
+              if ((vmask >> t) & 1u) den += c;
             }
           }
           q.den = den;
@@ -1010,10 +1014,9 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
             const uint32_t vmask = __ballot_sync(FULL, valid);
 #pragma unroll
             for (uint32_t t = 0; t < 32; ++t) {
-              if (t < lim) {
-                float a = __shfl_sync(FULL, nv, t);
-                if ((vmask >> t) & 1u) num += a;
-              }
+              // vmask has no bits from lim on
+              const float a = __shfl_sync(FULL, nv, t);
+              if ((vmask >> t) & 1u) num += a;
             }
           }
           const float den = q.den;
@@ -1214,64 +1217,74 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       grid_build(m.bx, nb, 2.0f * r + reach, m.gBall, S.hBall, err);
       uint32_t in_range = 0;
       // one warp per ball: candidates j > i in for_each_near order, ordered compaction, then the
-      // wall link; pass 0 counts, pass 1 evaluates the films and writes
-      for (int pass = 0; pass < 2; ++pass) {
-        for (uint32_t i = tid() >> 5; i < nb; i += nthr() >> 5) {
-          const uint32_t lane = tid() & 31u;
-          const V2 xi(m.bx[i]), v0i(m.ball_v0[i]);
-          uint32_t c = 0, inr = 0;
-          const uint32_t o = pass ? m.l_off[i] : 0u;
-          if (xi.finite()) {
-            struct XV {
-              V2 x, v0;
-            };
-            warp_near_multi(
-                S.hBall, m.gBall, 1u, [&](uint32_t) { return xi; },
-                [&](uint32_t j, bool valid) {
-                  XV d{V2(), V2()};
-                  if (valid && j > i) {
-                    d.x = V2(m.bx[j]);
-                    d.v0 = V2(m.ball_v0[j]);
-                  }
-                  return d;
-                },
-                [&](uint32_t j, uint32_t, XV d, bool valid) {
-              const bool cand = valid && j > i;
-              LinkEval L{false, false, V2(), 0.0f};
-              if (cand) L = link_pair(m, U, xi, v0i, d.x, d.v0, reach, range2, dxd, c_max, pass == 1);
-              inr += __popc(__ballot_sync(FULL, cand && L.in_range));
-              const uint32_t bal = __ballot_sync(FULL, cand && L.emit);
-              if (pass && cand && L.emit) {
-                const uint32_t q = o + c + __popc(bal & ((1u << lane) - 1u));
-                m.l_ball[q] = i; m.l_other[q] = j; m.l_n[q] = L.n.f2(); m.l_c[q] = L.c;
-              }
-              c += __popc(bal);
-            });
-            if (lane == 0) {
-              LinkEval W = link_wall(m, U, i, reach, dxd, c_max);
-              if (W.in_range) inr += 1;
-              if (W.emit) {
-                if (pass) { m.l_ball[o + c] = i; m.l_other[o + c] = NONE; m.l_n[o + c] = W.n.f2(); m.l_c[o + c] = W.c; }
-                ++c;
-              }
+      // wall link, each film evaluated once; ball i's links go to its slots [i K, i K + K) of the
+      // record scratch, then one compaction copies them to the link list in ball order
+      const uint32_t K = min(nb + 1u, 512u);
+      for (uint32_t i = tid() >> 5; i < nb; i += nthr() >> 5) {
+        const uint32_t lane = tid() & 31u;
+        const V2 xi(m.bx[i]), v0i(m.ball_v0[i]);
+        const uint32_t base = i * K;
+        uint32_t c = 0, inr = 0;
+        if (xi.finite()) {
+          struct XV {
+            V2 x, v0;
+          };
+          warp_near_multi(
+              S.hBall, m.gBall, 1u, [&](uint32_t) { return xi; },
+              [&](uint32_t j, bool valid) {
+                XV d{V2(), V2()};
+                if (valid && j > i) {
+                  d.x = V2(m.bx[j]);
+                  d.v0 = V2(m.ball_v0[j]);
+                }
+                return d;
+              },
+              [&](uint32_t j, uint32_t, XV d, bool valid) {
+                const bool cand = valid && j > i;
+                LinkEval L{false, false, V2(), 0.0f};
+                if (cand) L = link_pair(m, U, xi, v0i, d.x, d.v0, reach, range2, dxd, c_max, true);
+                inr += __popc(__ballot_sync(FULL, cand && L.in_range));
+                const uint32_t bal = __ballot_sync(FULL, cand && L.emit);
+                const uint32_t q = c + __popc(bal & ((1u << lane) - 1u));
+                if (cand && L.emit && q < K) {
+                  m.rec_i[base + q] = j;
+                  m.rec_J[base + q] = L.n.f2();
+                  m.rec_L[base + q] = L.c;
+                }
+                c += __popc(bal);
+              });
+          if (lane == 0) {
+            LinkEval W = link_wall(m, U, i, reach, dxd, c_max);
+            if (W.in_range) inr += 1;
+            if (W.emit) {
+              if (c < K) { m.rec_i[base + c] = NONE; m.rec_J[base + c] = W.n.f2(); m.rec_L[base + c] = W.c; }
+              ++c;
             }
           }
-          if (lane == 0 && !pass) {
-            m.l_off[i] = c;
-            in_range += inr;
-          }
-          __syncwarp();
         }
-        if (!pass) {
-          if (tid() == 0) m.l_off[nb] = 0;
-          __syncthreads();
-          uint32_t tot_in = block_sum_u(in_range);
-          uint32_t nl = block_exclusive_scan(m.l_off, nb + 1);
-          if (nl > m.cap_links) { if (tid() == 0) atomicOr(err, ERR_LINKS); __syncthreads(); return; }
-          if (tid() == 0) { S.n_links = nl; S.links_in_range = tot_in; }
+        if (lane == 0) {
+          if (c > K) { atomicOr(err, ERR_LINKS); c = K; }
+          m.l_off[i] = c;
+          in_range += inr;
         }
-        __syncthreads();
+        __syncwarp();
       }
+      if (tid() == 0) m.l_off[nb] = 0;
+      __syncthreads();
+      const uint32_t tot_in = block_sum_u(in_range);
+      const uint32_t nl = block_exclusive_scan(m.l_off, nb + 1);
+      if (nl > m.cap_links) { if (tid() == 0) atomicOr(err, ERR_LINKS); __syncthreads(); return; }
+      if (tid() == 0) { S.n_links = nl; S.links_in_range = tot_in; }
+      for (uint32_t i = tid() >> 5; i < nb; i += nthr() >> 5) {
+        const uint32_t o = m.l_off[i], cnt = m.l_off[i + 1] - o, base = i * K;
+        for (uint32_t q = tid() & 31u; q < cnt; q += 32) {
+          m.l_ball[o + q] = i;
+          m.l_other[o + q] = m.rec_i[base + q];
+          m.l_n[o + q] = m.rec_J[base + q];
+          m.l_c[o + q] = m.rec_L[base + q];
+        }
+      }
+      __syncthreads();
     }
     if (tid() == 0) {
       out.ctr.n_groups = S.n_groups;

@@ -100,14 +100,13 @@ __global__ void __launch_bounds__(256) pack_impacts_kernel(const MillDev* __rest
                                                            const uint32_t* __restrict__ n_sub_of,
                                                            MgImpactRecord* packed, uint32_t cap, uint32_t* cursor,
                                                            uint2* table) {
-  __shared__ uint32_t base, total;
+  __shared__ uint32_t base;
   const uint32_t mill = blockIdx.x;
   const MillDev& m = mills[mill];
   const uint32_t ns = n_sub_of[mill];
   if (threadIdx.x == 0) {
     uint32_t t = 0;
     for (uint32_t s = 0; s < ns; ++s) t += min(m.out[s].n_impacts, m.cap_impacts);
-    total = t;
     base = atomicAdd(cursor, t);
     table[mill] = make_uint2(base, t);
   }
