@@ -231,6 +231,61 @@ def run_batched(lib, backend, args):
                                 "2 mm discs; seed per mill"}}
 
 
+def run_serving(backend, args, plain_mfps):
+    """The request server under a Poisson stream of jobs drawn from the 512-mill mix's
+    distribution (mean args.serve_rate requests/s, horizons uniform in 0.5-10 s simulated, a
+    150 GiB admission budget), for args.serve_seconds of wall time. Every step admits what has
+    arrived and fits, advances all running jobs by one frame in one launch and retires finished
+    jobs. Frame latency: the wall time from the start of the step that computes a job's frame to
+    its end (what a client waiting for that frame sees)."""
+    import numpy as np
+    from milldynamics3_b200 import capi
+    from milldynamics3_b200.batch import mix_params
+    from milldynamics3_b200.server import Server
+    pool, _ = mix_params(backend, 1024, seed=3)
+    rng = np.random.default_rng(7)
+    server = Server(backend, memory_budget_bytes=150 << 30, max_active=args.serve_max_active)
+    lat, waits, active = [], [], []
+    submitted = finished = frames = 0
+    t_start = time.perf_counter()
+    next_arrival = t_start + rng.exponential(1.0 / args.serve_rate)
+    while time.perf_counter() - t_start < args.serve_seconds:
+        now = time.perf_counter()
+        while next_arrival <= now:
+            server.submit(pool[submitted % len(pool)], float(rng.uniform(0.5, 10.0)))
+            submitted += 1
+            next_arrival += rng.exponential(1.0 / args.serve_rate)
+        t0 = time.perf_counter()
+        server.step()
+        dt = time.perf_counter() - t0
+        n_adv = 0
+        for u in server.poll():
+            if u.state in (capi.JOB_RUNNING, capi.JOB_FINISHED):
+                n_adv += 1
+                if u.frames_done == 1:
+                    waits.append(u.queued_s)
+            finished += u.state == capi.JOB_FINISHED
+        frames += n_adv
+        lat.extend([1e3 * dt] * n_adv)
+        active.append(n_adv)
+    elapsed = time.perf_counter() - t_start
+    st = server.stats()
+    server.close()
+    lat.sort()
+    waits.sort()
+    pct = lambda a, q: a[min(len(a) - 1, int(q * len(a)))] if a else None
+    mfps = frames / elapsed
+    return {"requests_per_s": args.serve_rate, "seconds": elapsed, "submitted": submitted, "finished": finished,
+            "still_queued": st.queued, "mill_frames": frames, "mill_frames_per_s": mfps,
+            "frame_latency_ms": {"p50": pct(lat, 0.5), "p99": pct(lat, 0.99)},
+            "admission_wait_s": {"p50": pct(waits, 0.5), "p99": pct(waits, 0.99)},
+            "running_jobs_mean": float(sum(active) / max(len(active), 1)), "max_active": args.serve_max_active,
+            "plain_mill_frames_per_s": plain_mfps,
+            "ratio_vs_plain": mfps / plain_mfps if plain_mfps else None,
+            "workload": "Poisson arrivals of mills drawn from the 512-mill mix distribution, horizons U[0.5,10] s "
+                        "simulated, 150 GiB admission budget, one launch per frame for all running jobs"}
+
+
 def run_device(args):
     import numpy as np
     import torch
@@ -328,8 +383,12 @@ def run_device(args):
                 "gpu_launches": args.steps, "clocks": clocks, "stage_us_per_substep": stages,
                 "counters_per_substep": {f: round(tot[q] / max(nsum.value, 1), 2) for q, (f, _) in
                                          enumerate(capi.StepCounters._fields_) if f != "reserved0"}}
+        plain_mfps = None
         if args.batch_mills > 0:
             line["batched"] = run_batched(lib, b, args)
+            plain_mfps = line["batched"]["plain_mill_frames_per_s"]
+        if args.serve_seconds > 0:
+            line["serving"] = run_serving(b, args, plain_mfps)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
         print(json.dumps(line), flush=True)
@@ -349,6 +408,9 @@ def main():
     ap.add_argument("--batch-mills", type=int, default=512, help="mills of the batched leg (0: skip it)")
     ap.add_argument("--batch-frames", type=int, default=5)
     ap.add_argument("--plain-sample", type=int, default=16, help="mills of the mix timed on the plain path")
+    ap.add_argument("--serve-seconds", type=float, default=20.0, help="wall seconds of the serving leg (0: skip it)")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="mean job arrivals per second")
+    ap.add_argument("--serve-max-active", type=int, default=1024, help="jobs advanced per launch at most")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -340,6 +340,49 @@ int mg_batch_last_kernel_ms(MgBatch* batch, float* ms, uint64_t* launches);
 /* Device memory a handle holds (its arena plus launch blocks), for admission by footprint. */
 int mg_sim_footprint(const MgSim* sim, uint64_t* device_bytes);
 
+/* ---- request server: continuous batching of mill jobs. No single reference counterpart (the
+ * reference runs one Simulation per web worker, worker.ts:138-142, and seed sweeps one after
+ * another, batch.rs:40-191). Jobs (Params + a simulated horizon) wait in a queue and are admitted
+ * oldest first whenever the device bytes of their state fit under the budget; each
+ * mg_server_step advances every admitted job by one frame in one launch and retires the jobs
+ * that reached their horizon. A job's results are identical to the same mill stepped alone. */
+typedef struct MgServer MgServer;
+typedef struct MgServerConfig {
+  uint64_t memory_budget_bytes; /* device bytes all admitted jobs may hold together (0 = 150 GiB) */
+  uint32_t max_active;          /* jobs advanced per step at most (0 = 1024) */
+  uint32_t block_threads;       /* 0 = default */
+  float frame_dt;               /* simulated seconds per frame (0 = 1/60) */
+  uint32_t reserved[3];
+} MgServerConfig;
+enum { MG_JOB_QUEUED = 0, MG_JOB_RUNNING = 1, MG_JOB_FINISHED = 2, MG_JOB_CANCELLED = 3, MG_JOB_FAILED = 4 };
+/* One job's state after a frame (RUNNING) or at its end (FINISHED / CANCELLED / FAILED). */
+typedef struct MgJobUpdate {
+  uint64_t job_id;
+  uint32_t state, frames_done, frames_total, reserved0;
+  MgScalars scalars;                          /* power, torque, ... after the job's latest frame */
+  double stress_histogram_rate[MG_SE_BINS];   /* StressAccum::histogram_rate (stress.rs:174-238) */
+  uint64_t state_hash;                        /* extended state hash when FINISHED, else 0 */
+  double queued_s;                            /* wall seconds from submission to admission */
+  double first_frame_s;                       /* wall seconds from submission to its first frame's end */
+} MgJobUpdate;
+typedef struct MgServerStats {
+  uint32_t queued, active, finished_total, pending_updates;
+  uint64_t device_bytes_in_use, frames;
+  float last_frame_ms, last_kernel_ms;        /* wall time of the last step; device time of its launch */
+} MgServerStats;
+int mg_server_create(const MgServerConfig* cfg, MgServer** out);
+void mg_server_destroy(MgServer* server);
+const char* mg_server_last_error(const MgServer* server);
+/* Queues a job of ceil(horizon_s / frame_dt) frames; *job_id identifies it in the updates. */
+int mg_server_submit(MgServer* server, const MgParams* p, double horizon_s, uint64_t* job_id);
+/* A queued job leaves at once, a running one before the next frame (a CANCELLED update). */
+int mg_server_cancel(MgServer* server, uint64_t job_id);
+/* Admits what fits, advances every running job by one frame, retires the finished ones. */
+int mg_server_step(MgServer* server);
+/* Hands out (and forgets) up to cap pending updates, oldest first; *n_out receives the count. */
+int mg_server_poll(MgServer* server, MgJobUpdate* out, uint32_t cap, uint32_t* n_out);
+int mg_server_stats(MgServer* server, MgServerStats* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -150,6 +150,27 @@ class Options(_S):
                 ("spin_ns", C.c_uint32), ("reserved", C.c_uint32 * 4)]
 
 
+class ServerConfig(_S):
+    _fields_ = [("memory_budget_bytes", C.c_uint64), ("max_active", C.c_uint32), ("block_threads", C.c_uint32),
+                ("frame_dt", C.c_float), ("reserved", C.c_uint32 * 3)]
+
+
+JOB_QUEUED, JOB_RUNNING, JOB_FINISHED, JOB_CANCELLED, JOB_FAILED = 0, 1, 2, 3, 4
+
+
+class JobUpdate(_S):
+    _fields_ = [("job_id", C.c_uint64), ("state", C.c_uint32), ("frames_done", C.c_uint32),
+                ("frames_total", C.c_uint32), ("reserved0", C.c_uint32), ("scalars", Scalars),
+                ("stress_histogram_rate", C.c_double * SE_BINS), ("state_hash", C.c_uint64),
+                ("queued_s", C.c_double), ("first_frame_s", C.c_double)]
+
+
+class ServerStats(_S):
+    _fields_ = [("queued", C.c_uint32), ("active", C.c_uint32), ("finished_total", C.c_uint32),
+                ("pending_updates", C.c_uint32), ("device_bytes_in_use", C.c_uint64), ("frames", C.c_uint64),
+                ("last_frame_ms", C.c_float), ("last_kernel_ms", C.c_float)]
+
+
 P = C.POINTER
 f32p = P(C.c_float)
 u32p = P(C.c_uint32)
@@ -223,6 +244,14 @@ DEVICE_ONLY = [
     ("batch_stream", C.c_int, [vp, P(vp)]),
     ("batch_last_kernel_ms", C.c_int, [vp, P(C.c_float), P(C.c_uint64)]),
     ("sim_footprint", C.c_int, [vp, P(C.c_uint64)]),
+    ("server_create", C.c_int, [P(ServerConfig), P(vp)]),
+    ("server_destroy", None, [vp]),
+    ("server_last_error", C.c_char_p, [vp]),
+    ("server_submit", C.c_int, [vp, P(Params), C.c_double, P(C.c_uint64)]),
+    ("server_cancel", C.c_int, [vp, C.c_uint64]),
+    ("server_step", C.c_int, [vp]),
+    ("server_poll", C.c_int, [vp, P(JobUpdate), C.c_uint32, u32p]),
+    ("server_stats", C.c_int, [vp, P(ServerStats)]),
 ]
 
 STAGE_NAMES = [

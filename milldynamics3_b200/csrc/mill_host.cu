@@ -4,7 +4,10 @@
 // Simulation bookkeeping of lib.rs:470-565 (EMA power and torque, f64 energy budget, the stress
 // accumulator of stress.rs with its debounce table), exactly in sub-step order.
 #include <algorithm>
+#include <chrono>
+#include <cmath>
 #include <cstdarg>
+#include <deque>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -123,6 +126,10 @@ struct MgSim {
   Stress stress;
   // device state
   cudaStream_t stream = nullptr;
+  // a light handle (a request-server job): it borrows the server's stream, takes its arena from
+  // the device's stream-ordered memory pool and keeps its host blocks in pageable memory; it is
+  // only ever advanced by the server's batched launches
+  bool light = false;
   uint32_t nf = 0, nb = 0, cap_nf = 0, cap_nb = 0;
   MgBallMaterial bmat{};
   MgFluidMaterial fmat{};
@@ -175,7 +182,11 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
     s->md.nb = nb;
     return MG_OK;
   }
-  if (s->dmem) { cudaFree(s->dmem); s->dmem = nullptr; }
+  if (s->dmem) {
+    if (s->light) cudaFreeAsync(s->dmem, s->stream);
+    else cudaFree(s->dmem);
+    s->dmem = nullptr;
+  }
   uint32_t cf = std::max(nf, 1u), cb = std::max(nb, 1u);
   MillDev m{};
   m.cap_nf = cf;
@@ -261,7 +272,7 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
     m.impacts = a.take<MgImpactRecord>((size_t)MAX_SUB * m.cap_impacts);
     if (!pass) {
       s->dbytes = a.off + 256;
-      cudaError_t e = cudaMalloc(&s->dmem, s->dbytes);
+      cudaError_t e = s->light ? cudaMallocAsync(&s->dmem, s->dbytes, s->stream) : cudaMalloc(&s->dmem, s->dbytes);
       if (e != cudaSuccess) return fail(s, MG_ERR_CUDA, "cudaMalloc(%zu): %s", s->dbytes, cudaGetErrorString(e));
       cudaMemsetAsync(s->dmem, 0, s->dbytes, s->stream);
     }
@@ -500,6 +511,15 @@ int advance(MgSim* s, uint32_t n, float sub_dt) {
   return MG_OK;
 }
 
+// A light handle's host blocks (see MgSim::light); it launches nothing of its own.
+int init_light_handle(MgSim* s, cudaStream_t stream) {
+  s->light = true;
+  s->stream = stream;
+  s->h_uni = new StepUniform();
+  s->h_out = new StepOut[MAX_SUB]();
+  return MG_OK;
+}
+
 int init_handle(MgSim* s) {
   CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
   CK(cudaMalloc(&s->d_md, sizeof(MillDev)));
@@ -543,7 +563,8 @@ int upload_fluid(MgSim* s, const float* x, const float* v, const float* dye, con
   return MG_OK;
 }
 
-int create_sim(const MgParams* p, const float* xy, uint32_t n_init, MgSim** out) {
+// Simulation::new / with_initial_balls. With a server stream the handle is a light one (MgSim::light).
+int create_sim(const MgParams* p, const float* xy, uint32_t n_init, MgSim** out, cudaStream_t server_stream = nullptr) {
   if (!p || !out) return fail_global(MG_ERR_ARG, "null argument");
   std::string e;
   if (!mgh::params_validate(*p, &e)) return fail_global(MG_ERR_INVALID_PARAMS, "%s", e.c_str());
@@ -552,7 +573,7 @@ int create_sim(const MgParams* p, const float* xy, uint32_t n_init, MgSim** out)
     return fail_global(MG_ERR_NO_DEVICE, "no CUDA device visible");
   MgSim* s = new MgSim();
   s->params = *p;
-  int rc = init_handle(s);
+  int rc = server_stream ? init_light_handle(s, server_stream) : init_handle(s);
   if (rc) { g_err = s->err; mg_sim_destroy(s); return rc; }
   float radius = mgh::mill_radius(p->mill);
   mgh::Effective eff = mgh::effective_media(*p);
@@ -678,6 +699,15 @@ int mg_sim_create_with_balls(const MgParams* p, const float* xy, uint32_t n, MgS
 }
 void mg_sim_destroy(MgSim* s) {
   if (!s) return;
+  if (s->light) {
+    // the arena goes back to the pool in stream order; the stream belongs to the server
+    if (s->dmem) cudaFreeAsync(s->dmem, s->stream);
+    delete s->h_uni;
+    delete[] s->h_out;
+    delete[] s->h_imp;
+    delete s;
+    return;
+  }
   if (s->stream) cudaStreamSynchronize(s->stream);
   if (s->dmem) cudaFree(s->dmem);
   if (s->d_md) cudaFree(s->d_md);
@@ -1409,6 +1439,407 @@ int mg_batch_last_kernel_ms(MgBatch* b, float* ms, uint64_t* launches) {
 int mg_sim_footprint(const MgSim* s, uint64_t* device_bytes) {
   if (!s || !device_bytes) return fail_global(MG_ERR_ARG, "null argument");
   *device_bytes = (uint64_t)s->dbytes + sizeof(MillDev) + sizeof(StepUniform) + sizeof(SubAngles) * MAX_SUB;
+  return MG_OK;
+}
+
+}  // extern "C"
+
+// ====================================================================== request server
+// Continuous batching of mill jobs: submitted jobs wait in a queue and are admitted, oldest first,
+// whenever the device bytes their arenas need fit under the budget; every step advances all
+// admitted jobs by one frame in one launch (one thread block per job, each its own sub-step
+// count) and retires the jobs that reached their horizon, freeing their memory for the queue.
+// A job advances exactly as the same mill stepped alone (the same kernels on the same state), so
+// its results do not depend on what else is in the mix.
+struct MgServerJob {
+  uint64_t id = 0;
+  MgParams params{};
+  uint32_t frames_total = 0, frames_done = 0, n_sub = 0;
+  MgSim* sim = nullptr;
+  uint64_t bytes = 0;
+  bool cancel = false;
+  double t_submit = 0.0, t_admit = 0.0, t_first = -1.0;
+};
+
+struct MgServer {
+  MgServerConfig cfg{};
+  std::string err;
+  cudaStream_t stream = nullptr;
+  std::deque<MgServerJob*> queue;
+  std::vector<MgServerJob*> active;
+  std::vector<MgJobUpdate> pending;
+  uint64_t next_id = 1, in_use = 0, frames = 0;
+  uint32_t finished_total = 0;
+  // launch blocks, grown as needed (cap jobs, MAX_SUB sub-steps each)
+  uint32_t cap = 0;
+  MillDev *d_md = nullptr, *h_md = nullptr;
+  StepUniform *d_uni = nullptr, *h_uni = nullptr;
+  SubAngles *d_ang = nullptr, *h_ang = nullptr;
+  uint32_t *d_nsub = nullptr, *h_nsub = nullptr;
+  StepOut *d_out = nullptr, *h_out = nullptr;
+  uint2 *d_table = nullptr, *h_table = nullptr;
+  uint32_t* d_cursor = nullptr;
+  MgImpactRecord *d_packed = nullptr, *h_packed = nullptr;
+  uint64_t packed_cap = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_kernel_ms = 0.0f, last_frame_ms = 0.0f;
+};
+
+namespace {
+
+double wall_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+int sfail(MgServer* v, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (v) v->err = buf;
+  g_err = buf;
+  return code;
+}
+#define SCK(call)                                                                        \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) return sfail(v, MG_ERR_CUDA, "%s", cudaGetErrorString(e_));   \
+  } while (0)
+
+void server_free_blocks(MgServer* v) {
+  cudaFree(v->d_md); cudaFreeHost(v->h_md);
+  cudaFree(v->d_uni); cudaFreeHost(v->h_uni);
+  cudaFree(v->d_ang); cudaFreeHost(v->h_ang);
+  cudaFree(v->d_nsub); cudaFreeHost(v->h_nsub);
+  cudaFree(v->d_out); cudaFreeHost(v->h_out);
+  cudaFree(v->d_table); cudaFreeHost(v->h_table);
+  v->d_md = v->h_md = nullptr;
+  v->d_uni = v->h_uni = nullptr;
+  v->d_ang = v->h_ang = nullptr;
+  v->d_nsub = v->h_nsub = nullptr;
+  v->d_out = v->h_out = nullptr;
+  v->d_table = v->h_table = nullptr;
+  v->cap = 0;
+}
+
+int server_reserve(MgServer* v, uint32_t n, uint64_t packed) {
+  if (n > v->cap) {
+    SCK(cudaStreamSynchronize(v->stream));
+    server_free_blocks(v);
+    const uint32_t c = std::max(n, 2 * v->cap);
+    SCK(cudaMalloc(&v->d_md, sizeof(MillDev) * c));
+    SCK(cudaMallocHost(&v->h_md, sizeof(MillDev) * c));
+    SCK(cudaMalloc(&v->d_uni, sizeof(StepUniform) * c));
+    SCK(cudaMallocHost(&v->h_uni, sizeof(StepUniform) * c));
+    SCK(cudaMalloc(&v->d_ang, sizeof(SubAngles) * c * MAX_SUB));
+    SCK(cudaMallocHost(&v->h_ang, sizeof(SubAngles) * c * MAX_SUB));
+    SCK(cudaMalloc(&v->d_nsub, sizeof(uint32_t) * c));
+    SCK(cudaMallocHost(&v->h_nsub, sizeof(uint32_t) * c));
+    SCK(cudaMalloc(&v->d_out, sizeof(StepOut) * c * MAX_SUB));
+    SCK(cudaMallocHost(&v->h_out, sizeof(StepOut) * c * MAX_SUB));
+    SCK(cudaMalloc(&v->d_table, sizeof(uint2) * c));
+    SCK(cudaMallocHost(&v->h_table, sizeof(uint2) * c));
+    v->cap = c;
+  }
+  if (packed > v->packed_cap) {
+    SCK(cudaStreamSynchronize(v->stream));
+    cudaFree(v->d_packed);
+    cudaFreeHost(v->h_packed);
+    v->d_packed = v->h_packed = nullptr;
+    const uint64_t c = std::max<uint64_t>(packed, 2 * v->packed_cap);
+    SCK(cudaMalloc(&v->d_packed, sizeof(MgImpactRecord) * c));
+    SCK(cudaMallocHost(&v->h_packed, sizeof(MgImpactRecord) * c));
+    v->packed_cap = c;
+  }
+  return MG_OK;
+}
+
+MgJobUpdate job_update(const MgServerJob* j, uint32_t state) {
+  MgJobUpdate u;
+  std::memset(&u, 0, sizeof(u));
+  u.job_id = j->id;
+  u.state = state;
+  u.frames_done = j->frames_done;
+  u.frames_total = j->frames_total;
+  u.queued_s = j->t_admit > 0.0 ? j->t_admit - j->t_submit : 0.0;
+  u.first_frame_s = j->t_first >= 0.0 ? j->t_first - j->t_submit : 0.0;
+  if (j->sim) {
+    mg_get_scalars(j->sim, &u.scalars);
+    mg_stress_histogram_rate(j->sim, u.stress_histogram_rate);
+  }
+  return u;
+}
+
+void retire(MgServer* v, MgServerJob* j, uint32_t state) {
+  MgJobUpdate u = job_update(j, state);
+  if (j->sim && state == MG_JOB_FINISHED) mg_state_hash(j->sim, 1, &u.state_hash);
+  v->pending.push_back(u);
+  if (j->sim) {
+    mg_sim_destroy(j->sim);
+    v->in_use -= j->bytes;
+  }
+  v->finished_total += 1;
+  delete j;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mg_server_create(const MgServerConfig* cfg, MgServer** out) {
+  if (!out) return fail_global(MG_ERR_ARG, "null argument");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail_global(MG_ERR_NO_DEVICE, "no CUDA device visible");
+  MgServer* v = new MgServer();
+  if (cfg) v->cfg = *cfg;
+  if (v->cfg.memory_budget_bytes == 0) v->cfg.memory_budget_bytes = 150ull << 30;
+  if (v->cfg.max_active == 0) v->cfg.max_active = 1024;
+  if (!(v->cfg.frame_dt > 0.0f)) v->cfg.frame_dt = 1.0f / 60.0f;
+  if (v->cfg.block_threads != 0 && (v->cfg.block_threads % 32 != 0 || v->cfg.block_threads > 512)) {
+    delete v;
+    return fail_global(MG_ERR_ARG, "block_threads must be a multiple of 32 in [32, 512]");
+  }
+  auto setup = [&]() -> int {
+    SCK(cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking));
+    SCK(cudaEventCreate(&v->ev0));
+    SCK(cudaEventCreate(&v->ev1));
+    SCK(cudaMalloc(&v->d_cursor, sizeof(uint32_t)));
+    // retired jobs' arenas stay in the device pool for the next admissions
+    int dev = 0;
+    SCK(cudaGetDevice(&dev));
+    cudaMemPool_t pool;
+    SCK(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t keep = v->cfg.memory_budget_bytes;
+    SCK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    return MG_OK;
+  };
+  int rc = setup();
+  if (rc) {
+    std::string e = v->err;
+    mg_server_destroy(v);
+    g_err = e;
+    return rc;
+  }
+  *out = v;
+  return MG_OK;
+}
+
+void mg_server_destroy(MgServer* v) {
+  if (!v) return;
+  if (v->stream) cudaStreamSynchronize(v->stream);
+  for (MgServerJob* j : v->active) {
+    if (j->sim) mg_sim_destroy(j->sim);
+    delete j;
+  }
+  for (MgServerJob* j : v->queue) delete j;
+  if (v->stream) cudaStreamSynchronize(v->stream);
+  server_free_blocks(v);
+  cudaFree(v->d_packed);
+  cudaFreeHost(v->h_packed);
+  cudaFree(v->d_cursor);
+  if (v->ev0) cudaEventDestroy(v->ev0);
+  if (v->ev1) cudaEventDestroy(v->ev1);
+  if (v->stream) cudaStreamDestroy(v->stream);
+  delete v;
+}
+
+const char* mg_server_last_error(const MgServer* v) { return v ? v->err.c_str() : g_err.c_str(); }
+
+int mg_server_submit(MgServer* v, const MgParams* p, double horizon_s, uint64_t* job_id) {
+  if (!v || !p) return fail_global(MG_ERR_ARG, "null argument");
+  std::string e;
+  if (!mgh::params_validate(*p, &e)) return sfail(v, MG_ERR_INVALID_PARAMS, "%s", e.c_str());
+  if (!(horizon_s > 0.0) || !std::isfinite(horizon_s)) return sfail(v, MG_ERR_ARG, "horizon must be positive");
+  const uint32_t ns = std::max(mgh::effective_substeps(*p), 1u);
+  if (ns > MAX_SUB) return sfail(v, MG_ERR_ARG, "%u sub-steps per frame, at most %u", ns, MAX_SUB);
+  MgServerJob* j = new MgServerJob();
+  j->id = v->next_id++;
+  j->params = *p;
+  j->n_sub = ns;
+  j->frames_total = (uint32_t)std::max(1.0, std::ceil(horizon_s / (double)v->cfg.frame_dt - 1e-9));
+  j->t_submit = wall_s();
+  v->queue.push_back(j);
+  if (job_id) *job_id = j->id;
+  return MG_OK;
+}
+
+int mg_server_cancel(MgServer* v, uint64_t job_id) {
+  if (!v) return fail_global(MG_ERR_ARG, "null handle");
+  for (auto it = v->queue.begin(); it != v->queue.end(); ++it) {
+    if ((*it)->id == job_id) {
+      MgServerJob* j = *it;
+      v->queue.erase(it);
+      retire(v, j, MG_JOB_CANCELLED);
+      return MG_OK;
+    }
+  }
+  for (MgServerJob* j : v->active)
+    if (j->id == job_id) { j->cancel = true; return MG_OK; }
+  return sfail(v, MG_ERR_ARG, "no queued or running job %llu", (unsigned long long)job_id);
+}
+
+int mg_server_step(MgServer* v) {
+  if (!v) return fail_global(MG_ERR_ARG, "null handle");
+  const double t0 = wall_s();
+  // cancelled jobs leave before the frame
+  for (size_t k = 0; k < v->active.size();) {
+    if (v->active[k]->cancel) {
+      retire(v, v->active[k], MG_JOB_CANCELLED);
+      v->active.erase(v->active.begin() + (long)k);
+    } else {
+      ++k;
+    }
+  }
+  // admission, oldest first, by the device bytes each job's arena needs
+  while (!v->queue.empty() && v->active.size() < v->cfg.max_active) {
+    MgServerJob* j = v->queue.front();
+    MgSim* sim = nullptr;
+    int rc = create_sim(&j->params, nullptr, 0, &sim, v->stream);
+    if (!rc) rc = check_materials(sim);
+    if (rc) {
+      if (sim) mg_sim_destroy(sim);
+      v->queue.pop_front();
+      retire(v, j, MG_JOB_FAILED);
+      continue;
+    }
+    const uint64_t need = sim->dbytes;
+    if (v->in_use + need > v->cfg.memory_budget_bytes) {
+      mg_sim_destroy(sim);
+      if (v->active.empty()) {  // it could never fit
+        v->queue.pop_front();
+        retire(v, j, MG_JOB_FAILED);
+        continue;
+      }
+      break;  // wait for running jobs to free memory
+    }
+    j->sim = sim;
+    j->bytes = need;
+    j->t_admit = wall_s();
+    v->in_use += need;
+    v->queue.pop_front();
+    v->active.push_back(j);
+  }
+  const uint32_t n = (uint32_t)v->active.size();
+  if (n == 0) {
+    v->last_frame_ms = (float)(1e3 * (wall_s() - t0));
+    return MG_OK;
+  }
+  uint32_t stride = 0;
+  uint64_t packed = 0;
+  for (MgServerJob* j : v->active) {
+    stride = std::max(stride, j->n_sub);
+    packed += (uint64_t)j->sim->md.cap_impacts * j->n_sub;
+  }
+  int rc = server_reserve(v, n, packed);
+  if (rc) return rc;
+  size_t smem = 0;
+  const float frame_dt = v->cfg.frame_dt;
+  for (uint32_t k = 0; k < n; ++k) {
+    MgServerJob* j = v->active[k];
+    MgSim* s = j->sim;
+    const MgSimulationParams& q = s->params.simulation;
+    rc = fill_uniform(s, sim_drum(s), s->params.media, s->params.slurry, q.pbf_iterations, q.dem_iterations, 1, 1, 1);
+    if (rc) return sfail(v, rc, "job %llu: %s", (unsigned long long)j->id, s->err.c_str());
+    std::memcpy(&v->h_uni[k], s->h_uni, sizeof(StepUniform));
+    fill_desc(s);
+    v->h_md[k] = s->md;
+    v->h_md[k].out = v->d_out + (size_t)k * stride;
+    smem = std::max(smem, (size_t)s->md.smem_bytes);
+    v->h_nsub[k] = j->n_sub;
+    const float sub_dt = frame_dt / (float)j->n_sub;
+    const float omega = mgh::mill_omega(s->params.mill);
+    float angle = s->drum_angle;
+    for (uint32_t t = 0; t < j->n_sub; ++t) {
+      fill_angle(v->h_ang[(size_t)k * stride + t], angle, omega, sub_dt);
+      angle = mgh::rem_euclid_r(angle + omega * sub_dt, mgh::TAU_F);
+    }
+  }
+  SCK(cudaMemcpyAsync(v->d_md, v->h_md, sizeof(MillDev) * n, cudaMemcpyHostToDevice, v->stream));
+  SCK(cudaMemcpyAsync(v->d_uni, v->h_uni, sizeof(StepUniform) * n, cudaMemcpyHostToDevice, v->stream));
+  SCK(cudaMemcpyAsync(v->d_ang, v->h_ang, sizeof(SubAngles) * n * stride, cudaMemcpyHostToDevice, v->stream));
+  SCK(cudaMemcpyAsync(v->d_nsub, v->h_nsub, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, v->stream));
+  SCK(cudaEventRecord(v->ev0, v->stream));
+  SCK(launch_substeps(v->d_md, n, v->d_uni, v->d_ang, stride, v->d_nsub, v->cfg.block_threads, smem, v->stream));
+  SCK(cudaEventRecord(v->ev1, v->stream));
+  SCK(cudaMemsetAsync(v->d_cursor, 0, sizeof(uint32_t), v->stream));
+  SCK(launch_pack_impacts(v->d_md, n, v->d_nsub, v->d_packed, (uint32_t)std::min<uint64_t>(v->packed_cap, 0xFFFFFFF0ull),
+                          v->d_cursor, v->d_table, v->stream));
+  SCK(cudaMemcpyAsync(v->h_out, v->d_out, sizeof(StepOut) * n * stride, cudaMemcpyDeviceToHost, v->stream));
+  SCK(cudaMemcpyAsync(v->h_table, v->d_table, sizeof(uint2) * n, cudaMemcpyDeviceToHost, v->stream));
+  SCK(cudaStreamSynchronize(v->stream));
+  SCK(cudaEventElapsedTime(&v->last_kernel_ms, v->ev0, v->ev1));
+  uint64_t total = 0;
+  for (uint32_t k = 0; k < n; ++k) total = std::max<uint64_t>(total, (uint64_t)v->h_table[k].x + v->h_table[k].y);
+  if (total > v->packed_cap) return sfail(v, MG_ERR_CAPACITY, "impact records exceed the server buffer");
+  if (total)
+    SCK(cudaMemcpyAsync(v->h_packed, v->d_packed, sizeof(MgImpactRecord) * total, cudaMemcpyDeviceToHost, v->stream));
+  SCK(cudaStreamSynchronize(v->stream));
+  v->frames += 1;
+  const double t_end = wall_s();
+  std::vector<MgServerJob*> keep;
+  keep.reserve(n);
+  for (uint32_t k = 0; k < n; ++k) {
+    MgServerJob* j = v->active[k];
+    MgSim* s = j->sim;
+    const uint32_t ns = j->n_sub;
+    const StepOut* o = v->h_out + (size_t)k * stride;
+    uint32_t e = 0;
+    for (uint32_t t = 0; t < ns; ++t) e |= o[t].err;
+    if (e) {
+      retire(v, j, MG_JOB_FAILED);
+      continue;
+    }
+    std::memcpy(s->h_out, o, sizeof(StepOut) * ns);
+    const MgImpactRecord* rec = v->h_packed + v->h_table[k].x;
+    for (uint32_t t = 0; t < ns; ++t) {
+      const uint32_t ni = std::min(o[t].n_impacts, s->md.cap_impacts);
+      if (ni) std::memcpy(s->h_imp + (size_t)t * s->md.cap_impacts, rec, sizeof(MgImpactRecord) * ni);
+      rec += ni;
+    }
+    s->max_disp = 0.0f;
+    s->clamp_hits_frame = 0;
+    const float sub_dt = frame_dt / (float)ns;
+    const float omega = mgh::mill_omega(s->params.mill);
+    for (uint32_t t = 0; t < ns; ++t) fold_substep(s, t, sub_dt, omega);
+    s->last_fluid = o[ns - 1].fs;
+    s->last_dem = o[ns - 1].ds;
+    s->last_ctr = o[ns - 1].ctr;
+    s->launches += 1;
+    j->frames_done += 1;
+    if (j->t_first < 0.0) j->t_first = t_end;
+    if (j->frames_done >= j->frames_total) {
+      retire(v, j, MG_JOB_FINISHED);
+    } else {
+      v->pending.push_back(job_update(j, MG_JOB_RUNNING));
+      keep.push_back(j);
+    }
+  }
+  v->active.swap(keep);
+  v->last_frame_ms = (float)(1e3 * (wall_s() - t0));
+  return MG_OK;
+}
+
+int mg_server_poll(MgServer* v, MgJobUpdate* out, uint32_t cap, uint32_t* n_out) {
+  if (!v || (!out && cap)) return fail_global(MG_ERR_ARG, "null argument");
+  const uint32_t n = (uint32_t)std::min<size_t>(cap, v->pending.size());
+  if (n) std::memcpy(out, v->pending.data(), sizeof(MgJobUpdate) * n);
+  v->pending.erase(v->pending.begin(), v->pending.begin() + n);
+  if (n_out) *n_out = n;
+  return MG_OK;
+}
+
+int mg_server_stats(MgServer* v, MgServerStats* out) {
+  if (!v || !out) return fail_global(MG_ERR_ARG, "null argument");
+  std::memset(out, 0, sizeof(*out));
+  out->queued = (uint32_t)v->queue.size();
+  out->active = (uint32_t)v->active.size();
+  out->finished_total = v->finished_total;
+  out->pending_updates = (uint32_t)v->pending.size();
+  out->device_bytes_in_use = v->in_use;
+  out->frames = v->frames;
+  out->last_frame_ms = v->last_frame_ms;
+  out->last_kernel_ms = v->last_kernel_ms;
   return MG_OK;
 }
 

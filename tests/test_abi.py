@@ -71,3 +71,7 @@ def test_no_device_fails_loudly_without_gpu(device):
         from milldynamics3_b200.batch import Batch
         Batch(device, [device.params_default()] * 2)
     assert e.value.code == capi.MG_ERR_NO_DEVICE
+    with pytest.raises(MillError) as e:
+        from milldynamics3_b200.server import Server
+        Server(device)
+    assert e.value.code == capi.MG_ERR_NO_DEVICE
