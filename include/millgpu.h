@@ -176,7 +176,8 @@ typedef struct MgScalars {
 } MgScalars;
 
 /* Device-path options. cg_fp64: 0 = the reference's sequential f32 inner products in the
- * viscosity solve, 1 = f64 inner products and residual norms. block_threads: 0 = default.
+ * viscosity solve, 1 = f64 inner products and residual norms. block_threads: threads per mill
+ * block, a multiple of 32 up to 1024 (0 = 1024).
  * sweep_warps: warps that take balls in the per-ball drag and buoyancy sweeps (0 = default).
  * spin_ns: poll interval of a ball waiting for an earlier ball in those sweeps (0 = default).
  * None of them changes results. */

@@ -19,7 +19,13 @@ constexpr float GRAVITY = -9.81f;
 constexpr uint32_t NONE = 0xFFFFFFFFu;
 constexpr int MAX_LIFTERS = 64;
 // Per-ball sweeps (drag, buoyancy): warps taking balls and the poll interval of a waiting ball.
-constexpr uint32_t DEFAULT_SWEEP_WARPS = 16;
+constexpr uint32_t DEFAULT_SWEEP_WARPS = 32;
+// Largest block of the frame kernel (32 warps); per-warp scratch (the merge slot maps) is sized for it.
+constexpr uint32_t MAX_BLOCK_THREADS = 1024;
+constexpr uint32_t MAX_BLOCK_WARPS = MAX_BLOCK_THREADS / 32;
+// Threads per mill block when the options leave it open (measured fastest on B200, single mill
+// and batches alike).
+constexpr uint32_t DEFAULT_BLOCK_THREADS = 1024;
 constexpr uint32_t DEFAULT_SPIN_NS = 64;
 constexpr int MAX_BOUNDARY_POINTS = 1024;
 
@@ -268,7 +274,7 @@ struct MillDev {
   float *bth0, *bompre, *lam_bw, *lam_tot;
   double* f_cw;  // per-ball coupling work of the predict step
   uint32_t *rec_off, *rec_pred, *ball_done;  // per-ball sweep records (cap_nb + 1, cap_recs, cap_nb)
-  uint32_t* slot;  // per-warp fluid -> item maps of the in-order merges (16 x cap_nf, all NONE at rest)
+  uint32_t* slot;  // per-warp fluid -> item maps of the in-order merges (MAX_BLOCK_WARPS x cap_nf, all NONE at rest)
   uint32_t *pair_i, *pair_j;
   float* lam_bb;
   uint32_t *cs_i, *cs_j;  // contacts sorted by (i, j)

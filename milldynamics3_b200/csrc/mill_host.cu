@@ -263,7 +263,7 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
     m.lam_tot = a.take<float>(cb); m.f_cw = a.take<double>(cb);
     m.rec_off = a.take<uint32_t>(cb + 1); m.rec_pred = a.take<uint32_t>(m.cap_recs);
     m.ball_done = a.take<uint32_t>(cb);
-    m.slot = a.take<uint32_t>((size_t)16 * cf);
+    m.slot = a.take<uint32_t>((size_t)MAX_BLOCK_WARPS * cf);
     m.pair_i = a.take<uint32_t>(m.cap_pairs); m.pair_j = a.take<uint32_t>(m.cap_pairs);
     m.lam_bb = a.take<float>(m.cap_pairs);
     m.cs_i = a.take<uint32_t>(m.cap_pairs); m.cs_j = a.take<uint32_t>(m.cap_pairs); m.cs_l = a.take<float>(m.cap_pairs);
@@ -278,7 +278,7 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
     }
   }
   // the merge slot maps are kept all-NONE between uses
-  cudaMemsetAsync(m.slot, 0xFF, sizeof(uint32_t) * (size_t)16 * cf, s->stream);
+  cudaMemsetAsync(m.slot, 0xFF, sizeof(uint32_t) * (size_t)MAX_BLOCK_WARPS * cf, s->stream);
   // the clears must land before anything else touches the arena, whichever stream it uses
   CK(cudaStreamSynchronize(s->stream));
   m.nf = nf;
@@ -726,9 +726,9 @@ const char* mg_last_error(const MgSim* s) { return s ? s->err.c_str() : g_err.c_
 const char* mg_global_last_error(void) { return g_err.c_str(); }
 int mg_sim_set_options(MgSim* s, const MgOptions* o) {
   if (!s || !o) return fail(s, MG_ERR_ARG, "null argument");
-  if (o->block_threads != 0 && (o->block_threads % 32 != 0 || o->block_threads > 512))
-    return fail(s, MG_ERR_ARG, "block_threads must be a multiple of 32 in [32, 512]");
-  if (o->sweep_warps > 16) return fail(s, MG_ERR_ARG, "sweep_warps must be in [0, 16]");
+  if (o->block_threads != 0 && (o->block_threads % 32 != 0 || o->block_threads > MAX_BLOCK_THREADS))
+    return fail(s, MG_ERR_ARG, "block_threads must be a multiple of 32 in [32, %u]", MAX_BLOCK_THREADS);
+  if (o->sweep_warps > MAX_BLOCK_WARPS) return fail(s, MG_ERR_ARG, "sweep_warps must be in [0, %u]", MAX_BLOCK_WARPS);
   if (o->spin_ns > 100000) return fail(s, MG_ERR_ARG, "spin_ns must be at most 100000");
   s->opt = *o;
   return MG_OK;
@@ -1596,9 +1596,9 @@ int mg_server_create(const MgServerConfig* cfg, MgServer** out) {
   if (v->cfg.memory_budget_bytes == 0) v->cfg.memory_budget_bytes = 150ull << 30;
   if (v->cfg.max_active == 0) v->cfg.max_active = 1024;
   if (!(v->cfg.frame_dt > 0.0f)) v->cfg.frame_dt = 1.0f / 60.0f;
-  if (v->cfg.block_threads != 0 && (v->cfg.block_threads % 32 != 0 || v->cfg.block_threads > 512)) {
+  if (v->cfg.block_threads != 0 && (v->cfg.block_threads % 32 != 0 || v->cfg.block_threads > MAX_BLOCK_THREADS)) {
     delete v;
-    return fail_global(MG_ERR_ARG, "block_threads must be a multiple of 32 in [32, 512]");
+    return fail_global(MG_ERR_ARG, "block_threads must be a multiple of 32 in [32, %u]", MAX_BLOCK_THREADS);
   }
   auto setup = [&]() -> int {
     SCK(cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking));

@@ -9,10 +9,15 @@
 namespace mg {
 
 // n_sub is the sub-step stride of `angles`; mill b runs n_sub_of[b] sub-steps when n_sub_of is
-// given (a batch of mills with different sub-step counts), else n_sub.
-__global__ void __launch_bounds__(512) mill_substeps_kernel(const MillDev* __restrict__ mills, StepUniform* uni,
-                                                            const SubAngles* __restrict__ angles, uint32_t n_sub,
-                                                            const uint32_t* __restrict__ n_sub_of) {
+// given (a batch of mills with different sub-step counts), else n_sub. Two instantiations: up to
+// 512 threads per block (128 registers a thread) and up to 1024 (64 registers, more warps for the
+// per-ball stages); the results do not depend on the block size.
+template <int MAX_THREADS>
+__global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDev* __restrict__ mills,
+                                                                    StepUniform* uni,
+                                                                    const SubAngles* __restrict__ angles,
+                                                                    uint32_t n_sub,
+                                                                    const uint32_t* __restrict__ n_sub_of) {
   __shared__ MillDev m;
   __shared__ FluidShared fs;
   __shared__ DemShared ds;
@@ -85,13 +90,13 @@ __global__ void __launch_bounds__(512) probe_kernel(const MillDev* __restrict__ 
 cudaError_t launch_substeps(const MillDev* mills, uint32_t n_mills, StepUniform* uni, const SubAngles* angles,
                             uint32_t n_sub, const uint32_t* n_sub_of, uint32_t threads, size_t smem_bytes,
                             cudaStream_t stream) {
-  if (threads == 0 || threads > 512) threads = 512;
+  if (threads == 0 || threads > MAX_BLOCK_THREADS) threads = DEFAULT_BLOCK_THREADS;
+  auto kernel = threads > 512 ? mill_substeps_kernel<MAX_BLOCK_THREADS> : mill_substeps_kernel<512>;
   if (smem_bytes > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(mill_substeps_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem_bytes);
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
     if (e != cudaSuccess) return e;
   }
-  mill_substeps_kernel<<<n_mills, threads, smem_bytes, stream>>>(mills, uni, angles, n_sub, n_sub_of);
+  kernel<<<n_mills, threads, smem_bytes, stream>>>(mills, uni, angles, n_sub, n_sub_of);
   return cudaGetLastError();
 }
 
