@@ -552,6 +552,14 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
     const int lane = tid();
     float bin_acc = 0.0f;
     double ix = 0.0, iy = 0.0, ia = 0.0;
+    // the three f64 sums by the order-free exact path when it applies (same bits), else below
+    const bool exact = warp_exact_sum_f64(0.0, n, [&](uint32_t i, double& t) {
+                         if (m.wall_bin[i] < 0) return false; t = (double)m.dv_tmp[i].x; return true; }, ix) &&
+                       warp_exact_sum_f64(0.0, n, [&](uint32_t i, double& t) {
+                         if (m.wall_bin[i] < 0) return false; t = (double)m.dv_tmp[i].y; return true; }, iy) &&
+                       warp_exact_sum_f64(0.0, n, [&](uint32_t i, double& t) {
+                         if (m.wall_bin[i] < 0) return false; t = (double)m.f_tmp[i]; return true; }, ia);
+    if (!exact) ix = iy = ia = 0.0;
     for (uint32_t c = 0; c < n; c += 32) {
       int32_t bin = -1;
       float val = 0.0f, px = 0.0f, py = 0.0f, pa = 0.0f;
@@ -560,6 +568,15 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
         if (bin >= 0) { val = m.wall_val[c + lane]; px = m.dv_tmp[c + lane].x; py = m.dv_tmp[c + lane].y; pa = m.f_tmp[c + lane]; }
       }
       const uint32_t mask = __ballot_sync(FULL, bin >= 0);
+      if (exact) {
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+          const int bt = __shfl_sync(FULL, bin, t);
+          const float vt = __shfl_sync(FULL, val, t);
+          if (((mask >> t) & 1u) && bt == lane) bin_acc += vt;
+        }
+        continue;
+      }
 #pragma unroll
       for (int t = 0; t < 32; ++t) {
         const int bt = __shfl_sync(FULL, bin, t);
@@ -605,6 +622,15 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       const int lane = tid();
       float work = 0.0f;
       double ix = S.dscal[0], iy = S.dscal[1], ia = S.dscal[2];
+      // the three f64 sums by the order-free exact path when it applies (same bits), else below
+      double ex_ix, ex_iy, ex_ia;
+      const bool exact =
+          warp_exact_sum_f64(ix, n, [&](uint32_t i, double& t) {
+            if (m.wall_bin[i] < 0) return false; t = (double)(mass * V2(m.dv_tmp[i]).x); return true; }, ex_ix) &&
+          warp_exact_sum_f64(iy, n, [&](uint32_t i, double& t) {
+            if (m.wall_bin[i] < 0) return false; t = (double)(mass * V2(m.dv_tmp[i]).y); return true; }, ex_iy) &&
+          warp_exact_sum_f64(ia, n, [&](uint32_t i, double& t) {
+            if (m.wall_bin[i] < 0) return false; t = (double)cross2(V2(X[i]), mass * V2(m.dv_tmp[i])); return true; }, ex_ia);
       for (uint32_t c = 0; c < n; c += 32) {
         bool touched = c + lane < n && m.wall_bin[c + lane] >= 0;
         float wk = 0.0f, jx = 0.0f, jy = 0.0f, ja = 0.0f;
@@ -617,6 +643,14 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
           ja = cross2(x, mass * dv);
         }
         const uint32_t mask = __ballot_sync(FULL, touched);
+        if (exact) {
+#pragma unroll
+          for (int t = 0; t < 32; ++t) {
+            const float wt = __shfl_sync(FULL, wk, t);
+            if ((mask >> t) & 1u) work += wt;
+          }
+          continue;
+        }
 #pragma unroll
         for (int t = 0; t < 32; ++t) {
           const float wt = __shfl_sync(FULL, wk, t), xt = __shfl_sync(FULL, jx, t), yt = __shfl_sync(FULL, jy, t);
@@ -630,6 +664,11 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
         }
       }
       __syncwarp();
+      if (exact) {
+        ix = ex_ix;
+        iy = ex_iy;
+        ia = ex_ia;
+      }
       if (lane == 0) { S.dscal[0] = ix; S.dscal[1] = iy; S.dscal[2] = ia; out.fs.wall_work_j = work; }
     }
     __syncthreads();

@@ -346,13 +346,75 @@ __device__ __forceinline__ void warp_merge(bool acc, uint32_t j, float v0, V2 v1
   __syncwarp();
 }
 
+// Exponent of the value of the lowest set bit of a finite nonzero double: t is an integer
+// multiple of 2^granularity_exp(t).
+__device__ __forceinline__ int granularity_exp(double t) {
+  const unsigned long long bits = (unsigned long long)__double_as_longlong(t);
+  const int ex = (int)((bits >> 52) & 0x7ffull);
+  const unsigned long long mant = bits & 0xfffffffffffffull;
+  const unsigned long long sig = ex ? (mant | (1ull << 52)) : mant;
+  const int e = ex ? ex - 1075 : -1074;
+  return e + __ffsll((long long)sig) - 1;
+}
+
+// The f64 sum init + f(0) + ... + f(n-1) when it can be formed in any order with the same bits:
+// if every term (and init) is an integer multiple of 2^G and the sum of magnitudes stays below
+// 2^(G+52), every partial sum of every order is an integer multiple of 2^G below 2^(G+53) in
+// magnitude, exactly representable, so no addition rounds and the left-to-right result equals
+// the per-lane-then-tree result computed here. Terms widened from f32 (kinetic energies, wall
+// impulses) nearly always qualify. Returns false (and no sum) when the condition fails or a term
+// is not finite; the caller then folds in order.
+template <class F>
+__device__ __forceinline__ bool warp_exact_sum_f64(double init, uint32_t n, F f, double& out) {
+  const uint32_t lane = threadIdx.x & 31u;
+  double s = 0.0, sabs = 0.0;
+  int g = 2000;
+  bool finite = true;
+  for (uint32_t i = lane; i < n; i += 32) {
+    double t = 0.0;
+    if (!f(i, t) || t == 0.0) continue;
+    if (!isfinite(t)) { finite = false; continue; }
+    s += t;
+    sabs += fabs(t);
+    g = min(g, granularity_exp(t));
+  }
+  if (lane == 0 && init != 0.0) {
+    if (!isfinite(init)) finite = false;
+    else {
+      s += init;
+      sabs += fabs(init);
+      g = min(g, granularity_exp(init));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_xor_sync(FULL, s, o);
+    sabs += __shfl_xor_sync(FULL, sabs, o);
+    g = min(g, __shfl_xor_sync(FULL, g, o));
+  }
+  if (!__all_sync(FULL, finite)) return false;
+  if (g == 2000) {  // nothing but zero terms: init stays, unless it is a zero itself (sign)
+    if (init == 0.0) return false;
+    out = init;
+    return true;
+  }
+  if (!(sabs < ldexp(1.0, g + 52))) return false;
+  if (s == 0.0) return false;  // an exact zero: its sign depends on the order, fold in order
+  out = s;
+  return true;
+}
+
 // Sequential-order reduction acc = (((init + f(0)) + f(1)) + ...) + f(n-1), with the exact
 // rounding of a one-thread loop, computed by one warp: the lanes evaluate 32 consecutive terms in
 // parallel (coalesced loads), then every lane adds them in index order by shuffles. Terms for
 // which f returns false are skipped (not added). Returns the result to all lanes of the warp.
+// f64 sums first try warp_exact_sum_f64, whose result is the same bits when it applies.
 template <class T, class F>
 __device__ __forceinline__ T warp_ordered_sum(T init, uint32_t n, F f) {
   const uint32_t lane = threadIdx.x & 31u;
+  if constexpr (sizeof(T) == 8) {
+    double r;
+    if (warp_exact_sum_f64(init, n, f, r)) return r;
+  }
   T acc = init;
   // software pipeline: the next chunk's terms are evaluated (loads in flight) before the current
   // chunk is folded
