@@ -304,7 +304,18 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
   // step 5 friction (dem.rs:782-882)
   const MgMediaParams& md = U.media;
   auto load_contact = [&](uint32_t k) { return make_uint3(m.act_i[k], m.act_j[k], __float_as_uint(m.act_l[k])); };
-  run_chunked(na, m.dm_pa, m.dm_pb, load_contact, [&](uint32_t k, uint3 d) {
+  // dependency levels of the active contacts, shared by the friction and restitution sweeps:
+  // contacts of one level share no ball, so each level runs in parallel
+  const uint32_t nlev_c = compute_levels(na, m.dm_pa, m.dm_pb, m.dm_lvl);
+  bucket_levels(na, m.dm_lvl, nlev_c, m.lev_start, m.lev_cur, m.lev_items);
+  stage_mark(out.stage, 38);
+  auto contact_sweep = [&](auto body) {
+    run_levels(nlev_c, m.lev_start, [&](uint32_t q) {
+      const uint32_t k = m.lev_items[q];
+      body(k, load_contact(k));
+    });
+  };
+  contact_sweep([&](uint32_t k, uint3 d) {
     const uint32_t i = d.x, j = d.y;
     const float lambda_n = __uint_as_float(d.z);
     if (j != NONE) {
@@ -390,7 +401,7 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
   __syncthreads();
   // step 6 restitution with impact accounting (dem.rs:909-1019); per-item records are compacted
   // in sweep order afterwards
-  run_chunked(na, m.dm_pa, m.dm_pb, load_contact, [&](uint32_t k, uint3 d) {
+  contact_sweep([&](uint32_t k, uint3 d) {
     const uint32_t i = d.x, j = d.y;
     m.act_flag[k] = 0;
     if (j != NONE) {
