@@ -342,6 +342,52 @@ int mg_batch_last_kernel_ms(MgBatch* batch, float* ms, uint64_t* launches);
 /* Device memory a handle holds (its arena plus launch blocks), for admission by footprint. */
 int mg_sim_footprint(const MgSim* sim, uint64_t* device_bytes);
 
+/* ---- grinding-proxy statistics and seed sweeps ----
+ * StressMetrics (stress.rs:186-273), what Simulation::metrics().stress reports (lib.rs:370-390):
+ * per-ball impact rates by class (ball-ball drop, ball-ball shear, ball-wall drop, ball-wall
+ * shear), mean scaled stress energies, wall power per ball, effective power above the six
+ * thresholds (multiples of m g d) and the cumulative energies. */
+typedef struct MgStressMetrics {
+  float ball_mass_3d_kg, scale_energy_j;
+  float impacts_per_ball_per_s[4];
+  float impacts_total_per_ball_per_s;
+  float mean_se_scaled[4];
+  float mean_se_scaled_drop, mean_se_scaled_shear, stress_intensity_scaled;
+  float wall_power_per_ball_w, specific_power_w_per_kg;
+  float thresholds_scaled[6];
+  float effective_power_per_ball_w[6];
+  float reserved0;
+  double cumulative_wall_energy_per_ball_j, cumulative_specific_energy_j_per_kg;
+  double cumulative_effective_energy_per_ball_j[6];
+} MgStressMetrics;
+int mg_stress_metrics(MgSim* sim, MgStressMetrics* out);
+
+/* batch::run_seed (batch.rs:40-107): window means of one seed's run. values[k] is named by
+ * mg_seed_value_name(k): the 16 per-frame stress scalars averaged over the measured frames, then
+ * the exact window powers from the cumulative energies (specific power and the six effective
+ * powers per ball). */
+#define MG_SEED_VALUES 23
+typedef struct MgSeedResult {
+  uint64_t seed;
+  double window_s;                /* simulated seconds averaged over */
+  float coarse_graining_factor;   /* k of the run; the statistics are meaningless for k > 1 */
+  float reserved0;
+  double values[MG_SEED_VALUES];
+  double power_drift_rel_per_rev; /* least-squares slope of the wall power per revolution / mean */
+} MgSeedResult;
+const char* mg_seed_value_name(uint32_t k);
+/* run_seed for every seeds[i] (replacing params->simulation.seed): warm-up revolutions, then
+ * measured revolutions (>= 1). The device library advances all seeds together, one launch per
+ * frame (a batch); each seed's numbers are those of run_seed on that seed alone. */
+int mg_seed_sweep(const MgParams* params, const uint64_t* seeds, uint32_t n_seeds, float warmup_revolutions,
+                  float measure_revolutions, MgSeedResult* out);
+/* batch::combine (batch.rs:161-190): per value, the mean over seeds and its standard error
+ * (sample standard deviation with n - 1, over sqrt(n); 0 for one seed). */
+int mg_seed_combine(const MgSeedResult* results, uint32_t n, double* mean, double* std_err);
+/* batch.rs:141-159 drift_per_rev: slope of y against the frame index relative to the mean of y,
+ * per revolution of frames_per_rev frames (0 for fewer than two samples or a zero mean). */
+double mg_seed_drift_per_rev(const double* y, uint32_t n, double frames_per_rev);
+
 /* ---- request server: continuous batching of mill jobs. No single reference counterpart (the
  * reference runs one Simulation per web worker, worker.ts:138-142, and seed sweeps one after
  * another, batch.rs:40-191). Jobs (Params + a simulated horizon) wait in a queue and are admitted

@@ -171,6 +171,27 @@ class ServerStats(_S):
                 ("last_frame_ms", C.c_float), ("last_kernel_ms", C.c_float)]
 
 
+class StressMetrics(_S):
+    _fields_ = [("ball_mass_3d_kg", C.c_float), ("scale_energy_j", C.c_float),
+                ("impacts_per_ball_per_s", C.c_float * 4), ("impacts_total_per_ball_per_s", C.c_float),
+                ("mean_se_scaled", C.c_float * 4), ("mean_se_scaled_drop", C.c_float),
+                ("mean_se_scaled_shear", C.c_float), ("stress_intensity_scaled", C.c_float),
+                ("wall_power_per_ball_w", C.c_float), ("specific_power_w_per_kg", C.c_float),
+                ("thresholds_scaled", C.c_float * 6), ("effective_power_per_ball_w", C.c_float * 6),
+                ("reserved0", C.c_float), ("cumulative_wall_energy_per_ball_j", C.c_double),
+                ("cumulative_specific_energy_j_per_kg", C.c_double),
+                ("cumulative_effective_energy_per_ball_j", C.c_double * 6)]
+
+
+SEED_VALUES = 23
+
+
+class SeedResult(_S):
+    _fields_ = [("seed", C.c_uint64), ("window_s", C.c_double), ("coarse_graining_factor", C.c_float),
+                ("reserved0", C.c_float), ("values", C.c_double * SEED_VALUES),
+                ("power_drift_rel_per_rev", C.c_double)]
+
+
 P = C.POINTER
 f32p = P(C.c_float)
 u32p = P(C.c_uint32)
@@ -223,6 +244,11 @@ SIGNATURES = [
     ("probe_neighbor_lists", C.c_int, [f32p, C.c_uint32, C.c_float, u32p, u32p, C.c_uint32, u32p]),
     ("last_neighbor_lists", C.c_int, [vp, u32p, u32p, C.c_uint32, u32p]),
     ("last_ball_pairs", C.c_int, [vp, u32p, C.c_uint32, u32p]),
+    ("stress_metrics", C.c_int, [vp, P(StressMetrics)]),
+    ("seed_value_name", C.c_char_p, [C.c_uint32]),
+    ("seed_sweep", C.c_int, [P(Params), P(C.c_uint64), C.c_uint32, C.c_float, C.c_float, P(SeedResult)]),
+    ("seed_combine", C.c_int, [P(SeedResult), C.c_uint32, P(C.c_double), P(C.c_double)]),
+    ("seed_drift_per_rev", C.c_double, [P(C.c_double), C.c_uint32, C.c_double]),
 ]
 
 # entry points only the device library exports

@@ -1844,3 +1844,188 @@ int mg_server_stats(MgServer* v, MgServerStats* out) {
 }
 
 }  // extern "C"
+
+// ====================================================================== grinding statistics
+namespace {
+
+const double THRESHOLDS_REL[6] = {0.03, 0.1, 0.3, 1.0, 3.0, 10.0};  // stress.rs:42
+
+// StressAccum::metrics (stress.rs:186-237) with Simulation::metrics's arguments (lib.rs:383-390):
+// the ball count, the 3D ball mass m3 = disc mass * 4/3 r, m3 g d and the EMA power draw.
+MgStressMetrics stress_metrics_of(const MgSim* s) {
+  const double r = (double)s->bmat.radius;
+  const double m3 = (double)s->bmat.mass * 4.0 / 3.0 * r;
+  const double d = 2.0 * r;
+  const double scale_j = m3 * 9.81 * d;
+  const Stress& st = s->stress;
+  const double n = (double)std::max<uint32_t>(s->nb, 1u);
+  const double power_draw_w = (double)s->power;
+  MgStressMetrics o;
+  std::memset(&o, 0, sizeof(o));
+  for (int c = 0; c < 4; ++c) {
+    o.impacts_per_ball_per_s[c] = (float)(st.count_rate[c] / n);
+    if (st.count_rate[c] > 0.0) o.mean_se_scaled[c] = (float)(st.se_hat_rate[c] / st.count_rate[c]);
+  }
+  auto pooled = [&](int a, int b) {
+    double w = st.count_rate[a] + st.count_rate[b];
+    return w > 0.0 ? (float)((st.se_hat_rate[a] + st.se_hat_rate[b]) / w) : 0.0f;
+  };
+  const double total = st.total_rate();
+  const double power_per_ball = power_draw_w * d / n;
+  o.ball_mass_3d_kg = (float)m3;
+  o.scale_energy_j = (float)scale_j;
+  o.impacts_total_per_ball_per_s = (float)(total / n);
+  o.mean_se_scaled_drop = pooled(0, 2);
+  o.mean_se_scaled_shear = pooled(1, 3);
+  double se_sum = 0.0;
+  for (int c = 0; c < 4; ++c) se_sum += st.se_hat_rate[c];
+  o.stress_intensity_scaled = total > 0.0 ? (float)(se_sum / total) : 0.0f;
+  o.wall_power_per_ball_w = (float)power_per_ball;
+  o.specific_power_w_per_kg = (float)(power_per_ball / m3);
+  for (int q = 0; q < 6; ++q) {
+    o.thresholds_scaled[q] = (float)THRESHOLDS_REL[q];
+    o.effective_power_per_ball_w[q] = (float)(st.above_rate_j[q] / n);
+    o.cumulative_effective_energy_per_ball_j[q] = st.cum_above_j[q] / n;
+  }
+  o.cumulative_wall_energy_per_ball_j = st.cum_wall_j * d / n;
+  o.cumulative_specific_energy_j_per_kg = st.cum_wall_j * d / n / m3;
+  return o;
+}
+
+// batch.rs:126-139: the 16 per-frame scalars in name order
+void seed_frame_values(const MgStressMetrics& m, double* v) {
+  v[0] = m.specific_power_w_per_kg;
+  v[1] = m.wall_power_per_ball_w;
+  v[2] = m.impacts_total_per_ball_per_s;
+  v[3] = m.mean_se_scaled_drop;
+  v[4] = m.mean_se_scaled_shear;
+  v[5] = m.stress_intensity_scaled;
+  for (int c = 0; c < 4; ++c) v[6 + c] = m.impacts_per_ball_per_s[c];
+  for (int q = 0; q < 6; ++q) v[10 + q] = m.effective_power_per_ball_w[q];
+}
+
+// batch.rs:141-159
+double drift_per_rev_of(const double* y, size_t len, double frames_per_rev) {
+  if (len < 2) return 0.0;
+  const double n = (double)len;
+  double sum = 0.0;
+  for (size_t i = 0; i < len; ++i) sum += y[i];
+  const double mean = sum / n, xm = (n - 1.0) / 2.0;
+  double sxy = 0.0, sxx = 0.0;
+  for (size_t i = 0; i < len; ++i) {
+    sxy += ((double)i - xm) * (y[i] - mean);
+    sxx += ((double)i - xm) * ((double)i - xm);
+  }
+  return std::fabs(mean) > 0.0 && sxx > 0.0 ? sxy / sxx * frames_per_rev / std::fabs(mean) : 0.0;
+}
+
+const char* const SEED_VALUE_NAMES[MG_SEED_VALUES] = {
+    "specific_power_w_per_kg", "wall_power_per_ball_w", "impacts_total_per_ball_per_s", "mean_se_scaled_drop",
+    "mean_se_scaled_shear", "stress_intensity_scaled", "impacts_per_ball_per_s.ball_ball_drop",
+    "impacts_per_ball_per_s.ball_ball_shear", "impacts_per_ball_per_s.ball_wall_drop",
+    "impacts_per_ball_per_s.ball_wall_shear", "effective_power_per_ball_w.thr0", "effective_power_per_ball_w.thr1",
+    "effective_power_per_ball_w.thr2", "effective_power_per_ball_w.thr3", "effective_power_per_ball_w.thr4",
+    "effective_power_per_ball_w.thr5", "window_specific_power_w_per_kg", "window_effective_power_per_ball_w.thr0",
+    "window_effective_power_per_ball_w.thr1", "window_effective_power_per_ball_w.thr2",
+    "window_effective_power_per_ball_w.thr3", "window_effective_power_per_ball_w.thr4",
+    "window_effective_power_per_ball_w.thr5"};
+
+}  // namespace
+
+extern "C" {
+
+int mg_stress_metrics(MgSim* s, MgStressMetrics* out) {
+  if (!s || !out) return fail_global(MG_ERR_ARG, "null argument");
+  *out = stress_metrics_of(s);
+  return MG_OK;
+}
+
+const char* mg_seed_value_name(uint32_t k) { return k < MG_SEED_VALUES ? SEED_VALUE_NAMES[k] : ""; }
+
+// batch::run_seed for every seed at once: the seeds are the mills of one batch, so every frame of
+// the sweep is one launch; per seed the frames, statistics and sums are those of run_seed alone.
+int mg_seed_sweep(const MgParams* params, const uint64_t* seeds, uint32_t n_seeds, float warmup_revolutions,
+                  float measure_revolutions, MgSeedResult* out) {
+  if (!params || n_seeds == 0 || !seeds || !out) return fail_global(MG_ERR_ARG, "null argument or no seeds");
+  const double omega = (double)(mgh::mill_rpm(params->mill) * 2.0f * mgh::PI_F / 60.0f);
+  if (omega <= 1e-6) return fail_global(MG_ERR_ARG, "mill speed must be > 0");
+  if (!(measure_revolutions >= 1.0f && warmup_revolutions >= 0.0f))
+    return fail_global(MG_ERR_ARG, "measure_revolutions must be >= 1 and warmup_revolutions >= 0");
+  const double rev_s = 6.283185307179586 / omega;
+  const uint32_t warm = (uint32_t)std::round((double)warmup_revolutions * rev_s * 60.0);
+  const uint32_t meas = (uint32_t)std::max(std::round((double)measure_revolutions * rev_s * 60.0), 1.0);
+  const float frame_s = 1.0f / 60.0f;
+  std::vector<MgParams> ps(n_seeds, *params);
+  for (uint32_t i = 0; i < n_seeds; ++i) ps[i].simulation.seed = seeds[i];
+  MgBatch* b = nullptr;
+  int rc = mg_batch_create(ps.data(), n_seeds, &b);
+  if (rc) return rc;
+  if (warm) rc = mg_batch_step_frames(b, warm, frame_s);
+  std::vector<MgStressMetrics> start(n_seeds);
+  for (uint32_t i = 0; i < n_seeds && !rc; ++i) start[i] = stress_metrics_of(b->mills[i]);
+  std::vector<double> sum((size_t)n_seeds * 16, 0.0), powers((size_t)n_seeds * meas);
+  for (uint32_t f = 0; f < meas && !rc; ++f) {
+    rc = mg_batch_step_frames(b, 1, frame_s);
+    for (uint32_t i = 0; i < n_seeds && !rc; ++i) {
+      const MgStressMetrics m = stress_metrics_of(b->mills[i]);
+      double v[16];
+      seed_frame_values(m, v);
+      for (int k = 0; k < 16; ++k) sum[(size_t)i * 16 + k] += v[k];
+      powers[(size_t)i * meas + f] = (double)m.wall_power_per_ball_w;
+    }
+  }
+  if (rc) {
+    std::string e = b->err;
+    mg_batch_destroy(b);
+    return fail_global(rc, "%s", e.c_str());
+  }
+  const double n = (double)meas, window_s = n * (double)frame_s;
+  const float k_cg = mgh::effective_media(*params).scale_factor;
+  for (uint32_t i = 0; i < n_seeds; ++i) {
+    const MgStressMetrics end = stress_metrics_of(b->mills[i]);
+    MgSeedResult& r = out[i];
+    std::memset(&r, 0, sizeof(r));
+    r.seed = seeds[i];
+    r.window_s = window_s;
+    r.coarse_graining_factor = k_cg;
+    for (int k = 0; k < 16; ++k) r.values[k] = sum[(size_t)i * 16 + k] / n;
+    r.values[16] = (end.cumulative_specific_energy_j_per_kg - start[i].cumulative_specific_energy_j_per_kg) / window_s;
+    for (int q = 0; q < 6; ++q)
+      r.values[17 + q] =
+          (end.cumulative_effective_energy_per_ball_j[q] - start[i].cumulative_effective_energy_per_ball_j[q]) /
+          window_s;
+    r.power_drift_rel_per_rev = drift_per_rev_of(&powers[(size_t)i * meas], meas, rev_s * 60.0);
+  }
+  mg_batch_destroy(b);
+  return MG_OK;
+}
+
+// batch.rs:161-190 combine
+int mg_seed_combine(const MgSeedResult* r, uint32_t n, double* mean, double* std_err) {
+  if (n == 0) return fail_global(MG_ERR_ARG, "no results to combine");
+  if (!r || !mean || !std_err) return fail_global(MG_ERR_ARG, "null argument");
+  const double nn = (double)n;
+  for (int k = 0; k < MG_SEED_VALUES; ++k) {
+    double s = 0.0;
+    for (uint32_t i = 0; i < n; ++i) s += r[i].values[k];
+    const double m = s / nn;
+    double se = 0.0;
+    if (n >= 2) {
+      double v = 0.0;
+      for (uint32_t i = 0; i < n; ++i) {
+        double dv = r[i].values[k] - m;
+        v += dv * dv;
+      }
+      se = std::sqrt(v / (nn - 1.0) / nn);
+    }
+    mean[k] = m;
+    std_err[k] = se;
+  }
+  return MG_OK;
+}
+
+double mg_seed_drift_per_rev(const double* y, uint32_t n, double frames_per_rev) {
+  return y ? drift_per_rev_of(y, n, frames_per_rev) : 0.0;
+}
+
+}  // extern "C"

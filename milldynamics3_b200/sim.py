@@ -270,6 +270,12 @@ class Simulation:
         self._c(self.lib.stress_histogram_rate(self.h, out))
         return np.array(list(out))
 
+    def stress_metrics(self) -> capi.StressMetrics:
+        """Simulation::metrics (lib.rs:383-390 over StressAccum::metrics, stress.rs:186-237)."""
+        out = capi.StressMetrics()
+        self._c(self.lib.stress_metrics(self.h, C.byref(out)))
+        return out
+
     def last_step_stats(self):
         f, d, c = capi.FluidStepStats(), capi.DemStepStats(), capi.StepCounters()
         self._c(self.lib.last_step_stats(self.h, C.byref(f), C.byref(d), C.byref(c)))

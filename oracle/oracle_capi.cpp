@@ -404,3 +404,176 @@ float or_rng_next_f32(uint64_t* state) {
 int or_se_bin(double e) { return se_bin(e); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- stress metrics, seed sweeps
+namespace {
+
+const double THRESHOLDS_REL[6] = {0.03, 0.1, 0.3, 1.0, 3.0, 10.0};  // stress.rs:42
+
+// StressAccum::metrics (stress.rs:186-237) with Simulation::metrics's arguments (lib.rs:383-390)
+MgStressMetrics stress_metrics(const Simulation& sim) {
+  double m3, scale_j, d;
+  sim.stress_scales(&m3, &scale_j, &d);
+  const StressAccum& st = sim.stress;
+  const double n = (double)std::max<size_t>(sim.balls.len(), 1);
+  const double power_draw_w = (double)sim.power_draw_w;
+  MgStressMetrics o;
+  std::memset(&o, 0, sizeof(o));
+  for (int c = 0; c < 4; ++c) {
+    o.impacts_per_ball_per_s[c] = (float)(st.count_rate[c] / n);
+    if (st.count_rate[c] > 0.0) o.mean_se_scaled[c] = (float)(st.se_hat_rate[c] / st.count_rate[c]);
+  }
+  auto pooled = [&](int a, int b) {
+    double w = st.count_rate[a] + st.count_rate[b];
+    return w > 0.0 ? (float)((st.se_hat_rate[a] + st.se_hat_rate[b]) / w) : 0.0f;
+  };
+  const double total = st.total_rate();
+  const double power_per_ball = power_draw_w * d / n;
+  o.ball_mass_3d_kg = (float)m3;
+  o.scale_energy_j = (float)scale_j;
+  o.impacts_total_per_ball_per_s = (float)(total / n);
+  o.mean_se_scaled_drop = pooled(0, 2);
+  o.mean_se_scaled_shear = pooled(1, 3);
+  double se_sum = 0.0;
+  for (int c = 0; c < 4; ++c) se_sum += st.se_hat_rate[c];
+  o.stress_intensity_scaled = total > 0.0 ? (float)(se_sum / total) : 0.0f;
+  o.wall_power_per_ball_w = (float)power_per_ball;
+  o.specific_power_w_per_kg = (float)(power_per_ball / m3);
+  for (int q = 0; q < 6; ++q) {
+    o.thresholds_scaled[q] = (float)THRESHOLDS_REL[q];
+    o.effective_power_per_ball_w[q] = (float)(st.above_rate_j[q] / n);
+    o.cumulative_effective_energy_per_ball_j[q] = st.cum_above_j[q] / n;
+  }
+  o.cumulative_wall_energy_per_ball_j = st.cum_wall_j * d / n;
+  o.cumulative_specific_energy_j_per_kg = st.cum_wall_j * d / n / m3;
+  return o;
+}
+
+// batch.rs:126-139 values(): the 16 per-frame scalars in name order
+void frame_values(const MgStressMetrics& m, double* v) {
+  v[0] = m.specific_power_w_per_kg;
+  v[1] = m.wall_power_per_ball_w;
+  v[2] = m.impacts_total_per_ball_per_s;
+  v[3] = m.mean_se_scaled_drop;
+  v[4] = m.mean_se_scaled_shear;
+  v[5] = m.stress_intensity_scaled;
+  for (int c = 0; c < 4; ++c) v[6 + c] = m.impacts_per_ball_per_s[c];
+  for (int q = 0; q < 6; ++q) v[10 + q] = m.effective_power_per_ball_w[q];
+}
+
+// batch.rs:141-159
+double drift_per_rev(const double* y, size_t len, double frames_per_rev) {
+  if (len < 2) return 0.0;
+  const double n = (double)len;
+  double sum = 0.0;
+  for (size_t i = 0; i < len; ++i) sum += y[i];
+  const double mean = sum / n, xm = (n - 1.0) / 2.0;
+  double sxy = 0.0, sxx = 0.0;
+  for (size_t i = 0; i < len; ++i) {
+    sxy += ((double)i - xm) * (y[i] - mean);
+    sxx += ((double)i - xm) * ((double)i - xm);
+  }
+  return std::fabs(mean) > 0.0 && sxx > 0.0 ? sxy / sxx * frames_per_rev / std::fabs(mean) : 0.0;
+}
+
+const char* const SEED_VALUE_NAMES[MG_SEED_VALUES] = {
+    "specific_power_w_per_kg", "wall_power_per_ball_w", "impacts_total_per_ball_per_s", "mean_se_scaled_drop",
+    "mean_se_scaled_shear", "stress_intensity_scaled", "impacts_per_ball_per_s.ball_ball_drop",
+    "impacts_per_ball_per_s.ball_ball_shear", "impacts_per_ball_per_s.ball_wall_drop",
+    "impacts_per_ball_per_s.ball_wall_shear", "effective_power_per_ball_w.thr0", "effective_power_per_ball_w.thr1",
+    "effective_power_per_ball_w.thr2", "effective_power_per_ball_w.thr3", "effective_power_per_ball_w.thr4",
+    "effective_power_per_ball_w.thr5", "window_specific_power_w_per_kg", "window_effective_power_per_ball_w.thr0",
+    "window_effective_power_per_ball_w.thr1", "window_effective_power_per_ball_w.thr2",
+    "window_effective_power_per_ball_w.thr3", "window_effective_power_per_ball_w.thr4",
+    "window_effective_power_per_ball_w.thr5"};
+
+// batch.rs:40-107 run_seed
+int run_seed(const Params& params, uint64_t seed, float warmup_revolutions, float measure_revolutions,
+             MgSeedResult* out) {
+  Params p = params;
+  p.simulation.seed = seed;
+  const double omega = (double)(mill_rpm(p.mill) * 2.0f * PI_F / 60.0f);
+  if (omega <= 1e-6) { g_err = "mill speed must be > 0"; return MG_ERR_ARG; }
+  if (!(measure_revolutions >= 1.0f && warmup_revolutions >= 0.0f)) {
+    g_err = "measure_revolutions must be >= 1 and warmup_revolutions >= 0";
+    return MG_ERR_ARG;
+  }
+  const double rev_s = 6.283185307179586 / omega;
+  Simulation sim;
+  std::string e;
+  if (!Simulation::build(p, nullptr, &sim, &e)) { g_err = e; return MG_ERR_INVALID_PARAMS; }
+  const size_t warm = (size_t)std::round((double)warmup_revolutions * rev_s * 60.0);
+  const size_t meas = (size_t)std::max(std::round((double)measure_revolutions * rev_s * 60.0), 1.0);
+  const float frame_s = 1.0f / 60.0f;
+  for (size_t f = 0; f < warm; ++f) sim.step(frame_s);
+  const MgStressMetrics start = stress_metrics(sim);
+  double sum[16] = {};
+  std::vector<double> powers;
+  powers.reserve(meas);
+  for (size_t f = 0; f < meas; ++f) {
+    sim.step(frame_s);
+    const MgStressMetrics m = stress_metrics(sim);
+    double v[16];
+    frame_values(m, v);
+    for (int k = 0; k < 16; ++k) sum[k] += v[k];
+    powers.push_back((double)m.wall_power_per_ball_w);
+  }
+  const MgStressMetrics end = stress_metrics(sim);
+  const double n = (double)meas, window_s = n * (double)frame_s;
+  std::memset(out, 0, sizeof(*out));
+  out->seed = seed;
+  out->window_s = window_s;
+  out->coarse_graining_factor = effective_media(p).scale_factor;
+  for (int k = 0; k < 16; ++k) out->values[k] = sum[k] / n;
+  out->values[16] = (end.cumulative_specific_energy_j_per_kg - start.cumulative_specific_energy_j_per_kg) / window_s;
+  for (int q = 0; q < 6; ++q)
+    out->values[17 + q] =
+        (end.cumulative_effective_energy_per_ball_j[q] - start.cumulative_effective_energy_per_ball_j[q]) / window_s;
+  out->power_drift_rel_per_rev = drift_per_rev(powers.data(), powers.size(), rev_s * 60.0);
+  return MG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int or_stress_metrics(OrSim* s, MgStressMetrics* out) {
+  if (!s || !out) { g_err = "null argument"; return MG_ERR_ARG; }
+  *out = stress_metrics(s->sim);
+  return MG_OK;
+}
+const char* or_seed_value_name(uint32_t k) { return k < MG_SEED_VALUES ? SEED_VALUE_NAMES[k] : ""; }
+int or_seed_sweep(const MgParams* params, const uint64_t* seeds, uint32_t n_seeds, float warmup_revolutions,
+                  float measure_revolutions, MgSeedResult* out) {
+  if (!params || (n_seeds && (!seeds || !out))) { g_err = "null argument"; return MG_ERR_ARG; }
+  for (uint32_t i = 0; i < n_seeds; ++i) {
+    int rc = run_seed(to_p(params), seeds[i], warmup_revolutions, measure_revolutions, &out[i]);
+    if (rc) return rc;
+  }
+  return MG_OK;
+}
+// batch.rs:161-190 combine
+int or_seed_combine(const MgSeedResult* r, uint32_t n, double* mean, double* std_err) {
+  if (n == 0) { g_err = "no results to combine"; return MG_ERR_ARG; }
+  if (!r || !mean || !std_err) { g_err = "null argument"; return MG_ERR_ARG; }
+  const double nn = (double)n;
+  for (int k = 0; k < MG_SEED_VALUES; ++k) {
+    double s = 0.0;
+    for (uint32_t i = 0; i < n; ++i) s += r[i].values[k];
+    const double m = s / nn;
+    double se = 0.0;
+    if (n >= 2) {
+      double v = 0.0;
+      for (uint32_t i = 0; i < n; ++i) { double dv = r[i].values[k] - m; v += dv * dv; }
+      se = std::sqrt(v / (nn - 1.0) / nn);
+    }
+    mean[k] = m;
+    std_err[k] = se;
+  }
+  return MG_OK;
+}
+double or_seed_drift_per_rev(const double* y, uint32_t n, double frames_per_rev) {
+  return drift_per_rev(y, n, frames_per_rev);
+}
+
+}  // extern "C"
