@@ -291,7 +291,8 @@ STAGE_NAMES = [
     "buoyancy: predecessors", "buoyancy: sweep", "DEM: contact ordering", "viscosity: CG iterations (joint)",
     "drag sweep: ball prefetch (sum)", "drag sweep: ball waits (sum)", "drag sweep: ball chain work (sum)",
     "buoyancy sweep: ball prefetch (sum)", "buoyancy sweep: ball waits (sum)",
-    "buoyancy sweep: ball chain work (sum)", "DEM: contact levels", "unused (39)"]
+    "buoyancy sweep: ball chain work (sum)", "DEM: contact levels",
+    "DEM: projection rerun with all pairs (failed check)"]
 assert len(STAGE_NAMES) == 40
 
 

@@ -271,14 +271,15 @@ struct MillDev {
   float* ball_w0;
   // dem workspace
   float2 *bx0, *bvpre;
-  float *bth0, *bompre, *lam_bw, *lam_tot;
+  float *bth0, *bompre, *lam_bw;
+  float2* bxs;    // ball positions at the start of the projection sweep
+  float* bmove;   // per ball largest squared distance from bxs during the projection sweep
   double* f_cw;  // per-ball coupling work of the predict step
   uint32_t *rec_off, *rec_pred, *ball_done;  // per-ball sweep records (cap_nb + 1, cap_recs, cap_nb)
   uint32_t* slot;  // per-warp fluid -> item maps of the in-order merges (MAX_BLOCK_WARPS x cap_nf, all NONE at rest)
   uint32_t *pair_i, *pair_j;
   float* lam_bb;
-  uint32_t *cs_i, *cs_j;  // contacts sorted by (i, j)
-  float* cs_l;
+  uint32_t* pr_list;  // pairs within reach of touching at the start of the projection
   uint32_t* pair_cnt;  // per cell pair counts (cap cells + 1)
   // sweep replay (mill_replay.cuh): predecessors, levels, active contacts of the contact sweeps
   uint32_t *dm_pa, *dm_pb, *dm_lvl, *lev_start, *lev_cur, *lev_items;

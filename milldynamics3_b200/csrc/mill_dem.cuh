@@ -150,13 +150,12 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
   // step 2.5 wall CCD (dem.rs:674-706)
   const float cap_depth = -MAX_RECOVERY_FRACTION * 2.0f * r;
   for (uint32_t i = tid(); i < n; i += nthr()) {
-    V2 x(X[i]);
-    float d_end;
-    V2 nn;
-    drum_sdf_world(U, x, U.to_local_next, U.to_world_next, d_end, nn);
-    float c_end = d_end - r;
+    V2 x(X[i]), pl;
+    // only the distance is used; interior balls are decided without the lifters
+    const bool clear = x.finite() && drum_sdf_clear(U, rotate(x, U.to_local_next), r + cap_depth);
+    float c_end = clear ? 0.0f : drum_sdf_world_dist(U, x, U.to_local_next, pl) - r;
     float t_hit = 1.0f;
-    if (!(c_end >= cap_depth)) {
+    if (!clear && !(c_end >= cap_depth)) {
       float t;
       if (drum_toi_swept(U, V2(m.bx0[i]), x, U.drum_angle, U.drum_angle_next, r, t)) t_hit = fmin_r(1.0f, t);
     }
@@ -170,84 +169,160 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
     }
     m.lam_bw[i] = 0.0f;
   }
-  const uint32_t nitems = np + n;
   for (uint32_t k = tid(); k < np; k += nthr()) m.lam_bb[k] = 0.0f;
-  for (uint32_t k = tid(); k < nitems; k += nthr()) { m.dm_pa[k] = NONE; m.dm_pb[k] = NONE; }
-  // occurrence records of the projection sweep: pair k -> (i, 2k), (j, 2k+1); wall of ball b -> 2np+b
-  for (uint32_t q = tid(); q < 2 * np + n; q += nthr())
-    m.rec_i[q] = q < 2 * np ? ((q & 1u) ? m.pair_j[q >> 1] : m.pair_i[q >> 1]) : q - 2 * np;
+  // step 3 projection: pairs in grid order, then walls, `iters` times (dem.rs:711-750).
+  // A pair that stays apart never acts, so the sweep first runs only the pairs that start within
+  // 2r + reach of touching (their relative order kept) plus every wall, while recording how far
+  // each ball ever gets from its start position (the largest squared distance after any of its
+  // moves). Afterwards every other pair must have stayed apart at all times: its start distance
+  // less both balls' largest excursions exceeds 2r, with margins well above the f32 rounding of
+  // the excursions and of the distance test. Otherwise the positions are restored and all pairs
+  // run. Either way the sweep's result is that of the full order.
+  const float reach = 0.25f * r;
+  const float touch2 = (2.0f * r + reach) * (2.0f * r + reach);
+  for (uint32_t i = tid(); i < n; i += nthr()) { m.bxs[i] = X[i]; m.bmove[i] = 0.0f; }
+  for (uint32_t k = tid(); k < np; k += nthr())
+    m.act_flag[k] = (V2(X[m.pair_i[k]]) - V2(X[m.pair_j[k]])).len2() < touch2 ? 1u : 0u;
+  if (tid() == 0) m.act_flag[np] = 0;
+  __syncthreads();
+  const uint32_t ns = block_exclusive_scan(m.act_flag, np + 1);
+  for (uint32_t k = tid(); k < np; k += nthr())
+    if (m.act_flag[k + 1] != m.act_flag[k]) m.pr_list[m.act_flag[k]] = k;
   __syncthreads();
   stage_mark(out.stage, 15);
-  preds_from_records(m.rec_i, 2 * np + n, n, n, m.bk_start, m.bk_cur, m.bk_order, m.dm_pa, m.dm_pb,
-                     [&](uint32_t q) { return q < 2 * np ? q >> 1 : np + (q - 2 * np); },
-                     [&](uint32_t q) { return q < 2 * np ? (q & 1u) : 0u; });
-  stage_mark(out.stage, 20);
-  // sweep scratch (levels, level-ordered descriptors, multipliers): shared memory after the ball
-  // state when the items fit, global otherwise
   uint32_t *lvl = m.dm_lvl, *di = m.act_i, *dj = m.act_j;
   float* dl = m.act_l;
-  if (staged) {
-    const uint32_t used = (24u * n + 15u) & ~15u;
-    const uint32_t fit = m.smem_bytes > used ? (m.smem_bytes - used) / 16u : 0u;
-    if (nitems <= fit) {
-      lvl = reinterpret_cast<uint32_t*>(dsm + used);
-      di = lvl + nitems;
-      dj = di + nitems;
-      dl = reinterpret_cast<float*>(dj + nitems);
+  // the larger of the recorded and the new squared excursion; a NaN excursion is kept (and
+  // fails the check)
+  auto excursion = [](float cur, V2 d) {
+    const float e = d.len2();
+    return !(e <= cur) ? e : cur;
+  };
+  // npi pair items (pair plist[q], or pair q when plist is null), then the n walls
+  auto project = [&](uint32_t npi, const uint32_t* plist, bool track) {
+    const uint32_t nitems = npi + n;
+    for (uint32_t k = tid(); k < nitems; k += nthr()) { m.dm_pa[k] = NONE; m.dm_pb[k] = NONE; }
+    // occurrence records: pair item q -> (i, 2q), (j, 2q+1); wall of ball b -> 2 npi + b
+    for (uint32_t q = tid(); q < 2 * npi + n; q += nthr()) {
+      if (q < 2 * npi) {
+        const uint32_t k = plist ? plist[q >> 1] : q >> 1;
+        m.rec_i[q] = (q & 1u) ? m.pair_j[k] : m.pair_i[k];
+      } else {
+        m.rec_i[q] = q - 2 * npi;
+      }
+    }
+    __syncthreads();
+    preds_from_records(m.rec_i, 2 * npi + n, n, n, m.bk_start, m.bk_cur, m.bk_order, m.dm_pa, m.dm_pb,
+                       [&](uint32_t q) { return q < 2 * npi ? q >> 1 : npi + (q - 2 * npi); },
+                       [&](uint32_t q) { return q < 2 * npi ? (q & 1u) : 0u; });
+    stage_mark(out.stage, 20);
+    // sweep scratch (levels, level-ordered descriptors, multipliers): shared memory after the
+    // ball state when the items fit, global otherwise
+    lvl = m.dm_lvl; di = m.act_i; dj = m.act_j; dl = m.act_l;
+    if (staged) {
+      const uint32_t used = (24u * n + 15u) & ~15u;
+      const uint32_t fit = m.smem_bytes > used ? (m.smem_bytes - used) / 16u : 0u;
+      if (nitems <= fit) {
+        lvl = reinterpret_cast<uint32_t*>(dsm + used);
+        di = lvl + nitems;
+        dj = di + nitems;
+        dl = reinterpret_cast<float*>(dj + nitems);
+      }
+    }
+    const uint32_t nlev = compute_levels(nitems, m.dm_pa, m.dm_pb, lvl);
+    stage_mark(out.stage, 21);
+    bucket_levels(nitems, lvl, nlev, m.lev_start, m.lev_cur, m.lev_items);
+    // level-ordered sweep descriptors: balls (j = NONE for a wall) and a lambda accumulator
+    for (uint32_t q = tid(); q < nitems; q += nthr()) {
+      const uint32_t k = m.lev_items[q];
+      const uint32_t pk = k < npi ? (plist ? plist[k] : k) : NONE;
+      di[q] = k < npi ? m.pair_i[pk] : k - npi;
+      dj[q] = k < npi ? m.pair_j[pk] : NONE;
+      dl[q] = 0.0f;
+    }
+    __syncthreads();
+    stage_mark(out.stage, 22);
+    for (uint32_t it = 0; it < iters; ++it) {
+      run_levels(nlev, m.lev_start, [&](uint32_t q) {
+        const uint32_t i = di[q], j = dj[q];
+        if (j != NONE) {
+          V2 xi(X[i]), xj(X[j]);
+          // start positions and excursions so far, loaded beside the positions
+          V2 si, sj;
+          float ei = 0.0f, ej = 0.0f;
+          if (track) { si = V2(m.bxs[i]); sj = V2(m.bxs[j]); ei = m.bmove[i]; ej = m.bmove[j]; }
+          V2 delta = xi - xj;
+          float dist = delta.len();
+          float c = dist - 2.0f * r;
+          if (c >= 0.0f) return;
+          V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
+          float w_sum = w + w;
+          if (w_sum <= 0.0f) return;
+          float c_eff = fmax_r(c, cap_depth);
+          float d_lambda = -c_eff / w_sum;
+          const V2 xin = xi + w * d_lambda * n_hat, xjn = xj - w * d_lambda * n_hat;
+          X[i] = xin.f2();
+          X[j] = xjn.f2();
+          dl[q] += d_lambda;
+          if (track) {
+            m.bmove[i] = excursion(ei, V2(xin.f2()) - si);
+            m.bmove[j] = excursion(ej, V2(xjn.f2()) - sj);
+          }
+        } else {
+          V2 x(X[i]), pl, si;
+          float ei = 0.0f;
+          if (track) { si = V2(m.bxs[i]); ei = m.bmove[i]; }
+          if (x.finite() && drum_sdf_clear(U, rotate(x, U.to_local_next), r)) return;  // c >= 0 certainly
+          float d = drum_sdf_world_dist(U, x, U.to_local_next, pl);
+          float c = d - r;
+          if (c >= 0.0f) return;
+          if (w <= 0.0f) return;
+          V2 n_hat = drum_sdf_world_normal(U, x, pl, U.to_world_next);
+          float c_eff = fmax_r(c, cap_depth);
+          float d_lambda = -c_eff / w;
+          const V2 xn = x + w * d_lambda * n_hat;
+          X[i] = xn.f2();
+          dl[q] += d_lambda;
+          if (track) m.bmove[i] = excursion(ei, V2(xn.f2()) - si);
+        }
+      });
+    }
+    return nitems;
+  };
+  const uint32_t* plist = m.pr_list;
+  uint32_t npi = ns;
+  uint32_t nrun = project(ns, m.pr_list, ns < np);
+  if (ns < np) {
+    // every pair left out stayed more than 2r apart (triangle inequality over the excursions)
+    const double sep = 2.0 * (double)r * (1.0 + 1e-5);
+    bool bad = false;
+    for (uint32_t k = tid(); k < np; k += nthr()) {
+      if (m.act_flag[k + 1] != m.act_flag[k]) continue;
+      const uint32_t i = m.pair_i[k], j = m.pair_j[k];
+      const float2 a = m.bxs[i], b = m.bxs[j];
+      const double dx = (double)a.x - (double)b.x, dy = (double)a.y - (double)b.y;
+      const double ei = sqrt((double)m.bmove[i]), ej = sqrt((double)m.bmove[j]);
+      const double slack = 1e-6 * (fabs((double)a.x) + fabs((double)a.y) + fabs((double)b.x) + fabs((double)b.y) + ei + ej);
+      if (!(sqrt(dx * dx + dy * dy) - (ei + ej) * (1.0 + 1e-5) - slack >= sep)) bad = true;
+    }
+    if (__syncthreads_or(bad)) {
+      for (uint32_t i = tid(); i < n; i += nthr()) X[i] = m.bxs[i];
+      __syncthreads();
+      stage_mark(out.stage, 39);
+      plist = nullptr;
+      npi = np;
+      nrun = project(np, nullptr, false);
     }
   }
-  const uint32_t nlev = compute_levels(nitems, m.dm_pa, m.dm_pb, lvl);
-  stage_mark(out.stage, 21);
-  bucket_levels(nitems, lvl, nlev, m.lev_start, m.lev_cur, m.lev_items);
-  // level-ordered sweep descriptors: balls (j = NONE for a wall) and a lambda accumulator
-  for (uint32_t q = tid(); q < nitems; q += nthr()) {
-    uint32_t k = m.lev_items[q];
-    di[q] = k < np ? m.pair_i[k] : k - np;
-    dj[q] = k < np ? m.pair_j[k] : NONE;
-    dl[q] = 0.0f;
+  // the accumulated multipliers back to pair / ball order (ContactBook, dem.rs:437-454); pairs
+  // left out keep lambda 0
+  for (uint32_t q = tid(); q < nrun; q += nthr()) {
+    const uint32_t k = m.lev_items[q];
+    if (k < npi) m.lam_bb[plist ? plist[k] : k] = dl[q];
+    else m.lam_bw[k - npi] = dl[q];
   }
   __syncthreads();
-  stage_mark(out.stage, 22);
-  // step 3 projection: pairs in grid order, then walls, `iters` times (dem.rs:711-750)
-  for (uint32_t it = 0; it < iters; ++it) {
-    run_levels(nlev, m.lev_start, [&](uint32_t q) {
-      const uint32_t i = di[q], j = dj[q];
-      if (j != NONE) {
-        V2 xi(X[i]), xj(X[j]);
-        V2 delta = xi - xj;
-        float dist = delta.len();
-        float c = dist - 2.0f * r;
-        if (c >= 0.0f) return;
-        V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
-        float w_sum = w + w;
-        if (w_sum <= 0.0f) return;
-        float c_eff = fmax_r(c, cap_depth);
-        float d_lambda = -c_eff / w_sum;
-        X[i] = (xi + w * d_lambda * n_hat).f2();
-        X[j] = (xj - w * d_lambda * n_hat).f2();
-        dl[q] += d_lambda;
-      } else {
-        V2 x(X[i]);
-        float d;
-        V2 n_hat;
-        drum_sdf_world(U, x, U.to_local_next, U.to_world_next, d, n_hat);
-        float c = d - r;
-        if (c >= 0.0f) return;
-        if (w <= 0.0f) return;
-        float c_eff = fmax_r(c, cap_depth);
-        float d_lambda = -c_eff / w;
-        X[i] = (x + w * d_lambda * n_hat).f2();
-        dl[q] += d_lambda;
-      }
-    });
-  }
-  // the accumulated multipliers back to pair / ball order (ContactBook, dem.rs:437-454)
-  for (uint32_t q = tid(); q < nitems; q += nthr()) {
-    uint32_t k = m.lev_items[q];
-    if (k < np) m.lam_bb[k] = dl[q];
-    else m.lam_bw[k - np] = dl[q];
-  }
-  __syncthreads();
+  const uint32_t nitems = np + n;
   stage_mark(out.stage, 16);
   // step 4 velocity reconstruction (dem.rs:753-756)
   for (uint32_t i = tid(); i < n; i += nthr()) {

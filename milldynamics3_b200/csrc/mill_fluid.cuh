@@ -527,11 +527,12 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
   stage_mark(out.stage, 4);
   // ---- step 4: wall projection (pbf.rs:1635-1653)
   for (uint32_t i = tid(); i < n; i += nthr()) {
-    V2 x(X[i]);
-    float d;
-    V2 normal;
-    drum_sdf_world(U, x, U.to_local_next, U.to_world_next, d, normal);
+    V2 x(X[i]), pl;
+    // the normal only for particles outside the wall; interior particles skip the lifters
+    const float d = x.finite() && drum_sdf_clear(U, rotate(x, U.to_local_next), 0.0f)
+                        ? 0.0f : drum_sdf_world_dist(U, x, U.to_local_next, pl);
     if (d < 0.0f) {
+      const V2 normal = drum_sdf_world_normal(U, x, pl, U.to_world_next);
       x += -d * normal;
       X[i] = x.f2();
       V2 push = mass * (-d * normal) / dt;

@@ -62,6 +62,43 @@ __device__ __forceinline__ void drum_sdf_world(const StepUniform& U, V2 pw, V2 t
   normal = rotate(nl, to_world);
 }
 
+// drum_sdf_world in two halves, for callers that need the normal only in contact: the distance
+// (one SDF evaluation; pl receives the local point) and then the normal at the same point. Same
+// values as drum_sdf_world, including d = 0 and a zero normal for a non-finite point.
+__device__ __forceinline__ float drum_sdf_world_dist(const StepUniform& U, V2 pw, V2 to_local, V2& pl) {
+  if (!pw.finite()) { pl = V2(); return 0.0f; }
+  pl = rotate(pw, to_local);
+  return drum_sdf(U, pl);
+}
+
+__device__ __forceinline__ V2 drum_sdf_world_normal(const StepUniform& U, V2 pw, V2 pl, V2 to_world) {
+  if (!pw.finite()) return V2();
+  const float EPS = 1e-4f;
+  float gx = drum_sdf(U, pl + V2(EPS, 0.0f)) - drum_sdf(U, pl - V2(EPS, 0.0f));
+  float gy = drum_sdf(U, pl + V2(0.0f, EPS)) - drum_sdf(U, pl - V2(0.0f, EPS));
+  V2 grad = V2(gx, gy) / (2.0f * EPS);
+  V2 nl = grad.len2() > 1e-12f ? grad.normalize() : -pl.normalize_or_zero();
+  return rotate(nl, to_world);
+}
+
+// True when the f32 drum SDF at the local point pl is certainly >= bound, decided without
+// evaluating the lifters. Every point q of a lifter quad (R, -b), (R, b), (R - h, t), (R - h, -t)
+// with 0 < h < R and b, t > 0 has |q| >= R - h, so the circle term and each lifter term are both
+// at least (R - h) - |pl| in exact arithmetic; the margin (1e-4 R) exceeds the f32 rounding of the
+// full evaluation by orders of magnitude. False (evaluate in full) for other lifter shapes and for
+// non-finite points.
+__device__ __forceinline__ bool drum_sdf_clear(const StepUniform& U, V2 pl, float bound) {
+  double inner = (double)U.drum_radius;
+  if (U.lifter_count != 0) {
+    if (!(U.lifter_height > 0.0f && U.lifter_height < U.drum_radius && U.lifter_base_half > 0.0f &&
+          U.lifter_top_half > 0.0f))
+      return false;
+    inner -= (double)U.lifter_height;
+  }
+  const double pr = sqrt((double)pl.x * (double)pl.x + (double)pl.y * (double)pl.y);
+  return inner - pr >= (double)bound + 1e-4 * (double)U.drum_radius;
+}
+
 __device__ __forceinline__ V2 wall_velocity(float omega, V2 p) { return omega * V2(-p.y, p.x); }
 
 // geometry.rs:146-194 Drum::toi_swept; returns false for None.

@@ -260,13 +260,13 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
     m.ball_v0 = a.take<float2>(cb); m.ball_w0 = a.take<float>(cb);
     m.bx0 = a.take<float2>(cb); m.bvpre = a.take<float2>(cb);
     m.bth0 = a.take<float>(cb); m.bompre = a.take<float>(cb); m.lam_bw = a.take<float>(cb);
-    m.lam_tot = a.take<float>(cb); m.f_cw = a.take<double>(cb);
+    m.bxs = a.take<float2>(cb); m.bmove = a.take<float>(cb); m.f_cw = a.take<double>(cb);
     m.rec_off = a.take<uint32_t>(cb + 1); m.rec_pred = a.take<uint32_t>(m.cap_recs);
     m.ball_done = a.take<uint32_t>(cb);
     m.slot = a.take<uint32_t>((size_t)MAX_BLOCK_WARPS * cf);
     m.pair_i = a.take<uint32_t>(m.cap_pairs); m.pair_j = a.take<uint32_t>(m.cap_pairs);
     m.lam_bb = a.take<float>(m.cap_pairs);
-    m.cs_i = a.take<uint32_t>(m.cap_pairs); m.cs_j = a.take<uint32_t>(m.cap_pairs); m.cs_l = a.take<float>(m.cap_pairs);
+    m.pr_list = a.take<uint32_t>(m.cap_pairs);
     m.pair_cnt = a.take<uint32_t>(bcells + 1);
     m.out = a.take<StepOut>(MAX_SUB);
     m.impacts = a.take<MgImpactRecord>((size_t)MAX_SUB * m.cap_impacts);
