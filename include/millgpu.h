@@ -292,9 +292,9 @@ int mg_counter_totals(MgSim* sim, uint64_t* totals10, uint64_t* n_substeps, int 
  * iterations, 11 then keeping its bookkeeping). 32-37 are not wall-clock slots: they sum over
  * balls the cycles the drag (32-34) and buoyancy (35-37) sweeps spent prefetching each ball,
  * waiting for earlier balls and running the ball's dependent part; 38 the dependency levels of
- * the active contacts (friction and restitution); 39 the projection's check that the pairs left
- * out of its first run stayed apart, when it fails (the run with all pairs that follows adds to
- * 20-22 and 16). 40 slots in all. */
+ * the active contacts (friction and restitution); 39 the projection runs whose check that the
+ * pairs left out stayed apart failed (the run that follows adds to 20-22 and 16). 40 slots in
+ * all. */
 int mg_stage_cycles(MgSim* sim, uint64_t* cycles40, int reset);
 
 /* ---- parity probes of the grid stage (grid.rs, pbf.rs:262-288) ----

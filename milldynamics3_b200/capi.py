@@ -292,7 +292,7 @@ STAGE_NAMES = [
     "drag sweep: ball prefetch (sum)", "drag sweep: ball waits (sum)", "drag sweep: ball chain work (sum)",
     "buoyancy sweep: ball prefetch (sum)", "buoyancy sweep: ball waits (sum)",
     "buoyancy sweep: ball chain work (sum)", "DEM: contact levels",
-    "DEM: projection rerun with all pairs (failed check)"]
+    "DEM: projection runs that failed their check"]
 assert len(STAGE_NAMES) == 40
 
 

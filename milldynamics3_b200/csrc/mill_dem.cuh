@@ -14,6 +14,8 @@ namespace mg {
 constexpr float RESTITUTION_VELOCITY_THRESHOLD = 0.02f;
 constexpr float MAX_RECOVERY_FRACTION = 0.2f;
 constexpr float CCD_SKIN_FRACTION = 1e-2f;
+// projection runs over a subset of the pairs before the last one runs all of them
+constexpr uint32_t PROJECTION_ROUNDS = 4;
 
 struct DemShared {
   GridHdr hg;
@@ -176,18 +178,16 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
   // each ball ever gets from its start position (the largest squared distance after any of its
   // moves). Afterwards every other pair must have stayed apart at all times: its start distance
   // less both balls' largest excursions exceeds 2r, with margins well above the f32 rounding of
-  // the excursions and of the distance test. Otherwise the positions are restored and all pairs
-  // run. Either way the sweep's result is that of the full order.
+  // the excursions and of the distance test. Otherwise the positions are restored and the sweep
+  // runs again with the pairs it could not clear added. Either way the sweep's result is that of
+  // the full order.
   const float reach = 0.25f * r;
   const float touch2 = (2.0f * r + reach) * (2.0f * r + reach);
+  uint32_t* keep = reinterpret_cast<uint32_t*>(m.act_bin);  // pairs in the run (act_bin is free until step 5)
   for (uint32_t i = tid(); i < n; i += nthr()) { m.bxs[i] = X[i]; m.bmove[i] = 0.0f; }
-  for (uint32_t k = tid(); k < np; k += nthr())
-    m.act_flag[k] = (V2(X[m.pair_i[k]]) - V2(X[m.pair_j[k]])).len2() < touch2 ? 1u : 0u;
-  if (tid() == 0) m.act_flag[np] = 0;
   __syncthreads();
-  const uint32_t ns = block_exclusive_scan(m.act_flag, np + 1);
   for (uint32_t k = tid(); k < np; k += nthr())
-    if (m.act_flag[k + 1] != m.act_flag[k]) m.pr_list[m.act_flag[k]] = k;
+    keep[k] = (V2(m.bxs[m.pair_i[k]]) - V2(m.bxs[m.pair_j[k]])).len2() < touch2 ? 1u : 0u;
   __syncthreads();
   stage_mark(out.stage, 15);
   uint32_t *lvl = m.dm_lvl, *di = m.act_i, *dj = m.act_j;
@@ -289,37 +289,43 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
     }
     return nitems;
   };
-  const uint32_t* plist = m.pr_list;
-  uint32_t npi = ns;
-  uint32_t nrun = project(ns, m.pr_list, ns < np);
-  if (ns < np) {
+  // rounds: a failed check adds the pairs it could not clear and runs again from the start
+  // positions; the last round runs every pair
+  uint32_t ns = 0, nrun = 0;
+  for (uint32_t round = 0;; ++round) {
+    const bool all = round == PROJECTION_ROUNDS - 1;
+    for (uint32_t k = tid(); k < np; k += nthr()) m.act_flag[k] = all ? 1u : keep[k];
+    if (tid() == 0) m.act_flag[np] = 0;
+    __syncthreads();
+    ns = block_exclusive_scan(m.act_flag, np + 1);
+    for (uint32_t k = tid(); k < np; k += nthr())
+      if (m.act_flag[k + 1] != m.act_flag[k]) m.pr_list[m.act_flag[k]] = k;
+    __syncthreads();
+    nrun = project(ns, m.pr_list, ns < np);
+    if (ns == np) break;
     // every pair left out stayed more than 2r apart (triangle inequality over the excursions)
     const double sep = 2.0 * (double)r * (1.0 + 1e-5);
     bool bad = false;
     for (uint32_t k = tid(); k < np; k += nthr()) {
-      if (m.act_flag[k + 1] != m.act_flag[k]) continue;
+      if (keep[k]) continue;
       const uint32_t i = m.pair_i[k], j = m.pair_j[k];
       const float2 a = m.bxs[i], b = m.bxs[j];
       const double dx = (double)a.x - (double)b.x, dy = (double)a.y - (double)b.y;
       const double ei = sqrt((double)m.bmove[i]), ej = sqrt((double)m.bmove[j]);
       const double slack = 1e-6 * (fabs((double)a.x) + fabs((double)a.y) + fabs((double)b.x) + fabs((double)b.y) + ei + ej);
-      if (!(sqrt(dx * dx + dy * dy) - (ei + ej) * (1.0 + 1e-5) - slack >= sep)) bad = true;
+      if (!(sqrt(dx * dx + dy * dy) - (ei + ej) * (1.0 + 1e-5) - slack >= sep)) { keep[k] = 1u; bad = true; }
     }
-    if (__syncthreads_or(bad)) {
-      for (uint32_t i = tid(); i < n; i += nthr()) X[i] = m.bxs[i];
-      __syncthreads();
-      stage_mark(out.stage, 39);
-      plist = nullptr;
-      npi = np;
-      nrun = project(np, nullptr, false);
-    }
+    if (!__syncthreads_or(bad)) break;
+    for (uint32_t i = tid(); i < n; i += nthr()) { X[i] = m.bxs[i]; m.bmove[i] = 0.0f; }
+    __syncthreads();
+    stage_mark(out.stage, 39);
   }
   // the accumulated multipliers back to pair / ball order (ContactBook, dem.rs:437-454); pairs
   // left out keep lambda 0
   for (uint32_t q = tid(); q < nrun; q += nthr()) {
     const uint32_t k = m.lev_items[q];
-    if (k < npi) m.lam_bb[plist ? plist[k] : k] = dl[q];
-    else m.lam_bw[k - npi] = dl[q];
+    if (k < ns) m.lam_bb[m.pr_list[k]] = dl[q];
+    else m.lam_bw[k - ns] = dl[q];
   }
   __syncthreads();
   const uint32_t nitems = np + n;
