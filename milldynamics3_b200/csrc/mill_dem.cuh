@@ -198,23 +198,20 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
     const float e = d.len2();
     return !(e <= cur) ? e : cur;
   };
-  // npi pair items (pair plist[q], or pair q when plist is null), then the n walls
+  // One run: npi pair items (pair plist[q], or pair q when plist is null) by dependency levels in
+  // warp 0, then the n walls of the iteration at once: in each iteration every wall comes after
+  // every pair, and walls of different balls are independent.
   auto project = [&](uint32_t npi, const uint32_t* plist, bool track) {
-    const uint32_t nitems = npi + n;
-    for (uint32_t k = tid(); k < nitems; k += nthr()) { m.dm_pa[k] = NONE; m.dm_pb[k] = NONE; }
-    // occurrence records: pair item q -> (i, 2q), (j, 2q+1); wall of ball b -> 2 npi + b
-    for (uint32_t q = tid(); q < 2 * npi + n; q += nthr()) {
-      if (q < 2 * npi) {
-        const uint32_t k = plist ? plist[q >> 1] : q >> 1;
-        m.rec_i[q] = (q & 1u) ? m.pair_j[k] : m.pair_i[k];
-      } else {
-        m.rec_i[q] = q - 2 * npi;
-      }
+    for (uint32_t k = tid(); k < npi; k += nthr()) { m.dm_pa[k] = NONE; m.dm_pb[k] = NONE; }
+    // occurrence records: pair item q -> (i, 2q), (j, 2q+1)
+    for (uint32_t q = tid(); q < 2 * npi; q += nthr()) {
+      const uint32_t k = plist ? plist[q >> 1] : q >> 1;
+      m.rec_i[q] = (q & 1u) ? m.pair_j[k] : m.pair_i[k];
     }
+    for (uint32_t i = tid(); i < n; i += nthr()) m.lam_bw[i] = 0.0f;
     __syncthreads();
-    preds_from_records(m.rec_i, 2 * npi + n, n, n, m.bk_start, m.bk_cur, m.bk_order, m.dm_pa, m.dm_pb,
-                       [&](uint32_t q) { return q < 2 * npi ? q >> 1 : npi + (q - 2 * npi); },
-                       [&](uint32_t q) { return q < 2 * npi ? (q & 1u) : 0u; });
+    preds_from_records(m.rec_i, 2 * npi, n, n, m.bk_start, m.bk_cur, m.bk_order, m.dm_pa, m.dm_pb,
+                       [&](uint32_t q) { return q >> 1; }, [&](uint32_t q) { return q & 1u; });
     stage_mark(out.stage, 20);
     // sweep scratch (levels, level-ordered descriptors, multipliers): shared memory after the
     // ball state when the items fit, global otherwise
@@ -222,72 +219,71 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
     if (staged) {
       const uint32_t used = (24u * n + 15u) & ~15u;
       const uint32_t fit = m.smem_bytes > used ? (m.smem_bytes - used) / 16u : 0u;
-      if (nitems <= fit) {
+      if (npi <= fit) {
         lvl = reinterpret_cast<uint32_t*>(dsm + used);
-        di = lvl + nitems;
-        dj = di + nitems;
-        dl = reinterpret_cast<float*>(dj + nitems);
+        di = lvl + npi;
+        dj = di + npi;
+        dl = reinterpret_cast<float*>(dj + npi);
       }
     }
-    const uint32_t nlev = compute_levels(nitems, m.dm_pa, m.dm_pb, lvl);
+    const uint32_t nlev = compute_levels(npi, m.dm_pa, m.dm_pb, lvl);
     stage_mark(out.stage, 21);
-    bucket_levels(nitems, lvl, nlev, m.lev_start, m.lev_cur, m.lev_items);
-    // level-ordered sweep descriptors: balls (j = NONE for a wall) and a lambda accumulator
-    for (uint32_t q = tid(); q < nitems; q += nthr()) {
+    bucket_levels(npi, lvl, nlev, m.lev_start, m.lev_cur, m.lev_items);
+    // level-ordered sweep descriptors (the two balls) and a lambda accumulator
+    for (uint32_t q = tid(); q < npi; q += nthr()) {
       const uint32_t k = m.lev_items[q];
-      const uint32_t pk = k < npi ? (plist ? plist[k] : k) : NONE;
-      di[q] = k < npi ? m.pair_i[pk] : k - npi;
-      dj[q] = k < npi ? m.pair_j[pk] : NONE;
+      const uint32_t pk = plist ? plist[k] : k;
+      di[q] = m.pair_i[pk];
+      dj[q] = m.pair_j[pk];
       dl[q] = 0.0f;
     }
     __syncthreads();
     stage_mark(out.stage, 22);
     for (uint32_t it = 0; it < iters; ++it) {
-      run_levels(nlev, m.lev_start, [&](uint32_t q) {
-        const uint32_t i = di[q], j = dj[q];
-        if (j != NONE) {
-          V2 xi(X[i]), xj(X[j]);
-          // start positions and excursions so far, loaded beside the positions
-          V2 si, sj;
-          float ei = 0.0f, ej = 0.0f;
-          if (track) { si = V2(m.bxs[i]); sj = V2(m.bxs[j]); ei = m.bmove[i]; ej = m.bmove[j]; }
-          V2 delta = xi - xj;
-          float dist = delta.len();
-          float c = dist - 2.0f * r;
-          if (c >= 0.0f) return;
-          V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
-          float w_sum = w + w;
-          if (w_sum <= 0.0f) return;
-          float c_eff = fmax_r(c, cap_depth);
-          float d_lambda = -c_eff / w_sum;
-          const V2 xin = xi + w * d_lambda * n_hat, xjn = xj - w * d_lambda * n_hat;
-          X[i] = xin.f2();
-          X[j] = xjn.f2();
-          dl[q] += d_lambda;
-          if (track) {
-            m.bmove[i] = excursion(ei, V2(xin.f2()) - si);
-            m.bmove[j] = excursion(ej, V2(xjn.f2()) - sj);
-          }
-        } else {
-          V2 x(X[i]), pl, si;
-          float ei = 0.0f;
-          if (track) { si = V2(m.bxs[i]); ei = m.bmove[i]; }
-          if (x.finite() && drum_sdf_clear(U, rotate(x, U.to_local_next), r)) return;  // c >= 0 certainly
-          float d = drum_sdf_world_dist(U, x, U.to_local_next, pl);
-          float c = d - r;
-          if (c >= 0.0f) return;
-          if (w <= 0.0f) return;
-          V2 n_hat = drum_sdf_world_normal(U, x, pl, U.to_world_next);
-          float c_eff = fmax_r(c, cap_depth);
-          float d_lambda = -c_eff / w;
-          const V2 xn = x + w * d_lambda * n_hat;
-          X[i] = xn.f2();
-          dl[q] += d_lambda;
-          if (track) m.bmove[i] = excursion(ei, V2(xn.f2()) - si);
+      run_levels(nlev, m.lev_start, [&](uint32_t q) { return make_uint2(di[q], dj[q]); },
+                 [&](uint32_t q, uint2 d) {
+        const uint32_t i = d.x, j = d.y;
+        V2 xi(X[i]), xj(X[j]);
+        // start positions and excursions so far, loaded beside the positions
+        V2 si, sj;
+        float ei = 0.0f, ej = 0.0f;
+        if (track) { si = V2(m.bxs[i]); sj = V2(m.bxs[j]); ei = m.bmove[i]; ej = m.bmove[j]; }
+        V2 delta = xi - xj;
+        float dist = delta.len();
+        float c = dist - 2.0f * r;
+        if (c >= 0.0f) return;
+        V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
+        float w_sum = w + w;
+        if (w_sum <= 0.0f) return;
+        float c_eff = fmax_r(c, cap_depth);
+        float d_lambda = -c_eff / w_sum;
+        const V2 xin = xi + w * d_lambda * n_hat, xjn = xj - w * d_lambda * n_hat;
+        X[i] = xin.f2();
+        X[j] = xjn.f2();
+        dl[q] += d_lambda;
+        if (track) {
+          m.bmove[i] = excursion(ei, V2(xin.f2()) - si);
+          m.bmove[j] = excursion(ej, V2(xjn.f2()) - sj);
         }
       });
+      for (uint32_t i = tid(); i < n; i += nthr()) {
+        V2 x(X[i]), pl;
+        if (x.finite() && drum_sdf_clear(U, rotate(x, U.to_local_next), r)) continue;  // c >= 0 certainly
+        float d = drum_sdf_world_dist(U, x, U.to_local_next, pl);
+        float c = d - r;
+        if (c >= 0.0f) continue;
+        if (w <= 0.0f) continue;
+        V2 n_hat = drum_sdf_world_normal(U, x, pl, U.to_world_next);
+        float c_eff = fmax_r(c, cap_depth);
+        float d_lambda = -c_eff / w;
+        const V2 xn = x + w * d_lambda * n_hat;
+        X[i] = xn.f2();
+        m.lam_bw[i] += d_lambda;
+        if (track) m.bmove[i] = excursion(m.bmove[i], V2(xn.f2()) - V2(m.bxs[i]));
+      }
+      __syncthreads();
     }
-    return nitems;
+    return npi;
   };
   // rounds: a failed check adds the pairs it could not clear and runs again from the start
   // positions; the last round runs every pair
@@ -320,13 +316,9 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
     __syncthreads();
     stage_mark(out.stage, 39);
   }
-  // the accumulated multipliers back to pair / ball order (ContactBook, dem.rs:437-454); pairs
-  // left out keep lambda 0
-  for (uint32_t q = tid(); q < nrun; q += nthr()) {
-    const uint32_t k = m.lev_items[q];
-    if (k < ns) m.lam_bb[m.pr_list[k]] = dl[q];
-    else m.lam_bw[k - ns] = dl[q];
-  }
+  // the accumulated pair multipliers back to pair order (ContactBook, dem.rs:437-454; pairs left
+  // out keep lambda 0, walls accumulated in lam_bw in place)
+  for (uint32_t q = tid(); q < nrun; q += nthr()) m.lam_bb[m.pr_list[m.lev_items[q]]] = dl[q];
   __syncthreads();
   const uint32_t nitems = np + n;
   stage_mark(out.stage, 16);
@@ -357,6 +349,7 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
   if (tid() == 0) m.act_flag[nitems] = 0;
   __syncthreads();
   const uint32_t na = block_exclusive_scan(m.act_flag, nitems + 1);
+  const uint32_t na_p = m.act_flag[np];  // active pair contacts; the active walls follow them
   for (uint32_t q = tid(); q < nitems; q += nthr()) {
     uint32_t o = m.act_flag[q];
     if (m.act_flag[q + 1] == o) continue;
@@ -385,16 +378,21 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
   // step 5 friction (dem.rs:782-882)
   const MgMediaParams& md = U.media;
   auto load_contact = [&](uint32_t k) { return make_uint3(m.act_i[k], m.act_j[k], __float_as_uint(m.act_l[k])); };
-  // dependency levels of the active contacts, shared by the friction and restitution sweeps:
-  // contacts of one level share no ball, so each level runs in parallel
-  const uint32_t nlev_c = compute_levels(na, m.dm_pa, m.dm_pb, m.dm_lvl);
-  bucket_levels(na, m.dm_lvl, nlev_c, m.lev_start, m.lev_cur, m.lev_items);
+  // dependency levels of the active pair contacts, shared by the friction and restitution
+  // sweeps: contacts of one level share no ball, so each level runs in parallel. Every wall
+  // contact comes after every pair contact and touches one ball, so the walls then run at once.
+  const uint32_t nlev_c = compute_levels(na_p, m.dm_pa, m.dm_pb, m.dm_lvl);
+  bucket_levels(na_p, m.dm_lvl, nlev_c, m.lev_start, m.lev_cur, m.lev_items);
   stage_mark(out.stage, 38);
   auto contact_sweep = [&](auto body) {
-    run_levels(nlev_c, m.lev_start, [&](uint32_t q) {
-      const uint32_t k = m.lev_items[q];
-      body(k, load_contact(k));
-    });
+    run_levels(nlev_c, m.lev_start,
+               [&](uint32_t q) {
+                 const uint32_t k = m.lev_items[q];
+                 return make_uint4(k, m.act_i[k], m.act_j[k], __float_as_uint(m.act_l[k]));
+               },
+               [&](uint32_t, uint4 d) { body(d.x, make_uint3(d.y, d.z, d.w)); });
+    for (uint32_t k = na_p + tid(); k < na; k += nthr()) body(k, load_contact(k));
+    __syncthreads();
   };
   contact_sweep([&](uint32_t k, uint3 d) {
     const uint32_t i = d.x, j = d.y;

@@ -37,11 +37,25 @@ __device__ __forceinline__ float drum_sdf(const StepUniform& U, V2 p) {
   float r_top = r - U.lifter_height;
   V2 verts[4] = {V2(r, -U.lifter_base_half), V2(r, U.lifter_base_half), V2(r_top, U.lifter_top_half),
                  V2(r_top, -U.lifter_top_half)};
+  // A lifter whose distance certainly exceeds the circle term d cannot change fmin(d, -max_inside)
+  // (fmin and fmax only select), so it is skipped. A proper CCW quad (0 < h < R, b, t > 0) lies in
+  // the disk of centre (R - h/2, 0) and radius rho = sqrt(h^2/4 + max(b, t)^2) of its frame, and
+  // its convex_quad_sdf is then minus the distance for points outside it; the lifter is skipped
+  // when the point is farther than d + rho from the centre, with margins (1e-4 R in the reach,
+  // 2e-6 R and a relative 1e-5 in the comparison) far above the f32 rounding of either side.
+  const bool cull = U.lifter_height > 0.0f && U.lifter_height < r && U.lifter_base_half > 0.0f &&
+                    U.lifter_top_half > 0.0f;
+  const float cx = r - 0.5f * U.lifter_height;
+  const float wmax = fmaxf(U.lifter_base_half, U.lifter_top_half);
+  const float rho = sqrtf(0.25f * U.lifter_height * U.lifter_height + wmax * wmax);
+  const float reach = d + rho * 1.00001f + 1e-4f * r;
+  const float far2 = (reach + 2e-6f * r) * (reach + 2e-6f * r) * 1.00001f;
   float max_inside = -INFINITY;
   for (uint32_t k = 0; k < U.lifter_count; ++k) {
     float s = U.lifter_sin[k], c = U.lifter_cos[k];
     float pr = p.x * c + p.y * s;
     float pt = -p.x * s + p.y * c;
+    if (cull && reach > 0.0f && (pr - cx) * (pr - cx) + pt * pt > far2) continue;
     max_inside = fmax_r(max_inside, convex_quad_sdf(V2(pr, pt), verts));
   }
   return fmin_r(d, -max_inside);

@@ -97,54 +97,28 @@ __device__ void bucket_levels(uint32_t n, const uint32_t* lvl, uint32_t nlev, ui
   __syncthreads();
 }
 
-// Runs exec(q) for every level-ordered position q, level by level, in warp 0; the block waits at
-// the end. Positions [lev_start[l], lev_start[l+1]) form level l.
-template <class Exec>
-__device__ void run_levels(uint32_t nlev, const uint32_t* lev_start, Exec exec) {
-  if (threadIdx.x < 32) {
-    const uint32_t lane = threadIdx.x;
-    uint32_t s = lev_start[0];
-    // the level ends are loaded 32 at a time (one per lane) and handed out by shuffles, so no
-    // memory round trip sits between two levels
-    for (uint32_t b = 0; b < nlev; b += 32) {
-      const uint32_t ends = b + lane < nlev ? lev_start[b + lane + 1] : 0u;
-      const uint32_t cnt = min(32u, nlev - b);
-      for (uint32_t t = 0; t < cnt; ++t) {
-        const uint32_t e = __shfl_sync(FULL, ends, t);
-        for (uint32_t q = s + lane; q < e; q += 32) exec(q);
-        s = e;
-        __syncwarp();
-      }
-    }
-  }
-  __syncthreads();
-}
-
-// Chunked in-order replay in warp 0: in each chunk of 32 items, rounds run the items whose
-// in-chunk predecessors are done (earlier chunks are complete). At most 32 rounds per chunk.
-// load(k) fetches item k's descriptor once per chunk (all lanes together); exec(k, desc) runs it.
+// Runs exec(q, load(q)) for every level-ordered position q, level by level, in warp 0; the block
+// waits at the end. Positions [lev_start[l], lev_start[l+1]) form level l. load(q) must read only
+// what the levels do not write (the item's descriptor).
 template <class Load, class Exec>
-__device__ void run_chunked(uint32_t n, const uint32_t* pred_a, const uint32_t* pred_b, Load load, Exec exec) {
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    for (uint32_t c = 0; c < n; c += 32) {
-      uint32_t k = c + lane;
-      bool active = k < n;
-      int la = -1, lb = -1;
-      decltype(load(0u)) desc{};
-      if (active) {
-        uint32_t a = pred_a[k], b = pred_b[k];
-        if (a != NONE && a >= c) la = (int)(a - c);
-        if (b != NONE && b >= c) lb = (int)(b - c);
-        desc = load(k);
-      }
-      uint32_t done = __ballot_sync(FULL, !active);
-      for (int round = 0; round < 33 && done != FULL; ++round) {
-        bool ready = active && !((done >> lane) & 1u) && (la < 0 || ((done >> la) & 1u)) && (lb < 0 || ((done >> lb) & 1u));
-        if (ready) exec(k, desc);
-        __syncwarp();
-        done |= __ballot_sync(FULL, ready);
-      }
+__device__ void run_levels(uint32_t nlev, const uint32_t* lev_start, Load load, Exec exec) {
+  if (threadIdx.x < 32 && nlev > 0) {
+    const uint32_t lane = threadIdx.x;
+    // level t is [s, e); its first descriptor per lane and the next level's end are fetched one
+    // level ahead, so only the item's own dependent loads sit between two levels
+    uint32_t e = lev_start[1];
+    uint32_t q = lev_start[0] + lane;
+    auto d = q < e ? load(q) : decltype(load(0u)){};
+    for (uint32_t t = 0; t < nlev; ++t) {
+      const uint32_t e_next = t + 1 < nlev ? lev_start[t + 2] : e;
+      const uint32_t qn = e + lane;
+      const auto dn = qn < e_next ? load(qn) : decltype(load(0u)){};
+      if (q < e) exec(q, d);
+      for (uint32_t q2 = q + 32; q2 < e; q2 += 32) exec(q2, load(q2));  // levels wider than a warp
+      __syncwarp();
+      e = e_next;
+      q = qn;
+      d = dn;
     }
   }
   __syncthreads();
