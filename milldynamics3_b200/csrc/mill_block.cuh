@@ -188,7 +188,7 @@ __device__ __forceinline__ void small_sort_u32(uint32_t* a, uint32_t n) {
 }
 
 // Stable bucket sort: start[0..nbk] receives bucket offsets, order[] the record indices grouped by
-// key in ascending record order; cur[0..nbk) is scratch. Buckets are expected to be short.
+// key in ascending record order; cur[0..nbk) is scratch.
 __device__ inline void block_bucket_sort(const uint32_t* keys, uint32_t nrec, uint32_t nbk, uint32_t* start, uint32_t* cur,
                                   uint32_t* order) {
   for (uint32_t k = tid(); k <= nbk; k += nthr()) start[k] = 0;
@@ -196,14 +196,45 @@ __device__ inline void block_bucket_sort(const uint32_t* keys, uint32_t nrec, ui
   for (uint32_t r = tid(); r < nrec; r += nthr()) atomicAdd(&start[keys[r]], 1u);
   __syncthreads();
   block_exclusive_scan(start, nbk + 1);
-  for (uint32_t k = tid(); k < nbk; k += nthr()) cur[k] = start[k];
+  // buckets of more than 32 records (up to 64 of them) are filled in record order by one warp
+  // each; the others are scattered by atomics, then sorted by one thread
+  constexpr uint32_t SMALL = 32, NBIG = 64, BIG = 0xFFFFFFFFu;
+  __shared__ uint32_t big[NBIG];
+  __shared__ uint32_t nbig;
+  if (tid() == 0) nbig = 0;
   __syncthreads();
-  for (uint32_t r = tid(); r < nrec; r += nthr()) {
-    uint32_t slot = atomicAdd(&cur[keys[r]], 1u);
-    order[slot] = r;
+  for (uint32_t k = tid(); k < nbk; k += nthr()) {
+    uint32_t c = start[k];
+    if (start[k + 1] - c > SMALL) {
+      const uint32_t q = atomicAdd(&nbig, 1u);
+      if (q < NBIG) { big[q] = k; c = BIG; }
+    }
+    cur[k] = c;
   }
   __syncthreads();
-  for (uint32_t k = tid(); k < nbk; k += nthr()) small_sort_u32(order + start[k], start[k + 1] - start[k]);
+  for (uint32_t r = tid(); r < nrec; r += nthr()) {
+    const uint32_t k = keys[r];
+    if (cur[k] == BIG) continue;
+    uint32_t slot = atomicAdd(&cur[k], 1u);
+    order[slot] = r;
+  }
+  {
+    const uint32_t lane = tid() & 31u, nl = min(nbig, NBIG);
+    for (uint32_t q = tid() >> 5; q < nl; q += nthr() >> 5) {
+      const uint32_t k = big[q];
+      uint32_t o = start[k];
+      for (uint32_t c0 = 0; c0 < nrec; c0 += 32) {
+        const uint32_t r = c0 + lane;
+        const bool hit = r < nrec && keys[r] == k;
+        const uint32_t bal = __ballot_sync(0xffffffffu, hit);
+        if (hit) order[o + __popc(bal & ((1u << lane) - 1u))] = r;
+        o += __popc(bal);
+      }
+    }
+  }
+  __syncthreads();
+  for (uint32_t k = tid(); k < nbk; k += nthr())
+    if (cur[k] != BIG) small_sort_u32(order + start[k], start[k + 1] - start[k]);
   __syncthreads();
 }
 

@@ -504,9 +504,9 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       if (*err) return;
       // per-fluid sums of the balls' contributions in ball order (stable bucket sort by fluid)
       uint32_t nrec = pack_ball_items(m.item_j, m.item_n, m.cap_items, nb, m.rec_off, m.rec_i, m.rec_b);
-      for (uint32_t b = tid(); b < nb; b += nthr()) {
-        uint32_t o = m.rec_off[b], base = b * m.cap_items;
-        for (uint32_t s = 0; s < m.item_n[b]; ++s) m.rec_J[o + s] = m.item_v[base + s];
+      for (uint32_t b = tid() >> 5; b < nb; b += nthr() >> 5) {
+        const uint32_t o = m.rec_off[b], base = b * m.cap_items, cnt = m.item_n[b];
+        for (uint32_t s = tid() & 31u; s < cnt; s += 32) m.rec_J[o + s] = m.item_v[base + s];
       }
       __syncthreads();
       block_bucket_sort(m.rec_i, nrec, n, m.bk_start, m.bk_cur, m.bk_order);
@@ -1228,9 +1228,9 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       if (*err) return;
       uint32_t ng = block_exclusive_scan(m.g_off, nb + 1);
       if (ng > m.cap_groups) { if (tid() == 0) atomicOr(err, ERR_GROUPS); __syncthreads(); return; }
-      for (uint32_t b = tid(); b < nb; b += nthr()) {
-        uint32_t base = b * m.cap_items, o = m.g_off[b], cnt = m.g_off[b + 1] - o;
-        for (uint32_t s = 0; s < cnt; ++s) {
+      for (uint32_t b = tid() >> 5; b < nb; b += nthr() >> 5) {
+        const uint32_t base = b * m.cap_items, o = m.g_off[b], cnt = m.g_off[b + 1] - o;
+        for (uint32_t s = tid() & 31u; s < cnt; s += 32) {
           m.g_fluid[o + s] = m.item_j[base + s];
           m.g_ball[o + s] = b;
           m.g_c[o + s] = m.item_w[base + s];

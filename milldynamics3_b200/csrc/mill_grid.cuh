@@ -8,6 +8,12 @@
 
 namespace mg {
 
+// Cells with more points than this are filled in index order by a warp instead of sorted (up to
+// BIG_LIST such cells per build; further ones are sorted like the rest).
+constexpr uint32_t GRID_SMALL_CELL = 32;
+constexpr uint32_t BIG_LIST = 64;
+constexpr uint32_t BIG_CELL = 0xFFFFFFFFu;  // cursor mark of a cell filled by a warp
+
 __device__ __forceinline__ int2 cell_key(V2 p, float cell) {
   return make_int2(f2i_sat(floorf(p.x / cell)), f2i_sat(floorf(p.y / cell)));
 }
@@ -71,18 +77,50 @@ __device__ inline void grid_build(const float2* pts, uint32_t n, float cell, con
     }
     __syncthreads();
     block_exclusive_scan(gb.cell_start, total + 1);
-    for (uint32_t k = tid(); k < total; k += nthr()) gb.cursor[k] = gb.cell_start[k];
+    // cells of more than GRID_SMALL_CELL points (up to BIG_LIST of them) are filled in index order
+    // by one warp each; the others are scattered by atomics, then sorted by one thread
+    __shared__ uint32_t big[BIG_LIST];
+    __shared__ uint32_t nbig;
+    if (tid() == 0) nbig = 0;
+    __syncthreads();
+    for (uint32_t k = tid(); k < total; k += nthr()) {
+      uint32_t cur = gb.cell_start[k];
+      if (gb.cell_start[k + 1] - cur > GRID_SMALL_CELL) {
+        const uint32_t q = atomicAdd(&nbig, 1u);
+        if (q < BIG_LIST) { big[q] = k; cur = BIG_CELL; }
+      }
+      gb.cursor[k] = cur;
+    }
     __syncthreads();
     for (uint32_t i = tid(); i < n; i += nthr()) {
       if (!V2(pts[i]).finite()) continue;
       int2 k = gb.pkey[i];
       uint32_t c = (uint32_t)((k.x - hdr.min_cx) * hdr.height + (k.y - hdr.min_cy));
+      if (gb.cursor[c] == BIG_CELL) continue;
       uint32_t slot = atomicAdd(&gb.cursor[c], 1u);
       gb.indices[slot] = i;
     }
+    {
+      const uint32_t lane = tid() & 31u, nl = min(nbig, BIG_LIST);
+      for (uint32_t q = tid() >> 5; q < nl; q += nthr() >> 5) {
+        const uint32_t c = big[q];
+        uint32_t o = gb.cell_start[c];
+        for (uint32_t c0 = 0; c0 < n; c0 += 32) {
+          const uint32_t i = c0 + lane;
+          bool hit = false;
+          if (i < n && V2(pts[i]).finite()) {
+            const int2 k = gb.pkey[i];
+            hit = (uint32_t)((k.x - hdr.min_cx) * hdr.height + (k.y - hdr.min_cy)) == c;
+          }
+          const uint32_t bal = __ballot_sync(0xffffffffu, hit);
+          if (hit) gb.indices[o + __popc(bal & ((1u << lane) - 1u))] = i;
+          o += __popc(bal);
+        }
+      }
+    }
     __syncthreads();
     for (uint32_t k = tid(); k < total; k += nthr())
-      small_sort_u32(gb.indices + gb.cell_start[k], gb.cell_start[k + 1] - gb.cell_start[k]);
+      if (gb.cursor[k] != BIG_CELL) small_sort_u32(gb.indices + gb.cell_start[k], gb.cell_start[k + 1] - gb.cell_start[k]);
     __syncthreads();
   } else {
     // Sparse: rank every valid point by (key, index); O(n^2 / threads), used only for a

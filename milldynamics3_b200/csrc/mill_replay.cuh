@@ -140,9 +140,9 @@ __device__ uint32_t pack_ball_items(const uint32_t* item_j, const uint32_t* cnt,
   if (tid() == 0) rec_off[nb] = 0;
   __syncthreads();
   uint32_t total = block_exclusive_scan(rec_off, nb + 1);
-  for (uint32_t b = tid(); b < nb; b += nthr()) {
-    uint32_t o = rec_off[b], c = cnt[b];
-    for (uint32_t s = 0; s < c; ++s) { rec_key[o + s] = item_j[(size_t)b * cap + s]; rec_ball[o + s] = b; }
+  for (uint32_t b = tid() >> 5; b < nb; b += nthr() >> 5) {
+    const uint32_t o = rec_off[b], c = cnt[b];
+    for (uint32_t s = tid() & 31u; s < c; s += 32) { rec_key[o + s] = item_j[(size_t)b * cap + s]; rec_ball[o + s] = b; }
   }
   __syncthreads();
   return total;
