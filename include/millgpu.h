@@ -180,13 +180,18 @@ typedef struct MgScalars {
  * block, a multiple of 32 up to 1024 (0 = 1024).
  * sweep_warps: warps that take balls in the per-ball drag and buoyancy sweeps (0 = default).
  * spin_ns: poll interval of a ball waiting for an earlier ball in those sweeps (0 = default).
+ * mill_blocks: thread blocks that share a single mill's per-ball stages (adhesion, boundary
+ * groups, squeeze links) in the handle's own launches: 0 = default (8), 1 = the mill's block
+ * alone, at most 16 for handles from mg_sim_create / mg_sim_create_with_balls; the mills of a
+ * batch or a server always run one block each (0 or 1 only).
  * None of them changes results. */
 typedef struct MgOptions {
   uint32_t cg_fp64;
   uint32_t block_threads;
   uint32_t sweep_warps;
   uint32_t spin_ns;
-  uint32_t reserved[4];
+  uint32_t mill_blocks;
+  uint32_t reserved[3];
 } MgOptions;
 
 typedef struct MgSim MgSim;

@@ -147,7 +147,7 @@ class Scalars(_S):
 
 class Options(_S):
     _fields_ = [("cg_fp64", C.c_uint32), ("block_threads", C.c_uint32), ("sweep_warps", C.c_uint32),
-                ("spin_ns", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+                ("spin_ns", C.c_uint32), ("mill_blocks", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 class ServerConfig(_S):

@@ -26,6 +26,10 @@ constexpr uint32_t MAX_BLOCK_WARPS = MAX_BLOCK_THREADS / 32;
 // Threads per mill block when the options leave it open (measured fastest on B200, single mill
 // and batches alike).
 constexpr uint32_t DEFAULT_BLOCK_THREADS = 1024;
+// Thread blocks that run one mill's per-ball stages in a single-mill launch: the mill's own block
+// plus helper blocks (at most MAX_MILL_BLOCKS; DEFAULT_MILL_BLOCKS unless the caller sets it).
+constexpr uint32_t MAX_MILL_BLOCKS = 16;
+constexpr uint32_t DEFAULT_MILL_BLOCKS = 8;
 constexpr uint32_t DEFAULT_SPIN_NS = 64;
 constexpr int MAX_BOUNDARY_POINTS = 1024;
 
@@ -194,6 +198,7 @@ enum : uint32_t {
   ERR_LINKS = 1u << 6,
   ERR_IMPACTS = 1u << 7,
   ERR_BUDGET = 1u << 8,
+  ERR_WIDE = 1u << 9,  // a mill's helper blocks and its own block stopped waiting for each other
 };
 
 // ---------------------------------------------------------------- a spatial grid's buffers
@@ -214,6 +219,16 @@ struct GridHdr {
   int32_t width, height;
   uint32_t ncells;   // dense: width*height; sparse: unique keys
   uint32_t npoints;  // valid (finite) points
+};
+
+// Control block of a single-mill launch with helper blocks (mill_wide.cuh): the mill's block
+// publishes phases, the helper blocks count the phases they finished. Zeroed before each launch.
+struct WideCtl {
+  uint32_t seq;      // phases published so far
+  uint32_t phase;    // the last published phase
+  uint32_t done;     // helper-block phases finished, over the launch
+  uint32_t counter;  // a phase's count summed over the helper blocks
+  GridHdr hdr;       // the grid the phase searches
 };
 
 // ---------------------------------------------------------------- per-mill descriptor
@@ -276,7 +291,7 @@ struct MillDev {
   float* bmove;   // per ball largest squared distance from bxs during the projection sweep
   double* f_cw;  // per-ball coupling work of the predict step
   uint32_t *rec_off, *rec_pred, *ball_done;  // per-ball sweep records (cap_nb + 1, cap_recs, cap_nb)
-  uint32_t* slot;  // per-warp fluid -> item maps of the in-order merges (MAX_BLOCK_WARPS x cap_nf, all NONE at rest)
+  uint32_t* slot;  // per-warp fluid -> item maps of the in-order merges (warps of all the mill's blocks x cap_nf, all NONE at rest)
   uint32_t *pair_i, *pair_j;
   float* lam_bb;
   uint32_t* pr_list;  // pairs within reach of touching at the start of the projection
@@ -289,6 +304,8 @@ struct MillDev {
   MgImpactRecord* act_rec;
   uint32_t smem_balls;  // balls whose state fits the launch's dynamic shared memory (0: global)
   uint32_t smem_bytes;  // the launch's dynamic shared memory (staged ball state, then sweep scratch)
+  uint32_t helpers;     // helper blocks of this launch (set by the kernel; 0 in batches)
+  WideCtl* wide;        // their control block
   // outputs
   StepOut* out;             // one per sub-step of the launch
   MgImpactRecord* impacts;  // cap_impacts per sub-step of the launch

@@ -8,6 +8,7 @@
 #include "mill_geom.cuh"
 #include "mill_grid.cuh"
 #include "mill_replay.cuh"
+#include "mill_wide.cuh"
 
 namespace mg {
 
@@ -224,6 +225,236 @@ __device__ void joint_apply(const MillDev& m, float dt, const float2* xx, float2
   __syncthreads();
 }
 
+// ---------------------------------------------------------------- per-ball loops of the stages
+// Each runs for the balls w0, w0 + nw, ... (w0: the calling warp's index over all of the mill's
+// blocks, nw: their warp count), one warp per ball with no state shared between balls, so the
+// mill's block and its helper blocks (mill_wide.cuh) can split them.
+
+// Step 3.6b adhesion per ball (pbf.rs:1540-1602): candidates of each boundary point in
+// for_each_near order, 32 at a time, merged per fluid particle in first-seen order; the ball's
+// impulse and its items' velocity changes (item_v) and count (item_n).
+__device__ void adhesion_balls(const MillDev& m, const StepUniform& U, const GridHdr& hA, uint32_t w0, uint32_t nw) {
+  const uint32_t nb = m.nb, count_pb = U.boundary_count;
+  const float h = m.f_h, rho0 = m.f_rho0, mass = m.f_mass, dt = U.dt;
+  const float2* X = m.fx;
+  uint32_t* err = m.err;
+  const float wett = clamp_r(U.slurry.wettability, 0.0f, 1.0f);
+  const float h_adh = fmin_r(h, 2.0f * m.b_r);
+  const float adhesion_accel = wett * 2.0f * fabsf(GRAVITY);
+  const float range2 = h_adh * h_adh * (1.0f + 1e-4f);
+  const float inner2 = 0.25f * h_adh * h_adh * (1.0f - 1e-4f);
+  const uint32_t lane = tid() & 31u;
+  uint32_t* slot = m.slot + (size_t)w0 * m.cap_nf;
+  for (uint32_t b = w0; b < nb; b += nw) {
+    const uint32_t base = b * m.cap_items;
+    const MergeList L{m.item_j + base, m.item_w + base, m.item_v + base, nullptr, m.cap_items};
+    uint32_t cnt = 0;
+    bool overflow = false;
+    const V2 xb(m.bx[b]);
+    if (xb.finite()) {
+      warp_near_multi(
+          hA, m.gA, count_pb, [&](uint32_t q) { return xb + U.boundary_offset[q]; },
+          [&](uint32_t j, bool valid) { return valid ? V2(X[j]) : V2(); },
+          [&](uint32_t j, uint32_t q, V2 xj, bool valid) {
+            bool acc = false;
+            float w = 0.0f;
+            V2 dir;
+            if (valid) {
+              const V2 bp = xb + U.boundary_offset[q];
+              V2 delta = bp - xj;
+              float r2 = delta.len2();
+              if (!(r2 >= range2 || r2 <= inner2)) {
+                float r = sqrtf(r2);
+                if (!(!finite_f(r) || r <= 0.5f * h_adh || r >= h_adh)) {
+                  w = mass * adhesion_kernel(r, h_adh) / rho0;
+                  if (w > 0.0f) { acc = true; dir = w * (delta / r); }
+                }
+              }
+            }
+            warp_merge(acc, j, w, dir, 0.0f, slot, L, cnt, overflow);
+          });
+    }
+    for (uint32_t s = lane; s < min(cnt, m.cap_items); s += 32) slot[L.j[s]] = NONE;
+    __syncwarp();
+    if (__any_sync(FULL, overflow)) { if (lane == 0) atomicOr(err, ERR_ITEMS); cnt = 0; }
+    uint32_t used = 0;
+    if (cnt > 0) {
+      // dir_sum and weight_sum in item order (pbf.rs:1586-1594)
+      float weight_sum = 0.0f, dsx = 0.0f, dsy = 0.0f;
+      for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+        const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
+        float ww = 0.0f;
+        V2 dd;
+        if (s < cnt) { ww = L.v0[s]; dd = V2(L.v1[s]); }
+#pragma unroll
+        for (uint32_t t = 0; t < 32; ++t) {
+          const float xt = __shfl_sync(FULL, dd.x, t), yt = __shfl_sync(FULL, dd.y, t);
+          const float wt = __shfl_sync(FULL, ww, t);
+          if (t < lim) {
+            dsx += xt;
+            dsy += yt;
+            weight_sum += wt;
+          }
+        }
+      }
+      V2 dir_sum(dsx, dsy);
+      float pull_len = dir_sum.len();
+      if (weight_sum > 1e-9f && pull_len > 1e-9f) {
+        V2 ball_pull_dir = -dir_sum / pull_len;
+        float coverage = fmin_r(weight_sum, 1.0f);
+        float m_contrib = mass * weight_sum;
+        float attach = m_contrib / (m.b_m + m_contrib);
+        V2 dv_b = ball_pull_dir * (adhesion_accel * coverage * dt * attach);
+        if (lane == 0) {
+          m.imp[b] = (V2(m.imp[b]) + m.b_m * dv_b).f2();
+          V2 lever = ball_pull_dir * m.b_r;
+          m.ang[b] += m.b_m * cross2(lever, dv_b);
+        }
+        for (uint32_t s = lane; s < cnt; s += 32) {
+          float frac = L.v0[s] / weight_sum;
+          V2 dv_i = -(m.b_m * frac / mass) * dv_b;
+          L.v1[s] = dv_i.f2();
+        }
+        used = cnt;
+      }
+    }
+    if (lane == 0) m.item_n[b] = used;
+    __syncwarp();
+  }
+}
+
+// Boundary groups per ball (pbf.rs:2159-2232) on the fresh h-grid: candidates of each boundary
+// point merged per fluid particle in first-seen order; the ball's group count in g_off[b].
+__device__ void group_balls(const MillDev& m, const StepUniform& U, const GridHdr& hB, uint32_t w0, uint32_t nw) {
+  const uint32_t nb = m.nb, count_pb = U.boundary_count;
+  const float h = m.f_h;
+  const float2* X = m.fx;
+  uint32_t* err = m.err;
+  const float eta2 = VISC_ETA * h * h;
+  const float spiky_norm = -30.0f / (PI_F * powi5(h));
+  const float range2 = h * h * (1.0f + 1e-4f);
+  uint32_t* slot = m.slot + (size_t)w0 * m.cap_nf;
+  for (uint32_t b = w0; b < nb; b += nw) {
+    const uint32_t lane = tid() & 31u, base = b * m.cap_items;
+    const MergeList L{m.item_j + base, m.item_w + base, m.item_v + base, m.item_w2 + base, m.cap_items};
+    uint32_t cnt = 0;
+    bool overflow = false;
+    const V2 xb(m.bx[b]);
+    if (xb.finite()) {
+      struct XF {
+        V2 x;
+        float f;
+      };
+      warp_near_multi(
+          hB, m.gB, count_pb, [&](uint32_t q) { return xb + U.boundary_offset[q]; },
+          [&](uint32_t j, bool valid) {
+            XF d{V2(), 0.0f};
+            if (valid) {
+              d.x = V2(X[j]);
+              d.f = m.f_tmp[j];
+            }
+            return d;
+          },
+          [&](uint32_t j, uint32_t q, XF d, bool valid) {
+            bool acc = false;
+            float c = 0.0f, lever2_c = 0.0f;
+            V2 lever_c;
+            if (valid) {
+              const V2 bp = xb + U.boundary_offset[q];
+              V2 delta = d.x - bp;
+              float r2 = delta.len2();
+              if (!(r2 >= range2)) {
+                float r = sqrtf(r2);
+                if (!(!finite_f(r) || r >= h || r <= 1e-9f)) {
+                  float dot_abs = fabsf(spiky_norm * (h - r) * (h - r) * r);
+                  c = d.f * dot_abs / (r2 + eta2);
+                  if (c > 0.0f) {
+                    acc = true;
+                    V2 lever = bp - xb;
+                    lever_c = c * lever;
+                    lever2_c = c * lever.len2();
+                  }
+                }
+              }
+            }
+            warp_merge(acc, j, c, lever_c, lever2_c, slot, L, cnt, overflow);
+          });
+    }
+    for (uint32_t s = lane; s < min(cnt, m.cap_items); s += 32) slot[L.j[s]] = NONE;
+    __syncwarp();
+    if (__any_sync(FULL, overflow)) { if (lane == 0) atomicOr(err, ERR_ITEMS); cnt = 0; }
+    if (lane == 0) m.g_off[b] = cnt;
+    __syncwarp();
+  }
+}
+
+// Squeeze links per ball (pbf.rs:544-625): candidates j > i in for_each_near order, ordered
+// compaction, then the wall link, each film evaluated once; ball i's links go to its slots
+// [i K, i K + K) of the record scratch and its count to l_off[i]. Returns the thread's part of
+// the count of links in range.
+__device__ uint32_t link_balls(const MillDev& m, const StepUniform& U, const GridHdr& hBall, uint32_t w0, uint32_t nw) {
+  const uint32_t nb = m.nb;
+  const float h = m.f_h, dt = U.dt;
+  uint32_t* err = m.err;
+  const float r = m.b_r;
+  const double dxd = (double)(0.5f * h);
+  const float reach = (float)(8.0 * dxd);
+  const float c_max = 8.0f * m.b_m / fmax_r(dt, 1e-12f);
+  const float range2 = (2.0f * r + reach) * (2.0f * r + reach) * (1.0f + 1e-4f);
+  const uint32_t K = min(nb + 1u, 512u);
+  uint32_t in_range = 0;
+  for (uint32_t i = w0; i < nb; i += nw) {
+    const uint32_t lane = tid() & 31u;
+    const V2 xi(m.bx[i]), v0i(m.ball_v0[i]);
+    const uint32_t base = i * K;
+    uint32_t c = 0, inr = 0;
+    if (xi.finite()) {
+      struct XV {
+        V2 x, v0;
+      };
+      warp_near_multi(
+          hBall, m.gBall, 1u, [&](uint32_t) { return xi; },
+          [&](uint32_t j, bool valid) {
+            XV d{V2(), V2()};
+            if (valid && j > i) {
+              d.x = V2(m.bx[j]);
+              d.v0 = V2(m.ball_v0[j]);
+            }
+            return d;
+          },
+          [&](uint32_t j, uint32_t, XV d, bool valid) {
+            const bool cand = valid && j > i;
+            LinkEval L{false, false, V2(), 0.0f};
+            if (cand) L = link_pair(m, U, xi, v0i, d.x, d.v0, reach, range2, dxd, c_max, true);
+            inr += __popc(__ballot_sync(FULL, cand && L.in_range));
+            const uint32_t bal = __ballot_sync(FULL, cand && L.emit);
+            const uint32_t q = c + __popc(bal & ((1u << lane) - 1u));
+            if (cand && L.emit && q < K) {
+              m.rec_i[base + q] = j;
+              m.rec_J[base + q] = L.n.f2();
+              m.rec_L[base + q] = L.c;
+            }
+            c += __popc(bal);
+          });
+      if (lane == 0) {
+        LinkEval W = link_wall(m, U, i, reach, dxd, c_max);
+        if (W.in_range) inr += 1;
+        if (W.emit) {
+          if (c < K) { m.rec_i[base + c] = NONE; m.rec_J[base + c] = W.n.f2(); m.rec_L[base + c] = W.c; }
+          ++c;
+        }
+      }
+    }
+    if (lane == 0) {
+      if (c > K) { atomicOr(err, ERR_LINKS); c = K; }
+      m.l_off[i] = c;
+      in_range += inr;
+    }
+    __syncwarp();
+  }
+  return in_range;
+}
+
 __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err, FluidShared& S,
                            unsigned char* dsm) {
   uint32_t* done = m.ball_done;  // completion flags of the per-ball sweeps (moved to shared below)
@@ -417,89 +648,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
   if (wett > 0.0f && nb > 0 && m.b_r > 0.0f && count_pb > 0) {
     const float h_adh = fmin_r(h, 2.0f * m.b_r);
     if (h_adh > 0.0f) {
-      const float adhesion_accel = wett * 2.0f * fabsf(GRAVITY);
-      const float range2 = h_adh * h_adh * (1.0f + 1e-4f);
-      const float inner2 = 0.25f * h_adh * h_adh * (1.0f - 1e-4f);
-      // one warp per ball: candidates of each boundary point in for_each_near order, 32 at a time,
-      // merged per fluid particle in first-seen order
-      const uint32_t lane = tid() & 31u, nwarps = nthr() >> 5;
-      uint32_t* slot = m.slot + (size_t)(tid() >> 5) * m.cap_nf;
-      for (uint32_t b = tid() >> 5; b < nb; b += nwarps) {
-        const uint32_t base = b * m.cap_items;
-        const MergeList L{m.item_j + base, m.item_w + base, m.item_v + base, nullptr, m.cap_items};
-        uint32_t cnt = 0;
-        bool overflow = false;
-        const V2 xb(m.bx[b]);
-        if (xb.finite()) {
-          warp_near_multi(
-              S.hA, m.gA, count_pb, [&](uint32_t q) { return xb + U.boundary_offset[q]; },
-              [&](uint32_t j, bool valid) { return valid ? V2(X[j]) : V2(); },
-              [&](uint32_t j, uint32_t q, V2 xj, bool valid) {
-                bool acc = false;
-                float w = 0.0f;
-                V2 dir;
-                if (valid) {
-                  const V2 bp = xb + U.boundary_offset[q];
-                  V2 delta = bp - xj;
-                  float r2 = delta.len2();
-                  if (!(r2 >= range2 || r2 <= inner2)) {
-                    float r = sqrtf(r2);
-                    if (!(!finite_f(r) || r <= 0.5f * h_adh || r >= h_adh)) {
-                      w = mass * adhesion_kernel(r, h_adh) / rho0;
-                      if (w > 0.0f) { acc = true; dir = w * (delta / r); }
-                    }
-                  }
-                }
-                warp_merge(acc, j, w, dir, 0.0f, slot, L, cnt, overflow);
-              });
-        }
-        for (uint32_t s = lane; s < min(cnt, m.cap_items); s += 32) slot[L.j[s]] = NONE;
-        __syncwarp();
-        if (__any_sync(FULL, overflow)) { if (lane == 0) atomicOr(err, ERR_ITEMS); cnt = 0; }
-        uint32_t used = 0;
-        if (cnt > 0) {
-          // dir_sum and weight_sum in item order (pbf.rs:1586-1594)
-          float weight_sum = 0.0f, dsx = 0.0f, dsy = 0.0f;
-          for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
-            const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
-            float ww = 0.0f;
-            V2 dd;
-            if (s < cnt) { ww = L.v0[s]; dd = V2(L.v1[s]); }
-#pragma unroll
-            for (uint32_t t = 0; t < 32; ++t) {
-              const float xt = __shfl_sync(FULL, dd.x, t), yt = __shfl_sync(FULL, dd.y, t);
-              const float wt = __shfl_sync(FULL, ww, t);
-              if (t < lim) {
-                dsx += xt;
-                dsy += yt;
-                weight_sum += wt;
-              }
-            }
-          }
-          V2 dir_sum(dsx, dsy);
-          float pull_len = dir_sum.len();
-          if (weight_sum > 1e-9f && pull_len > 1e-9f) {
-            V2 ball_pull_dir = -dir_sum / pull_len;
-            float coverage = fmin_r(weight_sum, 1.0f);
-            float m_contrib = mass * weight_sum;
-            float attach = m_contrib / (m.b_m + m_contrib);
-            V2 dv_b = ball_pull_dir * (adhesion_accel * coverage * dt * attach);
-            if (lane == 0) {
-              m.imp[b] = (V2(m.imp[b]) + m.b_m * dv_b).f2();
-              V2 lever = ball_pull_dir * m.b_r;
-              m.ang[b] += m.b_m * cross2(lever, dv_b);
-            }
-            for (uint32_t s = lane; s < cnt; s += 32) {
-              float frac = L.v0[s] / weight_sum;
-              V2 dv_i = -(m.b_m * frac / mass) * dv_b;
-              L.v1[s] = dv_i.f2();
-            }
-            used = cnt;
-          }
-        }
-        if (lane == 0) m.item_n[b] = used;
-        __syncwarp();
-      }
+      wide_phase(m, WIDE_ADHESION, &S.hA, [&](uint32_t w0, uint32_t nw) { adhesion_balls(m, U, S.hA, w0, nw); });
       __syncthreads();
       if (*err) return;
       // per-fluid sums of the balls' contributions in ball order (stable bucket sort by fluid)
@@ -1164,65 +1313,10 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
     __syncthreads();
     if (nb > 0 && m.b_r > 0.0f) {
       grid_build(X, n, h, m.gB, S.hB, err);
-      const float spiky_norm = -30.0f / (PI_F * powi5(h));
-      const float range2 = h * h * (1.0f + 1e-4f);
       for (uint32_t j = tid(); j < n; j += nthr())
         m.f_tmp[j] = BALL_BC_GAIN * (mass * 2.0f * m.mu_eff[j] / (fmax_r(m.density[j], 1e-6f) * rho0));
       __syncthreads();
-      // one warp per ball, candidates merged per fluid particle in first-seen order
-      uint32_t* slot = m.slot + (size_t)(tid() >> 5) * m.cap_nf;
-      for (uint32_t b = tid() >> 5; b < nb; b += nthr() >> 5) {
-        const uint32_t lane = tid() & 31u, base = b * m.cap_items;
-        const MergeList L{m.item_j + base, m.item_w + base, m.item_v + base, m.item_w2 + base, m.cap_items};
-        uint32_t cnt = 0;
-        bool overflow = false;
-        const V2 xb(m.bx[b]);
-        if (xb.finite()) {
-          struct XF {
-            V2 x;
-            float f;
-          };
-          warp_near_multi(
-              S.hB, m.gB, count_pb, [&](uint32_t q) { return xb + U.boundary_offset[q]; },
-              [&](uint32_t j, bool valid) {
-                XF d{V2(), 0.0f};
-                if (valid) {
-                  d.x = V2(X[j]);
-                  d.f = m.f_tmp[j];
-                }
-                return d;
-              },
-              [&](uint32_t j, uint32_t q, XF d, bool valid) {
-                bool acc = false;
-                float c = 0.0f, lever2_c = 0.0f;
-                V2 lever_c;
-                if (valid) {
-                  const V2 bp = xb + U.boundary_offset[q];
-                  V2 delta = d.x - bp;
-                  float r2 = delta.len2();
-                  if (!(r2 >= range2)) {
-                    float r = sqrtf(r2);
-                    if (!(!finite_f(r) || r >= h || r <= 1e-9f)) {
-                      float dot_abs = fabsf(spiky_norm * (h - r) * (h - r) * r);
-                      c = d.f * dot_abs / (r2 + eta2);
-                      if (c > 0.0f) {
-                        acc = true;
-                        V2 lever = bp - xb;
-                        lever_c = c * lever;
-                        lever2_c = c * lever.len2();
-                      }
-                    }
-                  }
-                }
-                warp_merge(acc, j, c, lever_c, lever2_c, slot, L, cnt, overflow);
-              });
-        }
-        for (uint32_t s = lane; s < min(cnt, m.cap_items); s += 32) slot[L.j[s]] = NONE;
-        __syncwarp();
-        if (__any_sync(FULL, overflow)) { if (lane == 0) atomicOr(err, ERR_ITEMS); cnt = 0; }
-        if (lane == 0) m.g_off[b] = cnt;
-        __syncwarp();
-      }
+      wide_phase(m, WIDE_GROUPS, &S.hB, [&](uint32_t w0, uint32_t nw) { group_balls(m, U, S.hB, w0, nw); });
       if (tid() == 0) m.g_off[nb] = 0;
       __syncthreads();
       if (*err) return;
@@ -1252,66 +1346,16 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       const float r = m.b_r;
       const double dxd = (double)(0.5f * h);
       const float reach = (float)(8.0 * dxd);
-      const float c_max = 8.0f * m.b_m / fmax_r(dt, 1e-12f);
-      const float range2 = (2.0f * r + reach) * (2.0f * r + reach) * (1.0f + 1e-4f);
       grid_build(m.bx, nb, 2.0f * r + reach, m.gBall, S.hBall, err);
       uint32_t in_range = 0;
-      // one warp per ball: candidates j > i in for_each_near order, ordered compaction, then the
-      // wall link, each film evaluated once; ball i's links go to its slots [i K, i K + K) of the
-      // record scratch, then one compaction copies them to the link list in ball order
+      // ball i's links go to its slots [i K, i K + K) of the record scratch, then one compaction
+      // copies them to the link list in ball order
       const uint32_t K = min(nb + 1u, 512u);
-      for (uint32_t i = tid() >> 5; i < nb; i += nthr() >> 5) {
-        const uint32_t lane = tid() & 31u;
-        const V2 xi(m.bx[i]), v0i(m.ball_v0[i]);
-        const uint32_t base = i * K;
-        uint32_t c = 0, inr = 0;
-        if (xi.finite()) {
-          struct XV {
-            V2 x, v0;
-          };
-          warp_near_multi(
-              S.hBall, m.gBall, 1u, [&](uint32_t) { return xi; },
-              [&](uint32_t j, bool valid) {
-                XV d{V2(), V2()};
-                if (valid && j > i) {
-                  d.x = V2(m.bx[j]);
-                  d.v0 = V2(m.ball_v0[j]);
-                }
-                return d;
-              },
-              [&](uint32_t j, uint32_t, XV d, bool valid) {
-                const bool cand = valid && j > i;
-                LinkEval L{false, false, V2(), 0.0f};
-                if (cand) L = link_pair(m, U, xi, v0i, d.x, d.v0, reach, range2, dxd, c_max, true);
-                inr += __popc(__ballot_sync(FULL, cand && L.in_range));
-                const uint32_t bal = __ballot_sync(FULL, cand && L.emit);
-                const uint32_t q = c + __popc(bal & ((1u << lane) - 1u));
-                if (cand && L.emit && q < K) {
-                  m.rec_i[base + q] = j;
-                  m.rec_J[base + q] = L.n.f2();
-                  m.rec_L[base + q] = L.c;
-                }
-                c += __popc(bal);
-              });
-          if (lane == 0) {
-            LinkEval W = link_wall(m, U, i, reach, dxd, c_max);
-            if (W.in_range) inr += 1;
-            if (W.emit) {
-              if (c < K) { m.rec_i[base + c] = NONE; m.rec_J[base + c] = W.n.f2(); m.rec_L[base + c] = W.c; }
-              ++c;
-            }
-          }
-        }
-        if (lane == 0) {
-          if (c > K) { atomicOr(err, ERR_LINKS); c = K; }
-          m.l_off[i] = c;
-          in_range += inr;
-        }
-        __syncwarp();
-      }
+      wide_phase(m, WIDE_LINKS, &S.hBall,
+                 [&](uint32_t w0, uint32_t nw) { in_range += link_balls(m, U, S.hBall, w0, nw); });
       if (tid() == 0) m.l_off[nb] = 0;
       __syncthreads();
-      const uint32_t tot_in = block_sum_u(in_range);
+      const uint32_t tot_in = block_sum_u(in_range) + wide_counter(m);
       const uint32_t nl = block_exclusive_scan(m.l_off, nb + 1);
       if (nl > m.cap_links) { if (tid() == 0) atomicOr(err, ERR_LINKS); __syncthreads(); return; }
       if (tid() == 0) { S.n_links = nl; S.links_in_range = tot_in; }

@@ -130,6 +130,9 @@ struct MgSim {
   // the device's stream-ordered memory pool and keeps its host blocks in pageable memory; it is
   // only ever advanced by the server's batched launches
   bool light = false;
+  // thread blocks the arena's merge slot maps are sized for: a plain handle's single-mill launches
+  // may spread its per-ball stages over this many blocks (batch and server mills use one)
+  uint32_t mill_blocks_cap = 1;
   uint32_t nf = 0, nb = 0, cap_nf = 0, cap_nb = 0;
   MgBallMaterial bmat{};
   MgFluidMaterial fmat{};
@@ -263,7 +266,8 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
     m.bxs = a.take<float2>(cb); m.bmove = a.take<float>(cb); m.f_cw = a.take<double>(cb);
     m.rec_off = a.take<uint32_t>(cb + 1); m.rec_pred = a.take<uint32_t>(m.cap_recs);
     m.ball_done = a.take<uint32_t>(cb);
-    m.slot = a.take<uint32_t>((size_t)MAX_BLOCK_WARPS * cf);
+    m.slot = a.take<uint32_t>((size_t)MAX_BLOCK_WARPS * s->mill_blocks_cap * cf);
+    m.wide = a.take<WideCtl>(1);
     m.pair_i = a.take<uint32_t>(m.cap_pairs); m.pair_j = a.take<uint32_t>(m.cap_pairs);
     m.lam_bb = a.take<float>(m.cap_pairs);
     m.pr_list = a.take<uint32_t>(m.cap_pairs);
@@ -278,7 +282,7 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
     }
   }
   // the merge slot maps are kept all-NONE between uses
-  cudaMemsetAsync(m.slot, 0xFF, sizeof(uint32_t) * (size_t)MAX_BLOCK_WARPS * cf, s->stream);
+  cudaMemsetAsync(m.slot, 0xFF, sizeof(uint32_t) * (size_t)MAX_BLOCK_WARPS * s->mill_blocks_cap * cf, s->stream);
   // the clears must land before anything else touches the arena, whichever stream it uses
   CK(cudaStreamSynchronize(s->stream));
   m.nf = nf;
@@ -409,9 +413,11 @@ int run(MgSim* s, uint32_t n_sub) {
   CK(cudaMemcpyAsync(s->d_uni, s->h_uni, sizeof(StepUniform), cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemcpyAsync(s->d_ang, s->h_ang, sizeof(SubAngles) * n_sub, cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemsetAsync(s->md.err, 0, sizeof(uint32_t), s->stream));
+  const uint32_t mill_blocks = s->opt.mill_blocks ? s->opt.mill_blocks : std::min(DEFAULT_MILL_BLOCKS, s->mill_blocks_cap);
+  if (mill_blocks > 1) CK(cudaMemsetAsync(s->md.wide, 0, sizeof(WideCtl), s->stream));
   CK(cudaEventRecord(s->ev0, s->stream));
   CK(launch_substeps(s->d_md, 1, s->d_uni, s->d_ang, n_sub, nullptr, s->opt.block_threads, s->md.smem_bytes,
-                     s->stream));
+                     s->stream, mill_blocks));
   CK(cudaEventRecord(s->ev1, s->stream));
   CK(cudaMemcpyAsync(s->h_out, s->md.out, sizeof(StepOut) * n_sub, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
@@ -425,6 +431,7 @@ int run(MgSim* s, uint32_t n_sub) {
   }
   uint32_t e = 0;
   for (uint32_t k = 0; k < n_sub; ++k) e |= s->h_out[k].err;
+  if (e & ERR_WIDE) return fail(s, MG_ERR_CUDA, "the mill's thread blocks stopped waiting for one another (timeout)");
   if (e) return fail(s, MG_ERR_CAPACITY, "device capacity exceeded (error bits 0x%x)", e);
   size_t total_imp = 0;
   for (uint32_t k = 0; k < n_sub; ++k) total_imp += s->h_out[k].n_impacts;
@@ -564,7 +571,8 @@ int upload_fluid(MgSim* s, const float* x, const float* v, const float* dye, con
 }
 
 // Simulation::new / with_initial_balls. With a server stream the handle is a light one (MgSim::light).
-int create_sim(const MgParams* p, const float* xy, uint32_t n_init, MgSim** out, cudaStream_t server_stream = nullptr) {
+int create_sim(const MgParams* p, const float* xy, uint32_t n_init, MgSim** out, cudaStream_t server_stream = nullptr,
+               uint32_t mill_blocks_cap = 1) {
   if (!p || !out) return fail_global(MG_ERR_ARG, "null argument");
   std::string e;
   if (!mgh::params_validate(*p, &e)) return fail_global(MG_ERR_INVALID_PARAMS, "%s", e.c_str());
@@ -573,6 +581,7 @@ int create_sim(const MgParams* p, const float* xy, uint32_t n_init, MgSim** out,
     return fail_global(MG_ERR_NO_DEVICE, "no CUDA device visible");
   MgSim* s = new MgSim();
   s->params = *p;
+  s->mill_blocks_cap = std::max<uint32_t>(1u, std::min<uint32_t>(mill_blocks_cap, MAX_MILL_BLOCKS));
   int rc = server_stream ? init_light_handle(s, server_stream) : init_handle(s);
   if (rc) { g_err = s->err; mg_sim_destroy(s); return rc; }
   float radius = mgh::mill_radius(p->mill);
@@ -691,11 +700,11 @@ int mg_params_derived(const MgParams* pp, MgDerived* o) {
   return MG_OK;
 }
 
-int mg_sim_create(const MgParams* p, MgSim** out) { return create_sim(p, nullptr, 0, out); }
+int mg_sim_create(const MgParams* p, MgSim** out) { return create_sim(p, nullptr, 0, out, nullptr, MAX_MILL_BLOCKS); }
 int mg_sim_create_with_balls(const MgParams* p, const float* xy, uint32_t n, MgSim** out) {
   if (!xy && n) return fail_global(MG_ERR_ARG, "null positions");
   static const float dummy[2] = {0.0f, 0.0f};
-  return create_sim(p, xy ? xy : dummy, n, out);
+  return create_sim(p, xy ? xy : dummy, n, out, nullptr, MAX_MILL_BLOCKS);
 }
 void mg_sim_destroy(MgSim* s) {
   if (!s) return;
@@ -730,6 +739,8 @@ int mg_sim_set_options(MgSim* s, const MgOptions* o) {
     return fail(s, MG_ERR_ARG, "block_threads must be a multiple of 32 in [32, %u]", MAX_BLOCK_THREADS);
   if (o->sweep_warps > MAX_BLOCK_WARPS) return fail(s, MG_ERR_ARG, "sweep_warps must be in [0, %u]", MAX_BLOCK_WARPS);
   if (o->spin_ns > 100000) return fail(s, MG_ERR_ARG, "spin_ns must be at most 100000");
+  if (o->mill_blocks > s->mill_blocks_cap)
+    return fail(s, MG_ERR_ARG, "mill_blocks must be in [0, %u] for this handle", s->mill_blocks_cap);
   s->opt = *o;
   return MG_OK;
 }

@@ -11,23 +11,38 @@ namespace mg {
 // n_sub is the sub-step stride of `angles`; mill b runs n_sub_of[b] sub-steps when n_sub_of is
 // given (a batch of mills with different sub-step counts), else n_sub. Two instantiations: up to
 // 512 threads per block (128 registers a thread) and up to 1024 (64 registers, more warps for the
-// per-ball stages); the results do not depend on the block size.
+// per-ball stages); the results do not depend on the block size. With helpers > 0 the launch runs
+// one mill: block 0 is the mill's block and blocks 1..helpers take shares of its per-ball stages
+// (mill_wide.cuh); the results do not depend on the number of blocks either.
 template <int MAX_THREADS>
 __global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDev* __restrict__ mills,
                                                                     StepUniform* uni,
                                                                     const SubAngles* __restrict__ angles,
                                                                     uint32_t n_sub,
-                                                                    const uint32_t* __restrict__ n_sub_of) {
+                                                                    const uint32_t* __restrict__ n_sub_of,
+                                                                    uint32_t helpers) {
   __shared__ MillDev m;
   __shared__ FluidShared fs;
   __shared__ DemShared ds;
   extern __shared__ __align__(16) unsigned char dsm[];  // staged ball state (24 bytes per ball)
-  const uint32_t mill = blockIdx.x;
+  const uint32_t mill = helpers ? 0u : blockIdx.x;
   if (threadIdx.x == 0) {
     m = mills[mill];
-    *m.err = 0;
+    m.helpers = helpers;
+    if (blockIdx.x == 0 || helpers == 0) *m.err = 0;
+    g_wide_seq = 0;
   }
   __syncthreads();
+  if (helpers && blockIdx.x > 0) {
+    wide_helper(m, [&](uint32_t phase, const GridHdr& hdr, uint32_t w0, uint32_t nw) -> uint32_t {
+      const StepUniform& U = uni[0];
+      if (phase == WIDE_ADHESION) adhesion_balls(m, U, hdr, w0, nw);
+      else if (phase == WIDE_GROUPS) group_balls(m, U, hdr, w0, nw);
+      else if (phase == WIDE_LINKS) return link_balls(m, U, hdr, w0, nw);
+      return 0u;
+    });
+    return;
+  }
   const uint32_t my_sub = n_sub_of ? n_sub_of[mill] : n_sub;
   for (uint32_t s = 0; s < my_sub; ++s) {
     StepUniform& U = uni[mill];
@@ -56,6 +71,7 @@ __global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDe
     if (threadIdx.x == 0) out.err = *m.err;
     __syncthreads();
   }
+  wide_exit(m);
 }
 
 // Grid-stage probe: builds the grid of caller points and, per `mode`, leaves the grid (0), the
@@ -89,14 +105,23 @@ __global__ void __launch_bounds__(512) probe_kernel(const MillDev* __restrict__ 
 
 cudaError_t launch_substeps(const MillDev* mills, uint32_t n_mills, StepUniform* uni, const SubAngles* angles,
                             uint32_t n_sub, const uint32_t* n_sub_of, uint32_t threads, size_t smem_bytes,
-                            cudaStream_t stream) {
+                            cudaStream_t stream, uint32_t mill_blocks) {
   if (threads == 0 || threads > MAX_BLOCK_THREADS) threads = DEFAULT_BLOCK_THREADS;
   auto kernel = threads > 512 ? mill_substeps_kernel<MAX_BLOCK_THREADS> : mill_substeps_kernel<512>;
   if (smem_bytes > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
     if (e != cudaSuccess) return e;
   }
-  kernel<<<n_mills, threads, smem_bytes, stream>>>(mills, uni, angles, n_sub, n_sub_of);
+  uint32_t helpers = n_mills == 1 && mill_blocks > 1 ? min(mill_blocks, MAX_MILL_BLOCKS) - 1u : 0u;
+  if (helpers) {
+    // all of the mill's blocks wait for one another, so they must be resident together
+    void* args[] = {(void*)&mills, (void*)&uni, (void*)&angles, (void*)&n_sub, (void*)&n_sub_of, (void*)&helpers};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)kernel, dim3(1u + helpers), dim3(threads), args,
+                                                smem_bytes, stream);
+    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+  }
+  kernel<<<n_mills, threads, smem_bytes, stream>>>(mills, uni, angles, n_sub, n_sub_of, 0u);
   return cudaGetLastError();
 }
 

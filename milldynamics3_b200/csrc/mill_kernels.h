@@ -9,10 +9,12 @@ namespace mg {
 // mill b when n_sub_of is given, else n_sub. uni holds one StepUniform per mill; angles holds
 // n_mills * n_sub SubAngles, mill-major (n_sub is the stride). Each mill's sticky error word is
 // cleared at the start of the launch. smem_bytes of dynamic shared memory must be at least every
-// mill's MillDev::smem_bytes.
+// mill's MillDev::smem_bytes. With n_mills == 1 and mill_blocks > 1, the mill's per-ball stages
+// are shared with mill_blocks - 1 helper blocks (a cooperative launch; the mill's control block
+// must be zeroed before the launch and its slot maps sized for all the blocks' warps).
 cudaError_t launch_substeps(const MillDev* mills, uint32_t n_mills, StepUniform* uni, const SubAngles* angles,
                             uint32_t n_sub, const uint32_t* n_sub_of, uint32_t threads, size_t smem_bytes,
-                            cudaStream_t stream);
+                            cudaStream_t stream, uint32_t mill_blocks = 1);
 // Packs the impact records of n_mills mills after a launch: mill b's records of its sub-steps
 // 0..n_sub_of[b]-1 (StepOut::n_impacts each, at most cap_impacts) are appended in sub-step order
 // at an offset taken from *cursor (one atomic per mill); table[b] = {offset, count}. Records that

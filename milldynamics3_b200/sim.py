@@ -134,12 +134,14 @@ class Simulation:
     def reset_energy_budget(self):
         self._c(self.lib.sim_reset_energy_budget(self.h))
 
-    def set_options(self, cg_fp64: int = 0, block_threads: int = 0, sweep_warps: int = 0, spin_ns: int = 0):
+    def set_options(self, cg_fp64: int = 0, block_threads: int = 0, sweep_warps: int = 0, spin_ns: int = 0,
+                    mill_blocks: int = 0):
         o = capi.Options()
         o.cg_fp64 = cg_fp64
         o.block_threads = block_threads
         o.sweep_warps = sweep_warps
         o.spin_ns = spin_ns
+        o.mill_blocks = mill_blocks
         if hasattr(self.lib, "sim_set_options"):
             self._c(self.lib.sim_set_options(self.h, C.byref(o)))
         else:
