@@ -181,9 +181,9 @@ typedef struct MgScalars {
  * sweep_warps: warps that take balls in the per-ball drag and buoyancy sweeps (0 = default).
  * spin_ns: poll interval of a ball waiting for an earlier ball in those sweeps (0 = default).
  * mill_blocks: thread blocks that share a single mill's per-ball stages (adhesion, boundary
- * groups, squeeze links) in the handle's own launches: 0 = default (8), 1 = the mill's block
- * alone, at most 16 for handles from mg_sim_create / mg_sim_create_with_balls; the mills of a
- * batch or a server always run one block each (0 or 1 only).
+ * groups, squeeze links, drag and buoyancy item lists) in the handle's own launches: 0 = default
+ * (16), 1 = the mill's block alone, at most 16 for handles from mg_sim_create /
+ * mg_sim_create_with_balls; the mills of a batch or a server always run one block each (0 or 1).
  * None of them changes results. */
 typedef struct MgOptions {
   uint32_t cg_fp64;

@@ -29,7 +29,7 @@ constexpr uint32_t DEFAULT_BLOCK_THREADS = 1024;
 // Thread blocks that run one mill's per-ball stages in a single-mill launch: the mill's own block
 // plus helper blocks (at most MAX_MILL_BLOCKS; DEFAULT_MILL_BLOCKS unless the caller sets it).
 constexpr uint32_t MAX_MILL_BLOCKS = 16;
-constexpr uint32_t DEFAULT_MILL_BLOCKS = 8;
+constexpr uint32_t DEFAULT_MILL_BLOCKS = 16;
 constexpr uint32_t DEFAULT_SPIN_NS = 64;
 constexpr int MAX_BOUNDARY_POINTS = 1024;
 

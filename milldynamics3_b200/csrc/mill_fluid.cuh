@@ -455,6 +455,98 @@ __device__ uint32_t link_balls(const MillDev& m, const StepUniform& U, const Gri
   return in_range;
 }
 
+// Drag item lists per ball (pbf.rs:1794-1822): fluid particles within r + h of the ball centre in
+// for_each_near order, with their offsets and weights (item_j / item_v / item_w, count item_n).
+// Returns the thread's part of the item count.
+__device__ uint32_t drag_item_balls(const MillDev& m, const GridHdr& hB, uint32_t w0, uint32_t nw) {
+  const uint32_t nb = m.nb;
+  const float h = m.f_h;
+  const float2* X = m.fx;
+  uint32_t* err = m.err;
+  const float h_c = m.b_r + h;
+  const float w_hc0 = fmax_r(poly6(0.0f, h_c), 1e-12f);
+  uint32_t items = 0;
+  for (uint32_t b = w0; b < nb; b += nw) {
+    const uint32_t lane = tid() & 31u, base = b * m.cap_items;
+    uint32_t cnt = 0;
+    const V2 xb(m.bx[b]);
+    if (xb.finite()) {
+      warp_near_multi(
+          hB, m.gB, 1u, [&](uint32_t) { return xb; },
+          [&](uint32_t j, bool valid) { return valid ? V2(X[j]) : V2(); },
+          [&](uint32_t j, uint32_t, V2 xj, bool valid) {
+        bool keep = false;
+        V2 r_i;
+        float phi = 0.0f;
+        if (valid) {
+          r_i = xj - xb;
+          float r2 = r_i.len2();
+          if (!(!finite_f(r2) || r2 >= h_c * h_c)) {
+            phi = poly6(r2, h_c) / w_hc0;
+            keep = phi > 0.0f;
+          }
+        }
+        const uint32_t bal = __ballot_sync(FULL, keep);
+        const uint32_t pos = cnt + __popc(bal & ((1u << lane) - 1u));
+        if (keep && pos < m.cap_items) {
+          m.item_j[base + pos] = j;
+          m.item_v[base + pos] = r_i.f2();
+          m.item_w[base + pos] = phi;
+        }
+        cnt += __popc(bal);
+      });
+    }
+    if (cnt > m.cap_items) { if (lane == 0) atomicOr(err, ERR_ITEMS); cnt = 0; }
+    if (lane == 0) { m.item_n[b] = cnt; items += cnt; }
+    __syncwarp();
+  }
+  return items;
+}
+
+// Buoyancy item lists per ball (pbf.rs:2042-2060) on the stale step-2 grid: fluid particles with a
+// positive poly6 weight in for_each_near order, their weights, and the local density (item_v[0]).
+// Returns the thread's part of the item count.
+__device__ uint32_t buoyancy_item_balls(const MillDev& m, const GridHdr& hA, uint32_t w0, uint32_t nw) {
+  const uint32_t nb = m.nb;
+  const float h = m.f_h, mass = m.f_mass;
+  const float2* X = m.fx;
+  uint32_t* err = m.err;
+  uint32_t items = 0;
+  for (uint32_t b = w0; b < nb; b += nw) {
+    const uint32_t lane = tid() & 31u, base = b * m.cap_items;
+    uint32_t cnt = 0;
+    const V2 xb(m.bx[b]);
+    float rho_local = 0.0f;
+    if (xb.finite()) {
+      warp_near_multi(
+          hA, m.gA, 1u, [&](uint32_t) { return xb; },
+          [&](uint32_t j, bool valid) { return valid ? V2(X[j]) : V2(); },
+          [&](uint32_t j, uint32_t, V2 xj, bool valid) {
+        float w = 0.0f;
+        if (valid) w = mass * poly6((xb - xj).len2(), h);
+        const bool keep = w > 0.0f;
+        const uint32_t bal = __ballot_sync(FULL, keep);
+        const uint32_t pos = cnt + __popc(bal & ((1u << lane) - 1u));
+        if (keep && pos < m.cap_items) { m.item_j[base + pos] = j; m.item_w[base + pos] = w; }
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+          const float wt = __shfl_sync(FULL, w, t);
+          if ((bal >> t) & 1u) rho_local += wt;
+        }
+        cnt += __popc(bal);
+      });
+    }
+    if (cnt > m.cap_items) { if (lane == 0) atomicOr(err, ERR_ITEMS); cnt = 0; }
+    if (lane == 0) {
+      m.item_n[b] = rho_local > 0.0f ? cnt : 0u;
+      if (rho_local > 0.0f) items += cnt;
+      m.item_v[base] = make_float2(rho_local, 0.0f);
+    }
+    __syncwarp();
+  }
+  return items;
+}
+
 __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err, FluidShared& S,
                            unsigned char* dsm) {
   uint32_t* done = m.ball_done;  // completion flags of the per-ball sweeps (moved to shared below)
@@ -855,40 +947,10 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       grid_build(X, n, fmax_r(h_c, 1e-6f), m.gB, S.hB, err);
       // item lists per ball in for_each_near order (positions do not change during the sweep):
       // one warp per ball, an ordered compaction of each 32-candidate chunk
-      for (uint32_t b = tid() >> 5; b < nb; b += nthr() >> 5) {
-        const uint32_t lane = tid() & 31u, base = b * m.cap_items;
-        uint32_t cnt = 0;
-        const V2 xb(m.bx[b]);
-        if (xb.finite()) {
-          warp_near_multi(
-              S.hB, m.gB, 1u, [&](uint32_t) { return xb; },
-              [&](uint32_t j, bool valid) { return valid ? V2(X[j]) : V2(); },
-              [&](uint32_t j, uint32_t, V2 xj, bool valid) {
-            bool keep = false;
-            V2 r_i;
-            float phi = 0.0f;
-            if (valid) {
-              r_i = xj - xb;
-              float r2 = r_i.len2();
-              if (!(!finite_f(r2) || r2 >= h_c * h_c)) {
-                phi = poly6(r2, h_c) / w_hc0;
-                keep = phi > 0.0f;
-              }
-            }
-            const uint32_t bal = __ballot_sync(FULL, keep);
-            const uint32_t pos = cnt + __popc(bal & ((1u << lane) - 1u));
-            if (keep && pos < m.cap_items) {
-              m.item_j[base + pos] = j;
-              m.item_v[base + pos] = r_i.f2();
-              m.item_w[base + pos] = phi;
-            }
-            cnt += __popc(bal);
-          });
-        }
-        if (cnt > m.cap_items) { if (lane == 0) atomicOr(err, ERR_ITEMS); cnt = 0; }
-        if (lane == 0) { m.item_n[b] = cnt; atomicAdd(&out.ctr.n_coupling_items, cnt); }
-        __syncwarp();
-      }
+      uint32_t n_items = 0;
+      wide_phase(m, WIDE_DRAG_ITEMS, &S.hB, [&](uint32_t w0, uint32_t nw) { n_items += drag_item_balls(m, S.hB, w0, nw); });
+      n_items = block_sum_u(n_items) + wide_counter(m);
+      if (tid() == 0) out.ctr.n_coupling_items += n_items;
       __syncthreads();
       if (*err) return;
       stage_mark(out.stage, 24);
@@ -1084,38 +1146,10 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
   // ---- step 6.6: buoyancy, Gauss-Seidel over balls on the stale step-2 grid (pbf.rs:2035-2122)
   if (nb > 0 && m.b_r > 0.0f) {
     const float area = PI_F * m.b_r * m.b_r;
-    for (uint32_t b = tid() >> 5; b < nb; b += nthr() >> 5) {
-      const uint32_t lane = tid() & 31u, base = b * m.cap_items;
-      uint32_t cnt = 0;
-      const V2 xb(m.bx[b]);
-      float rho_local = 0.0f;
-      if (xb.finite()) {
-        warp_near_multi(
-            S.hA, m.gA, 1u, [&](uint32_t) { return xb; },
-            [&](uint32_t j, bool valid) { return valid ? V2(X[j]) : V2(); },
-            [&](uint32_t j, uint32_t, V2 xj, bool valid) {
-          float w = 0.0f;
-          if (valid) w = mass * poly6((xb - xj).len2(), h);
-          const bool keep = w > 0.0f;
-          const uint32_t bal = __ballot_sync(FULL, keep);
-          const uint32_t pos = cnt + __popc(bal & ((1u << lane) - 1u));
-          if (keep && pos < m.cap_items) { m.item_j[base + pos] = j; m.item_w[base + pos] = w; }
-#pragma unroll
-          for (int t = 0; t < 32; ++t) {
-            const float wt = __shfl_sync(FULL, w, t);
-            if ((bal >> t) & 1u) rho_local += wt;
-          }
-          cnt += __popc(bal);
-        });
-      }
-      if (cnt > m.cap_items) { if (lane == 0) atomicOr(err, ERR_ITEMS); cnt = 0; }
-      if (lane == 0) {
-        m.item_n[b] = rho_local > 0.0f ? cnt : 0u;
-        if (rho_local > 0.0f) atomicAdd(&out.ctr.n_coupling_items, cnt);
-        m.item_v[base] = make_float2(rho_local, 0.0f);
-      }
-      __syncwarp();
-    }
+    uint32_t n_items = 0;
+    wide_phase(m, WIDE_BUOYANCY_ITEMS, &S.hA, [&](uint32_t w0, uint32_t nw) { n_items += buoyancy_item_balls(m, S.hA, w0, nw); });
+    n_items = block_sum_u(n_items) + wide_counter(m);
+    if (tid() == 0) out.ctr.n_coupling_items += n_items;
     __syncthreads();
     if (*err) return;
     stage_mark(out.stage, 27);

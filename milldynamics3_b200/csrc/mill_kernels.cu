@@ -39,6 +39,8 @@ __global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDe
       if (phase == WIDE_ADHESION) adhesion_balls(m, U, hdr, w0, nw);
       else if (phase == WIDE_GROUPS) group_balls(m, U, hdr, w0, nw);
       else if (phase == WIDE_LINKS) return link_balls(m, U, hdr, w0, nw);
+      else if (phase == WIDE_DRAG_ITEMS) return drag_item_balls(m, hdr, w0, nw);
+      else if (phase == WIDE_BUOYANCY_ITEMS) return buoyancy_item_balls(m, hdr, w0, nw);
       return 0u;
     });
     return;

@@ -14,7 +14,14 @@
 
 namespace mg {
 
-enum : uint32_t { WIDE_EXIT = 0, WIDE_ADHESION = 1, WIDE_GROUPS = 2, WIDE_LINKS = 3 };
+enum : uint32_t {
+  WIDE_EXIT = 0,
+  WIDE_ADHESION = 1,
+  WIDE_GROUPS = 2,
+  WIDE_LINKS = 3,
+  WIDE_DRAG_ITEMS = 4,
+  WIDE_BUOYANCY_ITEMS = 5
+};
 
 constexpr long long WIDE_TIMEOUT_CYCLES = 20000000000LL;  // ~10 s at 2 GHz
 
