@@ -187,6 +187,50 @@ __device__ __forceinline__ void small_sort_u32(uint32_t* a, uint32_t n) {
   }
 }
 
+// Ascending sort of a[0..n), n <= 256, by one full warp: element e = 32 r + lane sits in lane
+// `lane`'s register r (the tail padded with the largest value); a bitonic network whose
+// partners are 32 or more apart swap registers and the nearer ones exchange by shuffles.
+__device__ __forceinline__ void warp_sort256_u32(uint32_t* a, uint32_t n) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t v[8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const uint32_t e = 32u * r + lane;
+    v[r] = e < n ? a[e] : 0xFFFFFFFFu;
+  }
+#pragma unroll
+  for (uint32_t k = 2; k <= 256; k <<= 1) {
+#pragma unroll
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+        const uint32_t rj = j >> 5;
+#pragma unroll
+        for (uint32_t r = 0; r < 8; ++r) {
+          const uint32_t rr = r ^ rj;
+          if (rr > r) {
+            const bool up = ((32u * r + lane) & k) == 0;
+            const uint32_t x = v[r], y = v[rr];
+            if ((x > y) == up) { v[r] = y; v[rr] = x; }
+          }
+        }
+      } else {
+#pragma unroll
+        for (uint32_t r = 0; r < 8; ++r) {
+          const uint32_t y = __shfl_xor_sync(0xffffffffu, v[r], (int)j);
+          const bool up = ((32u * r + lane) & k) == 0;
+          const bool lower = (lane & j) == 0;
+          v[r] = lower == up ? min(v[r], y) : max(v[r], y);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const uint32_t e = 32u * r + lane;
+    if (e < n) a[e] = v[r];
+  }
+}
+
 // Stable bucket sort: start[0..nbk] receives bucket offsets, order[] the record indices grouped by
 // key in ascending record order; cur[0..nbk) is scratch.
 __device__ inline void block_bucket_sort(const uint32_t* keys, uint32_t nrec, uint32_t nbk, uint32_t* start, uint32_t* cur,
@@ -196,32 +240,47 @@ __device__ inline void block_bucket_sort(const uint32_t* keys, uint32_t nrec, ui
   for (uint32_t r = tid(); r < nrec; r += nthr()) atomicAdd(&start[keys[r]], 1u);
   __syncthreads();
   block_exclusive_scan(start, nbk + 1);
-  // buckets of more than 32 records (up to 64 of them) are filled in record order by one warp
-  // each; the others are scattered by atomics, then sorted by one thread
-  constexpr uint32_t SMALL = 32, NBIG = 64, BIG = 0xFFFFFFFFu;
-  __shared__ uint32_t big[NBIG];
-  __shared__ uint32_t nbig;
-  if (tid() == 0) nbig = 0;
+  // Buckets of up to 32 records: scattered by atomics, then sorted by one thread. 33 to 256
+  // records (up to 256 such buckets): scattered, then sorted by one warp in registers. More than
+  // 256 (up to 64 such buckets): filled in record order by one warp. Buckets beyond those lists
+  // are scattered and sorted by one thread.
+  constexpr uint32_t SMALL = 32, MID = 256, NMID = 256, NBIG = 64;
+  constexpr uint32_t BIG_MARK = 0xFFFFFFFFu, MID_MARK = 0xFFFFFFFEu;
+  __shared__ uint32_t big[NBIG], mid[NMID];
+  __shared__ uint32_t nbig, nmid;
+  if (tid() == 0) { nbig = 0; nmid = 0; }
   __syncthreads();
   for (uint32_t k = tid(); k < nbk; k += nthr()) {
     uint32_t c = start[k];
-    if (start[k + 1] - c > SMALL) {
+    const uint32_t sz = start[k + 1] - c;
+    if (sz > MID) {
       const uint32_t q = atomicAdd(&nbig, 1u);
-      if (q < NBIG) { big[q] = k; c = BIG; }
+      if (q < NBIG) { big[q] = k; c = BIG_MARK; }
+    } else if (sz > SMALL) {
+      const uint32_t q = atomicAdd(&nmid, 1u);
+      if (q < NMID) mid[q] = k;
     }
     cur[k] = c;
   }
   __syncthreads();
   for (uint32_t r = tid(); r < nrec; r += nthr()) {
     const uint32_t k = keys[r];
-    if (cur[k] == BIG) continue;
+    if (cur[k] == BIG_MARK) continue;
     uint32_t slot = atomicAdd(&cur[k], 1u);
     order[slot] = r;
   }
+  __syncthreads();
+  const uint32_t nl_mid = min(nmid, NMID), nl_big = min(nbig, NBIG);
+  for (uint32_t q = tid(); q < nl_mid; q += nthr()) cur[mid[q]] = MID_MARK;
   {
-    const uint32_t lane = tid() & 31u, nl = min(nbig, NBIG);
-    for (uint32_t q = tid() >> 5; q < nl; q += nthr() >> 5) {
-      const uint32_t k = big[q];
+    const uint32_t lane = tid() & 31u;
+    for (uint32_t q = tid() >> 5; q < nl_mid + nl_big; q += nthr() >> 5) {
+      if (q < nl_mid) {
+        const uint32_t k = mid[q];
+        warp_sort256_u32(order + start[k], start[k + 1] - start[k]);
+        continue;
+      }
+      const uint32_t k = big[q - nl_mid];
       uint32_t o = start[k];
       for (uint32_t c0 = 0; c0 < nrec; c0 += 32) {
         const uint32_t r = c0 + lane;
@@ -234,7 +293,7 @@ __device__ inline void block_bucket_sort(const uint32_t* keys, uint32_t nrec, ui
   }
   __syncthreads();
   for (uint32_t k = tid(); k < nbk; k += nthr())
-    if (cur[k] != BIG) small_sort_u32(order + start[k], start[k + 1] - start[k]);
+    if (cur[k] < MID_MARK) small_sort_u32(order + start[k], start[k + 1] - start[k]);
   __syncthreads();
 }
 

@@ -229,6 +229,8 @@ struct WideCtl {
   uint32_t done;     // helper-block phases finished, over the launch
   uint32_t counter;  // a phase's count summed over the helper blocks
   GridHdr hdr;       // the grid the phase searches
+  const float2* vin; // the vectors a phase reads and writes (joint operator)
+  float2* vout;
 };
 
 // ---------------------------------------------------------------- per-mill descriptor

@@ -160,32 +160,37 @@ __device__ __forceinline__ LinkEval link_wall(const MillDev& m, const StepUnifor
   return L;
 }
 
-// Joint-system operator of pbf.rs:703-737 applied to xx, written to out (all rows).
-__device__ void joint_apply(const MillDev& m, float dt, const float2* xx, float2* out) {
-  uint32_t n = m.nf, nb = m.nb;
-  float mass = m.f_mass;
-  float k = dt * mass;
-  for (uint32_t i = tid(); i < n; i += nthr()) m.cg_lv[i] = laplacian_row(m, xx, i).f2();
-  __syncthreads();
+// Rows t0, t0 + stride, ... of the joint-system operator of pbf.rs:703-737 applied to xx, written
+// to out: fluid rows 0..n-1 (Laplacian, then the boundary groups), then ball rows n..n+nb-1
+// (linear and angular).
+__device__ void joint_apply_rows(const MillDev& m, float dt, const float2* xx, float2* out, uint32_t t0,
+                                 uint32_t stride) {
+  const uint32_t n = m.nf, nb = m.nb;
+  const float mass = m.f_mass;
+  const float k = dt * mass;
   // (the loops are unrolled so that the independent loads of consecutive terms overlap; the
   // additions keep their order)
-  for (uint32_t i = tid(); i < n; i += nthr()) {
-    V2 o = mass * (V2(xx[i]) + dt * V2(m.cg_lv[i]));
-    const uint32_t q0 = m.fg_start[i], q1 = m.fg_start[i + 1];
+  for (uint32_t t = t0; t < n + nb; t += stride) {
+    if (t < n) {
+      const uint32_t i = t;
+      const V2 lv(laplacian_row(m, xx, i).f2());
+      V2 o = mass * (V2(xx[i]) + dt * lv);
+      const uint32_t q0 = m.fg_start[i], q1 = m.fg_start[i + 1];
 #pragma unroll 4
-    for (uint32_t q = q0; q < q1; ++q) {
-      uint32_t g = m.fg_list[q];
-      uint32_t bi = m.g_ball[g];
-      V2 vb(xx[n + bi]);
-      float w = xx[n + nb + bi].x;
-      V2 rel = V2(xx[i]) - vb;
-      V2 lc(m.g_lc[g]);
-      V2 d = k * (m.g_c[g] * rel - w * V2(-lc.y, lc.x));
-      o += d;
+      for (uint32_t q = q0; q < q1; ++q) {
+        uint32_t g = m.fg_list[q];
+        uint32_t bi = m.g_ball[g];
+        V2 vb(xx[n + bi]);
+        float w = xx[n + nb + bi].x;
+        V2 rel = V2(xx[i]) - vb;
+        V2 lc(m.g_lc[g]);
+        V2 d = k * (m.g_c[g] * rel - w * V2(-lc.y, lc.x));
+        o += d;
+      }
+      out[i] = o.f2();
+      continue;
     }
-    out[i] = o.f2();
-  }
-  for (uint32_t bi = tid(); bi < nb; bi += nthr()) {
+    const uint32_t bi = t - n;
     V2 vb(xx[n + bi]);
     float w = xx[n + nb + bi].x;
     V2 o = m.b_m * vb;
@@ -222,7 +227,55 @@ __device__ void joint_apply(const MillDev& m, float dt, const float2* xx, float2
     out[n + bi] = o.f2();
     out[n + nb + bi] = make_float2(oa, 0.0f);
   }
-  __syncthreads();
+}
+
+// The joint-system operator over all of the mill's blocks (all rows written on return).
+__device__ void joint_apply(const MillDev& m, float dt, const float2* xx, float2* out) {
+  wide_phase(m, WIDE_JOINT_APPLY, nullptr, xx, out, [&](uint32_t w0, uint32_t nw) {
+    joint_apply_rows(m, dt, xx, out, w0 * 32u + (tid() & 31u), nw * 32u);
+  });
+}
+
+// Rows t0, t0 + stride, ... of the joint solve's set-up (pbf.rs:641-700): the start vector x, the
+// right-hand side and the Jacobi diagonal, fluid rows then ball rows.
+__device__ void cg_setup_rows(const MillDev& m, float dt, uint32_t t0, uint32_t stride) {
+  const uint32_t n = m.nf, nb = m.nb;
+  const float mass = m.f_mass;
+  const float2* V = m.fv;
+  float2 *x = m.cg_x, *bvec = m.cg_b;
+  float* diag = m.cg_diag;
+  const bool use_guess = *m.guess_valid_dev != 0;
+  for (uint32_t t = t0; t < n + nb; t += stride) {
+    if (t < n) {
+      const uint32_t i = t;
+      V2 v(V[i]);
+      x[i] = (use_guess ? v + V2(m.fguess[i]) : v).f2();
+      bvec[i] = (mass * v).f2();
+      float sw = 0.0f;
+      for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) sw += m.visc_w[k];
+      float d = mass * (1.0f + dt * (0.5f * CENTRAL_VISC * sw));
+      for (uint32_t q = m.fg_start[i]; q < m.fg_start[i + 1]; ++q) d += dt * mass * m.g_c[m.fg_list[q]];
+      diag[i] = d;
+      m.dv_tmp[i] = V[i];  // v_in for the warm start of the next sub-step
+      continue;
+    }
+    const uint32_t b = t - n;
+    V2 v0(m.ball_v0[b]);
+    float w0 = m.ball_w0[b];
+    x[n + b] = v0.f2();
+    x[n + nb + b] = make_float2(w0, 0.0f);
+    bvec[n + b] = (m.b_m * v0).f2();
+    bvec[n + nb + b] = make_float2(m.b_I * w0, 0.0f);
+    float dl = m.b_m, da = m.b_I;
+    for (uint32_t g = m.g_off[b]; g < m.g_off[b + 1]; ++g) {
+      dl += dt * mass * m.g_c[g];
+      da += dt * mass * m.g_l2[g];
+    }
+    for (uint32_t q = m.lo_start[b]; q < m.lo_start[b + 1]; ++q) dl += dt * m.l_c[m.lo_list[q]];
+    for (uint32_t l = m.l_off[b]; l < m.l_off[b + 1]; ++l) dl += dt * m.l_c[l];
+    diag[n + b] = dl;
+    diag[n + nb + b] = da;
+  }
 }
 
 // ---------------------------------------------------------------- per-ball loops of the stages
@@ -1462,36 +1515,9 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       block_bucket_sort(m.rec_b, S.n_links, nb + 1, m.lo_start, m.bk_start, m.lo_list);
       float2 *x = m.cg_x, *bvec = m.cg_b, *r = m.cg_r, *z = m.cg_z, *p = m.cg_p, *ap = m.cg_ap;
       float *diag = m.cg_diag, *inv = m.cg_inv;
-      const bool use_guess = *m.guess_valid_dev != 0;
-      for (uint32_t i = tid(); i < n; i += nthr()) {
-        V2 v(V[i]);
-        x[i] = (use_guess ? v + V2(m.fguess[i]) : v).f2();
-        bvec[i] = (mass * v).f2();
-        float sw = 0.0f;
-        for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) sw += m.visc_w[k];
-        float d = mass * (1.0f + dt * (0.5f * CENTRAL_VISC * sw));
-        for (uint32_t q = m.fg_start[i]; q < m.fg_start[i + 1]; ++q) d += dt * mass * m.g_c[m.fg_list[q]];
-        diag[i] = d;
-        m.dv_tmp[i] = V[i];  // v_in for the warm start of the next sub-step
-      }
-      for (uint32_t b = tid(); b < nb; b += nthr()) {
-        V2 v0(m.ball_v0[b]);
-        float w0 = m.ball_w0[b];
-        x[n + b] = v0.f2();
-        x[n + nb + b] = make_float2(w0, 0.0f);
-        bvec[n + b] = (m.b_m * v0).f2();
-        bvec[n + nb + b] = make_float2(m.b_I * w0, 0.0f);
-        float dl = m.b_m, da = m.b_I;
-        for (uint32_t g = m.g_off[b]; g < m.g_off[b + 1]; ++g) {
-          dl += dt * mass * m.g_c[g];
-          da += dt * mass * m.g_l2[g];
-        }
-        for (uint32_t q = m.lo_start[b]; q < m.lo_start[b + 1]; ++q) dl += dt * m.l_c[m.lo_list[q]];
-        for (uint32_t l = m.l_off[b]; l < m.l_off[b + 1]; ++l) dl += dt * m.l_c[l];
-        diag[n + b] = dl;
-        diag[n + nb + b] = da;
-      }
-      __syncthreads();
+      wide_phase(m, WIDE_CG_SETUP, nullptr, [&](uint32_t w0, uint32_t nw) {
+        cg_setup_rows(m, dt, w0 * 32u + (tid() & 31u), nw * 32u);
+      });
       for (uint32_t e = tid(); e < len; e += nthr()) inv[e] = 1.0f / fmax_r(diag[e], 1e-20f);
       __syncthreads();
       joint_apply(m, dt, x, ap);

@@ -20,7 +20,9 @@ enum : uint32_t {
   WIDE_GROUPS = 2,
   WIDE_LINKS = 3,
   WIDE_DRAG_ITEMS = 4,
-  WIDE_BUOYANCY_ITEMS = 5
+  WIDE_BUOYANCY_ITEMS = 5,
+  WIDE_CG_SETUP = 6,
+  WIDE_JOINT_APPLY = 7
 };
 
 constexpr long long WIDE_TIMEOUT_CYCLES = 20000000000LL;  // ~10 s at 2 GHz
@@ -40,7 +42,8 @@ __device__ inline bool wide_wait(const uint32_t* p, uint32_t target) {
 // Mill block: one phase over all of the mill's warps. share(w0, nw) is called by every thread of
 // the block with w0 = the thread's warp and nw = the warps of all of the mill's blocks.
 template <class F>
-__device__ void wide_phase(const MillDev& m, uint32_t phase, const GridHdr* hdr, F share) {
+__device__ void wide_phase(const MillDev& m, uint32_t phase, const GridHdr* hdr, const float2* vin, float2* vout,
+                           F share) {
   const uint32_t warp = tid() >> 5, nwarps = nthr() >> 5;
   if (m.helpers == 0) {
     share(warp, nwarps);
@@ -51,6 +54,8 @@ __device__ void wide_phase(const MillDev& m, uint32_t phase, const GridHdr* hdr,
   WideCtl* c = m.wide;
   if (tid() == 0) {
     if (hdr) c->hdr = *hdr;
+    c->vin = vin;
+    c->vout = vout;
     c->phase = phase;
     c->counter = 0;
     g_wide_seq += 1;
@@ -64,6 +69,11 @@ __device__ void wide_phase(const MillDev& m, uint32_t phase, const GridHdr* hdr,
     __threadfence();
   }
   __syncthreads();
+}
+
+template <class F>
+__device__ void wide_phase(const MillDev& m, uint32_t phase, const GridHdr* hdr, F share) {
+  wide_phase(m, phase, hdr, nullptr, nullptr, share);
 }
 
 // Mill block: the helper blocks' count of the last phase (call after wide_phase).
@@ -84,12 +94,14 @@ __device__ inline void wide_exit(const MillDev& m) {
   }
 }
 
-// Helper block: runs its share of every published phase until WIDE_EXIT. run(phase, hdr, w0, nw)
-// returns the thread's part of the phase's count.
+// Helper block: runs its share of every published phase until WIDE_EXIT. run(phase, hdr, vin,
+// vout, w0, nw) returns the thread's part of the phase's count.
 template <class Run>
 __device__ void wide_helper(const MillDev& m, Run run) {
   __shared__ uint32_t ph;
   __shared__ GridHdr hdr;
+  __shared__ const float2* vin;
+  __shared__ float2* vout;
   WideCtl* c = m.wide;
   const uint32_t nwarps = nthr() >> 5;
   const uint32_t w0 = blockIdx.x * nwarps + (tid() >> 5), nw = (1u + m.helpers) * nwarps;
@@ -102,12 +114,14 @@ __device__ void wide_helper(const MillDev& m, Run run) {
         __threadfence();
         ph = *reinterpret_cast<const volatile uint32_t*>(&c->phase);
         hdr = c->hdr;
+        vin = c->vin;
+        vout = c->vout;
       }
     }
     __syncthreads();
     const uint32_t p = ph;
     if (p == WIDE_EXIT) return;
-    const uint32_t part = block_sum_u(run(p, hdr, w0, nw));
+    const uint32_t part = block_sum_u(run(p, hdr, vin, vout, w0, nw));
     if (tid() == 0) {
       if (part) atomicAdd(&c->counter, part);
       __threadfence();
