@@ -285,6 +285,7 @@ struct MillDev {
   float2 *cg_x, *cg_b, *cg_r, *cg_z, *cg_p, *cg_ap, *cg_lv;
   float *cg_diag, *cg_inv;
   float2* ball_v0;
+  float* drag_pre;  // per ball: the drag sweep's geometry-only quantities (8 floats)
   float* ball_w0;
   // dem workspace
   float2 *bx0, *bvpre;

@@ -54,14 +54,7 @@ __device__ double block_dot(const float2* a, const float2* b, uint32_t len, bool
       acc += (double)a[e].x * (double)b[e].x + (double)a[e].y * (double)b[e].y;
     return block_sum_d(acc);
   }
-  if (tid() < 32) {
-    float s = warp_ordered_sum(0.0f, len, [&](uint32_t e, float& t) { t = V2(a[e]).dot(V2(b[e])); return true; });
-    if (tid() == 0) S.fscal[7] = s;
-  }
-  __syncthreads();
-  double r = (double)S.fscal[7];
-  __syncthreads();
-  return r;
+  return (double)block_seq_sum_f32(0.0f, len, [&](uint32_t e) { return V2(a[e]).dot(V2(b[e])); });
 }
 
 // pbf.rs:738-744 residual norm sqrt(sum inv_diag |r|^2), sequential f32 or f64.
@@ -72,14 +65,7 @@ __device__ double block_res_norm(const float2* r, const float* inv, uint32_t len
       acc += (double)inv[e] * ((double)r[e].x * (double)r[e].x + (double)r[e].y * (double)r[e].y);
     return sqrt(block_sum_d(acc));
   }
-  if (tid() < 32) {
-    float s = warp_ordered_sum(0.0f, len, [&](uint32_t e, float& t) { t = inv[e] * V2(r[e]).len2(); return true; });
-    if (tid() == 0) S.fscal[6] = sqrtf(s);
-  }
-  __syncthreads();
-  double v = (double)S.fscal[6];
-  __syncthreads();
-  return v;
+  return (double)sqrtf(block_seq_sum_f32(0.0f, len, [&](uint32_t e) { return inv[e] * V2(r[e]).len2(); }));
 }
 
 // pbf.rs:359-377 laplacian row i.
@@ -600,6 +586,77 @@ __device__ uint32_t buoyancy_item_balls(const MillDev& m, const GridHdr& hA, uin
   return items;
 }
 
+// The drag sweep's per-ball quantities that read only the item geometry (pbf.rs:1845-1905), for
+// the balls w0, w0 + nw, ...: entrained mass and inertia, centroid and the s-gate sums, summed in
+// item order; written to drag_pre[8 b ..] (mass, inertia, centroid x, y, s_acc, s_scale).
+__device__ void drag_pre_balls(const MillDev& m, uint32_t w0, uint32_t nw) {
+  const uint32_t nb = m.nb, lane = tid() & 31u;
+  const float mass = m.f_mass;
+  for (uint32_t b = w0; b < nb; b += nw) {
+    const uint32_t cnt = m.item_n[b], base = b * m.cap_items;
+    float m_ent = 0.0f, i_ent = 0.0f, rsx = 0.0f, rsy = 0.0f;
+    for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+      const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
+      float w = 0.0f, r2w = 0.0f;
+      V2 rw;
+      if (s < cnt) {
+        V2 r_i(m.item_v[base + s]);
+        w = mass * m.item_w[base + s];
+        rw = w * r_i;
+        r2w = w * r_i.len2();
+      }
+#pragma unroll
+      for (uint32_t t = 0; t < 32; ++t) {
+        const float wt = __shfl_sync(FULL, w, t), xt = __shfl_sync(FULL, rw.x, t);
+        const float yt = __shfl_sync(FULL, rw.y, t), it = __shfl_sync(FULL, r2w, t);
+        if (t < lim) {
+          m_ent += wt;
+          rsx += xt;
+          rsy += yt;
+          i_ent += it;
+        }
+      }
+    }
+    V2 r_bar;
+    float s_acc = 0.0f, s_scale = 0.0f;
+    if (cnt > 0 && !(m_ent <= 1e-12f)) {
+      r_bar = V2(rsx, rsy) / m_ent;
+      if (i_ent > 1e-12f) {
+        const V2 p_bar(-r_bar.y, r_bar.x);
+        for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+          const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
+          float sv = 0.0f, ss = 0.0f;
+          if (s < cnt) {
+            V2 r_i(m.item_v[base + s]);
+            float phi = m.item_w[base + s];
+            V2 perp_i(-r_i.y, r_i.x);
+            float phi2 = phi * phi;
+            sv = mass * phi2 * cross2(r_i, perp_i - p_bar);
+            ss = mass * phi2 * r_i.len2();
+          }
+#pragma unroll
+          for (uint32_t t = 0; t < 32; ++t) {
+            const float at = __shfl_sync(FULL, sv, t), st = __shfl_sync(FULL, ss, t);
+            if (t < lim) {
+              s_acc += at;
+              s_scale += st;
+            }
+          }
+        }
+      }
+    }
+    if (lane == 0) {
+      float* P = m.drag_pre + 8u * b;
+      P[0] = m_ent;
+      P[1] = i_ent;
+      P[2] = r_bar.x;
+      P[3] = r_bar.y;
+      P[4] = s_acc;
+      P[5] = s_scale;
+    }
+  }
+}
+
 __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err, FluidShared& S,
                            unsigned char* dsm) {
   uint32_t* done = m.ball_done;  // completion flags of the per-ball sweeps (moved to shared below)
@@ -1010,6 +1067,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       const uint32_t nrec = pack_ball_items(m.item_j, m.item_n, m.cap_items, nb, m.rec_off, m.rec_i, m.rec_b);
       ball_item_preds(m.rec_i, m.rec_b, nrec, n, m.bk_start, m.bk_cur, m.bk_order, m.rec_pred);
       stage_mark(out.stage, 25);
+      wide_phase(m, WIDE_DRAG_PRE, nullptr, [&](uint32_t w0, uint32_t nw) { drag_pre_balls(m, w0, nw); });
       const float i_b = m.b_I;
       const bool want_mom = U.want_momentum != 0;
       // Lane l holds item l of the ball (items from 32 on are read from the lists when needed).
@@ -1028,8 +1086,8 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
       auto item_j = [&](const DragBall& q, uint32_t base, uint32_t s) { return s < 32 ? q.j : m.item_j[base + s]; };
       ball_dataflow(
           nb, m.rec_off, m.rec_pred, done, U.sweep_warps, U.spin_ns, err, &out.stage[32],
-          // before the wait: entrained mass, centroid, inertia and the s-gate sums (pbf.rs:1845-1905)
-          // read only the item geometry, which the sweep does not change
+          // before the wait: the item data and the geometry-only quantities computed for every ball
+          // ahead of the sweep (drag_pre_balls)
           [&](uint32_t b, int lane) {
             DragBall q;
             q.cnt = m.item_n[b];
@@ -1045,62 +1103,15 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
             }
             q.vb = V2(m.bv[b]);
             q.omb = m.bom[b];
-            float m_ent = 0.0f, i_ent = 0.0f, rsx = 0.0f, rsy = 0.0f;
-            for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
-              const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
-              float w = 0.0f, r2w = 0.0f;
-              V2 rw;
-              if (s < cnt) {
-                V2 r_i = item_r(q, base, s);
-                w = mass * item_phi(q, base, s);
-                rw = w * r_i;
-                r2w = w * r_i.len2();
-              }
-#pragma unroll
-              for (uint32_t t = 0; t < 32; ++t) {
-                const float wt = __shfl_sync(FULL, w, t), xt = __shfl_sync(FULL, rw.x, t);
-                const float yt = __shfl_sync(FULL, rw.y, t), it = __shfl_sync(FULL, r2w, t);
-                if (t < lim) {
-                  m_ent += wt;
-                  rsx += xt;
-                  rsy += yt;
-                  i_ent += it;
-                }
-              }
-            }
-            q.m_ent = m_ent;
-            q.i_ent = i_ent;
-            if (m_ent <= 1e-12f) return q;
+            const float* P = m.drag_pre + 8u * b;
+            q.m_ent = P[0];
+            q.i_ent = P[1];
+            if (q.m_ent <= 1e-12f) return q;
             q.live = true;
-            q.r_bar = V2(rsx, rsy) / m_ent;
-            q.s_acc = 0.0f;
-            q.s_scale = 0.0f;
-            if (i_ent > 1e-12f) {
-              q.p_bar = V2(-q.r_bar.y, q.r_bar.x);
-              float s_acc = 0.0f, s_scale = 0.0f;
-              for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
-                const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
-                float sv = 0.0f, ss = 0.0f;
-                if (s < cnt) {
-                  V2 r_i = item_r(q, base, s);
-                  float phi = item_phi(q, base, s);
-                  V2 perp_i(-r_i.y, r_i.x);
-                  float phi2 = phi * phi;
-                  sv = mass * phi2 * cross2(r_i, perp_i - q.p_bar);
-                  ss = mass * phi2 * r_i.len2();
-                }
-#pragma unroll
-                for (uint32_t t = 0; t < 32; ++t) {
-                  const float at = __shfl_sync(FULL, sv, t), st = __shfl_sync(FULL, ss, t);
-                  if (t < lim) {
-                    s_acc += at;
-                    s_scale += st;
-                  }
-                }
-              }
-              q.s_acc = s_acc;
-              q.s_scale = s_scale;
-            }
+            q.r_bar = V2(P[2], P[3]);
+            q.s_acc = P[4];
+            q.s_scale = P[5];
+            if (q.i_ent > 1e-12f) q.p_bar = V2(-q.r_bar.y, q.r_bar.x);
             return q;
           },
           // on the chain: entrained velocity and angular momentum, the relaxation, the fluid updates
@@ -1119,16 +1130,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
                 vw = w * vj;
                 lw = w * cross2(r_i, vj);
               }
-#pragma unroll
-              for (uint32_t t = 0; t < 32; ++t) {
-                const float xt = __shfl_sync(FULL, vw.x, t), yt = __shfl_sync(FULL, vw.y, t);
-                const float lt = __shfl_sync(FULL, lw, t);
-                if (t < lim) {
-                  vsx += xt;
-                  vsy += yt;
-                  l_sum += lt;
-                }
-              }
+              lane_seq_sum3(vsx, vsy, l_sum, vw.x, vw.y, lw, lim);
             }
             const float m_ent = q.m_ent, i_ent = q.i_ent;
             V2 v_bar = V2(vsx, vsy) / m_ent;
@@ -1615,14 +1617,11 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
     m.f_tmp[i] = sqrtf(2.0f * (gxx * gxx + gyy * gyy + 2.0f * dxy * dxy));
   }
   __syncthreads();
-  if (tid() < 32) {
+  {
+    const float s = block_seq_sum_f32<true>(0.0f, n, [&](uint32_t i) { return m.f_tmp[i]; });
     uint32_t c = 0;
-    float s = warp_ordered_sum(0.0f, n, [&](uint32_t i, float& t) {
-      t = m.f_tmp[i];
-      return finite_f(t);
-    });
-    for (uint32_t i = tid(); i < n; i += 32) c += finite_f(m.f_tmp[i]) ? 1u : 0u;
-    c = warp_sum(c);
+    for (uint32_t i = tid(); i < n; i += nthr()) c += finite_f(m.f_tmp[i]) ? 1u : 0u;
+    c = block_sum_u(c);
     if (tid() == 0) out.fs.mean_shear_rate_per_s = c == 0 ? 0.0f : s / (float)c;
   }
   __syncthreads();

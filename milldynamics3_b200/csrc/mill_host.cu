@@ -261,6 +261,7 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
     m.cg_z = a.take<float2>(len); m.cg_p = a.take<float2>(len); m.cg_ap = a.take<float2>(len);
     m.cg_lv = a.take<float2>(cf); m.cg_diag = a.take<float>(len); m.cg_inv = a.take<float>(len);
     m.ball_v0 = a.take<float2>(cb); m.ball_w0 = a.take<float>(cb);
+    m.drag_pre = a.take<float>((size_t)8 * cb);
     m.bx0 = a.take<float2>(cb); m.bvpre = a.take<float2>(cb);
     m.bth0 = a.take<float>(cb); m.bompre = a.take<float>(cb); m.lam_bw = a.take<float>(cb);
     m.bxs = a.take<float2>(cb); m.bmove = a.take<float>(cb); m.f_cw = a.take<double>(cb);

@@ -45,6 +45,7 @@ __global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDe
       else if (phase == WIDE_BUOYANCY_ITEMS) return buoyancy_item_balls(m, hdr, w0, nw);
       else if (phase == WIDE_CG_SETUP) cg_setup_rows(m, U.dt, t0, stride);
       else if (phase == WIDE_JOINT_APPLY) joint_apply_rows(m, U.dt, vin, vout, t0, stride);
+      else if (phase == WIDE_DRAG_PRE) drag_pre_balls(m, w0, nw);
       return 0u;
     });
     return;
@@ -114,7 +115,8 @@ cudaError_t launch_substeps(const MillDev* mills, uint32_t n_mills, StepUniform*
                             cudaStream_t stream, uint32_t mill_blocks) {
   if (threads == 0 || threads > MAX_BLOCK_THREADS) threads = DEFAULT_BLOCK_THREADS;
   auto kernel = threads > 512 ? mill_substeps_kernel<MAX_BLOCK_THREADS> : mill_substeps_kernel<512>;
-  if (smem_bytes > 48 * 1024) {
+  // (the opt-in is needed whenever static plus dynamic shared memory passes 48 KB)
+  if (smem_bytes > 0) {
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
     if (e != cudaSuccess) return e;
   }

@@ -235,6 +235,72 @@ __device__ void ball_dataflow(uint32_t nb, const uint32_t* rec_off, const uint32
   __syncthreads();
 }
 
+// Three in-order sums over the lanes' values t = 0..lim-1, added to a, b, c (the same on every
+// lane): the lanes store their values to the warp's shared scratch and lane 0 adds them in lane
+// order (independent loads, three interleaved chains of additions), then broadcasts the sums.
+__shared__ float g_seq_buf[MAX_BLOCK_WARPS][3][32];
+__device__ __forceinline__ void lane_seq_sum3(float& a, float& b, float& c, float va, float vb, float vc,
+                                              uint32_t lim) {
+  const uint32_t lane = threadIdx.x & 31u;
+  float(*B)[32] = g_seq_buf[threadIdx.x >> 5];
+  B[0][lane] = va;
+  B[1][lane] = vb;
+  B[2][lane] = vc;
+  __syncwarp();
+  if (lane == 0) {
+    for (uint32_t t = 0; t < lim; ++t) {
+      a += B[0][t];
+      b += B[1][t];
+      c += B[2][t];
+    }
+  }
+  __syncwarp();
+  a = __shfl_sync(FULL, a, 0);
+  b = __shfl_sync(FULL, b, 0);
+  c = __shfl_sync(FULL, c, 0);
+}
+
+// Block-wide in-order f32 sum init + term(0) + term(1) + ... + term(n-1), every term added (the
+// reference's sequential f32 accumulations): all threads evaluate a chunk of terms into shared
+// memory (the warps' scratch above, free outside the per-ball sweeps), then thread 0 adds them in
+// order with the loads running ahead of the additions. All threads call it; all get the result.
+// With SKIP_NONFINITE, non-finite terms are left out (not added).
+template <bool SKIP_NONFINITE = false, class Term>
+__device__ float block_seq_sum_f32(float init, uint32_t n, Term term) {
+  constexpr uint32_t CHUNK = MAX_BLOCK_WARPS * 3 * 32;
+  float* buf = &g_seq_buf[0][0][0];
+  __shared__ float res;
+  float acc = init;
+  for (uint32_t c0 = 0; c0 < n; c0 += CHUNK) {
+    const uint32_t cnt = min(CHUNK, n - c0);
+    for (uint32_t k = tid(); k < cnt; k += nthr()) buf[k] = term(c0 + k);
+    __syncthreads();
+    if (tid() == 0) {
+      uint32_t k = 0;
+      for (; k + 8 <= cnt; k += 8) {
+        const float x0 = buf[k], x1 = buf[k + 1], x2 = buf[k + 2], x3 = buf[k + 3];
+        const float x4 = buf[k + 4], x5 = buf[k + 5], x6 = buf[k + 6], x7 = buf[k + 7];
+        if (!SKIP_NONFINITE || finite_f(x0)) acc += x0;
+        if (!SKIP_NONFINITE || finite_f(x1)) acc += x1;
+        if (!SKIP_NONFINITE || finite_f(x2)) acc += x2;
+        if (!SKIP_NONFINITE || finite_f(x3)) acc += x3;
+        if (!SKIP_NONFINITE || finite_f(x4)) acc += x4;
+        if (!SKIP_NONFINITE || finite_f(x5)) acc += x5;
+        if (!SKIP_NONFINITE || finite_f(x6)) acc += x6;
+        if (!SKIP_NONFINITE || finite_f(x7)) acc += x7;
+      }
+      for (; k < cnt; ++k)
+        if (!SKIP_NONFINITE || finite_f(buf[k])) acc += buf[k];
+    }
+    __syncthreads();
+  }
+  if (tid() == 0) res = acc;
+  __syncthreads();
+  const float r = res;
+  __syncthreads();
+  return r;
+}
+
 // In-order sum over the lanes' values t = 0..lim-1 (every lane computes the same chain).
 __device__ __forceinline__ float lane_seq_sum(float acc, float v, uint32_t lim) {
 #pragma unroll

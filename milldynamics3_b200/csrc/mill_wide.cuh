@@ -22,7 +22,8 @@ enum : uint32_t {
   WIDE_DRAG_ITEMS = 4,
   WIDE_BUOYANCY_ITEMS = 5,
   WIDE_CG_SETUP = 6,
-  WIDE_JOINT_APPLY = 7
+  WIDE_JOINT_APPLY = 7,
+  WIDE_DRAG_PRE = 8
 };
 
 constexpr long long WIDE_TIMEOUT_CYCLES = 20000000000LL;  // ~10 s at 2 GHz
