@@ -320,7 +320,6 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
   // out keep lambda 0, walls accumulated in lam_bw in place)
   for (uint32_t q = tid(); q < nrun; q += nthr()) m.lam_bb[m.pr_list[m.lev_items[q]]] = dl[q];
   __syncthreads();
-  const uint32_t nitems = np + n;
   stage_mark(out.stage, 16);
   // step 4 velocity reconstruction (dem.rs:753-756)
   for (uint32_t i = tid(); i < n; i += nthr()) {
@@ -328,41 +327,49 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
     OM[i] = angle_diff(TH[i], m.bth0[i], err) / dt;
   }
   __syncthreads();
-  // contacts sorted by (i, j) (dem.rs:459-467): bucket by i (stable), then by j inside a bucket
-  block_bucket_sort(m.pair_i, np, n, m.bk_start, m.bk_cur, m.bk_order);
+  // The contact sweeps visit only contacts with lambda_n > 0: pairs sorted by (i, j)
+  // (dem.rs:459-467), then walls in ball order. The active pairs are compacted (ascending pair
+  // index), bucketed by i (stable) and sorted by j inside a bucket (pairs are distinct, so j
+  // decides): the order of sorting every pair and keeping the active ones.
+  for (uint32_t k = tid(); k < np; k += nthr()) m.act_flag[k] = m.lam_bb[k] > 0.0f ? 1u : 0u;
+  if (tid() == 0) m.act_flag[np] = 0;
+  __syncthreads();
+  const uint32_t na_p = block_exclusive_scan(m.act_flag, np + 1);  // active pair contacts
+  for (uint32_t k = tid(); k < np; k += nthr()) {
+    const uint32_t o = m.act_flag[k];
+    if (m.act_flag[k + 1] != o) {
+      m.pr_list[o] = k;
+      m.dm_lvl[o] = m.pair_i[k];
+    }
+  }
+  __syncthreads();
+  block_bucket_sort(m.dm_lvl, na_p, n, m.bk_start, m.bk_cur, m.bk_order);
   for (uint32_t b = tid(); b < n; b += nthr()) {
-    uint32_t s = m.bk_start[b], e = m.bk_start[b + 1];
+    const uint32_t s = m.bk_start[b], e = m.bk_start[b + 1];
     for (uint32_t a = s + 1; a < e; ++a) {
-      uint32_t v = m.bk_order[a];
-      uint32_t vj = m.pair_j[v];
+      const uint32_t v = m.bk_order[a], vj = m.pair_j[m.pr_list[v]];
       uint32_t q = a;
-      while (q > s && m.pair_j[m.bk_order[q - 1]] > vj) { m.bk_order[q] = m.bk_order[q - 1]; --q; }
+      while (q > s && m.pair_j[m.pr_list[m.bk_order[q - 1]]] > vj) { m.bk_order[q] = m.bk_order[q - 1]; --q; }
       m.bk_order[q] = v;
     }
   }
   __syncthreads();
-  // the contact sweeps visit only contacts with lambda_n > 0: sorted pairs, then walls
-  for (uint32_t q = tid(); q < nitems; q += nthr()) {
-    float l = q < np ? m.lam_bb[m.bk_order[q]] : m.lam_bw[q - np];
-    m.act_flag[q] = l > 0.0f ? 1u : 0u;
+  for (uint32_t q = tid(); q < na_p; q += nthr()) {
+    const uint32_t k = m.pr_list[m.bk_order[q]];
+    m.act_i[q] = m.pair_i[k];
+    m.act_j[q] = m.pair_j[k];
+    m.act_l[q] = m.lam_bb[k];
   }
-  if (tid() == 0) m.act_flag[nitems] = 0;
+  for (uint32_t b = tid(); b < n; b += nthr()) m.act_flag[b] = m.lam_bw[b] > 0.0f ? 1u : 0u;
+  if (tid() == 0) m.act_flag[n] = 0;
   __syncthreads();
-  const uint32_t na = block_exclusive_scan(m.act_flag, nitems + 1);
-  const uint32_t na_p = m.act_flag[np];  // active pair contacts; the active walls follow them
-  for (uint32_t q = tid(); q < nitems; q += nthr()) {
-    uint32_t o = m.act_flag[q];
-    if (m.act_flag[q + 1] == o) continue;
-    if (q < np) {
-      uint32_t k = m.bk_order[q];
-      m.act_i[o] = m.pair_i[k];
-      m.act_j[o] = m.pair_j[k];
-      m.act_l[o] = m.lam_bb[k];
-    } else {
-      m.act_i[o] = q - np;
-      m.act_j[o] = NONE;
-      m.act_l[o] = m.lam_bw[q - np];
-    }
+  const uint32_t na = na_p + block_exclusive_scan(m.act_flag, n + 1);  // then the active walls
+  for (uint32_t b = tid(); b < n; b += nthr()) {
+    const uint32_t o = na_p + m.act_flag[b];
+    if (na_p + m.act_flag[b + 1] == o) continue;
+    m.act_i[o] = b;
+    m.act_j[o] = NONE;
+    m.act_l[o] = m.lam_bw[b];
   }
   __syncthreads();
   for (uint32_t k = tid(); k < na; k += nthr()) { m.dm_pa[k] = NONE; m.dm_pb[k] = NONE; }

@@ -920,6 +920,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
         if (bin >= 0) { val = m.wall_val[c + lane]; px = m.dv_tmp[c + lane].x; py = m.dv_tmp[c + lane].y; pa = m.f_tmp[c + lane]; }
       }
       const uint32_t mask = __ballot_sync(FULL, bin >= 0);
+      if (mask == 0u) continue;  // no particle of the chunk touched the wall
       if (exact) {
 #pragma unroll
         for (int t = 0; t < 32; ++t) {
@@ -995,6 +996,7 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
           ja = cross2(x, mass * dv);
         }
         const uint32_t mask = __ballot_sync(FULL, touched);
+        if (mask == 0u) continue;
         if (exact) {
 #pragma unroll
           for (int t = 0; t < 32; ++t) {
