@@ -239,15 +239,24 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
     }
     __syncthreads();
     stage_mark(out.stage, 22);
+    // the item body takes its constants and pointers by value, so that they stay in registers
+    float2* const Xp = X;
+    float* const dlp = dl;
+    const float2* const bxs = m.bxs;
+    float* const bmv = m.bmove;
+    const uint32_t* const dip = di;
+    const uint32_t* const djp = dj;
     for (uint32_t it = 0; it < iters; ++it) {
-      run_levels(nlev, m.lev_start, [&](uint32_t q) { return make_uint2(di[q], dj[q]); },
-                 [&](uint32_t q, uint2 d) {
+      run_levels(nlev, m.lev_start, [dip, djp](uint32_t q) { return make_uint2(dip[q], djp[q]); },
+                 [Xp, dlp, bxs, bmv, track, r, w, cap_depth, excursion](uint32_t q, uint2 d) {
+        float2* const X = Xp;
+        float* const dl = dlp;
         const uint32_t i = d.x, j = d.y;
         V2 xi(X[i]), xj(X[j]);
         // start positions and excursions so far, loaded beside the positions
         V2 si, sj;
         float ei = 0.0f, ej = 0.0f;
-        if (track) { si = V2(m.bxs[i]); sj = V2(m.bxs[j]); ei = m.bmove[i]; ej = m.bmove[j]; }
+        if (track) { si = V2(bxs[i]); sj = V2(bxs[j]); ei = bmv[i]; ej = bmv[j]; }
         V2 delta = xi - xj;
         float dist = delta.len();
         float c = dist - 2.0f * r;
@@ -262,8 +271,8 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
         X[j] = xjn.f2();
         dl[q] += d_lambda;
         if (track) {
-          m.bmove[i] = excursion(ei, V2(xin.f2()) - si);
-          m.bmove[j] = excursion(ej, V2(xjn.f2()) - sj);
+          bmv[i] = excursion(ei, V2(xin.f2()) - si);
+          bmv[j] = excursion(ej, V2(xjn.f2()) - sj);
         }
       });
       for (uint32_t i = tid(); i < n; i += nthr()) {
@@ -402,50 +411,57 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
     __syncthreads();
   };
   contact_sweep([&](uint32_t k, uint3 d) {
+    // this body's constants and pointers as locals (they stay in registers)
+    float2* const X_l = X;
+    float2* const V_l = V;
+    float* const TH_l = TH;
+    float* const OM_l = OM;
+    const float w_l = w, w_rot_l = w_rot, r_l = r, dt_l = dt;
+    const MgMediaParams md_l = md;
     const uint32_t i = d.x, j = d.y;
     const float lambda_n = __uint_as_float(d.z);
     if (j != NONE) {
-      V2 delta = V2(X[i]) - V2(X[j]);
+      V2 delta = V2(X_l[i]) - V2(X_l[j]);
       float dist = delta.len();
       V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
       V2 t_hat(-n_hat.y, n_hat.x);
-      float v_t = (V2(V[i]) - V2(V[j])).dot(t_hat) - r * OM[i] - r * OM[j];
-      float w_sum_t = w + w + r * r * w_rot + r * r * w_rot;
+      float v_t = (V2(V_l[i]) - V2(V_l[j])).dot(t_hat) - r_l * OM_l[i] - r_l * OM_l[j];
+      float w_sum_t = w_l + w_l + r_l * r_l * w_rot_l + r_l * r_l * w_rot_l;
       if (w_sum_t <= 0.0f) return;
-      float raw = -v_t * dt / w_sum_t;
-      float mu = effective_friction(md.friction_ball_ball, md.friction_ball_ball_static, v_t, md.friction_velocity_scale_m_s);
+      float raw = -v_t * dt_l / w_sum_t;
+      float mu = effective_friction(md_l.friction_ball_ball, md_l.friction_ball_ball_static, v_t, md_l.friction_velocity_scale_m_s);
       float max_mag = mu * lambda_n;
       float dlt = clamp_r(raw, -max_mag, max_mag);
-      X[i] = (V2(X[i]) + w * dlt * t_hat).f2();
-      X[j] = (V2(X[j]) - w * dlt * t_hat).f2();
-      TH[i] -= r * w_rot * dlt;
-      TH[j] -= r * w_rot * dlt;
-      V2 dv = w * dlt * t_hat / dt;
-      float domega = -r * w_rot * dlt / dt;
-      V[i] = (V2(V[i]) + dv).f2();
-      V[j] = (V2(V[j]) - dv).f2();
-      OM[i] += domega;
-      OM[j] += domega;
+      X_l[i] = (V2(X_l[i]) + w_l * dlt * t_hat).f2();
+      X_l[j] = (V2(X_l[j]) - w_l * dlt * t_hat).f2();
+      TH_l[i] -= r_l * w_rot_l * dlt;
+      TH_l[j] -= r_l * w_rot_l * dlt;
+      V2 dv = w_l * dlt * t_hat / dt_l;
+      float domega = -r_l * w_rot_l * dlt / dt_l;
+      V_l[i] = (V2(V_l[i]) + dv).f2();
+      V_l[j] = (V2(V_l[j]) - dv).f2();
+      OM_l[i] += domega;
+      OM_l[j] += domega;
     } else {
       m.act_bin[k] = -2;  // no work terms unless the contact completes below
       float dd;
       V2 n_hat;
-      drum_sdf_world(U, V2(X[i]), U.to_local_next, U.to_world_next, dd, n_hat);
+      drum_sdf_world(U, V2(X_l[i]), U.to_local_next, U.to_world_next, dd, n_hat);
       V2 t_hat(-n_hat.y, n_hat.x);
-      V2 v_wall = wall_velocity(U.drum_omega, V2(X[i]) - r * n_hat);
-      float v_t = (V2(V[i]) - v_wall).dot(t_hat) - r * OM[i];
-      float w_sum_t = w + r * r * w_rot;
+      V2 v_wall = wall_velocity(U.drum_omega, V2(X_l[i]) - r_l * n_hat);
+      float v_t = (V2(V_l[i]) - v_wall).dot(t_hat) - r_l * OM_l[i];
+      float w_sum_t = w_l + r_l * r_l * w_rot_l;
       if (w_sum_t <= 0.0f) return;
-      float raw = -v_t * dt / w_sum_t;
-      float mu = effective_friction(md.friction_ball_wall, md.friction_ball_wall_static, v_t, md.friction_velocity_scale_m_s);
+      float raw = -v_t * dt_l / w_sum_t;
+      float mu = effective_friction(md_l.friction_ball_wall, md_l.friction_ball_wall_static, v_t, md_l.friction_velocity_scale_m_s);
       float max_mag = mu * lambda_n;
       float dlt = clamp_r(raw, -max_mag, max_mag);
-      X[i] = (V2(X[i]) + w * dlt * t_hat).f2();
-      TH[i] -= r * w_rot * dlt;
-      V[i] = (V2(V[i]) + w * dlt * t_hat / dt).f2();
-      OM[i] += -r * w_rot * dlt / dt;
-      m.act_w1[k] = (dlt / dt) * t_hat.dot(v_wall);
-      m.act_w2[k] = (lambda_n / dt) * n_hat.dot(v_wall);
+      X_l[i] = (V2(X_l[i]) + w_l * dlt * t_hat).f2();
+      TH_l[i] -= r_l * w_rot_l * dlt;
+      V_l[i] = (V2(V_l[i]) + w_l * dlt * t_hat / dt_l).f2();
+      OM_l[i] += -r_l * w_rot_l * dlt / dt_l;
+      m.act_w1[k] = (dlt / dt_l) * t_hat.dot(v_wall);
+      m.act_w2[k] = (lambda_n / dt_l) * n_hat.dot(v_wall);
       m.act_bin[k] = 0;
     }
   });
@@ -488,10 +504,15 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
   // step 6 restitution with impact accounting (dem.rs:909-1019); per-item records are compacted
   // in sweep order afterwards
   contact_sweep([&](uint32_t k, uint3 d) {
+    // this body's constants and pointers as locals (they stay in registers)
+    float2* const X_l = X;
+    float2* const V_l = V;
+    const float w_l = w, r_l = r, impact_threshold_l = impact_threshold;
+    const MgMediaParams md_l = md;
     const uint32_t i = d.x, j = d.y;
     m.act_flag[k] = 0;
     if (j != NONE) {
-      V2 delta = V2(X[i]) - V2(X[j]);
+      V2 delta = V2(X_l[i]) - V2(X_l[j]);
       float dist = delta.len();
       V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
       float v_n_pre = (V2(m.bvpre[i]) - V2(m.bvpre[j])).dot(n_hat);
@@ -501,26 +522,26 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
         int bin = impact_energy_bin(0.5f * (m.b_m * 0.5f) * v_n_pre * v_n_pre);
         if (bin >= 0) atomicAdd(&S.hist[bin], 1u);
       }
-      float e = fresh ? md.restitution_ball_ball : 0.0f;
-      if (-v_n_pre > impact_threshold) {
+      float e = fresh ? md_l.restitution_ball_ball : 0.0f;
+      if (-v_n_pre > impact_threshold_l) {
         V2 t_hat(-n_hat.y, n_hat.x);
-        float slip = (V2(m.bvpre[i]) - V2(m.bvpre[j])).dot(t_hat) - r * m.bompre[i] - r * m.bompre[j];
+        float slip = (V2(m.bvpre[i]) - V2(m.bvpre[j])).dot(t_hat) - r_l * m.bompre[i] - r_l * m.bompre[j];
         m.act_rec[k] = MgImpactRecord{MG_IMPACT_BALL_BALL, i, j, -v_n_pre, fabsf(slip), e};
         m.act_flag[k] = 1;
       }
       float target = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
-      float v_n_now = (V2(V[i]) - V2(V[j])).dot(n_hat);
+      float v_n_now = (V2(V_l[i]) - V2(V_l[j])).dot(n_hat);
       float dvn = target - v_n_now;
-      float w_sum = w + w;
+      float w_sum = w_l + w_l;
       if (w_sum <= 0.0f) return;
       float impulse = dvn / w_sum;
-      V[i] = (V2(V[i]) + w * impulse * n_hat).f2();
-      V[j] = (V2(V[j]) - w * impulse * n_hat).f2();
+      V_l[i] = (V2(V_l[i]) + w_l * impulse * n_hat).f2();
+      V_l[j] = (V2(V_l[j]) - w_l * impulse * n_hat).f2();
     } else {
       float dd;
       V2 n_hat;
-      drum_sdf_world(U, V2(X[i]), U.to_local_next, U.to_world_next, dd, n_hat);
-      V2 v_wall = wall_velocity(U.drum_omega, V2(X[i]) - r * n_hat);
+      drum_sdf_world(U, V2(X_l[i]), U.to_local_next, U.to_world_next, dd, n_hat);
+      V2 v_wall = wall_velocity(U.drum_omega, V2(X_l[i]) - r_l * n_hat);
       float v_n_pre = (V2(m.bvpre[i]) - v_wall).dot(n_hat);
       bool fresh = v_n_pre < -RESTITUTION_VELOCITY_THRESHOLD;
       if (fresh) {
@@ -528,18 +549,18 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
         int bin = impact_energy_bin(0.5f * m.b_m * v_n_pre * v_n_pre);
         if (bin >= 0) atomicAdd(&S.hist[bin], 1u);
       }
-      float e = fresh ? md.restitution_ball_wall : 0.0f;
-      if (-v_n_pre > impact_threshold) {
+      float e = fresh ? md_l.restitution_ball_wall : 0.0f;
+      if (-v_n_pre > impact_threshold_l) {
         V2 t_hat(-n_hat.y, n_hat.x);
-        float slip = (V2(m.bvpre[i]) - v_wall).dot(t_hat) - r * m.bompre[i];
+        float slip = (V2(m.bvpre[i]) - v_wall).dot(t_hat) - r_l * m.bompre[i];
         m.act_rec[k] = MgImpactRecord{MG_IMPACT_BALL_WALL, i, MG_WALL_PARTNER, -v_n_pre, fabsf(slip), e};
         m.act_flag[k] = 1;
       }
       float target = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
-      float v_n_now = (V2(V[i]) - v_wall).dot(n_hat);
+      float v_n_now = (V2(V_l[i]) - v_wall).dot(n_hat);
       float dvn = target - v_n_now;
-      if (w <= 0.0f) return;
-      V[i] = (V2(V[i]) + dvn * n_hat).f2();
+      if (w_l <= 0.0f) return;
+      V_l[i] = (V2(V_l[i]) + dvn * n_hat).f2();
     }
   });
   if (tid() == 0) m.act_flag[na] = 0;

@@ -1119,7 +1119,13 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
           // on the chain: entrained velocity and angular momentum, the relaxation, the fluid updates
           [&](uint32_t b, int lane, DragBall& q) {
             if (!q.live) return;
+            // descriptor fields in registers (stores through V would otherwise force reloads)
             const uint32_t base = b * m.cap_items, cnt = q.cnt;
+            const float b_m = m.b_m, b_rtrue = m.b_rtrue;
+            float2* const Vl = V;
+            // the enclosing scope's constants as locals of this body (one load each, up front)
+            const float mass_l = mass, rho0_l = rho0, mass_true_l = mass_true, beta_l = beta_b, dt_l = dt;
+            const float i_b_l = i_b, h_c_l = h_c, rot_cap_l = rot_cap;
             float l_sum = 0.0f, vsx = 0.0f, vsy = 0.0f;
             for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
               const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
@@ -1127,8 +1133,8 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
               V2 vw;
               if (s < cnt) {
                 V2 r_i = item_r(q, base, s);
-                V2 vj(V[item_j(q, base, s)]);
-                float w = mass * item_phi(q, base, s);
+                V2 vj(Vl[item_j(q, base, s)]);
+                float w = mass_l * item_phi(q, base, s);
                 vw = w * vj;
                 lw = w * cross2(r_i, vj);
               }
@@ -1138,37 +1144,37 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
             V2 v_bar = V2(vsx, vsy) / m_ent;
             V2 v_rel = v_bar - q.vb;
             float speed_rel = v_rel.len();
-            float inv_tau_form = (speed_rel > 1e-6f && rho0 > 0.0f)
-                                     ? 0.5f * rho0 * 1.0f * (2.0f * m.b_rtrue) * speed_rel / mass_true
+            float inv_tau_form = (speed_rel > 1e-6f && rho0_l > 0.0f)
+                                     ? 0.5f * rho0_l * 1.0f * (2.0f * b_rtrue) * speed_rel / mass_true_l
                                      : 0.0f;
-            float bt = beta_b * (1.0f - expf_r(-dt * (0.0f + inv_tau_form)));
-            float a_lin = bt * m_ent / (m.b_m + m_ent);
+            float bt = beta_l * (1.0f - expf_r(-dt_l * (0.0f + inv_tau_form)));
+            float a_lin = bt * m_ent / (b_m + m_ent);
             V2 dv_b = a_lin * v_rel;
             float dw_b = 0.0f, c_rot = 0.0f;
             if (i_ent > 1e-12f) {
               float omega_bar = l_sum / i_ent;
-              float a_rot = bt * i_ent / (i_b + i_ent);
+              float a_rot = bt * i_ent / (i_b_l + i_ent);
               float candidate_dw = a_rot * (omega_bar - q.omb);
               if (fabsf(q.s_acc) > 0.1f * q.s_scale) {
-                float raw_c_rot = -i_b * candidate_dw / q.s_acc;
-                float max_lever = 2.0f * h_c;
-                float cap = max_lever > 1e-9f ? rot_cap / max_lever : 0.0f;
+                float raw_c_rot = -i_b_l * candidate_dw / q.s_acc;
+                float max_lever = 2.0f * h_c_l;
+                float cap = max_lever > 1e-9f ? rot_cap_l / max_lever : 0.0f;
                 c_rot = clamp_r(raw_c_rot, -cap, cap);
-                dw_b = -c_rot * q.s_acc / i_b;
+                dw_b = -c_rot * q.s_acc / i_b_l;
               }
             }
             for (uint32_t s = lane; s < cnt; s += 32) {
               const uint32_t j = item_j(q, base, s);
               V2 r_i = item_r(q, base, s);
               float phi = item_phi(q, base, s);
-              V2 dv_i = -(m.b_m / m_ent) * dv_b * phi;
+              V2 dv_i = -(b_m / m_ent) * dv_b * phi;
               if (c_rot != 0.0f) {
                 V2 perp_i(-r_i.y, r_i.x);
                 dv_i += c_rot * phi * (perp_i - q.p_bar);
               }
-              V[j] = (V2(V[j]) + dv_i).f2();
+              Vl[j] = (V2(Vl[j]) + dv_i).f2();
               if (s < 32) q.dv_i = dv_i;
-              else if (want_mom) m.rec_M[m.rec_off[b] + s] = (mass * dv_i).f2();
+              else if (want_mom) m.rec_M[m.rec_off[b] + s] = (mass_l * dv_i).f2();
             }
             q.dv_b = dv_b;
             q.dw_b = dw_b;
@@ -1272,8 +1278,12 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
         [&](uint32_t b, int lane, BuoyBall& q) {
           if (q.cnt == 0) return;
           const uint32_t base = b * m.cap_items, cnt = q.cnt;
+          // this body's constants and pointers as locals (they stay in registers)
+          float2* const X_l = X;
+          float2* const V_l = V;
+          const float rho0_l = rho0, om_abs_l = om_abs, area_l = area, dt_l = dt, mass_l = mass;
           const float rho_local = q.rho_local;
-          const float rho_eff = fmin_r(rho_local, rho0);
+          const float rho_eff = fmin_r(rho_local, rho0_l);
           float num = 0.0f;
           for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
             const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
@@ -1282,13 +1292,13 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
             if (s < cnt) {
               if (s < 32) {
                 valid = q.valid;
-                nv = q.w * cross2(q.d, V2(V[q.j])) / q.d2;
+                nv = q.w * cross2(q.d, V2(V_l[q.j])) / q.d2;
               } else {
                 uint32_t j = m.item_j[base + s];
-                V2 d(X[j]);
+                V2 d(X_l[j]);
                 float d2 = d.len2();
                 valid = !(d2 <= 1e-12f);
-                nv = m.item_w[base + s] * cross2(d, V2(V[j])) / d2;
+                nv = m.item_w[base + s] * cross2(d, V2(V_l[j])) / d2;
               }
             }
             const uint32_t vmask = __ballot_sync(FULL, valid);
@@ -1300,16 +1310,16 @@ __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out,
             }
           }
           const float den = q.den;
-          float omega_local = den > 0.0f ? clamp_r(num / den, -om_abs, om_abs) : 0.0f;
+          float omega_local = den > 0.0f ? clamp_r(num / den, -om_abs_l, om_abs_l) : 0.0f;
           V2 g_eff = V2(0.0f, GRAVITY) + omega_local * omega_local * q.xb;
-          V2 impulse = -rho_eff * area * g_eff * dt;
+          V2 impulse = -rho_eff * area_l * g_eff * dt_l;
           for (uint32_t s = lane; s < cnt; s += 32) {
             const uint32_t j = s < 32 ? q.j : m.item_j[base + s];
             float frac = (s < 32 ? q.w : m.item_w[base + s]) / rho_local;
-            V2 dv = -(impulse * frac) / mass;
-            V[j] = (V2(V[j]) + dv).f2();
+            V2 dv = -(impulse * frac) / mass_l;
+            V_l[j] = (V2(V_l[j]) + dv).f2();
             if (s < 32) q.dv = dv;
-            else if (want_mom) m.rec_M[m.rec_off[b] + s] = (mass * dv).f2();
+            else if (want_mom) m.rec_M[m.rec_off[b] + s] = (mass_l * dv).f2();
           }
           q.impulse = impulse;
         },

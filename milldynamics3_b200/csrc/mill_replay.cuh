@@ -248,7 +248,18 @@ __device__ __forceinline__ void lane_seq_sum3(float& a, float& b, float& c, floa
   B[2][lane] = vc;
   __syncwarp();
   if (lane == 0) {
-    for (uint32_t t = 0; t < lim; ++t) {
+    // four terms' loads ahead of their additions
+    uint32_t t = 0;
+    for (; t + 4 <= lim; t += 4) {
+      const float a0 = B[0][t], a1 = B[0][t + 1], a2 = B[0][t + 2], a3 = B[0][t + 3];
+      const float b0 = B[1][t], b1 = B[1][t + 1], b2 = B[1][t + 2], b3 = B[1][t + 3];
+      const float c0 = B[2][t], c1 = B[2][t + 1], c2 = B[2][t + 2], c3 = B[2][t + 3];
+      a += a0; b += b0; c += c0;
+      a += a1; b += b1; c += c1;
+      a += a2; b += b2; c += c2;
+      a += a3; b += b3; c += c3;
+    }
+    for (; t < lim; ++t) {
       a += B[0][t];
       b += B[1][t];
       c += B[2][t];
