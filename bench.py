@@ -28,7 +28,7 @@ sys.path.insert(0, ROOT)
 METRIC = "sub-steps/s (1 mill) & batched mill-frames/s on 1 B200; p50/p99 frame latency"
 UNIT = "sub-steps/s"
 # DRAM bytes (read + write) of one realtime frame launch, from an ncu capture (see profiles/)
-REALTIME_LAUNCH_DRAM_BYTES = 1.392e6 + 0.232e6
+REALTIME_LAUNCH_DRAM_BYTES = 2.076e6 + 0.273e6
 
 
 def dist_env():
