@@ -184,7 +184,7 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
   const float reach = 0.25f * r;
   const float touch2 = (2.0f * r + reach) * (2.0f * r + reach);
   uint32_t* keep = reinterpret_cast<uint32_t*>(m.act_bin);  // pairs in the run (act_bin is free until step 5)
-  for (uint32_t i = tid(); i < n; i += nthr()) { m.bxs[i] = X[i]; m.bmove[i] = 0.0f; }
+  for (uint32_t i = tid(); i < n; i += nthr()) m.bxs[i] = X[i];
   __syncthreads();
   for (uint32_t k = tid(); k < np; k += nthr())
     keep[k] = (V2(m.bxs[m.pair_i[k]]) - V2(m.bxs[m.pair_j[k]])).len2() < touch2 ? 1u : 0u;
@@ -192,6 +192,7 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
   stage_mark(out.stage, 15);
   uint32_t *lvl = m.dm_lvl, *di = m.act_i, *dj = m.act_j;
   float* dl = m.act_l;
+  float* bm = m.bmove;  // per ball largest squared excursion of the run (shared memory when it fits)
   // the larger of the recorded and the new squared excursion; a NaN excursion is kept (and
   // fails the check)
   auto excursion = [](float cur, V2 d) {
@@ -216,6 +217,7 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
     // sweep scratch (levels, level-ordered descriptors, multipliers): shared memory after the
     // ball state when the items fit, global otherwise
     lvl = m.dm_lvl; di = m.act_i; dj = m.act_j; dl = m.act_l;
+    bm = m.bmove;
     if (staged) {
       const uint32_t used = (24u * n + 15u) & ~15u;
       const uint32_t fit = m.smem_bytes > used ? (m.smem_bytes - used) / 16u : 0u;
@@ -224,8 +226,13 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
         di = lvl + npi;
         dj = di + npi;
         dl = reinterpret_cast<float*>(dj + npi);
+        // the excursions too when they fit: they are read and written level after level, and a
+        // global store leaves the next level's read an L2 round trip
+        const uint32_t off = used + 16u * npi;
+        if (off + 4u * n <= m.smem_bytes) bm = reinterpret_cast<float*>(dsm + off);
       }
     }
+    for (uint32_t i = tid(); i < n; i += nthr()) bm[i] = 0.0f;
     const uint32_t nlev = compute_levels(npi, m.dm_pa, m.dm_pb, lvl);
     stage_mark(out.stage, 21);
     bucket_levels(npi, lvl, nlev, m.lev_start, m.lev_cur, m.lev_items);
@@ -243,7 +250,7 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
     float2* const Xp = X;
     float* const dlp = dl;
     const float2* const bxs = m.bxs;
-    float* const bmv = m.bmove;
+    float* const bmv = bm;
     const uint32_t* const dip = di;
     const uint32_t* const djp = dj;
     for (uint32_t it = 0; it < iters; ++it) {
@@ -253,6 +260,7 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
         float* const dl = dlp;
         const uint32_t i = d.x, j = d.y;
         V2 xi(X[i]), xj(X[j]);
+        const float dlq = dl[q];  // loaded beside the positions (only this item writes it)
         // start positions and excursions so far, loaded beside the positions
         V2 si, sj;
         float ei = 0.0f, ej = 0.0f;
@@ -269,7 +277,7 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
         const V2 xin = xi + w * d_lambda * n_hat, xjn = xj - w * d_lambda * n_hat;
         X[i] = xin.f2();
         X[j] = xjn.f2();
-        dl[q] += d_lambda;
+        dl[q] = dlq + d_lambda;
         if (track) {
           bmv[i] = excursion(ei, V2(xin.f2()) - si);
           bmv[j] = excursion(ej, V2(xjn.f2()) - sj);
@@ -288,7 +296,7 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
         const V2 xn = x + w * d_lambda * n_hat;
         X[i] = xn.f2();
         m.lam_bw[i] += d_lambda;
-        if (track) m.bmove[i] = excursion(m.bmove[i], V2(xn.f2()) - V2(m.bxs[i]));
+        if (track) bm[i] = excursion(bm[i], V2(xn.f2()) - V2(m.bxs[i]));
       }
       __syncthreads();
     }
@@ -316,12 +324,12 @@ __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, M
       const uint32_t i = m.pair_i[k], j = m.pair_j[k];
       const float2 a = m.bxs[i], b = m.bxs[j];
       const double dx = (double)a.x - (double)b.x, dy = (double)a.y - (double)b.y;
-      const double ei = sqrt((double)m.bmove[i]), ej = sqrt((double)m.bmove[j]);
+      const double ei = sqrt((double)bm[i]), ej = sqrt((double)bm[j]);
       const double slack = 1e-6 * (fabs((double)a.x) + fabs((double)a.y) + fabs((double)b.x) + fabs((double)b.y) + ei + ej);
       if (!(sqrt(dx * dx + dy * dy) - (ei + ej) * (1.0 + 1e-5) - slack >= sep)) { keep[k] = 1u; bad = true; }
     }
     if (!__syncthreads_or(bad)) break;
-    for (uint32_t i = tid(); i < n; i += nthr()) { X[i] = m.bxs[i]; m.bmove[i] = 0.0f; }
+    for (uint32_t i = tid(); i < n; i += nthr()) X[i] = m.bxs[i];
     __syncthreads();
     stage_mark(out.stage, 39);
   }

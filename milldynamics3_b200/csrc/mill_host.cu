@@ -309,7 +309,7 @@ void fill_desc(MgSim* s) {
   s->md.b_m = s->bmat.mass;
   s->md.b_I = s->bmat.inertia;
   s->md.b_rtrue = s->bmat.true_radius;
-  s->md.smem_bytes = (uint32_t)stage_smem_bytes(s->nf, s->nb);
+  s->md.smem_bytes = (uint32_t)stage_smem_bytes(s->nf, s->nb, s->mill_blocks_cap > 1);
   s->md.smem_balls = (size_t)s->nb * 24 <= s->md.smem_bytes ? s->nb : 0u;
 }
 

@@ -24,14 +24,21 @@ cudaError_t launch_pack_impacts(const MillDev* mills, uint32_t n_mills, const ui
                                 cudaStream_t stream);
 // Largest dynamic shared-memory allotment of a launch. The region holds, one phase at a time,
 // the fluid positions and velocities plus completion flags of the drag / buoyancy sweeps
-// (16 nf + 4 nb bytes) and the ball state of the DEM sweeps (24 nb bytes); it is sized to the
-// larger of the two so that the rest of the SM's L1 / shared storage stays L1 cache.
+// (16 nf + 4 nb bytes) and the ball state of the DEM sweeps (24 nb bytes), with sweep_scratch
+// also the projection sweep's scratch after it (16 bytes per item, reserved for 8 items a ball,
+// and 4 nb of excursions); it is sized to the largest of them (without the projection scratch
+// when that does not fit), and the rest of the SM's L1 / shared storage stays L1 cache. Batches
+// leave the projection scratch out: the L1 it takes costs more across mills than it saves.
 constexpr size_t MAX_STAGE_SMEM = 200 * 1024;
-inline size_t stage_smem_bytes(uint32_t nf, uint32_t nb) {
-  size_t fluid = 16 * (size_t)nf + 4 * (size_t)nb + 64, balls = 24 * (size_t)nb;
-  size_t need = ((fluid > balls ? fluid : balls) + 255) & ~size_t(255);
+inline size_t stage_smem_bytes(uint32_t nf, uint32_t nb, bool sweep_scratch) {
+  const size_t fluid = 16 * (size_t)nf + 4 * (size_t)nb + 64, balls = 24 * (size_t)nb;
+  const size_t sweep = sweep_scratch ? balls + 16 + 132 * (size_t)nb : balls;
+  auto up = [](size_t v) { return (v + 255) & ~size_t(255); };
+  const size_t want = up(fluid > sweep ? fluid : sweep);
+  if (want <= MAX_STAGE_SMEM) return want;
+  const size_t need = up(fluid > balls ? fluid : balls);
   if (need <= MAX_STAGE_SMEM) return need;
-  return balls <= MAX_STAGE_SMEM ? ((balls + 255) & ~size_t(255)) : 0;
+  return up(balls) <= MAX_STAGE_SMEM ? up(balls) : 0;
 }
 // Sets the message mg_global_last_error() returns on this host thread; returns code.
 int set_global_error(int code, const char* msg);
