@@ -274,6 +274,38 @@ int mg_energy_budget(MgSim* sim, MgEnergyBudget* out);
 int mg_state_hash(MgSim* sim, int extended, uint64_t* out);
 /* metrics::mixing_index (metrics.rs:506-576); *valid = 0 for None */
 int mg_mixing_index(MgSim* sim, float* out, int* valid);
+
+/* metrics::Metrics, the fields metrics::compute fills (metrics.rs:78-273): charge toe/shoulder,
+ * centroid, slurry pool extent and depth, free-surface line, mixing index, ball kinetic energy,
+ * ball-ball and ball-wall overlap, fluid density and compression errors. Option fields are
+ * present when their bit is set in `valid`. */
+#define MG_METRIC_TOE_SHOULDER 0x01u
+#define MG_METRIC_CENTROID 0x02u
+#define MG_METRIC_POOL_EXTENT 0x04u
+#define MG_METRIC_FREE_SURFACE 0x08u
+#define MG_METRIC_POOL_DEPTH 0x10u
+#define MG_METRIC_MIXING 0x20u
+#define MG_METRIC_DENSITY 0x40u /* the four fluid density / compression error fields */
+typedef struct MgMetrics {
+  uint32_t valid;
+  float toe_angle_rad, shoulder_angle_rad;
+  float charge_centroid_m[2];
+  float pool_angle_min_rad, pool_angle_max_rad;
+  float free_surface_angle_rad, free_surface_offset_m;
+  float pool_depth_m;
+  float mixing_index;
+  float total_kinetic_energy_j;
+  float max_ball_overlap_fraction, max_ball_wall_overlap_fraction;
+  float max_fluid_density_error_fraction, mean_fluid_density_error_fraction;
+  float max_fluid_compression_error_fraction, mean_fluid_compression_error_fraction;
+  float drum_omega_rad_s;
+  uint32_t fluid_particle_count;
+} MgMetrics;
+/* metrics::compute(balls, fluid, drum, drum_angle) (metrics.rs:195-273) on the handle's current
+ * state, as one kernel launch on the handle's stream. The launch rebuilds the fluid neighbour
+ * lists for the current positions in the handle's sub-step scratch, so mg_last_neighbor_lists
+ * afterwards returns those. */
+int mg_metrics(MgSim* sim, MgMetrics* out);
 /* StressAccum::histogram_rate (stress.rs:174-176), 28 bins per second */
 int mg_stress_histogram_rate(MgSim* sim, double* out28);
 /* stats of the last sub-step taken by any step call */

@@ -171,6 +171,23 @@ class ServerStats(_S):
                 ("last_frame_ms", C.c_float), ("last_kernel_ms", C.c_float)]
 
 
+METRIC_TOE_SHOULDER, METRIC_CENTROID, METRIC_POOL_EXTENT, METRIC_FREE_SURFACE = 0x01, 0x02, 0x04, 0x08
+METRIC_POOL_DEPTH, METRIC_MIXING, METRIC_DENSITY = 0x10, 0x20, 0x40
+
+
+class Metrics(_S):
+    _fields_ = [("valid", C.c_uint32), ("toe_angle_rad", C.c_float), ("shoulder_angle_rad", C.c_float),
+                ("charge_centroid_m", C.c_float * 2), ("pool_angle_min_rad", C.c_float),
+                ("pool_angle_max_rad", C.c_float), ("free_surface_angle_rad", C.c_float),
+                ("free_surface_offset_m", C.c_float), ("pool_depth_m", C.c_float), ("mixing_index", C.c_float),
+                ("total_kinetic_energy_j", C.c_float), ("max_ball_overlap_fraction", C.c_float),
+                ("max_ball_wall_overlap_fraction", C.c_float), ("max_fluid_density_error_fraction", C.c_float),
+                ("mean_fluid_density_error_fraction", C.c_float),
+                ("max_fluid_compression_error_fraction", C.c_float),
+                ("mean_fluid_compression_error_fraction", C.c_float), ("drum_omega_rad_s", C.c_float),
+                ("fluid_particle_count", C.c_uint32)]
+
+
 class StressMetrics(_S):
     _fields_ = [("ball_mass_3d_kg", C.c_float), ("scale_energy_j", C.c_float),
                 ("impacts_per_ball_per_s", C.c_float * 4), ("impacts_total_per_ball_per_s", C.c_float),
@@ -245,6 +262,7 @@ SIGNATURES = [
     ("last_neighbor_lists", C.c_int, [vp, u32p, u32p, C.c_uint32, u32p]),
     ("last_ball_pairs", C.c_int, [vp, u32p, C.c_uint32, u32p]),
     ("stress_metrics", C.c_int, [vp, P(StressMetrics)]),
+    ("metrics", C.c_int, [vp, P(Metrics)]),
     ("seed_value_name", C.c_char_p, [C.c_uint32]),
     ("seed_sweep", C.c_int, [P(Params), P(C.c_uint64), C.c_uint32, C.c_float, C.c_float, P(SeedResult)]),
     ("seed_combine", C.c_int, [P(SeedResult), C.c_uint32, P(C.c_double), P(C.c_double)]),

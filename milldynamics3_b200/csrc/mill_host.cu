@@ -146,6 +146,7 @@ struct MgSim {
   SubAngles* d_ang = nullptr;
   StepOut* h_out = nullptr;
   MgImpactRecord* h_imp = nullptr;
+  MgMetrics* d_metrics = nullptr;  // mg_metrics output (in the arena)
   uint32_t guess_valid_host = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_kernel_ms = 0.0f;
@@ -269,6 +270,7 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
     m.ball_done = a.take<uint32_t>(cb);
     m.slot = a.take<uint32_t>((size_t)MAX_BLOCK_WARPS * s->mill_blocks_cap * cf);
     m.wide = a.take<WideCtl>(1);
+    s->d_metrics = a.take<MgMetrics>(1);
     m.pair_i = a.take<uint32_t>(m.cap_pairs); m.pair_j = a.take<uint32_t>(m.cap_pairs);
     m.lam_bb = a.take<float>(m.cap_pairs);
     m.pr_list = a.take<uint32_t>(m.cap_pairs);
@@ -1029,6 +1031,31 @@ int mg_mixing_index(MgSim* s, float* out, int* valid) {
   *valid = 1;
   if (std::fabs(denom) < 1e-9f) { *out = 1.0f; return MG_OK; }
   *out = mgh::clamp_r((s0 - observed) / denom, 0.0f, 1.0f);
+  return MG_OK;
+}
+// metrics::compute (metrics.rs:195-273) on the device, for the current drum angle
+int mg_metrics(MgSim* s, MgMetrics* out) {
+  if (!s || !out) return fail_global(MG_ERR_ARG, "null argument");
+  MgDrum drum = sim_drum(s);
+  int rc = fill_uniform(s, drum, s->params.media, s->params.slurry, 1, 1, 1, 1, 0);
+  if (rc) return rc;
+  StepUniform& U = *s->h_uni;
+  const float a = s->drum_angle;
+  U.drum_angle = U.drum_angle_next = a;
+  U.to_local_next = V2(mgh::cosf_r(-a), mgh::sinf_r(-a));  // Vec2::from_angle(-angle)
+  U.to_world_next = V2(mgh::cosf_r(a), mgh::sinf_r(a));
+  U.to_local0 = U.to_local_next;
+  rc = check_materials(s);
+  if (!rc) rc = push_desc(s);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(s->d_uni, s->h_uni, sizeof(StepUniform), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemsetAsync(s->md.err, 0, sizeof(uint32_t), s->stream));
+  CK(launch_metrics(s->d_md, s->d_uni, s->d_metrics, s->stream));
+  uint32_t e = 0;
+  CK(cudaMemcpyAsync(out, s->d_metrics, sizeof(MgMetrics), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(&e, s->md.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (e) return fail(s, MG_ERR_CAPACITY, "device capacity exceeded in the metrics (error bits 0x%x)", e);
   return MG_OK;
 }
 int mg_stress_histogram_rate(MgSim* s, double* out28) {

@@ -5,6 +5,7 @@
 #include "mill_dem.cuh"
 #include "mill_fluid.cuh"
 #include "mill_kernels.h"
+#include "mill_metrics.cuh"
 
 namespace mg {
 
@@ -163,6 +164,11 @@ cudaError_t launch_pack_impacts(const MillDev* mills, uint32_t n_mills, const ui
                                 MgImpactRecord* packed, uint32_t cap, uint32_t* cursor, uint2* table,
                                 cudaStream_t stream) {
   pack_impacts_kernel<<<n_mills, 256, 0, stream>>>(mills, n_sub_of, packed, cap, cursor, table);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_metrics(const MillDev* mill, const StepUniform* uni, MgMetrics* out, cudaStream_t stream) {
+  metrics_kernel<<<1, 1024, 0, stream>>>(mill, uni, out);
   return cudaGetLastError();
 }
 

@@ -42,6 +42,9 @@ inline size_t stage_smem_bytes(uint32_t nf, uint32_t nb, bool sweep_scratch) {
 }
 // Sets the message mg_global_last_error() returns on this host thread; returns code.
 int set_global_error(int code, const char* msg);
+// metrics::compute on mill[0]'s state (one block); uni holds the mill's geometry with
+// to_local_next / to_world_next set for the current drum angle.
+cudaError_t launch_metrics(const MillDev* mill, const StepUniform* uni, MgMetrics* out, cudaStream_t stream);
 // Grid-stage probe over the descriptor's fx[0..nf): mode 0 grid, 1 candidate pairs, 2 neighbours.
 cudaError_t launch_probe(const MillDev* mill, float cell, int mode, uint32_t* result, cudaStream_t stream);
 

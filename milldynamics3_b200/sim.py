@@ -272,6 +272,12 @@ class Simulation:
         self._c(self.lib.stress_histogram_rate(self.h, out))
         return np.array(list(out))
 
+    def metrics(self) -> capi.Metrics:
+        """metrics::compute on the current state (metrics.rs:195-273)."""
+        out = capi.Metrics()
+        self._c(self.lib.metrics(self.h, C.byref(out)))
+        return out
+
     def stress_metrics(self) -> capi.StressMetrics:
         """Simulation::metrics (lib.rs:383-390 over StressAccum::metrics, stress.rs:186-237)."""
         out = capi.StressMetrics()

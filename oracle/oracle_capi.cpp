@@ -284,6 +284,11 @@ int or_state_hash(OrSim* s, int ext, uint64_t* out) {
   *out = state_hash(s->sim.balls, s->sim.fluid, ext != 0);
   return MG_OK;
 }
+int or_metrics(OrSim* s, MgMetrics* out) {
+  if (!s || !out) { g_err = "null argument"; return MG_ERR_ARG; }
+  metrics_compute(s->sim.balls, s->sim.fluid, s->sim.drum(), s->sim.drum_angle, out);
+  return MG_OK;
+}
 int or_mixing_index(OrSim* s, float* out, int* valid) {
   float m = 0.0f;
   *valid = mixing_index(s->sim.fluid, s->sim.drum(), &m) ? 1 : 0;

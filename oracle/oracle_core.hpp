@@ -24,6 +24,8 @@
 #include <string>
 #include <vector>
 
+struct MgMetrics;  // include/millgpu.h
+
 namespace orc {
 
 constexpr float PI_F = 3.14159265358979323846f;
@@ -442,6 +444,7 @@ struct Simulation {
 };
 
 bool mixing_index(const Fluid& f, const Drum& d, float* out);
+void metrics_compute(const Balls& b, const Fluid& f, const Drum& d, float drum_angle, ::MgMetrics* out);
 uint64_t state_hash(const Balls& b, const Fluid& f, bool extended);
 
 }  // namespace orc
