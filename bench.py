@@ -161,9 +161,16 @@ def cpu_baseline(seconds=10.0):
         sim.step(1.0 / 60.0)
         frames += 1
     dt = time.perf_counter() - t0
+    # metrics::compute on the same state, one thread
+    calls = 0
+    t1 = time.perf_counter()
+    while calls < 5 or time.perf_counter() - t1 < 1.0:
+        sim.metrics()
+        calls += 1
+    met_ms = 1e3 * (time.perf_counter() - t1) / calls
     return {"value": frames * n_sub / dt, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": "%d frames of the realtime mill on the oracle (C++ restatement), 1 thread, %.1f s"
-                      % (frames, dt)}
+                      % (frames, dt), "metrics_ms_per_call": met_ms}
 
 
 def run_batched(lib, backend, args):
@@ -363,6 +370,12 @@ def run_device(args):
     e2e = world * args.steps * n_sub / te
     launches = C.c_uint64()
     lib.sim_last_kernel_ms(sim.h, None, C.byref(launches))
+    # metrics::compute through the C ABI (one kernel launch, result copied back), per call
+    sim.metrics()
+    t0 = time.perf_counter()
+    for _ in range(20):
+        sim.metrics()
+    met_ms = 1e3 * (time.perf_counter() - t0) / 20
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
@@ -381,6 +394,8 @@ def run_device(args):
                              "kernel_ms_per_launch": k_ms, "algorithmic_bytes_per_launch": per_launch_bytes},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
                 "gpu_launches": args.steps, "clocks": clocks, "stage_us_per_substep": stages,
+                "metrics": {"call": "mg_metrics (metrics::compute on the realtime mill's state, one kernel)",
+                            "ms_per_call": met_ms},
                 "counters_per_substep": {f: round(tot[q] / max(nsum.value, 1), 2) for q, (f, _) in
                                          enumerate(capi.StepCounters._fields_) if f != "reserved0"}}
         plain_mfps = None
@@ -391,6 +406,7 @@ def run_device(args):
             line["serving"] = run_serving(b, args, plain_mfps)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+            line["metrics"]["cpu_ms_per_call"] = line["cpu_baseline"].pop("metrics_ms_per_call")
         print(json.dumps(line), flush=True)
     sim.close()
     if world > 1:
