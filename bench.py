@@ -168,9 +168,16 @@ def cpu_baseline(seconds=10.0):
         sim.metrics()
         calls += 1
     met_ms = 1e3 * (time.perf_counter() - t1) / calls
+    # surface::extract_surface on the same state, one thread
+    calls = 0
+    t1 = time.perf_counter()
+    while calls < 5 or time.perf_counter() - t1 < 1.0:
+        sim.surface_flat()
+        calls += 1
+    surf_ms = 1e3 * (time.perf_counter() - t1) / calls
     return {"value": frames * n_sub / dt, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": "%d frames of the realtime mill on the oracle (C++ restatement), 1 thread, %.1f s"
-                      % (frames, dt), "metrics_ms_per_call": met_ms}
+                      % (frames, dt), "metrics_ms_per_call": met_ms, "surface_ms_per_call": surf_ms}
 
 
 def run_batched(lib, backend, args):
@@ -376,6 +383,16 @@ def run_device(args):
     for _ in range(20):
         sim.metrics()
     met_ms = 1e3 * (time.perf_counter() - t0) / 20
+    # Simulation::fluid_surface through the C ABI (two kernel launches, flattened polygons copied
+    # back into a host buffer), per call
+    surf_buf = torch.zeros(capi.SURFACE_OUT_CAP, dtype=torch.float32).pin_memory()
+    surf_len = C.c_uint32()
+    lib.fluid_surface(sim.h, fptr(surf_buf), surf_buf.numel(), C.byref(surf_len))
+    t0 = time.perf_counter()
+    for _ in range(20):
+        lib.fluid_surface(sim.h, fptr(surf_buf), surf_buf.numel(), C.byref(surf_len))
+    surf_ms = 1e3 * (time.perf_counter() - t0) / 20
+    surf_polys = int(surf_buf[0].item())
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
@@ -396,6 +413,9 @@ def run_device(args):
                 "gpu_launches": args.steps, "clocks": clocks, "stage_us_per_substep": stages,
                 "metrics": {"call": "mg_metrics (metrics::compute on the realtime mill's state, one kernel)",
                             "ms_per_call": met_ms},
+                "surface": {"call": "mg_fluid_surface (surface::extract_surface on the realtime mill's state, "
+                                    "two kernels, flattened polygons to a host buffer)",
+                            "ms_per_call": surf_ms, "polygons": surf_polys, "floats": surf_len.value},
                 "counters_per_substep": {f: round(tot[q] / max(nsum.value, 1), 2) for q, (f, _) in
                                          enumerate(capi.StepCounters._fields_) if f != "reserved0"}}
         plain_mfps = None
@@ -407,6 +427,7 @@ def run_device(args):
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
             line["metrics"]["cpu_ms_per_call"] = line["cpu_baseline"].pop("metrics_ms_per_call")
+            line["surface"]["cpu_ms_per_call"] = line["cpu_baseline"].pop("surface_ms_per_call")
         print(json.dumps(line), flush=True)
     sim.close()
     if world > 1:

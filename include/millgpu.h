@@ -306,6 +306,21 @@ typedef struct MgMetrics {
  * lists for the current positions in the handle's sub-step scratch, so mg_last_neighbor_lists
  * afterwards returns those. */
 int mg_metrics(MgSim* sim, MgMetrics* out);
+
+/* Free-surface extraction for rendering. */
+#define MG_SURFACE_GRID 128 /* grid points per axis over [-R, R] (surface.rs:27) */
+/* Simulation::fluid_surface (lib.rs:354-361: surface::extract_surface, surface.rs:233-272) on the
+ * handle's current state, flattened as mill-wasm's fluid_surface returns it (flatten_polygons,
+ * surface.rs:420-430): [n_polys, len_0, x, y, ..., len_1, x, y, ...], world frame. Two kernel
+ * launches on the handle's stream (splatted field; contour, chaining, smoothing and wall
+ * projection). *len receives the number of floats (1 when there is no surface). out may be NULL
+ * to query the length; MG_ERR_CAPACITY when out is non-NULL and cap < *len (nothing copied). */
+int mg_fluid_surface(MgSim* sim, float* out, uint32_t cap, uint32_t* len);
+/* The masked occupancy field build_field returns (surface.rs:84-131), MG_SURFACE_GRID^2 floats,
+ * row gj * MG_SURFACE_GRID + gi, and analytic_phi_full (surface.rs:71-74) of the fluid. No
+ * counterpart in the reference's public API: build_field is private there; this exposes it for
+ * checks against the oracle. */
+int mg_surface_field(MgSim* sim, float* field, float* phi_full);
 /* StressAccum::histogram_rate (stress.rs:174-176), 28 bins per second */
 int mg_stress_histogram_rate(MgSim* sim, double* out28);
 /* stats of the last sub-step taken by any step call */

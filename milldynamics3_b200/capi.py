@@ -171,6 +171,9 @@ class ServerStats(_S):
                 ("last_frame_ms", C.c_float), ("last_kernel_ms", C.c_float)]
 
 
+SURFACE_GRID = 128  # MG_SURFACE_GRID
+# most floats mg_fluid_surface can return: 1 + 9 * (2 segments in each of the (G - 1)^2 cells)
+SURFACE_OUT_CAP = 1 + 9 * 2 * (SURFACE_GRID - 1) ** 2
 METRIC_TOE_SHOULDER, METRIC_CENTROID, METRIC_POOL_EXTENT, METRIC_FREE_SURFACE = 0x01, 0x02, 0x04, 0x08
 METRIC_POOL_DEPTH, METRIC_MIXING, METRIC_DENSITY = 0x10, 0x20, 0x40
 
@@ -263,6 +266,8 @@ SIGNATURES = [
     ("last_ball_pairs", C.c_int, [vp, u32p, C.c_uint32, u32p]),
     ("stress_metrics", C.c_int, [vp, P(StressMetrics)]),
     ("metrics", C.c_int, [vp, P(Metrics)]),
+    ("fluid_surface", C.c_int, [vp, f32p, C.c_uint32, u32p]),
+    ("surface_field", C.c_int, [vp, f32p, f32p]),
     ("seed_value_name", C.c_char_p, [C.c_uint32]),
     ("seed_sweep", C.c_int, [P(Params), P(C.c_uint64), C.c_uint32, C.c_float, C.c_float, P(SeedResult)]),
     ("seed_combine", C.c_int, [P(SeedResult), C.c_uint32, P(C.c_double), P(C.c_double)]),

@@ -147,6 +147,9 @@ struct MgSim {
   StepOut* h_out = nullptr;
   MgImpactRecord* h_imp = nullptr;
   MgMetrics* d_metrics = nullptr;  // mg_metrics output (in the arena)
+  void* surf_mem = nullptr;        // mg_fluid_surface scratch (allocated on first use)
+  uint32_t* h_surf = nullptr;      // pinned staging of the surface header and output head
+  SurfDev surf{};
   uint32_t guess_valid_host = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_kernel_ms = 0.0f;
@@ -714,6 +717,11 @@ void mg_sim_destroy(MgSim* s) {
   if (s->light) {
     // the arena goes back to the pool in stream order; the stream belongs to the server
     if (s->dmem) cudaFreeAsync(s->dmem, s->stream);
+    if (s->surf_mem) cudaFreeAsync(s->surf_mem, s->stream);
+    if (s->h_surf) {
+      cudaStreamSynchronize(s->stream);
+      cudaFreeHost(s->h_surf);
+    }
     delete s->h_uni;
     delete[] s->h_out;
     delete[] s->h_imp;
@@ -722,6 +730,8 @@ void mg_sim_destroy(MgSim* s) {
   }
   if (s->stream) cudaStreamSynchronize(s->stream);
   if (s->dmem) cudaFree(s->dmem);
+  if (s->surf_mem) cudaFree(s->surf_mem);
+  if (s->h_surf) cudaFreeHost(s->h_surf);
   if (s->d_md) cudaFree(s->d_md);
   if (s->d_uni) cudaFree(s->d_uni);
   if (s->d_ang) cudaFree(s->d_ang);
@@ -1034,8 +1044,9 @@ int mg_mixing_index(MgSim* s, float* out, int* valid) {
   return MG_OK;
 }
 // metrics::compute (metrics.rs:195-273) on the device, for the current drum angle
-int mg_metrics(MgSim* s, MgMetrics* out) {
-  if (!s || !out) return fail_global(MG_ERR_ARG, "null argument");
+// Uploads the uniform of the handle's current state (drum at s->drum_angle, rotations
+// from_angle(-angle) and from_angle(angle)) for the launches that read the state in place.
+static int push_state_uniform(MgSim* s) {
   MgDrum drum = sim_drum(s);
   int rc = fill_uniform(s, drum, s->params.media, s->params.slurry, 1, 1, 1, 1, 0);
   if (rc) return rc;
@@ -1049,6 +1060,13 @@ int mg_metrics(MgSim* s, MgMetrics* out) {
   if (!rc) rc = push_desc(s);
   if (rc) return rc;
   CK(cudaMemcpyAsync(s->d_uni, s->h_uni, sizeof(StepUniform), cudaMemcpyHostToDevice, s->stream));
+  return MG_OK;
+}
+
+int mg_metrics(MgSim* s, MgMetrics* out) {
+  if (!s || !out) return fail_global(MG_ERR_ARG, "null argument");
+  int rc = push_state_uniform(s);
+  if (rc) return rc;
   CK(cudaMemsetAsync(s->md.err, 0, sizeof(uint32_t), s->stream));
   CK(launch_metrics(s->d_md, s->d_uni, s->d_metrics, s->stream));
   uint32_t e = 0;
@@ -1058,6 +1076,72 @@ int mg_metrics(MgSim* s, MgMetrics* out) {
   if (e) return fail(s, MG_ERR_CAPACITY, "device capacity exceeded in the metrics (error bits 0x%x)", e);
   return MG_OK;
 }
+// The free-surface scratch, allocated on first use: field, chains, polygon records, output and
+// header in one block.
+constexpr uint32_t SURF_STAGE = 16384;
+static int surf_scratch(MgSim* s) {
+  if (s->surf_mem) return MG_OK;
+  const size_t n_field = (size_t)SURF_G * SURF_G;
+  const size_t bytes = 4 * (n_field + 2 * (size_t)SURF_MAX_SEGS + SURF_WALK_CAP + 3 * (size_t)SURF_MAX_SEGS +
+                            SURF_OUT_CAP + 4);
+  cudaError_t e = s->light ? cudaMallocAsync(&s->surf_mem, bytes, s->stream) : cudaMalloc(&s->surf_mem, bytes);
+  if (e != cudaSuccess) {
+    s->surf_mem = nullptr;
+    return fail(s, MG_ERR_CUDA, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  }
+  float* f = (float*)s->surf_mem;
+  SurfDev& sd = s->surf;
+  sd.field = f;
+  sd.segs = (uint32_t*)(f + n_field);
+  sd.walk = sd.segs + 2 * (size_t)SURF_MAX_SEGS;
+  sd.poly = sd.walk + SURF_WALK_CAP;
+  sd.hdr = sd.poly + 3 * (size_t)SURF_MAX_SEGS;  // the output follows the header, so that one
+  sd.phi_full = (float*)(sd.hdr + 2);            // copy brings back both when the surface is small
+  sd.out = (float*)(sd.hdr + 4);
+  e = cudaMallocHost(&s->h_surf, sizeof(uint32_t) * (4 + SURF_STAGE));
+  if (e != cudaSuccess) {
+    s->h_surf = nullptr;
+    return fail(s, MG_ERR_CUDA, "cudaMallocHost: %s", cudaGetErrorString(e));
+  }
+  return MG_OK;
+}
+
+int mg_fluid_surface(MgSim* s, float* out, uint32_t cap, uint32_t* len) {
+  if (!s || !len) return fail_global(MG_ERR_ARG, "null argument");
+  int rc = surf_scratch(s);
+  if (!rc) rc = push_state_uniform(s);
+  if (rc) return rc;
+  CK(launch_surface(s->d_md, s->d_uni, s->surf, true, s->stream));
+  // header and the first SURF_STAGE floats in one copy; the rest, if any, in a second
+  const uint32_t first = out ? std::min<uint32_t>(cap, SURF_STAGE) : 0u;
+  CK(cudaMemcpyAsync(s->h_surf, s->surf.hdr, sizeof(uint32_t) * (4 + first), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  const uint32_t n = s->h_surf[0];
+  *len = n;
+  if (!out) return MG_OK;
+  if (cap < n) return fail(s, MG_ERR_CAPACITY, "surface needs %u floats, buffer holds %u", n, cap);
+  std::memcpy(out, s->h_surf + 4, sizeof(float) * std::min(n, first));
+  if (n > first) {
+    CK(cudaMemcpyAsync(out + first, s->surf.out + first, sizeof(float) * (n - first), cudaMemcpyDeviceToHost,
+                       s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+  }
+  return MG_OK;
+}
+
+int mg_surface_field(MgSim* s, float* field, float* phi_full) {
+  if (!s) return fail_global(MG_ERR_ARG, "null handle");
+  int rc = surf_scratch(s);
+  if (!rc) rc = push_state_uniform(s);
+  if (rc) return rc;
+  CK(launch_surface(s->d_md, s->d_uni, s->surf, false, s->stream));
+  if (field)
+    CK(cudaMemcpyAsync(field, s->surf.field, sizeof(float) * SURF_G * SURF_G, cudaMemcpyDeviceToHost, s->stream));
+  if (phi_full) CK(cudaMemcpyAsync(phi_full, s->surf.phi_full, sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return MG_OK;
+}
+
 int mg_stress_histogram_rate(MgSim* s, double* out28) {
   if (!s || !out28) return fail_global(MG_ERR_ARG, "null argument");
   std::memcpy(out28, s->stress.hist_rate, sizeof(double) * MG_SE_BINS);

@@ -6,6 +6,7 @@
 #include "mill_fluid.cuh"
 #include "mill_kernels.h"
 #include "mill_metrics.cuh"
+#include "mill_surface.cuh"
 
 namespace mg {
 
@@ -169,6 +170,18 @@ cudaError_t launch_pack_impacts(const MillDev* mills, uint32_t n_mills, const ui
 
 cudaError_t launch_metrics(const MillDev* mill, const StepUniform* uni, MgMetrics* out, cudaStream_t stream) {
   metrics_kernel<<<1, 1024, 0, stream>>>(mill, uni, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_surface(const MillDev* mill, const StepUniform* uni, const SurfDev& sd, bool contour,
+                           cudaStream_t stream) {
+  surface_field_kernel<<<SURF_TILES_AXIS * SURF_TILES_AXIS, SURF_TILE * SURF_TILE, 0, stream>>>(mill, uni, sd);
+  if (contour) {
+    cudaError_t e = cudaFuncSetAttribute(surface_contour_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(SurfShared));
+    if (e != cudaSuccess) return e;
+    surface_contour_kernel<<<1, SURF_THREADS, sizeof(SurfShared), stream>>>(mill, uni, sd);
+  }
   return cudaGetLastError();
 }
 

@@ -45,6 +45,32 @@ int set_global_error(int code, const char* msg);
 // metrics::compute on mill[0]'s state (one block); uni holds the mill's geometry with
 // to_local_next / to_world_next set for the current drum angle.
 cudaError_t launch_metrics(const MillDev* mill, const StepUniform* uni, MgMetrics* out, cudaStream_t stream);
+
+// Free-surface extraction (surface.rs:233-272): the 128 x 128 grid points over [-R, R] of the
+// occupancy field, and its (128 - 1)^2 marching-squares cells with at most two segments each.
+constexpr int SURF_G = MG_SURFACE_GRID;
+constexpr int SURF_CELLS_AXIS = SURF_G - 1;
+constexpr int SURF_CELLS = SURF_CELLS_AXIS * SURF_CELLS_AXIS;
+constexpr uint32_t SURF_MAX_SEGS = 2 * SURF_CELLS;
+// chains hold at most S + P <= 2 S edge ids (S segments, P polygons), and backward walks stage
+// at most S more
+constexpr uint32_t SURF_WALK_CAP = 3 * SURF_MAX_SEGS;
+// 1 + P + 2 T floats with T <= 2 (S + P) smoothed points
+constexpr uint32_t SURF_OUT_CAP = 1 + 9 * SURF_MAX_SEGS;
+// Device scratch of the free-surface launches.
+struct SurfDev {
+  float* field;      // SURF_G^2, row gj * SURF_G + gi
+  uint32_t* segs;    // segment edge ids and partners when they exceed shared memory (2 S)
+  uint32_t* walk;    // chains (edge ids), then backward-walk staging
+  uint32_t* poly;    // per polygon: chain offset, chain length, first output point
+  float* out;        // flattened polygons
+  uint32_t* hdr;     // [0] output floats, [1] polygons
+  float* phi_full;   // analytic_phi_full of the fluid
+};
+// The occupancy field and phi_full of mill 0 (one launch), then with `contour` the flattened
+// polygons into sd.out and their length into sd.hdr[0] (a second launch).
+cudaError_t launch_surface(const MillDev* mill, const StepUniform* uni, const SurfDev& sd, bool contour,
+                           cudaStream_t stream);
 // Grid-stage probe over the descriptor's fx[0..nf): mode 0 grid, 1 candidate pairs, 2 neighbours.
 cudaError_t launch_probe(const MillDev* mill, float cell, int mode, uint32_t* result, cudaStream_t stream);
 

@@ -18,8 +18,9 @@ LIB_PATH = os.path.join(LIB_DIR, "libmillgpu.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["mill_kernels.cu", "mill_host.cu", "mill_params.cpp", "mill_noalloc.cu"]
-HEADERS = ["mill_common.cuh", "mill_block.cuh", "mill_grid.cuh", "mill_geom.cuh", "mill_fluid.cuh",
-           "mill_dem.cuh", "mill_replay.cuh", "mill_kernels.h", "mill_params.h"]
+# every header beside the sources (the build is stale when any of them is newer than the library)
+HEADERS = sorted(f for f in os.listdir(os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc"))
+                 if f.endswith((".cuh", ".h")))
 
 # Arithmetic contract: IEEE f32 division and square root, no fused multiply-add contraction in
 # device code (-fmad=false) or host code (-ffp-contract=off), no fast-math.

@@ -34,6 +34,20 @@ def _ptr(a):
     return a.ctypes.data_as(capi.f32p)
 
 
+def unflatten_polygons(flat) -> list:
+    """Inverse of flatten_polygons (surface.rs:420-430): [n_polys, len_0, x, y, ...] to a list of
+    (len_k, 2) float32 arrays."""
+    flat = np.asarray(flat, np.float32)
+    polys, k = [], 1
+    for _ in range(int(flat[0])):
+        n = int(flat[k])
+        polys.append(flat[k + 1:k + 1 + 2 * n].reshape(n, 2).copy())
+        k += 1 + 2 * n
+    if k != len(flat):
+        raise ValueError(f"flattened polygons end at {k}, buffer holds {len(flat)}")
+    return polys
+
+
 @dataclass
 class CouplingImpulses:
     """coupling.rs:37-63"""
@@ -277,6 +291,27 @@ class Simulation:
         out = capi.Metrics()
         self._c(self.lib.metrics(self.h, C.byref(out)))
         return out
+
+    def surface_flat(self) -> np.ndarray:
+        """Simulation::fluid_surface flattened (lib.rs:354-361, surface.rs:233-272 and 420-430):
+        [n_polys, len_0, x, y, ..., len_1, x, y, ...] as float32."""
+        n = C.c_uint32(0)
+        out = np.empty(capi.SURFACE_OUT_CAP, np.float32)
+        self._c(self.lib.fluid_surface(self.h, _ptr(out), len(out), C.byref(n)))
+        return out[:n.value].copy()
+
+    def surface(self) -> list:
+        """The free-surface polygons as a list of (n, 2) float32 arrays (surface.rs:233-272)."""
+        return unflatten_polygons(self.surface_flat())
+
+    def surface_field(self):
+        """build_field's masked occupancy field (MG_SURFACE_GRID^2 floats, row-major in gj) and
+        analytic_phi_full (surface.rs:71-131)."""
+        g = capi.SURFACE_GRID
+        field = np.zeros((g, g), np.float32)
+        phi = C.c_float(0.0)
+        self._c(self.lib.surface_field(self.h, _ptr(field), C.byref(phi)))
+        return field, phi.value
 
     def stress_metrics(self) -> capi.StressMetrics:
         """Simulation::metrics (lib.rs:383-390 over StressAccum::metrics, stress.rs:186-237)."""

@@ -289,6 +289,24 @@ int or_metrics(OrSim* s, MgMetrics* out) {
   metrics_compute(s->sim.balls, s->sim.fluid, s->sim.drum(), s->sim.drum_angle, out);
   return MG_OK;
 }
+int or_fluid_surface(OrSim* s, float* out, uint32_t cap, uint32_t* len) {
+  if (!s || !len) { g_err = "null argument"; return MG_ERR_ARG; }
+  const std::vector<float> flat = surface_extract_flat(s->sim.fluid, s->sim.drum(), s->sim.drum_angle);
+  *len = (uint32_t)flat.size();
+  if (!out) return MG_OK;
+  if (cap < flat.size()) { g_err = "output buffer too small"; return MG_ERR_CAPACITY; }
+  std::copy(flat.begin(), flat.end(), out);
+  return MG_OK;
+}
+int or_surface_field(OrSim* s, float* field, float* phi_full) {
+  if (!s) { g_err = "null argument"; return MG_ERR_ARG; }
+  if (field) {
+    const std::vector<float> f = surface_build_field(s->sim.fluid, s->sim.drum(), s->sim.drum_angle);
+    std::copy(f.begin(), f.end(), field);
+  }
+  if (phi_full) *phi_full = surface_phi_full(s->sim.fluid);
+  return MG_OK;
+}
 int or_mixing_index(OrSim* s, float* out, int* valid) {
   float m = 0.0f;
   *valid = mixing_index(s->sim.fluid, s->sim.drum(), &m) ? 1 : 0;

@@ -445,6 +445,9 @@ struct Simulation {
 
 bool mixing_index(const Fluid& f, const Drum& d, float* out);
 void metrics_compute(const Balls& b, const Fluid& f, const Drum& d, float drum_angle, ::MgMetrics* out);
+float surface_phi_full(const Fluid& f);
+std::vector<float> surface_build_field(const Fluid& f, const Drum& drum, float drum_angle);
+std::vector<float> surface_extract_flat(const Fluid& f, const Drum& drum, float drum_angle);
 uint64_t state_hash(const Balls& b, const Fluid& f, bool extended);
 
 }  // namespace orc
