@@ -321,6 +321,9 @@ int mg_fluid_surface(MgSim* sim, float* out, uint32_t cap, uint32_t* len);
  * counterpart in the reference's public API: build_field is private there; this exposes it for
  * checks against the oracle. */
 int mg_surface_field(MgSim* sim, float* field, float* phi_full);
+/* FluidParticles::densities (pbf.rs:1124-1145) of the current positions: out receives n_fluid
+ * floats. Computed by the mg_metrics launch (which it runs). */
+int mg_fluid_densities(MgSim* sim, float* out);
 /* StressAccum::histogram_rate (stress.rs:174-176), 28 bins per second */
 int mg_stress_histogram_rate(MgSim* sim, double* out28);
 /* stats of the last sub-step taken by any step call */

@@ -267,6 +267,7 @@ SIGNATURES = [
     ("stress_metrics", C.c_int, [vp, P(StressMetrics)]),
     ("metrics", C.c_int, [vp, P(Metrics)]),
     ("fluid_surface", C.c_int, [vp, f32p, C.c_uint32, u32p]),
+    ("fluid_densities", C.c_int, [vp, f32p]),
     ("surface_field", C.c_int, [vp, f32p, f32p]),
     ("seed_value_name", C.c_char_p, [C.c_uint32]),
     ("seed_sweep", C.c_int, [P(Params), P(C.c_uint64), C.c_uint32, C.c_float, C.c_float, P(SeedResult)]),

@@ -1142,6 +1142,20 @@ int mg_surface_field(MgSim* s, float* field, float* phi_full) {
   return MG_OK;
 }
 
+int mg_fluid_densities(MgSim* s, float* out) {
+  if (!s || !out) return fail_global(MG_ERR_ARG, "null argument");
+  // the metrics launch computes FluidParticles::densities into the sub-step scratch
+  int rc = push_state_uniform(s);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(s->md.err, 0, sizeof(uint32_t), s->stream));
+  CK(launch_metrics(s->d_md, s->d_uni, s->d_metrics, s->stream));
+  uint32_t e = 0;
+  if (s->nf) CK(cudaMemcpyAsync(out, s->md.f_tmp, sizeof(float) * s->nf, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(&e, s->md.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (e) return fail(s, MG_ERR_CAPACITY, "device capacity exceeded computing the densities (error bits 0x%x)", e);
+  return MG_OK;
+}
 int mg_stress_histogram_rate(MgSim* s, double* out28) {
   if (!s || !out28) return fail_global(MG_ERR_ARG, "null argument");
   std::memcpy(out28, s->stress.hist_rate, sizeof(double) * MG_SE_BINS);

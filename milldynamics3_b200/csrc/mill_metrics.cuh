@@ -284,21 +284,22 @@ __global__ void __launch_bounds__(1024) metrics_kernel(const MillDev* __restrict
     // fluid density errors (metrics.rs:649-711) on FluidParticles::densities (pbf.rs:1124-1141):
     // each particle's density adds its neighbours in candidate-pair order, which is the order of
     // its neighbour list
+    // (the densities themselves are left in m.f_tmp for mg_fluid_densities)
     const float rest = m.f_rho0;
+    grid_build(m.fx, nf, h, m.gA, hdr, m.err);
+    __shared__ uint32_t n_edges;
+    build_neighbor_lists(m.fx, nf, h, hdr, m.gA, m.nbr_off, m.nbrs, m.cap_edges, m.err, &n_edges);
+    const float mass = m.f_mass;
+    const float self_c = mass * poly6(0.0f, h);
+    float* rho = m.f_tmp;
+    for (uint32_t i = tid(); i < nf; i += nthr()) {
+      const V2 xi(m.fx[i]);
+      float d = self_c;
+      for (uint32_t q = m.nbr_off[i]; q < m.nbr_off[i + 1]; ++q) d += mass * poly6((xi - V2(m.fx[m.nbrs[q]])).len2(), h);
+      rho[i] = d;
+    }
+    __syncthreads();
     if (rest > 0.0f) {
-      grid_build(m.fx, nf, h, m.gA, hdr, m.err);
-      __shared__ uint32_t n_edges;
-      build_neighbor_lists(m.fx, nf, h, hdr, m.gA, m.nbr_off, m.nbrs, m.cap_edges, m.err, &n_edges);
-      const float mass = m.f_mass;
-      const float self_c = mass * poly6(0.0f, h);
-      float* rho = m.f_tmp;
-      for (uint32_t i = tid(); i < nf; i += nthr()) {
-        const V2 xi(m.fx[i]);
-        float d = self_c;
-        for (uint32_t q = m.nbr_off[i]; q < m.nbr_off[i + 1]; ++q) d += mass * poly6((xi - V2(m.fx[m.nbrs[q]])).len2(), h);
-        rho[i] = d;
-      }
-      __syncthreads();
       float mx = 0.0f, cmx = 0.0f;
       for (uint32_t i = tid(); i < nf; i += nthr()) {
         mx = fmax_r(mx, fabsf(rho[i] - rest) / rest);

@@ -304,6 +304,12 @@ class Simulation:
         """The free-surface polygons as a list of (n, 2) float32 arrays (surface.rs:233-272)."""
         return unflatten_polygons(self.surface_flat())
 
+    def fluid_densities(self) -> np.ndarray:
+        """FluidParticles::densities (pbf.rs:1124-1145) of the current positions."""
+        out = np.zeros(max(self.counts()[1], 1), np.float32)
+        self._c(self.lib.fluid_densities(self.h, _ptr(out)))
+        return out[:self.counts()[1]]
+
     def surface_field(self):
         """build_field's masked occupancy field (MG_SURFACE_GRID^2 floats, row-major in gj) and
         analytic_phi_full (surface.rs:71-131)."""

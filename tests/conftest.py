@@ -22,7 +22,6 @@ P = C.POINTER
 ORACLE_EXTRA = [
     ("sim_set_cg_fp64", C.c_int, [C.c_void_p, C.c_int]),
     ("stress_set_debounce_factor", C.c_int, [C.c_void_p, C.c_double]),
-    ("fluid_densities", C.c_int, [C.c_void_p, capi.f32p]),
     ("total_mechanical_energy", C.c_double, [C.c_void_p]),
     ("probe_near", C.c_int, [capi.f32p, C.c_uint32, C.c_float, C.c_float, C.c_float, capi.u32p, C.c_uint32,
                              capi.u32p]),

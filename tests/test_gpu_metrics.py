@@ -66,3 +66,16 @@ def test_metrics_match_mixing_index_and_repeat(device):
     if mi is not None:
         assert a["mixing_index"] == mi
     s.close()
+
+
+@pytest.mark.parametrize("frames", [0, 5])
+def test_device_fluid_densities_match_oracle(device, oracle, frames):
+    out = []
+    for b in (device, oracle):
+        s = Simulation(b, _realtime(b))
+        for _ in range(frames):
+            s.step(1.0 / 60.0)
+        out.append(s.fluid_densities())
+        s.close()
+    assert len(out[0]) == len(out[1]) > 0
+    assert np.array_equal(out[0].view(np.uint32), out[1].view(np.uint32))
