@@ -488,6 +488,23 @@ int mg_server_step(MgServer* server);
 int mg_server_poll(MgServer* server, MgJobUpdate* out, uint32_t cap, uint32_t* n_out);
 int mg_server_stats(MgServer* server, MgServerStats* out);
 
+/* Seed-sweep jobs: the web batch planner's repeat runs (web/src/batch/plan.ts, protocol.ts) as a
+ * job type of the serving loop. A sweep queues one job per seed 1..=n_seeds (the literal numbers,
+ * plan.ts:29-32) of the same Params; each runs batch::run_seed's window (warm-up revolutions,
+ * then measured revolutions, batch.rs:40-107) while other jobs share the launches, and streams
+ * ordinary job updates. The planner's rules are enforced at submission: 1 <= n_seeds <=
+ * MG_SWEEP_MAX_SEEDS, warm-up >= 0, measured revolutions an integer >= 1, a drum speed > 0, and
+ * no coarse-graining (k = 1; plan.ts:13-26, 78-91). mg_server_cancel(sweep_id) cancels every seed. */
+#define MG_SWEEP_MAX_SEEDS 50
+int mg_server_submit_sweep(MgServer* server, const MgParams* p, uint32_t n_seeds, float warmup_revolutions,
+                           float measure_revolutions, uint64_t* sweep_id);
+/* *state: MG_JOB_QUEUED / RUNNING until every seed has finished, then FINISHED (or CANCELLED /
+ * FAILED if a seed was); *seeds_finished counts finished seeds. Once FINISHED, results[n_seeds]
+ * receives each seed's MgSeedResult (seed order) and mean / std_err[MG_SEED_VALUES] their
+ * batch::combine (any of the three may be NULL). */
+int mg_server_sweep_result(MgServer* server, uint64_t sweep_id, MgSeedResult* results, double* mean,
+                           double* std_err, uint32_t* state, uint32_t* seeds_finished);
+
 #ifdef __cplusplus
 }
 #endif

@@ -172,6 +172,7 @@ class ServerStats(_S):
 
 
 SURFACE_GRID = 128  # MG_SURFACE_GRID
+SWEEP_MAX_SEEDS = 50  # MG_SWEEP_MAX_SEEDS
 # most floats mg_fluid_surface can return: 1 + 9 * (2 segments in each of the (G - 1)^2 cells)
 SURFACE_OUT_CAP = 1 + 9 * 2 * (SURFACE_GRID - 1) ** 2
 METRIC_TOE_SHOULDER, METRIC_CENTROID, METRIC_POOL_EXTENT, METRIC_FREE_SURFACE = 0x01, 0x02, 0x04, 0x08
@@ -299,6 +300,9 @@ DEVICE_ONLY = [
     ("server_last_error", C.c_char_p, [vp]),
     ("server_submit", C.c_int, [vp, P(Params), C.c_double, P(C.c_uint64)]),
     ("server_cancel", C.c_int, [vp, C.c_uint64]),
+    ("server_submit_sweep", C.c_int, [vp, P(Params), C.c_uint32, C.c_float, C.c_float, P(C.c_uint64)]),
+    ("server_sweep_result", C.c_int, [vp, C.c_uint64, P(SeedResult), P(C.c_double), P(C.c_double),
+                                      P(C.c_uint32), P(C.c_uint32)]),
     ("server_step", C.c_int, [vp]),
     ("server_poll", C.c_int, [vp, P(JobUpdate), C.c_uint32, u32p]),
     ("server_stats", C.c_int, [vp, P(ServerStats)]),

@@ -1588,6 +1588,14 @@ int mg_sim_footprint(const MgSim* s, uint64_t* device_bytes) {
 // count) and retires the jobs that reached their horizon, freeing their memory for the queue.
 // A job advances exactly as the same mill stepped alone (the same kernels on the same state), so
 // its results do not depend on what else is in the mix.
+struct SeedAcc;  // run_seed's window accumulators (with the grinding statistics below)
+bool seed_window(const MgParams& p, float warmup_revolutions, float measure_revolutions, uint32_t* warm,
+                 uint32_t* meas, double* rev_s);
+SeedAcc* seed_acc_new(const MgParams& p, uint32_t warm, uint32_t meas, double rev_s);
+void seed_acc_free(SeedAcc* a);
+void seed_acc_observe(SeedAcc* a, const MgSim* s, uint32_t frames_done);
+void seed_acc_finish(const SeedAcc* a, const MgSim* s, MgSeedResult* r);
+
 struct MgServerJob {
   uint64_t id = 0;
   MgParams params{};
@@ -1596,6 +1604,16 @@ struct MgServerJob {
   uint64_t bytes = 0;
   bool cancel = false;
   double t_submit = 0.0, t_admit = 0.0, t_first = -1.0;
+  // a seed of a sweep: the sweep's id, the seed's index in it and its run_seed window
+  uint64_t sweep = 0;
+  uint32_t sweep_index = 0;
+  SeedAcc* acc = nullptr;
+};
+
+// A seed-sweep job: one server job per seed, combined when all have finished.
+struct MgServerSweep {
+  uint32_t n_seeds = 0, finished = 0, state = MG_JOB_QUEUED;
+  std::vector<MgSeedResult> results;
 };
 
 struct MgServer {
@@ -1605,6 +1623,7 @@ struct MgServer {
   std::deque<MgServerJob*> queue;
   std::vector<MgServerJob*> active;
   std::vector<MgJobUpdate> pending;
+  std::map<uint64_t, MgServerSweep> sweeps;
   uint64_t next_id = 1, in_use = 0, frames = 0;
   uint32_t finished_total = 0;
   // launch blocks, grown as needed (cap jobs, MAX_SUB sub-steps each)
@@ -1712,6 +1731,19 @@ void retire(MgServer* v, MgServerJob* j, uint32_t state) {
   MgJobUpdate u = job_update(j, state);
   if (j->sim && state == MG_JOB_FINISHED) mg_state_hash(j->sim, 1, &u.state_hash);
   v->pending.push_back(u);
+  if (j->sweep) {
+    MgServerSweep& sw = v->sweeps[j->sweep];
+    if (state == MG_JOB_FINISHED && j->sim && j->acc) {
+      seed_acc_finish(j->acc, j->sim, &sw.results[j->sweep_index]);
+      sw.finished += 1;
+      if (sw.finished == sw.n_seeds && sw.state != MG_JOB_CANCELLED && sw.state != MG_JOB_FAILED)
+        sw.state = MG_JOB_FINISHED;
+    } else if (sw.state != MG_JOB_FAILED) {
+      sw.state = state == MG_JOB_FAILED ? MG_JOB_FAILED : MG_JOB_CANCELLED;
+    }
+    seed_acc_free(j->acc);
+    j->acc = nullptr;
+  }
   if (j->sim) {
     mg_sim_destroy(j->sim);
     v->in_use -= j->bytes;
@@ -1801,8 +1833,81 @@ int mg_server_submit(MgServer* v, const MgParams* p, double horizon_s, uint64_t*
   return MG_OK;
 }
 
+// The web batch planner's repeat runs (web/src/batch/plan.ts:5-33, 78-91; protocol.ts): seeds
+// 1..=n_seeds of the same Params, each batch::run_seed over the same window, then combine.
+int mg_server_submit_sweep(MgServer* v, const MgParams* p, uint32_t n_seeds, float warmup_revolutions,
+                           float measure_revolutions, uint64_t* sweep_id) {
+  if (!v || !p) return fail_global(MG_ERR_ARG, "null argument");
+  std::string e;
+  if (!mgh::params_validate(*p, &e)) return sfail(v, MG_ERR_INVALID_PARAMS, "%s", e.c_str());
+  if (n_seeds < 1 || n_seeds > MG_SWEEP_MAX_SEEDS)
+    return sfail(v, MG_ERR_ARG, "seeds must be from 1 to %u", (unsigned)MG_SWEEP_MAX_SEEDS);
+  if (!(measure_revolutions >= 1.0f) || measure_revolutions != std::floor(measure_revolutions))
+    return sfail(v, MG_ERR_ARG, "measured revolutions must be an integer >= 1");
+  if (!(warmup_revolutions >= 0.0f) || !std::isfinite(warmup_revolutions))
+    return sfail(v, MG_ERR_ARG, "warm-up revolutions must be a number >= 0");
+  if (!(mgh::mill_rpm(p->mill) > 0.0f))
+    return sfail(v, MG_ERR_ARG, "the drum speed is 0; whole-revolution windows are undefined");
+  const float k = mgh::effective_media(*p).scale_factor;
+  if (k > 1.0f)
+    return sfail(v, MG_ERR_ARG,
+                 "coarse-graining is active (k = %.2f): the statistics are meaningless; raise max balls so that k = 1",
+                 k);
+  const uint32_t ns = std::max(mgh::effective_substeps(*p), 1u);
+  if (ns > MAX_SUB) return sfail(v, MG_ERR_ARG, "%u sub-steps per frame, at most %u", ns, MAX_SUB);
+  uint32_t warm = 0, meas = 0;
+  double rev_s = 0.0;
+  if (!seed_window(*p, warmup_revolutions, measure_revolutions, &warm, &meas, &rev_s))
+    return sfail(v, MG_ERR_ARG, "invalid revolutions");
+  const uint64_t id = v->next_id++;
+  MgServerSweep& sw = v->sweeps[id];
+  sw.n_seeds = n_seeds;
+  sw.results.assign(n_seeds, MgSeedResult{});
+  for (uint32_t i = 0; i < n_seeds; ++i) {
+    MgServerJob* j = new MgServerJob();
+    j->id = v->next_id++;
+    j->params = *p;
+    j->params.simulation.seed = i + 1;  // the literal numbers 1..N (plan.ts:29-32)
+    j->n_sub = ns;
+    j->frames_total = warm + meas;
+    j->t_submit = wall_s();
+    j->sweep = id;
+    j->sweep_index = i;
+    j->acc = seed_acc_new(j->params, warm, meas, rev_s);
+    v->queue.push_back(j);
+  }
+  if (sweep_id) *sweep_id = id;
+  return MG_OK;
+}
+
+int mg_server_sweep_result(MgServer* v, uint64_t sweep_id, MgSeedResult* results, double* mean, double* std_err,
+                           uint32_t* state, uint32_t* seeds_finished) {
+  if (!v) return fail_global(MG_ERR_ARG, "null handle");
+  auto it = v->sweeps.find(sweep_id);
+  if (it == v->sweeps.end()) return sfail(v, MG_ERR_ARG, "no sweep %llu", (unsigned long long)sweep_id);
+  const MgServerSweep& sw = it->second;
+  if (state) *state = sw.state;
+  if (seeds_finished) *seeds_finished = sw.finished;
+  if (sw.state != MG_JOB_FINISHED) return MG_OK;
+  if (results) std::memcpy(results, sw.results.data(), sizeof(MgSeedResult) * sw.n_seeds);
+  if (mean && std_err) return mg_seed_combine(sw.results.data(), sw.n_seeds, mean, std_err);
+  return MG_OK;
+}
+
 int mg_server_cancel(MgServer* v, uint64_t job_id) {
   if (!v) return fail_global(MG_ERR_ARG, "null handle");
+  auto sw = v->sweeps.find(job_id);
+  if (sw != v->sweeps.end()) {
+    // every seed of the sweep still queued or running
+    std::vector<uint64_t> ids;
+    for (MgServerJob* j : v->queue)
+      if (j->sweep == job_id) ids.push_back(j->id);
+    for (MgServerJob* j : v->active)
+      if (j->sweep == job_id) ids.push_back(j->id);
+    for (uint64_t id : ids) mg_server_cancel(v, id);
+    if (sw->second.state != MG_JOB_FINISHED) sw->second.state = MG_JOB_CANCELLED;
+    return MG_OK;
+  }
   for (auto it = v->queue.begin(); it != v->queue.end(); ++it) {
     if ((*it)->id == job_id) {
       MgServerJob* j = *it;
@@ -1853,6 +1958,11 @@ int mg_server_step(MgServer* v) {
     j->sim = sim;
     j->bytes = need;
     j->t_admit = wall_s();
+    if (j->acc) {
+      seed_acc_observe(j->acc, sim, 0);  // the window's start when there is no warm-up
+      MgServerSweep& sw = v->sweeps[j->sweep];
+      if (sw.state == MG_JOB_QUEUED) sw.state = MG_JOB_RUNNING;
+    }
     v->in_use += need;
     v->queue.pop_front();
     v->active.push_back(j);
@@ -1944,6 +2054,7 @@ int mg_server_step(MgServer* v) {
     s->last_ctr = o[ns - 1].ctr;
     s->launches += 1;
     j->frames_done += 1;
+    if (j->acc) seed_acc_observe(j->acc, s, j->frames_done);
     if (j->t_first < 0.0) j->t_first = t_end;
     if (j->frames_done >= j->frames_total) {
       retire(v, j, MG_JOB_FINISHED);
@@ -2069,6 +2180,69 @@ const char* const SEED_VALUE_NAMES[MG_SEED_VALUES] = {
 
 }  // namespace
 
+// batch::run_seed's window (batch.rs:40-107) of one seed, fed frame by frame: `warm` frames of
+// warm-up, then `meas` measured frames whose stress scalars are averaged, with the window powers
+// from the cumulative energies and the drift of the wall power per revolution.
+struct SeedAcc {
+  uint32_t warm = 0, meas = 0;
+  double rev_s = 0.0;
+  float k_cg = 1.0f;
+  uint64_t seed = 0;
+  MgStressMetrics start{};
+  double sum[16] = {};
+  std::vector<double> powers;
+};
+
+// Frames of run_seed's warm-up and measured windows (batch.rs:56-62); false when the mill speed
+// or the revolutions are out of range.
+bool seed_window(const MgParams& p, float warmup_revolutions, float measure_revolutions, uint32_t* warm,
+                 uint32_t* meas, double* rev_s) {
+  const double omega = (double)(mgh::mill_rpm(p.mill) * 2.0f * mgh::PI_F / 60.0f);
+  if (omega <= 1e-6 || !(measure_revolutions >= 1.0f && warmup_revolutions >= 0.0f)) return false;
+  *rev_s = 6.283185307179586 / omega;
+  *warm = (uint32_t)std::round((double)warmup_revolutions * *rev_s * 60.0);
+  *meas = (uint32_t)std::max(std::round((double)measure_revolutions * *rev_s * 60.0), 1.0);
+  return true;
+}
+
+SeedAcc* seed_acc_new(const MgParams& p, uint32_t warm, uint32_t meas, double rev_s) {
+  SeedAcc* a = new SeedAcc();
+  a->warm = warm;
+  a->meas = meas;
+  a->rev_s = rev_s;
+  a->seed = p.simulation.seed;
+  a->k_cg = mgh::effective_media(p).scale_factor;
+  a->powers.assign(meas, 0.0);
+  return a;
+}
+void seed_acc_free(SeedAcc* a) { delete a; }
+// Called with the initial state (frames_done 0) and after every frame.
+void seed_acc_observe(SeedAcc* a, const MgSim* s, uint32_t frames_done) {
+  if (frames_done == a->warm) a->start = stress_metrics_of(s);
+  if (frames_done <= a->warm || frames_done > a->warm + a->meas) return;
+  const MgStressMetrics m = stress_metrics_of(s);
+  double v[16];
+  seed_frame_values(m, v);
+  for (int k = 0; k < 16; ++k) a->sum[k] += v[k];
+  a->powers[frames_done - a->warm - 1] = (double)m.wall_power_per_ball_w;
+}
+// The seed's result once its last measured frame has been observed.
+void seed_acc_finish(const SeedAcc* a, const MgSim* s, MgSeedResult* r) {
+  const MgStressMetrics end = stress_metrics_of(s);
+  const double n = (double)a->meas, window_s = n * (double)(1.0f / 60.0f);
+  std::memset(r, 0, sizeof(*r));
+  r->seed = a->seed;
+  r->window_s = window_s;
+  r->coarse_graining_factor = a->k_cg;
+  for (int k = 0; k < 16; ++k) r->values[k] = a->sum[k] / n;
+  r->values[16] = (end.cumulative_specific_energy_j_per_kg - a->start.cumulative_specific_energy_j_per_kg) / window_s;
+  for (int q = 0; q < 6; ++q)
+    r->values[17 + q] =
+        (end.cumulative_effective_energy_per_ball_j[q] - a->start.cumulative_effective_energy_per_ball_j[q]) /
+        window_s;
+  r->power_drift_rel_per_rev = drift_per_rev_of(a->powers.data(), a->meas, a->rev_s * 60.0);
+}
+
 extern "C" {
 
 int mg_stress_metrics(MgSim* s, MgStressMetrics* out) {
@@ -2084,54 +2258,31 @@ const char* mg_seed_value_name(uint32_t k) { return k < MG_SEED_VALUES ? SEED_VA
 int mg_seed_sweep(const MgParams* params, const uint64_t* seeds, uint32_t n_seeds, float warmup_revolutions,
                   float measure_revolutions, MgSeedResult* out) {
   if (!params || n_seeds == 0 || !seeds || !out) return fail_global(MG_ERR_ARG, "null argument or no seeds");
-  const double omega = (double)(mgh::mill_rpm(params->mill) * 2.0f * mgh::PI_F / 60.0f);
-  if (omega <= 1e-6) return fail_global(MG_ERR_ARG, "mill speed must be > 0");
-  if (!(measure_revolutions >= 1.0f && warmup_revolutions >= 0.0f))
-    return fail_global(MG_ERR_ARG, "measure_revolutions must be >= 1 and warmup_revolutions >= 0");
-  const double rev_s = 6.283185307179586 / omega;
-  const uint32_t warm = (uint32_t)std::round((double)warmup_revolutions * rev_s * 60.0);
-  const uint32_t meas = (uint32_t)std::max(std::round((double)measure_revolutions * rev_s * 60.0), 1.0);
+  uint32_t warm = 0, meas = 0;
+  double rev_s = 0.0;
+  if (!seed_window(*params, warmup_revolutions, measure_revolutions, &warm, &meas, &rev_s))
+    return fail_global(MG_ERR_ARG, "mill speed must be > 0, measure_revolutions >= 1 and warmup_revolutions >= 0");
   const float frame_s = 1.0f / 60.0f;
   std::vector<MgParams> ps(n_seeds, *params);
   for (uint32_t i = 0; i < n_seeds; ++i) ps[i].simulation.seed = seeds[i];
   MgBatch* b = nullptr;
   int rc = mg_batch_create(ps.data(), n_seeds, &b);
   if (rc) return rc;
+  std::vector<SeedAcc*> acc(n_seeds);
+  for (uint32_t i = 0; i < n_seeds; ++i) acc[i] = seed_acc_new(ps[i], warm, meas, rev_s);
   if (warm) rc = mg_batch_step_frames(b, warm, frame_s);
-  std::vector<MgStressMetrics> start(n_seeds);
-  for (uint32_t i = 0; i < n_seeds && !rc; ++i) start[i] = stress_metrics_of(b->mills[i]);
-  std::vector<double> sum((size_t)n_seeds * 16, 0.0), powers((size_t)n_seeds * meas);
+  for (uint32_t i = 0; i < n_seeds && !rc; ++i) seed_acc_observe(acc[i], b->mills[i], warm);
   for (uint32_t f = 0; f < meas && !rc; ++f) {
     rc = mg_batch_step_frames(b, 1, frame_s);
-    for (uint32_t i = 0; i < n_seeds && !rc; ++i) {
-      const MgStressMetrics m = stress_metrics_of(b->mills[i]);
-      double v[16];
-      seed_frame_values(m, v);
-      for (int k = 0; k < 16; ++k) sum[(size_t)i * 16 + k] += v[k];
-      powers[(size_t)i * meas + f] = (double)m.wall_power_per_ball_w;
-    }
+    for (uint32_t i = 0; i < n_seeds && !rc; ++i) seed_acc_observe(acc[i], b->mills[i], warm + f + 1);
   }
+  if (!rc)
+    for (uint32_t i = 0; i < n_seeds; ++i) seed_acc_finish(acc[i], b->mills[i], &out[i]);
+  for (SeedAcc* a : acc) seed_acc_free(a);
   if (rc) {
     std::string e = b->err;
     mg_batch_destroy(b);
     return fail_global(rc, "%s", e.c_str());
-  }
-  const double n = (double)meas, window_s = n * (double)frame_s;
-  const float k_cg = mgh::effective_media(*params).scale_factor;
-  for (uint32_t i = 0; i < n_seeds; ++i) {
-    const MgStressMetrics end = stress_metrics_of(b->mills[i]);
-    MgSeedResult& r = out[i];
-    std::memset(&r, 0, sizeof(r));
-    r.seed = seeds[i];
-    r.window_s = window_s;
-    r.coarse_graining_factor = k_cg;
-    for (int k = 0; k < 16; ++k) r.values[k] = sum[(size_t)i * 16 + k] / n;
-    r.values[16] = (end.cumulative_specific_energy_j_per_kg - start[i].cumulative_specific_energy_j_per_kg) / window_s;
-    for (int q = 0; q < 6; ++q)
-      r.values[17 + q] =
-          (end.cumulative_effective_energy_per_ball_j[q] - start[i].cumulative_effective_energy_per_ball_j[q]) /
-          window_s;
-    r.power_drift_rel_per_rev = drift_per_rev_of(&powers[(size_t)i * meas], meas, rev_s * 60.0);
   }
   mg_batch_destroy(b);
   return MG_OK;

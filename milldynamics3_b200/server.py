@@ -49,6 +49,29 @@ class Server:
         self._c(self.lib.server_submit(self.h, C.byref(params), C.c_double(horizon_s), C.byref(jid)))
         return jid.value
 
+    def submit_sweep(self, params: capi.Params, n_seeds: int, warmup_revolutions: float,
+                     measure_revolutions: float) -> int:
+        """A seed-sweep job: seeds 1..n_seeds of `params`, each batch::run_seed over the window,
+        sharing the server's launches with the other jobs (web/src/batch/plan.ts semantics).
+        Returns the sweep id (cancel() takes it too)."""
+        sid = C.c_uint64()
+        self._c(self.lib.server_submit_sweep(self.h, C.byref(params), n_seeds, C.c_float(warmup_revolutions),
+                                             C.c_float(measure_revolutions), C.byref(sid)))
+        return sid.value
+
+    def sweep_result(self, sweep_id: int, n_seeds: int):
+        """(state, seeds finished, per-seed SeedResults, mean, std_err); the last three are None
+        until the sweep has FINISHED."""
+        res = (capi.SeedResult * n_seeds)()
+        mean = (C.c_double * capi.SEED_VALUES)()
+        se = (C.c_double * capi.SEED_VALUES)()
+        st, done = C.c_uint32(), C.c_uint32()
+        self._c(self.lib.server_sweep_result(self.h, C.c_uint64(sweep_id), res, mean, se, C.byref(st),
+                                             C.byref(done)))
+        if st.value != capi.JOB_FINISHED:
+            return st.value, done.value, None, None, None
+        return st.value, done.value, [r.copy() for r in res], list(mean), list(se)
+
     def cancel(self, job_id: int):
         self._c(self.lib.server_cancel(self.h, C.c_uint64(job_id)))
 

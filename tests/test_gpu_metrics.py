@@ -79,3 +79,15 @@ def test_device_fluid_densities_match_oracle(device, oracle, frames):
         s.close()
     assert len(out[0]) == len(out[1]) > 0
     assert np.array_equal(out[0].view(np.uint32), out[1].view(np.uint32))
+
+
+def test_device_metrics_json_matches_oracle(device, oracle):
+    from milldynamics3_b200 import wire
+    out = []
+    for b in (device, oracle):
+        s = Simulation(b, _realtime(b))
+        for _ in range(4):
+            s.step(1.0 / 60.0)
+        out.append(wire.metrics_to_json(s))
+        s.close()
+    assert out[0] == out[1]

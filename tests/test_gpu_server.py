@@ -108,3 +108,61 @@ def test_admission_waits_for_memory_and_cancel(device):
         assert final[jid].state_hash == _alone(device, ps[k], 2)[0], f"job {k}"
     assert server.stats().device_bytes_in_use == 0
     server.close()
+
+
+def _run_until_sweep_done(srv, sid, n, max_steps=5000):
+    for _ in range(max_steps):
+        st, done, res, mean, se = srv.sweep_result(sid, n)
+        if st not in (capi.JOB_QUEUED, capi.JOB_RUNNING):
+            return st, done, res, mean, se
+        srv.step()
+        srv.poll()
+    raise AssertionError("sweep did not finish")
+
+
+def test_sweep_job_matches_seed_sweep_and_oracle(device, oracle):
+    from milldynamics3_b200 import seeds
+    p = device.preset(device.params_default(), "realtime")
+    srv = Server(device)
+    other = srv.submit(mix_params(device, 1, seed=9)[0][0], 0.5)   # an ordinary job in the same launches
+    sid = srv.submit_sweep(p, 3, 0.25, 1.0)
+    st, done, res, mean, se = _run_until_sweep_done(srv, sid, 3)
+    assert st == capi.JOB_FINISHED and done == 3 and other > 0
+    ref = seeds.run_seeds(device, p, [1, 2, 3], 0.25, 1.0)
+    for r, d in zip(res, ref):
+        assert r.seed == d.seed and r.window_s == d.window_s
+        assert list(r.values) == d.values and r.power_drift_rel_per_rev == d.power_drift_rel_per_rev
+    po = oracle.preset(oracle.params_default(), "realtime")
+    assert list(res[0].values) == seeds.run_seed(oracle, po, 1, 0.25, 1.0).values
+    c = seeds.combine(device, ref)
+    assert mean == c.mean and se == c.std_err
+
+
+def test_sweep_job_rules_and_cancel(device):
+    from milldynamics3_b200.sim import MillError
+    srv = Server(device)
+    p = device.preset(device.params_default(), "realtime")
+    for bad in [(0, 0.0, 1.0), (capi.SWEEP_MAX_SEEDS + 1, 0.0, 1.0), (2, -1.0, 1.0), (2, 0.0, 1.5), (2, 0.0, 0.0)]:
+        with pytest.raises(MillError):
+            srv.submit_sweep(p, *bad)
+    q = device.params_default()
+    q.mill.speed_value = 0.0
+    with pytest.raises(MillError):
+        srv.submit_sweep(q, 2, 0.0, 1.0)
+    cg = device.params_default()
+    cg.mill.diameter_m = 1.0
+    cg.media.ball_diameter_m = 0.02
+    cg.simulation.max_balls = 300
+    cg.simulation.coarse_graining_mode = capi.CG_AUTO
+    device.validate(cg)
+    if device.derived(cg).eff_scale_factor > 1.0:
+        with pytest.raises(MillError):
+            srv.submit_sweep(cg, 2, 0.0, 1.0)
+    sid = srv.submit_sweep(p, 2, 0.0, 1.0)
+    srv.step()
+    srv.cancel(sid)
+    for _ in range(3):
+        srv.step()
+    st, done, res, _, _ = srv.sweep_result(sid, 2)
+    assert st == capi.JOB_CANCELLED and res is None
+    assert srv.stats().active == 0
