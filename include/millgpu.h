@@ -369,7 +369,9 @@ int mg_probe_neighbor_lists(const float* xy, uint32_t n, float h, uint32_t* offs
  * is one fixed static device array (at most 16384 points per call; a larger n returns
  * MG_ERR_CAPACITY). Calls on one device share that scratch and must not overlap (issue them on
  * one stream). The first call on a device resolves the scratch address; make it before capturing
- * a stream. */
+ * a stream. The address is kept for the life of the process and belongs to the device's primary
+ * context (the CUDA runtime's): do not call cudaDeviceReset between calls, and do not call it with
+ * another context current on the device. */
 int mg_neighbor_lists_noalloc(const float* xy_dev, uint32_t n, float h, uint32_t* offsets_dev, uint32_t* nbrs_dev,
                               uint32_t cap, uint32_t* n_edges_dev, uint32_t* status_dev, void* stream);
 /* neighbour CSR / ball pair list of the last fluid / ball sub-step taken on this handle */
@@ -504,6 +506,11 @@ int mg_server_submit_sweep(MgServer* server, const MgParams* p, uint32_t n_seeds
  * batch::combine (any of the three may be NULL). */
 int mg_server_sweep_result(MgServer* server, uint64_t sweep_id, MgSeedResult* results, double* mean,
                            double* std_err, uint32_t* state, uint32_t* seeds_finished);
+/* Forgets a sweep's record (read its result first): seeds still queued or running are cancelled,
+ * and the id is unknown afterwards. When one seed fails, the sweep is FAILED and its other seeds
+ * leave without this call (queued ones at the next admission, running ones before the next
+ * frame). */
+int mg_server_sweep_release(MgServer* server, uint64_t sweep_id);
 
 #ifdef __cplusplus
 }

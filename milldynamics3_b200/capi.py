@@ -303,6 +303,7 @@ DEVICE_ONLY = [
     ("server_submit_sweep", C.c_int, [vp, P(Params), C.c_uint32, C.c_float, C.c_float, P(C.c_uint64)]),
     ("server_sweep_result", C.c_int, [vp, C.c_uint64, P(SeedResult), P(C.c_double), P(C.c_double),
                                       P(C.c_uint32), P(C.c_uint32)]),
+    ("server_sweep_release", C.c_int, [vp, C.c_uint64]),
     ("server_step", C.c_int, [vp]),
     ("server_poll", C.c_int, [vp, P(JobUpdate), C.c_uint32, u32p]),
     ("server_stats", C.c_int, [vp, P(ServerStats)]),

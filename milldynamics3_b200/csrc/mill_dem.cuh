@@ -56,7 +56,7 @@ __device__ __forceinline__ int impact_energy_bin(float e) {
 
 // dem.rs:253-261 f32 mechanical energy, summed in ball order (three adds per ball); called by
 // warp 0, result in every lane
-__device__ float mech_energy_seq(const MillDev& m, const float2* X, const float2* V, const float* OM) {
+static __device__ float mech_energy_seq(const MillDev& m, const float2* X, const float2* V, const float* OM) {
   const uint32_t lane = threadIdx.x & 31u;
   float e = 0.0f;
   for (uint32_t c = 0; c < m.nb; c += 32) {
@@ -81,7 +81,7 @@ __device__ float mech_energy_seq(const MillDev& m, const float2* X, const float2
   return e;
 }
 
-__device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, MgImpactRecord* impacts,
+static __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, MgImpactRecord* impacts,
                          uint32_t* err, DemShared& S, unsigned char* dsm) {
   const uint32_t n = m.nb;
   const float dt = U.dt;

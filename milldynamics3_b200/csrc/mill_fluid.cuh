@@ -35,7 +35,7 @@ __device__ __forceinline__ float fluid_vmax(const StepUniform& U) {
 }
 
 // pbf.rs:924-926: 0.5 m sum |v|^2 in f64, summed in particle order.
-__device__ double kinetic_energy_seq(const float2* v, uint32_t n, float mass, FluidShared& S) {
+static __device__ double kinetic_energy_seq(const float2* v, uint32_t n, float mass, FluidShared& S) {
   if (tid() < 32) {
     double s = warp_ordered_sum(0.0, n, [&](uint32_t i, double& t) { t = (double)V2(v[i]).len2(); return true; });
     if (tid() == 0) S.dscal[7] = 0.5 * (double)mass * s;
@@ -47,7 +47,7 @@ __device__ double kinetic_energy_seq(const float2* v, uint32_t n, float mass, Fl
 }
 
 // pbf.rs:292-294 dot in the reference's sequential f32 order, or in f64 (deterministic tree).
-__device__ double block_dot(const float2* a, const float2* b, uint32_t len, bool fp64, FluidShared& S) {
+static __device__ double block_dot(const float2* a, const float2* b, uint32_t len, bool fp64, FluidShared& S) {
   if (fp64) {
     double acc = 0.0;
     for (uint32_t e = tid(); e < len; e += nthr())
@@ -58,7 +58,7 @@ __device__ double block_dot(const float2* a, const float2* b, uint32_t len, bool
 }
 
 // pbf.rs:738-744 residual norm sqrt(sum inv_diag |r|^2), sequential f32 or f64.
-__device__ double block_res_norm(const float2* r, const float* inv, uint32_t len, bool fp64, FluidShared& S) {
+static __device__ double block_res_norm(const float2* r, const float* inv, uint32_t len, bool fp64, FluidShared& S) {
   if (fp64) {
     double acc = 0.0;
     for (uint32_t e = tid(); e < len; e += nthr())
@@ -149,7 +149,7 @@ __device__ __forceinline__ LinkEval link_wall(const MillDev& m, const StepUnifor
 // Rows t0, t0 + stride, ... of the joint-system operator of pbf.rs:703-737 applied to xx, written
 // to out: fluid rows 0..n-1 (Laplacian, then the boundary groups), then ball rows n..n+nb-1
 // (linear and angular).
-__device__ void joint_apply_rows(const MillDev& m, float dt, const float2* xx, float2* out, uint32_t t0,
+static __device__ void joint_apply_rows(const MillDev& m, float dt, const float2* xx, float2* out, uint32_t t0,
                                  uint32_t stride) {
   const uint32_t n = m.nf, nb = m.nb;
   const float mass = m.f_mass;
@@ -216,7 +216,7 @@ __device__ void joint_apply_rows(const MillDev& m, float dt, const float2* xx, f
 }
 
 // The joint-system operator over all of the mill's blocks (all rows written on return).
-__device__ void joint_apply(const MillDev& m, float dt, const float2* xx, float2* out) {
+static __device__ void joint_apply(const MillDev& m, float dt, const float2* xx, float2* out) {
   wide_phase(m, WIDE_JOINT_APPLY, nullptr, xx, out, [&](uint32_t w0, uint32_t nw) {
     joint_apply_rows(m, dt, xx, out, w0 * 32u + (tid() & 31u), nw * 32u);
   });
@@ -224,7 +224,7 @@ __device__ void joint_apply(const MillDev& m, float dt, const float2* xx, float2
 
 // Rows t0, t0 + stride, ... of the joint solve's set-up (pbf.rs:641-700): the start vector x, the
 // right-hand side and the Jacobi diagonal, fluid rows then ball rows.
-__device__ void cg_setup_rows(const MillDev& m, float dt, uint32_t t0, uint32_t stride) {
+static __device__ void cg_setup_rows(const MillDev& m, float dt, uint32_t t0, uint32_t stride) {
   const uint32_t n = m.nf, nb = m.nb;
   const float mass = m.f_mass;
   const float2* V = m.fv;
@@ -272,7 +272,7 @@ __device__ void cg_setup_rows(const MillDev& m, float dt, uint32_t t0, uint32_t 
 // Step 3.6b adhesion per ball (pbf.rs:1540-1602): candidates of each boundary point in
 // for_each_near order, 32 at a time, merged per fluid particle in first-seen order; the ball's
 // impulse and its items' velocity changes (item_v) and count (item_n).
-__device__ void adhesion_balls(const MillDev& m, const StepUniform& U, const GridHdr& hA, uint32_t w0, uint32_t nw) {
+static __device__ void adhesion_balls(const MillDev& m, const StepUniform& U, const GridHdr& hA, uint32_t w0, uint32_t nw) {
   const uint32_t nb = m.nb, count_pb = U.boundary_count;
   const float h = m.f_h, rho0 = m.f_rho0, mass = m.f_mass, dt = U.dt;
   const float2* X = m.fx;
@@ -364,7 +364,7 @@ __device__ void adhesion_balls(const MillDev& m, const StepUniform& U, const Gri
 
 // Boundary groups per ball (pbf.rs:2159-2232) on the fresh h-grid: candidates of each boundary
 // point merged per fluid particle in first-seen order; the ball's group count in g_off[b].
-__device__ void group_balls(const MillDev& m, const StepUniform& U, const GridHdr& hB, uint32_t w0, uint32_t nw) {
+static __device__ void group_balls(const MillDev& m, const StepUniform& U, const GridHdr& hB, uint32_t w0, uint32_t nw) {
   const uint32_t nb = m.nb, count_pb = U.boundary_count;
   const float h = m.f_h;
   const float2* X = m.fx;
@@ -431,7 +431,7 @@ __device__ void group_balls(const MillDev& m, const StepUniform& U, const GridHd
 // compaction, then the wall link, each film evaluated once; ball i's links go to its slots
 // [i K, i K + K) of the record scratch and its count to l_off[i]. Returns the thread's part of
 // the count of links in range.
-__device__ uint32_t link_balls(const MillDev& m, const StepUniform& U, const GridHdr& hBall, uint32_t w0, uint32_t nw) {
+static __device__ uint32_t link_balls(const MillDev& m, const StepUniform& U, const GridHdr& hBall, uint32_t w0, uint32_t nw) {
   const uint32_t nb = m.nb;
   const float h = m.f_h, dt = U.dt;
   uint32_t* err = m.err;
@@ -497,7 +497,7 @@ __device__ uint32_t link_balls(const MillDev& m, const StepUniform& U, const Gri
 // Drag item lists per ball (pbf.rs:1794-1822): fluid particles within r + h of the ball centre in
 // for_each_near order, with their offsets and weights (item_j / item_v / item_w, count item_n).
 // Returns the thread's part of the item count.
-__device__ uint32_t drag_item_balls(const MillDev& m, const GridHdr& hB, uint32_t w0, uint32_t nw) {
+static __device__ uint32_t drag_item_balls(const MillDev& m, const GridHdr& hB, uint32_t w0, uint32_t nw) {
   const uint32_t nb = m.nb;
   const float h = m.f_h;
   const float2* X = m.fx;
@@ -545,7 +545,7 @@ __device__ uint32_t drag_item_balls(const MillDev& m, const GridHdr& hB, uint32_
 // Buoyancy item lists per ball (pbf.rs:2042-2060) on the stale step-2 grid: fluid particles with a
 // positive poly6 weight in for_each_near order, their weights, and the local density (item_v[0]).
 // Returns the thread's part of the item count.
-__device__ uint32_t buoyancy_item_balls(const MillDev& m, const GridHdr& hA, uint32_t w0, uint32_t nw) {
+static __device__ uint32_t buoyancy_item_balls(const MillDev& m, const GridHdr& hA, uint32_t w0, uint32_t nw) {
   const uint32_t nb = m.nb;
   const float h = m.f_h, mass = m.f_mass;
   const float2* X = m.fx;
@@ -589,7 +589,7 @@ __device__ uint32_t buoyancy_item_balls(const MillDev& m, const GridHdr& hA, uin
 // The drag sweep's per-ball quantities that read only the item geometry (pbf.rs:1845-1905), for
 // the balls w0, w0 + nw, ...: entrained mass and inertia, centroid and the s-gate sums, summed in
 // item order; written to drag_pre[8 b ..] (mass, inertia, centroid x, y, s_acc, s_scale).
-__device__ void drag_pre_balls(const MillDev& m, uint32_t w0, uint32_t nw) {
+static __device__ void drag_pre_balls(const MillDev& m, uint32_t w0, uint32_t nw) {
   const uint32_t nb = m.nb, lane = tid() & 31u;
   const float mass = m.f_mass;
   for (uint32_t b = w0; b < nb; b += nw) {
@@ -657,7 +657,7 @@ __device__ void drag_pre_balls(const MillDev& m, uint32_t w0, uint32_t nw) {
   }
 }
 
-__device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err, FluidShared& S,
+static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err, FluidShared& S,
                            unsigned char* dsm) {
   uint32_t* done = m.ball_done;  // completion flags of the per-ball sweeps (moved to shared below)
   const uint32_t n = m.nf, nb = m.nb;

@@ -310,16 +310,25 @@ __device__ __forceinline__ void warp_near_multi(const GridHdr& hdr, const GridBu
 // The cells a point's neighbour list visits, in the order build_neighbor_lists (pbf.rs:262-288)
 // produces: the forward-offset sweep of for_each_candidate_pair (grid.rs:291-362) reaches a point
 // in cell C from (-1,-1), (-1,0), (0,-1) before C's own pairs, then C's targets (+1,0), (+1,+1),
-// (0,+1), (-1,+1), and finally from (+1,-1). Keys never saturate here (grid_build flags that).
+// (0,+1), (-1,+1), and finally from (+1,-1). A key at the edge of the i32 range (grid_build sets
+// ERR_CELLS then) saturates instead of wrapping, and a stencil cell that saturates onto one already
+// visited is not visited again, as in for_each_near.
 __constant__ int STENCIL_DX[9] = {-1, -1, 0, 0, 1, 1, 0, -1, 1};
 __constant__ int STENCIL_DY[9] = {-1, 0, -1, 0, 0, 1, 1, 1, -1};
 
 template <class F>
 __device__ __forceinline__ void for_each_stencil_neighbor(const GridHdr& hdr, const GridBuf& gb, uint32_t self,
                                                           int2 c, F f) {
+  // only a key within one cell of the i32 range's ends can saturate
+  const bool edge = c.x <= INT32_MIN + 1 || c.x >= INT32_MAX - 1 || c.y <= INT32_MIN + 1 || c.y >= INT32_MAX - 1;
   for (int q = 0; q < 9; ++q) {
     uint32_t s, e;
-    if (!cell_range(hdr, gb, make_int2(c.x + STENCIL_DX[q], c.y + STENCIL_DY[q]), s, e)) continue;
+    const int2 k = make_int2(sat_add(c.x, STENCIL_DX[q]), sat_add(c.y, STENCIL_DY[q]));
+    bool dup = false;
+    if (edge)
+      for (int u = 0; u < q; ++u)
+        dup = dup || key_eq(k, make_int2(sat_add(c.x, STENCIL_DX[u]), sat_add(c.y, STENCIL_DY[u])));
+    if (dup || !cell_range(hdr, gb, k, s, e)) continue;
     for (uint32_t a = s; a < e; ++a) {
       uint32_t j = gb.indices[a];
       if (j != self) f(j);

@@ -180,7 +180,10 @@ int fail(MgSim* s, int code, const char* fmt, ...) {
 
 uint32_t cap_items_for() { return 256; }
 
-// Sizes the device arena for nf fluid particles and nb balls (capacities documented in DESIGN.md).
+// Sizes the device arena for nf fluid particles and nb balls. Capacities: fluid edges 64 nf + 1024,
+// ball pairs 64 nb + 1024, boundary groups 256 nb, squeeze links nb min(nb + 1, 512) + 1024,
+// 256 coupling items per ball, 4 nb + 256 impact records per sub-step, up to MAX_SUB sub-steps per
+// launch; a bound that is exceeded sets its ERR_* bit and the call returns MG_ERR_CAPACITY.
 int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
   if (s->dmem && nf <= s->cap_nf && nb <= s->cap_nb) {
     s->nf = nf;
@@ -1731,8 +1734,9 @@ void retire(MgServer* v, MgServerJob* j, uint32_t state) {
   MgJobUpdate u = job_update(j, state);
   if (j->sim && state == MG_JOB_FINISHED) mg_state_hash(j->sim, 1, &u.state_hash);
   v->pending.push_back(u);
-  if (j->sweep) {
-    MgServerSweep& sw = v->sweeps[j->sweep];
+  auto sit = j->sweep ? v->sweeps.find(j->sweep) : v->sweeps.end();
+  if (sit != v->sweeps.end()) {
+    MgServerSweep& sw = sit->second;
     if (state == MG_JOB_FINISHED && j->sim && j->acc) {
       seed_acc_finish(j->acc, j->sim, &sw.results[j->sweep_index]);
       sw.finished += 1;
@@ -1741,6 +1745,16 @@ void retire(MgServer* v, MgServerJob* j, uint32_t state) {
     } else if (sw.state != MG_JOB_FAILED) {
       sw.state = state == MG_JOB_FAILED ? MG_JOB_FAILED : MG_JOB_CANCELLED;
     }
+    if (state != MG_JOB_FINISHED) {
+      // the sweep cannot finish any more: its other seeds leave too (queued ones at the next
+      // admission, running ones before the next frame) instead of holding slots and memory
+      for (MgServerJob* o : v->queue)
+        if (o->sweep == j->sweep) o->cancel = true;
+      for (MgServerJob* o : v->active)
+        if (o->sweep == j->sweep) o->cancel = true;
+    }
+  }
+  if (j->acc) {
     seed_acc_free(j->acc);
     j->acc = nullptr;
   }
@@ -1894,6 +1908,18 @@ int mg_server_sweep_result(MgServer* v, uint64_t sweep_id, MgSeedResult* results
   return MG_OK;
 }
 
+int mg_server_sweep_release(MgServer* v, uint64_t sweep_id) {
+  if (!v) return fail_global(MG_ERR_ARG, "null handle");
+  auto it = v->sweeps.find(sweep_id);
+  if (it == v->sweeps.end()) return sfail(v, MG_ERR_ARG, "no sweep %llu", (unsigned long long)sweep_id);
+  for (MgServerJob* j : v->queue)
+    if (j->sweep == sweep_id) j->cancel = true;
+  for (MgServerJob* j : v->active)
+    if (j->sweep == sweep_id) j->cancel = true;
+  v->sweeps.erase(it);
+  return MG_OK;
+}
+
 int mg_server_cancel(MgServer* v, uint64_t job_id) {
   if (!v) return fail_global(MG_ERR_ARG, "null handle");
   auto sw = v->sweeps.find(job_id);
@@ -1936,6 +1962,11 @@ int mg_server_step(MgServer* v) {
   // admission, oldest first, by the device bytes each job's arena needs
   while (!v->queue.empty() && v->active.size() < v->cfg.max_active) {
     MgServerJob* j = v->queue.front();
+    if (j->cancel) {  // a seed of a sweep that failed or was released
+      v->queue.pop_front();
+      retire(v, j, MG_JOB_CANCELLED);
+      continue;
+    }
     MgSim* sim = nullptr;
     int rc = create_sim(&j->params, nullptr, 0, &sim, v->stream);
     if (!rc) rc = check_materials(sim);
@@ -1960,8 +1991,8 @@ int mg_server_step(MgServer* v) {
     j->t_admit = wall_s();
     if (j->acc) {
       seed_acc_observe(j->acc, sim, 0);  // the window's start when there is no warm-up
-      MgServerSweep& sw = v->sweeps[j->sweep];
-      if (sw.state == MG_JOB_QUEUED) sw.state = MG_JOB_RUNNING;
+      auto sit = v->sweeps.find(j->sweep);
+      if (sit != v->sweeps.end() && sit->second.state == MG_JOB_QUEUED) sit->second.state = MG_JOB_RUNNING;
     }
     v->in_use += need;
     v->queue.pop_front();

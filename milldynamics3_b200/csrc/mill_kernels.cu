@@ -1,87 +1,15 @@
 // Kernels of the B200 mill sub-step. One thread block owns one mill for the whole launch
 // ("mill block"): it runs `n_sub` coupled sub-steps back to back with the mill's state resident in
 // HBM/L2, so a batch of mills is one launch with gridDim = number of mills and a plain single mill
-// is the same launch with one block.
-#include "mill_dem.cuh"
-#include "mill_fluid.cuh"
+// is the same launch with one block. The sub-step kernel itself is in mill_substeps.cuh
+// (instantiated in mill_substeps_512.cu / mill_substeps_1024.cu); this file holds its dispatch and
+// the grid probe, impact packing, metrics and free-surface kernels.
+#include "mill_grid.cuh"
 #include "mill_kernels.h"
 #include "mill_metrics.cuh"
 #include "mill_surface.cuh"
 
 namespace mg {
-
-// n_sub is the sub-step stride of `angles`; mill b runs n_sub_of[b] sub-steps when n_sub_of is
-// given (a batch of mills with different sub-step counts), else n_sub. Two instantiations: up to
-// 512 threads per block (128 registers a thread) and up to 1024 (64 registers, more warps for the
-// per-ball stages); the results do not depend on the block size. With helpers > 0 the launch runs
-// one mill: block 0 is the mill's block and blocks 1..helpers take shares of its per-ball stages
-// (mill_wide.cuh); the results do not depend on the number of blocks either.
-template <int MAX_THREADS>
-__global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDev* __restrict__ mills,
-                                                                    StepUniform* uni,
-                                                                    const SubAngles* __restrict__ angles,
-                                                                    uint32_t n_sub,
-                                                                    const uint32_t* __restrict__ n_sub_of,
-                                                                    uint32_t helpers) {
-  __shared__ MillDev m;
-  __shared__ FluidShared fs;
-  __shared__ DemShared ds;
-  extern __shared__ __align__(16) unsigned char dsm[];  // staged ball state (24 bytes per ball)
-  const uint32_t mill = helpers ? 0u : blockIdx.x;
-  if (threadIdx.x == 0) {
-    m = mills[mill];
-    m.helpers = helpers;
-    if (blockIdx.x == 0 || helpers == 0) *m.err = 0;
-    g_wide_seq = 0;
-  }
-  __syncthreads();
-  if (helpers && blockIdx.x > 0) {
-    wide_helper(m, [&](uint32_t phase, const GridHdr& hdr, const float2* vin, float2* vout, uint32_t w0,
-                       uint32_t nw) -> uint32_t {
-      const StepUniform& U = uni[0];
-      const uint32_t t0 = w0 * 32u + (threadIdx.x & 31u), stride = nw * 32u;
-      if (phase == WIDE_ADHESION) adhesion_balls(m, U, hdr, w0, nw);
-      else if (phase == WIDE_GROUPS) group_balls(m, U, hdr, w0, nw);
-      else if (phase == WIDE_LINKS) return link_balls(m, U, hdr, w0, nw);
-      else if (phase == WIDE_DRAG_ITEMS) return drag_item_balls(m, hdr, w0, nw);
-      else if (phase == WIDE_BUOYANCY_ITEMS) return buoyancy_item_balls(m, hdr, w0, nw);
-      else if (phase == WIDE_CG_SETUP) cg_setup_rows(m, U.dt, t0, stride);
-      else if (phase == WIDE_JOINT_APPLY) joint_apply_rows(m, U.dt, vin, vout, t0, stride);
-      else if (phase == WIDE_DRAG_PRE) drag_pre_balls(m, w0, nw);
-      return 0u;
-    });
-    return;
-  }
-  const uint32_t my_sub = n_sub_of ? n_sub_of[mill] : n_sub;
-  for (uint32_t s = 0; s < my_sub; ++s) {
-    StepUniform& U = uni[mill];
-    StepOut& out = m.out[s];
-    if (threadIdx.x == 0) {
-      const SubAngles& a = angles[(size_t)mill * n_sub + s];
-      U.drum_angle = a.drum_angle;
-      U.drum_angle_next = a.drum_angle_next;
-      U.dt = a.dt;
-      U.to_local_next = a.to_local_next;
-      U.to_world_next = a.to_world_next;
-      U.to_local0 = a.to_local0;
-      memset(&out.ctr, 0, sizeof(out.ctr));
-      memset(out.stage, 0, sizeof(out.stage));
-      g_stage_last = clock64();
-    }
-    __syncthreads();
-    if (*m.err) break;
-    // Without the fluid half, imp/ang hold the caller's external impulses (DEM-only entry point).
-    if (U.run_fluid) fluid_step(m, U, out, m.err, fs, dsm);
-    __syncthreads();
-    if (*m.err) break;
-    if (U.run_dem) dem_step(m, U, out, m.impacts + (size_t)s * m.cap_impacts, m.err, ds, dsm);
-    __syncthreads();
-    if (threadIdx.x == 0) out.stage[14] = out.stage[15] + out.stage[16] + out.stage[17] + out.stage[18] + out.stage[20] + out.stage[21] + out.stage[22] + out.stage[30];
-    if (threadIdx.x == 0) out.err = *m.err;
-    __syncthreads();
-  }
-  wide_exit(m);
-}
 
 // Grid-stage probe: builds the grid of caller points and, per `mode`, leaves the grid (0), the
 // candidate pairs (1) or the neighbour CSR (2) in the descriptor's buffers.
@@ -116,23 +44,10 @@ cudaError_t launch_substeps(const MillDev* mills, uint32_t n_mills, StepUniform*
                             uint32_t n_sub, const uint32_t* n_sub_of, uint32_t threads, size_t smem_bytes,
                             cudaStream_t stream, uint32_t mill_blocks) {
   if (threads == 0 || threads > MAX_BLOCK_THREADS) threads = DEFAULT_BLOCK_THREADS;
-  auto kernel = threads > 512 ? mill_substeps_kernel<MAX_BLOCK_THREADS> : mill_substeps_kernel<512>;
-  // (the opt-in is needed whenever static plus dynamic shared memory passes 48 KB)
-  if (smem_bytes > 0) {
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
-    if (e != cudaSuccess) return e;
-  }
-  uint32_t helpers = n_mills == 1 && mill_blocks > 1 ? min(mill_blocks, MAX_MILL_BLOCKS) - 1u : 0u;
-  if (helpers) {
-    // all of the mill's blocks wait for one another, so they must be resident together
-    void* args[] = {(void*)&mills, (void*)&uni, (void*)&angles, (void*)&n_sub, (void*)&n_sub_of, (void*)&helpers};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)kernel, dim3(1u + helpers), dim3(threads), args,
-                                                smem_bytes, stream);
-    if (e != cudaSuccess) return e;
-    return cudaGetLastError();
-  }
-  kernel<<<n_mills, threads, smem_bytes, stream>>>(mills, uni, angles, n_sub, n_sub_of, 0u);
-  return cudaGetLastError();
+  if (threads > 512)
+    return launch_substeps_1024(mills, n_mills, uni, angles, n_sub, n_sub_of, threads, smem_bytes, stream,
+                                mill_blocks);
+  return launch_substeps_512(mills, n_mills, uni, angles, n_sub, n_sub_of, threads, smem_bytes, stream, mill_blocks);
 }
 
 // One block per mill: appends the mill's impact records (sub-step order) to the packed buffer.

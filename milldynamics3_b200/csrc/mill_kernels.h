@@ -15,6 +15,13 @@ namespace mg {
 cudaError_t launch_substeps(const MillDev* mills, uint32_t n_mills, StepUniform* uni, const SubAngles* angles,
                             uint32_t n_sub, const uint32_t* n_sub_of, uint32_t threads, size_t smem_bytes,
                             cudaStream_t stream, uint32_t mill_blocks = 1);
+// The two instantiations behind launch_substeps (blocks of up to 512 and up to 1024 threads).
+cudaError_t launch_substeps_512(const MillDev* mills, uint32_t n_mills, StepUniform* uni, const SubAngles* angles,
+                                uint32_t n_sub, const uint32_t* n_sub_of, uint32_t threads, size_t smem_bytes,
+                                cudaStream_t stream, uint32_t mill_blocks);
+cudaError_t launch_substeps_1024(const MillDev* mills, uint32_t n_mills, StepUniform* uni, const SubAngles* angles,
+                                 uint32_t n_sub, const uint32_t* n_sub_of, uint32_t threads, size_t smem_bytes,
+                                 cudaStream_t stream, uint32_t mill_blocks);
 // Packs the impact records of n_mills mills after a launch: mill b's records of its sub-steps
 // 0..n_sub_of[b]-1 (StepOut::n_impacts each, at most cap_impacts) are appended in sub-step order
 // at an offset taken from *cursor (one atomic per mill); table[b] = {offset, count}. Records that

@@ -56,7 +56,7 @@ __device__ uint32_t met_compact(uint32_t n, uint32_t* flags, T* dst, Pred pred, 
 
 // Stable ascending sort of src[0..k) into dst (sort_by(partial_cmp): equal values, -0.0 and 0.0
 // included, keep their order), by rank counting.
-__device__ void met_rank_sort(const float* src, float* dst, uint32_t k) {
+static __device__ void met_rank_sort(const float* src, float* dst, uint32_t k) {
   for (uint32_t i = tid(); i < k; i += nthr()) {
     const float a = src[i];
     uint32_t r = 0;
@@ -70,7 +70,7 @@ __device__ void met_rank_sort(const float* src, float* dst, uint32_t k) {
 }
 
 // metrics.rs:292-307 over sorted angles a[0..n), n >= 2 (one thread).
-__device__ void met_largest_gap(const float* a, uint32_t n, float* start, float* end, float* gap) {
+static __device__ void met_largest_gap(const float* a, uint32_t n, float* start, float* end, float* gap) {
   float max_gap = a[0] + TAU_F - a[n - 1];
   uint32_t gap_k = n - 1;
   for (uint32_t i = 0; i + 1 < n; ++i) {

@@ -18,7 +18,11 @@
 //     overlap: issue them on one stream, or order them with events. Overlapping calls race on the
 //     scratch and give undefined results;
 //   * the first call on a device resolves the scratch's address (cudaGetSymbolAddress) once; make
-//     that first call before capturing a stream.
+//     that first call before capturing a stream;
+//   * that address is cached per device ordinal for the life of the process and is valid in the
+//     device's primary context only (the one the CUDA runtime uses): a cudaDeviceReset between
+//     calls, or a call made while another context is current on the device, would hand the kernel
+//     a stale address, so neither is allowed.
 #include <cmath>
 #include <cstdio>
 #include <mutex>

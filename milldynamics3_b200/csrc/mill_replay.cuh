@@ -42,7 +42,7 @@ __device__ void preds_from_records(const uint32_t* key, uint32_t nrec, uint32_t 
 
 // Levels of items [0, n) (warp 0; chunks of 32 items, in-chunk propagation by shuffles).
 // Returns the number of levels (block-uniform).
-__device__ uint32_t compute_levels(uint32_t n, const uint32_t* pred_a, const uint32_t* pred_b, uint32_t* lvl) {
+static __device__ uint32_t compute_levels(uint32_t n, const uint32_t* pred_a, const uint32_t* pred_b, uint32_t* lvl) {
   __shared__ uint32_t nlev;
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
@@ -84,7 +84,7 @@ __device__ uint32_t compute_levels(uint32_t n, const uint32_t* pred_a, const uin
 }
 
 // Groups items by level: lev_start[0..nlev], lev_items[] (order inside a level is irrelevant).
-__device__ void bucket_levels(uint32_t n, const uint32_t* lvl, uint32_t nlev, uint32_t* lev_start, uint32_t* lev_cur,
+static __device__ void bucket_levels(uint32_t n, const uint32_t* lvl, uint32_t nlev, uint32_t* lev_start, uint32_t* lev_cur,
                               uint32_t* lev_items) {
   for (uint32_t l = tid(); l <= nlev; l += nthr()) lev_start[l] = 0;
   __syncthreads();
@@ -134,7 +134,7 @@ __shared__ uint32_t g_ticket;
 
 // Packs the per-ball item lists (item_j[b * cap + s], s < cnt[b]) into records in ball order:
 // rec_off[0..nb], rec_key[r] = fluid index, rec_ball[r] = ball. Returns the record count.
-__device__ uint32_t pack_ball_items(const uint32_t* item_j, const uint32_t* cnt, uint32_t cap, uint32_t nb,
+static __device__ uint32_t pack_ball_items(const uint32_t* item_j, const uint32_t* cnt, uint32_t cap, uint32_t nb,
                                     uint32_t* rec_off, uint32_t* rec_key, uint32_t* rec_ball) {
   for (uint32_t b = tid(); b < nb; b += nthr()) rec_off[b] = cnt[b];
   if (tid() == 0) rec_off[nb] = 0;
@@ -149,7 +149,7 @@ __device__ uint32_t pack_ball_items(const uint32_t* item_j, const uint32_t* cnt,
 }
 
 // rec_pred[r] = the ball of the previous record with the same fluid index (NONE if first).
-__device__ void ball_item_preds(const uint32_t* rec_key, const uint32_t* rec_ball, uint32_t nrec, uint32_t nf,
+static __device__ void ball_item_preds(const uint32_t* rec_key, const uint32_t* rec_ball, uint32_t nrec, uint32_t nf,
                                 uint32_t* start, uint32_t* cur, uint32_t* order, uint32_t* rec_pred) {
   block_bucket_sort(rec_key, nrec, nf, start, cur, order);
   for (uint32_t j = tid(); j < nf; j += nthr()) {

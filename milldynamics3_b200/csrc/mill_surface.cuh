@@ -175,7 +175,7 @@ struct SurfShared {
 
 // Cases of every cell at threshold thr and the exclusive segment prefix; returns the segment
 // count. Cell c = cj * 127 + ci; thread t owns cells [t * k, t * k + k).
-__device__ uint32_t surf_cases(SurfShared& sh, float thr) {
+static __device__ uint32_t surf_cases(SurfShared& sh, float thr) {
   const float* field = sh.field;
   const uint32_t c0 = tid() * SURF_CELLS_PER_THREAD;
   uint32_t cnt = 0;
@@ -253,7 +253,7 @@ __device__ __forceinline__ uint32_t surf_partner(const SurfShared& sh, uint32_t 
 // (surface.rs:307-311) lists at most these two segments for an edge, the lower cell's first, so
 // extend_chain's "first unvisited candidate" at an edge is the partner of the current segment
 // whenever that partner is unvisited.
-__device__ void surf_links(const SurfShared& sh, uint32_t S, uint32_t* seg_e, uint32_t* seg_n) {
+static __device__ void surf_links(const SurfShared& sh, uint32_t S, uint32_t* seg_e, uint32_t* seg_n) {
   const uint32_t c0 = tid() * SURF_CELLS_PER_THREAD;
   for (uint32_t q = 0; q < SURF_CELLS_PER_THREAD; ++q) {
     const uint32_t c = c0 + q;

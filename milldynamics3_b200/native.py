@@ -17,7 +17,8 @@ LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libmillgpu.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["mill_kernels.cu", "mill_host.cu", "mill_params.cpp", "mill_noalloc.cu"]
+SOURCES = ["mill_substeps_1024.cu", "mill_substeps_512.cu", "mill_kernels.cu", "mill_host.cu", "mill_params.cpp",
+           "mill_noalloc.cu"]
 # every header beside the sources (the build is stale when any of them is newer than the library)
 HEADERS = sorted(f for f in os.listdir(os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc"))
                  if f.endswith((".cuh", ".h")))
@@ -26,7 +27,7 @@ HEADERS = sorted(f for f in os.listdir(os.path.join(os.path.dirname(os.path.absp
 # device code (-fmad=false) or host code (-ffp-contract=off), no fast-math.
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
               "-prec-div=true", "-prec-sqrt=true", "-ftz=false", "--expt-relaxed-constexpr",
-              "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math", "-shared"]
+              "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math"]
 
 
 def nvcc() -> str:
@@ -45,17 +46,35 @@ def _stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    """Compiles libmillgpu.so in-tree for sm_100a (nvcc cross-compiles without a GPU)."""
+    """Compiles libmillgpu.so in-tree for sm_100a (nvcc cross-compiles without a GPU): every
+    source to an object in parallel, then one link."""
     if not force and not _stale():
         return LIB_PATH
     os.makedirs(LIB_DIR, exist_ok=True)
+    objs, procs = [], []
+    for f in SOURCES:
+        o = os.path.join(LIB_DIR, os.path.splitext(f)[0] + ".o")
+        cmd = [nvcc()] + NVCC_FLAGS + ["-c", "-o", o, os.path.join(CSRC, f)]
+        procs.append((cmd, subprocess.Popen(cmd, cwd=CSRC, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                                            text=True)))
+        objs.append(o)
+    logs, failed = [], []
+    for cmd, p in procs:
+        out, _ = p.communicate()
+        logs.append(out)
+        if p.returncode != 0:
+            failed.append(" ".join(cmd) + "\n" + out)
+    if failed:
+        raise RuntimeError("building libmillgpu.so failed:\n" + "\n".join(failed))
     tmp = LIB_PATH + ".tmp"
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", tmp] + [os.path.join(CSRC, f) for f in SOURCES]
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp] + objs
     r = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("building libmillgpu.so failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError("linking libmillgpu.so failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
     if verbose:
-        print(r.stdout + r.stderr)
+        print("".join(logs) + r.stdout + r.stderr)
+    for o in objs:
+        os.remove(o)
     os.replace(tmp, LIB_PATH)
     return LIB_PATH
 

@@ -72,6 +72,11 @@ class Server:
             return st.value, done.value, None, None, None
         return st.value, done.value, [r.copy() for r in res], list(mean), list(se)
 
+    def release_sweep(self, sweep_id: int):
+        """Forgets the sweep's record (its result cannot be read afterwards); seeds still queued
+        or running are cancelled."""
+        self._c(self.lib.server_sweep_release(self.h, C.c_uint64(sweep_id)))
+
     def cancel(self, job_id: int):
         self._c(self.lib.server_cancel(self.h, C.c_uint64(job_id)))
 

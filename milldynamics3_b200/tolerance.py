@@ -388,7 +388,8 @@ def compare(base, table, out=print):
     return failed
 
 
-def main(argv=None) -> int:
+def main(argv=None, backend=None) -> int:
+    """The tolerance_probe command line on the device library, or on `backend` when one is given."""
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--seeds", type=int, default=3)
     ap.add_argument("--settle-revs", type=float, default=2.0)
@@ -396,14 +397,8 @@ def main(argv=None) -> int:
     ap.add_argument("--baseline")
     ap.add_argument("--compare")
     ap.add_argument("--only", type=lambda s: s.split(","))
-    ap.add_argument("--oracle", action="store_true", help="run on the CPU oracle (test infrastructure)")
     a = ap.parse_args(argv)
-    if a.oracle:
-        import os
-        sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests"))
-        from conftest import ORACLE_EXTRA, build_oracle
-        backend = Backend(capi.Lib(build_oracle(), "or_", ORACLE_EXTRA))
-    else:
+    if backend is None:
         from . import native
         backend = Backend(native.load())
     t0 = time.perf_counter()

@@ -72,16 +72,40 @@ class _Num:
         self.text = text
 
 
+def _ryu_text(v, f32: bool) -> str:
+    """The text serde_json writes for a finite float (the ryu crate's format32 / format64): the
+    shortest digits that read back to the same value, in plain notation when the decimal point
+    falls within reach (10^-6 <= |v| < 10^13 for f32, 10^-5 <= |v| < 10^16 for f64, whole numbers
+    with a trailing '.0'), else as d.ddd followed by 'e' and the exponent without '+' or leading
+    zeros ('1e-7', '2.5e20')."""
+    neg = bool(np.signbit(v))
+    if v == 0:
+        return "-0.0" if neg else "0.0"
+    sci = np.format_float_scientific(abs(v), unique=True, trim="-")
+    mant, ex = sci.split("e")
+    digits = mant.replace(".", "")
+    kk = int(ex) + 1  # 10^(kk-1) <= |v| < 10^kk
+    n = len(digits)
+    hi, lo = (13, -6) if f32 else (16, -5)
+    if kk - n >= 0 and kk <= hi:
+        t = digits + "0" * (kk - n) + ".0"
+    elif 0 < kk <= hi:
+        t = digits[:kk] + "." + digits[kk:]
+    elif lo < kk <= 0:
+        t = "0." + "0" * (-kk) + digits
+    elif n == 1:
+        t = digits + "e" + str(kk - 1)
+    else:
+        t = digits[0] + "." + digits[1:] + "e" + str(kk - 1)
+    return "-" + t if neg else t
+
+
 def _num(x, kind: str):
     if kind == "f32":
         v = F(x)
-        if not np.isfinite(v):
-            return None
-        if v == 0 or 1e-5 <= abs(v) < 1e16:
-            return _Num(np.format_float_positional(v, unique=True, trim="0"))
-        return _Num(np.format_float_scientific(v, unique=True, trim="0"))
-    x = float(x)
-    return _Num(repr(x)) if math.isfinite(x) else None
+        return _Num(_ryu_text(v, True)) if np.isfinite(v) else None
+    v = np.float64(x)
+    return _Num(_ryu_text(v, False)) if np.isfinite(v) else None
 
 
 def _dumps(obj) -> str:
@@ -95,7 +119,7 @@ def _dumps(obj) -> str:
     if isinstance(obj, int):
         return str(obj)
     if isinstance(obj, float):
-        return repr(obj) if math.isfinite(obj) else "null"
+        return _ryu_text(np.float64(obj), False) if math.isfinite(obj) else "null"
     if isinstance(obj, str):
         return json.dumps(obj)
     if isinstance(obj, dict):

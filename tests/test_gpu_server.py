@@ -166,3 +166,35 @@ def test_sweep_job_rules_and_cancel(device):
     st, done, res, _, _ = srv.sweep_result(sid, 2)
     assert st == capi.JOB_CANCELLED and res is None
     assert srv.stats().active == 0
+
+
+def test_sweep_that_fails_cancels_its_other_seeds_and_release_forgets_it(device):
+    from milldynamics3_b200.sim import MillError
+    p = device.preset(device.params_default(), "realtime")
+    # a budget no mill fits: the first seed fails at admission (nothing running could free memory),
+    # and its two siblings leave as cancelled instead of waiting in the queue
+    srv = Server(device, memory_budget_bytes=1 << 20)
+    sid = srv.submit_sweep(p, 3, 0.0, 1.0)
+    srv.step()
+    ups = srv.poll()
+    states = sorted(u.state for u in ups)
+    assert states == sorted([capi.JOB_FAILED, capi.JOB_CANCELLED, capi.JOB_CANCELLED])
+    st, done, res, _, _ = srv.sweep_result(sid, 3)
+    assert st == capi.JOB_FAILED and done == 0 and res is None
+    s = srv.stats()
+    assert s.active == 0 and s.queued == 0
+    srv.release_sweep(sid)
+    with pytest.raises(MillError):
+        srv.sweep_result(sid, 3)
+    srv.close()
+    # releasing a running sweep cancels its seeds before the next frame
+    srv = Server(device)
+    sid = srv.submit_sweep(p, 2, 0.0, 1.0)
+    srv.step()
+    assert srv.stats().active == 2
+    srv.release_sweep(sid)
+    srv.step()
+    assert srv.stats().active == 0
+    with pytest.raises(MillError):
+        srv.release_sweep(sid)
+    srv.close()

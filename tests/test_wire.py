@@ -88,7 +88,19 @@ def test_f32_numbers_are_shortest_and_exact(oracle):
     p.lifters.height_m = 1e-7
     d = wire.params_to_json(p)
     assert '"diameter_m":0.1,' in d and '"density_kg_m3":7850.0,' in d
+    assert '"height_m":1e-7,' in d
     assert _bytes(wire.params_from_json(d)) == _bytes(p)
+
+
+@pytest.mark.parametrize("value,kind,text", [
+    (1e-7, "f32", "1e-7"), (2.5e20, "f32", "2.5e20"), (1e-6, "f32", "0.000001"), (1e13, "f32", "1e13"),
+    (1.5e12, "f32", "1500000000000.0"), (-0.0, "f32", "-0.0"), (0.072, "f32", "0.072"), (3.0, "f32", "3.0"),
+    (1e-5, "f64", "0.00001"), (2.5e-7, "f64", "2.5e-7"), (1e16, "f64", "1e16"), (1e15, "f64", "1000000000000000.0"),
+    (1.7976931348623157e308, "f64", "1.7976931348623157e308"), (5e-324, "f64", "5e-324")])
+def test_numbers_are_written_as_serde_json_writes_them(value, kind, text):
+    # serde_json prints floats with the ryu crate: shortest digits, plain notation in a window of
+    # exponents, otherwise mantissa 'e' exponent with no '+' and no leading zeros
+    assert wire._num(value, kind).text == text
 
 
 def test_metrics_json_has_the_metrics_struct_fields(oracle):

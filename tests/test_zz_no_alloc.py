@@ -47,12 +47,18 @@ def _run_noalloc(fn, torch, pts, h, cap, stream):
             int(st.item()))
 
 
-@pytest.mark.parametrize("seed,n,h", [(1, 794, 0.00252), (2, 12700, 0.0011), (3, 100, 0.01), (4, 16384, 0.0009)])
-def test_matches_existing_entry_point_on_two_calls_in_a_row(device_lib, seed, n, h):
+# The last case puts one point far outside the cloud: its bounding box then holds far more cells
+# than 2 n + 512, so the grid takes the sparse (sorted-key) path instead of the dense one.
+@pytest.mark.parametrize("seed,n,h,outlier", [(1, 794, 0.00252, False), (2, 12700, 0.0011, False),
+                                              (3, 100, 0.01, False), (4, 16384, 0.0009, False),
+                                              (6, 16000, 0.0009, True)])
+def test_matches_existing_entry_point_on_two_calls_in_a_row(device_lib, seed, n, h, outlier):
     torch = pytest.importorskip("torch")
     fn = _bind(device_lib)
     pts = _cloud(seed, n, 0.03)
     pts[n // 3] = np.nan  # a non-finite point is skipped by both
+    if outlier:
+        pts[7] = (1.0e3, 1.0e3)
     rc_ref, off_ref, nbrs_ref = probe_neighbor_lists(device_lib, pts, h)
     assert rc_ref == 0
     stream = torch.cuda.Stream()
