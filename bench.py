@@ -417,7 +417,7 @@ def run_device(args):
                                     "two kernels, flattened polygons to a host buffer)",
                             "ms_per_call": surf_ms, "polygons": surf_polys, "floats": surf_len.value},
                 "counters_per_substep": {f: round(tot[q] / max(nsum.value, 1), 2) for q, (f, _) in
-                                         enumerate(capi.StepCounters._fields_) if f != "reserved0"}}
+                                         enumerate(capi.StepCounters._fields_)}}
         plain_mfps = None
         if args.batch_mills > 0:
             line["batched"] = run_batched(lib, b, args)

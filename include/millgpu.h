@@ -146,7 +146,7 @@ typedef struct MgStepCounters {
   uint32_t density_iters, cg_iters, n_groups, n_links, links_in_range;
   uint32_t n_ball_pairs, n_fluid_edges, n_active_contacts;
   uint32_t n_coupling_items; /* entrained (ball, fluid) items of drag plus buoyancy */
-  uint32_t reserved0;
+  uint32_t ccd_clamps;       /* balls the wall CCD (dem.rs:674-706) held at their time of impact */
 } MgStepCounters;
 
 /* dem.rs:277-309 Balls' uniform material fields */
@@ -184,14 +184,23 @@ typedef struct MgScalars {
  * groups, squeeze links, drag and buoyancy item lists) in the handle's own launches: 0 = default
  * (16), 1 = the mill's block alone, at most 16 for handles from mg_sim_create /
  * mg_sim_create_with_balls; the mills of a batch or a server always run one block each (0 or 1).
- * None of them changes results. */
+ * None of them changes results.
+ * test_wait_limit_us, test_faults: for tests of the failure path only (leave both 0).
+ * test_wait_limit_us > 0 shortens the device's bounded waits (the mill block's wait for its helper
+ * blocks, a ball's wait for earlier balls in the drag and buoyancy sweeps) from about a second or
+ * more to about that many microseconds. test_faults bit 1: the mill's block waits for one more
+ * helper block than was launched (a helper that never answers: its wait runs out, the step returns
+ * MG_ERR_CUDA); bit 2: the drag sweep never flags ball 0 done (balls that share a fluid particle
+ * with it wait until their limit runs out, the step returns MG_ERR_STATE). */
 typedef struct MgOptions {
   uint32_t cg_fp64;
   uint32_t block_threads;
   uint32_t sweep_warps;
   uint32_t spin_ns;
   uint32_t mill_blocks;
-  uint32_t reserved[3];
+  uint32_t test_wait_limit_us;
+  uint32_t test_faults;
+  uint32_t reserved;
 } MgOptions;
 
 typedef struct MgSim MgSim;

@@ -119,7 +119,7 @@ class ImpactRecord(_S):
 class StepCounters(_S):
     _fields_ = [(n, C.c_uint32) for n in (
         "density_iters", "cg_iters", "n_groups", "n_links", "links_in_range", "n_ball_pairs",
-        "n_fluid_edges", "n_active_contacts", "n_coupling_items", "reserved0")]
+        "n_fluid_edges", "n_active_contacts", "n_coupling_items", "ccd_clamps")]
 
 
 class BallMaterial(_S):
@@ -147,7 +147,8 @@ class Scalars(_S):
 
 class Options(_S):
     _fields_ = [("cg_fp64", C.c_uint32), ("block_threads", C.c_uint32), ("sweep_warps", C.c_uint32),
-                ("spin_ns", C.c_uint32), ("mill_blocks", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("spin_ns", C.c_uint32), ("mill_blocks", C.c_uint32), ("test_wait_limit_us", C.c_uint32),
+                ("test_faults", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class ServerConfig(_S):

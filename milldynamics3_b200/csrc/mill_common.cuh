@@ -31,6 +31,11 @@ constexpr uint32_t DEFAULT_BLOCK_THREADS = 1024;
 constexpr uint32_t MAX_MILL_BLOCKS = 16;
 constexpr uint32_t DEFAULT_MILL_BLOCKS = 16;
 constexpr uint32_t DEFAULT_SPIN_NS = 64;
+// Bounds of the device's waits: polls of a ball waiting for an earlier ball in a per-ball sweep
+// (about a second at the default poll interval), and clock cycles of a wait between a mill's
+// block and its helper blocks (about 10 s at 2 GHz).
+constexpr uint32_t SPIN_LIMIT = 1u << 24;
+constexpr long long WIDE_TIMEOUT_CYCLES = 20000000000LL;
 constexpr int MAX_BOUNDARY_POINTS = 1024;
 
 // ---------------------------------------------------------------- scalar helpers (f32::max etc.)
@@ -163,6 +168,8 @@ struct StepUniform {
   uint32_t want_momentum;  // accumulate CouplingImpulses::fluid_momentum_change (coupling.rs:49-51)
   uint32_t sweep_warps;    // warps taking balls in the per-ball sweeps
   uint32_t spin_ns;        // poll interval of a waiting ball
+  uint32_t spin_limit;     // polls after which a waiting ball gives up (ERR_BUDGET)
+  uint32_t skip_done_ball; // tests only: the drag sweep never flags this ball done (NONE: none)
 };
 
 // The per-sub-step part of the uniform block (drum angle and its rotations, dt), one per sub-step
@@ -308,6 +315,8 @@ struct MillDev {
   uint32_t smem_balls;  // balls whose state fits the launch's dynamic shared memory (0: global)
   uint32_t smem_bytes;  // the launch's dynamic shared memory (staged ball state, then sweep scratch)
   uint32_t helpers;     // helper blocks of this launch (set by the kernel; 0 in batches)
+  uint32_t test_extra_helpers;  // tests only: helper blocks the mill's block waits for but were not launched
+  long long wide_wait_cycles;   // the mill block's bound on a wait for its helper blocks (clock cycles)
   WideCtl* wide;        // their control block
   // outputs
   StepOut* out;             // one per sub-step of the launch

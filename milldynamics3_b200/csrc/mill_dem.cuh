@@ -162,6 +162,7 @@ static __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut&
       if (drum_toi_swept(U, V2(m.bx0[i]), x, U.drum_angle, U.drum_angle_next, r, t)) t_hit = fmin_r(1.0f, t);
     }
     if (t_hit < 1.0f) {
+      atomicAdd(&out.ctr.ccd_clamps, 1u);
       V2 x0(m.bx0[i]);
       float path_len = (x - x0).len();
       float skin = CCD_SKIN_FRACTION * r;

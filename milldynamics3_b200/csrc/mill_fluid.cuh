@@ -1087,7 +1087,7 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
       auto item_phi = [&](const DragBall& q, uint32_t base, uint32_t s) { return s < 32 ? q.phi : m.item_w[base + s]; };
       auto item_j = [&](const DragBall& q, uint32_t base, uint32_t s) { return s < 32 ? q.j : m.item_j[base + s]; };
       ball_dataflow(
-          nb, m.rec_off, m.rec_pred, done, U.sweep_warps, U.spin_ns, err, &out.stage[32],
+          nb, m.rec_off, m.rec_pred, done, U.sweep_warps, U.spin_ns, U.spin_limit, U.skip_done_ball, err, &out.stage[32],
           // before the wait: the item data and the geometry-only quantities computed for every ball
           // ahead of the sweep (drag_pre_balls)
           [&](uint32_t b, int lane) {
@@ -1229,7 +1229,7 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
       bool valid;
     };
     ball_dataflow(
-        nb, m.rec_off, m.rec_pred, done, U.sweep_warps, U.spin_ns, err, &out.stage[35],
+        nb, m.rec_off, m.rec_pred, done, U.sweep_warps, U.spin_ns, U.spin_limit, NONE, err, &out.stage[35],
         // before the wait: item geometry and the weight sum, which the sweep does not change
         [&](uint32_t b, int lane) {
           BuoyBall q;

@@ -319,6 +319,9 @@ void fill_desc(MgSim* s) {
   s->md.b_rtrue = s->bmat.true_radius;
   s->md.smem_bytes = (uint32_t)stage_smem_bytes(s->nf, s->nb, s->mill_blocks_cap > 1);
   s->md.smem_balls = (size_t)s->nb * 24 <= s->md.smem_bytes ? s->nb : 0u;
+  // the mill block's bound on a wait for its helper blocks: ~10 s, or the tests' short limit
+  s->md.wide_wait_cycles = s->opt.test_wait_limit_us ? 2000LL * s->opt.test_wait_limit_us : WIDE_TIMEOUT_CYCLES;
+  s->md.test_extra_helpers = (s->opt.test_faults & 1u) ? 1u : 0u;
 }
 
 int push_desc(MgSim* s) {
@@ -369,6 +372,13 @@ int fill_uniform(MgSim* s, const MgDrum& drum, const MgMediaParams& media, const
   U.cg_fp64 = s->opt.cg_fp64;
   U.sweep_warps = s->opt.sweep_warps ? s->opt.sweep_warps : DEFAULT_SWEEP_WARPS;
   U.spin_ns = s->opt.spin_ns ? s->opt.spin_ns : DEFAULT_SPIN_NS;
+  // polls of a waiting ball before it gives up: about a second, or the tests' short limit
+  U.spin_limit = s->opt.test_wait_limit_us
+                     ? std::max<uint32_t>(1u, (uint32_t)std::min<uint64_t>(
+                                                  (uint64_t)s->opt.test_wait_limit_us * 1000u / std::max(U.spin_ns, 1u),
+                                                  SPIN_LIMIT))
+                     : SPIN_LIMIT;
+  U.skip_done_ball = (s->opt.test_faults & 2u) ? 0u : NONE;
   // pbf.rs:190-219: boundary points at dx = h / 2 (adhesion and viscosity groups)
   U.boundary_count = 0;
   float br = s->bmat.radius, dx = 0.5f * s->fmat.h;
@@ -441,6 +451,9 @@ int run(MgSim* s, uint32_t n_sub) {
   uint32_t e = 0;
   for (uint32_t k = 0; k < n_sub; ++k) e |= s->h_out[k].err;
   if (e & ERR_WIDE) return fail(s, MG_ERR_CUDA, "the mill's thread blocks stopped waiting for one another (timeout)");
+  if (e & ERR_BUDGET)
+    return fail(s, MG_ERR_STATE, "a bounded device wait ran out (a ball of a per-ball sweep waited for an earlier "
+                                 "ball that never finished; error bits 0x%x)", e);
   if (e) return fail(s, MG_ERR_CAPACITY, "device capacity exceeded (error bits 0x%x)", e);
   size_t total_imp = 0;
   for (uint32_t k = 0; k < n_sub; ++k) total_imp += s->h_out[k].n_impacts;
@@ -757,6 +770,8 @@ int mg_sim_set_options(MgSim* s, const MgOptions* o) {
   if (o->spin_ns > 100000) return fail(s, MG_ERR_ARG, "spin_ns must be at most 100000");
   if (o->mill_blocks > s->mill_blocks_cap)
     return fail(s, MG_ERR_ARG, "mill_blocks must be in [0, %u] for this handle", s->mill_blocks_cap);
+  if (o->test_wait_limit_us > 10000000u) return fail(s, MG_ERR_ARG, "test_wait_limit_us must be at most 10000000");
+  if (o->test_faults & ~3u) return fail(s, MG_ERR_ARG, "test_faults: only bits 1 and 2 are defined");
   s->opt = *o;
   return MG_OK;
 }

@@ -163,7 +163,6 @@ static __device__ void ball_item_preds(const uint32_t* rec_key, const uint32_t* 
   __syncthreads();
 }
 
-constexpr uint32_t SPIN_LIMIT = 1u << 24;
 
 // Runs fn(b, lane) once per ball, one warp per ball, in a dependency-respecting order. done[] is
 // nb words of scratch (shared or global). Waits are bounded: a wait that runs out sets
@@ -179,11 +178,11 @@ constexpr uint32_t SPIN_LIMIT = 1u << 24;
 // together and sleep together, so the warp never diverges here (lanes that spun on their own
 // were measured to leave the shuffle-heavy code after the wait several times slower).
 __device__ __forceinline__ void wait_ball_done(volatile uint32_t* vdone, uint32_t p, uint32_t spin_ns,
-                                               uint32_t* err) {
+                                               uint32_t spin_limit, uint32_t* err) {
   for (uint32_t spins = 0;; ++spins) {
     const bool ok = p == NONE || vdone[p] != 0u;
     if (__all_sync(FULL, ok)) break;
-    if (spins > SPIN_LIMIT) {
+    if (spins > spin_limit) {
       if ((threadIdx.x & 31u) == 0) atomicOr(err, ERR_BUDGET);
       break;
     }
@@ -191,11 +190,13 @@ __device__ __forceinline__ void wait_ball_done(volatile uint32_t* vdone, uint32_
   }
 }
 
-// Warps from `warps` on sit the sweep out (they wait at the closing barrier).
+// Warps from `warps` on sit the sweep out (they wait at the closing barrier). A wait gives up after
+// spin_limit polls. skip_done names a ball whose done flag is never set (tests of the bounded
+// wait only; NONE otherwise).
 template <class Pre, class Run, class Post>
 __device__ void ball_dataflow(uint32_t nb, const uint32_t* rec_off, const uint32_t* rec_pred, uint32_t* done,
-                              uint32_t warps, uint32_t spin_ns, uint32_t* err, unsigned long long* acct, Pre pre,
-                              Run run, Post post) {
+                              uint32_t warps, uint32_t spin_ns, uint32_t spin_limit, uint32_t skip_done, uint32_t* err,
+                              unsigned long long* acct, Pre pre, Run run, Post post) {
   for (uint32_t b = tid(); b < nb; b += nthr()) done[b] = 0u;
   if (tid() == 0) g_ticket = 0;
   __syncthreads();
@@ -213,15 +214,16 @@ __device__ void ball_dataflow(uint32_t nb, const uint32_t* rec_off, const uint32
     const uint32_t p0 = r0 + lane < r1 ? rec_pred[r0 + lane] : NONE;
     auto st = pre(b, lane);
     const long long t1 = clock64();
-    wait_ball_done(vdone, p0, spin_ns, err);
-    for (uint32_t c = r0 + 32; c < r1; c += 32) wait_ball_done(vdone, c + lane < r1 ? rec_pred[c + lane] : NONE, spin_ns, err);
+    wait_ball_done(vdone, p0, spin_ns, spin_limit, err);
+    for (uint32_t c = r0 + 32; c < r1; c += 32)
+      wait_ball_done(vdone, c + lane < r1 ? rec_pred[c + lane] : NONE, spin_ns, spin_limit, err);
     __syncwarp();
     __threadfence_block();
     const long long t2 = clock64();
     run(b, lane, st);
     __threadfence_block();
     __syncwarp();
-    if (lane == 0) vdone[b] = 1u;
+    if (lane == 0 && b != skip_done) vdone[b] = 1u;
     post(b, lane, st);
     t_pre += (unsigned long long)(t1 - t0);
     t_wait += (unsigned long long)(t2 - t1);

@@ -72,7 +72,10 @@ __global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDe
     // Without the fluid half, imp/ang hold the caller's external impulses (DEM-only entry point).
     if (U.run_fluid) fluid_step(m, U, out, m.err, fs, dsm);
     __syncthreads();
-    if (*m.err) break;
+    if (*m.err) {  // the mill stops; the host reads the error bits from this sub-step's record
+      if (threadIdx.x == 0) out.err = *m.err;
+      break;
+    }
     if (U.run_dem) dem_step(m, U, out, m.impacts + (size_t)s * m.cap_impacts, m.err, ds, dsm);
     __syncthreads();
     if (threadIdx.x == 0) out.stage[14] = out.stage[15] + out.stage[16] + out.stage[17] + out.stage[18] + out.stage[20] + out.stage[21] + out.stage[22] + out.stage[30];

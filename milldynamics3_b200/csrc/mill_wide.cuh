@@ -26,15 +26,14 @@ enum : uint32_t {
   WIDE_DRAG_PRE = 8
 };
 
-constexpr long long WIDE_TIMEOUT_CYCLES = 20000000000LL;  // ~10 s at 2 GHz
 
 __shared__ uint32_t g_wide_seq;  // phases the mill's block has published in this launch
 
-// Waits (thread 0) until *p >= target; false when the bound ran out.
-__device__ inline bool wide_wait(const uint32_t* p, uint32_t target) {
+// Waits (thread 0) until *p >= target; false when `limit` clock cycles ran out first.
+__device__ inline bool wide_wait(const uint32_t* p, uint32_t target, long long limit = WIDE_TIMEOUT_CYCLES) {
   const long long t0 = clock64();
   while ((int32_t)(*reinterpret_cast<const volatile uint32_t*>(p) - target) < 0) {
-    if (clock64() - t0 > WIDE_TIMEOUT_CYCLES) return false;
+    if (clock64() - t0 > limit) return false;
     __nanosleep(64);
   }
   return true;
@@ -66,7 +65,13 @@ __device__ void wide_phase(const MillDev& m, uint32_t phase, const GridHdr* hdr,
   share(warp, (1u + m.helpers) * nwarps);
   __syncthreads();
   if (tid() == 0) {
-    if (!wide_wait(&c->done, g_wide_seq * m.helpers)) atomicOr(m.err, ERR_WIDE);
+    const long long lim = m.wide_wait_cycles > 0 ? m.wide_wait_cycles : WIDE_TIMEOUT_CYCLES;
+    if (!wide_wait(&c->done, g_wide_seq * (m.helpers + m.test_extra_helpers), lim)) {
+      atomicOr(m.err, ERR_WIDE);
+      // the helper blocks that did answer finish this phase before the mill's block goes on and
+      // overwrites what they read (bounded too); the launch then ends at the next error check
+      wide_wait(&c->done, g_wide_seq * m.helpers);
+    }
     __threadfence();
   }
   __syncthreads();

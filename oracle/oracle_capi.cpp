@@ -185,8 +185,7 @@ int or_dem_step_recorded(OrSim* s, const MgDrum* drum, float drum_angle, const M
   StepCounters ctr;
   DemStepStats ds = dem_step_recorded(&s->sim.balls, d, drum_angle, m, it, dt, (impulses || angular) ? &imp : nullptr,
                                       &recs, &ctr, &s->sim.dbg);
-  s->sim.last_counters.n_ball_pairs = ctr.n_ball_pairs;
-  s->sim.last_counters.n_active_contacts = ctr.n_active_contacts;
+  s->sim.last_counters = ctr;  // the DEM half's counters; the fluid ones read 0, as on the device
   s->sim.last_dem_stats = ds;
   if (dstats) std::memcpy(dstats, &ds, sizeof(ds));
   if (n_out) *n_out = (uint32_t)recs.size();

@@ -353,7 +353,7 @@ struct ImpactRecord {
 struct StepCounters {
   uint32_t density_iters = 0, cg_iters = 0, n_groups = 0, n_links = 0, links_in_range = 0;
   uint32_t n_ball_pairs = 0, n_fluid_edges = 0, n_active_contacts = 0;
-  uint32_t n_coupling_items = 0, reserved0 = 0;
+  uint32_t n_coupling_items = 0, ccd_clamps = 0;
 };
 
 // Last sub-step's internal structures, kept for parity checks of the device path.

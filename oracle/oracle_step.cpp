@@ -1157,6 +1157,7 @@ DemStepStats dem_step_recorded(Balls* bp, const Drum& drum, float drum_angle, co
   }
   for (size_t i = 0; i < n; ++i) {
     if (toi[i] < 1.0f) {
+      if (ctr) ctr->ccd_clamps += 1;
       float path_len = (B.x[i] - x0[i]).length();
       float skin = CCD_CONTACT_SKIN_FRACTION * r;
       float t_skin = path_len > 1e-9f ? skin / path_len : 1.0f;
