@@ -1350,3 +1350,88 @@ DemStepStats dem_step_recorded(Balls* bp, const Drum& drum, float drum_angle, co
 }
 
 }  // namespace orc
+
+// ---------------------------------------------------------------- probes of the viscosity stage
+// C entry points over the functions above, for the reference unit tests that call them directly
+// (pbf.rs:2428, 2476, 2513). Test infrastructure like the rest of the oracle.
+extern "C" {
+
+// morris_weights + laplacian_apply_into (pbf.rs:312-377) on caller points: the neighbour lists of
+// pbf.rs:262-288 at h, per-particle densities and viscosities as given; out[2n] = (L v)_i,
+// *w_max = the largest weight.
+int or_probe_viscous_operator(const float* xy, const float* v, const float* density, const float* mu, uint32_t n,
+                              float h, float mass, float* out, float* w_max) {
+  using namespace orc;
+  std::vector<Vec2> x(n), vv(n), o(n);
+  for (uint32_t i = 0; i < n; ++i) { x[i] = Vec2(xy[2 * i], xy[2 * i + 1]); vv[i] = Vec2(v[2 * i], v[2 * i + 1]); }
+  Nbr nb;
+  neighbor_lists(x, h, &nb.off, &nb.idx);
+  std::vector<float> dens(density, density + n), m(mu, mu + n);
+  ViscWeights w = morris_weights(x, nb, dens, mass, m, h);
+  laplacian_apply_into(nb, w, vv.data(), n, o.data());
+  float wm = 0.0f;
+  for (float q : w.w) wm = fmax_r(wm, q);
+  for (uint32_t i = 0; i < n; ++i) { out[2 * i] = o[i].x; out[2 * i + 1] = o[i].y; }
+  if (w_max) *w_max = wm;
+  return 0;
+}
+
+// squeeze_links (pbf.rs:544-625) of balls at bx[2 nb] (radius r, mass ball_mass) in a drum of
+// drum_radius; closing (2 nb, may be null: no approach filter) as the reference's Option. Links
+// go to ball/other (other = 0xFFFFFFFF for the wall), nrm[2], c; *n_out all links (even beyond
+// cap), *in_range the pairs and walls within range.
+int or_probe_squeeze_links(const float* bx, uint32_t nb, float r, float ball_mass, float drum_radius, float dx,
+                           float mu, float dt, const float* closing, uint32_t* ball, uint32_t* other, float* nrm,
+                           float* c, uint32_t cap, uint32_t* n_out, uint32_t* in_range) {
+  using namespace orc;
+  Balls b;
+  for (uint32_t i = 0; i < nb; ++i) b.x.push_back(Vec2(bx[2 * i], bx[2 * i + 1]));
+  b.v.assign(nb, Vec2());
+  b.theta.assign(nb, 0.0f);
+  b.omega.assign(nb, 0.0f);
+  b.radius = r;
+  b.mass = ball_mass;
+  std::vector<Vec2> cl;
+  for (uint32_t i = 0; closing && i < nb; ++i) cl.push_back(Vec2(closing[2 * i], closing[2 * i + 1]));
+  size_t ir = 0;
+  std::vector<SqueezeLink> links = squeeze_links(b, drum_radius, dx, mu, dt, closing ? &cl : nullptr, &ir);
+  for (size_t k = 0; k < links.size() && k < cap; ++k) {
+    ball[k] = links[k].ball;
+    other[k] = links[k].other;
+    nrm[2 * k] = links[k].n.x;
+    nrm[2 * k + 1] = links[k].n.y;
+    c[k] = links[k].c;
+  }
+  *n_out = (uint32_t)links.size();
+  if (in_range) *in_range = (uint32_t)ir;
+  return 0;
+}
+
+// solve_viscosity_with_balls (pbf.rs:641-791) for n fluid particles without neighbours (their
+// Laplacian rows are empty, as in the reference test's NeighborLists{offsets: [0; n + 1]}), no
+// boundary groups, the given links and no warm start: fluid_v[2n], ball_v[2nb] and ball_w[nb]
+// are solved in place; *iters receives the PCG iterations.
+int or_probe_joint_solve(uint32_t n, float* fluid_v, uint32_t nb, float* ball_v, float* ball_w, uint32_t nl,
+                         const uint32_t* l_ball, const uint32_t* l_other, const float* l_n, const float* l_c,
+                         float mass, float ball_mass, float ball_inertia, float dt, uint32_t* iters) {
+  using namespace orc;
+  Nbr nbr;
+  nbr.off.assign(n + 1, 0);
+  ViscWeights w;
+  std::vector<BoundaryGroup> groups;
+  std::vector<SqueezeLink> links;
+  for (uint32_t k = 0; k < nl; ++k)
+    links.push_back({l_ball[k], l_other[k], Vec2(l_n[2 * k], l_n[2 * k + 1]), l_c[k]});
+  std::vector<Vec2> v(n), bv(nb), guess;
+  std::vector<float> bw(ball_w, ball_w + nb);
+  for (uint32_t i = 0; i < n; ++i) v[i] = Vec2(fluid_v[2 * i], fluid_v[2 * i + 1]);
+  for (uint32_t i = 0; i < nb; ++i) bv[i] = Vec2(ball_v[2 * i], ball_v[2 * i + 1]);
+  uint32_t it = solve_viscosity_with_balls(nbr, w, groups, links, mass, ball_mass, ball_inertia, dt, guess, &v, &bv,
+                                           &bw, false);
+  for (uint32_t i = 0; i < n; ++i) { fluid_v[2 * i] = v[i].x; fluid_v[2 * i + 1] = v[i].y; }
+  for (uint32_t i = 0; i < nb; ++i) { ball_v[2 * i] = bv[i].x; ball_v[2 * i + 1] = bv[i].y; ball_w[i] = bw[i]; }
+  if (iters) *iters = it;
+  return 0;
+}
+
+}  // extern "C"

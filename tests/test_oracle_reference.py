@@ -5,9 +5,14 @@ tunnelling and dissipation; lib.rs energy; metrics.rs mixing index), with the sa
 assertions (tests/scenarios_ref.py)."""
 from __future__ import annotations
 
+import ctypes as C
+
+import numpy as np
 import pytest
 
 import scenarios_ref as R
+
+F = np.float32
 
 
 @pytest.mark.parametrize("name", [
@@ -93,3 +98,133 @@ def test_bingham_slurry_damps_more_than_newtonian(oracle):
 
 def test_bingham_realtime_mill_steps(oracle):
     R.bingham_realtime_mill(oracle)
+
+
+# ---- the reference tests that call viscosity-stage functions directly (pbf.rs:2428, 2476,
+# 2513), through the oracle's probes of those functions. On the device the same functions run
+# inside the sub-step only; the step tests compare them with the oracle's bit for bit.
+
+def _f32p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _u32p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def _poly6(r2, h):
+    """pbf.rs:119-126 poly6 in f32 (2D: 4 / (pi h^8) (h^2 - r^2)^3 inside the support), for the
+    test's own densities."""
+    h = F(h)
+    h2 = h * h
+    if not (F(r2) < h2):
+        return F(0.0)
+    d = h2 - F(r2)
+    h8 = (h2 * h2) * (h2 * h2)
+    return ((F(4.0) / (F(np.pi) * h8)) * d) * d * d
+
+
+def test_viscous_operator_vanishes_for_rigid_rotation(oracle_lib):
+    # pbf.rs:2428 viscous_operator_vanishes_for_rigid_rotation_even_at_a_free_edge
+    from milldynamics3_b200.sim import probe_neighbor_lists
+    dx = F(0.02)
+    h = F(2.0) * dx
+    pts = []
+    for j in range(-4, 5):
+        for i in range(-4, 5):
+            pts.append((dx * (F(i) + F(0.5) * F(j & 1)), dx * F(0.8660254) * F(j)))
+    x = np.array(pts, F)
+    n = len(x)
+    rc, off, nbrs = probe_neighbor_lists(oracle_lib, x, float(h))
+    assert rc == 0
+    mass = F(1.0)
+    dens = np.empty(n, F)
+    for i in range(n):
+        s = F(0.0)
+        for k in range(off[i], off[i + 1]):
+            d = x[i] - x[nbrs[k]]
+            s = F(s + _poly6(d[0] * d[0] + d[1] * d[1], h))
+        dens[i] = mass * F(_poly6(F(0.0), h) + s)
+    mu = np.ones(n, F)
+    omega = F(3.0)
+    v = np.stack([omega * -x[:, 1], omega * x[:, 0]], 1).astype(F)
+    fn = oracle_lib.dll.or_probe_viscous_operator
+    fn.restype = C.c_int
+    out = np.zeros((n, 2), F)
+    wmax = C.c_float()
+    assert fn(_f32p(x), _f32p(v), _f32p(dens), _f32p(mu), n, C.c_float(h), C.c_float(mass), _f32p(out),
+              C.byref(wmax)) == 0
+    scale = F(wmax.value) * omega * F(4.0) * dx
+    worst = np.sqrt(out[:, 0] * out[:, 0] + out[:, 1] * out[:, 1]).max()
+    assert worst < F(1e-4) * scale, (worst, scale)
+    # a genuine shear, v = (y, 0), is dissipative
+    shear = np.stack([x[:, 1], np.zeros(n, F)], 1).astype(F)
+    assert fn(_f32p(x), _f32p(shear), _f32p(dens), _f32p(mu), n, C.c_float(h), C.c_float(mass), _f32p(out),
+              None) == 0
+    dissipated = np.add.accumulate((out[:, 0] * shear[:, 0] + out[:, 1] * shear[:, 1]).astype(F), dtype=F)[-1]
+    assert dissipated > 0.0
+
+
+def _links(oracle_lib, bx, r, m, drum_radius, dx, mu, dt, closing=None):
+    fn = oracle_lib.dll.or_probe_squeeze_links
+    fn.restype = C.c_int
+    bx = np.asarray(bx, F).reshape(-1, 2)
+    cap = 16
+    ball, other = np.zeros(cap, np.uint32), np.zeros(cap, np.uint32)
+    nrm, c = np.zeros((cap, 2), F), np.zeros(cap, F)
+    nout, inr = C.c_uint32(), C.c_uint32()
+    cl = None if closing is None else _f32p(np.asarray(closing, F).reshape(-1, 2))
+    assert fn(_f32p(bx), len(bx), C.c_float(r), C.c_float(m), C.c_float(drum_radius), C.c_float(dx), C.c_float(mu),
+              C.c_float(dt), cl, _u32p(ball), _u32p(other), _f32p(nrm), _f32p(c), cap, C.byref(nout),
+              C.byref(inr)) == 0
+    k = nout.value
+    return ball[:k], other[:k], nrm[:k], c[:k]
+
+
+def _two_balls(radius, gap):
+    half = F(radius) + F(0.5) * F(gap)
+    return [(-half, F(0.1)), (half, F(0.1))]
+
+
+def test_squeeze_links_exist_only_below_the_resolved_range(oracle_lib):
+    # pbf.rs:2476 squeeze_links_exist_only_for_gaps_below_the_resolved_range
+    dx = F(0.0125)
+    _, _, nrm, c = _links(oracle_lib, _two_balls(0.04, F(0.4) * dx), 0.04, 1.0, 0.5, dx, 100.0, 1e-3)
+    assert len(c) == 1 and c[0] > 0.0
+    assert np.hypot(nrm[0, 0] - 1.0, nrm[0, 1]) < 1e-6
+    _, _, _, c = _links(oracle_lib, _two_balls(0.04, F(9.0) * dx), 0.04, 1.0, 0.5, dx, 100.0, 1e-3)
+    assert len(c) == 0
+    # a ball hugging the wall gets a wall link with the outward normal
+    wall = [(0.0, -(F(0.5) - F(0.04) - F(0.3) * dx))]
+    _, other, nrm, c = _links(oracle_lib, wall, 0.04, 1.0, 0.5, dx, 100.0, 1e-3)
+    assert len(c) == 1 and other[0] == 0xFFFFFFFF
+    assert np.hypot(nrm[0, 0], nrm[0, 1] + 1.0) < 1e-5
+    # the approach filter the sub-step uses: only closing pairs keep their link
+    _, _, _, c = _links(oracle_lib, _two_balls(0.04, F(0.4) * dx), 0.04, 1.0, 0.5, dx, 100.0, 1e-3,
+                        closing=[(1.0, 0.0), (-1.0, 0.0)])
+    assert len(c) == 1
+    _, _, _, c = _links(oracle_lib, _two_balls(0.04, F(0.4) * dx), 0.04, 1.0, 0.5, dx, 100.0, 1e-3,
+                        closing=[(-1.0, 0.0), (1.0, 0.0)])
+    assert len(c) == 0
+
+
+def test_squeeze_link_damps_the_approach_and_conserves_momentum(oracle_lib):
+    # pbf.rs:2513 squeeze_link_damps_the_approach_and_conserves_momentum
+    m, dt = F(2.0), F(1e-3)
+    c = F(3.0) * m / dt
+    fn = oracle_lib.dll.or_probe_joint_solve
+    fn.restype = C.c_int
+    v = np.array([[0.3, -0.2]], F)
+    bv = np.array([[1.0, 0.5], [-1.0, 0.5]], F)
+    bw = np.zeros(2, F)
+    lb, lo = np.array([0], np.uint32), np.array([1], np.uint32)
+    ln, lc = np.array([[1.0, 0.0]], F), np.array([c], F)
+    it = C.c_uint32()
+    assert fn(1, _f32p(v), 2, _f32p(bv), _f32p(bw), 1, _u32p(lb), _u32p(lo), _f32p(ln), _f32p(lc), C.c_float(0.01),
+              C.c_float(m), C.c_float(0.1), C.c_float(dt), C.byref(it)) == 0
+    closing = (bv[0] - bv[1])[0]
+    assert abs(closing - 2.0 / 7.0) < 1e-3, closing
+    total = bv[0] + bv[1]
+    assert np.hypot(total[0], total[1] - 1.0) < 1e-4
+    assert abs(bv[0, 1] - 0.5) < 1e-5 and abs(bv[1, 1] - 0.5) < 1e-5
+    assert np.hypot(v[0, 0] - 0.3, v[0, 1] + 0.2) < 1e-6
