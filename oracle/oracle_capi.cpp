@@ -13,10 +13,41 @@ using namespace orc;
 static_assert(sizeof(MgParams) == sizeof(Params), "param layout");
 static_assert(sizeof(MgMediaParams) == sizeof(MediaParams), "media layout");
 static_assert(sizeof(MgSlurryParams) == sizeof(SlurryParams), "slurry layout");
-static_assert(sizeof(MgFluidStepStats) == sizeof(FluidStepStats), "fluid stats layout");
-static_assert(sizeof(MgDemStepStats) == sizeof(DemStepStats), "dem stats layout");
+static_assert(sizeof(Real) != sizeof(float) || sizeof(MgFluidStepStats) == sizeof(FluidStepStats),
+              "fluid stats layout");
+static_assert(sizeof(Real) != sizeof(float) || sizeof(MgDemStepStats) == sizeof(DemStepStats), "dem stats layout");
 static_assert(sizeof(MgImpactRecord) == sizeof(ImpactRecord), "impact layout");
 static_assert(sizeof(MgStepCounters) == sizeof(StepCounters), "counter layout");
+
+// The stats structs hold Real (f32 in the parity oracle, where this is a plain copy; f64 in the
+// FP64 oracle, rounded to the ABI's f32 here).
+static void to_mg(const FluidStepStats& a, MgFluidStepStats* o) {
+  o->viscosity_iterations = a.viscosity_iterations;
+  o->mean_shear_rate_per_s = (float)a.mean_shear_rate_per_s;
+  o->coupling_clamp_hits = a.coupling_clamp_hits;
+  o->wall_work_j = (float)a.wall_work_j;
+  o->wall_impulse[0] = (float)a.wall_impulse[0];
+  o->wall_impulse[1] = (float)a.wall_impulse[1];
+  o->wall_angular_impulse = (float)a.wall_angular_impulse;
+  for (int k = 0; k < WALL_IMPULSE_BINS; ++k) o->wall_normal_impulse_by_angle[k] = (float)a.wall_normal_impulse_by_angle[k];
+  o->ke_delta_noslip_j = (float)a.ke_delta_noslip_j;
+  o->ke_delta_drag_j = (float)a.ke_delta_drag_j;
+  o->ke_delta_buoyancy_j = (float)a.ke_delta_buoyancy_j;
+  o->ke_delta_viscosity_j = (float)a.ke_delta_viscosity_j;
+  o->ke_delta_clamp_j = (float)a.ke_delta_clamp_j;
+}
+static void to_mg(const DemStepStats& a, MgDemStepStats* o) {
+  o->wall_work_j = (float)a.wall_work_j;
+  o->collision_count = a.collision_count;
+  for (int k = 0; k < IMPACT_BINS; ++k) o->impact_energy_histogram[k] = a.impact_energy_histogram[k];
+  o->dissipated_energy_j = (float)a.dissipated_energy_j;
+  o->max_substep_displacement_over_diameter = (float)a.max_substep_displacement_over_diameter;
+  o->coupling_work_j = (float)a.coupling_work_j;
+}
+static std::vector<Real> reals(const float* a, uint32_t n) { return std::vector<Real>(a, a + n); }
+template <class V> static void put_reals(const V& v, float* out) {
+  if (out) for (size_t k = 0; k < v.size(); ++k) out[k] = (float)v[k];
+}
 
 struct OrSim {
   Simulation sim;
@@ -141,8 +172,8 @@ int or_coupling_step_recorded(OrSim* s, const MgDrum* drum, float drum_angle, co
   s->sim.last_counters = ctr;
   s->sim.fluid_stats = fs;
   s->sim.last_dem_stats = ds;
-  if (fstats) std::memcpy(fstats, &fs, sizeof(fs));
-  if (dstats) std::memcpy(dstats, &ds, sizeof(ds));
+  if (fstats) to_mg(fs, fstats);
+  if (dstats) to_mg(ds, dstats);
   if (n_out) *n_out = (uint32_t)recs.size();
   if (out)
     for (size_t k = 0; k < recs.size() && k < cap; ++k) std::memcpy(&out[k], &recs[k], sizeof(ImpactRecord));
@@ -162,9 +193,9 @@ int or_fluid_step_coupled(OrSim* s, const MgDrum* drum, float drum_angle, const 
                      s->sim.opt);
   s->sim.last_counters = ctr;
   s->sim.fluid_stats = fs;
-  if (fstats) std::memcpy(fstats, &fs, sizeof(fs));
+  if (fstats) to_mg(fs, fstats);
   put(imp.impulses, impulses);
-  if (angular) std::copy(imp.angular_impulses.begin(), imp.angular_impulses.end(), angular);
+  put_reals(imp.angular_impulses, angular);
   if (clamp_hits) *clamp_hits = imp.clamp_hits;
   if (fluid_momentum) { fluid_momentum[0] = imp.fluid_momentum_change.x; fluid_momentum[1] = imp.fluid_momentum_change.y; }
   return MG_OK;
@@ -187,7 +218,7 @@ int or_dem_step_recorded(OrSim* s, const MgDrum* drum, float drum_angle, const M
                                       &recs, &ctr, &s->sim.dbg);
   s->sim.last_counters = ctr;  // the DEM half's counters; the fluid ones read 0, as on the device
   s->sim.last_dem_stats = ds;
-  if (dstats) std::memcpy(dstats, &ds, sizeof(ds));
+  if (dstats) to_mg(ds, dstats);
   if (n_out) *n_out = (uint32_t)recs.size();
   if (out)
     for (size_t k = 0; k < recs.size() && k < cap; ++k) std::memcpy(&out[k], &recs[k], sizeof(ImpactRecord));
@@ -203,21 +234,21 @@ int or_get_balls(OrSim* s, float* x, float* v, float* theta, float* omega) {
   const Balls& b = s->sim.balls;
   put(b.x, x);
   put(b.v, v);
-  if (theta) std::copy(b.theta.begin(), b.theta.end(), theta);
-  if (omega) std::copy(b.omega.begin(), b.omega.end(), omega);
+  put_reals(b.theta, theta);
+  put_reals(b.omega, omega);
   return MG_OK;
 }
 int or_set_balls(OrSim* s, uint32_t n, const float* x, const float* v, const float* theta, const float* omega) {
   Balls& b = s->sim.balls;
   b.x = vecs(x, n);
   b.v = v ? vecs(v, n) : std::vector<Vec2>(n);
-  b.theta = theta ? std::vector<float>(theta, theta + n) : std::vector<float>(n, 0.0f);
-  b.omega = omega ? std::vector<float>(omega, omega + n) : std::vector<float>(n, 0.0f);
+  b.theta = theta ? reals(theta, n) : std::vector<Real>(n, Real(0));
+  b.omega = omega ? reals(omega, n) : std::vector<Real>(n, Real(0));
   return MG_OK;
 }
 int or_get_ball_material(const OrSim* s, MgBallMaterial* o) {
   const Balls& b = s->sim.balls;
-  *o = {b.radius, b.mass, b.inertia, b.true_radius};
+  *o = {(float)b.radius, (float)b.mass, (float)b.inertia, (float)b.true_radius};
   return MG_OK;
 }
 int or_set_ball_material(OrSim* s, const MgBallMaterial* m) {
@@ -232,7 +263,7 @@ int or_get_fluid(OrSim* s, float* x, float* v, float* dye, float* guess, uint32_
   const Fluid& f = s->sim.fluid;
   put(f.x, x);
   put(f.v, v);
-  if (dye) std::copy(f.dye.begin(), f.dye.end(), dye);
+  put_reals(f.dye, dye);
   if (guess_len) *guess_len = (uint32_t)f.viscous_guess.size();
   put(f.viscous_guess, guess);
   return MG_OK;
@@ -241,14 +272,14 @@ int or_set_fluid(OrSim* s, uint32_t n, const float* x, const float* v, const flo
   Fluid& f = s->sim.fluid;
   f.x = vecs(x, n);
   f.v = v ? vecs(v, n) : std::vector<Vec2>(n);
-  f.dye = dye ? std::vector<float>(dye, dye + n) : std::vector<float>(n, 0.0f);
+  f.dye = dye ? reals(dye, n) : std::vector<Real>(n, Real(0));
   if (guess) f.viscous_guess = vecs(guess, n);
   else f.viscous_guess.clear();
   return MG_OK;
 }
 int or_get_fluid_material(const OrSim* s, MgFluidMaterial* o) {
   const Fluid& f = s->sim.fluid;
-  *o = {f.particle_mass, f.h, f.rest_density};
+  *o = {(float)f.particle_mass, (float)f.h, (float)f.rest_density};
   return MG_OK;
 }
 int or_set_fluid_material(OrSim* s, const MgFluidMaterial* m) {
@@ -290,26 +321,26 @@ int or_metrics(OrSim* s, MgMetrics* out) {
 }
 int or_fluid_surface(OrSim* s, float* out, uint32_t cap, uint32_t* len) {
   if (!s || !len) { g_err = "null argument"; return MG_ERR_ARG; }
-  const std::vector<float> flat = surface_extract_flat(s->sim.fluid, s->sim.drum(), s->sim.drum_angle);
+  const std::vector<Real> flat = surface_extract_flat(s->sim.fluid, s->sim.drum(), s->sim.drum_angle);
   *len = (uint32_t)flat.size();
   if (!out) return MG_OK;
   if (cap < flat.size()) { g_err = "output buffer too small"; return MG_ERR_CAPACITY; }
-  std::copy(flat.begin(), flat.end(), out);
+  put_reals(flat, out);
   return MG_OK;
 }
 int or_surface_field(OrSim* s, float* field, float* phi_full) {
   if (!s) { g_err = "null argument"; return MG_ERR_ARG; }
   if (field) {
-    const std::vector<float> f = surface_build_field(s->sim.fluid, s->sim.drum(), s->sim.drum_angle);
-    std::copy(f.begin(), f.end(), field);
+    const std::vector<Real> f = surface_build_field(s->sim.fluid, s->sim.drum(), s->sim.drum_angle);
+    put_reals(f, field);
   }
   if (phi_full) *phi_full = surface_phi_full(s->sim.fluid);
   return MG_OK;
 }
 int or_mixing_index(OrSim* s, float* out, int* valid) {
-  float m = 0.0f;
+  Real m = Real(0);
   *valid = mixing_index(s->sim.fluid, s->sim.drum(), &m) ? 1 : 0;
-  *out = m;
+  *out = (float)m;
   return MG_OK;
 }
 int or_stress_histogram_rate(OrSim* s, double* out) {
@@ -322,14 +353,13 @@ int or_stress_set_debounce_factor(OrSim* s, double f) {
   return MG_OK;
 }
 int or_last_step_stats(OrSim* s, MgFluidStepStats* f, MgDemStepStats* d, MgStepCounters* c) {
-  if (f) std::memcpy(f, &s->sim.fluid_stats, sizeof(*f));
-  if (d) std::memcpy(d, &s->sim.last_dem_stats, sizeof(*d));
+  if (f) to_mg(s->sim.fluid_stats, f);
+  if (d) to_mg(s->sim.last_dem_stats, d);
   if (c) std::memcpy(c, &s->sim.last_counters, sizeof(*c));
   return MG_OK;
 }
 int or_fluid_densities(OrSim* s, float* out) {
-  std::vector<float> d = fluid_densities(s->sim.fluid);
-  std::copy(d.begin(), d.end(), out);
+  put_reals(fluid_densities(s->sim.fluid), out);
   return MG_OK;
 }
 double or_total_mechanical_energy(OrSim* s) { return s->sim.total_mechanical_energy_j(); }
@@ -397,14 +427,19 @@ int or_last_ball_pairs(OrSim* s, uint32_t* pairs, uint32_t cap, uint32_t* n_out)
 // ---- scalar helpers the reference's unit tests exercise
 void or_sdf_world(const MgDrum* drum, float px, float py, float angle, float* d, float* nx, float* ny) {
   Vec2 n;
-  to_drum(drum).sdf_world(Vec2(px, py), angle, d, &n);
-  *nx = n.x;
-  *ny = n.y;
+  Real dd;
+  to_drum(drum).sdf_world(Vec2(px, py), angle, &dd, &n);
+  *d = (float)dd;
+  *nx = (float)n.x;
+  *ny = (float)n.y;
 }
 float or_sdf_local(const MgDrum* drum, float px, float py) { return to_drum(drum).sdf(Vec2(px, py)); }
 int or_toi_swept(const MgDrum* drum, float x0, float y0, float x1, float y1, float a0, float a1, float radius,
                  float* t) {
-  return to_drum(drum).toi_swept(Vec2(x0, y0), Vec2(x1, y1), a0, a1, radius, t) ? 1 : 0;
+  Real tt = (Real)*t;  // left as the caller gave it unless the function writes it
+  const int hit = to_drum(drum).toi_swept(Vec2(x0, y0), Vec2(x1, y1), a0, a1, radius, &tt) ? 1 : 0;
+  *t = (float)tt;
+  return hit;
 }
 float or_effective_friction(float mk, float ms, float vt, float vs) { return effective_friction(mk, ms, vt, vs); }
 int or_impact_energy_bin(float e) { return impact_energy_bin(e); }

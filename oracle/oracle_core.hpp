@@ -28,57 +28,58 @@ struct MgMetrics;  // include/millgpu.h
 
 namespace orc {
 
-constexpr float PI_F = 3.14159265358979323846f;
-constexpr float TAU_F = 6.28318530717958647692f;
+// The arithmetic type of the restated kernels. The parity oracle is built with Real = float (the
+// reference's f32); the FP64 oracle is the same source built with -DORC_REAL=double, for the
+// per-output error reports of the f32 path. Params and their derived quantities stay f32 in both
+// builds (they are the reference's f32 inputs), so both builds step the same inputs.
+#ifndef ORC_REAL
+#define ORC_REAL float
+#endif
+using Real = ORC_REAL;
+
+constexpr Real PI_F = Real(3.14159265358979323846);
+constexpr Real TAU_F = Real(6.28318530717958647692);
 
 // Transcendentals. Every f32 exp/sin/cos/atan2/log10 of the reference is evaluated here as the
 // f32 rounding of the f64 function (error <= 0.5 ulp + 2^-29, against <= ~0.502 ulp for the
 // platform's f32 functions the Rust build calls), so that the device path, which evaluates them
-// the same way, can agree bit for bit.
-inline float expf_r(float x) { return (float)std::exp((double)x); }
-inline float sinf_r(float x) { return (float)std::sin((double)x); }
-inline float cosf_r(float x) { return (float)std::cos((double)x); }
-inline float atan2f_r(float y, float x) { return (float)std::atan2((double)y, (double)x); }
-inline float log10f_r(float x) { return (float)std::log10((double)x); }
+// the same way, can agree bit for bit. With T = double they are the f64 functions themselves.
+template <class T> inline T expf_r(T x) { return (T)std::exp((double)x); }
+template <class T> inline T sinf_r(T x) { return (T)std::sin((double)x); }
+template <class T> inline T cosf_r(T x) { return (T)std::cos((double)x); }
+template <class T> inline T atan2f_r(T y, T x) { return (T)std::atan2((double)y, (double)x); }
+template <class T> inline T log10f_r(T x) { return (T)std::log10((double)x); }
 
 // f32::max / f32::min (IEEE maxNum/minNum: a NaN operand yields the other operand).
-inline float fmax_r(float a, float b) {
+template <class T> inline T fmax_r(T a, T b) {
   if (std::isnan(a)) return b;
   if (std::isnan(b)) return a;
   return a > b ? a : b;
 }
-inline float fmin_r(float a, float b) {
+template <class T> inline T fmin_r(T a, T b) {
   if (std::isnan(a)) return b;
   if (std::isnan(b)) return a;
   return a < b ? a : b;
 }
-inline double dmax_r(double a, double b) {
-  if (std::isnan(a)) return b;
-  if (std::isnan(b)) return a;
-  return a > b ? a : b;
-}
+inline double dmax_r(double a, double b) { return fmax_r<double>(a, b); }
 // f32::clamp: `if x < lo {lo}; if x > hi {hi}` (a NaN passes through).
-inline float clamp_r(float x, float lo, float hi) {
+template <class T> inline T clamp_r(T x, T lo, T hi) {
   if (x < lo) x = lo;
   if (x > hi) x = hi;
   return x;
 }
-inline double dclamp_r(double x, double lo, double hi) {
-  if (x < lo) x = lo;
-  if (x > hi) x = hi;
-  return x;
-}
+inline double dclamp_r(double x, double lo, double hi) { return clamp_r<double>(x, lo, hi); }
 // Rust `f as i32`: saturating, NaN -> 0.
-inline int32_t f2i_sat(float f) {
+template <class T> inline int32_t f2i_sat(T f) {
   if (std::isnan(f)) return 0;
-  if (f >= 2147483648.0f) return INT32_MAX;
-  if (f <= -2147483648.0f) return INT32_MIN;
+  if (f >= T(2147483648.0)) return INT32_MAX;
+  if (f <= -T(2147483648.0)) return INT32_MIN;
   return (int32_t)f;
 }
 // Rust `f as u32` / `f as usize`: saturating at 0 below, NaN -> 0.
-inline uint32_t f2u_sat(float f) {
-  if (std::isnan(f) || f <= 0.0f) return 0;
-  if (f >= 4294967296.0f) return UINT32_MAX;
+template <class T> inline uint32_t f2u_sat(T f) {
+  if (std::isnan(f) || f <= T(0.0)) return 0;
+  if (f >= T(4294967296.0)) return UINT32_MAX;
   return (uint32_t)f;
 }
 inline uint64_t d2u64_sat(double f) {
@@ -92,48 +93,48 @@ inline int32_t sat_add_i32(int32_t a, int32_t b) {
   if (s < INT32_MIN) return INT32_MIN;
   return (int32_t)s;
 }
-inline float signum_r(float x) {
+template <class T> inline T signum_r(T x) {
   if (std::isnan(x)) return x;
-  return std::signbit(x) ? -1.0f : 1.0f;
+  return std::signbit(x) ? -T(1.0) : T(1.0);
 }
 // f32::rem_euclid: r = self % rhs; if r < 0 { r + |rhs| } else { r }.
-inline float rem_euclid_r(float x, float m) {
-  float r = std::fmod(x, m);
-  return r < 0.0f ? r + std::fabs(m) : r;
+template <class T> inline T rem_euclid_r(T x, T m) {
+  T r = std::fmod(x, m);
+  return r < T(0.0) ? r + std::fabs(m) : r;
 }
 // powi lowered by LLVM to binary exponentiation (x^3 = x * x^2, x^5 = x * x^4, x^6 = x^2 * x^4,
 // x^8 = x^4 * x^4); the same products compiler-rt's __powisf2 forms.
-inline float powi3(float x) { return x * (x * x); }
-inline float powi5(float x) { float x2 = x * x; float x4 = x2 * x2; return x * x4; }
-inline float powi6(float x) { float x2 = x * x; float x4 = x2 * x2; return x2 * x4; }
-inline float powi8(float x) { float x2 = x * x; float x4 = x2 * x2; return x4 * x4; }
+template <class T> inline T powi3(T x) { return x * (x * x); }
+template <class T> inline T powi5(T x) { T x2 = x * x; T x4 = x2 * x2; return x * x4; }
+template <class T> inline T powi6(T x) { T x2 = x * x; T x4 = x2 * x2; return x2 * x4; }
+template <class T> inline T powi8(T x) { T x2 = x * x; T x4 = x2 * x2; return x4 * x4; }
 
 struct Vec2 {
-  float x, y;
-  Vec2() : x(0.0f), y(0.0f) {}
-  Vec2(float a, float b) : x(a), y(b) {}
+  Real x, y;
+  Vec2() : x(Real(0.0)), y(Real(0.0)) {}
+  Vec2(Real a, Real b) : x(a), y(b) {}
   Vec2 operator+(Vec2 o) const { return Vec2(x + o.x, y + o.y); }
   Vec2 operator-(Vec2 o) const { return Vec2(x - o.x, y - o.y); }
   Vec2 operator-() const { return Vec2(-x, -y); }
-  Vec2 operator*(float s) const { return Vec2(x * s, y * s); }
-  Vec2 operator/(float s) const { return Vec2(x / s, y / s); }
+  Vec2 operator*(Real s) const { return Vec2(x * s, y * s); }
+  Vec2 operator/(Real s) const { return Vec2(x / s, y / s); }
   Vec2& operator+=(Vec2 o) { x += o.x; y += o.y; return *this; }
   Vec2& operator-=(Vec2 o) { x -= o.x; y -= o.y; return *this; }
-  Vec2& operator*=(float s) { x *= s; y *= s; return *this; }
-  float dot(Vec2 o) const { return (x * o.x) + (y * o.y); }
-  float length_squared() const { return dot(*this); }
-  float length() const { return std::sqrt(dot(*this)); }
+  Vec2& operator*=(Real s) { x *= s; y *= s; return *this; }
+  Real dot(Vec2 o) const { return (x * o.x) + (y * o.y); }
+  Real length_squared() const { return dot(*this); }
+  Real length() const { return std::sqrt(dot(*this)); }
   bool is_finite() const { return std::isfinite(x) && std::isfinite(y); }
-  Vec2 normalize() const { float rcp = 1.0f / length(); return *this * rcp; }
+  Vec2 normalize() const { Real rcp = Real(1.0) / length(); return *this * rcp; }
   Vec2 normalize_or_zero() const {
-    float rcp = 1.0f / length();
-    if (std::isfinite(rcp) && rcp > 0.0f) return *this * rcp;
+    Real rcp = Real(1.0) / length();
+    if (std::isfinite(rcp) && rcp > Real(0.0)) return *this * rcp;
     return Vec2();
   }
-  static Vec2 from_angle(float a) { return Vec2(cosf_r(a), sinf_r(a)); }
+  static Vec2 from_angle(Real a) { return Vec2(cosf_r(a), sinf_r(a)); }
 };
-inline Vec2 operator*(float s, Vec2 v) { return Vec2(s * v.x, s * v.y); }
-inline float cross2(Vec2 a, Vec2 b) { return a.x * b.y - a.y * b.x; }
+inline Vec2 operator*(Real s, Vec2 v) { return Vec2(s * v.x, s * v.y); }
+inline Real cross2(Vec2 a, Vec2 b) { return a.x * b.y - a.y * b.x; }
 
 // ---------------------------------------------------------------- params (params.rs)
 
@@ -206,7 +207,7 @@ struct Rng {
 
 // ---------------------------------------------------------------- grid.rs
 struct UniformGrid {
-  float cell_size = 1.0f;
+  Real cell_size = Real(1.0);
   bool dense = false;
   int32_t min_cx = 0, min_cy = 0;
   int64_t width = 0, height = 0;
@@ -214,10 +215,10 @@ struct UniformGrid {
   std::vector<uint32_t> cell_start;
   std::vector<uint32_t> indices;
 
-  static std::pair<int32_t, int32_t> cell_key(Vec2 p, float cell) {
+  static std::pair<int32_t, int32_t> cell_key(Vec2 p, Real cell) {
     return {f2i_sat(std::floor(p.x / cell)), f2i_sat(std::floor(p.y / cell))};
   }
-  static UniformGrid build(const std::vector<Vec2>& pts, float cell);
+  static UniformGrid build(const std::vector<Vec2>& pts, Real cell);
   bool cell_range(std::pair<int32_t, int32_t> key, size_t* s, size_t* e) const;
   template <class F> void for_each_candidate_pair(F f) const;
   template <class F> void for_each_near(Vec2 p, F f) const;
@@ -281,31 +282,31 @@ void UniformGrid::for_each_near(Vec2 p, F f) const {
 
 // ---------------------------------------------------------------- geometry.rs
 struct Drum {
-  float radius_m = 0.0f;
-  float omega = 0.0f;
+  Real radius_m = Real(0.0);
+  Real omega = Real(0.0);
   LiftersParams lifters{};
-  float sdf(Vec2 p_local) const;
-  float sdf_lifters(Vec2 p_local) const;
-  void sdf_world(Vec2 p_world, float drum_angle, float* d, Vec2* normal) const;
+  Real sdf(Vec2 p_local) const;
+  Real sdf_lifters(Vec2 p_local) const;
+  void sdf_world(Vec2 p_world, Real drum_angle, Real* d, Vec2* normal) const;
   Vec2 wall_velocity(Vec2 p) const { return omega * Vec2(-p.y, p.x); }
-  bool toi_swept(Vec2 x0, Vec2 x1, float a0, float a1, float radius, float* t_out) const;
+  bool toi_swept(Vec2 x0, Vec2 x1, Real a0, Real a1, Real radius, Real* t_out) const;
 };
 inline Vec2 rotate(Vec2 v, Vec2 u) { return Vec2(v.x * u.x - v.y * u.y, v.x * u.y + v.y * u.x); }
-float convex_polygon_sdf(Vec2 p, const Vec2* verts, int n);
-float lifter_cross_section_sdf(float pr, float pt, float r, float height, float base_half, float top_half);
+Real convex_polygon_sdf(Vec2 p, const Vec2* verts, int n);
+Real lifter_cross_section_sdf(Real pr, Real pt, Real r, Real height, Real base_half, Real top_half);
 
 // ---------------------------------------------------------------- dem.rs / pbf.rs state
 struct Balls {
   std::vector<Vec2> x, v;
-  std::vector<float> theta, omega;
-  float radius = 0.0f, mass = 0.0f, inertia = 0.0f, true_radius = 0.0f;
+  std::vector<Real> theta, omega;
+  Real radius = Real(0.0), mass = Real(0.0), inertia = Real(0.0), true_radius = Real(0.0);
   size_t len() const { return x.size(); }
 };
 struct Fluid {
   std::vector<Vec2> x, v;
-  std::vector<float> dye;
+  std::vector<Real> dye;
   std::vector<Vec2> viscous_guess;
-  float particle_mass = 0.0f, h = 0.0f, rest_density = 0.0f;
+  Real particle_mass = Real(0.0), h = Real(0.0), rest_density = Real(0.0);
   size_t len() const { return x.size(); }
 };
 
@@ -315,34 +316,34 @@ constexpr uint32_t WALL_ID = 0xFFFFFFFFu;
 
 struct CouplingImpulses {
   std::vector<Vec2> impulses;
-  std::vector<float> angular_impulses;
+  std::vector<Real> angular_impulses;
   uint32_t clamp_hits = 0;
   Vec2 fluid_momentum_change;
   void zeros(size_t nb) {
     impulses.assign(nb, Vec2());
-    angular_impulses.assign(nb, 0.0f);
+    angular_impulses.assign(nb, Real(0.0));
     clamp_hits = 0;
     fluid_momentum_change = Vec2();
   }
 };
 struct FluidStepStats {
   uint32_t viscosity_iterations = 0;
-  float mean_shear_rate_per_s = 0.0f;
+  Real mean_shear_rate_per_s = Real(0.0);
   uint32_t coupling_clamp_hits = 0;
-  float wall_work_j = 0.0f;
-  float wall_impulse[2] = {0.0f, 0.0f};
-  float wall_angular_impulse = 0.0f;
-  float wall_normal_impulse_by_angle[WALL_IMPULSE_BINS] = {};
-  float ke_delta_noslip_j = 0.0f, ke_delta_drag_j = 0.0f, ke_delta_buoyancy_j = 0.0f;
-  float ke_delta_viscosity_j = 0.0f, ke_delta_clamp_j = 0.0f;
+  Real wall_work_j = Real(0.0);
+  Real wall_impulse[2] = {Real(0.0), Real(0.0)};
+  Real wall_angular_impulse = Real(0.0);
+  Real wall_normal_impulse_by_angle[WALL_IMPULSE_BINS] = {};
+  Real ke_delta_noslip_j = Real(0.0), ke_delta_drag_j = Real(0.0), ke_delta_buoyancy_j = Real(0.0);
+  Real ke_delta_viscosity_j = Real(0.0), ke_delta_clamp_j = Real(0.0);
 };
 struct DemStepStats {
-  float wall_work_j = 0.0f;
+  Real wall_work_j = Real(0.0);
   uint32_t collision_count = 0;
   uint32_t impact_energy_histogram[IMPACT_BINS] = {};
-  float dissipated_energy_j = 0.0f;
-  float max_substep_displacement_over_diameter = 0.0f;
-  float coupling_work_j = 0.0f;
+  Real dissipated_energy_j = Real(0.0);
+  Real max_substep_displacement_over_diameter = Real(0.0);
+  Real coupling_work_j = Real(0.0);
 };
 struct ImpactRecord {
   uint32_t kind;  // 0 ball-ball, 1 ball-wall
@@ -362,31 +363,31 @@ struct Debug {
   std::vector<std::pair<uint32_t, uint32_t>> ball_pairs;
 };
 
-void fluid_seed_lattice(Fluid* f, const SlurryParams& s, float drum_r, uint32_t res,
-                        const std::vector<Vec2>& balls, float ball_r);
-void balls_seed_lattice(Balls* b, const EffectiveMedia& e, float drum_r, uint64_t seed);
-float ball_mass(float d, float rho);
-float ball_inertia(float m, float r);
+void fluid_seed_lattice(Fluid* f, const SlurryParams& s, Real drum_r, uint32_t res,
+                        const std::vector<Vec2>& balls, Real ball_r);
+void balls_seed_lattice(Balls* b, const EffectiveMedia& e, Real drum_r, uint64_t seed);
+Real ball_mass(Real d, Real rho);
+Real ball_inertia(Real m, Real r);
 
 // Reduction mode of the viscosity solve's inner products: 0 = the reference's sequential f32 sums,
 // 1 = f64 sums (the device path's FP64 mode).
 struct SolveOptions { int cg_fp64 = 0; };
 
-void fluid_step_coupled(Fluid* f, const Drum& drum, float drum_angle, const SlurryParams& slurry,
-                        uint32_t iterations, float dt, const Balls& balls, CouplingImpulses* out,
+void fluid_step_coupled(Fluid* f, const Drum& drum, Real drum_angle, const SlurryParams& slurry,
+                        uint32_t iterations, Real dt, const Balls& balls, CouplingImpulses* out,
                         FluidStepStats* stats, StepCounters* ctr, Debug* dbg, const SolveOptions& opt);
-DemStepStats dem_step_recorded(Balls* b, const Drum& drum, float drum_angle, const MediaParams& media,
-                               uint32_t iterations, float dt, const CouplingImpulses* ext,
+DemStepStats dem_step_recorded(Balls* b, const Drum& drum, Real drum_angle, const MediaParams& media,
+                               uint32_t iterations, Real dt, const CouplingImpulses* ext,
                                std::vector<ImpactRecord>* impacts, StepCounters* ctr, Debug* dbg);
 double dem_mechanical_energy_f64(const Balls& b);
 double fluid_mechanical_energy(const Fluid& f);
-std::vector<float> fluid_densities(const Fluid& f);
-std::vector<std::pair<uint32_t, uint32_t>> candidate_pairs(const std::vector<Vec2>& pts, float cell);
-void neighbor_lists(const std::vector<Vec2>& x, float h, std::vector<uint32_t>* offsets,
+std::vector<Real> fluid_densities(const Fluid& f);
+std::vector<std::pair<uint32_t, uint32_t>> candidate_pairs(const std::vector<Vec2>& pts, Real cell);
+void neighbor_lists(const std::vector<Vec2>& x, Real h, std::vector<uint32_t>* offsets,
                     std::vector<uint32_t>* nbrs);
-float effective_friction(float mu_k, float mu_s, float v_t, float vs);
-int impact_energy_bin(float e);
-float restitution_velocity_threshold(float r);
+Real effective_friction(Real mu_k, Real mu_s, Real v_t, Real vs);
+int impact_energy_bin(Real e);
+Real restitution_velocity_threshold(Real r);
 
 // ---------------------------------------------------------------- stress.rs
 constexpr int SE_BINS = 28;
@@ -413,15 +414,15 @@ struct EnergyBudget {
 
 struct Simulation {
   Params params{};
-  float drum_angle = 0.0f;
+  Real drum_angle = Real(0.0);
   double sim_time = 0.0;
   Balls balls;
   Fluid fluid;
   FluidStepStats fluid_stats;
-  float power_draw_w = 0.0f, torque_nm = 0.0f, collision_rate_per_s = 0.0f, dissipated_power_w = 0.0f;
+  Real power_draw_w = Real(0.0), torque_nm = Real(0.0), collision_rate_per_s = Real(0.0), dissipated_power_w = Real(0.0);
   std::vector<ImpactRecord> impact_log;
   StressAccum stress;
-  float max_substep_displacement_over_diameter = 0.0f;
+  Real max_substep_displacement_over_diameter = Real(0.0);
   uint32_t coupling_clamp_hits = 0;
   EnergyBudget energy_budget;
   double energy_budget_e0 = 0.0;
@@ -433,21 +434,21 @@ struct Simulation {
   static bool build(const Params& p, const std::vector<Vec2>* initial, Simulation* out, std::string* err);
   double total_mechanical_energy_j() const;
   EnergyBudget energy_budget_now() const;
-  float fixed_sub_dt() const;
+  Real fixed_sub_dt() const;
   void reset_frame_stats();
-  void step(float dt);
+  void step(Real dt);
   void step_fixed();
-  void advance_one_sub_step(float sub_dt);
-  void update_grinding_stats(const DemStepStats& s, float fluid_wall_work, float sub_dt, float omega);
+  void advance_one_sub_step(Real sub_dt);
+  void update_grinding_stats(const DemStepStats& s, Real fluid_wall_work, Real sub_dt, Real omega);
   void stress_scales(double* m3, double* scale_j, double* d) const;
   Drum drum() const;
 };
 
-bool mixing_index(const Fluid& f, const Drum& d, float* out);
-void metrics_compute(const Balls& b, const Fluid& f, const Drum& d, float drum_angle, ::MgMetrics* out);
-float surface_phi_full(const Fluid& f);
-std::vector<float> surface_build_field(const Fluid& f, const Drum& drum, float drum_angle);
-std::vector<float> surface_extract_flat(const Fluid& f, const Drum& drum, float drum_angle);
+bool mixing_index(const Fluid& f, const Drum& d, Real* out);
+void metrics_compute(const Balls& b, const Fluid& f, const Drum& d, Real drum_angle, ::MgMetrics* out);
+Real surface_phi_full(const Fluid& f);
+std::vector<Real> surface_build_field(const Fluid& f, const Drum& drum, Real drum_angle);
+std::vector<Real> surface_extract_flat(const Fluid& f, const Drum& drum, Real drum_angle);
 uint64_t state_hash(const Balls& b, const Fluid& f, bool extended);
 
 }  // namespace orc

@@ -177,33 +177,33 @@ bool preset_apply(Params* p, const char* id) {
 }
 
 // ------------------------------------------------------------------ dem.rs:230-239, 355-409
-float ball_mass(float d, float rho) { float r = d * 0.5f; return rho * PI_F * r * r; }
-float ball_inertia(float m, float r) { return 0.5f * m * r * r; }
+Real ball_mass(Real d, Real rho) { Real r = d * Real(0.5); return rho * PI_F * r * r; }
+Real ball_inertia(Real m, Real r) { return Real(0.5) * m * r * r; }
 
-void balls_seed_lattice(Balls* b, const EffectiveMedia& e, float drum_r, uint64_t seed) {
-  float r = e.diameter_m * 0.5f;
-  float mass = ball_mass(e.diameter_m, e.density_kg_m3);
-  float inertia = ball_inertia(mass, r);
+void balls_seed_lattice(Balls* b, const EffectiveMedia& e, Real drum_r, uint64_t seed) {
+  Real r = e.diameter_m * Real(0.5);
+  Real mass = ball_mass(e.diameter_m, e.density_kg_m3);
+  Real inertia = ball_inertia(mass, r);
   size_t count = e.ball_count;
   Rng rng(seed);
   std::vector<Vec2> x;
-  if (r > 0.0f && count > 0) {
-    float spacing = 2.0f * r * 1.02f;
-    float row_h = spacing * (std::sqrt(3.0f) * 0.5f);
-    float fill_r = fmax_r(drum_r - r, 0.0f);
-    int32_t n_rows = f2i_sat(std::ceil(2.0f * fill_r / row_h)) + 1;
+  if (r > Real(0.0) && count > 0) {
+    Real spacing = Real(2.0) * r * Real(1.02);
+    Real row_h = spacing * (std::sqrt(Real(3.0)) * Real(0.5));
+    Real fill_r = fmax_r(drum_r - r, Real(0.0));
+    int32_t n_rows = f2i_sat(std::ceil(Real(2.0) * fill_r / row_h)) + 1;
     bool done = false;
     for (int32_t row = -n_rows / 2; row <= n_rows / 2 && !done; ++row) {
-      float y = (float)row * row_h;
+      Real y = (Real)row * row_h;
       if (std::fabs(y) > fill_r) continue;
-      float half_width = std::sqrt(fmax_r(fill_r * fill_r - y * y, 0.0f));
-      float offset = (((row % 2) + 2) % 2 == 0) ? 0.0f : spacing * 0.5f;
-      int32_t n_cols = f2i_sat(std::floor(2.0f * half_width / spacing));
+      Real half_width = std::sqrt(fmax_r(fill_r * fill_r - y * y, Real(0.0)));
+      Real offset = (((row % 2) + 2) % 2 == 0) ? Real(0.0) : spacing * Real(0.5);
+      int32_t n_cols = f2i_sat(std::floor(Real(2.0) * half_width / spacing));
       for (int32_t col = -n_cols / 2; col <= n_cols / 2; ++col) {
-        float cx = (float)col * spacing + offset;
+        Real cx = (Real)col * spacing + offset;
         if (cx * cx + y * y > fill_r * fill_r) continue;
-        float jx = rng.range_f32(-0.05f, 0.05f);
-        float jy = rng.range_f32(-0.05f, 0.05f);
+        Real jx = rng.range_f32(-Real(0.05), Real(0.05));
+        Real jy = rng.range_f32(-Real(0.05), Real(0.05));
         Vec2 jitter = Vec2(jx, jy) * r;
         x.push_back(Vec2(cx, y) + jitter);
         if (x.size() >= count) { done = true; break; }
@@ -214,45 +214,45 @@ void balls_seed_lattice(Balls* b, const EffectiveMedia& e, float drum_r, uint64_
   size_t n = x.size();
   b->x = x;
   b->v.assign(n, Vec2());
-  b->theta.assign(n, 0.0f);
-  b->omega.assign(n, 0.0f);
+  b->theta.assign(n, Real(0.0));
+  b->omega.assign(n, Real(0.0));
   b->radius = r;
   b->mass = mass;
   b->inertia = inertia;
-  b->true_radius = e.true_diameter_m * 0.5f;
+  b->true_radius = e.true_diameter_m * Real(0.5);
 }
 
 // pbf.rs:2370-2388
-static float dye_value(uint32_t pattern, Vec2 p) {
-  if (pattern == DYE_LEFT_RIGHT) return p.x < 0.0f ? 0.0f : 1.0f;
-  if (pattern == DYE_TOP_BOTTOM) return p.y < 0.0f ? 0.0f : 1.0f;
-  return 0.0f;
+static Real dye_value(uint32_t pattern, Vec2 p) {
+  if (pattern == DYE_LEFT_RIGHT) return p.x < Real(0.0) ? Real(0.0) : Real(1.0);
+  if (pattern == DYE_TOP_BOTTOM) return p.y < Real(0.0) ? Real(0.0) : Real(1.0);
+  return Real(0.0);
 }
 
 // pbf.rs:1044-1119
-void fluid_seed_lattice(Fluid* f, const SlurryParams& s, float drum_r, uint32_t res,
-                        const std::vector<Vec2>& balls, float ball_r) {
-  float dx = drum_r / (float)std::max(res, 1u);
-  float h = 2.0f * dx;
-  float rest_density = s.density_kg_m3;
-  float row_h = dx * (std::sqrt(3.0f) * 0.5f);
-  float cell_area = dx * row_h;
-  float particle_mass = rest_density * cell_area;
-  float target_area = s.fill_fraction * PI_F * drum_r * drum_r;
-  size_t target_count = f2u_sat(fmax_r(std::round(target_area / cell_area), 0.0f));
+void fluid_seed_lattice(Fluid* f, const SlurryParams& s, Real drum_r, uint32_t res,
+                        const std::vector<Vec2>& balls, Real ball_r) {
+  Real dx = drum_r / (Real)std::max(res, 1u);
+  Real h = Real(2.0) * dx;
+  Real rest_density = s.density_kg_m3;
+  Real row_h = dx * (std::sqrt(Real(3.0)) * Real(0.5));
+  Real cell_area = dx * row_h;
+  Real particle_mass = rest_density * cell_area;
+  Real target_area = s.fill_fraction * PI_F * drum_r * drum_r;
+  size_t target_count = f2u_sat(fmax_r(std::round(target_area / cell_area), Real(0.0)));
   std::vector<Vec2> x;
-  std::vector<float> dye;
-  if (target_count > 0 && dx > 0.0f) {
-    int32_t n_rows = f2i_sat(std::ceil(2.0f * drum_r / row_h)) + 1;
+  std::vector<Real> dye;
+  if (target_count > 0 && dx > Real(0.0)) {
+    int32_t n_rows = f2i_sat(std::ceil(Real(2.0) * drum_r / row_h)) + 1;
     bool done = false;
     for (int32_t row = -n_rows / 2; row <= n_rows / 2 && !done; ++row) {
-      float y = (float)row * row_h;
+      Real y = (Real)row * row_h;
       if (std::fabs(y) > drum_r) continue;
-      float half_width = std::sqrt(fmax_r(drum_r * drum_r - y * y, 0.0f));
-      float offset = (((row % 2) + 2) % 2 == 0) ? 0.0f : dx * 0.5f;
-      int32_t n_cols = f2i_sat(std::floor(2.0f * half_width / dx));
+      Real half_width = std::sqrt(fmax_r(drum_r * drum_r - y * y, Real(0.0)));
+      Real offset = (((row % 2) + 2) % 2 == 0) ? Real(0.0) : dx * Real(0.5);
+      int32_t n_cols = f2i_sat(std::floor(Real(2.0) * half_width / dx));
       for (int32_t col = -n_cols / 2; col <= n_cols / 2; ++col) {
-        float cx = (float)col * dx + offset;
+        Real cx = (Real)col * dx + offset;
         if (cx * cx + y * y > drum_r * drum_r) continue;
         Vec2 p(cx, y);
         bool overlaps = false;
@@ -276,7 +276,7 @@ void fluid_seed_lattice(Fluid* f, const SlurryParams& s, float drum_r, uint32_t 
 }
 
 // ------------------------------------------------------------------ grid.rs:101-270
-UniformGrid UniformGrid::build(const std::vector<Vec2>& pts, float cell) {
+UniformGrid UniformGrid::build(const std::vector<Vec2>& pts, Real cell) {
   UniformGrid g;
   g.cell_size = cell;
   std::vector<std::pair<std::pair<int32_t, int32_t>, uint32_t>> keyed;
@@ -357,7 +357,7 @@ bool UniformGrid::cell_range(std::pair<int32_t, int32_t> key, size_t* s, size_t*
   return true;
 }
 
-std::vector<std::pair<uint32_t, uint32_t>> candidate_pairs(const std::vector<Vec2>& pts, float cell) {
+std::vector<std::pair<uint32_t, uint32_t>> candidate_pairs(const std::vector<Vec2>& pts, Real cell) {
   std::vector<std::pair<uint32_t, uint32_t>> out;
   UniformGrid g = UniformGrid::build(pts, cell);
   g.for_each_candidate_pair([&](uint32_t i, uint32_t j) { out.push_back({i, j}); });
@@ -365,91 +365,91 @@ std::vector<std::pair<uint32_t, uint32_t>> candidate_pairs(const std::vector<Vec
 }
 
 // ------------------------------------------------------------------ geometry.rs
-float Drum::sdf(Vec2 p) const {
-  float d = radius_m - p.length();
+Real Drum::sdf(Vec2 p) const {
+  Real d = radius_m - p.length();
   if (lifters.count == 0) return d;
   return fmin_r(d, sdf_lifters(p));
 }
 
-float Drum::sdf_lifters(Vec2 p) const {
+Real Drum::sdf_lifters(Vec2 p) const {
   uint32_t n = lifters.count;
-  const float rads_per_deg = PI_F / 180.0f;
-  float phase = lifters.phase_deg * rads_per_deg;
-  float max_inside = -INFINITY;
+  const Real rads_per_deg = PI_F / Real(180.0);
+  Real phase = lifters.phase_deg * rads_per_deg;
+  Real max_inside = -INFINITY;
   for (uint32_t k = 0; k < n; ++k) {
-    float theta_i = phase + (float)k * TAU_F / (float)n;
-    float s = sinf_r(theta_i), c = cosf_r(theta_i);
-    float pr = p.x * c + p.y * s;
-    float pt = -p.x * s + p.y * c;
-    float inside = lifter_cross_section_sdf(pr, pt, radius_m, lifters.height_m, lifters.base_width_m * 0.5f,
-                                            lifters.top_width_m * 0.5f);
+    Real theta_i = phase + (Real)k * TAU_F / (Real)n;
+    Real s = sinf_r(theta_i), c = cosf_r(theta_i);
+    Real pr = p.x * c + p.y * s;
+    Real pt = -p.x * s + p.y * c;
+    Real inside = lifter_cross_section_sdf(pr, pt, radius_m, lifters.height_m, lifters.base_width_m * Real(0.5),
+                                            lifters.top_width_m * Real(0.5));
     max_inside = fmax_r(max_inside, inside);
   }
   return -max_inside;
 }
 
-void Drum::sdf_world(Vec2 pw, float angle, float* d, Vec2* normal) const {
-  if (!pw.is_finite()) { *d = 0.0f; *normal = Vec2(); return; }
+void Drum::sdf_world(Vec2 pw, Real angle, Real* d, Vec2* normal) const {
+  if (!pw.is_finite()) { *d = Real(0.0); *normal = Vec2(); return; }
   Vec2 to_local = Vec2::from_angle(-angle);
   Vec2 pl = rotate(pw, to_local);
-  const float EPS = 1e-4f;
-  float dd = sdf(pl);
-  float gx = sdf(pl + Vec2(EPS, 0.0f)) - sdf(pl - Vec2(EPS, 0.0f));
-  float gy = sdf(pl + Vec2(0.0f, EPS)) - sdf(pl - Vec2(0.0f, EPS));
-  Vec2 grad = Vec2(gx, gy) / (2.0f * EPS);
-  Vec2 nl = grad.length_squared() > 1e-12f ? grad.normalize() : -pl.normalize_or_zero();
+  const Real EPS = Real(1e-4);
+  Real dd = sdf(pl);
+  Real gx = sdf(pl + Vec2(EPS, Real(0.0))) - sdf(pl - Vec2(EPS, Real(0.0)));
+  Real gy = sdf(pl + Vec2(Real(0.0), EPS)) - sdf(pl - Vec2(Real(0.0), EPS));
+  Vec2 grad = Vec2(gx, gy) / (Real(2.0) * EPS);
+  Vec2 nl = grad.length_squared() > Real(1e-12) ? grad.normalize() : -pl.normalize_or_zero();
   Vec2 to_world = Vec2::from_angle(angle);
   *d = dd;
   *normal = rotate(nl, to_world);
 }
 
-bool Drum::toi_swept(Vec2 x0, Vec2 x1, float a0, float a1, float radius, float* t_out) const {
+bool Drum::toi_swept(Vec2 x0, Vec2 x1, Real a0, Real a1, Real radius, Real* t_out) const {
   Vec2 local0 = rotate(x0, Vec2::from_angle(-a0));
-  if (sdf(local0) - radius <= 0.0f) return false;
+  if (sdf(local0) - radius <= Real(0.0)) return false;
   Vec2 path = x1 - x0;
-  float path_len = path.length();
-  float dangle = a1 - a0;
-  float pos_bound = x0.length() + path_len;
-  float bound = path_len + std::fabs(dangle) * pos_bound;
-  if (bound < 1e-9f) return false;
-  float t = 0.0f;
+  Real path_len = path.length();
+  Real dangle = a1 - a0;
+  Real pos_bound = x0.length() + path_len;
+  Real bound = path_len + std::fabs(dangle) * pos_bound;
+  if (bound < Real(1e-9)) return false;
+  Real t = Real(0.0);
   for (int it = 0; it < 32; ++it) {
-    float angle_t = a0 + dangle * t;
+    Real angle_t = a0 + dangle * t;
     Vec2 x_t = x0 + path * t;
     Vec2 local = rotate(x_t, Vec2::from_angle(-angle_t));
-    float d = sdf(local) - radius;
-    if (d <= 0.0f) { *t_out = t; return true; }
-    float step_t = fmax_r(d / bound, 1e-6f);
+    Real d = sdf(local) - radius;
+    if (d <= Real(0.0)) { *t_out = t; return true; }
+    Real step_t = fmax_r(d / bound, Real(1e-6));
     t += step_t;
-    if (t >= 1.0f) return false;
+    if (t >= Real(1.0)) return false;
   }
-  *t_out = fmin_r(t, 1.0f);
+  *t_out = fmin_r(t, Real(1.0));
   return true;
 }
 
-float lifter_cross_section_sdf(float pr, float pt, float r, float height, float base_half, float top_half) {
-  float r_top = r - height;
+Real lifter_cross_section_sdf(Real pr, Real pt, Real r, Real height, Real base_half, Real top_half) {
+  Real r_top = r - height;
   Vec2 verts[4] = {Vec2(r, -base_half), Vec2(r, base_half), Vec2(r_top, top_half), Vec2(r_top, -top_half)};
   return convex_polygon_sdf(Vec2(pr, pt), verts, 4);
 }
 
-float convex_polygon_sdf(Vec2 p, const Vec2* verts, int n) {
-  float min_dist_sq = 3.40282347e38f;
+Real convex_polygon_sdf(Vec2 p, const Vec2* verts, int n) {
+  Real min_dist_sq = Real(3.40282347e38);
   bool inside = true;
   for (int i = 0; i < n; ++i) {
     Vec2 a = verts[i];
     Vec2 b = verts[(i + 1) % n];
     Vec2 edge = b - a;
     Vec2 to_p = p - a;
-    float len_sq = edge.length_squared();
-    if (len_sq < 1e-12f) continue;
-    float t = clamp_r(to_p.dot(edge) / len_sq, 0.0f, 1.0f);
+    Real len_sq = edge.length_squared();
+    if (len_sq < Real(1e-12)) continue;
+    Real t = clamp_r(to_p.dot(edge) / len_sq, Real(0.0), Real(1.0));
     Vec2 closest = a + edge * t;
     min_dist_sq = fmin_r(min_dist_sq, (p - closest).length_squared());
-    float cross = edge.x * to_p.y - edge.y * to_p.x;
-    if (cross < 0.0f) inside = false;
+    Real cross = edge.x * to_p.y - edge.y * to_p.x;
+    if (cross < Real(0.0)) inside = false;
   }
-  float dist = std::sqrt(min_dist_sq);
+  Real dist = std::sqrt(min_dist_sq);
   return inside ? dist : -dist;
 }
 

@@ -69,7 +69,7 @@ void StressAccum::update(const std::vector<ImpactRecord>& recs, double m3, doubl
 // ------------------------------------------------------------------ lib.rs:138-204
 bool Simulation::build(const Params& p, const std::vector<Vec2>* initial, Simulation* s, std::string* err) {
   if (!params_validate(p, err)) return false;
-  float radius = mill_radius(p.mill);
+  Real radius = mill_radius(p.mill);
   EffectiveMedia eff = effective_media(p);
   s->params = p;
   balls_seed_lattice(&s->balls, eff, radius, p.simulation.seed);
@@ -77,25 +77,25 @@ bool Simulation::build(const Params& p, const std::vector<Vec2>* initial, Simula
     size_t n = initial->size();
     s->balls.x = *initial;
     s->balls.v.assign(n, Vec2());
-    s->balls.theta.assign(n, 0.0f);
-    s->balls.omega.assign(n, 0.0f);
+    s->balls.theta.assign(n, Real(0.0));
+    s->balls.omega.assign(n, Real(0.0));
   }
   uint32_t res = effective_fluid_resolution(p);
   if (p.slurry.enabled) {
     fluid_seed_lattice(&s->fluid, p.slurry, radius, res, s->balls.x, s->balls.radius);
   } else {
     SlurryParams sp = p.slurry;
-    sp.fill_fraction = 0.0f;
-    fluid_seed_lattice(&s->fluid, sp, radius, res, std::vector<Vec2>(), 0.0f);
+    sp.fill_fraction = Real(0.0);
+    fluid_seed_lattice(&s->fluid, sp, radius, res, std::vector<Vec2>(), Real(0.0));
   }
   if (initial) {
-    float w = mill_omega(p.mill);
+    Real w = mill_omega(p.mill);
     for (size_t i = 0; i < s->balls.len(); ++i) s->balls.v[i] = w * Vec2(-s->balls.x[i].y, s->balls.x[i].x);
     for (size_t i = 0; i < s->balls.len(); ++i) s->balls.omega[i] = w;
     for (size_t i = 0; i < s->fluid.len(); ++i) s->fluid.v[i] = w * Vec2(-s->fluid.x[i].y, s->fluid.x[i].x);
   }
   s->energy_budget_e0 = dem_mechanical_energy_f64(s->balls) + fluid_mechanical_energy(s->fluid);
-  s->drum_angle = 0.0f;
+  s->drum_angle = Real(0.0);
   s->sim_time = 0.0;
   return true;
 }
@@ -131,22 +131,22 @@ Drum Simulation::drum() const {
 }
 
 // lib.rs:426-464
-float Simulation::fixed_sub_dt() const { return 1.0f / (60.0f * (float)std::max(effective_substeps(params), 1u)); }
+Real Simulation::fixed_sub_dt() const { return Real(1.0) / (Real(60.0) * (Real)std::max(effective_substeps(params), 1u)); }
 void Simulation::reset_frame_stats() {
-  max_substep_displacement_over_diameter = 0.0f;
+  max_substep_displacement_over_diameter = Real(0.0);
   coupling_clamp_hits = 0;
 }
 void Simulation::step_fixed() { advance_one_sub_step(fixed_sub_dt()); }
-void Simulation::step(float dt) {
+void Simulation::step(Real dt) {
   uint32_t n = std::max(effective_substeps(params), 1u);
-  float sub_dt = dt / (float)n;
+  Real sub_dt = dt / (Real)n;
   reset_frame_stats();
   for (uint32_t k = 0; k < n; ++k) advance_one_sub_step(sub_dt);
 }
 
 // lib.rs:470-509
-void Simulation::advance_one_sub_step(float sub_dt) {
-  float omega = mill_omega(params.mill);
+void Simulation::advance_one_sub_step(Real sub_dt) {
+  Real omega = mill_omega(params.mill);
   Drum d = drum();
   impact_log.clear();
   CouplingImpulses imp;
@@ -177,33 +177,33 @@ void Simulation::advance_one_sub_step(float sub_dt) {
 }
 
 // lib.rs:516-565
-void Simulation::update_grinding_stats(const DemStepStats& s, float fluid_wall_work, float sub_dt, float omega) {
-  float alpha = 1.0f - expf_r(-sub_dt / 1.0f);
-  float power_instant = (s.wall_work_j + fluid_wall_work) / sub_dt;
+void Simulation::update_grinding_stats(const DemStepStats& s, Real fluid_wall_work, Real sub_dt, Real omega) {
+  Real alpha = Real(1.0) - expf_r(-sub_dt / Real(1.0));
+  Real power_instant = (s.wall_work_j + fluid_wall_work) / sub_dt;
   power_draw_w += alpha * (power_instant - power_draw_w);
-  float torque_instant = std::fabs(omega) > 1e-6f ? power_instant / omega : 0.0f;
+  Real torque_instant = std::fabs(omega) > Real(1e-6) ? power_instant / omega : Real(0.0);
   torque_nm += alpha * (torque_instant - torque_nm);
   double m3, scale_j, d;
   stress_scales(&m3, &scale_j, &d);
   stress.update(impact_log, m3, scale_j, d, sim_time, (double)sub_dt, (double)alpha,
                 (double)(s.wall_work_j + fluid_wall_work));
-  collision_rate_per_s = (float)stress.total_rate();
-  float dissipated_instant = fmax_r(s.dissipated_energy_j, 0.0f) / sub_dt;
+  collision_rate_per_s = (Real)stress.total_rate();
+  Real dissipated_instant = fmax_r(s.dissipated_energy_j, Real(0.0)) / sub_dt;
   dissipated_power_w += alpha * (dissipated_instant - dissipated_power_w);
   max_substep_displacement_over_diameter =
       fmax_r(max_substep_displacement_over_diameter, s.max_substep_displacement_over_diameter);
 }
 
 // ------------------------------------------------------------------ metrics.rs:506-576
-bool mixing_index(const Fluid& f, const Drum& d, float* out) {
+bool mixing_index(const Fluid& f, const Drum& d, Real* out) {
   const int G = 16;
   size_t n = f.len();
-  if (n == 0 || d.radius_m <= 0.0f) return false;
-  float r = d.radius_m;
-  float cell = 2.0f * r / (float)G;
-  float dye_sum[G * G] = {};
+  if (n == 0 || d.radius_m <= Real(0.0)) return false;
+  Real r = d.radius_m;
+  Real cell = Real(2.0) * r / (Real)G;
+  Real dye_sum[G * G] = {};
   uint32_t count[G * G] = {};
-  float total_dye = 0.0f;
+  Real total_dye = Real(0.0);
   for (size_t i = 0; i < n; ++i) {
     Vec2 p = f.x[i];
     int32_t gi = std::min(std::max(f2i_sat(std::floor((p.x + r) / cell)), 0), G - 1);
@@ -213,38 +213,38 @@ bool mixing_index(const Fluid& f, const Drum& d, float* out) {
     count[idx] += 1;
     total_dye += f.dye[i];
   }
-  float p_mean = total_dye / (float)n;
-  std::vector<float> means;
+  Real p_mean = total_dye / (Real)n;
+  std::vector<Real> means;
   std::vector<uint32_t> counts;
   for (int idx = 0; idx < G * G; ++idx)
-    if (count[idx] > 0) { means.push_back(dye_sum[idx] / (float)count[idx]); counts.push_back(count[idx]); }
+    if (count[idx] > 0) { means.push_back(dye_sum[idx] / (Real)count[idx]); counts.push_back(count[idx]); }
   if (means.size() < 2) return false;
   uint32_t wsum = 0;
   for (uint32_t c : counts) wsum += c;
-  float weight_sum = (float)wsum;
-  float ov = 0.0f;
+  Real weight_sum = (Real)wsum;
+  Real ov = Real(0.0);
   for (size_t q = 0; q < means.size(); ++q) {
-    float dm = means[q] - p_mean;
-    ov += (float)counts[q] * (dm * dm);
+    Real dm = means[q] - p_mean;
+    ov += (Real)counts[q] * (dm * dm);
   }
-  float observed_var = ov / weight_sum;
-  float s0_sq = p_mean * (1.0f - p_mean);
-  float wa = 0.0f;
-  for (uint32_t c : counts) wa += (float)c * (float)c;
-  float weighted_avg = wa / weight_sum;
-  float sr_sq = s0_sq / fmax_r(weighted_avg, 1.0f);
-  if (s0_sq < 1e-9f) return false;
-  float denom = s0_sq - sr_sq;
-  if (std::fabs(denom) < 1e-9f) { *out = 1.0f; return true; }
-  float m = (s0_sq - observed_var) / denom;
-  *out = clamp_r(m, 0.0f, 1.0f);
+  Real observed_var = ov / weight_sum;
+  Real s0_sq = p_mean * (Real(1.0) - p_mean);
+  Real wa = Real(0.0);
+  for (uint32_t c : counts) wa += (Real)c * (Real)c;
+  Real weighted_avg = wa / weight_sum;
+  Real sr_sq = s0_sq / fmax_r(weighted_avg, Real(1.0));
+  if (s0_sq < Real(1e-9)) return false;
+  Real denom = s0_sq - sr_sq;
+  if (std::fabs(denom) < Real(1e-9)) { *out = Real(1.0); return true; }
+  Real m = (s0_sq - observed_var) / denom;
+  *out = clamp_r(m, Real(0.0), Real(1.0));
   return true;
 }
 
 // examples/perf_probe.rs:230-262
 uint64_t state_hash(const Balls& b, const Fluid& f, bool extended) {
   uint64_t h = 0xcbf29ce484222325ull;
-  auto mix = [&](float v) {
+  auto mix = [&](Real v) {
     uint32_t bits;
     std::memcpy(&bits, &v, 4);
     for (int k = 0; k < 4; ++k) {

@@ -7,66 +7,66 @@
 
 namespace orc {
 
-static const float GRAVITY = -9.81f;
+static const Real GRAVITY = -Real(9.81);
 
 // ------------------------------------------------------------------ pbf.rs:45-116 constants
-static const float EPSILON_RELAX = 200.0f;
+static const Real EPSILON_RELAX = Real(200.0);
 static const uint32_t ADAPTIVE_MAX_EXTRA_ITERATIONS = 6;
-static const float COMPRESSION_CONVERGENCE_TOLERANCE = 0.02f;
-static const float OVERLAP_PUSH_MARGIN = 0.05f;
-static const float REFERENCE_SURFACE_TENSION_N_M = 0.072f;
-static const float COHESION_ACCEL_FACTOR = 2.0f;
-static const float ADHESION_ACCEL_FACTOR = 2.0f;
-static const float VISCOSITY_CG_TOLERANCE = 1e-3f;
+static const Real COMPRESSION_CONVERGENCE_TOLERANCE = Real(0.02);
+static const Real OVERLAP_PUSH_MARGIN = Real(0.05);
+static const Real REFERENCE_SURFACE_TENSION_N_M = Real(0.072);
+static const Real COHESION_ACCEL_FACTOR = Real(2.0);
+static const Real ADHESION_ACCEL_FACTOR = Real(2.0);
+static const Real VISCOSITY_CG_TOLERANCE = Real(1e-3);
 static const uint32_t VISCOSITY_CG_MAX_ITERS = 50;
-static const float VISCOSITY_ETA_FACTOR = 0.01f;
-static const float BALL_FORM_DRAG_COEFFICIENT = 1.0f;
-static const float CENTRAL_VISCOSITY_FACTOR = 4.0f;
-static const float BALL_BC_GAIN = 0.5f;
-static const float BINGHAM_PLASTIC_RATIO = 100.0f;
-static const float SQUEEZE_GAIN = 1.0f;
-static const float SQUEEZE_STIFFNESS_CAP = 8.0f;
+static const Real VISCOSITY_ETA_FACTOR = Real(0.01);
+static const Real BALL_FORM_DRAG_COEFFICIENT = Real(1.0);
+static const Real CENTRAL_VISCOSITY_FACTOR = Real(4.0);
+static const Real BALL_BC_GAIN = Real(0.5);
+static const Real BINGHAM_PLASTIC_RATIO = Real(100.0);
+static const Real SQUEEZE_GAIN = Real(1.0);
+static const Real SQUEEZE_STIFFNESS_CAP = Real(8.0);
 static const double MIN_FILM_GAP_RATIO = 0.02;
-static const float F_CLAMP_G_MULTIPLE = 60.0f;
-static const float FLUID_SPEED_SAFETY_FACTOR = 5.0f;
+static const Real F_CLAMP_G_MULTIPLE = Real(60.0);
+static const Real FLUID_SPEED_SAFETY_FACTOR = Real(5.0);
 
 // pbf.rs:119-181 kernels
-static float poly6(float r2, float h) {
-  if (r2 >= h * h || r2 < 0.0f) return 0.0f;
-  float h2 = h * h;
-  float term = h2 - r2;
-  return 4.0f / (PI_F * powi8(h)) * term * term * term;
+static Real poly6(Real r2, Real h) {
+  if (r2 >= h * h || r2 < Real(0.0)) return Real(0.0);
+  Real h2 = h * h;
+  Real term = h2 - r2;
+  return Real(4.0) / (PI_F * powi8(h)) * term * term * term;
 }
-static Vec2 spiky_grad(Vec2 delta, float r, float h) {
-  if (r <= 1e-9f || r >= h) return Vec2();
-  float coeff = -30.0f / (PI_F * powi5(h)) * (h - r) * (h - r);
+static Vec2 spiky_grad(Vec2 delta, Real r, Real h) {
+  if (r <= Real(1e-9) || r >= h) return Vec2();
+  Real coeff = -Real(30.0) / (PI_F * powi5(h)) * (h - r) * (h - r);
   return (delta / r) * coeff;
 }
-static float cohesion_kernel(float r, float h) {
-  if (r <= 0.0f || r >= h) return 0.0f;
-  float coeff = 35840.0f / (209.0f * PI_F * powi8(h));
-  float term = powi3(h - r) * powi3(r);
-  if (r <= 0.5f * h) return coeff * (2.0f * term - powi6(h) / 64.0f);
+static Real cohesion_kernel(Real r, Real h) {
+  if (r <= Real(0.0) || r >= h) return Real(0.0);
+  Real coeff = Real(35840.0) / (Real(209.0) * PI_F * powi8(h));
+  Real term = powi3(h - r) * powi3(r);
+  if (r <= Real(0.5) * h) return coeff * (Real(2.0) * term - powi6(h) / Real(64.0));
   return coeff * term;
 }
-static float adhesion_kernel(float r, float h) {
-  if (r <= 0.5f * h || r >= h) return 0.0f;
-  float coeff = 35840.0f / (163.0f * PI_F * powi8(h));
+static Real adhesion_kernel(Real r, Real h) {
+  if (r <= Real(0.5) * h || r >= h) return Real(0.0);
+  Real coeff = Real(35840.0) / (Real(163.0) * PI_F * powi8(h));
   return coeff * powi3(h - r) * powi3(r);
 }
 
 // pbf.rs:190-219
-static uint32_t boundary_points_per_ball(float ball_radius, float dx) {
-  float circumference = TAU_F * ball_radius;
+static uint32_t boundary_points_per_ball(Real ball_radius, Real dx) {
+  Real circumference = TAU_F * ball_radius;
   return std::max(f2u_sat(std::round(circumference / dx)), 6u);
 }
-static std::vector<Vec2> ball_boundary_particles(const Balls& b, float dx) {
+static std::vector<Vec2> ball_boundary_particles(const Balls& b, Real dx) {
   std::vector<Vec2> out;
-  if (b.len() == 0 || b.radius <= 0.0f || dx <= 0.0f) return out;
+  if (b.len() == 0 || b.radius <= Real(0.0) || dx <= Real(0.0)) return out;
   uint32_t count = boundary_points_per_ball(b.radius, dx);
   std::vector<Vec2> offsets(count);
   for (uint32_t k = 0; k < count; ++k) {
-    float angle = TAU_F * (float)k / (float)count;
+    Real angle = TAU_F * (Real)k / (Real)count;
     offsets[k] = Vec2(cosf_r(angle), sinf_r(angle)) * b.radius;
   }
   out.reserve(b.len() * count);
@@ -76,7 +76,7 @@ static std::vector<Vec2> ball_boundary_particles(const Balls& b, float dx) {
 }
 
 // pbf.rs:262-288
-void neighbor_lists(const std::vector<Vec2>& x, float h, std::vector<uint32_t>* offsets,
+void neighbor_lists(const std::vector<Vec2>& x, Real h, std::vector<uint32_t>* offsets,
                     std::vector<uint32_t>* nbrs) {
   UniformGrid g = UniformGrid::build(x, h);
   size_t n = x.size();
@@ -102,8 +102,8 @@ struct Nbr {
 };
 
 // pbf.rs:292-294 (sequential f32 sum) and its f64 counterpart
-static float dot_f32(const std::vector<Vec2>& a, const std::vector<Vec2>& b) {
-  float s = 0.0f;
+static Real dot_f32(const std::vector<Vec2>& a, const std::vector<Vec2>& b) {
+  Real s = Real(0.0);
   for (size_t i = 0; i < a.size(); ++i) s += a[i].dot(b[i]);
   return s;
 }
@@ -114,24 +114,24 @@ static double dot_f64(const std::vector<Vec2>& a, const std::vector<Vec2>& b) {
 }
 
 // pbf.rs:312-351
-struct ViscWeights { std::vector<float> w; std::vector<Vec2> dir; };
-static ViscWeights morris_weights(const std::vector<Vec2>& x, const Nbr& nb, const std::vector<float>& density,
-                                  float mass, const std::vector<float>& mu, float h) {
-  float eta2 = VISCOSITY_ETA_FACTOR * h * h;
+struct ViscWeights { std::vector<Real> w; std::vector<Vec2> dir; };
+static ViscWeights morris_weights(const std::vector<Vec2>& x, const Nbr& nb, const std::vector<Real>& density,
+                                  Real mass, const std::vector<Real>& mu, Real h) {
+  Real eta2 = VISCOSITY_ETA_FACTOR * h * h;
   ViscWeights vw;
-  vw.w.assign(nb.idx.size(), 0.0f);
+  vw.w.assign(nb.idx.size(), Real(0.0));
   vw.dir.assign(nb.idx.size(), Vec2());
   for (size_t i = 0; i < x.size(); ++i) {
-    float rho_i = fmax_r(density[i], 1e-6f);
+    Real rho_i = fmax_r(density[i], Real(1e-6));
     for (size_t k = nb.b(i); k < nb.e(i); ++k) {
       size_t ju = nb.idx[k];
-      float rho_j = fmax_r(density[ju], 1e-6f);
+      Real rho_j = fmax_r(density[ju], Real(1e-6));
       Vec2 delta = x[i] - x[ju];
-      float r = delta.length();
+      Real r = delta.length();
       Vec2 grad = spiky_grad(delta, r, h);
-      float numerator = (mass * (mu[i] + mu[ju]) / (rho_i * rho_j)) * std::fabs(delta.dot(grad));
+      Real numerator = (mass * (mu[i] + mu[ju]) / (rho_i * rho_j)) * std::fabs(delta.dot(grad));
       vw.w[k] = numerator / (delta.length_squared() + eta2);
-      vw.dir[k] = r > 1e-9f ? delta / r : Vec2(1.0f, 0.0f);
+      vw.dir[k] = r > Real(1e-9) ? delta / r : Vec2(Real(1.0), Real(0.0));
     }
   }
   return vw;
@@ -149,16 +149,16 @@ static void laplacian_apply_into(const Nbr& nb, const ViscWeights& w, const Vec2
     out[i] = sum;
   }
 }
-static float viscosity_diag(float sum_w) { return 0.5f * CENTRAL_VISCOSITY_FACTOR * sum_w; }
+static Real viscosity_diag(Real sum_w) { return Real(0.5) * CENTRAL_VISCOSITY_FACTOR * sum_w; }
 
 // pbf.rs:423-480 (fluid-only CG); `fp64` selects f64 inner products and norms.
-static uint32_t solve_implicit_viscosity(const Nbr& nb, const ViscWeights& w, std::vector<Vec2>* vp, float dt,
+static uint32_t solve_implicit_viscosity(const Nbr& nb, const ViscWeights& w, std::vector<Vec2>* vp, Real dt,
                                          bool fp64) {
   std::vector<Vec2>& v = *vp;
   size_t n = v.size();
   double b_norm = fp64 ? std::sqrt(dot_f64(v, v)) : (double)std::sqrt(dot_f32(v, v));
   if (b_norm <= 0.0 || !std::isfinite(b_norm)) return 0;
-  float target_f = VISCOSITY_CG_TOLERANCE * (float)b_norm;
+  Real target_f = VISCOSITY_CG_TOLERANCE * (Real)b_norm;
   double target_d = (double)VISCOSITY_CG_TOLERANCE * b_norm;
   std::vector<Vec2> lv(n), ax(n), r(n), p, ap(n);
   auto apply = [&](const std::vector<Vec2>& in, std::vector<Vec2>& out) {
@@ -169,17 +169,17 @@ static uint32_t solve_implicit_viscosity(const Nbr& nb, const ViscWeights& w, st
   for (size_t i = 0; i < n; ++i) r[i] = v[i] - ax[i];
   p = r;
   if (!fp64) {
-    float rs_old = dot_f32(r, r);
+    Real rs_old = dot_f32(r, r);
     if (std::sqrt(rs_old) <= target_f) return 0;
     for (uint32_t iter = 1; iter <= VISCOSITY_CG_MAX_ITERS; ++iter) {
       apply(p, ap);
-      float p_ap = dot_f32(p, ap);
-      if (p_ap <= 0.0f || !std::isfinite(p_ap)) return iter;
-      float alpha = rs_old / p_ap;
+      Real p_ap = dot_f32(p, ap);
+      if (p_ap <= Real(0.0) || !std::isfinite(p_ap)) return iter;
+      Real alpha = rs_old / p_ap;
       for (size_t i = 0; i < n; ++i) { v[i] += alpha * p[i]; r[i] -= alpha * ap[i]; }
-      float rs_new = dot_f32(r, r);
+      Real rs_new = dot_f32(r, r);
       if (std::sqrt(rs_new) <= target_f) return iter;
-      float beta = rs_new / rs_old;
+      Real beta = rs_new / rs_old;
       for (size_t i = 0; i < n; ++i) p[i] = r[i] + beta * p[i];
       rs_old = rs_new;
     }
@@ -190,11 +190,11 @@ static uint32_t solve_implicit_viscosity(const Nbr& nb, const ViscWeights& w, st
       apply(p, ap);
       double p_ap = dot_f64(p, ap);
       if (p_ap <= 0.0 || !std::isfinite(p_ap)) return iter;
-      float alpha = (float)(rs_old / p_ap);
+      Real alpha = (Real)(rs_old / p_ap);
       for (size_t i = 0; i < n; ++i) { v[i] += alpha * p[i]; r[i] -= alpha * ap[i]; }
       double rs_new = dot_f64(r, r);
       if (std::sqrt(rs_new) <= target_d) return iter;
-      float beta = (float)(rs_new / rs_old);
+      Real beta = (Real)(rs_new / rs_old);
       for (size_t i = 0; i < n; ++i) p[i] = r[i] + beta * p[i];
       rs_old = rs_new;
     }
@@ -202,8 +202,8 @@ static uint32_t solve_implicit_viscosity(const Nbr& nb, const ViscWeights& w, st
   return VISCOSITY_CG_MAX_ITERS;
 }
 
-struct BoundaryGroup { uint32_t fluid, ball; float c; Vec2 lever_c; float lever2_c; };
-struct SqueezeLink { uint32_t ball, other; Vec2 n; float c; };
+struct BoundaryGroup { uint32_t fluid, ball; Real c; Vec2 lever_c; Real lever2_c; };
+struct SqueezeLink { uint32_t ball, other; Vec2 n; Real c; };
 
 // mac/lubrication.rs:19-115 (the subset pbf.rs:544-625 uses)
 static const double H_START = 8.0;
@@ -236,19 +236,19 @@ static double resolved_ratio(double h_cells) {
 }
 
 // pbf.rs:544-625
-static std::vector<SqueezeLink> squeeze_links(const Balls& balls, float drum_radius, float dx, float mu, float dt,
+static std::vector<SqueezeLink> squeeze_links(const Balls& balls, Real drum_radius, Real dx, Real mu, Real dt,
                                               const std::vector<Vec2>* closing, size_t* in_range_out) {
   std::vector<SqueezeLink> out;
   size_t in_range = 0;
-  float r = balls.radius;
+  Real r = balls.radius;
   *in_range_out = 0;
-  if (balls.len() == 0 || r <= 0.0f || mu <= 0.0f) return out;
+  if (balls.len() == 0 || r <= Real(0.0) || mu <= Real(0.0)) return out;
   double a = (double)r, b = (double)drum_radius, dxd = (double)dx, mud = (double)mu;
-  float gain = SQUEEZE_GAIN;
-  float reach = (float)(H_START * dxd);
-  float c_max = SQUEEZE_STIFFNESS_CAP * balls.mass / fmax_r(dt, 1e-12f);
-  UniformGrid grid = UniformGrid::build(balls.x, 2.0f * r + reach);
-  float range2 = (2.0f * r + reach) * (2.0f * r + reach) * (1.0f + 1e-4f);
+  Real gain = SQUEEZE_GAIN;
+  Real reach = (Real)(H_START * dxd);
+  Real c_max = SQUEEZE_STIFFNESS_CAP * balls.mass / fmax_r(dt, Real(1e-12));
+  UniformGrid grid = UniformGrid::build(balls.x, Real(2.0) * r + reach);
+  Real range2 = (Real(2.0) * r + reach) * (Real(2.0) * r + reach) * (Real(1.0) + Real(1e-4));
   SqueezeFilm pair_film(1.0 / a, 1.0 / a, mud);
   SqueezeFilm wall_film(1.0 / a, -1.0 / b, mud);
   for (size_t i = 0; i < balls.len(); ++i) {
@@ -258,27 +258,27 @@ static std::vector<SqueezeLink> squeeze_links(const Balls& balls, float drum_rad
       if ((size_t)j <= i) return;
       Vec2 e = balls.x[j] - xi;
       if (e.length_squared() >= range2 || !e.is_finite()) return;
-      float dist = e.length();
-      float gap = dist - 2.0f * r;
-      if (gap >= reach || dist < 1e-9f) return;
+      Real dist = e.length();
+      Real gap = dist - Real(2.0) * r;
+      if (gap >= reach || dist < Real(1e-9)) return;
       in_range += 1;
       Vec2 n = e / dist;
-      if (closing && n.dot((*closing)[i] - (*closing)[j]) <= 0.0f) return;
+      if (closing && n.dot((*closing)[i] - (*closing)[j]) <= Real(0.0)) return;
       double weight = 1.0 - resolved_ratio((double)gap / dxd);
       double hh = dmax_r((double)gap, MIN_FILM_GAP_RATIO * a);
       double c = weight * pair_film.coefficient(hh);
-      out.push_back({(uint32_t)i, j, n, fmin_r(gain * (float)c, c_max)});
+      out.push_back({(uint32_t)i, j, n, fmin_r(gain * (Real)c, c_max)});
     });
-    float dist = xi.length();
-    float gap = drum_radius - r - dist;
-    if (gap < reach && dist > 1e-9f) {
+    Real dist = xi.length();
+    Real gap = drum_radius - r - dist;
+    if (gap < reach && dist > Real(1e-9)) {
       in_range += 1;
       Vec2 n = xi / dist;
-      if (closing && n.dot((*closing)[i]) <= 0.0f) continue;
+      if (closing && n.dot((*closing)[i]) <= Real(0.0)) continue;
       double weight = 1.0 - resolved_ratio((double)gap / dxd);
       double hh = dmax_r((double)gap, MIN_FILM_GAP_RATIO * a);
       double c = weight * wall_film.coefficient(hh);
-      out.push_back({(uint32_t)i, WALL_ID, n, fmin_r(gain * (float)c, c_max)});
+      out.push_back({(uint32_t)i, WALL_ID, n, fmin_r(gain * (Real)c, c_max)});
     }
   }
   *in_range_out = in_range;
@@ -288,13 +288,13 @@ static std::vector<SqueezeLink> squeeze_links(const Balls& balls, float drum_rad
 // pbf.rs:641-791 (joint fluid + ball Jacobi-PCG); `fp64` selects f64 inner products and norms.
 static uint32_t solve_viscosity_with_balls(const Nbr& nb, const ViscWeights& weights,
                                            const std::vector<BoundaryGroup>& groups,
-                                           const std::vector<SqueezeLink>& links, float mass, float ball_mass_,
-                                           float ball_inertia_, float dt, const std::vector<Vec2>& guess,
+                                           const std::vector<SqueezeLink>& links, Real mass, Real ball_mass_,
+                                           Real ball_inertia_, Real dt, const std::vector<Vec2>& guess,
                                            std::vector<Vec2>* vp, std::vector<Vec2>* ball_vp,
-                                           std::vector<float>* ball_wp, bool fp64) {
+                                           std::vector<Real>* ball_wp, bool fp64) {
   std::vector<Vec2>& v = *vp;
   std::vector<Vec2>& ball_v = *ball_vp;
-  std::vector<float>& ball_w = *ball_wp;
+  std::vector<Real>& ball_w = *ball_wp;
   size_t n = v.size(), nbn = ball_v.size(), len = n + 2 * nbn;
   auto perp = [](Vec2 l) { return Vec2(-l.y, l.x); };
   std::vector<Vec2> x;
@@ -305,46 +305,46 @@ static uint32_t solve_viscosity_with_balls(const Nbr& nb, const ViscWeights& wei
     for (size_t i = 0; i < n; ++i) x.push_back(v[i]);
   }
   for (size_t i = 0; i < nbn; ++i) x.push_back(ball_v[i]);
-  for (size_t i = 0; i < nbn; ++i) x.push_back(Vec2(ball_w[i], 0.0f));
+  for (size_t i = 0; i < nbn; ++i) x.push_back(Vec2(ball_w[i], Real(0.0)));
   std::vector<Vec2> b;
   b.reserve(len);
   for (size_t i = 0; i < n; ++i) b.push_back(mass * v[i]);
   for (size_t i = 0; i < nbn; ++i) b.push_back(ball_mass_ * ball_v[i]);
-  for (size_t i = 0; i < nbn; ++i) b.push_back(Vec2(ball_inertia_ * ball_w[i], 0.0f));
-  std::vector<float> diag(len, 0.0f);
+  for (size_t i = 0; i < nbn; ++i) b.push_back(Vec2(ball_inertia_ * ball_w[i], Real(0.0)));
+  std::vector<Real> diag(len, Real(0.0));
   for (size_t i = 0; i < n; ++i) {
-    float sw = 0.0f;
+    Real sw = Real(0.0);
     for (size_t k = nb.b(i); k < nb.e(i); ++k) sw += weights.w[k];
-    diag[i] = mass * (1.0f + dt * viscosity_diag(sw));
+    diag[i] = mass * (Real(1.0) + dt * viscosity_diag(sw));
   }
   for (size_t bi = 0; bi < nbn; ++bi) { diag[n + bi] = ball_mass_; diag[n + nbn + bi] = ball_inertia_; }
   for (const auto& g : groups) {
-    float d = dt * mass * g.c;
+    Real d = dt * mass * g.c;
     diag[g.fluid] += d;
     diag[n + g.ball] += d;
     diag[n + nbn + g.ball] += dt * mass * g.lever2_c;
   }
   for (const auto& l : links) {
-    float d = dt * l.c;
+    Real d = dt * l.c;
     diag[n + l.ball] += d;
     if (l.other != WALL_ID) diag[n + l.other] += d;
   }
-  std::vector<float> inv_diag(len);
-  for (size_t i = 0; i < len; ++i) inv_diag[i] = 1.0f / fmax_r(diag[i], 1e-20f);
+  std::vector<Real> inv_diag(len);
+  for (size_t i = 0; i < len; ++i) inv_diag[i] = Real(1.0) / fmax_r(diag[i], Real(1e-20));
   std::vector<Vec2> lv(n);
   auto apply = [&](const std::vector<Vec2>& xx, std::vector<Vec2>& out) {
     laplacian_apply_into(nb, weights, xx.data(), n, lv.data());
     for (size_t i = 0; i < n; ++i) out[i] = mass * (xx[i] + dt * lv[i]);
     for (size_t bi = 0; bi < nbn; ++bi) {
       out[n + bi] = ball_mass_ * xx[n + bi];
-      out[n + nbn + bi] = Vec2(ball_inertia_ * xx[n + nbn + bi].x, 0.0f);
+      out[n + nbn + bi] = Vec2(ball_inertia_ * xx[n + nbn + bi].x, Real(0.0));
     }
     for (const auto& g : groups) {
       size_t i = g.fluid, bi = g.ball;
       Vec2 vb = xx[n + bi];
-      float w = xx[n + nbn + bi].x;
+      Real w = xx[n + nbn + bi].x;
       Vec2 rel = xx[i] - vb;
-      float k = dt * mass;
+      Real k = dt * mass;
       Vec2 d = k * (g.c * rel - w * perp(g.lever_c));
       out[i] += d;
       out[n + bi] -= d;
@@ -360,7 +360,7 @@ static uint32_t solve_viscosity_with_balls(const Nbr& nb, const ViscWeights& wei
     }
   };
   auto res_norm_f = [&](const std::vector<Vec2>& r) {
-    float s = 0.0f;
+    Real s = Real(0.0);
     for (size_t i = 0; i < r.size(); ++i) s += inv_diag[i] * r[i].length_squared();
     return std::sqrt(s);
   };
@@ -377,22 +377,22 @@ static uint32_t solve_viscosity_with_balls(const Nbr& nb, const ViscWeights& wei
   for (size_t i = 0; i < len; ++i) z[i] = r[i] * inv_diag[i];
   uint32_t iters = 0;
   if (!fp64) {
-    float b_norm = res_norm_f(b);
-    if (b_norm > 0.0f && std::isfinite(b_norm) && res_norm_f(r) > VISCOSITY_CG_TOLERANCE * b_norm) {
-      float target = VISCOSITY_CG_TOLERANCE * b_norm;
+    Real b_norm = res_norm_f(b);
+    if (b_norm > Real(0.0) && std::isfinite(b_norm) && res_norm_f(r) > VISCOSITY_CG_TOLERANCE * b_norm) {
+      Real target = VISCOSITY_CG_TOLERANCE * b_norm;
       std::vector<Vec2> p = z, ap(len);
-      float rz_old = dot_f32(r, z);
+      Real rz_old = dot_f32(r, z);
       for (uint32_t iter = 1; iter <= 4 * VISCOSITY_CG_MAX_ITERS; ++iter) {
         iters = iter;
         apply(p, ap);
-        float p_ap = dot_f32(p, ap);
-        if (p_ap <= 0.0f || !std::isfinite(p_ap)) break;
-        float alpha = rz_old / p_ap;
+        Real p_ap = dot_f32(p, ap);
+        if (p_ap <= Real(0.0) || !std::isfinite(p_ap)) break;
+        Real alpha = rz_old / p_ap;
         for (size_t i = 0; i < len; ++i) { x[i] += alpha * p[i]; r[i] -= alpha * ap[i]; }
         if (res_norm_f(r) <= target) break;
         for (size_t i = 0; i < len; ++i) z[i] = r[i] * inv_diag[i];
-        float rz_new = dot_f32(r, z);
-        float beta = rz_new / rz_old;
+        Real rz_new = dot_f32(r, z);
+        Real beta = rz_new / rz_old;
         for (size_t i = 0; i < len; ++i) p[i] = z[i] + beta * p[i];
         rz_old = rz_new;
       }
@@ -408,12 +408,12 @@ static uint32_t solve_viscosity_with_balls(const Nbr& nb, const ViscWeights& wei
         apply(p, ap);
         double p_ap = dot_f64(p, ap);
         if (p_ap <= 0.0 || !std::isfinite(p_ap)) break;
-        float alpha = (float)(rz_old / p_ap);
+        Real alpha = (Real)(rz_old / p_ap);
         for (size_t i = 0; i < len; ++i) { x[i] += alpha * p[i]; r[i] -= alpha * ap[i]; }
         if (res_norm_d(r) <= target) break;
         for (size_t i = 0; i < len; ++i) z[i] = r[i] * inv_diag[i];
         double rz_new = dot_f64(r, z);
-        float beta = (float)(rz_new / rz_old);
+        Real beta = (Real)(rz_new / rz_old);
         for (size_t i = 0; i < len; ++i) p[i] = z[i] + beta * p[i];
         rz_old = rz_new;
       }
@@ -426,78 +426,78 @@ static uint32_t solve_viscosity_with_balls(const Nbr& nb, const ViscWeights& wei
 }
 
 // pbf.rs:800-868
-static std::vector<float> shear_rates(const std::vector<Vec2>& x, const std::vector<Vec2>& v, const Nbr& nb,
-                                      const std::vector<float>& density, float mass, float h) {
+static std::vector<Real> shear_rates(const std::vector<Vec2>& x, const std::vector<Vec2>& v, const Nbr& nb,
+                                      const std::vector<Real>& density, Real mass, Real h) {
   size_t n = x.size();
-  std::vector<float> out(n, 0.0f);
+  std::vector<Real> out(n, Real(0.0));
   for (size_t i = 0; i < n; ++i) {
-    float gxx = 0.0f, gxy = 0.0f, gyx = 0.0f, gyy = 0.0f;
+    Real gxx = Real(0.0), gxy = Real(0.0), gyx = Real(0.0), gyy = Real(0.0);
     for (size_t k = nb.b(i); k < nb.e(i); ++k) {
       size_t ju = nb.idx[k];
       Vec2 delta = x[i] - x[ju];
-      float r = delta.length();
+      Real r = delta.length();
       Vec2 grad = spiky_grad(delta, r, h);
-      float coeff = mass / fmax_r(density[ju], 1e-6f);
+      Real coeff = mass / fmax_r(density[ju], Real(1e-6));
       Vec2 dv = v[ju] - v[i];
       gxx += coeff * dv.x * grad.x;
       gxy += coeff * dv.x * grad.y;
       gyx += coeff * dv.y * grad.x;
       gyy += coeff * dv.y * grad.y;
     }
-    float dxy = 0.5f * (gxy + gyx);
-    out[i] = std::sqrt(2.0f * (gxx * gxx + gyy * gyy + 2.0f * dxy * dxy));
+    Real dxy = Real(0.5) * (gxy + gyx);
+    out[i] = std::sqrt(Real(2.0) * (gxx * gxx + gyy * gyy + Real(2.0) * dxy * dxy));
   }
   return out;
 }
-static float mean_shear_rate(const std::vector<Vec2>& x, const std::vector<Vec2>& v, const Nbr& nb,
-                             const std::vector<float>& density, float mass, float h) {
-  std::vector<float> rates = shear_rates(x, v, nb, density, mass, h);
-  float sum = 0.0f;
+static Real mean_shear_rate(const std::vector<Vec2>& x, const std::vector<Vec2>& v, const Nbr& nb,
+                             const std::vector<Real>& density, Real mass, Real h) {
+  std::vector<Real> rates = shear_rates(x, v, nb, density, mass, h);
+  Real sum = Real(0.0);
   uint32_t count = 0;
-  for (float g : rates)
+  for (Real g : rates)
     if (std::isfinite(g)) { sum += g; count += 1; }
-  return count == 0 ? 0.0f : sum / (float)count;
+  return count == 0 ? Real(0.0) : sum / (Real)count;
 }
-static std::vector<float> bingham_viscosity(const std::vector<float>& rates, float mu, float tau_y) {
-  float gamma0 = tau_y / (BINGHAM_PLASTIC_RATIO * mu);
-  std::vector<float> out(rates.size());
+static std::vector<Real> bingham_viscosity(const std::vector<Real>& rates, Real mu, Real tau_y) {
+  Real gamma0 = tau_y / (BINGHAM_PLASTIC_RATIO * mu);
+  std::vector<Real> out(rates.size());
   for (size_t i = 0; i < rates.size(); ++i) {
-    float g = std::isfinite(rates[i]) ? rates[i] : 0.0f;
-    float extra = g < 1e-4f * gamma0 ? tau_y / gamma0 : tau_y * (1.0f - expf_r(-g / gamma0)) / g;
+    Real g = std::isfinite(rates[i]) ? rates[i] : Real(0.0);
+    Real extra = g < Real(1e-4) * gamma0 ? tau_y / gamma0 : tau_y * (Real(1.0) - expf_r(-g / gamma0)) / g;
     out[i] = mu + extra;
   }
   return out;
 }
 
 // pbf.rs:924-926, 957-996
-static double kinetic_energy_f64(const std::vector<Vec2>& v, float mass) {
+static double kinetic_energy_f64(const std::vector<Vec2>& v, Real mass) {
   double s = 0.0;
   for (const Vec2& q : v) s += (double)q.length_squared();
   return 0.5 * (double)mass * s;
 }
-static float impulse_clamp(float ball_mass_, float dt) { return F_CLAMP_G_MULTIPLE * ball_mass_ * 9.81f * dt; }
-static float fluid_speed_clamp_v_max(const Drum& d) {
-  return FLUID_SPEED_SAFETY_FACTOR * (std::fabs(d.omega) * d.radius_m + std::sqrt(4.0f * std::fabs(GRAVITY) * d.radius_m));
+static Real impulse_clamp(Real ball_mass_, Real dt) { return F_CLAMP_G_MULTIPLE * ball_mass_ * Real(9.81) * dt; }
+static Real fluid_speed_clamp_v_max(const Drum& d) {
+  return FLUID_SPEED_SAFETY_FACTOR * (std::fabs(d.omega) * d.radius_m + std::sqrt(Real(4.0) * std::fabs(GRAVITY) * d.radius_m));
 }
-static void clamp_fluid_speed(std::vector<Vec2>* v, float v_max) {
+static void clamp_fluid_speed(std::vector<Vec2>* v, Real v_max) {
   for (Vec2& q : *v) {
-    float speed = q.length();
+    Real speed = q.length();
     if (!std::isfinite(speed)) q = Vec2();
     else if (speed > v_max) q *= v_max / speed;
   }
 }
 
 // pbf.rs:1124-1150
-std::vector<float> fluid_densities(const Fluid& f) {
+std::vector<Real> fluid_densities(const Fluid& f) {
   size_t n = f.len();
-  std::vector<float> density(n, 0.0f);
+  std::vector<Real> density(n, Real(0.0));
   if (n == 0) return density;
   UniformGrid g = UniformGrid::build(f.x, f.h);
-  float self_c = f.particle_mass * poly6(0.0f, f.h);
+  Real self_c = f.particle_mass * poly6(Real(0.0), f.h);
   std::fill(density.begin(), density.end(), self_c);
   g.for_each_candidate_pair([&](uint32_t i, uint32_t j) {
-    float r2 = (f.x[i] - f.x[j]).length_squared();
-    float w = poly6(r2, f.h);
+    Real r2 = (f.x[i] - f.x[j]).length_squared();
+    Real w = poly6(r2, f.h);
     density[i] += f.particle_mass * w;
     density[j] += f.particle_mass * w;
   });
@@ -511,24 +511,24 @@ double fluid_mechanical_energy(const Fluid& f) {
 }
 
 // pbf.rs:1174-2365
-void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const SlurryParams& slurry,
-                        uint32_t iterations, float dt, const Balls& balls, CouplingImpulses* coupling,
+void fluid_step_coupled(Fluid* fl, const Drum& drum, Real drum_angle, const SlurryParams& slurry,
+                        uint32_t iterations, Real dt, const Balls& balls, CouplingImpulses* coupling,
                         FluidStepStats* stats_out, StepCounters* ctr, Debug* dbg, const SolveOptions& opt) {
   size_t n = fl->len();
   coupling->zeros(balls.len());
   *stats_out = FluidStepStats();
-  if (n == 0 || dt <= 0.0f) return;
+  if (n == 0 || dt <= Real(0.0)) return;
   std::vector<Vec2>& X = fl->x;
   std::vector<Vec2>& V = fl->v;
   // step 0: sanitize
   for (size_t i = 0; i < n; ++i)
     if (!X[i].is_finite() || !V[i].is_finite()) { X[i] = Vec2(); V[i] = Vec2(); }
-  float h = fl->h, rest_density = fl->rest_density, mass = fl->particle_mass;
+  Real h = fl->h, rest_density = fl->rest_density, mass = fl->particle_mass;
   bool have_ball_grid = balls.len() > 0;
   UniformGrid ball_grid;
   if (have_ball_grid) {
-    float contact_radius = balls.radius + OVERLAP_PUSH_MARGIN * h;
-    ball_grid = UniformGrid::build(balls.x, fmax_r(fmax_r(2.0f * balls.radius, contact_radius), 1e-6f));
+    Real contact_radius = balls.radius + OVERLAP_PUSH_MARGIN * h;
+    ball_grid = UniformGrid::build(balls.x, fmax_r(fmax_r(Real(2.0) * balls.radius, contact_radius), Real(1e-6)));
   }
   // step 1: predict
   std::vector<Vec2> x0 = X;
@@ -536,7 +536,7 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
     V[i].y += GRAVITY * dt;
     X[i] += V[i] * dt;
   }
-  float drum_angle_next = drum_angle + drum.omega * dt;
+  Real drum_angle_next = drum_angle + drum.omega * dt;
   // step 2: grid + neighbour lists
   UniformGrid grid = UniformGrid::build(X, h);
   Nbr nb;
@@ -555,22 +555,22 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
   if (ctr) ctr->n_fluid_edges = (uint32_t)nb.idx.size();
   if (dbg) { dbg->nbr_offsets = nb.off; dbg->nbrs = nb.idx; }
   // step 3: density constraint iterations
-  std::vector<float> density(n, 0.0f), lambda(n, 0.0f);
+  std::vector<Real> density(n, Real(0.0)), lambda(n, Real(0.0));
   std::vector<Vec2> delta_p(n), grad_cache(nb.idx.size());
   uint32_t base_iterations = std::max(iterations, 1u);
   uint32_t iter_count = 0;
   for (;;) {
-    float max_c = 0.0f;
+    Real max_c = Real(0.0);
     for (size_t i = 0; i < n; ++i) {
-      float rho = mass * poly6(0.0f, h);
+      Real rho = mass * poly6(Real(0.0), h);
       Vec2 grad_self;
-      float sum_grad_sq = 0.0f;
+      Real sum_grad_sq = Real(0.0);
       for (size_t k = nb.b(i); k < nb.e(i); ++k) {
         size_t ju = nb.idx[k];
         Vec2 delta = X[i] - X[ju];
-        float r2 = delta.length_squared();
+        Real r2 = delta.length_squared();
         rho += mass * poly6(r2, h);
-        float r = delta.length();
+        Real r = delta.length();
         Vec2 raw_grad = spiky_grad(delta, r, h);
         grad_cache[k] = raw_grad;
         Vec2 grad = raw_grad * (mass / rest_density);
@@ -578,7 +578,7 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
         sum_grad_sq += grad.length_squared();
       }
       density[i] = rho;
-      float c_i = fmax_r(density[i] / rest_density - 1.0f, 0.0f);
+      Real c_i = fmax_r(density[i] / rest_density - Real(1.0), Real(0.0));
       max_c = fmax_r(max_c, c_i);
       sum_grad_sq += grad_self.length_squared();
       lambda[i] = -c_i / (sum_grad_sq + EPSILON_RELAX);
@@ -601,7 +601,7 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
   // step 3.5: ball overlap push
   std::vector<Vec2> push_velocity_excess(n);
   if (have_ball_grid) {
-    float contact_radius = balls.radius + OVERLAP_PUSH_MARGIN * h;
+    Real contact_radius = balls.radius + OVERLAP_PUSH_MARGIN * h;
     std::vector<uint32_t> nearby;
     for (size_t i = 0; i < n; ++i) {
       nearby.clear();
@@ -609,18 +609,18 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
       for (uint32_t bb : nearby) {
         size_t b = bb;
         Vec2 delta = X[i] - balls.x[b];
-        float dist = delta.length();
+        Real dist = delta.length();
         if (std::isnan(dist) || dist >= contact_radius) continue;
-        Vec2 n_hat = dist > 1e-9f ? delta / dist : Vec2(1.0f, 0.0f);
-        float push_mag = fmin_r(contact_radius - dist, 0.5f * balls.radius);
+        Vec2 n_hat = dist > Real(1e-9) ? delta / dist : Vec2(Real(1.0), Real(0.0));
+        Real push_mag = fmin_r(contact_radius - dist, Real(0.5) * balls.radius);
         Vec2 push = push_mag * n_hat;
         X[i] += push;
         Vec2 lever = n_hat * balls.radius;
         Vec2 v_surface = balls.v[b] + balls.omega[b] * Vec2(-lever.y, lever.x);
-        float arrest_speed = fmax_r(-(V[i] - v_surface).dot(n_hat), 0.0f);
-        float full_impulse_mag = mass * push_mag / dt;
-        float reduced_mass = balls.mass > 0.0f ? (mass * balls.mass) / (mass + balls.mass) : mass;
-        float impulse_mag = fmin_r(full_impulse_mag, reduced_mass * arrest_speed);
+        Real arrest_speed = fmax_r(-(V[i] - v_surface).dot(n_hat), Real(0.0));
+        Real full_impulse_mag = mass * push_mag / dt;
+        Real reduced_mass = balls.mass > Real(0.0) ? (mass * balls.mass) / (mass + balls.mass) : mass;
+        Real impulse_mag = fmin_r(full_impulse_mag, reduced_mass * arrest_speed);
         push_velocity_excess[i] += ((full_impulse_mag - impulse_mag) / mass) * n_hat;
         Vec2 reaction = -impulse_mag * n_hat;
         coupling->impulses[b] += reaction;
@@ -631,17 +631,17 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
   }
   // step 3.6a: cohesion
   std::vector<Vec2> cohesion_dv(n);
-  float cohesion_accel = (fmax_r(slurry.surface_tension_n_m, 0.0f) / REFERENCE_SURFACE_TENSION_N_M) *
+  Real cohesion_accel = (fmax_r((Real)slurry.surface_tension_n_m, Real(0.0)) / REFERENCE_SURFACE_TENSION_N_M) *
                          COHESION_ACCEL_FACTOR * std::fabs(GRAVITY);
-  if (cohesion_accel > 0.0f) {
+  if (cohesion_accel > Real(0.0)) {
     for (size_t i = 0; i < n; ++i) {
       Vec2 pull;
       for (size_t k = nb.b(i); k < nb.e(i); ++k) {
         size_t ju = nb.idx[k];
         Vec2 delta = X[i] - X[ju];
-        float r = delta.length();
-        if (r <= 1e-9f) continue;
-        float w = mass * cohesion_kernel(r, h) / rest_density;
+        Real r = delta.length();
+        if (r <= Real(1e-9)) continue;
+        Real w = mass * cohesion_kernel(r, h) / rest_density;
         pull -= w * (delta / r);
       }
       cohesion_dv[i] = cohesion_accel * pull * dt;
@@ -649,20 +649,20 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
   }
   // step 3.6b: adhesion (queries the stale step-2 grid)
   std::vector<Vec2> adhesion_dv(n);
-  float wettability = clamp_r(slurry.wettability, 0.0f, 1.0f);
-  if (wettability > 0.0f && balls.len() > 0 && balls.radius > 0.0f) {
-    float dx = 0.5f * h;
-    float h_adh = fmin_r(h, 2.0f * balls.radius);
+  Real wettability = clamp_r((Real)slurry.wettability, Real(0.0), Real(1.0));
+  if (wettability > Real(0.0) && balls.len() > 0 && balls.radius > Real(0.0)) {
+    Real dx = Real(0.5) * h;
+    Real h_adh = fmin_r(h, Real(2.0) * balls.radius);
     std::vector<Vec2> bpos = ball_boundary_particles(balls, dx);
     size_t count_per_ball = boundary_points_per_ball(balls.radius, dx);
-    if (!bpos.empty() && h_adh > 0.0f) {
-      float adhesion_accel = wettability * ADHESION_ACCEL_FACTOR * std::fabs(GRAVITY);
-      struct Item { size_t j; Vec2 dir; float w; };
+    if (!bpos.empty() && h_adh > Real(0.0)) {
+      Real adhesion_accel = wettability * ADHESION_ACCEL_FACTOR * std::fabs(GRAVITY);
+      struct Item { size_t j; Vec2 dir; Real w; };
       std::vector<Item> items;
       std::vector<uint32_t> slot(n, UINT32_MAX);
       std::vector<uint32_t> nearby;
-      float range2 = h_adh * h_adh * (1.0f + 1e-4f);
-      float inner2 = 0.25f * h_adh * h_adh * (1.0f - 1e-4f);
+      Real range2 = h_adh * h_adh * (Real(1.0) + Real(1e-4));
+      Real inner2 = Real(0.25) * h_adh * h_adh * (Real(1.0) - Real(1e-4));
       for (size_t b = 0; b < balls.len(); ++b) {
         if (!balls.x[b].is_finite()) continue;
         size_t start = b * count_per_ball;
@@ -675,12 +675,12 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
           for (uint32_t jj : nearby) {
             size_t ju = jj;
             Vec2 delta = bp - X[ju];
-            float r2 = delta.length_squared();
+            Real r2 = delta.length_squared();
             if (r2 >= range2 || r2 <= inner2) continue;
-            float r = std::sqrt(r2);
-            if (!std::isfinite(r) || r <= 0.5f * h_adh || r >= h_adh) continue;
-            float w = mass * adhesion_kernel(r, h_adh) / rest_density;
-            if (w <= 0.0f) continue;
+            Real r = std::sqrt(r2);
+            if (!std::isfinite(r) || r <= Real(0.5) * h_adh || r >= h_adh) continue;
+            Real w = mass * adhesion_kernel(r, h_adh) / rest_density;
+            if (w <= Real(0.0)) continue;
             Vec2 n_hat = delta / r;
             if (slot[ju] == UINT32_MAX) {
               slot[ju] = (uint32_t)items.size();
@@ -694,22 +694,22 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
         }
         for (auto& it : items) slot[it.j] = UINT32_MAX;
         if (items.empty()) continue;
-        float weight_sum = 0.0f;
+        Real weight_sum = Real(0.0);
         Vec2 dir_sum;
         for (auto& it : items) { dir_sum += it.dir; weight_sum += it.w; }
-        if (weight_sum <= 1e-9f) continue;
-        float pull_len = dir_sum.length();
-        if (pull_len <= 1e-9f) continue;
+        if (weight_sum <= Real(1e-9)) continue;
+        Real pull_len = dir_sum.length();
+        if (pull_len <= Real(1e-9)) continue;
         Vec2 ball_pull_dir = -dir_sum / pull_len;
-        float coverage = fmin_r(weight_sum, 1.0f);
-        float m_contrib = mass * weight_sum;
-        float attach = m_contrib / (balls.mass + m_contrib);
+        Real coverage = fmin_r(weight_sum, Real(1.0));
+        Real m_contrib = mass * weight_sum;
+        Real attach = m_contrib / (balls.mass + m_contrib);
         Vec2 dv_b = ball_pull_dir * (adhesion_accel * coverage * dt * attach);
         coupling->impulses[b] += balls.mass * dv_b;
         Vec2 lever = ball_pull_dir * balls.radius;
         coupling->angular_impulses[b] += balls.mass * cross2(lever, dv_b);
         for (auto& it : items) {
-          float frac = it.w / weight_sum;
+          Real frac = it.w / weight_sum;
           Vec2 dv_i = -(balls.mass * frac / mass) * dv_b;
           adhesion_dv[it.j] += dv_i;
           coupling->fluid_momentum_change += mass * dv_i;
@@ -721,20 +721,20 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
   std::vector<uint8_t> touched(n, 0);
   double acct_wall_impulse[2] = {0.0, 0.0};
   double acct_wall_angular = 0.0;
-  float acct_wall_bins[WALL_IMPULSE_BINS] = {};
+  Real acct_wall_bins[WALL_IMPULSE_BINS] = {};
   for (size_t i = 0; i < n; ++i) {
-    float d;
+    Real d;
     Vec2 normal;
     drum.sdf_world(X[i], drum_angle_next, &d, &normal);
-    if (d < 0.0f) {
+    if (d < Real(0.0)) {
       X[i] += -d * normal;
       touched[i] = 1;
       Vec2 push = mass * (-d * normal) / dt;
       acct_wall_impulse[0] += (double)push.x;
       acct_wall_impulse[1] += (double)push.y;
       acct_wall_angular += (double)cross2(X[i], push);
-      float angle = atan2f_r(X[i].y, X[i].x);
-      size_t bin = f2u_sat(((angle + PI_F) / TAU_F) * (float)WALL_IMPULSE_BINS);
+      Real angle = atan2f_r(X[i].y, X[i].x);
+      size_t bin = f2u_sat(((angle + PI_F) / TAU_F) * (Real)WALL_IMPULSE_BINS);
       acct_wall_bins[std::min(bin, (size_t)WALL_IMPULSE_BINS - 1)] += mass * -d / dt;
     }
   }
@@ -744,15 +744,15 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
   for (size_t i = 0; i < n; ++i) V[i] += cohesion_dv[i];
   for (size_t i = 0; i < n; ++i) V[i] += adhesion_dv[i];
   // step 6: wall no-slip
-  float beta = clamp_r(slurry.wall_no_slip, 0.0f, 1.0f);
-  float wall_work_j = 0.0f;
+  Real beta = clamp_r((Real)slurry.wall_no_slip, Real(0.0), Real(1.0));
+  Real wall_work_j = Real(0.0);
   double ke_before_noslip = kinetic_energy_f64(V, mass);
-  if (beta > 0.0f) {
+  if (beta > Real(0.0)) {
     for (size_t i = 0; i < n; ++i) {
       if (!touched[i]) continue;
       Vec2 v_wall = drum.wall_velocity(X[i]);
       Vec2 v_old = V[i];
-      V[i] = (1.0f - beta) * v_old + beta * v_wall;
+      V[i] = (Real(1.0) - beta) * v_old + beta * v_wall;
       Vec2 dv = V[i] - v_old;
       wall_work_j += mass * dv.dot(v_wall);
       acct_wall_impulse[0] += (double)(mass * dv.x);
@@ -763,20 +763,20 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
   double ke_mark = kinetic_energy_f64(V, mass);
   double ke_delta_noslip = ke_mark - ke_before_noslip;
   // step 6.5: ball drag (Gauss-Seidel over balls)
-  float mu = fmax_r(slurry.viscosity_pa_s, 0.0f);
-  if (balls.len() > 0 && balls.radius > 0.0f && balls.true_radius > 0.0f && mu > 1e-6f) {
-    float beta_b = clamp_r(slurry.ball_no_slip, 0.0f, 1.0f);
-    float rot_cap = 0.2f * fluid_speed_clamp_v_max(drum);
-    float rho_ball = balls.mass / (PI_F * balls.radius * balls.radius);
-    float mass_true = rho_ball * PI_F * balls.true_radius * balls.true_radius;
-    float inv_tau_stokes = 0.0f;
-    if (beta_b > 0.0f) {
-      float h_c = balls.radius + h;
-      float w_hc0 = fmax_r(poly6(0.0f, h_c), 1e-12f);
-      UniformGrid cgrid = UniformGrid::build(X, fmax_r(h_c, 1e-6f));
-      float i_b = balls.inertia;
+  Real mu = fmax_r((Real)slurry.viscosity_pa_s, Real(0.0));
+  if (balls.len() > 0 && balls.radius > Real(0.0) && balls.true_radius > Real(0.0) && mu > Real(1e-6)) {
+    Real beta_b = clamp_r((Real)slurry.ball_no_slip, Real(0.0), Real(1.0));
+    Real rot_cap = Real(0.2) * fluid_speed_clamp_v_max(drum);
+    Real rho_ball = balls.mass / (PI_F * balls.radius * balls.radius);
+    Real mass_true = rho_ball * PI_F * balls.true_radius * balls.true_radius;
+    Real inv_tau_stokes = Real(0.0);
+    if (beta_b > Real(0.0)) {
+      Real h_c = balls.radius + h;
+      Real w_hc0 = fmax_r(poly6(Real(0.0), h_c), Real(1e-12));
+      UniformGrid cgrid = UniformGrid::build(X, fmax_r(h_c, Real(1e-6)));
+      Real i_b = balls.inertia;
       std::vector<uint32_t> nearby;
-      struct Item { size_t j; Vec2 r_i; float phi; };
+      struct Item { size_t j; Vec2 r_i; Real phi; };
       std::vector<Item> items;
       for (size_t b = 0; b < balls.len(); ++b) {
         if (!balls.x[b].is_finite()) continue;
@@ -784,16 +784,16 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
         cgrid.for_each_near(balls.x[b], [&](uint32_t j) { nearby.push_back(j); });
         if (nearby.empty()) continue;
         items.clear();
-        float m_ent = 0.0f, i_ent = 0.0f, l_sum = 0.0f;
+        Real m_ent = Real(0.0), i_ent = Real(0.0), l_sum = Real(0.0);
         Vec2 r_sum, v_sum;
         for (uint32_t jj : nearby) {
           size_t ju = jj;
           Vec2 r_i = X[ju] - balls.x[b];
-          float r2 = r_i.length_squared();
+          Real r2 = r_i.length_squared();
           if (!std::isfinite(r2) || r2 >= h_c * h_c) continue;
-          float phi = poly6(r2, h_c) / w_hc0;
-          if (phi <= 0.0f) continue;
-          float w = mass * phi;
+          Real phi = poly6(r2, h_c) / w_hc0;
+          if (phi <= Real(0.0)) continue;
+          Real w = mass * phi;
           m_ent += w;
           r_sum += w * r_i;
           v_sum += w * V[ju];
@@ -802,43 +802,43 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
           items.push_back({ju, r_i, phi});
         }
         if (ctr) ctr->n_coupling_items += (uint32_t)items.size();
-        if (m_ent <= 1e-12f || items.empty()) continue;
+        if (m_ent <= Real(1e-12) || items.empty()) continue;
         Vec2 r_bar = r_sum / m_ent;
         Vec2 v_bar = v_sum / m_ent;
         Vec2 v_rel = v_bar - balls.v[b];
-        float speed_rel = v_rel.length();
-        float inv_tau_form = (speed_rel > 1e-6f && rest_density > 0.0f)
-                                 ? 0.5f * rest_density * BALL_FORM_DRAG_COEFFICIENT * (2.0f * balls.true_radius) *
+        Real speed_rel = v_rel.length();
+        Real inv_tau_form = (speed_rel > Real(1e-6) && rest_density > Real(0.0))
+                                 ? Real(0.5) * rest_density * BALL_FORM_DRAG_COEFFICIENT * (Real(2.0) * balls.true_radius) *
                                        speed_rel / mass_true
-                                 : 0.0f;
-        float bt = beta_b * (1.0f - expf_r(-dt * (inv_tau_stokes + inv_tau_form)));
-        float a_lin = bt * m_ent / (balls.mass + m_ent);
+                                 : Real(0.0);
+        Real bt = beta_b * (Real(1.0) - expf_r(-dt * (inv_tau_stokes + inv_tau_form)));
+        Real a_lin = bt * m_ent / (balls.mass + m_ent);
         Vec2 dv_b = a_lin * v_rel;
-        float dw_b = 0.0f, c_rot = 0.0f;
+        Real dw_b = Real(0.0), c_rot = Real(0.0);
         Vec2 p_bar;
-        if (i_ent > 1e-12f) {
-          float omega_bar = l_sum / i_ent;
-          float a_rot = bt * i_ent / (i_b + i_ent);
-          float candidate_dw = a_rot * (omega_bar - balls.omega[b]);
+        if (i_ent > Real(1e-12)) {
+          Real omega_bar = l_sum / i_ent;
+          Real a_rot = bt * i_ent / (i_b + i_ent);
+          Real candidate_dw = a_rot * (omega_bar - balls.omega[b]);
           p_bar = Vec2(-r_bar.y, r_bar.x);
-          float s = 0.0f, s_scale = 0.0f;
+          Real s = Real(0.0), s_scale = Real(0.0);
           for (auto& it : items) {
             Vec2 perp_i(-it.r_i.y, it.r_i.x);
-            float phi2 = it.phi * it.phi;
+            Real phi2 = it.phi * it.phi;
             s += mass * phi2 * cross2(it.r_i, perp_i - p_bar);
             s_scale += mass * phi2 * it.r_i.length_squared();
           }
-          if (std::fabs(s) > 0.1f * s_scale) {
-            float raw_c_rot = -i_b * candidate_dw / s;
-            float max_lever = 2.0f * h_c;
-            float c_rot_cap = max_lever > 1e-9f ? rot_cap / max_lever : 0.0f;
+          if (std::fabs(s) > Real(0.1) * s_scale) {
+            Real raw_c_rot = -i_b * candidate_dw / s;
+            Real max_lever = Real(2.0) * h_c;
+            Real c_rot_cap = max_lever > Real(1e-9) ? rot_cap / max_lever : Real(0.0);
             c_rot = clamp_r(raw_c_rot, -c_rot_cap, c_rot_cap);
             dw_b = -c_rot * s / i_b;
           }
         }
         for (auto& it : items) {
           Vec2 dv_i = -(balls.mass / m_ent) * dv_b * it.phi;
-          if (c_rot != 0.0f) {
+          if (c_rot != Real(0.0)) {
             Vec2 perp_i(-it.r_i.y, it.r_i.x);
             dv_i += c_rot * it.phi * (perp_i - p_bar);
           }
@@ -854,44 +854,44 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
   double ke_delta_drag = ke_after_drag - ke_mark;
   ke_mark = ke_after_drag;
   // step 6.6: buoyancy (Gauss-Seidel over balls on the stale step-2 grid)
-  if (balls.len() > 0 && balls.radius > 0.0f) {
-    float area = PI_F * balls.radius * balls.radius;
+  if (balls.len() > 0 && balls.radius > Real(0.0)) {
+    Real area = PI_F * balls.radius * balls.radius;
     std::vector<uint32_t> nearby;
-    std::vector<std::pair<size_t, float>> weights;
+    std::vector<std::pair<size_t, Real>> weights;
     for (size_t b = 0; b < balls.len(); ++b) {
       if (!balls.x[b].is_finite()) continue;
       nearby.clear();
       grid.for_each_near(balls.x[b], [&](uint32_t j) { nearby.push_back(j); });
       if (nearby.empty()) continue;
-      float rho_local = 0.0f;
+      Real rho_local = Real(0.0);
       weights.clear();
       for (uint32_t jj : nearby) {
         size_t ju = jj;
-        float r2 = (balls.x[b] - X[ju]).length_squared();
-        float w = mass * poly6(r2, h);
-        if (w > 0.0f) { rho_local += w; weights.push_back({ju, w}); }
+        Real r2 = (balls.x[b] - X[ju]).length_squared();
+        Real w = mass * poly6(r2, h);
+        if (w > Real(0.0)) { rho_local += w; weights.push_back({ju, w}); }
       }
-      if (ctr && rho_local > 0.0f) ctr->n_coupling_items += (uint32_t)weights.size();
-      if (rho_local <= 0.0f) continue;
-      float rho_eff = fmin_r(rho_local, rest_density);
-      float omega_num = 0.0f, omega_den = 0.0f;
+      if (ctr && rho_local > Real(0.0)) ctr->n_coupling_items += (uint32_t)weights.size();
+      if (rho_local <= Real(0.0)) continue;
+      Real rho_eff = fmin_r(rho_local, rest_density);
+      Real omega_num = Real(0.0), omega_den = Real(0.0);
       for (auto& jw : weights) {
         Vec2 d = X[jw.first];
-        float d2 = d.length_squared();
-        if (d2 <= 1e-12f) continue;
+        Real d2 = d.length_squared();
+        if (d2 <= Real(1e-12)) continue;
         omega_num += jw.second * cross2(d, V[jw.first]) / d2;
         omega_den += jw.second;
       }
-      float omega_local = omega_den > 0.0f
+      Real omega_local = omega_den > Real(0.0)
                               ? clamp_r(omega_num / omega_den, -std::fabs(drum.omega), std::fabs(drum.omega))
-                              : 0.0f;
-      Vec2 g_vec(0.0f, GRAVITY);
+                              : Real(0.0);
+      Vec2 g_vec(Real(0.0), GRAVITY);
       Vec2 centripetal = omega_local * omega_local * balls.x[b];
       Vec2 g_eff = g_vec + centripetal;
       Vec2 impulse_on_ball = -rho_eff * area * g_eff * dt;
       coupling->impulses[b] += impulse_on_ball;
       for (auto& jw : weights) {
-        float frac = jw.second / rho_local;
+        Real frac = jw.second / rho_local;
         Vec2 dv = -(impulse_on_ball * frac) / mass;
         V[jw.first] += dv;
         coupling->fluid_momentum_change += mass * dv;
@@ -904,34 +904,34 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
   // density recompute at final x over the step-2 neighbour lists
   uint32_t viscosity_iterations = 0;
   for (size_t i = 0; i < n; ++i) {
-    float rho = mass * poly6(0.0f, h);
+    Real rho = mass * poly6(Real(0.0), h);
     for (size_t k = nb.b(i); k < nb.e(i); ++k) {
-      float r2 = (X[i] - X[nb.idx[k]]).length_squared();
+      Real r2 = (X[i] - X[nb.idx[k]]).length_squared();
       rho += mass * poly6(r2, h);
     }
     density[i] = rho;
   }
   // step 7: implicit viscosity
-  if (mu > 0.0f) {
-    std::vector<float> mu_eff;
-    if (slurry.rheology == RHEO_BINGHAM && slurry.yield_stress_pa > 0.0f) {
+  if (mu > Real(0.0)) {
+    std::vector<Real> mu_eff;
+    if (slurry.rheology == RHEO_BINGHAM && slurry.yield_stress_pa > Real(0.0)) {
       mu_eff = bingham_viscosity(shear_rates(X, V, nb, density, mass, h), mu, slurry.yield_stress_pa);
     } else {
       mu_eff.assign(n, mu);
     }
     ViscWeights weights = morris_weights(X, nb, density, mass, mu_eff, h);
     std::vector<BoundaryGroup> groups;
-    if (balls.len() > 0 && balls.radius > 0.0f) {
-      float dx = 0.5f * h;
+    if (balls.len() > 0 && balls.radius > Real(0.0)) {
+      Real dx = Real(0.5) * h;
       size_t count = boundary_points_per_ball(balls.radius, dx);
       std::vector<Vec2> pts = ball_boundary_particles(balls, dx);
       UniformGrid grid_now = UniformGrid::build(X, h);
-      float eta2 = VISCOSITY_ETA_FACTOR * h * h;
-      float spiky_norm = -30.0f / (PI_F * powi5(h));
-      float range2 = h * h * (1.0f + 1e-4f);
-      std::vector<float> fluid_factor(n);
+      Real eta2 = VISCOSITY_ETA_FACTOR * h * h;
+      Real spiky_norm = -Real(30.0) / (PI_F * powi5(h));
+      Real range2 = h * h * (Real(1.0) + Real(1e-4));
+      std::vector<Real> fluid_factor(n);
       for (size_t j = 0; j < n; ++j)
-        fluid_factor[j] = BALL_BC_GAIN * (mass * 2.0f * mu_eff[j] / (fmax_r(density[j], 1e-6f) * rest_density));
+        fluid_factor[j] = BALL_BC_GAIN * (mass * Real(2.0) * mu_eff[j] / (fmax_r(density[j], Real(1e-6)) * rest_density));
       std::vector<uint32_t> slot(n, UINT32_MAX);
       size_t group_start = 0, current_ball = SIZE_MAX;
       for (size_t k = 0; k < pts.size(); ++k) {
@@ -945,16 +945,16 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
         if (!balls.x[bi].is_finite()) continue;
         grid_now.for_each_near(bp, [&](uint32_t j) {
           Vec2 delta = X[j] - bp;
-          float r2 = delta.length_squared();
+          Real r2 = delta.length_squared();
           if (r2 >= range2) return;
-          float r = std::sqrt(r2);
-          if (!std::isfinite(r) || r >= h || r <= 1e-9f) return;
-          float dot_abs = std::fabs(spiky_norm * (h - r) * (h - r) * r);
-          float c = fluid_factor[j] * dot_abs / (r2 + eta2);
-          if (c > 0.0f) {
+          Real r = std::sqrt(r2);
+          if (!std::isfinite(r) || r >= h || r <= Real(1e-9)) return;
+          Real dot_abs = std::fabs(spiky_norm * (h - r) * (h - r) * r);
+          Real c = fluid_factor[j] * dot_abs / (r2 + eta2);
+          if (c > Real(0.0)) {
             Vec2 lever = bp - balls.x[bi];
             Vec2 lever_c = c * lever;
-            float lever2_c = c * lever.length_squared();
+            Real lever2_c = c * lever.length_squared();
             uint32_t s = slot[j];
             if (s == UINT32_MAX) {
               slot[j] = (uint32_t)groups.size();
@@ -972,7 +972,7 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
     std::vector<Vec2> ball_v0(balls.len());
     for (size_t bi = 0; bi < balls.len(); ++bi) ball_v0[bi] = balls.v[bi] + coupling->impulses[bi] / balls.mass;
     size_t links_in_range = 0;
-    std::vector<SqueezeLink> links = squeeze_links(balls, drum.radius_m, 0.5f * h, mu, dt, &ball_v0, &links_in_range);
+    std::vector<SqueezeLink> links = squeeze_links(balls, drum.radius_m, Real(0.5) * h, mu, dt, &ball_v0, &links_in_range);
     if (ctr) {
       ctr->n_groups = (uint32_t)groups.size();
       ctr->n_links = (uint32_t)links.size();
@@ -982,10 +982,10 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
       viscosity_iterations = solve_implicit_viscosity(nb, weights, &V, dt, opt.cg_fp64 != 0);
     } else {
       std::vector<Vec2> ball_v = ball_v0;
-      std::vector<float> ball_w(balls.len());
+      std::vector<Real> ball_w(balls.len());
       for (size_t bi = 0; bi < balls.len(); ++bi)
         ball_w[bi] = balls.omega[bi] + coupling->angular_impulses[bi] / balls.inertia;
-      std::vector<float> ball_w0 = ball_w;
+      std::vector<Real> ball_w0 = ball_w;
       std::vector<Vec2> guess;
       guess.swap(fl->viscous_guess);
       std::vector<Vec2> v_in = V;
@@ -998,7 +998,7 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
       }
       for (size_t bi = 0; bi < balls.len(); ++bi) {
         Vec2 dv = ball_v[bi] - ball_v0[bi];
-        float dw = ball_w[bi] - ball_w0[bi];
+        Real dw = ball_w[bi] - ball_w0[bi];
         if (dv.is_finite() && std::isfinite(dw)) {
           coupling->impulses[bi] += balls.mass * dv;
           coupling->angular_impulses[bi] += balls.inertia * dw;
@@ -1008,18 +1008,18 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
     }
   }
   if (ctr) ctr->cg_iters = viscosity_iterations;
-  float mean_shear = mean_shear_rate(X, V, nb, density, mass, h);
+  Real mean_shear = mean_shear_rate(X, V, nb, density, mass, h);
   double ke_after_visc = kinetic_energy_f64(V, mass);
   double ke_delta_visc = ke_after_visc - ke_mark;
   clamp_fluid_speed(&V, fluid_speed_clamp_v_max(drum));
   double ke_delta_clamp = kinetic_energy_f64(V, mass) - ke_after_visc;
   // step 8: impulse clamp
   if (balls.len() > 0) {
-    float clamp = impulse_clamp(balls.mass, dt);
-    float angular_clamp = clamp * balls.radius;
+    Real clamp = impulse_clamp(balls.mass, dt);
+    Real angular_clamp = clamp * balls.radius;
     for (size_t b = 0; b < balls.len(); ++b) {
-      float mag = coupling->impulses[b].length();
-      if (mag > clamp && mag > 1e-9f) {
+      Real mag = coupling->impulses[b].length();
+      if (mag > clamp && mag > Real(1e-9)) {
         coupling->impulses[b] *= clamp / mag;
         coupling->clamp_hits += 1;
       }
@@ -1031,52 +1031,52 @@ void fluid_step_coupled(Fluid* fl, const Drum& drum, float drum_angle, const Slu
   st.mean_shear_rate_per_s = mean_shear;
   st.coupling_clamp_hits = coupling->clamp_hits;
   st.wall_work_j = wall_work_j;
-  st.wall_impulse[0] = (float)acct_wall_impulse[0];
-  st.wall_impulse[1] = (float)acct_wall_impulse[1];
-  st.wall_angular_impulse = (float)acct_wall_angular;
+  st.wall_impulse[0] = (Real)acct_wall_impulse[0];
+  st.wall_impulse[1] = (Real)acct_wall_impulse[1];
+  st.wall_angular_impulse = (Real)acct_wall_angular;
   for (int k = 0; k < WALL_IMPULSE_BINS; ++k) st.wall_normal_impulse_by_angle[k] = acct_wall_bins[k];
-  st.ke_delta_noslip_j = (float)ke_delta_noslip;
-  st.ke_delta_drag_j = (float)ke_delta_drag;
-  st.ke_delta_buoyancy_j = (float)ke_delta_buoy;
-  st.ke_delta_viscosity_j = (float)ke_delta_visc;
-  st.ke_delta_clamp_j = (float)ke_delta_clamp;
+  st.ke_delta_noslip_j = (Real)ke_delta_noslip;
+  st.ke_delta_drag_j = (Real)ke_delta_drag;
+  st.ke_delta_buoyancy_j = (Real)ke_delta_buoy;
+  st.ke_delta_viscosity_j = (Real)ke_delta_visc;
+  st.ke_delta_clamp_j = (Real)ke_delta_clamp;
 }
 
 // ------------------------------------------------------------------ dem.rs
-static const float RESTITUTION_VELOCITY_THRESHOLD = 0.02f;
-static const float RESTITUTION_THRESHOLD_FROUDE = 0.1428f;
-static const float MAX_RECOVERY_FRACTION = 0.2f;
-static const float CCD_CONTACT_SKIN_FRACTION = 1e-2f;
-static const float IMPACT_ENERGY_MIN_J = 1e-6f;
-static const float IMPACT_ENERGY_MAX_J = 1.0f;
+static const Real RESTITUTION_VELOCITY_THRESHOLD = Real(0.02);
+static const Real RESTITUTION_THRESHOLD_FROUDE = Real(0.1428);
+static const Real MAX_RECOVERY_FRACTION = Real(0.2);
+static const Real CCD_CONTACT_SKIN_FRACTION = Real(1e-2);
+static const Real IMPACT_ENERGY_MIN_J = Real(1e-6);
+static const Real IMPACT_ENERGY_MAX_J = Real(1.0);
 
 // dem.rs:43-46
-float restitution_velocity_threshold(float r) {
-  return RESTITUTION_THRESHOLD_FROUDE * std::sqrt(-GRAVITY * 2.0f * r);
+Real restitution_velocity_threshold(Real r) {
+  return RESTITUTION_THRESHOLD_FROUDE * std::sqrt(-GRAVITY * Real(2.0) * r);
 }
 // dem.rs:99-109
-int impact_energy_bin(float e) {
-  if (!std::isfinite(e) || e <= 0.0f) return -1;
-  float ec = clamp_r(e, IMPACT_ENERGY_MIN_J, IMPACT_ENERGY_MAX_J);
-  float log_min = log10f_r(IMPACT_ENERGY_MIN_J);
-  float log_max = log10f_r(IMPACT_ENERGY_MAX_J);
-  float t = (log10f_r(ec) - log_min) / (log_max - log_min);
-  uint32_t idx = f2u_sat(t * (float)IMPACT_BINS);
+int impact_energy_bin(Real e) {
+  if (!std::isfinite(e) || e <= Real(0.0)) return -1;
+  Real ec = clamp_r(e, IMPACT_ENERGY_MIN_J, IMPACT_ENERGY_MAX_J);
+  Real log_min = log10f_r(IMPACT_ENERGY_MIN_J);
+  Real log_max = log10f_r(IMPACT_ENERGY_MAX_J);
+  Real t = (log10f_r(ec) - log_min) / (log_max - log_min);
+  uint32_t idx = f2u_sat(t * (Real)IMPACT_BINS);
   return (int)std::min(idx, (uint32_t)IMPACT_BINS - 1);
 }
 // dem.rs:127-138
-float effective_friction(float mu_k, float mu_s, float v_t, float vs) {
+Real effective_friction(Real mu_k, Real mu_s, Real v_t, Real vs) {
   if (mu_s <= mu_k) return mu_k;
-  float ratio = v_t / vs;
-  float weight = expf_r(-(ratio * ratio));
+  Real ratio = v_t / vs;
+  Real weight = expf_r(-(ratio * ratio));
   return mu_k + (mu_s - mu_k) * weight;
 }
 // dem.rs:253-273
-static float mechanical_energy_j(const Balls& b) {
-  float e = 0.0f;
+static Real mechanical_energy_j(const Balls& b) {
+  Real e = Real(0.0);
   for (size_t i = 0; i < b.len(); ++i) {
-    e += 0.5f * b.mass * b.v[i].length_squared();
-    e += 0.5f * b.inertia * b.omega[i] * b.omega[i];
+    e += Real(0.5) * b.mass * b.v[i].length_squared();
+    e += Real(0.5) * b.inertia * b.omega[i] * b.omega[i];
     e += b.mass * std::fabs(GRAVITY) * b.x[i].y;
   }
   return e;
@@ -1091,31 +1091,31 @@ double dem_mechanical_energy_f64(const Balls& b) {
   return e;
 }
 // dem.rs:1071-1080
-static float angle_diff(float a, float b) {
-  float d = a - b;
-  while (d > PI_F) d -= 2.0f * PI_F;
-  while (d < -PI_F) d += 2.0f * PI_F;
+static Real angle_diff(Real a, Real b) {
+  Real d = a - b;
+  while (d > PI_F) d -= Real(2.0) * PI_F;
+  while (d < -PI_F) d += Real(2.0) * PI_F;
   return d;
 }
 
 // dem.rs:530-1066
-DemStepStats dem_step_recorded(Balls* bp, const Drum& drum, float drum_angle, const MediaParams& media,
-                               uint32_t iterations, float dt, const CouplingImpulses* ext,
+DemStepStats dem_step_recorded(Balls* bp, const Drum& drum, Real drum_angle, const MediaParams& media,
+                               uint32_t iterations, Real dt, const CouplingImpulses* ext,
                                std::vector<ImpactRecord>* impacts, StepCounters* ctr, Debug* dbg) {
   Balls& B = *bp;
   DemStepStats out;
-  if (B.len() == 0 || dt <= 0.0f) return out;
+  if (B.len() == 0 || dt <= Real(0.0)) return out;
   size_t n = B.len();
-  float w = B.mass > 0.0f ? 1.0f / B.mass : 0.0f;
-  float w_rot = B.inertia > 0.0f ? 1.0f / B.inertia : 0.0f;
-  float r = B.radius;
-  float impact_threshold = restitution_velocity_threshold(r);
+  Real w = B.mass > Real(0.0) ? Real(1.0) / B.mass : Real(0.0);
+  Real w_rot = B.inertia > Real(0.0) ? Real(1.0) / B.inertia : Real(0.0);
+  Real r = B.radius;
+  Real impact_threshold = restitution_velocity_threshold(r);
   for (size_t i = 0; i < n; ++i)
     if (!B.x[i].is_finite() || !B.v[i].is_finite()) { B.x[i] = Vec2(); B.v[i] = Vec2(); }
   std::vector<Vec2> x0 = B.x;
-  std::vector<float> theta0 = B.theta;
+  std::vector<Real> theta0 = B.theta;
   std::vector<Vec2> v_pre = B.v;
-  std::vector<float> omega_pre = B.omega;
+  std::vector<Real> omega_pre = B.omega;
   double coupling_work = 0.0;
   for (size_t i = 0; i < n; ++i) {
     B.v[i].y += GRAVITY * dt;
@@ -1131,67 +1131,67 @@ DemStepStats dem_step_recorded(Balls* bp, const Drum& drum, float drum_angle, co
     B.x[i] += B.v[i] * dt;
     B.theta[i] += B.omega[i] * dt;
   }
-  float e_after_predict = mechanical_energy_j(B);
-  float max_disp = 0.0f;
-  for (size_t i = 0; i < n; ++i) max_disp = fmax_r(max_disp, B.v[i].length() * dt / fmax_r(2.0f * r, 1e-12f));
-  float max_speed = 0.0f;
+  Real e_after_predict = mechanical_energy_j(B);
+  Real max_disp = Real(0.0);
+  for (size_t i = 0; i < n; ++i) max_disp = fmax_r(max_disp, B.v[i].length() * dt / fmax_r(Real(2.0) * r, Real(1e-12)));
+  Real max_speed = Real(0.0);
   for (size_t i = 0; i < n; ++i) max_speed = fmax_r(max_speed, B.v[i].length());
-  float solve_margin = (float)std::max(iterations, 1u) * MAX_RECOVERY_FRACTION * 2.0f * r;
-  float cell_size = fmax_r(fmax_r(2.0f * r * 1.05f, 2.0f * r + max_speed * dt + solve_margin), 1e-6f);
+  Real solve_margin = (Real)std::max(iterations, 1u) * MAX_RECOVERY_FRACTION * Real(2.0) * r;
+  Real cell_size = fmax_r(fmax_r(Real(2.0) * r * Real(1.05), Real(2.0) * r + max_speed * dt + solve_margin), Real(1e-6));
   UniformGrid grid = UniformGrid::build(B.x, cell_size);
   std::vector<std::pair<uint32_t, uint32_t>> pairs;
   grid.for_each_candidate_pair([&](uint32_t i, uint32_t j) { pairs.push_back({i, j}); });
   if (ctr) ctr->n_ball_pairs = (uint32_t)pairs.size();
   if (dbg) dbg->ball_pairs = pairs;
   // step 2.5: wall CCD
-  float drum_angle_next = drum_angle + drum.omega * dt;
-  std::vector<float> toi(n, 1.0f);
+  Real drum_angle_next = drum_angle + drum.omega * dt;
+  std::vector<Real> toi(n, Real(1.0));
   for (size_t i = 0; i < n; ++i) {
-    float d_end;
+    Real d_end;
     Vec2 nn;
     drum.sdf_world(B.x[i], drum_angle_next, &d_end, &nn);
-    float c_end = d_end - r;
-    if (c_end >= -MAX_RECOVERY_FRACTION * 2.0f * r) continue;
-    float t;
+    Real c_end = d_end - r;
+    if (c_end >= -MAX_RECOVERY_FRACTION * Real(2.0) * r) continue;
+    Real t;
     if (drum.toi_swept(x0[i], B.x[i], drum_angle, drum_angle_next, r, &t)) toi[i] = fmin_r(toi[i], t);
   }
   for (size_t i = 0; i < n; ++i) {
-    if (toi[i] < 1.0f) {
+    if (toi[i] < Real(1.0)) {
       if (ctr) ctr->ccd_clamps += 1;
-      float path_len = (B.x[i] - x0[i]).length();
-      float skin = CCD_CONTACT_SKIN_FRACTION * r;
-      float t_skin = path_len > 1e-9f ? skin / path_len : 1.0f;
-      float t_cl = fmin_r(toi[i] + t_skin, 1.0f);
+      Real path_len = (B.x[i] - x0[i]).length();
+      Real skin = CCD_CONTACT_SKIN_FRACTION * r;
+      Real t_skin = path_len > Real(1e-9) ? skin / path_len : Real(1.0);
+      Real t_cl = fmin_r(toi[i] + t_skin, Real(1.0));
       B.x[i] = x0[i] + (B.x[i] - x0[i]) * t_cl;
     }
   }
-  std::vector<float> lam_bb(pairs.size(), 0.0f), lam_bw(n, 0.0f);
+  std::vector<Real> lam_bb(pairs.size(), Real(0.0)), lam_bw(n, Real(0.0));
   // step 3: projection
   for (uint32_t it = 0; it < std::max(iterations, 1u); ++it) {
     for (size_t k = 0; k < pairs.size(); ++k) {
       size_t i = pairs[k].first, j = pairs[k].second;
       Vec2 delta = B.x[i] - B.x[j];
-      float dist = delta.length();
-      float c = dist - 2.0f * r;
-      if (c >= 0.0f) continue;
-      Vec2 n_hat = dist > 1e-9f ? delta / dist : Vec2(1.0f, 0.0f);
-      float w_sum = w + w;
-      if (w_sum <= 0.0f) continue;
-      float c_eff = fmax_r(c, -MAX_RECOVERY_FRACTION * 2.0f * r);
-      float d_lambda = -c_eff / w_sum;
+      Real dist = delta.length();
+      Real c = dist - Real(2.0) * r;
+      if (c >= Real(0.0)) continue;
+      Vec2 n_hat = dist > Real(1e-9) ? delta / dist : Vec2(Real(1.0), Real(0.0));
+      Real w_sum = w + w;
+      if (w_sum <= Real(0.0)) continue;
+      Real c_eff = fmax_r(c, -MAX_RECOVERY_FRACTION * Real(2.0) * r);
+      Real d_lambda = -c_eff / w_sum;
       B.x[i] += w * d_lambda * n_hat;
       B.x[j] -= w * d_lambda * n_hat;
       lam_bb[k] += d_lambda;
     }
     for (size_t i = 0; i < n; ++i) {
-      float d;
+      Real d;
       Vec2 n_hat;
       drum.sdf_world(B.x[i], drum_angle_next, &d, &n_hat);
-      float c = d - r;
-      if (c >= 0.0f) continue;
-      if (w <= 0.0f) continue;
-      float c_eff = fmax_r(c, -MAX_RECOVERY_FRACTION * 2.0f * r);
-      float d_lambda = -c_eff / w;
+      Real c = d - r;
+      if (c >= Real(0.0)) continue;
+      if (w <= Real(0.0)) continue;
+      Real c_eff = fmax_r(c, -MAX_RECOVERY_FRACTION * Real(2.0) * r);
+      Real d_lambda = -c_eff / w;
       B.x[i] += w * d_lambda * n_hat;
       lam_bw[i] += d_lambda;
     }
@@ -1201,59 +1201,59 @@ DemStepStats dem_step_recorded(Balls* bp, const Drum& drum, float drum_angle, co
     B.v[i] = (B.x[i] - x0[i]) / dt;
     B.omega[i] = angle_diff(B.theta[i], theta0[i]) / dt;
   }
-  struct C3 { uint32_t i, j; float l; };
+  struct C3 { uint32_t i, j; Real l; };
   std::vector<C3> bb(pairs.size());
   for (size_t k = 0; k < pairs.size(); ++k) bb[k] = {pairs[k].first, pairs[k].second, lam_bb[k]};
   std::sort(bb.begin(), bb.end(), [](const C3& a, const C3& b) { return a.i != b.i ? a.i < b.i : a.j < b.j; });
   if (ctr) {
     uint32_t act = 0;
-    for (auto& c : bb) act += c.l > 0.0f;
+    for (auto& c : bb) act += c.l > Real(0.0);
     ctr->n_active_contacts = act;
   }
   // step 5: friction
   for (const C3& c : bb) {
-    if (c.l <= 0.0f) continue;
+    if (c.l <= Real(0.0)) continue;
     size_t iu = c.i, ju = c.j;
     Vec2 delta = B.x[iu] - B.x[ju];
-    float dist = delta.length();
-    Vec2 n_hat = dist > 1e-9f ? delta / dist : Vec2(1.0f, 0.0f);
+    Real dist = delta.length();
+    Vec2 n_hat = dist > Real(1e-9) ? delta / dist : Vec2(Real(1.0), Real(0.0));
     Vec2 t_hat(-n_hat.y, n_hat.x);
-    float v_t = (B.v[iu] - B.v[ju]).dot(t_hat) - r * B.omega[iu] - r * B.omega[ju];
-    float w_sum_t = w + w + r * r * w_rot + r * r * w_rot;
-    if (w_sum_t <= 0.0f) continue;
-    float raw = -v_t * dt / w_sum_t;
-    float mu = effective_friction(media.friction_ball_ball, media.friction_ball_ball_static, v_t,
+    Real v_t = (B.v[iu] - B.v[ju]).dot(t_hat) - r * B.omega[iu] - r * B.omega[ju];
+    Real w_sum_t = w + w + r * r * w_rot + r * r * w_rot;
+    if (w_sum_t <= Real(0.0)) continue;
+    Real raw = -v_t * dt / w_sum_t;
+    Real mu = effective_friction(media.friction_ball_ball, media.friction_ball_ball_static, v_t,
                                   media.friction_velocity_scale_m_s);
-    float max_mag = mu * c.l;
-    float dlt = clamp_r(raw, -max_mag, max_mag);
+    Real max_mag = mu * c.l;
+    Real dlt = clamp_r(raw, -max_mag, max_mag);
     B.x[iu] += w * dlt * t_hat;
     B.x[ju] -= w * dlt * t_hat;
     B.theta[iu] -= r * w_rot * dlt;
     B.theta[ju] -= r * w_rot * dlt;
     Vec2 dv = w * dlt * t_hat / dt;
-    float domega = -r * w_rot * dlt / dt;
+    Real domega = -r * w_rot * dlt / dt;
     B.v[iu] += dv;
     B.v[ju] -= dv;
     B.omega[iu] += domega;
     B.omega[ju] += domega;
   }
-  float wall_work_j = 0.0f;
+  Real wall_work_j = Real(0.0);
   for (size_t i = 0; i < n; ++i) {
-    float lambda_n = lam_bw[i];
-    if (lambda_n <= 0.0f) continue;
-    float dd;
+    Real lambda_n = lam_bw[i];
+    if (lambda_n <= Real(0.0)) continue;
+    Real dd;
     Vec2 n_hat;
     drum.sdf_world(B.x[i], drum_angle_next, &dd, &n_hat);
     Vec2 t_hat(-n_hat.y, n_hat.x);
     Vec2 v_wall = drum.wall_velocity(B.x[i] - r * n_hat);
-    float v_t = (B.v[i] - v_wall).dot(t_hat) - r * B.omega[i];
-    float w_sum_t = w + r * r * w_rot;
-    if (w_sum_t <= 0.0f) continue;
-    float raw = -v_t * dt / w_sum_t;
-    float mu = effective_friction(media.friction_ball_wall, media.friction_ball_wall_static, v_t,
+    Real v_t = (B.v[i] - v_wall).dot(t_hat) - r * B.omega[i];
+    Real w_sum_t = w + r * r * w_rot;
+    if (w_sum_t <= Real(0.0)) continue;
+    Real raw = -v_t * dt / w_sum_t;
+    Real mu = effective_friction(media.friction_ball_wall, media.friction_ball_wall_static, v_t,
                                   media.friction_velocity_scale_m_s);
-    float max_mag = mu * lambda_n;
-    float dlt = clamp_r(raw, -max_mag, max_mag);
+    Real max_mag = mu * lambda_n;
+    Real dlt = clamp_r(raw, -max_mag, max_mag);
     B.x[i] += w * dlt * t_hat;
     B.theta[i] -= r * w_rot * dlt;
     B.v[i] += w * dlt * t_hat / dt;
@@ -1270,82 +1270,82 @@ DemStepStats dem_step_recorded(Balls* bp, const Drum& drum, float drum_angle, co
   uint32_t collision_count = 0;
   uint32_t hist[IMPACT_BINS] = {};
   for (const C3& c : bb) {
-    if (c.l <= 0.0f) continue;
+    if (c.l <= Real(0.0)) continue;
     size_t iu = c.i, ju = c.j;
     Vec2 delta = B.x[iu] - B.x[ju];
-    float dist = delta.length();
-    Vec2 n_hat = dist > 1e-9f ? delta / dist : Vec2(1.0f, 0.0f);
-    float v_n_pre = (v_pre[iu] - v_pre[ju]).dot(n_hat);
+    Real dist = delta.length();
+    Vec2 n_hat = dist > Real(1e-9) ? delta / dist : Vec2(Real(1.0), Real(0.0));
+    Real v_n_pre = (v_pre[iu] - v_pre[ju]).dot(n_hat);
     bool fresh = v_n_pre < -RESTITUTION_VELOCITY_THRESHOLD;
     if (fresh) {
       collision_count += 1;
-      float e_imp = 0.5f * (B.mass * 0.5f) * v_n_pre * v_n_pre;
+      Real e_imp = Real(0.5) * (B.mass * Real(0.5)) * v_n_pre * v_n_pre;
       int bin = impact_energy_bin(e_imp);
       if (bin >= 0) hist[bin] += 1;
     }
-    float e = fresh ? media.restitution_ball_ball : 0.0f;
+    Real e = fresh ? media.restitution_ball_ball : Real(0.0);
     if (-v_n_pre > impact_threshold && impacts) {
       Vec2 t_hat(-n_hat.y, n_hat.x);
-      float slip = (v_pre[iu] - v_pre[ju]).dot(t_hat) - r * omega_pre[iu] - r * omega_pre[ju];
-      impacts->push_back({0u, c.i, c.j, -v_n_pre, std::fabs(slip), e});
+      Real slip = (v_pre[iu] - v_pre[ju]).dot(t_hat) - r * omega_pre[iu] - r * omega_pre[ju];
+      impacts->push_back({0u, c.i, c.j, (float)-v_n_pre, (float)std::fabs(slip), (float)e});
     }
-    float target = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
-    float v_n_now = (B.v[iu] - B.v[ju]).dot(n_hat);
-    float delta_v_n = target - v_n_now;
-    float w_sum = w + w;
-    if (w_sum <= 0.0f) continue;
-    float impulse = delta_v_n / w_sum;
+    Real target = fmax_r(fmax_r(-e * v_n_pre, Real(0.0)), fmax_r(v_n_pre, Real(0.0)));
+    Real v_n_now = (B.v[iu] - B.v[ju]).dot(n_hat);
+    Real delta_v_n = target - v_n_now;
+    Real w_sum = w + w;
+    if (w_sum <= Real(0.0)) continue;
+    Real impulse = delta_v_n / w_sum;
     B.v[iu] += w * impulse * n_hat;
     B.v[ju] -= w * impulse * n_hat;
   }
   for (size_t i = 0; i < n; ++i) {
-    float lambda_n = lam_bw[i];
-    if (lambda_n <= 0.0f) continue;
-    float dd;
+    Real lambda_n = lam_bw[i];
+    if (lambda_n <= Real(0.0)) continue;
+    Real dd;
     Vec2 n_hat;
     drum.sdf_world(B.x[i], drum_angle_next, &dd, &n_hat);
     Vec2 v_wall = drum.wall_velocity(B.x[i] - r * n_hat);
-    float v_n_pre = (v_pre[i] - v_wall).dot(n_hat);
+    Real v_n_pre = (v_pre[i] - v_wall).dot(n_hat);
     bool fresh = v_n_pre < -RESTITUTION_VELOCITY_THRESHOLD;
     if (fresh) {
       collision_count += 1;
-      float e_imp = 0.5f * B.mass * v_n_pre * v_n_pre;
+      Real e_imp = Real(0.5) * B.mass * v_n_pre * v_n_pre;
       int bin = impact_energy_bin(e_imp);
       if (bin >= 0) hist[bin] += 1;
     }
-    float e = fresh ? media.restitution_ball_wall : 0.0f;
+    Real e = fresh ? media.restitution_ball_wall : Real(0.0);
     if (-v_n_pre > impact_threshold && impacts) {
       Vec2 t_hat(-n_hat.y, n_hat.x);
-      float slip = (v_pre[i] - v_wall).dot(t_hat) - r * omega_pre[i];
-      impacts->push_back({1u, (uint32_t)i, WALL_ID, -v_n_pre, std::fabs(slip), e});
+      Real slip = (v_pre[i] - v_wall).dot(t_hat) - r * omega_pre[i];
+      impacts->push_back({1u, (uint32_t)i, WALL_ID, (float)-v_n_pre, (float)std::fabs(slip), (float)e});
     }
-    float target = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
-    float v_n_now = (B.v[i] - v_wall).dot(n_hat);
-    float delta_v_n = target - v_n_now;
-    if (w <= 0.0f) continue;
+    Real target = fmax_r(fmax_r(-e * v_n_pre, Real(0.0)), fmax_r(v_n_pre, Real(0.0)));
+    Real v_n_now = (B.v[i] - v_wall).dot(n_hat);
+    Real delta_v_n = target - v_n_now;
+    if (w <= Real(0.0)) continue;
     B.v[i] += delta_v_n * n_hat;
   }
   // step 7: rolling resistance
-  if (media.rolling_friction > 0.0f && B.inertia > 0.0f) {
-    std::vector<float> total(n, 0.0f);
-    for (const C3& c : bb) { total[c.i] += fmax_r(c.l, 0.0f); total[c.j] += fmax_r(c.l, 0.0f); }
-    for (size_t i = 0; i < n; ++i) total[i] += fmax_r(lam_bw[i], 0.0f);
+  if (media.rolling_friction > Real(0.0) && B.inertia > Real(0.0)) {
+    std::vector<Real> total(n, Real(0.0));
+    for (const C3& c : bb) { total[c.i] += fmax_r(c.l, Real(0.0)); total[c.j] += fmax_r(c.l, Real(0.0)); }
+    for (size_t i = 0; i < n; ++i) total[i] += fmax_r(lam_bw[i], Real(0.0));
     for (size_t i = 0; i < n; ++i) {
-      float ln = total[i];
-      if (ln <= 0.0f || B.omega[i] == 0.0f) continue;
-      float normal_force = ln / dt;
-      float max_dw = media.rolling_friction * normal_force * r / B.inertia * dt;
-      float dw = fmin_r(max_dw, std::fabs(B.omega[i]));
+      Real ln = total[i];
+      if (ln <= Real(0.0) || B.omega[i] == Real(0.0)) continue;
+      Real normal_force = ln / dt;
+      Real max_dw = media.rolling_friction * normal_force * r / B.inertia * dt;
+      Real dw = fmin_r(max_dw, std::fabs(B.omega[i]));
       B.omega[i] -= signum_r(B.omega[i]) * dw;
     }
   }
-  float e_final = mechanical_energy_j(B);
+  Real e_final = mechanical_energy_j(B);
   out.wall_work_j = wall_work_j;
   out.collision_count = collision_count;
   for (int k = 0; k < IMPACT_BINS; ++k) out.impact_energy_histogram[k] = hist[k];
   out.dissipated_energy_j = e_after_predict + wall_work_j - e_final;
   out.max_substep_displacement_over_diameter = max_disp;
-  out.coupling_work_j = (float)coupling_work;
+  out.coupling_work_j = (Real)coupling_work;
   return out;
 }
 
@@ -1366,11 +1366,11 @@ int or_probe_viscous_operator(const float* xy, const float* v, const float* dens
   for (uint32_t i = 0; i < n; ++i) { x[i] = Vec2(xy[2 * i], xy[2 * i + 1]); vv[i] = Vec2(v[2 * i], v[2 * i + 1]); }
   Nbr nb;
   neighbor_lists(x, h, &nb.off, &nb.idx);
-  std::vector<float> dens(density, density + n), m(mu, mu + n);
+  std::vector<Real> dens(density, density + n), m(mu, mu + n);
   ViscWeights w = morris_weights(x, nb, dens, mass, m, h);
   laplacian_apply_into(nb, w, vv.data(), n, o.data());
-  float wm = 0.0f;
-  for (float q : w.w) wm = fmax_r(wm, q);
+  Real wm = Real(0.0);
+  for (Real q : w.w) wm = fmax_r(wm, q);
   for (uint32_t i = 0; i < n; ++i) { out[2 * i] = o[i].x; out[2 * i + 1] = o[i].y; }
   if (w_max) *w_max = wm;
   return 0;
@@ -1387,8 +1387,8 @@ int or_probe_squeeze_links(const float* bx, uint32_t nb, float r, float ball_mas
   Balls b;
   for (uint32_t i = 0; i < nb; ++i) b.x.push_back(Vec2(bx[2 * i], bx[2 * i + 1]));
   b.v.assign(nb, Vec2());
-  b.theta.assign(nb, 0.0f);
-  b.omega.assign(nb, 0.0f);
+  b.theta.assign(nb, Real(0.0));
+  b.omega.assign(nb, Real(0.0));
   b.radius = r;
   b.mass = ball_mass;
   std::vector<Vec2> cl;
@@ -1423,7 +1423,7 @@ int or_probe_joint_solve(uint32_t n, float* fluid_v, uint32_t nb, float* ball_v,
   for (uint32_t k = 0; k < nl; ++k)
     links.push_back({l_ball[k], l_other[k], Vec2(l_n[2 * k], l_n[2 * k + 1]), l_c[k]});
   std::vector<Vec2> v(n), bv(nb), guess;
-  std::vector<float> bw(ball_w, ball_w + nb);
+  std::vector<Real> bw(ball_w, ball_w + nb);
   for (uint32_t i = 0; i < n; ++i) v[i] = Vec2(fluid_v[2 * i], fluid_v[2 * i + 1]);
   for (uint32_t i = 0; i < nb; ++i) bv[i] = Vec2(ball_v[2 * i], ball_v[2 * i + 1]);
   uint32_t it = solve_viscosity_with_balls(nbr, w, groups, links, mass, ball_mass, ball_inertia, dt, guess, &v, &bv,

@@ -24,31 +24,31 @@ namespace orc {
 namespace {
 
 constexpr int GRID = MG_SURFACE_GRID;            // surface.rs:27
-constexpr float SPLAT_RADIUS_FACTOR = 1.5f;      // surface.rs:29
-constexpr float THRESHOLD_FRACTION = 0.5f;       // surface.rs:31
+constexpr Real SPLAT_RADIUS_FACTOR = Real(1.5);      // surface.rs:29
+constexpr Real THRESHOLD_FRACTION = Real(0.5);       // surface.rs:31
 
 // surface.rs:39-46
-float splat_kernel(float r2, float radius) {
-  const float radius2 = radius * radius;
-  if (r2 >= radius2) return 0.0f;
-  const float t = 1.0f - r2 / radius2;
+Real splat_kernel(Real r2, Real radius) {
+  const Real radius2 = radius * radius;
+  if (r2 >= radius2) return Real(0.0);
+  const Real t = Real(1.0) - r2 / radius2;
   return t * t * t;
 }
 
 // surface.rs:140-143: round half away from zero, clamp to the grid, NaN casts to 0
-int grid_index(float world, float drum_radius_m, float cell_size) {
-  float raw = std::round((world + drum_radius_m) / cell_size);
-  if (raw < 0.0f) raw = 0.0f;
-  if (raw > (float)(GRID - 1)) raw = (float)(GRID - 1);
+int grid_index(Real world, Real drum_radius_m, Real cell_size) {
+  Real raw = std::round((world + drum_radius_m) / cell_size);
+  if (raw < Real(0.0)) raw = Real(0.0);
+  if (raw > (Real)(GRID - 1)) raw = (Real)(GRID - 1);
   return std::isnan(raw) ? 0 : (int)raw;
 }
 
 // surface.rs:145-150
-Vec2 grid_point(int gi, int gj, float drum_radius_m, float cell_size) {
-  return Vec2(-drum_radius_m + (float)gi * cell_size, -drum_radius_m + (float)gj * cell_size);
+Vec2 grid_point(int gi, int gj, Real drum_radius_m, Real cell_size) {
+  return Vec2(-drum_radius_m + (Real)gi * cell_size, -drum_radius_m + (Real)gj * cell_size);
 }
 
-Vec2 lerp(Vec2 a, Vec2 b, float s) { return Vec2(a.x * (1.0f - s) + b.x * s, a.y * (1.0f - s) + b.y * s); }
+Vec2 lerp(Vec2 a, Vec2 b, Real s) { return Vec2(a.x * (Real(1.0) - s) + b.x * s, a.y * (Real(1.0) - s) + b.y * s); }
 
 // EdgeId (surface.rs:155-161): kind 0 Horizontal(i, j), kind 1 Vertical(i, j)
 struct EdgeId {
@@ -62,20 +62,20 @@ struct EdgeHash {
 };
 
 // surface.rs:166-187
-Vec2 interp_edge(EdgeId e, const std::vector<float>& field, float threshold, float drum_radius_m,
-                 float cell_size) {
+Vec2 interp_edge(EdgeId e, const std::vector<Real>& field, Real threshold, Real drum_radius_m,
+                 Real cell_size) {
   const int gi0 = e.i, gj0 = e.j;
   const int gi1 = e.kind == 0 ? e.i + 1 : e.i;
   const int gj1 = e.kind == 0 ? e.j : e.j + 1;
-  const float v0 = field[gj0 * GRID + gi0];
-  const float v1 = field[gj1 * GRID + gi1];
-  float t;
-  if (std::fabs(v1 - v0) > 1e-9f) {
+  const Real v0 = field[gj0 * GRID + gi0];
+  const Real v1 = field[gj1 * GRID + gi1];
+  Real t;
+  if (std::fabs(v1 - v0) > Real(1e-9)) {
     t = (threshold - v0) / (v1 - v0);
-    if (t < 0.0f) t = 0.0f;
-    if (t > 1.0f) t = 1.0f;
+    if (t < Real(0.0)) t = Real(0.0);
+    if (t > Real(1.0)) t = Real(1.0);
   } else {
-    t = 0.5f;
+    t = Real(0.5);
   }
   return lerp(grid_point(gi0, gj0, drum_radius_m, cell_size), grid_point(gi1, gj1, drum_radius_m, cell_size), t);
 }
@@ -135,24 +135,24 @@ std::vector<Vec2> chaikin_smooth_closed(const std::vector<Vec2>& pts) {
   out.reserve(2 * n);
   for (size_t i = 0; i < n; ++i) {
     const Vec2 p0 = pts[i], p1 = pts[(i + 1) % n];
-    out.push_back(lerp(p0, p1, 0.25f));
-    out.push_back(lerp(p0, p1, 0.75f));
+    out.push_back(lerp(p0, p1, Real(0.25)));
+    out.push_back(lerp(p0, p1, Real(0.75)));
   }
   return out;
 }
 
 // surface.rs:359-366
-Vec2 project_inside_wall(Vec2 p, const Drum& drum, float drum_angle) {
-  float d;
+Vec2 project_inside_wall(Vec2 p, const Drum& drum, Real drum_angle) {
+  Real d;
   Vec2 n;
   drum.sdf_world(p, drum_angle, &d, &n);
-  return d < 0.0f ? p - d * n : p;
+  return d < Real(0.0) ? p - d * n : p;
 }
 
 // surface.rs:279-351
-std::vector<std::vector<Vec2>> polygons_at_threshold(const std::vector<float>& field, float threshold,
-                                                     float drum_radius_m, float cell_size, const Drum& drum,
-                                                     float drum_angle) {
+std::vector<std::vector<Vec2>> polygons_at_threshold(const std::vector<Real>& field, Real threshold,
+                                                     Real drum_radius_m, Real cell_size, const Drum& drum,
+                                                     Real drum_angle) {
   Segments segs;
   for (int cj = 0; cj < GRID - 1; ++cj)
     for (int ci = 0; ci < GRID - 1; ++ci) {
@@ -193,19 +193,19 @@ std::vector<std::vector<Vec2>> polygons_at_threshold(const std::vector<float>& f
 }  // namespace
 
 // surface.rs:71-74
-float surface_phi_full(const Fluid& f) {
-  const float splat_radius = SPLAT_RADIUS_FACTOR * f.h;
-  const float number_density = f.rest_density / fmax_r(f.particle_mass, 1e-12f);
-  return number_density * (PI_F * splat_radius * splat_radius / 4.0f);
+Real surface_phi_full(const Fluid& f) {
+  const Real splat_radius = SPLAT_RADIUS_FACTOR * f.h;
+  const Real number_density = f.rest_density / fmax_r(f.particle_mass, Real(1e-12));
+  return number_density * (PI_F * splat_radius * splat_radius / Real(4.0));
 }
 
 // surface.rs:84-131
-std::vector<float> surface_build_field(const Fluid& f, const Drum& drum, float drum_angle) {
-  const float drum_radius_m = drum.radius_m;
-  std::vector<float> field((size_t)GRID * GRID, 0.0f);
-  if (f.len() == 0 || drum_radius_m <= 0.0f) return field;
-  const float splat_radius = SPLAT_RADIUS_FACTOR * f.h;
-  const float cell_size = 2.0f * drum_radius_m / ((float)GRID - 1.0f);
+std::vector<Real> surface_build_field(const Fluid& f, const Drum& drum, Real drum_angle) {
+  const Real drum_radius_m = drum.radius_m;
+  std::vector<Real> field((size_t)GRID * GRID, Real(0.0));
+  if (f.len() == 0 || drum_radius_m <= Real(0.0)) return field;
+  const Real splat_radius = SPLAT_RADIUS_FACTOR * f.h;
+  const Real cell_size = Real(2.0) * drum_radius_m / ((Real)GRID - Real(1.0));
   for (const Vec2& p : f.x) {
     const int gi_min = grid_index(p.x - splat_radius, drum_radius_m, cell_size);
     const int gi_max = grid_index(p.x + splat_radius, drum_radius_m, cell_size);
@@ -220,32 +220,32 @@ std::vector<float> surface_build_field(const Fluid& f, const Drum& drum, float d
   const Vec2 to_local = Vec2::from_angle(-drum_angle);
   for (int gj = 0; gj < GRID; ++gj)
     for (int gi = 0; gi < GRID; ++gi) {
-      float& v = field[(size_t)gj * GRID + gi];
-      if (v == 0.0f) continue;
-      if (drum.sdf(rotate(grid_point(gi, gj, drum_radius_m, cell_size), to_local)) < 0.0f) v = 0.0f;
+      Real& v = field[(size_t)gj * GRID + gi];
+      if (v == Real(0.0)) continue;
+      if (drum.sdf(rotate(grid_point(gi, gj, drum_radius_m, cell_size), to_local)) < Real(0.0)) v = Real(0.0);
     }
   return field;
 }
 
 // surface.rs:233-272 followed by surface.rs:420-430
-std::vector<float> surface_extract_flat(const Fluid& f, const Drum& drum, float drum_angle) {
+std::vector<Real> surface_extract_flat(const Fluid& f, const Drum& drum, Real drum_angle) {
   std::vector<std::vector<Vec2>> polys;
-  const float drum_radius_m = drum.radius_m;
-  if (f.len() != 0 && drum_radius_m > 0.0f) {
-    const std::vector<float> field = surface_build_field(f, drum, drum_angle);
-    const float cell_size = 2.0f * drum_radius_m / ((float)GRID - 1.0f);
+  const Real drum_radius_m = drum.radius_m;
+  if (f.len() != 0 && drum_radius_m > Real(0.0)) {
+    const std::vector<Real> field = surface_build_field(f, drum, drum_angle);
+    const Real cell_size = Real(2.0) * drum_radius_m / ((Real)GRID - Real(1.0));
     polys = polygons_at_threshold(field, THRESHOLD_FRACTION * surface_phi_full(f), drum_radius_m, cell_size, drum,
                                   drum_angle);
     if (polys.empty()) {
-      float peak = 0.0f;
-      for (float v : field) peak = fmax_r(peak, v);
-      if (peak > 0.0f)
+      Real peak = Real(0.0);
+      for (Real v : field) peak = fmax_r(peak, v);
+      if (peak > Real(0.0))
         polys = polygons_at_threshold(field, THRESHOLD_FRACTION * peak, drum_radius_m, cell_size, drum, drum_angle);
     }
   }
-  std::vector<float> out{(float)polys.size()};
+  std::vector<Real> out{(Real)polys.size()};
   for (const auto& poly : polys) {
-    out.push_back((float)poly.size());
+    out.push_back((Real)poly.size());
     for (const Vec2& p : poly) {
       out.push_back(p.x);
       out.push_back(p.y);

@@ -17,6 +17,7 @@ from milldynamics3_b200.sim import Backend  # noqa: E402
 
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_SO = os.path.join(ORACLE_DIR, "liboracle.so")
+ORACLE64_SO = os.path.join(ORACLE_DIR, "liboracle64.so")  # the same restatement in f64
 
 P = C.POINTER
 ORACLE_EXTRA = [
@@ -47,14 +48,21 @@ def build_oracle():
     srcs = [f for f in os.listdir(ORACLE_DIR) if f.endswith((".cpp", ".hpp"))] + ["Makefile"]
     newest = max(os.path.getmtime(os.path.join(ORACLE_DIR, f)) for f in srcs)
     newest = max(newest, os.path.getmtime(os.path.join(ROOT, "include", "millgpu.h")))
-    if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < newest:
-        subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
+    stale = [so for so in (ORACLE_SO, ORACLE64_SO) if not os.path.exists(so) or os.path.getmtime(so) < newest]
+    if stale:
+        subprocess.run(["make", "-s", "-C", ORACLE_DIR, "all"], check=True)
     return ORACLE_SO
 
 
 @pytest.fixture(scope="session")
 def oracle_lib():
     return capi.Lib(build_oracle(), "or_", ORACLE_EXTRA)
+
+
+@pytest.fixture(scope="session")
+def oracle64():
+    build_oracle()
+    return Backend(capi.Lib(ORACLE64_SO, "or_", ORACLE_EXTRA))
 
 
 @pytest.fixture(scope="session")
