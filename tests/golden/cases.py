@@ -18,52 +18,16 @@ overrides, params.rs:62-77 and following) and advanced by Simulation::step / ste
 """
 from __future__ import annotations
 
-import math
-
-import numpy as np
-
-
-def set_path(p, path, value):
-    obj = p
-    parts = path.split(".")
-    for part in parts[:-1]:
-        obj = getattr(obj, part)
-    setattr(obj, parts[-1], value)
+from milldynamics3_b200 import workloads
 
 
 def dem_500(p):
-    from milldynamics3_b200 import capi
-    for k, v in {"slurry.enabled": 0, "mill.diameter_m": 0.45, "mill.speed_mode": capi.SPEED_PERCENT_CRITICAL,
-                 "mill.speed_value": 60.0, "media.fill_fraction": 0.3, "media.ball_diameter_m": 0.01,
-                 "media.density_kg_m3": 7800.0, "media.friction_ball_ball": 0.3, "media.friction_ball_wall": 0.3,
-                 "media.friction_ball_ball_static": 0.3, "media.friction_ball_wall_static": 0.3,
-                 "media.restitution_ball_ball": 0.5, "media.restitution_ball_wall": 0.5}.items():
-        set_path(p, k, v)
-    return p
+    """The DEM-only configuration with 500 discs (the 0.45 m drum)."""
+    return workloads.dem_only_params(p, diameter_m=0.45)
 
 
 def large_res100(p, viscosity):
-    for k, v in {"mill.diameter_m": 0.221, "media.ball_diameter_m": 0.002, "simulation.resolution": 100,
-                 "slurry.viscosity_pa_s": viscosity}.items():
-        set_path(p, k, v)
-    return p
-
-
-def lower_drum_discs(n, drum_radius, ball_radius, seed, top=0.35):
-    """n non-overlapping disc centres drawn uniformly (rejection sampling) in the drum below
-    y = top * R, one radius clear of the wall; float32, shape (n, 2)."""
-    rng = np.random.default_rng(seed)
-    rmax = drum_radius - 1.05 * ball_radius
-    pts = np.zeros((0, 2))
-    min2 = (2.02 * ball_radius) ** 2
-    while len(pts) < n:
-        x, y = rng.uniform(-rmax, rmax), rng.uniform(-rmax, top * rmax)
-        if x * x + y * y > rmax * rmax:
-            continue
-        if len(pts) and (((pts - (x, y)) ** 2).sum(axis=1) < min2).any():
-            continue
-        pts = np.vstack([pts, (x, y)])
-    return pts.astype(np.float32)
+    return workloads.large_params(p, 100, viscosity)
 
 
 # name -> (builder(backend) -> (params, initial balls or None), advance: list of ("frame"|"sub", count))
@@ -71,10 +35,7 @@ def cases():
     def realtime(b):
         return b.preset(b.params_default(), "realtime"), None
 
-    def realtime_300(b):
-        p = b.preset(b.params_default(), "realtime")
-        set_path(p, "media.density_kg_m3", 7800.0)
-        return p, lower_drum_discs(300, 0.0315, 0.001, seed=2024)
+    realtime_300 = workloads.realtime_300
 
     return {
         "realtime_1_substep": (realtime, [("sub", 1)]),
