@@ -191,7 +191,10 @@ typedef struct MgScalars {
  * more to about that many microseconds. test_faults bit 1: the mill's block waits for one more
  * helper block than was launched (a helper that never answers: its wait runs out, the step returns
  * MG_ERR_CUDA); bit 2: the drag sweep never flags ball 0 done (balls that share a fluid particle
- * with it wait until their limit runs out, the step returns MG_ERR_STATE). */
+ * with it wait until their limit runs out, the step returns MG_ERR_STATE).
+ * block_regs: 0 = the register budget follows the block size (128 registers a thread up to 512
+ * threads, 64 above); 64 = the 64-register build at any block size (two 512-thread blocks per
+ * SM, for batches of small mills). */
 typedef struct MgOptions {
   uint32_t cg_fp64;
   uint32_t block_threads;
@@ -200,7 +203,7 @@ typedef struct MgOptions {
   uint32_t mill_blocks;
   uint32_t test_wait_limit_us;
   uint32_t test_faults;
-  uint32_t reserved;
+  uint32_t block_regs;
 } MgOptions;
 
 typedef struct MgSim MgSim;

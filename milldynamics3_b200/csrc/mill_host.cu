@@ -12,6 +12,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "mill_kernels.h"
@@ -436,7 +437,7 @@ int run(MgSim* s, uint32_t n_sub) {
   if (mill_blocks > 1) CK(cudaMemsetAsync(s->md.wide, 0, sizeof(WideCtl), s->stream));
   CK(cudaEventRecord(s->ev0, s->stream));
   CK(launch_substeps(s->d_md, 1, s->d_uni, s->d_ang, n_sub, nullptr, s->opt.block_threads, s->md.smem_bytes,
-                     s->stream, mill_blocks));
+                     s->stream, mill_blocks, nullptr, s->opt.block_regs == 64));
   CK(cudaEventRecord(s->ev1, s->stream));
   CK(cudaMemcpyAsync(s->h_out, s->md.out, sizeof(StepOut) * n_sub, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
@@ -772,6 +773,7 @@ int mg_sim_set_options(MgSim* s, const MgOptions* o) {
     return fail(s, MG_ERR_ARG, "mill_blocks must be in [0, %u] for this handle", s->mill_blocks_cap);
   if (o->test_wait_limit_us > 10000000u) return fail(s, MG_ERR_ARG, "test_wait_limit_us must be at most 10000000");
   if (o->test_faults & ~3u) return fail(s, MG_ERR_ARG, "test_faults: only bits 1 and 2 are defined");
+  if (o->block_regs != 0 && o->block_regs != 64) return fail(s, MG_ERR_ARG, "block_regs must be 0 or 64");
   s->opt = *o;
   return MG_OK;
 }
@@ -1347,6 +1349,12 @@ struct MgBatch {
   uint2* h_table = nullptr;
   size_t smem = 0;
   uint32_t threads = 0;
+  bool regs64 = false;
+  // blocks run the mills longest first (block k -> mill order[k]): the cost of a mill is its
+  // device cycles in the last frame (an estimate from its sizes before the first one)
+  std::vector<uint32_t> order;
+  std::vector<double> cost;
+  uint32_t* d_order = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_kernel_ms = 0.0f;
   uint64_t launches = 0;
@@ -1373,6 +1381,36 @@ int bfail(MgBatch* b, int code, const char* fmt, ...) {
 
 // Uploads the descriptors and mill-uniform blocks of every mill (at creation and after options
 // change).
+// Runs f(i) for i in [0, n) on up to 16 host threads (each i once; the calls must be
+// independent).
+template <class F>
+void parallel_for(uint32_t n, F f) {
+  const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const uint32_t t = std::min<uint32_t>({16u, hw, (n + 31u) / 32u});
+  if (t <= 1) {
+    for (uint32_t i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (uint32_t w = 0; w < t; ++w)
+    pool.emplace_back([&, w]() {
+      for (uint32_t i = w; i < n; i += t) f(i);
+    });
+  for (std::thread& th : pool) th.join();
+}
+
+// The mills' block order, longest first; uploaded when it changed.
+int batch_order(MgBatch* b) {
+  const uint32_t n = (uint32_t)b->mills.size();
+  std::vector<uint32_t> order(n);
+  for (uint32_t i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return b->cost[x] > b->cost[y]; });
+  if (order == b->order) return MG_OK;
+  b->order = order;
+  BCK(cudaMemcpyAsync(b->d_order, b->order.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, b->stream));
+  return MG_OK;
+}
+
 int batch_upload(MgBatch* b) {
   const uint32_t n = (uint32_t)b->mills.size();
   std::vector<MillDev> md(n);
@@ -1433,7 +1471,14 @@ int mg_batch_create(const MgParams* params, uint32_t n_mills, MgBatch** out) {
     BCK(cudaMallocHost(&b->h_table, sizeof(uint2) * n_mills));
     BCK(cudaEventCreate(&b->ev0));
     BCK(cudaEventCreate(&b->ev1));
+    BCK(cudaMalloc(&b->d_order, sizeof(uint32_t) * n_mills));
     BCK(cudaMemcpyAsync(b->d_nsub, b->n_sub.data(), sizeof(uint32_t) * n_mills, cudaMemcpyHostToDevice, b->stream));
+    // before the first frame: sub-steps times particles, balls weighted for their sweeps
+    b->cost.resize(n_mills);
+    for (uint32_t i = 0; i < n_mills; ++i)
+      b->cost[i] = (double)b->n_sub[i] * ((double)b->mills[i]->nf + 4.0 * (double)b->mills[i]->nb);
+    int orc = batch_order(b);
+    if (orc) return orc;
     return batch_upload(b);
   };
   if (!rc) rc = setup();
@@ -1463,6 +1508,7 @@ void mg_batch_destroy(MgBatch* b) {
   if (b->d_cursor) cudaFree(b->d_cursor);
   if (b->d_table) cudaFree(b->d_table);
   if (b->h_table) cudaFreeHost(b->h_table);
+  if (b->d_order) cudaFree(b->d_order);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -1480,6 +1526,7 @@ int mg_batch_set_options(MgBatch* b, const MgOptions* opt) {
     if (rc) return bfail(b, rc, "%s", s->err.c_str());
   }
   b->threads = opt->block_threads;
+  b->regs64 = opt->block_regs == 64;
   return batch_upload(b);
 }
 
@@ -1521,7 +1568,10 @@ int mg_batch_step_frames(MgBatch* b, uint32_t frames, float frame_dt) {
     }
     BCK(cudaMemcpyAsync(b->d_ang, b->h_ang, sizeof(SubAngles) * n * b->stride, cudaMemcpyHostToDevice, b->stream));
     BCK(cudaEventRecord(b->ev0, b->stream));
-    BCK(launch_substeps(b->d_md, n, b->d_uni, b->d_ang, b->stride, b->d_nsub, b->threads, b->smem, b->stream));
+    int orc = batch_order(b);
+    if (orc) return orc;
+    BCK(launch_substeps(b->d_md, n, b->d_uni, b->d_ang, b->stride, b->d_nsub, b->threads, b->smem, b->stream, 1,
+                        b->d_order, b->regs64));
     BCK(cudaEventRecord(b->ev1, b->stream));
     BCK(cudaMemsetAsync(b->d_cursor, 0, sizeof(uint32_t), b->stream));
     BCK(launch_pack_impacts(b->d_md, n, b->d_nsub, b->d_packed, b->packed_cap, b->d_cursor, b->d_table, b->stream));
@@ -1538,12 +1588,21 @@ int mg_batch_step_frames(MgBatch* b, uint32_t frames, float frame_dt) {
                           b->stream));
     BCK(cudaStreamSynchronize(b->stream));
     for (uint32_t i = 0; i < n; ++i) {
+      const StepOut* o = b->h_out + (size_t)i * b->stride;
+      uint32_t e = 0;
+      for (uint32_t k = 0; k < b->n_sub[i]; ++k) e |= o[k].err;
+      if (e) return bfail(b, MG_ERR_CAPACITY, "mill %u: device capacity exceeded (error bits 0x%x)", i, e);
+    }
+    // the mills' host folds (EMA, energy budget, stress accumulator) are independent of one
+    // another: they run on several host threads
+    parallel_for(n, [&](uint32_t i) {
       MgSim* s = b->mills[i];
       const uint32_t ns = b->n_sub[i];
       const StepOut* o = b->h_out + (size_t)i * b->stride;
-      uint32_t e = 0;
-      for (uint32_t k = 0; k < ns; ++k) e |= o[k].err;
-      if (e) return bfail(b, MG_ERR_CAPACITY, "mill %u: device capacity exceeded (error bits 0x%x)", i, e);
+      double cyc = 0.0;
+      for (uint32_t k = 0; k < ns; ++k)
+        for (int q = 0; q <= 14; ++q) cyc += (double)o[k].stage[q];
+      b->cost[i] = cyc;
       std::memcpy(s->h_out, o, sizeof(StepOut) * ns);
       const MgImpactRecord* rec = b->h_packed + b->h_table[i].x;
       for (uint32_t k = 0; k < ns; ++k) {
@@ -1564,7 +1623,7 @@ int mg_batch_step_frames(MgBatch* b, uint32_t frames, float frame_dt) {
       s->last_dem = o[ns - 1].ds;
       s->last_ctr = o[ns - 1].ctr;
       s->launches += 1;
-    }
+    });
   }
   return MG_OK;
 }
@@ -1626,6 +1685,7 @@ struct MgServerJob {
   uint64_t sweep = 0;
   uint32_t sweep_index = 0;
   SeedAcc* acc = nullptr;
+  double cost = -1.0;  // device cycles of the job's last frame (its block order in the launch)
 };
 
 // A seed-sweep job: one server job per seed, combined when all have finished.
@@ -1652,6 +1712,7 @@ struct MgServer {
   uint32_t *d_nsub = nullptr, *h_nsub = nullptr;
   StepOut *d_out = nullptr, *h_out = nullptr;
   uint2 *d_table = nullptr, *h_table = nullptr;
+  uint32_t *d_order = nullptr, *h_order = nullptr;  // block k runs job h_order[k] (longest first)
   uint32_t* d_cursor = nullptr;
   MgImpactRecord *d_packed = nullptr, *h_packed = nullptr;
   uint64_t packed_cap = 0;
@@ -1688,6 +1749,8 @@ void server_free_blocks(MgServer* v) {
   cudaFree(v->d_nsub); cudaFreeHost(v->h_nsub);
   cudaFree(v->d_out); cudaFreeHost(v->h_out);
   cudaFree(v->d_table); cudaFreeHost(v->h_table);
+  cudaFree(v->d_order); cudaFreeHost(v->h_order);
+  v->d_order = v->h_order = nullptr;
   v->d_md = v->h_md = nullptr;
   v->d_uni = v->h_uni = nullptr;
   v->d_ang = v->h_ang = nullptr;
@@ -1714,6 +1777,8 @@ int server_reserve(MgServer* v, uint32_t n, uint64_t packed) {
     SCK(cudaMallocHost(&v->h_out, sizeof(StepOut) * c * MAX_SUB));
     SCK(cudaMalloc(&v->d_table, sizeof(uint2) * c));
     SCK(cudaMallocHost(&v->h_table, sizeof(uint2) * c));
+    SCK(cudaMalloc(&v->d_order, sizeof(uint32_t) * c));
+    SCK(cudaMallocHost(&v->h_order, sizeof(uint32_t) * c));
     v->cap = c;
   }
   if (packed > v->packed_cap) {
@@ -2052,8 +2117,19 @@ int mg_server_step(MgServer* v) {
   SCK(cudaMemcpyAsync(v->d_uni, v->h_uni, sizeof(StepUniform) * n, cudaMemcpyHostToDevice, v->stream));
   SCK(cudaMemcpyAsync(v->d_ang, v->h_ang, sizeof(SubAngles) * n * stride, cudaMemcpyHostToDevice, v->stream));
   SCK(cudaMemcpyAsync(v->d_nsub, v->h_nsub, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, v->stream));
+  // blocks run the jobs longest first (the last frame's device cycles; before their first frame,
+  // sub-steps times particles)
+  for (uint32_t k = 0; k < n; ++k) {
+    MgServerJob* j = v->active[k];
+    if (j->cost < 0.0) j->cost = (double)j->n_sub * ((double)j->sim->nf + 4.0 * (double)j->sim->nb);
+    v->h_order[k] = k;
+  }
+  std::stable_sort(v->h_order, v->h_order + n,
+                   [&](uint32_t x, uint32_t y) { return v->active[x]->cost > v->active[y]->cost; });
+  SCK(cudaMemcpyAsync(v->d_order, v->h_order, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, v->stream));
   SCK(cudaEventRecord(v->ev0, v->stream));
-  SCK(launch_substeps(v->d_md, n, v->d_uni, v->d_ang, stride, v->d_nsub, v->cfg.block_threads, smem, v->stream));
+  SCK(launch_substeps(v->d_md, n, v->d_uni, v->d_ang, stride, v->d_nsub, v->cfg.block_threads, smem, v->stream, 1,
+                      v->d_order));
   SCK(cudaEventRecord(v->ev1, v->stream));
   SCK(cudaMemsetAsync(v->d_cursor, 0, sizeof(uint32_t), v->stream));
   SCK(launch_pack_impacts(v->d_md, n, v->d_nsub, v->d_packed, (uint32_t)std::min<uint64_t>(v->packed_cap, 0xFFFFFFF0ull),
@@ -2070,19 +2146,24 @@ int mg_server_step(MgServer* v) {
   SCK(cudaStreamSynchronize(v->stream));
   v->frames += 1;
   const double t_end = wall_s();
-  std::vector<MgServerJob*> keep;
-  keep.reserve(n);
-  for (uint32_t k = 0; k < n; ++k) {
+  std::vector<uint32_t> failed(n, 0u);
+  // the jobs' host folds are independent of one another: several host threads
+  parallel_for(n, [&](uint32_t k) {
     MgServerJob* j = v->active[k];
     MgSim* s = j->sim;
     const uint32_t ns = j->n_sub;
     const StepOut* o = v->h_out + (size_t)k * stride;
     uint32_t e = 0;
-    for (uint32_t t = 0; t < ns; ++t) e |= o[t].err;
-    if (e) {
-      retire(v, j, MG_JOB_FAILED);
-      continue;
+    double cyc = 0.0;
+    for (uint32_t t = 0; t < ns; ++t) {
+      e |= o[t].err;
+      for (int q = 0; q <= 14; ++q) cyc += (double)o[t].stage[q];
     }
+    if (e) {
+      failed[k] = 1u;
+      return;
+    }
+    j->cost = cyc;
     std::memcpy(s->h_out, o, sizeof(StepOut) * ns);
     const MgImpactRecord* rec = v->h_packed + v->h_table[k].x;
     for (uint32_t t = 0; t < ns; ++t) {
@@ -2099,6 +2180,16 @@ int mg_server_step(MgServer* v) {
     s->last_dem = o[ns - 1].ds;
     s->last_ctr = o[ns - 1].ctr;
     s->launches += 1;
+  });
+  std::vector<MgServerJob*> keep;
+  keep.reserve(n);
+  for (uint32_t k = 0; k < n; ++k) {
+    MgServerJob* j = v->active[k];
+    if (failed[k]) {
+      retire(v, j, MG_JOB_FAILED);
+      continue;
+    }
+    MgSim* s = j->sim;
     j->frames_done += 1;
     if (j->acc) seed_acc_observe(j->acc, s, j->frames_done);
     if (j->t_first < 0.0) j->t_first = t_end;

@@ -42,12 +42,13 @@ __global__ void __launch_bounds__(512) probe_kernel(const MillDev* __restrict__ 
 
 cudaError_t launch_substeps(const MillDev* mills, uint32_t n_mills, StepUniform* uni, const SubAngles* angles,
                             uint32_t n_sub, const uint32_t* n_sub_of, uint32_t threads, size_t smem_bytes,
-                            cudaStream_t stream, uint32_t mill_blocks) {
+                            cudaStream_t stream, uint32_t mill_blocks, const uint32_t* block_mill, bool regs64) {
   if (threads == 0 || threads > MAX_BLOCK_THREADS) threads = DEFAULT_BLOCK_THREADS;
-  if (threads > 512)
+  if (threads > 512 || regs64)
     return launch_substeps_1024(mills, n_mills, uni, angles, n_sub, n_sub_of, threads, smem_bytes, stream,
-                                mill_blocks);
-  return launch_substeps_512(mills, n_mills, uni, angles, n_sub, n_sub_of, threads, smem_bytes, stream, mill_blocks);
+                                mill_blocks, block_mill);
+  return launch_substeps_512(mills, n_mills, uni, angles, n_sub, n_sub_of, threads, smem_bytes, stream, mill_blocks,
+                             block_mill);
 }
 
 // One block per mill: appends the mill's impact records (sub-step order) to the packed buffer.

@@ -11,17 +11,21 @@ namespace mg {
 // cleared at the start of the launch. smem_bytes of dynamic shared memory must be at least every
 // mill's MillDev::smem_bytes. With n_mills == 1 and mill_blocks > 1, the mill's per-ball stages
 // are shared with mill_blocks - 1 helper blocks (a cooperative launch; the mill's control block
-// must be zeroed before the launch and its slot maps sized for all the blocks' warps).
+// must be zeroed before the launch and its slot maps sized for all the blocks' warps). Without
+// helpers, block b runs mill block_mill[b] when block_mill is given. The instantiation: blocks of
+// more than 512 threads, or any block size with regs64, run the 64-register build (two 512-thread
+// blocks fit one SM); otherwise the 128-register build of up to 512 threads.
 cudaError_t launch_substeps(const MillDev* mills, uint32_t n_mills, StepUniform* uni, const SubAngles* angles,
                             uint32_t n_sub, const uint32_t* n_sub_of, uint32_t threads, size_t smem_bytes,
-                            cudaStream_t stream, uint32_t mill_blocks = 1);
+                            cudaStream_t stream, uint32_t mill_blocks = 1, const uint32_t* block_mill = nullptr,
+                            bool regs64 = false);
 // The two instantiations behind launch_substeps (blocks of up to 512 and up to 1024 threads).
 cudaError_t launch_substeps_512(const MillDev* mills, uint32_t n_mills, StepUniform* uni, const SubAngles* angles,
                                 uint32_t n_sub, const uint32_t* n_sub_of, uint32_t threads, size_t smem_bytes,
-                                cudaStream_t stream, uint32_t mill_blocks);
+                                cudaStream_t stream, uint32_t mill_blocks, const uint32_t* block_mill);
 cudaError_t launch_substeps_1024(const MillDev* mills, uint32_t n_mills, StepUniform* uni, const SubAngles* angles,
                                  uint32_t n_sub, const uint32_t* n_sub_of, uint32_t threads, size_t smem_bytes,
-                                 cudaStream_t stream, uint32_t mill_blocks);
+                                 cudaStream_t stream, uint32_t mill_blocks, const uint32_t* block_mill);
 // Packs the impact records of n_mills mills after a launch: mill b's records of its sub-steps
 // 0..n_sub_of[b]-1 (StepOut::n_impacts each, at most cap_impacts) are appended in sub-step order
 // at an offset taken from *cursor (one atomic per mill); table[b] = {offset, count}. Records that

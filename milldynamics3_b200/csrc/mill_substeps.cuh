@@ -14,19 +14,22 @@ namespace mg {
 // 512 threads per block (128 registers a thread) and up to 1024 (64 registers, more warps for the
 // per-ball stages); the results do not depend on the block size. With helpers > 0 the launch runs
 // one mill: block 0 is the mill's block and blocks 1..helpers take shares of its per-ball stages
-// (mill_wide.cuh); the results do not depend on the number of blocks either.
+// (mill_wide.cuh); the results do not depend on the number of blocks either. Without helpers,
+// block b runs mill block_mill[b] when block_mill is given (an order of the mills, e.g. longest
+// first, so that the last wave of blocks holds the short mills), else mill b.
 template <int MAX_THREADS>
 __global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDev* __restrict__ mills,
                                                                     StepUniform* uni,
                                                                     const SubAngles* __restrict__ angles,
                                                                     uint32_t n_sub,
                                                                     const uint32_t* __restrict__ n_sub_of,
+                                                                    const uint32_t* __restrict__ block_mill,
                                                                     uint32_t helpers) {
   __shared__ MillDev m;
   __shared__ FluidShared fs;
   __shared__ DemShared ds;
   extern __shared__ __align__(16) unsigned char dsm[];  // staged ball state (24 bytes per ball)
-  const uint32_t mill = helpers ? 0u : blockIdx.x;
+  const uint32_t mill = helpers ? 0u : (block_mill ? block_mill[blockIdx.x] : blockIdx.x);
   if (threadIdx.x == 0) {
     m = mills[mill];
     m.helpers = helpers;
@@ -88,7 +91,7 @@ __global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDe
 template <int MAX_THREADS>
 cudaError_t launch_substeps_impl(const MillDev* mills, uint32_t n_mills, StepUniform* uni, const SubAngles* angles,
                                  uint32_t n_sub, const uint32_t* n_sub_of, uint32_t threads, size_t smem_bytes,
-                                 cudaStream_t stream, uint32_t mill_blocks) {
+                                 cudaStream_t stream, uint32_t mill_blocks, const uint32_t* block_mill) {
   auto kernel = mill_substeps_kernel<MAX_THREADS>;
   // (the opt-in is needed whenever static plus dynamic shared memory passes 48 KB)
   if (smem_bytes > 0) {
@@ -98,13 +101,15 @@ cudaError_t launch_substeps_impl(const MillDev* mills, uint32_t n_mills, StepUni
   uint32_t helpers = n_mills == 1 && mill_blocks > 1 ? min(mill_blocks, MAX_MILL_BLOCKS) - 1u : 0u;
   if (helpers) {
     // all of the mill's blocks wait for one another, so they must be resident together
-    void* args[] = {(void*)&mills, (void*)&uni, (void*)&angles, (void*)&n_sub, (void*)&n_sub_of, (void*)&helpers};
+    const uint32_t* no_order = nullptr;
+    void* args[] = {(void*)&mills,    (void*)&uni,      (void*)&angles, (void*)&n_sub,
+                    (void*)&n_sub_of, (void*)&no_order, (void*)&helpers};
     cudaError_t e = cudaLaunchCooperativeKernel((const void*)kernel, dim3(1u + helpers), dim3(threads), args,
                                                 smem_bytes, stream);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
   }
-  kernel<<<n_mills, threads, smem_bytes, stream>>>(mills, uni, angles, n_sub, n_sub_of, 0u);
+  kernel<<<n_mills, threads, smem_bytes, stream>>>(mills, uni, angles, n_sub, n_sub_of, block_mill, 0u);
   return cudaGetLastError();
 }
 

@@ -18,10 +18,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE64_SO = os.path.join(ROOT, "oracle", "liboracle64.so")
 
 
-def oracle64_backend():
-    """The FP64 oracle behind the same C API as the parity oracle."""
+def oracle64_backend(build=True):
+    """The FP64 oracle behind the same C API as the parity oracle (built first unless `build` is
+    false: the pool's worker processes only load what the parent built)."""
     from conftest import ORACLE_EXTRA, build_oracle
-    build_oracle()
+    if build:
+        build_oracle()
     return Backend(capi.Lib(ORACLE64_SO, "or_", ORACLE_EXTRA))
 
 
@@ -158,7 +160,7 @@ def _fp64_job(job, f64=None):
     """One FP64-oracle run (picklable for a process pool): params bytes, the f32 initial state."""
     pbytes, (bl, bm, fl, fm), settle_s, measure_s = job
     if f64 is None:
-        f64 = oracle64_backend()
+        f64 = oracle64_backend(build=False)
     p = capi.Params.from_buffer_copy(pbytes)
     s = Simulation(f64, p)
     s.set_balls(bl["x"], bl["v"], bl["theta"], bl["omega"])
