@@ -168,6 +168,9 @@ struct StepUniform {
   uint32_t want_momentum;  // accumulate CouplingImpulses::fluid_momentum_change (coupling.rs:49-51)
   uint32_t sweep_warps;    // warps taking balls in the per-ball sweeps
   uint32_t spin_ns;        // poll interval of a waiting ball
+  double now_s;            // the sub-step's SubAngles::now_s and alpha (the stress fold)
+  float alpha;
+  uint32_t fold_stress;    // 1: fold each sub-step's impacts into the stress accumulator (Simulation::step)
   uint32_t spin_limit;     // polls after which a waiting ball gives up (ERR_BUDGET)
   uint32_t skip_done_ball; // tests only: the drag sweep never flags this ball done (NONE: none)
 };
@@ -177,6 +180,17 @@ struct StepUniform {
 struct SubAngles {
   float drum_angle, drum_angle_next, dt, pad;
   V2 to_local_next, to_world_next, to_local0;
+  double now_s;  // Simulation::sim_time when the sub-step's impacts are folded (stress.rs now_s)
+  float alpha;   // its EMA weight, 1 - exp(-dt / 1 s) in f32 (lib.rs:516-537)
+  float pad2;
+};
+
+// stress.rs:80-99 StressAccum without its debounce map (which is the hash table below): the EMA
+// rates, the cumulative sums and the update count, in f64 as the reference keeps them.
+struct StressState {
+  double count_rate[4], se_hat_rate[4], hist_rate[MG_SE_BINS], above_rate_j[6];
+  double cum_wall_j, cum_above_j[6];
+  unsigned long long updates;
 };
 
 // ---------------------------------------------------------------- per-sub-step outputs
@@ -206,6 +220,7 @@ enum : uint32_t {
   ERR_IMPACTS = 1u << 7,
   ERR_BUDGET = 1u << 8,
   ERR_WIDE = 1u << 9,  // a mill's helper blocks and its own block stopped waiting for each other
+  ERR_STRESS = 1u << 10,  // the impact debounce table had no free slot
 };
 
 // ---------------------------------------------------------------- a spatial grid's buffers
@@ -314,6 +329,14 @@ struct MillDev {
   MgImpactRecord* act_rec;
   uint32_t smem_balls;  // balls whose state fits the launch's dynamic shared memory (0: global)
   uint32_t smem_bytes;  // the launch's dynamic shared memory (staged ball state, then sweep scratch)
+  // the impact-energy accumulator (stress.rs:110-171) on the device: its state, the debounce
+  // table (keys (ball, partner) with (0, 0) free, the time each was last counted; st_cap a power
+  // of two) and, when set, where the launch leaves a copy of the state for the host
+  StressState* stress;
+  uint2* st_key;
+  double* st_time;
+  uint32_t st_cap;
+  StressState* stress_copy;
   uint32_t helpers;     // helper blocks of this launch (set by the kernel; 0 in batches)
   uint32_t test_extra_helpers;  // tests only: helper blocks the mill's block waits for but were not launched
   long long wide_wait_cycles;   // the mill block's bound on a wait for its helper blocks (clock cycles)

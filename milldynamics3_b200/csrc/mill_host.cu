@@ -17,6 +17,7 @@
 
 #include "mill_kernels.h"
 #include "mill_params.h"
+#include "mill_stress.cuh"
 
 using namespace mg;
 
@@ -34,64 +35,12 @@ int fail_global(int code, const char* fmt, ...) {
   return code;
 }
 
-// ------------------------------------------------------------------ stress.rs:28-171 on the host
-struct Stress {
-  double count_rate[4] = {}, se_hat_rate[4] = {}, hist_rate[MG_SE_BINS] = {}, above_rate_j[6] = {};
-  double cum_wall_j = 0.0, cum_above_j[6] = {};
-  std::map<std::pair<uint32_t, uint32_t>, double> last_counted;
-  bool has_factor = false;
-  double factor = 0.25;
-  uint64_t updates = 0;
-
-  static int se_bin(double e_hat) {
-    if (std::isnan(e_hat) || e_hat <= 0.0) return 0;
-    double t = (std::log10(e_hat) + 3.0) * 4.0;
-    if (!(t > 0.0)) t = 0.0;
-    if (t >= 27.0) return 27;
-    return (int)t;
-  }
-  void update(const MgImpactRecord* recs, uint32_t n, double m3, double scale_j, double d, double now_s,
-              double sub_dt, double alpha, double wall_work_j) {
-    static const double THR[6] = {0.03, 0.1, 0.3, 1.0, 3.0, 10.0};
-    double window = (has_factor ? factor : 0.25) * std::sqrt(d / 9.81);
-    updates += 1;
-    if (updates % 4096 == 0) {
-      for (auto it = last_counted.begin(); it != last_counted.end();) {
-        if (!(now_s - it->second < 4.0 * window)) it = last_counted.erase(it);
-        else ++it;
-      }
-    }
-    double count[4] = {}, se_hat[4] = {}, hist[MG_SE_BINS] = {}, above[6] = {};
-    for (uint32_t k = 0; k < n; ++k) {
-      const MgImpactRecord& r = recs[k];
-      if (window > 0.0) {
-        std::pair<uint32_t, uint32_t> key = {std::min(r.ball, r.partner), std::max(r.ball, r.partner)};
-        if (r.partner == MG_WALL_PARTNER) key = {r.ball, MG_WALL_PARTNER};
-        auto it = last_counted.find(key);
-        if (it != last_counted.end() && now_s - it->second < window) continue;
-        last_counted[key] = now_s;
-      }
-      bool bb = r.kind == MG_IMPACT_BALL_BALL;
-      double vn = r.normal_speed, vs = r.slip_speed;
-      int cls = bb ? (vs > vn ? 1 : 0) : (vs > vn ? 3 : 2);
-      double m_red = bb ? 0.5 * m3 : m3;
-      double se = 0.5 * m_red * (vn * vn + vs * vs);
-      double e_hat = se / scale_j;
-      count[cls] += 1.0;
-      se_hat[cls] += e_hat;
-      hist[se_bin(e_hat)] += 1.0;
-      for (int q = 0; q < 6; ++q)
-        if (e_hat >= THR[q]) above[q] += se;
-    }
-    cum_wall_j += wall_work_j;
-    for (int q = 0; q < 6; ++q) cum_above_j[q] += above[q];
-    auto ema = [&](double* s, double inst) { *s += alpha * (inst / sub_dt - *s); };
-    for (int c = 0; c < 4; ++c) { ema(&count_rate[c], count[c]); ema(&se_hat_rate[c], se_hat[c]); }
-    for (int b = 0; b < MG_SE_BINS; ++b) ema(&hist_rate[b], hist[b]);
-    for (int q = 0; q < 6; ++q) ema(&above_rate_j[q], above[q]);
-  }
-  double total_rate() const { return count_rate[0] + count_rate[1] + count_rate[2] + count_rate[3]; }
-};
+// ------------------------------------------------------------------ stress.rs:28-171
+// The accumulator itself runs on the device (mill_stress.cuh, folded after every sub-step of
+// Simulation::step); the handle keeps a copy of its state, refreshed after every launch.
+double stress_total_rate(const StressState& st) {
+  return st.count_rate[0] + st.count_rate[1] + st.count_rate[2] + st.count_rate[3];
+}
 
 // ------------------------------------------------------------------ device arena
 struct Arena {
@@ -124,7 +73,7 @@ struct MgSim {
   MgStepCounters last_ctr{};
   MgEnergyBudget budget{};
   double e0 = 0.0;
-  Stress stress;
+  StressState stress{};  // the device accumulator's state after the last launch
   // device state
   cudaStream_t stream = nullptr;
   // a light handle (a request-server job): it borrows the server's stream, takes its arena from
@@ -193,7 +142,16 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
     s->md.nb = nb;
     return MG_OK;
   }
+  // the stress accumulator's debounce table survives a new arena: its live keys are carried over
+  std::vector<uint2> old_keys;
+  std::vector<double> old_times;
   if (s->dmem) {
+    old_keys.resize(s->md.st_cap);
+    old_times.resize(s->md.st_cap);
+    CK(cudaMemcpyAsync(old_keys.data(), s->md.st_key, sizeof(uint2) * s->md.st_cap, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(old_times.data(), s->md.st_time, sizeof(double) * s->md.st_cap, cudaMemcpyDeviceToHost,
+                       s->stream));
+    CK(cudaStreamSynchronize(s->stream));
     if (s->light) cudaFreeAsync(s->dmem, s->stream);
     else cudaFree(s->dmem);
     s->dmem = nullptr;
@@ -210,6 +168,9 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
   m.cap_links = cb * std::min<uint32_t>(cb + 1u, 512u) + 1024u;
   m.cap_recs = std::max({8u * cf + 1024u, m.cap_groups, m.cap_links, 2u * m.cap_pairs + cb + 64u});
   m.cap_impacts = 4u * cb + 256u;
+  // debounce table: eight slots per impact record a sub-step can hold, a power of two
+  m.st_cap = 1u;
+  while (m.st_cap < 8u * m.cap_impacts) m.st_cap <<= 1;
   const uint32_t fcells = 2u * cf + 513u, bcells = 2u * cb + 513u;
   const uint32_t nbig = std::max(cf, cb) + 2u;
   // pass 1: measure, pass 2: carve
@@ -218,6 +179,9 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
     a.base = pass ? (char*)s->dmem : nullptr;
     m.guess_valid_dev = a.take<uint32_t>(1);
     m.err = a.take<uint32_t>(1);
+    m.stress = a.take<StressState>(1);
+    m.st_key = a.take<uint2>(m.st_cap);
+    m.st_time = a.take<double>(m.st_cap);
     m.fx = a.take<float2>(cf); m.fv = a.take<float2>(cf); m.fguess = a.take<float2>(cf); m.fdye = a.take<float>(cf);
     m.bx = a.take<float2>(cb); m.bv = a.take<float2>(cb); m.bth = a.take<float>(cb); m.bom = a.take<float>(cb);
     m.imp = a.take<float2>(cb); m.ang = a.take<float>(cb);
@@ -293,6 +257,22 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
   }
   // the merge slot maps are kept all-NONE between uses
   cudaMemsetAsync(m.slot, 0xFF, sizeof(uint32_t) * (size_t)MAX_BLOCK_WARPS * s->mill_blocks_cap * cf, s->stream);
+  // the stress accumulator: its state as the handle last saw it, its table re-filled
+  CK(cudaMemcpyAsync(m.stress, &s->stress, sizeof(StressState), cudaMemcpyHostToDevice, s->stream));
+  if (!old_keys.empty()) {
+    std::vector<uint2> keys(m.st_cap, make_uint2(0u, 0u));
+    std::vector<double> times(m.st_cap, 0.0);
+    const uint32_t mask = m.st_cap - 1u;
+    for (size_t q = 0; q < old_keys.size(); ++q) {
+      const uint2 k = old_keys[q];
+      if (k.x == 0u && k.y == 0u) continue;
+      uint32_t slot = stress_slot(k, mask);
+      for (uint32_t probe = 0; probe < m.st_cap; ++probe, slot = (slot + 1u) & mask)
+        if (keys[slot].x == 0u && keys[slot].y == 0u) { keys[slot] = k; times[slot] = old_times[q]; break; }
+    }
+    CK(cudaMemcpyAsync(m.st_key, keys.data(), sizeof(uint2) * m.st_cap, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(m.st_time, times.data(), sizeof(double) * m.st_cap, cudaMemcpyHostToDevice, s->stream));
+  }
   // the clears must land before anything else touches the arena, whichever stream it uses
   CK(cudaStreamSynchronize(s->stream));
   m.nf = nf;
@@ -413,11 +393,16 @@ int fill_uniform(MgSim* s, const MgDrum& drum, const MgMediaParams& media, const
   return MG_OK;
 }
 
-void fill_angle(SubAngles& A, float angle, float omega, float dt) {
+// now_s: Simulation::sim_time when the sub-step's impacts are folded (the stress accumulator's
+// clock); alpha: the sub-step's EMA weight 1 - exp(-dt / 1 s) in f32 (lib.rs:516-537).
+void fill_angle(SubAngles& A, float angle, float omega, float dt, double now_s = 0.0) {
   A.drum_angle = angle;
   A.drum_angle_next = angle + omega * dt;
   A.dt = dt;
   A.pad = 0.0f;
+  A.now_s = now_s;
+  A.alpha = 1.0f - mgh::expf_r(-dt / 1.0f);
+  A.pad2 = 0.0f;
   float an = A.drum_angle_next;
   A.to_local_next = V2(mgh::cosf_r(-an), mgh::sinf_r(-an));
   A.to_world_next = V2(mgh::cosf_r(an), mgh::sinf_r(an));
@@ -440,6 +425,7 @@ int run(MgSim* s, uint32_t n_sub) {
                      s->stream, mill_blocks, nullptr, s->opt.block_regs == 64));
   CK(cudaEventRecord(s->ev1, s->stream));
   CK(cudaMemcpyAsync(s->h_out, s->md.out, sizeof(StepOut) * n_sub, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(&s->stress, s->md.stress, sizeof(StressState), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   CK(cudaEventElapsedTime(&s->last_kernel_ms, s->ev0, s->ev1));
   s->launches += 1;
@@ -503,14 +489,9 @@ void fold_substep(MgSim* s, uint32_t k, float sub_dt, float omega) {
   s->power += alpha * (p_inst - s->power);
   float t_inst = std::fabs(omega) > 1e-6f ? p_inst / omega : 0.0f;
   s->torque += alpha * (t_inst - s->torque);
-  double r = (double)s->bmat.radius;
-  double m3 = (double)s->bmat.mass * 4.0 / 3.0 * r;
-  double d = 2.0 * r;
-  double scale_j = m3 * 9.81 * d;
-  uint32_t ni = std::min(s->h_out[k].n_impacts, s->md.cap_impacts);
-  s->stress.update(s->h_imp + (size_t)k * s->md.cap_impacts, ni, m3, scale_j, d, s->sim_time, (double)sub_dt,
-                   (double)alpha, (double)(ds.wall_work_j + fs.wall_work_j));
-  s->collision_rate = (float)s->stress.total_rate();
+  // the stress accumulator folded this sub-step's impacts on the device; s->stress holds its
+  // state after the launch's last sub-step, which is what the frame reports
+  s->collision_rate = (float)stress_total_rate(s->stress);
   float diss = mgh::fmax_r(ds.dissipated_energy_j, 0.0f) / sub_dt;
   s->dissipated_power += alpha * (diss - s->dissipated_power);
   s->max_disp = mgh::fmax_r(s->max_disp, ds.max_substep_displacement_over_diameter);
@@ -525,13 +506,16 @@ int advance(MgSim* s, uint32_t n, float sub_dt) {
   const MgSimulationParams& q = s->params.simulation;
   int rc = fill_uniform(s, drum, s->params.media, s->params.slurry, q.pbf_iterations, q.dem_iterations, 1, 1, 1);
   if (rc) return rc;
+  s->h_uni->fold_stress = 1u;
   uint32_t done = 0;
   while (done < n) {
     uint32_t chunk = std::min(n - done, MAX_SUB);
     float angle = s->drum_angle;
+    double now = s->sim_time;
     for (uint32_t k = 0; k < chunk; ++k) {
-      fill_angle(s->h_ang[k], angle, omega, sub_dt);
+      fill_angle(s->h_ang[k], angle, omega, sub_dt, now);
       angle = mgh::rem_euclid_r(angle + omega * sub_dt, mgh::TAU_F);
+      now += (double)sub_dt;
     }
     rc = run(s, chunk);
     if (rc) return rc;
@@ -1178,7 +1162,7 @@ int mg_fluid_densities(MgSim* s, float* out) {
 }
 int mg_stress_histogram_rate(MgSim* s, double* out28) {
   if (!s || !out28) return fail_global(MG_ERR_ARG, "null argument");
-  std::memcpy(out28, s->stress.hist_rate, sizeof(double) * MG_SE_BINS);
+  std::memcpy(out28, s->stress.hist_rate, sizeof(double) * MG_SE_BINS);  // the device state after the last launch
   return MG_OK;
 }
 int mg_last_step_stats(MgSim* s, MgFluidStepStats* f, MgDemStepStats* d, MgStepCounters* c) {
@@ -1355,6 +1339,9 @@ struct MgBatch {
   std::vector<uint32_t> order;
   std::vector<double> cost;
   uint32_t* d_order = nullptr;
+  // the mills' stress-accumulator states after each launch (one block, copied back at once)
+  StressState* d_stress = nullptr;
+  StressState* h_stress = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_kernel_ms = 0.0f;
   uint64_t launches = 0;
@@ -1425,7 +1412,9 @@ int batch_upload(MgBatch* b) {
     fill_desc(s);
     md[i] = s->md;
     md[i].out = b->d_out + (size_t)i * b->stride;
+    md[i].stress_copy = b->d_stress + i;
     uni[i] = *s->h_uni;
+    uni[i].fold_stress = 1u;
     b->smem = std::max(b->smem, (size_t)s->md.smem_bytes);
   }
   BCK(cudaMemcpyAsync(b->d_md, md.data(), sizeof(MillDev) * n, cudaMemcpyHostToDevice, b->stream));
@@ -1472,6 +1461,8 @@ int mg_batch_create(const MgParams* params, uint32_t n_mills, MgBatch** out) {
     BCK(cudaEventCreate(&b->ev0));
     BCK(cudaEventCreate(&b->ev1));
     BCK(cudaMalloc(&b->d_order, sizeof(uint32_t) * n_mills));
+    BCK(cudaMalloc(&b->d_stress, sizeof(StressState) * n_mills));
+    BCK(cudaMallocHost(&b->h_stress, sizeof(StressState) * n_mills));
     BCK(cudaMemcpyAsync(b->d_nsub, b->n_sub.data(), sizeof(uint32_t) * n_mills, cudaMemcpyHostToDevice, b->stream));
     // before the first frame: sub-steps times particles, balls weighted for their sweeps
     b->cost.resize(n_mills);
@@ -1509,6 +1500,8 @@ void mg_batch_destroy(MgBatch* b) {
   if (b->d_table) cudaFree(b->d_table);
   if (b->h_table) cudaFreeHost(b->h_table);
   if (b->d_order) cudaFree(b->d_order);
+  if (b->d_stress) cudaFree(b->d_stress);
+  if (b->h_stress) cudaFreeHost(b->h_stress);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -1550,6 +1543,7 @@ int mg_batch_step_frames(MgBatch* b, uint32_t frames, float frame_dt) {
     fill_desc(s);
     md[i] = s->md;
     md[i].out = b->d_out + (size_t)i * b->stride;
+    md[i].stress_copy = b->d_stress + i;
     b->smem = std::max(b->smem, (size_t)s->md.smem_bytes);
   }
   BCK(cudaMemcpyAsync(b->d_md, md.data(), sizeof(MillDev) * n, cudaMemcpyHostToDevice, b->stream));
@@ -1561,9 +1555,11 @@ int mg_batch_step_frames(MgBatch* b, uint32_t frames, float frame_dt) {
       const float sub_dt = frame_dt / (float)ns;
       const float omega = mgh::mill_omega(s->params.mill);
       float angle = s->drum_angle;
+      double now = s->sim_time;
       for (uint32_t k = 0; k < ns; ++k) {
-        fill_angle(b->h_ang[(size_t)i * b->stride + k], angle, omega, sub_dt);
+        fill_angle(b->h_ang[(size_t)i * b->stride + k], angle, omega, sub_dt, now);
         angle = mgh::rem_euclid_r(angle + omega * sub_dt, mgh::TAU_F);
+        now += (double)sub_dt;
       }
     }
     BCK(cudaMemcpyAsync(b->d_ang, b->h_ang, sizeof(SubAngles) * n * b->stride, cudaMemcpyHostToDevice, b->stream));
@@ -1577,6 +1573,7 @@ int mg_batch_step_frames(MgBatch* b, uint32_t frames, float frame_dt) {
     BCK(launch_pack_impacts(b->d_md, n, b->d_nsub, b->d_packed, b->packed_cap, b->d_cursor, b->d_table, b->stream));
     BCK(cudaMemcpyAsync(b->h_out, b->d_out, sizeof(StepOut) * n * b->stride, cudaMemcpyDeviceToHost, b->stream));
     BCK(cudaMemcpyAsync(b->h_table, b->d_table, sizeof(uint2) * n, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaMemcpyAsync(b->h_stress, b->d_stress, sizeof(StressState) * n, cudaMemcpyDeviceToHost, b->stream));
     BCK(cudaStreamSynchronize(b->stream));
     BCK(cudaEventElapsedTime(&b->last_kernel_ms, b->ev0, b->ev1));
     b->launches += 1;
@@ -1603,6 +1600,7 @@ int mg_batch_step_frames(MgBatch* b, uint32_t frames, float frame_dt) {
       for (uint32_t k = 0; k < ns; ++k)
         for (int q = 0; q <= 14; ++q) cyc += (double)o[k].stage[q];
       b->cost[i] = cyc;
+      s->stress = b->h_stress[i];
       std::memcpy(s->h_out, o, sizeof(StepOut) * ns);
       const MgImpactRecord* rec = b->h_packed + b->h_table[i].x;
       for (uint32_t k = 0; k < ns; ++k) {
@@ -1713,6 +1711,7 @@ struct MgServer {
   StepOut *d_out = nullptr, *h_out = nullptr;
   uint2 *d_table = nullptr, *h_table = nullptr;
   uint32_t *d_order = nullptr, *h_order = nullptr;  // block k runs job h_order[k] (longest first)
+  StressState *d_stress = nullptr, *h_stress = nullptr;  // the jobs' stress states after a launch
   uint32_t* d_cursor = nullptr;
   MgImpactRecord *d_packed = nullptr, *h_packed = nullptr;
   uint64_t packed_cap = 0;
@@ -1751,6 +1750,8 @@ void server_free_blocks(MgServer* v) {
   cudaFree(v->d_table); cudaFreeHost(v->h_table);
   cudaFree(v->d_order); cudaFreeHost(v->h_order);
   v->d_order = v->h_order = nullptr;
+  cudaFree(v->d_stress); cudaFreeHost(v->h_stress);
+  v->d_stress = v->h_stress = nullptr;
   v->d_md = v->h_md = nullptr;
   v->d_uni = v->h_uni = nullptr;
   v->d_ang = v->h_ang = nullptr;
@@ -1779,6 +1780,8 @@ int server_reserve(MgServer* v, uint32_t n, uint64_t packed) {
     SCK(cudaMallocHost(&v->h_table, sizeof(uint2) * c));
     SCK(cudaMalloc(&v->d_order, sizeof(uint32_t) * c));
     SCK(cudaMallocHost(&v->h_order, sizeof(uint32_t) * c));
+    SCK(cudaMalloc(&v->d_stress, sizeof(StressState) * c));
+    SCK(cudaMallocHost(&v->h_stress, sizeof(StressState) * c));
     v->cap = c;
   }
   if (packed > v->packed_cap) {
@@ -2099,18 +2102,22 @@ int mg_server_step(MgServer* v) {
     const MgSimulationParams& q = s->params.simulation;
     rc = fill_uniform(s, sim_drum(s), s->params.media, s->params.slurry, q.pbf_iterations, q.dem_iterations, 1, 1, 1);
     if (rc) return sfail(v, rc, "job %llu: %s", (unsigned long long)j->id, s->err.c_str());
+    s->h_uni->fold_stress = 1u;
     std::memcpy(&v->h_uni[k], s->h_uni, sizeof(StepUniform));
     fill_desc(s);
     v->h_md[k] = s->md;
     v->h_md[k].out = v->d_out + (size_t)k * stride;
+    v->h_md[k].stress_copy = v->d_stress + k;
     smem = std::max(smem, (size_t)s->md.smem_bytes);
     v->h_nsub[k] = j->n_sub;
     const float sub_dt = frame_dt / (float)j->n_sub;
     const float omega = mgh::mill_omega(s->params.mill);
     float angle = s->drum_angle;
+    double now = s->sim_time;
     for (uint32_t t = 0; t < j->n_sub; ++t) {
-      fill_angle(v->h_ang[(size_t)k * stride + t], angle, omega, sub_dt);
+      fill_angle(v->h_ang[(size_t)k * stride + t], angle, omega, sub_dt, now);
       angle = mgh::rem_euclid_r(angle + omega * sub_dt, mgh::TAU_F);
+      now += (double)sub_dt;
     }
   }
   SCK(cudaMemcpyAsync(v->d_md, v->h_md, sizeof(MillDev) * n, cudaMemcpyHostToDevice, v->stream));
@@ -2136,6 +2143,7 @@ int mg_server_step(MgServer* v) {
                           v->d_cursor, v->d_table, v->stream));
   SCK(cudaMemcpyAsync(v->h_out, v->d_out, sizeof(StepOut) * n * stride, cudaMemcpyDeviceToHost, v->stream));
   SCK(cudaMemcpyAsync(v->h_table, v->d_table, sizeof(uint2) * n, cudaMemcpyDeviceToHost, v->stream));
+  SCK(cudaMemcpyAsync(v->h_stress, v->d_stress, sizeof(StressState) * n, cudaMemcpyDeviceToHost, v->stream));
   SCK(cudaStreamSynchronize(v->stream));
   SCK(cudaEventElapsedTime(&v->last_kernel_ms, v->ev0, v->ev1));
   uint64_t total = 0;
@@ -2164,6 +2172,7 @@ int mg_server_step(MgServer* v) {
       return;
     }
     j->cost = cyc;
+    s->stress = v->h_stress[k];
     std::memcpy(s->h_out, o, sizeof(StepOut) * ns);
     const MgImpactRecord* rec = v->h_packed + v->h_table[k].x;
     for (uint32_t t = 0; t < ns; ++t) {
@@ -2242,7 +2251,7 @@ MgStressMetrics stress_metrics_of(const MgSim* s) {
   const double m3 = (double)s->bmat.mass * 4.0 / 3.0 * r;
   const double d = 2.0 * r;
   const double scale_j = m3 * 9.81 * d;
-  const Stress& st = s->stress;
+  const StressState& st = s->stress;
   const double n = (double)std::max<uint32_t>(s->nb, 1u);
   const double power_draw_w = (double)s->power;
   MgStressMetrics o;
@@ -2255,7 +2264,7 @@ MgStressMetrics stress_metrics_of(const MgSim* s) {
     double w = st.count_rate[a] + st.count_rate[b];
     return w > 0.0 ? (float)((st.se_hat_rate[a] + st.se_hat_rate[b]) / w) : 0.0f;
   };
-  const double total = st.total_rate();
+  const double total = stress_total_rate(st);
   const double power_per_ball = power_draw_w * d / n;
   o.ball_mass_3d_kg = (float)m3;
   o.scale_energy_j = (float)scale_j;

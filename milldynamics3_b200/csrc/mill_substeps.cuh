@@ -6,6 +6,7 @@
 #include "mill_dem.cuh"
 #include "mill_fluid.cuh"
 #include "mill_kernels.h"
+#include "mill_stress.cuh"
 
 namespace mg {
 
@@ -66,6 +67,8 @@ __global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDe
       U.to_local_next = a.to_local_next;
       U.to_world_next = a.to_world_next;
       U.to_local0 = a.to_local0;
+      U.now_s = a.now_s;
+      U.alpha = a.alpha;
       memset(&out.ctr, 0, sizeof(out.ctr));
       memset(out.stage, 0, sizeof(out.stage));
       g_stage_last = clock64();
@@ -81,10 +84,18 @@ __global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDe
     }
     if (U.run_dem) dem_step(m, U, out, m.impacts + (size_t)s * m.cap_impacts, m.err, ds, dsm);
     __syncthreads();
-    if (threadIdx.x == 0) out.stage[14] = out.stage[15] + out.stage[16] + out.stage[17] + out.stage[18] + out.stage[20] + out.stage[21] + out.stage[22] + out.stage[30];
-    if (threadIdx.x == 0) out.err = *m.err;
+    if (threadIdx.x == 0) {
+      out.stage[14] = out.stage[15] + out.stage[16] + out.stage[17] + out.stage[18] + out.stage[20] + out.stage[21] +
+                      out.stage[22] + out.stage[30];
+      // Simulation::step's grinding stats: the sub-step's impacts into the stress accumulator
+      if (U.fold_stress && !*m.err)
+        stress_update(m, m.impacts + (size_t)s * m.cap_impacts, min(out.n_impacts, m.cap_impacts), U.now_s,
+                      (double)U.dt, (double)U.alpha, (double)(out.ds.wall_work_j + out.fs.wall_work_j), m.err);
+      out.err = *m.err;
+    }
     __syncthreads();
   }
+  if (threadIdx.x == 0 && m.stress_copy) *m.stress_copy = *m.stress;
   wide_exit(m);
 }
 
