@@ -194,7 +194,10 @@ typedef struct MgScalars {
  * with it wait until their limit runs out, the step returns MG_ERR_STATE).
  * block_regs: 0 = the register budget follows the block size (128 registers a thread up to 512
  * threads, 64 above); 64 = the 64-register build at any block size (two 512-thread blocks per
- * SM, for batches of small mills). */
+ * SM, for batches of small mills).
+ * sweep_order: the order in which the warps of the drag and buoyancy sweeps take balls; 0 = by
+ * dependency level (a ball after every ball it waits for, the chain's early links first), 1 =
+ * ball index order. Results are the same either way. */
 typedef struct MgOptions {
   uint32_t cg_fp64;
   uint32_t block_threads;
@@ -204,6 +207,7 @@ typedef struct MgOptions {
   uint32_t test_wait_limit_us;
   uint32_t test_faults;
   uint32_t block_regs;
+  uint32_t sweep_order;
 } MgOptions;
 
 typedef struct MgSim MgSim;

@@ -47,12 +47,13 @@ class Batch:
             raise MillError(rc, m.decode() if m else "")
 
     def set_options(self, cg_fp64: int = 0, block_threads: int = 0, sweep_warps: int = 0, spin_ns: int = 0,
-                    block_regs: int = 0):
+                    block_regs: int = 0, sweep_order: int = 0):
         """Device options of every mill (MgOptions); block_regs = 64 runs the 64-register build,
         so that two blocks of 512 threads share an SM."""
         o = capi.Options()
         o.cg_fp64, o.block_threads, o.sweep_warps, o.spin_ns = cg_fp64, block_threads, sweep_warps, spin_ns
         o.block_regs = block_regs
+        o.sweep_order = sweep_order
         self._c(self.lib.batch_set_options(self.h, C.byref(o)))
 
     def step_frames(self, frames: int = 1, frame_dt: float = 1.0 / 60.0):

@@ -148,7 +148,7 @@ class Scalars(_S):
 class Options(_S):
     _fields_ = [("cg_fp64", C.c_uint32), ("block_threads", C.c_uint32), ("sweep_warps", C.c_uint32),
                 ("spin_ns", C.c_uint32), ("mill_blocks", C.c_uint32), ("test_wait_limit_us", C.c_uint32),
-                ("test_faults", C.c_uint32), ("block_regs", C.c_uint32)]
+                ("test_faults", C.c_uint32), ("block_regs", C.c_uint32), ("sweep_order", C.c_uint32)]
 
 
 class ServerConfig(_S):

@@ -173,6 +173,7 @@ struct StepUniform {
   uint32_t fold_stress;    // 1: fold each sub-step's impacts into the stress accumulator (Simulation::step)
   uint32_t spin_limit;     // polls after which a waiting ball gives up (ERR_BUDGET)
   uint32_t skip_done_ball; // tests only: the drag sweep never flags this ball done (NONE: none)
+  uint32_t sweep_order;    // per-ball sweeps: 0 claim balls by dependency level, 1 by index
 };
 
 // The per-sub-step part of the uniform block (drum angle and its rotations, dt), one per sub-step

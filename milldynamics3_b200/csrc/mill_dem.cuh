@@ -81,7 +81,224 @@ static __device__ float mech_energy_seq(const MillDev& m, const float2* X, const
   return e;
 }
 
-static __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, MgImpactRecord* impacts,
+// `iters` iterations of the projection (dem.rs:711-750): the pair items by dependency levels in
+// warp 0 (level-ordered descriptors di/dj, multipliers dl), then every wall at once. With track,
+// bm[i] keeps ball i's largest squared excursion from its start position m.bxs[i]. Its own
+// function, so that the item bodies are register-allocated apart from the step around them.
+static __device__ __noinline__ void project_iterations(const MillDev& m, const StepUniform& U, float2* X, float* dl,
+                                                       float* bm, const uint32_t* di, const uint32_t* dj,
+                                                       uint32_t nlev, uint32_t iters, uint32_t n, bool track, float r,
+                                                       float w, float cap_depth) {
+  // the larger of the recorded and the new squared excursion; a NaN excursion is kept (and
+  // fails the check)
+  auto excursion = [](float cur, V2 d) {
+    const float e = d.len2();
+    return !(e <= cur) ? e : cur;
+  };
+  float2* const Xp = X;
+  float* const dlp = dl;
+  const float2* const bxs = m.bxs;
+  float* const bmv = bm;
+  const uint32_t* const dip = di;
+  const uint32_t* const djp = dj;
+  for (uint32_t it = 0; it < iters; ++it) {
+    run_levels(nlev, m.lev_start, [dip, djp](uint32_t q) { return make_uint2(dip[q], djp[q]); },
+               [Xp, dlp, bxs, bmv, track, r, w, cap_depth, excursion](uint32_t q, uint2 d) {
+      float2* const X = Xp;
+      float* const dl = dlp;
+      const uint32_t i = d.x, j = d.y;
+      V2 xi(X[i]), xj(X[j]);
+      const float dlq = dl[q];  // loaded beside the positions (only this item writes it)
+      // start positions and excursions so far, loaded beside the positions
+      V2 si, sj;
+      float ei = 0.0f, ej = 0.0f;
+      if (track) { si = V2(bxs[i]); sj = V2(bxs[j]); ei = bmv[i]; ej = bmv[j]; }
+      V2 delta = xi - xj;
+      float dist = delta.len();
+      float c = dist - 2.0f * r;
+      if (c >= 0.0f) return;
+      V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
+      float w_sum = w + w;
+      if (w_sum <= 0.0f) return;
+      float c_eff = fmax_r(c, cap_depth);
+      float d_lambda = -c_eff / w_sum;
+      const V2 xin = xi + w * d_lambda * n_hat, xjn = xj - w * d_lambda * n_hat;
+      X[i] = xin.f2();
+      X[j] = xjn.f2();
+      dl[q] = dlq + d_lambda;
+      if (track) {
+        bmv[i] = excursion(ei, V2(xin.f2()) - si);
+        bmv[j] = excursion(ej, V2(xjn.f2()) - sj);
+      }
+    });
+    for (uint32_t i = tid(); i < n; i += nthr()) {
+      V2 x(X[i]), pl;
+      if (x.finite() && drum_sdf_clear(U, rotate(x, U.to_local_next), r)) continue;  // c >= 0 certainly
+      float d = drum_sdf_world_dist(U, x, U.to_local_next, pl);
+      float c = d - r;
+      if (c >= 0.0f) continue;
+      if (w <= 0.0f) continue;
+      V2 n_hat = drum_sdf_world_normal(U, x, pl, U.to_world_next);
+      float c_eff = fmax_r(c, cap_depth);
+      float d_lambda = -c_eff / w;
+      const V2 xn = x + w * d_lambda * n_hat;
+      X[i] = xn.f2();
+      m.lam_bw[i] += d_lambda;
+      if (track) bm[i] = excursion(bm[i], V2(xn.f2()) - V2(m.bxs[i]));
+    }
+    __syncthreads();
+  }
+}
+
+// Runs body(k, (i, j, lambda_n)) for the active contacts in sweep order: the pair contacts by
+// dependency levels in warp 0 (contacts of one level share no ball), then the wall contacts at once
+// (every wall contact comes after every pair contact and touches one ball); the block waits at the
+// end.
+template <class Body>
+__device__ __forceinline__ void contact_sweep(const MillDev& m, uint32_t nlev_c, uint32_t na_p, uint32_t na, Body body) {
+  run_levels(nlev_c, m.lev_start,
+             [&](uint32_t q) {
+               const uint32_t k = m.lev_items[q];
+               return make_uint4(k, m.act_i[k], m.act_j[k], __float_as_uint(m.act_l[k]));
+             },
+             [&](uint32_t, uint4 d) { body(d.x, make_uint3(d.y, d.z, d.w)); });
+  for (uint32_t k = na_p + tid(); k < na; k += nthr())
+    body(k, make_uint3(m.act_i[k], m.act_j[k], __float_as_uint(m.act_l[k])));
+  __syncthreads();
+}
+
+// Step 5 friction sweep (dem.rs:782-882) over the active contacts; wall contacts leave their work
+// terms in act_w1 / act_w2 (act_bin -2: none). Its own function, like project_iterations.
+static __device__ __noinline__ void friction_sweep(const MillDev& m, const StepUniform& U, float2* X, float2* V,
+                                                   float* TH, float* OM, uint32_t nlev_c, uint32_t na_p, uint32_t na,
+                                                   float w, float w_rot, float r, float dt) {
+  const MgMediaParams& md = U.media;
+  contact_sweep(m, nlev_c, na_p, na, [&](uint32_t k, uint3 d) {
+    // this body's constants and pointers as locals (they stay in registers)
+    float2* const X_l = X;
+    float2* const V_l = V;
+    float* const TH_l = TH;
+    float* const OM_l = OM;
+    const float w_l = w, w_rot_l = w_rot, r_l = r, dt_l = dt;
+    const MgMediaParams md_l = md;
+    const uint32_t i = d.x, j = d.y;
+    const float lambda_n = __uint_as_float(d.z);
+    if (j != NONE) {
+      V2 delta = V2(X_l[i]) - V2(X_l[j]);
+      float dist = delta.len();
+      V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
+      V2 t_hat(-n_hat.y, n_hat.x);
+      float v_t = (V2(V_l[i]) - V2(V_l[j])).dot(t_hat) - r_l * OM_l[i] - r_l * OM_l[j];
+      float w_sum_t = w_l + w_l + r_l * r_l * w_rot_l + r_l * r_l * w_rot_l;
+      if (w_sum_t <= 0.0f) return;
+      float raw = -v_t * dt_l / w_sum_t;
+      float mu = effective_friction(md_l.friction_ball_ball, md_l.friction_ball_ball_static, v_t, md_l.friction_velocity_scale_m_s);
+      float max_mag = mu * lambda_n;
+      float dlt = clamp_r(raw, -max_mag, max_mag);
+      X_l[i] = (V2(X_l[i]) + w_l * dlt * t_hat).f2();
+      X_l[j] = (V2(X_l[j]) - w_l * dlt * t_hat).f2();
+      TH_l[i] -= r_l * w_rot_l * dlt;
+      TH_l[j] -= r_l * w_rot_l * dlt;
+      V2 dv = w_l * dlt * t_hat / dt_l;
+      float domega = -r_l * w_rot_l * dlt / dt_l;
+      V_l[i] = (V2(V_l[i]) + dv).f2();
+      V_l[j] = (V2(V_l[j]) - dv).f2();
+      OM_l[i] += domega;
+      OM_l[j] += domega;
+    } else {
+      m.act_bin[k] = -2;  // no work terms unless the contact completes below
+      float dd;
+      V2 n_hat;
+      drum_sdf_world(U, V2(X_l[i]), U.to_local_next, U.to_world_next, dd, n_hat);
+      V2 t_hat(-n_hat.y, n_hat.x);
+      V2 v_wall = wall_velocity(U.drum_omega, V2(X_l[i]) - r_l * n_hat);
+      float v_t = (V2(V_l[i]) - v_wall).dot(t_hat) - r_l * OM_l[i];
+      float w_sum_t = w_l + r_l * r_l * w_rot_l;
+      if (w_sum_t <= 0.0f) return;
+      float raw = -v_t * dt_l / w_sum_t;
+      float mu = effective_friction(md_l.friction_ball_wall, md_l.friction_ball_wall_static, v_t, md_l.friction_velocity_scale_m_s);
+      float max_mag = mu * lambda_n;
+      float dlt = clamp_r(raw, -max_mag, max_mag);
+      X_l[i] = (V2(X_l[i]) + w_l * dlt * t_hat).f2();
+      TH_l[i] -= r_l * w_rot_l * dlt;
+      V_l[i] = (V2(V_l[i]) + w_l * dlt * t_hat / dt_l).f2();
+      OM_l[i] += -r_l * w_rot_l * dlt / dt_l;
+      m.act_w1[k] = (dlt / dt_l) * t_hat.dot(v_wall);
+      m.act_w2[k] = (lambda_n / dt_l) * n_hat.dot(v_wall);
+      m.act_bin[k] = 0;
+    }
+  });
+}
+
+// Step 6 restitution sweep (dem.rs:909-1019) over the active contacts, with the impact accounting
+// (collision count and energy histogram in S, impact records flagged in act_flag / act_rec).
+static __device__ __noinline__ void restitution_sweep(const MillDev& m, const StepUniform& U, DemShared& S, float2* X,
+                                                      float2* V, uint32_t nlev_c, uint32_t na_p, uint32_t na, float w,
+                                                      float r, float impact_threshold) {
+  const MgMediaParams& md = U.media;
+  contact_sweep(m, nlev_c, na_p, na, [&](uint32_t k, uint3 d) {
+    // this body's constants and pointers as locals (they stay in registers)
+    float2* const X_l = X;
+    float2* const V_l = V;
+    const float w_l = w, r_l = r, impact_threshold_l = impact_threshold;
+    const MgMediaParams md_l = md;
+    const uint32_t i = d.x, j = d.y;
+    m.act_flag[k] = 0;
+    if (j != NONE) {
+      V2 delta = V2(X_l[i]) - V2(X_l[j]);
+      float dist = delta.len();
+      V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
+      float v_n_pre = (V2(m.bvpre[i]) - V2(m.bvpre[j])).dot(n_hat);
+      bool fresh = v_n_pre < -RESTITUTION_VELOCITY_THRESHOLD;
+      if (fresh) {
+        atomicAdd(&S.collisions, 1u);
+        int bin = impact_energy_bin(0.5f * (m.b_m * 0.5f) * v_n_pre * v_n_pre);
+        if (bin >= 0) atomicAdd(&S.hist[bin], 1u);
+      }
+      float e = fresh ? md_l.restitution_ball_ball : 0.0f;
+      if (-v_n_pre > impact_threshold_l) {
+        V2 t_hat(-n_hat.y, n_hat.x);
+        float slip = (V2(m.bvpre[i]) - V2(m.bvpre[j])).dot(t_hat) - r_l * m.bompre[i] - r_l * m.bompre[j];
+        m.act_rec[k] = MgImpactRecord{MG_IMPACT_BALL_BALL, i, j, -v_n_pre, fabsf(slip), e};
+        m.act_flag[k] = 1;
+      }
+      float target = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
+      float v_n_now = (V2(V_l[i]) - V2(V_l[j])).dot(n_hat);
+      float dvn = target - v_n_now;
+      float w_sum = w_l + w_l;
+      if (w_sum <= 0.0f) return;
+      float impulse = dvn / w_sum;
+      V_l[i] = (V2(V_l[i]) + w_l * impulse * n_hat).f2();
+      V_l[j] = (V2(V_l[j]) - w_l * impulse * n_hat).f2();
+    } else {
+      float dd;
+      V2 n_hat;
+      drum_sdf_world(U, V2(X_l[i]), U.to_local_next, U.to_world_next, dd, n_hat);
+      V2 v_wall = wall_velocity(U.drum_omega, V2(X_l[i]) - r_l * n_hat);
+      float v_n_pre = (V2(m.bvpre[i]) - v_wall).dot(n_hat);
+      bool fresh = v_n_pre < -RESTITUTION_VELOCITY_THRESHOLD;
+      if (fresh) {
+        atomicAdd(&S.collisions, 1u);
+        int bin = impact_energy_bin(0.5f * m.b_m * v_n_pre * v_n_pre);
+        if (bin >= 0) atomicAdd(&S.hist[bin], 1u);
+      }
+      float e = fresh ? md_l.restitution_ball_wall : 0.0f;
+      if (-v_n_pre > impact_threshold_l) {
+        V2 t_hat(-n_hat.y, n_hat.x);
+        float slip = (V2(m.bvpre[i]) - v_wall).dot(t_hat) - r_l * m.bompre[i];
+        m.act_rec[k] = MgImpactRecord{MG_IMPACT_BALL_WALL, i, MG_WALL_PARTNER, -v_n_pre, fabsf(slip), e};
+        m.act_flag[k] = 1;
+      }
+      float target = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
+      float v_n_now = (V2(V_l[i]) - v_wall).dot(n_hat);
+      float dvn = target - v_n_now;
+      if (w_l <= 0.0f) return;
+      V_l[i] = (V2(V_l[i]) + dvn * n_hat).f2();
+    }
+  });
+}
+
+static __device__ __noinline__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, MgImpactRecord* impacts,
                          uint32_t* err, DemShared& S, unsigned char* dsm) {
   const uint32_t n = m.nb;
   const float dt = U.dt;
@@ -194,12 +411,6 @@ static __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut&
   uint32_t *lvl = m.dm_lvl, *di = m.act_i, *dj = m.act_j;
   float* dl = m.act_l;
   float* bm = m.bmove;  // per ball largest squared excursion of the run (shared memory when it fits)
-  // the larger of the recorded and the new squared excursion; a NaN excursion is kept (and
-  // fails the check)
-  auto excursion = [](float cur, V2 d) {
-    const float e = d.len2();
-    return !(e <= cur) ? e : cur;
-  };
   // One run: npi pair items (pair plist[q], or pair q when plist is null) by dependency levels in
   // warp 0, then the n walls of the iteration at once: in each iteration every wall comes after
   // every pair, and walls of different balls are independent.
@@ -247,60 +458,7 @@ static __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut&
     }
     __syncthreads();
     stage_mark(out.stage, 22);
-    // the item body takes its constants and pointers by value, so that they stay in registers
-    float2* const Xp = X;
-    float* const dlp = dl;
-    const float2* const bxs = m.bxs;
-    float* const bmv = bm;
-    const uint32_t* const dip = di;
-    const uint32_t* const djp = dj;
-    for (uint32_t it = 0; it < iters; ++it) {
-      run_levels(nlev, m.lev_start, [dip, djp](uint32_t q) { return make_uint2(dip[q], djp[q]); },
-                 [Xp, dlp, bxs, bmv, track, r, w, cap_depth, excursion](uint32_t q, uint2 d) {
-        float2* const X = Xp;
-        float* const dl = dlp;
-        const uint32_t i = d.x, j = d.y;
-        V2 xi(X[i]), xj(X[j]);
-        const float dlq = dl[q];  // loaded beside the positions (only this item writes it)
-        // start positions and excursions so far, loaded beside the positions
-        V2 si, sj;
-        float ei = 0.0f, ej = 0.0f;
-        if (track) { si = V2(bxs[i]); sj = V2(bxs[j]); ei = bmv[i]; ej = bmv[j]; }
-        V2 delta = xi - xj;
-        float dist = delta.len();
-        float c = dist - 2.0f * r;
-        if (c >= 0.0f) return;
-        V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
-        float w_sum = w + w;
-        if (w_sum <= 0.0f) return;
-        float c_eff = fmax_r(c, cap_depth);
-        float d_lambda = -c_eff / w_sum;
-        const V2 xin = xi + w * d_lambda * n_hat, xjn = xj - w * d_lambda * n_hat;
-        X[i] = xin.f2();
-        X[j] = xjn.f2();
-        dl[q] = dlq + d_lambda;
-        if (track) {
-          bmv[i] = excursion(ei, V2(xin.f2()) - si);
-          bmv[j] = excursion(ej, V2(xjn.f2()) - sj);
-        }
-      });
-      for (uint32_t i = tid(); i < n; i += nthr()) {
-        V2 x(X[i]), pl;
-        if (x.finite() && drum_sdf_clear(U, rotate(x, U.to_local_next), r)) continue;  // c >= 0 certainly
-        float d = drum_sdf_world_dist(U, x, U.to_local_next, pl);
-        float c = d - r;
-        if (c >= 0.0f) continue;
-        if (w <= 0.0f) continue;
-        V2 n_hat = drum_sdf_world_normal(U, x, pl, U.to_world_next);
-        float c_eff = fmax_r(c, cap_depth);
-        float d_lambda = -c_eff / w;
-        const V2 xn = x + w * d_lambda * n_hat;
-        X[i] = xn.f2();
-        m.lam_bw[i] += d_lambda;
-        if (track) bm[i] = excursion(bm[i], V2(xn.f2()) - V2(m.bxs[i]));
-      }
-      __syncthreads();
-    }
+    project_iterations(m, U, X, dl, bm, di, dj, nlev, iters, n, track, r, w, cap_depth);
     return npi;
   };
   // rounds: a failed check adds the pairs it could not clear and runs again from the start
@@ -402,78 +560,13 @@ static __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut&
   stage_mark(out.stage, 30);
   // step 5 friction (dem.rs:782-882)
   const MgMediaParams& md = U.media;
-  auto load_contact = [&](uint32_t k) { return make_uint3(m.act_i[k], m.act_j[k], __float_as_uint(m.act_l[k])); };
   // dependency levels of the active pair contacts, shared by the friction and restitution
   // sweeps: contacts of one level share no ball, so each level runs in parallel. Every wall
   // contact comes after every pair contact and touches one ball, so the walls then run at once.
   const uint32_t nlev_c = compute_levels(na_p, m.dm_pa, m.dm_pb, m.dm_lvl);
   bucket_levels(na_p, m.dm_lvl, nlev_c, m.lev_start, m.lev_cur, m.lev_items);
   stage_mark(out.stage, 38);
-  auto contact_sweep = [&](auto body) {
-    run_levels(nlev_c, m.lev_start,
-               [&](uint32_t q) {
-                 const uint32_t k = m.lev_items[q];
-                 return make_uint4(k, m.act_i[k], m.act_j[k], __float_as_uint(m.act_l[k]));
-               },
-               [&](uint32_t, uint4 d) { body(d.x, make_uint3(d.y, d.z, d.w)); });
-    for (uint32_t k = na_p + tid(); k < na; k += nthr()) body(k, load_contact(k));
-    __syncthreads();
-  };
-  contact_sweep([&](uint32_t k, uint3 d) {
-    // this body's constants and pointers as locals (they stay in registers)
-    float2* const X_l = X;
-    float2* const V_l = V;
-    float* const TH_l = TH;
-    float* const OM_l = OM;
-    const float w_l = w, w_rot_l = w_rot, r_l = r, dt_l = dt;
-    const MgMediaParams md_l = md;
-    const uint32_t i = d.x, j = d.y;
-    const float lambda_n = __uint_as_float(d.z);
-    if (j != NONE) {
-      V2 delta = V2(X_l[i]) - V2(X_l[j]);
-      float dist = delta.len();
-      V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
-      V2 t_hat(-n_hat.y, n_hat.x);
-      float v_t = (V2(V_l[i]) - V2(V_l[j])).dot(t_hat) - r_l * OM_l[i] - r_l * OM_l[j];
-      float w_sum_t = w_l + w_l + r_l * r_l * w_rot_l + r_l * r_l * w_rot_l;
-      if (w_sum_t <= 0.0f) return;
-      float raw = -v_t * dt_l / w_sum_t;
-      float mu = effective_friction(md_l.friction_ball_ball, md_l.friction_ball_ball_static, v_t, md_l.friction_velocity_scale_m_s);
-      float max_mag = mu * lambda_n;
-      float dlt = clamp_r(raw, -max_mag, max_mag);
-      X_l[i] = (V2(X_l[i]) + w_l * dlt * t_hat).f2();
-      X_l[j] = (V2(X_l[j]) - w_l * dlt * t_hat).f2();
-      TH_l[i] -= r_l * w_rot_l * dlt;
-      TH_l[j] -= r_l * w_rot_l * dlt;
-      V2 dv = w_l * dlt * t_hat / dt_l;
-      float domega = -r_l * w_rot_l * dlt / dt_l;
-      V_l[i] = (V2(V_l[i]) + dv).f2();
-      V_l[j] = (V2(V_l[j]) - dv).f2();
-      OM_l[i] += domega;
-      OM_l[j] += domega;
-    } else {
-      m.act_bin[k] = -2;  // no work terms unless the contact completes below
-      float dd;
-      V2 n_hat;
-      drum_sdf_world(U, V2(X_l[i]), U.to_local_next, U.to_world_next, dd, n_hat);
-      V2 t_hat(-n_hat.y, n_hat.x);
-      V2 v_wall = wall_velocity(U.drum_omega, V2(X_l[i]) - r_l * n_hat);
-      float v_t = (V2(V_l[i]) - v_wall).dot(t_hat) - r_l * OM_l[i];
-      float w_sum_t = w_l + r_l * r_l * w_rot_l;
-      if (w_sum_t <= 0.0f) return;
-      float raw = -v_t * dt_l / w_sum_t;
-      float mu = effective_friction(md_l.friction_ball_wall, md_l.friction_ball_wall_static, v_t, md_l.friction_velocity_scale_m_s);
-      float max_mag = mu * lambda_n;
-      float dlt = clamp_r(raw, -max_mag, max_mag);
-      X_l[i] = (V2(X_l[i]) + w_l * dlt * t_hat).f2();
-      TH_l[i] -= r_l * w_rot_l * dlt;
-      V_l[i] = (V2(V_l[i]) + w_l * dlt * t_hat / dt_l).f2();
-      OM_l[i] += -r_l * w_rot_l * dlt / dt_l;
-      m.act_w1[k] = (dlt / dt_l) * t_hat.dot(v_wall);
-      m.act_w2[k] = (lambda_n / dt_l) * n_hat.dot(v_wall);
-      m.act_bin[k] = 0;
-    }
-  });
+  friction_sweep(m, U, X, V, TH, OM, nlev_c, na_p, na, w, w_rot, r, dt);
   if (tid() < 32) {
     // wall work summed in wall-contact order, two adds per contact (dem.rs:870, 881)
     const uint32_t lane = tid();
@@ -512,66 +605,7 @@ static __device__ void dem_step(const MillDev& m, const StepUniform& U, StepOut&
   __syncthreads();
   // step 6 restitution with impact accounting (dem.rs:909-1019); per-item records are compacted
   // in sweep order afterwards
-  contact_sweep([&](uint32_t k, uint3 d) {
-    // this body's constants and pointers as locals (they stay in registers)
-    float2* const X_l = X;
-    float2* const V_l = V;
-    const float w_l = w, r_l = r, impact_threshold_l = impact_threshold;
-    const MgMediaParams md_l = md;
-    const uint32_t i = d.x, j = d.y;
-    m.act_flag[k] = 0;
-    if (j != NONE) {
-      V2 delta = V2(X_l[i]) - V2(X_l[j]);
-      float dist = delta.len();
-      V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
-      float v_n_pre = (V2(m.bvpre[i]) - V2(m.bvpre[j])).dot(n_hat);
-      bool fresh = v_n_pre < -RESTITUTION_VELOCITY_THRESHOLD;
-      if (fresh) {
-        atomicAdd(&S.collisions, 1u);
-        int bin = impact_energy_bin(0.5f * (m.b_m * 0.5f) * v_n_pre * v_n_pre);
-        if (bin >= 0) atomicAdd(&S.hist[bin], 1u);
-      }
-      float e = fresh ? md_l.restitution_ball_ball : 0.0f;
-      if (-v_n_pre > impact_threshold_l) {
-        V2 t_hat(-n_hat.y, n_hat.x);
-        float slip = (V2(m.bvpre[i]) - V2(m.bvpre[j])).dot(t_hat) - r_l * m.bompre[i] - r_l * m.bompre[j];
-        m.act_rec[k] = MgImpactRecord{MG_IMPACT_BALL_BALL, i, j, -v_n_pre, fabsf(slip), e};
-        m.act_flag[k] = 1;
-      }
-      float target = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
-      float v_n_now = (V2(V_l[i]) - V2(V_l[j])).dot(n_hat);
-      float dvn = target - v_n_now;
-      float w_sum = w_l + w_l;
-      if (w_sum <= 0.0f) return;
-      float impulse = dvn / w_sum;
-      V_l[i] = (V2(V_l[i]) + w_l * impulse * n_hat).f2();
-      V_l[j] = (V2(V_l[j]) - w_l * impulse * n_hat).f2();
-    } else {
-      float dd;
-      V2 n_hat;
-      drum_sdf_world(U, V2(X_l[i]), U.to_local_next, U.to_world_next, dd, n_hat);
-      V2 v_wall = wall_velocity(U.drum_omega, V2(X_l[i]) - r_l * n_hat);
-      float v_n_pre = (V2(m.bvpre[i]) - v_wall).dot(n_hat);
-      bool fresh = v_n_pre < -RESTITUTION_VELOCITY_THRESHOLD;
-      if (fresh) {
-        atomicAdd(&S.collisions, 1u);
-        int bin = impact_energy_bin(0.5f * m.b_m * v_n_pre * v_n_pre);
-        if (bin >= 0) atomicAdd(&S.hist[bin], 1u);
-      }
-      float e = fresh ? md_l.restitution_ball_wall : 0.0f;
-      if (-v_n_pre > impact_threshold_l) {
-        V2 t_hat(-n_hat.y, n_hat.x);
-        float slip = (V2(m.bvpre[i]) - v_wall).dot(t_hat) - r_l * m.bompre[i];
-        m.act_rec[k] = MgImpactRecord{MG_IMPACT_BALL_WALL, i, MG_WALL_PARTNER, -v_n_pre, fabsf(slip), e};
-        m.act_flag[k] = 1;
-      }
-      float target = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
-      float v_n_now = (V2(V_l[i]) - v_wall).dot(n_hat);
-      float dvn = target - v_n_now;
-      if (w_l <= 0.0f) return;
-      V_l[i] = (V2(V_l[i]) + dvn * n_hat).f2();
-    }
-  });
+  restitution_sweep(m, U, S, X, V, nlev_c, na_p, na, w, r, impact_threshold);
   if (tid() == 0) m.act_flag[na] = 0;
   __syncthreads();
   const uint32_t nrec = block_exclusive_scan(m.act_flag, na + 1);

@@ -657,6 +657,647 @@ static __device__ void drag_pre_balls(const MillDev& m, uint32_t w0, uint32_t nw
   }
 }
 
+// The per-ball sweeps' slot for the ball a warp is running (one per warp; indices DS_* for the drag
+// sweep, BS_* for the buoyancy sweep) and the running sweep's constants (DK_* / BK_*), in shared
+// memory so that the per-ball bodies keep few values in registers across the dependency wait.
+enum : uint32_t {
+  DS_M_ENT = 0, DS_I_ENT = 1, DS_R_BAR = 2, DS_S_ACC = 4, DS_S_SCALE = 5, DS_PRE = 6,  // drag_pre[0..5]
+  DS_VB = 6, DS_OMB = 8, DS_DV_B = 9, DS_DW_B = 11, DS_SLOT = 12
+};
+enum : uint32_t { BS_RHO_LOCAL = 0, BS_DEN = 1, BS_XB = 2, BS_IMPULSE = 4 };
+enum : uint32_t {
+  DK_MASS, DK_RHO0, DK_MASS_TRUE, DK_BETA, DK_DT, DK_I_B, DK_H_C, DK_ROT_CAP, DK_B_M, DK_B_RTRUE
+};
+enum : uint32_t { BK_RHO0, BK_OM_ABS, BK_AREA, BK_DT, BK_MASS };
+constexpr uint32_t SWEEP_CONSTS = 10;  // DK_* and BK_* indices are below it
+constexpr uint32_t DRAG_LIVE = 0x80000000u;
+__shared__ float g_ball_slot[MAX_BLOCK_WARPS][DS_SLOT];
+__shared__ float g_sweep_const[SWEEP_CONSTS];
+
+// The drag sweep proper (pbf.rs:1824-2011): balls in dependency order over the item lists, on the
+// velocities V; the constants are in g_sweep_const. Its own function, so that the per-ball bodies
+// are register-allocated apart from the set-up around them.
+static __device__ __noinline__ void drag_sweep(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err,
+                                               float2* V, uint32_t* done, const uint32_t* order) {
+  const uint32_t nb = m.nb;
+  const bool want_mom = U.want_momentum != 0;
+  // Lane l holds item l of the ball (items from 32 on are read from the lists when needed); the
+  // ball's own quantities sit in its warp's slot (g_ball_slot) from the prefetch to the post.
+  struct DragBall {
+    uint32_t cnt;  // item count, DRAG_LIVE set when the ball takes part (entrained mass > 1e-12)
+    uint32_t j;
+    V2 r_i;
+    float phi;
+    V2 dv_i;
+  };
+  ball_dataflow(
+      nb, m.rec_off, m.rec_pred, done, order, U.sweep_warps, U.spin_ns, U.spin_limit, U.skip_done_ball, err,
+      &out.stage[32],
+      // before the wait: the item data and the geometry-only quantities computed for every ball
+      // ahead of the sweep (drag_pre_balls)
+      [&](uint32_t b, int lane) {
+        DragBall q;
+        q.cnt = m.item_n[b];
+        q.j = 0;
+        q.phi = 0.0f;
+        if (q.cnt == 0) return q;
+        const uint32_t base = b * m.cap_items;
+        if ((uint32_t)lane < q.cnt) {
+          q.j = m.item_j[base + lane];
+          q.r_i = V2(m.item_v[base + lane]);
+          q.phi = m.item_w[base + lane];
+        }
+        // slot: entrained mass, inertia, centroid x, y, s_acc, s_scale (drag_pre), the ball's
+        // velocity x, y and spin
+        float* sl = g_ball_slot[threadIdx.x >> 5];
+        __syncwarp();  // the previous ball's post has read the slot
+        if (lane < DS_PRE) sl[lane] = m.drag_pre[8u * b + lane];
+        else if (lane < DS_OMB) sl[lane] = reinterpret_cast<const float*>(m.bv + b)[lane - DS_VB];
+        else if (lane == DS_OMB) sl[lane] = m.bom[b];
+        if (!(m.drag_pre[8u * b] <= 1e-12f)) q.cnt |= DRAG_LIVE;  // (a NaN mass takes part too)
+        return q;
+      },
+      // on the chain: entrained velocity and angular momentum, the relaxation, the fluid updates
+      [&](uint32_t b, int lane, DragBall& q) {
+        if (!(q.cnt & DRAG_LIVE)) return;
+        const uint32_t base = b * m.cap_items, cnt = q.cnt & ~DRAG_LIVE;
+        const float* sl = g_ball_slot[threadIdx.x >> 5];
+        const float* K = g_sweep_const;
+        float2* const Vl = V;
+        const float mass_l = K[DK_MASS];
+        float l_sum = 0.0f, vsx = 0.0f, vsy = 0.0f;
+        for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+          const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
+          float lw = 0.0f;
+          V2 vw;
+          if (s < cnt) {
+            const V2 r_i = s < 32 ? q.r_i : V2(m.item_v[base + s]);
+            const V2 vj(Vl[s < 32 ? q.j : m.item_j[base + s]]);
+            const float w = mass_l * (s < 32 ? q.phi : m.item_w[base + s]);
+            vw = w * vj;
+            lw = w * cross2(r_i, vj);
+          }
+          lane_seq_sum3(vsx, vsy, l_sum, vw.x, vw.y, lw, lim);
+        }
+        const float m_ent = sl[DS_M_ENT], i_ent = sl[DS_I_ENT], b_m = K[DK_B_M], i_b = K[DK_I_B];
+        V2 v_bar = V2(vsx, vsy) / m_ent;
+        V2 v_rel = v_bar - V2(sl[DS_VB], sl[DS_VB + 1]);
+        float speed_rel = v_rel.len();
+        const float rho0_l = K[DK_RHO0];
+        float inv_tau_form = (speed_rel > 1e-6f && rho0_l > 0.0f)
+                                 ? 0.5f * rho0_l * 1.0f * (2.0f * K[DK_B_RTRUE]) * speed_rel / K[DK_MASS_TRUE]
+                                 : 0.0f;
+        float bt = K[DK_BETA] * (1.0f - expf_r(-K[DK_DT] * (0.0f + inv_tau_form)));
+        float a_lin = bt * m_ent / (b_m + m_ent);
+        V2 dv_b = a_lin * v_rel;
+        float dw_b = 0.0f, c_rot = 0.0f;
+        if (i_ent > 1e-12f) {
+          float omega_bar = l_sum / i_ent;
+          float a_rot = bt * i_ent / (i_b + i_ent);
+          float candidate_dw = a_rot * (omega_bar - sl[DS_OMB]);
+          const float s_acc = sl[DS_S_ACC];
+          if (fabsf(s_acc) > 0.1f * sl[DS_S_SCALE]) {
+            float raw_c_rot = -i_b * candidate_dw / s_acc;
+            float max_lever = 2.0f * K[DK_H_C];
+            float cap = max_lever > 1e-9f ? K[DK_ROT_CAP] / max_lever : 0.0f;
+            c_rot = clamp_r(raw_c_rot, -cap, cap);
+            dw_b = -c_rot * s_acc / i_b;
+          }
+        }
+        const V2 p_bar(-sl[DS_R_BAR + 1], sl[DS_R_BAR]);  // read only when c_rot != 0 (i_ent > 1e-12)
+        for (uint32_t s = lane; s < cnt; s += 32) {
+          const uint32_t j = s < 32 ? q.j : m.item_j[base + s];
+          const V2 r_i = s < 32 ? q.r_i : V2(m.item_v[base + s]);
+          const float phi = s < 32 ? q.phi : m.item_w[base + s];
+          V2 dv_i = -(b_m / m_ent) * dv_b * phi;
+          if (c_rot != 0.0f) {
+            V2 perp_i(-r_i.y, r_i.x);
+            dv_i += c_rot * phi * (perp_i - p_bar);
+          }
+          Vl[j] = (V2(Vl[j]) + dv_i).f2();
+          if (s < 32) q.dv_i = dv_i;
+          else if (want_mom) m.rec_M[m.rec_off[b] + s] = (mass_l * dv_i).f2();
+        }
+        if (lane == 0) {
+          float* slw = g_ball_slot[threadIdx.x >> 5];
+          slw[DS_DV_B] = dv_b.x;
+          slw[DS_DV_B + 1] = dv_b.y;
+          slw[DS_DW_B] = dw_b;
+        }
+      },
+      // after the flag: the ball's impulse and angular impulse, the momentum records
+      [&](uint32_t b, int lane, DragBall& q) {
+        if (!(q.cnt & DRAG_LIVE)) return;
+        const uint32_t cnt = q.cnt & ~DRAG_LIVE;
+        if (want_mom && (uint32_t)lane < cnt) m.rec_M[m.rec_off[b] + lane] = (m.f_mass * q.dv_i).f2();
+        if (lane == 0) {
+          const float* sl = g_ball_slot[threadIdx.x >> 5];
+          const V2 dv_b(sl[DS_DV_B], sl[DS_DV_B + 1]), r_bar(sl[DS_R_BAR], sl[DS_R_BAR + 1]);
+          m.imp[b] = (V2(m.imp[b]) + m.b_m * dv_b).f2();
+          m.ang[b] += m.b_I * sl[DS_DW_B] + m.b_m * cross2(r_bar, dv_b);
+          m.item_n[b] = cnt | 0x80000000u;  // mark: contributed fluid momentum records
+        }
+      });
+}
+
+// Step 6.5 (pbf.rs:1777-2013): the drag sweep on the velocities V (positions X), in its own
+// function so that the sweep's per-ball state gets the whole register budget. Returns false when
+// the item lists failed (the error is in *err).
+static __device__ __noinline__ bool drag_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err,
+                                              FluidShared& S, float2* X, float2* V, uint32_t* done,
+                                              uint32_t* scratch, uint32_t scratch_words,
+                                              const uint32_t** order_out) {
+  const uint32_t n = m.nf, nb = m.nb;
+  const float h = m.f_h, rho0 = m.f_rho0, mass = m.f_mass, dt = U.dt;
+  (void)rho0;
+  const float mu = fmax_r(U.slurry.viscosity_pa_s, 0.0f);
+  if (nb > 0 && m.b_r > 0.0f && m.b_rtrue > 0.0f && mu > 1e-6f) {
+    const float beta_b = clamp_r(U.slurry.ball_no_slip, 0.0f, 1.0f);
+    const float rot_cap = 0.2f * fluid_vmax(U);
+    const float rho_ball = m.b_m / (PI_F * m.b_r * m.b_r);
+    const float mass_true = rho_ball * PI_F * m.b_rtrue * m.b_rtrue;
+    if (beta_b > 0.0f) {
+      const float h_c = m.b_r + h;
+      const float w_hc0 = fmax_r(poly6(0.0f, h_c), 1e-12f);
+      grid_build(X, n, fmax_r(h_c, 1e-6f), m.gB, S.hB, err);
+      // item lists per ball in for_each_near order (positions do not change during the sweep):
+      // one warp per ball, an ordered compaction of each 32-candidate chunk
+      uint32_t n_items = 0;
+      wide_phase(m, WIDE_DRAG_ITEMS, &S.hB, [&](uint32_t w0, uint32_t nw) { n_items += drag_item_balls(m, S.hB, w0, nw); });
+      n_items = block_sum_u(n_items) + wide_counter(m);
+      if (tid() == 0) out.ctr.n_coupling_items += n_items;
+      __syncthreads();
+      if (*err) return false;
+      stage_mark(out.stage, 24);
+      const uint32_t nrec = pack_ball_items(m.item_j, m.item_n, m.cap_items, nb, m.rec_off, m.rec_i, m.rec_b);
+      LevelScratch L;
+      const bool by_level = U.sweep_order == 0 && level_scratch(nb, scratch, scratch_words, L);
+      ball_item_preds(m.rec_i, m.rec_b, nrec, n, nb, m.bk_start, m.bk_cur, m.bk_order, m.rec_pred,
+                      by_level ? &L : nullptr);
+      const uint32_t* order = by_level ? ball_level_order(nb, m.rec_off, m.rec_pred, L) : nullptr;
+      *order_out = order;
+      stage_mark(out.stage, 25);
+      wide_phase(m, WIDE_DRAG_PRE, nullptr, [&](uint32_t w0, uint32_t nw) { drag_pre_balls(m, w0, nw); });
+      // the sweep's constants, read from shared memory by the per-ball bodies
+      if (tid() == 0) {
+        float* K = g_sweep_const;
+        K[DK_MASS] = mass;
+        K[DK_RHO0] = rho0;
+        K[DK_MASS_TRUE] = mass_true;
+        K[DK_BETA] = beta_b;
+        K[DK_DT] = dt;
+        K[DK_I_B] = m.b_I;
+        K[DK_H_C] = h_c;
+        K[DK_ROT_CAP] = rot_cap;
+        K[DK_B_M] = m.b_m;
+        K[DK_B_RTRUE] = m.b_rtrue;
+      }
+      __syncthreads();
+      drag_sweep(m, U, out, err, V, done, order);
+      if (tid() == 0 && U.want_momentum) {
+        V2 mom(S.fscal[0], S.fscal[1]);
+        for (uint32_t b = 0; b < nb; ++b) {
+          if (!(m.item_n[b] & 0x80000000u)) continue;
+          for (uint32_t r = m.rec_off[b]; r < m.rec_off[b + 1]; ++r) mom += V2(m.rec_M[r]);
+        }
+        S.fscal[0] = mom.x;
+        S.fscal[1] = mom.y;
+      }
+      __syncthreads();
+      stage_mark(out.stage, 26);
+    }
+  }
+  return true;
+}
+
+// The buoyancy sweep proper (pbf.rs:2042-2121): balls in dependency order over the item lists,
+// on the velocities V at positions X. Its own function, like drag_sweep.
+static __device__ __noinline__ void buoyancy_sweep(const MillDev& m, const StepUniform& U, StepOut& out,
+                                                   uint32_t* err, const float2* X, float2* V, uint32_t* done,
+                                                   const uint32_t* order) {
+  const uint32_t nb = m.nb;
+  const bool want_mom = U.want_momentum != 0;
+  if (tid() == 0) {
+    float* K = g_sweep_const;
+    K[BK_RHO0] = m.f_rho0;
+    K[BK_OM_ABS] = fabsf(U.drum_omega);
+    K[BK_AREA] = PI_F * m.b_r * m.b_r;
+    K[BK_DT] = U.dt;
+    K[BK_MASS] = m.f_mass;
+  }
+  __syncthreads();
+  // Lane l holds item l of the ball (items from 32 on are read from the lists when needed); the
+  // ball's local density, weight sum, position and impulse sit in its warp's slot.
+  struct BuoyBall {
+    uint32_t cnt, j;
+    float w, frac, d2;
+    V2 d, dv;
+    bool valid;
+  };
+  ball_dataflow(
+      nb, m.rec_off, m.rec_pred, done, order, U.sweep_warps, U.spin_ns, U.spin_limit, NONE, err, &out.stage[35],
+      // before the wait: item geometry, the weight sum and the weight fractions, which the sweep does
+      // not change
+      [&](uint32_t b, int lane) {
+        BuoyBall q;
+        q.cnt = m.item_n[b];
+        q.j = 0;
+        q.w = 0.0f;
+        q.valid = false;
+        if (q.cnt == 0) return q;
+        const uint32_t base = b * m.cap_items, cnt = q.cnt;
+        const float rho_local = m.item_v[base].x;
+        if ((uint32_t)lane < cnt) {
+          q.j = m.item_j[base + lane];
+          q.w = m.item_w[base + lane];
+          q.d = V2(X[q.j]);
+          q.d2 = q.d.len2();
+          q.valid = !(q.d2 <= 1e-12f);
+          q.frac = q.w / rho_local;
+        }
+        // the weight sum over the valid items in item order (an invalid item adds -0.0: no change)
+        float den = 0.0f;
+        for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+          const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
+          float dvw = -0.0f;
+          if (s < cnt) {
+            if (s < 32) {
+              if (q.valid) dvw = q.w;
+            } else if (!(V2(X[m.item_j[base + s]]).len2() <= 1e-12f)) {
+              dvw = m.item_w[base + s];
+            }
+          }
+          lane_seq_sum1(den, dvw, lim);
+        }
+        float* sl = g_ball_slot[threadIdx.x >> 5];
+        __syncwarp();  // the previous ball's post has read the slot
+        if (lane == 0) {
+          sl[BS_RHO_LOCAL] = rho_local;
+          sl[BS_DEN] = den;
+        } else if (lane <= 2) {
+          sl[BS_XB + lane - 1] = reinterpret_cast<const float*>(m.bx + b)[lane - 1];
+        }
+        return q;
+      },
+      // on the chain: the local rotation rate from the current velocities, the fluid updates
+      [&](uint32_t b, int lane, BuoyBall& q) {
+        if (q.cnt == 0) return;
+        const uint32_t base = b * m.cap_items, cnt = q.cnt;
+        const float* sl = g_ball_slot[threadIdx.x >> 5];
+        const float* K = g_sweep_const;
+        float2* const V_l = V;
+        // the rotation-rate numerator over the valid items in item order (invalid items add -0.0)
+        float num = 0.0f;
+        for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+          const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
+          float nv = -0.0f;
+          if (s < cnt) {
+            if (s < 32) {
+              if (q.valid) nv = q.w * cross2(q.d, V2(V_l[q.j])) / q.d2;
+            } else {
+              uint32_t j = m.item_j[base + s];
+              V2 d(X[j]);
+              float d2 = d.len2();
+              if (!(d2 <= 1e-12f)) nv = m.item_w[base + s] * cross2(d, V2(V_l[j])) / d2;
+            }
+          }
+          lane_seq_sum1(num, nv, lim);
+        }
+        const float rho_local = sl[BS_RHO_LOCAL], den = sl[BS_DEN], om_abs = K[BK_OM_ABS];
+        const float rho_eff = fmin_r(rho_local, K[BK_RHO0]);
+        float omega_local = den > 0.0f ? clamp_r(num / den, -om_abs, om_abs) : 0.0f;
+        V2 g_eff = V2(0.0f, GRAVITY) + omega_local * omega_local * V2(sl[BS_XB], sl[BS_XB + 1]);
+        V2 impulse = -rho_eff * K[BK_AREA] * g_eff * K[BK_DT];
+        const float mass_l = K[BK_MASS];
+        for (uint32_t s = lane; s < cnt; s += 32) {
+          const uint32_t j = s < 32 ? q.j : m.item_j[base + s];
+          float frac = s < 32 ? q.frac : m.item_w[base + s] / rho_local;
+          V2 dv = -(impulse * frac) / mass_l;
+          V_l[j] = (V2(V_l[j]) + dv).f2();
+          if (s < 32) q.dv = dv;
+          else if (want_mom) m.rec_M[m.rec_off[b] + s] = (mass_l * dv).f2();
+        }
+        if (lane == 0) {
+          float* slw = g_ball_slot[threadIdx.x >> 5];
+          slw[BS_IMPULSE] = impulse.x;
+          slw[BS_IMPULSE + 1] = impulse.y;
+        }
+      },
+      // after the flag: the ball's impulse, the momentum records
+      [&](uint32_t b, int lane, BuoyBall& q) {
+        if (q.cnt == 0) return;
+        if (want_mom && (uint32_t)lane < q.cnt) m.rec_M[m.rec_off[b] + lane] = (m.f_mass * q.dv).f2();
+        if (lane == 0) {
+          const float* sl = g_ball_slot[threadIdx.x >> 5];
+          m.imp[b] = (V2(m.imp[b]) + V2(sl[BS_IMPULSE], sl[BS_IMPULSE + 1])).f2();
+        }
+      });
+}
+
+// Step 6.6 (pbf.rs:2035-2122): the buoyancy sweep on the stale step-2 grid, in its own function
+// like the drag sweep. Returns false when the item lists failed (the error is in *err).
+static __device__ __noinline__ bool buoyancy_step(const MillDev& m, const StepUniform& U, StepOut& out,
+                                                  uint32_t* err, FluidShared& S, float2* X, float2* V,
+                                                  uint32_t* done, uint32_t* scratch, uint32_t scratch_words,
+                                                  const uint32_t* drag_order) {
+  const uint32_t n = m.nf, nb = m.nb;
+  if (nb > 0 && m.b_r > 0.0f) {
+    uint32_t n_items = 0;
+    wide_phase(m, WIDE_BUOYANCY_ITEMS, &S.hA, [&](uint32_t w0, uint32_t nw) { n_items += buoyancy_item_balls(m, S.hA, w0, nw); });
+    n_items = block_sum_u(n_items) + wide_counter(m);
+    if (tid() == 0) out.ctr.n_coupling_items += n_items;
+    __syncthreads();
+    if (*err) return false;
+    stage_mark(out.stage, 27);
+    const uint32_t nrec = pack_ball_items(m.item_j, m.item_n, m.cap_items, nb, m.rec_off, m.rec_i, m.rec_b);
+    // Claim order: a buoyancy item (a particle within h of the ball) is a drag item too (within
+    // r + h), so every buoyancy predecessor is reached by a chain of drag predecessors and the drag
+    // sweep's level order (when it ran) is topological here as well; it is checked all the same
+    // (index order otherwise). Without a drag sweep, the buoyancy records' own levels.
+    LevelScratch L;
+    const bool by_level = U.sweep_order == 0 && level_scratch(nb, scratch, scratch_words, L);
+    const bool reuse = by_level && drag_order != nullptr;
+    ball_item_preds(m.rec_i, m.rec_b, nrec, n, nb, m.bk_start, m.bk_cur, m.bk_order, m.rec_pred,
+                    by_level && !reuse ? &L : nullptr);
+    const uint32_t* order = nullptr;
+    if (reuse) order = order_respects(L.pos, m.rec_b, m.rec_pred, nrec) ? drag_order : nullptr;
+    else if (by_level) order = ball_level_order(nb, m.rec_off, m.rec_pred, L);
+    stage_mark(out.stage, 28);
+    buoyancy_sweep(m, U, out, err, X, V, done, order);
+    if (tid() == 0 && U.want_momentum) {
+      V2 mom(S.fscal[0], S.fscal[1]);
+      for (uint32_t r = 0; r < nrec; ++r) mom += V2(m.rec_M[r]);
+      S.fscal[0] = mom.x;
+      S.fscal[1] = mom.y;
+    }
+    __syncthreads();
+    stage_mark(out.stage, 29);
+  }
+  return true;
+}
+
+// Step 7 (pbf.rs:2146-2300): implicit viscosity on the velocities V at positions X (Morris weights,
+// ball boundary groups, squeeze links, the fluid-only or joint fluid + ball CG and the ball
+// impulses from it), in its own function so that it is register-allocated apart from the rest
+// of the fluid step. visc_iters receives the CG iterations. Returns false when a capacity ran out
+// or a grid failed (the error is in *err).
+static __device__ __noinline__ bool viscosity_step(const MillDev& m, const StepUniform& U, StepOut& out,
+                                                  uint32_t* err, FluidShared& S, float2* X, float2* V, float mu,
+                                                  uint32_t& visc_iters) {
+  const uint32_t n = m.nf, nb = m.nb;
+  const float h = m.f_h, rho0 = m.f_rho0, mass = m.f_mass, dt = U.dt;
+  const bool fp64 = U.cg_fp64 != 0;
+  if (mu > 0.0f) {
+    const bool bingham = U.slurry.rheology == MG_RHEOLOGY_BINGHAM && U.slurry.yield_stress_pa > 0.0f;
+    const float tau_y = U.slurry.yield_stress_pa;
+    for (uint32_t i = tid(); i < n; i += nthr()) {
+      float mu_i = mu;
+      if (bingham) {
+        // pbf.rs:821-868 shear rate then Papanastasiou viscosity
+        V2 xi(X[i]), vi(V[i]);
+        float gxx = 0.0f, gxy = 0.0f, gyx = 0.0f, gyy = 0.0f;
+        for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
+          uint32_t j = m.nbrs[k];
+          V2 delta = xi - V2(X[j]);
+          float r = delta.len();
+          V2 grad = spiky_grad(delta, r, h);
+          float coeff = mass / fmax_r(m.density[j], 1e-6f);
+          V2 dv = V2(V[j]) - vi;
+          gxx += coeff * dv.x * grad.x;
+          gxy += coeff * dv.x * grad.y;
+          gyx += coeff * dv.y * grad.x;
+          gyy += coeff * dv.y * grad.y;
+        }
+        float dxy = 0.5f * (gxy + gyx);
+        float g = sqrtf(2.0f * (gxx * gxx + gyy * gyy + 2.0f * dxy * dxy));
+        float gamma0 = tau_y / (100.0f * mu);
+        g = finite_f(g) ? g : 0.0f;
+        float extra = g < 1e-4f * gamma0 ? tau_y / gamma0 : tau_y * (1.0f - expf_r(-g / gamma0)) / g;
+        mu_i = mu + extra;
+      }
+      m.mu_eff[i] = mu_i;
+    }
+    __syncthreads();
+    const float eta2 = VISC_ETA * h * h;
+    for (uint32_t i = tid(); i < n; i += nthr()) {
+      V2 xi(X[i]);
+      float rho_i = fmax_r(m.density[i], 1e-6f);
+      float mu_i = m.mu_eff[i];
+      for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
+        uint32_t j = m.nbrs[k];
+        float rho_j = fmax_r(m.density[j], 1e-6f);
+        V2 delta = xi - V2(X[j]);
+        float r = delta.len();
+        V2 grad = spiky_grad(delta, r, h);
+        float numerator = (mass * (mu_i + m.mu_eff[j]) / (rho_i * rho_j)) * fabsf(delta.dot(grad));
+        m.visc_w[k] = numerator / (delta.len2() + eta2);
+        m.visc_dir[k] = (r > 1e-9f ? delta / r : V2(1.0f, 0.0f)).f2();
+      }
+    }
+    __syncthreads();
+    stage_mark(out.stage, 8);
+    // boundary groups (pbf.rs:2159-2232) on a fresh h-grid, one ball per thread, merged per fluid
+    if (tid() == 0) { S.n_groups = 0; S.n_links = 0; S.links_in_range = 0; }
+    __syncthreads();
+    if (nb > 0 && m.b_r > 0.0f) {
+      grid_build(X, n, h, m.gB, S.hB, err);
+      for (uint32_t j = tid(); j < n; j += nthr())
+        m.f_tmp[j] = BALL_BC_GAIN * (mass * 2.0f * m.mu_eff[j] / (fmax_r(m.density[j], 1e-6f) * rho0));
+      __syncthreads();
+      wide_phase(m, WIDE_GROUPS, &S.hB, [&](uint32_t w0, uint32_t nw) { group_balls(m, U, S.hB, w0, nw); });
+      if (tid() == 0) m.g_off[nb] = 0;
+      __syncthreads();
+      if (*err) return false;
+      uint32_t ng = block_exclusive_scan(m.g_off, nb + 1);
+      if (ng > m.cap_groups) { if (tid() == 0) atomicOr(err, ERR_GROUPS); __syncthreads(); return false; }
+      for (uint32_t b = tid() >> 5; b < nb; b += nthr() >> 5) {
+        const uint32_t base = b * m.cap_items, o = m.g_off[b], cnt = m.g_off[b + 1] - o;
+        for (uint32_t s = tid() & 31u; s < cnt; s += 32) {
+          m.g_fluid[o + s] = m.item_j[base + s];
+          m.g_ball[o + s] = b;
+          m.g_c[o + s] = m.item_w[base + s];
+          m.g_lc[o + s] = m.item_v[base + s];
+          m.g_l2[o + s] = m.item_w2[base + s];
+        }
+      }
+      if (tid() == 0) S.n_groups = ng;
+      __syncthreads();
+    }
+    stage_mark(out.stage, 9);
+    // ball_v0 (pbf.rs:2237-2239) and squeeze links (pbf.rs:544-625)
+    for (uint32_t b = tid(); b < nb; b += nthr()) {
+      m.ball_v0[b] = (V2(m.bv[b]) + V2(m.imp[b]) / m.b_m).f2();
+      m.ball_w0[b] = m.bom[b] + m.ang[b] / m.b_I;
+    }
+    __syncthreads();
+    if (nb > 0 && m.b_r > 0.0f) {
+      const float r = m.b_r;
+      const double dxd = (double)(0.5f * h);
+      const float reach = (float)(8.0 * dxd);
+      grid_build(m.bx, nb, 2.0f * r + reach, m.gBall, S.hBall, err);
+      uint32_t in_range = 0;
+      // ball i's links go to its slots [i K, i K + K) of the record scratch, then one compaction
+      // copies them to the link list in ball order
+      const uint32_t K = min(nb + 1u, 512u);
+      wide_phase(m, WIDE_LINKS, &S.hBall,
+                 [&](uint32_t w0, uint32_t nw) { in_range += link_balls(m, U, S.hBall, w0, nw); });
+      if (tid() == 0) m.l_off[nb] = 0;
+      __syncthreads();
+      const uint32_t tot_in = block_sum_u(in_range) + wide_counter(m);
+      const uint32_t nl = block_exclusive_scan(m.l_off, nb + 1);
+      if (nl > m.cap_links) { if (tid() == 0) atomicOr(err, ERR_LINKS); __syncthreads(); return false; }
+      if (tid() == 0) { S.n_links = nl; S.links_in_range = tot_in; }
+      for (uint32_t i = tid() >> 5; i < nb; i += nthr() >> 5) {
+        const uint32_t o = m.l_off[i], cnt = m.l_off[i + 1] - o, base = i * K;
+        for (uint32_t q = tid() & 31u; q < cnt; q += 32) {
+          m.l_ball[o + q] = i;
+          m.l_other[o + q] = m.rec_i[base + q];
+          m.l_n[o + q] = m.rec_J[base + q];
+          m.l_c[o + q] = m.rec_L[base + q];
+        }
+      }
+      __syncthreads();
+    }
+    if (tid() == 0) {
+      out.ctr.n_groups = S.n_groups;
+      out.ctr.n_links = S.n_links;
+      out.ctr.links_in_range = S.links_in_range;
+    }
+    __syncthreads();
+    stage_mark(out.stage, 10);
+    if (S.n_groups == 0 && S.links_in_range == 0) {
+      // ---- fluid-only CG (pbf.rs:423-480), solution in place in V
+      float2 *r = m.cg_r, *p = m.cg_p, *ap = m.cg_ap;
+      double bn2 = block_dot(V, V, n, fp64, S);
+      double b_norm = fp64 ? sqrt(bn2) : (double)sqrtf((float)bn2);
+      if (b_norm > 0.0 && isfinite(b_norm)) {
+        const float target_f = VISC_CG_TOL * (float)b_norm;
+        const double target_d = (double)VISC_CG_TOL * b_norm;
+        auto apply = [&](const float2* in, float2* o) {
+          for (uint32_t i = tid(); i < n; i += nthr()) o[i] = (V2(in[i]) + dt * laplacian_row(m, in, i)).f2();
+          __syncthreads();
+        };
+        apply(V, m.cg_ap);
+        for (uint32_t i = tid(); i < n; i += nthr()) { r[i] = (V2(V[i]) - V2(ap[i])).f2(); p[i] = r[i]; }
+        __syncthreads();
+        double rs_old = block_dot(r, r, n, fp64, S);
+        bool done = fp64 ? sqrt(rs_old) <= target_d : sqrtf((float)rs_old) <= target_f;
+        if (!done) {
+          visc_iters = VISC_CG_MAX;
+          for (uint32_t it = 1; it <= VISC_CG_MAX; ++it) {
+            apply(p, ap);
+            double p_ap = block_dot(p, ap, n, fp64, S);
+            if (p_ap <= 0.0 || !isfinite(p_ap)) { visc_iters = it; break; }
+            float alpha = fp64 ? (float)(rs_old / p_ap) : (float)rs_old / (float)p_ap;
+            for (uint32_t i = tid(); i < n; i += nthr()) {
+              V[i] = (V2(V[i]) + alpha * V2(p[i])).f2();
+              r[i] = (V2(r[i]) - alpha * V2(ap[i])).f2();
+            }
+            __syncthreads();
+            double rs_new = block_dot(r, r, n, fp64, S);
+            bool conv = fp64 ? sqrt(rs_new) <= target_d : sqrtf((float)rs_new) <= target_f;
+            if (conv) { visc_iters = it; break; }
+            float bt = fp64 ? (float)(rs_new / rs_old) : (float)rs_new / (float)rs_old;
+            for (uint32_t i = tid(); i < n; i += nthr()) p[i] = (V2(r[i]) + bt * V2(p[i])).f2();
+            __syncthreads();
+            rs_old = rs_new;
+          }
+        }
+      }
+    } else {
+      // ---- joint fluid + ball Jacobi-PCG (pbf.rs:641-791)
+      const uint32_t len = n + 2 * nb;
+      // per-fluid group lists and per-ball "other" link lists (stable, in group / link order)
+      for (uint32_t g = tid(); g < S.n_groups; g += nthr()) m.rec_i[g] = m.g_fluid[g];
+      __syncthreads();
+      block_bucket_sort(m.rec_i, S.n_groups, n, m.fg_start, m.bk_start, m.fg_list);
+      for (uint32_t l = tid(); l < S.n_links; l += nthr()) m.rec_b[l] = m.l_other[l] == NONE ? nb : m.l_other[l];
+      __syncthreads();
+      block_bucket_sort(m.rec_b, S.n_links, nb + 1, m.lo_start, m.bk_start, m.lo_list);
+      float2 *x = m.cg_x, *bvec = m.cg_b, *r = m.cg_r, *z = m.cg_z, *p = m.cg_p, *ap = m.cg_ap;
+      float *diag = m.cg_diag, *inv = m.cg_inv;
+      wide_phase(m, WIDE_CG_SETUP, nullptr, [&](uint32_t w0, uint32_t nw) {
+        cg_setup_rows(m, dt, w0 * 32u + (tid() & 31u), nw * 32u);
+      });
+      for (uint32_t e = tid(); e < len; e += nthr()) inv[e] = 1.0f / fmax_r(diag[e], 1e-20f);
+      __syncthreads();
+      joint_apply(m, dt, x, ap);
+      for (uint32_t e = tid(); e < len; e += nthr()) {
+        V2 re = V2(bvec[e]) - V2(ap[e]);
+        r[e] = re.f2();
+        z[e] = (re * inv[e]).f2();
+      }
+      __syncthreads();
+      double b_norm = block_res_norm(bvec, inv, len, fp64, S);
+      double r_norm = block_res_norm(r, inv, len, fp64, S);
+      stage_mark(out.stage, 23);
+      double tol_b = fp64 ? (double)VISC_CG_TOL * b_norm : (double)(VISC_CG_TOL * (float)b_norm);
+      if (b_norm > 0.0 && isfinite(b_norm) && r_norm > tol_b) {
+        for (uint32_t e = tid(); e < len; e += nthr()) p[e] = z[e];
+        __syncthreads();
+        double rz_old = block_dot(r, z, len, fp64, S);
+        for (uint32_t it = 1; it <= 4 * VISC_CG_MAX; ++it) {
+          visc_iters = it;
+          joint_apply(m, dt, p, ap);
+          double p_ap = block_dot(p, ap, len, fp64, S);
+          if (p_ap <= 0.0 || !isfinite(p_ap)) break;
+          float alpha = fp64 ? (float)(rz_old / p_ap) : (float)rz_old / (float)p_ap;
+          for (uint32_t e = tid(); e < len; e += nthr()) {
+            x[e] = (V2(x[e]) + alpha * V2(p[e])).f2();
+            r[e] = (V2(r[e]) - alpha * V2(ap[e])).f2();
+          }
+          __syncthreads();
+          if (block_res_norm(r, inv, len, fp64, S) <= tol_b) break;
+          for (uint32_t e = tid(); e < len; e += nthr()) z[e] = (V2(r[e]) * inv[e]).f2();
+          __syncthreads();
+          double rz_new = block_dot(r, z, len, fp64, S);
+          float bt = fp64 ? (float)(rz_new / rz_old) : (float)rz_new / (float)rz_old;
+          for (uint32_t e = tid(); e < len; e += nthr()) p[e] = (V2(z[e]) + bt * V2(p[e])).f2();
+          __syncthreads();
+          rz_old = rz_new;
+        }
+      }
+      stage_mark(out.stage, 31);
+      for (uint32_t i = tid(); i < n; i += nthr()) {
+        V2 vn(x[i]);
+        V[i] = vn.f2();
+        V2 d = vn - V2(m.dv_tmp[i]);
+        m.fguess[i] = (d.finite() ? d : V2()).f2();
+      }
+      __syncthreads();
+      // ball impulses from the solved velocities (pbf.rs:2237-2298), one thread per ball
+      for (uint32_t b = tid(); b < nb; b += nthr()) {
+        V2 dv = V2(x[n + b]) - V2(m.ball_v0[b]);
+        float dw = x[n + nb + b].x - m.ball_w0[b];
+        if (dv.finite() && finite_f(dw)) {
+          m.imp[b] = (V2(m.imp[b]) + m.b_m * dv).f2();
+          m.ang[b] += m.b_I * dw;
+        }
+      }
+      if (tid() == 0) m.guess_valid_dev[0] = 1u;
+      if (U.want_momentum && tid() < 32) {
+        // the fluid's momentum change loses b_m * dv per ball, in ball order (a - t == a + (-t))
+        auto term = [&](uint32_t b, float& t, int c) {
+          V2 dv = V2(x[n + b]) - V2(m.ball_v0[b]);
+          float dw = x[n + nb + b].x - m.ball_w0[b];
+          if (!(dv.finite() && finite_f(dw))) return false;
+          V2 p = m.b_m * dv;
+          t = -(c ? p.y : p.x);
+          return true;
+        };
+        const float mx = warp_ordered_sum(S.fscal[0], nb, [&](uint32_t b, float& t) { return term(b, t, 0); });
+        const float my = warp_ordered_sum(S.fscal[1], nb, [&](uint32_t b, float& t) { return term(b, t, 1); });
+        if (tid() == 0) {
+          S.fscal[0] = mx;
+          S.fscal[1] = my;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  return true;
+}
+
 static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err, FluidShared& S,
                            unsigned char* dsm) {
   uint32_t* done = m.ball_done;  // completion flags of the per-ball sweeps (moved to shared below)
@@ -1035,11 +1676,15 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
   // step 6.6. X does not change in between.
   float2* Vg = V;
   float2* Xg = X;
+  uint32_t* sweep_scratch = nullptr;  // the rest of the region: the sweeps' claim orders
+  uint32_t sweep_words = 0;
   if (16u * n + 4u * nb + 64u <= m.smem_bytes) {
     float2* sX = reinterpret_cast<float2*>(dsm);
     float2* sV = sX + n;
     for (uint32_t i = tid(); i < n; i += nthr()) { sX[i] = Xg[i]; sV[i] = Vg[i]; }
     done = reinterpret_cast<uint32_t*>(sV + n);
+    sweep_scratch = done + nb;
+    sweep_words = (m.smem_bytes - (16u * n + 4u * nb)) / 4u;
     X = sX;
     V = sV;
     __syncthreads();
@@ -1048,296 +1693,14 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
   }
   // ---- step 6.5: ball drag, Gauss-Seidel over balls (pbf.rs:1777-2013)
   const float mu = fmax_r(U.slurry.viscosity_pa_s, 0.0f);
-  if (nb > 0 && m.b_r > 0.0f && m.b_rtrue > 0.0f && mu > 1e-6f) {
-    const float beta_b = clamp_r(U.slurry.ball_no_slip, 0.0f, 1.0f);
-    const float rot_cap = 0.2f * fluid_vmax(U);
-    const float rho_ball = m.b_m / (PI_F * m.b_r * m.b_r);
-    const float mass_true = rho_ball * PI_F * m.b_rtrue * m.b_rtrue;
-    if (beta_b > 0.0f) {
-      const float h_c = m.b_r + h;
-      const float w_hc0 = fmax_r(poly6(0.0f, h_c), 1e-12f);
-      grid_build(X, n, fmax_r(h_c, 1e-6f), m.gB, S.hB, err);
-      // item lists per ball in for_each_near order (positions do not change during the sweep):
-      // one warp per ball, an ordered compaction of each 32-candidate chunk
-      uint32_t n_items = 0;
-      wide_phase(m, WIDE_DRAG_ITEMS, &S.hB, [&](uint32_t w0, uint32_t nw) { n_items += drag_item_balls(m, S.hB, w0, nw); });
-      n_items = block_sum_u(n_items) + wide_counter(m);
-      if (tid() == 0) out.ctr.n_coupling_items += n_items;
-      __syncthreads();
-      if (*err) return;
-      stage_mark(out.stage, 24);
-      const uint32_t nrec = pack_ball_items(m.item_j, m.item_n, m.cap_items, nb, m.rec_off, m.rec_i, m.rec_b);
-      ball_item_preds(m.rec_i, m.rec_b, nrec, n, m.bk_start, m.bk_cur, m.bk_order, m.rec_pred);
-      stage_mark(out.stage, 25);
-      wide_phase(m, WIDE_DRAG_PRE, nullptr, [&](uint32_t w0, uint32_t nw) { drag_pre_balls(m, w0, nw); });
-      const float i_b = m.b_I;
-      const bool want_mom = U.want_momentum != 0;
-      // Lane l holds item l of the ball (items from 32 on are read from the lists when needed).
-      struct DragBall {
-        uint32_t cnt, j;
-        V2 r_i;
-        float phi, m_ent, i_ent, s_acc, s_scale;
-        V2 r_bar, p_bar, vb;
-        float omb;
-        V2 dv_b, dv_i;
-        float dw_b;
-        bool live;
-      };
-      auto item_r = [&](const DragBall& q, uint32_t base, uint32_t s) { return s < 32 ? q.r_i : V2(m.item_v[base + s]); };
-      auto item_phi = [&](const DragBall& q, uint32_t base, uint32_t s) { return s < 32 ? q.phi : m.item_w[base + s]; };
-      auto item_j = [&](const DragBall& q, uint32_t base, uint32_t s) { return s < 32 ? q.j : m.item_j[base + s]; };
-      ball_dataflow(
-          nb, m.rec_off, m.rec_pred, done, U.sweep_warps, U.spin_ns, U.spin_limit, U.skip_done_ball, err, &out.stage[32],
-          // before the wait: the item data and the geometry-only quantities computed for every ball
-          // ahead of the sweep (drag_pre_balls)
-          [&](uint32_t b, int lane) {
-            DragBall q;
-            q.cnt = m.item_n[b];
-            q.live = false;
-            q.j = 0;
-            q.phi = 0.0f;
-            if (q.cnt == 0) return q;
-            const uint32_t base = b * m.cap_items, cnt = q.cnt;
-            if ((uint32_t)lane < cnt) {
-              q.j = m.item_j[base + lane];
-              q.r_i = V2(m.item_v[base + lane]);
-              q.phi = m.item_w[base + lane];
-            }
-            q.vb = V2(m.bv[b]);
-            q.omb = m.bom[b];
-            const float* P = m.drag_pre + 8u * b;
-            q.m_ent = P[0];
-            q.i_ent = P[1];
-            if (q.m_ent <= 1e-12f) return q;
-            q.live = true;
-            q.r_bar = V2(P[2], P[3]);
-            q.s_acc = P[4];
-            q.s_scale = P[5];
-            if (q.i_ent > 1e-12f) q.p_bar = V2(-q.r_bar.y, q.r_bar.x);
-            return q;
-          },
-          // on the chain: entrained velocity and angular momentum, the relaxation, the fluid updates
-          [&](uint32_t b, int lane, DragBall& q) {
-            if (!q.live) return;
-            // descriptor fields in registers (stores through V would otherwise force reloads)
-            const uint32_t base = b * m.cap_items, cnt = q.cnt;
-            const float b_m = m.b_m, b_rtrue = m.b_rtrue;
-            float2* const Vl = V;
-            // the enclosing scope's constants as locals of this body (one load each, up front)
-            const float mass_l = mass, rho0_l = rho0, mass_true_l = mass_true, beta_l = beta_b, dt_l = dt;
-            const float i_b_l = i_b, h_c_l = h_c, rot_cap_l = rot_cap;
-            float l_sum = 0.0f, vsx = 0.0f, vsy = 0.0f;
-            for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
-              const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
-              float lw = 0.0f;
-              V2 vw;
-              if (s < cnt) {
-                V2 r_i = item_r(q, base, s);
-                V2 vj(Vl[item_j(q, base, s)]);
-                float w = mass_l * item_phi(q, base, s);
-                vw = w * vj;
-                lw = w * cross2(r_i, vj);
-              }
-              lane_seq_sum3(vsx, vsy, l_sum, vw.x, vw.y, lw, lim);
-            }
-            const float m_ent = q.m_ent, i_ent = q.i_ent;
-            V2 v_bar = V2(vsx, vsy) / m_ent;
-            V2 v_rel = v_bar - q.vb;
-            float speed_rel = v_rel.len();
-            float inv_tau_form = (speed_rel > 1e-6f && rho0_l > 0.0f)
-                                     ? 0.5f * rho0_l * 1.0f * (2.0f * b_rtrue) * speed_rel / mass_true_l
-                                     : 0.0f;
-            float bt = beta_l * (1.0f - expf_r(-dt_l * (0.0f + inv_tau_form)));
-            float a_lin = bt * m_ent / (b_m + m_ent);
-            V2 dv_b = a_lin * v_rel;
-            float dw_b = 0.0f, c_rot = 0.0f;
-            if (i_ent > 1e-12f) {
-              float omega_bar = l_sum / i_ent;
-              float a_rot = bt * i_ent / (i_b_l + i_ent);
-              float candidate_dw = a_rot * (omega_bar - q.omb);
-              if (fabsf(q.s_acc) > 0.1f * q.s_scale) {
-                float raw_c_rot = -i_b_l * candidate_dw / q.s_acc;
-                float max_lever = 2.0f * h_c_l;
-                float cap = max_lever > 1e-9f ? rot_cap_l / max_lever : 0.0f;
-                c_rot = clamp_r(raw_c_rot, -cap, cap);
-                dw_b = -c_rot * q.s_acc / i_b_l;
-              }
-            }
-            for (uint32_t s = lane; s < cnt; s += 32) {
-              const uint32_t j = item_j(q, base, s);
-              V2 r_i = item_r(q, base, s);
-              float phi = item_phi(q, base, s);
-              V2 dv_i = -(b_m / m_ent) * dv_b * phi;
-              if (c_rot != 0.0f) {
-                V2 perp_i(-r_i.y, r_i.x);
-                dv_i += c_rot * phi * (perp_i - q.p_bar);
-              }
-              Vl[j] = (V2(Vl[j]) + dv_i).f2();
-              if (s < 32) q.dv_i = dv_i;
-              else if (want_mom) m.rec_M[m.rec_off[b] + s] = (mass_l * dv_i).f2();
-            }
-            q.dv_b = dv_b;
-            q.dw_b = dw_b;
-          },
-          // after the flag: the ball's impulse and angular impulse, the momentum records
-          [&](uint32_t b, int lane, DragBall& q) {
-            if (!q.live) return;
-            if (want_mom && (uint32_t)lane < q.cnt) m.rec_M[m.rec_off[b] + lane] = (mass * q.dv_i).f2();
-            if (lane == 0) {
-              m.imp[b] = (V2(m.imp[b]) + m.b_m * q.dv_b).f2();
-              m.ang[b] += i_b * q.dw_b + m.b_m * cross2(q.r_bar, q.dv_b);
-              m.item_n[b] = q.cnt | 0x80000000u;  // mark: contributed fluid momentum records
-            }
-          });
-      if (tid() == 0 && U.want_momentum) {
-        V2 mom(S.fscal[0], S.fscal[1]);
-        for (uint32_t b = 0; b < nb; ++b) {
-          if (!(m.item_n[b] & 0x80000000u)) continue;
-          for (uint32_t r = m.rec_off[b]; r < m.rec_off[b + 1]; ++r) mom += V2(m.rec_M[r]);
-        }
-        S.fscal[0] = mom.x;
-        S.fscal[1] = mom.y;
-      }
-      __syncthreads();
-      stage_mark(out.stage, 26);
-    }
-  }
+  const uint32_t* drag_order = nullptr;  // the drag sweep's claim order, when it ran by level
+  if (!drag_step(m, U, out, err, S, X, V, done, sweep_scratch, sweep_words, &drag_order)) return;
   stage_mark(out.stage, 19);
   double ke_after_drag = kinetic_energy_seq(V, n, mass, S);
   const double ke_delta_drag = ke_after_drag - ke_mark;
   ke_mark = ke_after_drag;
   // ---- step 6.6: buoyancy, Gauss-Seidel over balls on the stale step-2 grid (pbf.rs:2035-2122)
-  if (nb > 0 && m.b_r > 0.0f) {
-    const float area = PI_F * m.b_r * m.b_r;
-    uint32_t n_items = 0;
-    wide_phase(m, WIDE_BUOYANCY_ITEMS, &S.hA, [&](uint32_t w0, uint32_t nw) { n_items += buoyancy_item_balls(m, S.hA, w0, nw); });
-    n_items = block_sum_u(n_items) + wide_counter(m);
-    if (tid() == 0) out.ctr.n_coupling_items += n_items;
-    __syncthreads();
-    if (*err) return;
-    stage_mark(out.stage, 27);
-    const uint32_t nrec = pack_ball_items(m.item_j, m.item_n, m.cap_items, nb, m.rec_off, m.rec_i, m.rec_b);
-    ball_item_preds(m.rec_i, m.rec_b, nrec, n, m.bk_start, m.bk_cur, m.bk_order, m.rec_pred);
-    stage_mark(out.stage, 28);
-    const float om_abs = fabsf(U.drum_omega);
-    const bool want_mom = U.want_momentum != 0;
-    // Lane l holds item l of the ball (items from 32 on are read from the lists when needed).
-    struct BuoyBall {
-      uint32_t cnt, j;
-      float w, rho_local, d2, den;
-      V2 d, xb, impulse, dv;
-      bool valid;
-    };
-    ball_dataflow(
-        nb, m.rec_off, m.rec_pred, done, U.sweep_warps, U.spin_ns, U.spin_limit, NONE, err, &out.stage[35],
-        // before the wait: item geometry and the weight sum, which the sweep does not change
-        [&](uint32_t b, int lane) {
-          BuoyBall q;
-          q.cnt = m.item_n[b];
-          q.j = 0;
-          q.w = 0.0f;
-          q.valid = false;
-          if (q.cnt == 0) return q;
-          const uint32_t base = b * m.cap_items, cnt = q.cnt;
-          q.rho_local = m.item_v[base].x;
-          q.xb = V2(m.bx[b]);
-          if ((uint32_t)lane < cnt) {
-            q.j = m.item_j[base + lane];
-            q.w = m.item_w[base + lane];
-            q.d = V2(X[q.j]);
-            q.d2 = q.d.len2();
-            q.valid = !(q.d2 <= 1e-12f);
-          }
-          float den = 0.0f;
-          for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
-            const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
-            bool valid = false;
-            float dvw = 0.0f;
-            if (s < cnt) {
-              if (s < 32) {
-                valid = q.valid;
-                dvw = q.w;
-              } else {
-                float d2 = V2(X[m.item_j[base + s]]).len2();
-                valid = !(d2 <= 1e-12f);
-                dvw = m.item_w[base + s];
-              }
-            }
-            const uint32_t vmask = __ballot_sync(FULL, valid);
-#pragma unroll
-            for (uint32_t t = 0; t < 32; ++t) {
-              // vmask has no bits from lim on
-              const float c = __shfl_sync(FULL, dvw, t);
-              if ((vmask >> t) & 1u) den += c;
-            }
-          }
-          q.den = den;
-          return q;
-        },
-        // on the chain: the local rotation rate from the current velocities, the fluid updates
-        [&](uint32_t b, int lane, BuoyBall& q) {
-          if (q.cnt == 0) return;
-          const uint32_t base = b * m.cap_items, cnt = q.cnt;
-          // this body's constants and pointers as locals (they stay in registers)
-          float2* const X_l = X;
-          float2* const V_l = V;
-          const float rho0_l = rho0, om_abs_l = om_abs, area_l = area, dt_l = dt, mass_l = mass;
-          const float rho_local = q.rho_local;
-          const float rho_eff = fmin_r(rho_local, rho0_l);
-          float num = 0.0f;
-          for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
-            const uint32_t s = c0 + lane, lim = min(32u, cnt - c0);
-            float nv = 0.0f;
-            bool valid = false;
-            if (s < cnt) {
-              if (s < 32) {
-                valid = q.valid;
-                nv = q.w * cross2(q.d, V2(V_l[q.j])) / q.d2;
-              } else {
-                uint32_t j = m.item_j[base + s];
-                V2 d(X_l[j]);
-                float d2 = d.len2();
-                valid = !(d2 <= 1e-12f);
-                nv = m.item_w[base + s] * cross2(d, V2(V_l[j])) / d2;
-              }
-            }
-            const uint32_t vmask = __ballot_sync(FULL, valid);
-#pragma unroll
-            for (uint32_t t = 0; t < 32; ++t) {
-              // vmask has no bits from lim on
-              const float a = __shfl_sync(FULL, nv, t);
-              if ((vmask >> t) & 1u) num += a;
-            }
-          }
-          const float den = q.den;
-          float omega_local = den > 0.0f ? clamp_r(num / den, -om_abs_l, om_abs_l) : 0.0f;
-          V2 g_eff = V2(0.0f, GRAVITY) + omega_local * omega_local * q.xb;
-          V2 impulse = -rho_eff * area_l * g_eff * dt_l;
-          for (uint32_t s = lane; s < cnt; s += 32) {
-            const uint32_t j = s < 32 ? q.j : m.item_j[base + s];
-            float frac = (s < 32 ? q.w : m.item_w[base + s]) / rho_local;
-            V2 dv = -(impulse * frac) / mass_l;
-            V_l[j] = (V2(V_l[j]) + dv).f2();
-            if (s < 32) q.dv = dv;
-            else if (want_mom) m.rec_M[m.rec_off[b] + s] = (mass_l * dv).f2();
-          }
-          q.impulse = impulse;
-        },
-        // after the flag: the ball's impulse, the momentum records
-        [&](uint32_t b, int lane, BuoyBall& q) {
-          if (q.cnt == 0) return;
-          if (want_mom && (uint32_t)lane < q.cnt) m.rec_M[m.rec_off[b] + lane] = (mass * q.dv).f2();
-          if (lane == 0) m.imp[b] = (V2(m.imp[b]) + q.impulse).f2();
-        });
-    if (tid() == 0 && U.want_momentum) {
-      V2 mom(S.fscal[0], S.fscal[1]);
-      for (uint32_t r = 0; r < nrec; ++r) mom += V2(m.rec_M[r]);
-      S.fscal[0] = mom.x;
-      S.fscal[1] = mom.y;
-    }
-    __syncthreads();
-    stage_mark(out.stage, 29);
-  }
+  if (!buoyancy_step(m, U, out, err, S, X, V, done, sweep_scratch, sweep_words, drag_order)) return;
   double ke_after_buoy = kinetic_energy_seq(V, n, mass, S);
   const double ke_delta_buoy = ke_after_buoy - ke_mark;
   ke_mark = ke_after_buoy;
@@ -1359,255 +1722,7 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
   stage_mark(out.stage, 7);
   // ---- step 7: implicit viscosity (pbf.rs:2146-2300)
   uint32_t visc_iters = 0;
-  const bool fp64 = U.cg_fp64 != 0;
-  if (mu > 0.0f) {
-    const bool bingham = U.slurry.rheology == MG_RHEOLOGY_BINGHAM && U.slurry.yield_stress_pa > 0.0f;
-    const float tau_y = U.slurry.yield_stress_pa;
-    for (uint32_t i = tid(); i < n; i += nthr()) {
-      float mu_i = mu;
-      if (bingham) {
-        // pbf.rs:821-868 shear rate then Papanastasiou viscosity
-        V2 xi(X[i]), vi(V[i]);
-        float gxx = 0.0f, gxy = 0.0f, gyx = 0.0f, gyy = 0.0f;
-        for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
-          uint32_t j = m.nbrs[k];
-          V2 delta = xi - V2(X[j]);
-          float r = delta.len();
-          V2 grad = spiky_grad(delta, r, h);
-          float coeff = mass / fmax_r(m.density[j], 1e-6f);
-          V2 dv = V2(V[j]) - vi;
-          gxx += coeff * dv.x * grad.x;
-          gxy += coeff * dv.x * grad.y;
-          gyx += coeff * dv.y * grad.x;
-          gyy += coeff * dv.y * grad.y;
-        }
-        float dxy = 0.5f * (gxy + gyx);
-        float g = sqrtf(2.0f * (gxx * gxx + gyy * gyy + 2.0f * dxy * dxy));
-        float gamma0 = tau_y / (100.0f * mu);
-        g = finite_f(g) ? g : 0.0f;
-        float extra = g < 1e-4f * gamma0 ? tau_y / gamma0 : tau_y * (1.0f - expf_r(-g / gamma0)) / g;
-        mu_i = mu + extra;
-      }
-      m.mu_eff[i] = mu_i;
-    }
-    __syncthreads();
-    const float eta2 = VISC_ETA * h * h;
-    for (uint32_t i = tid(); i < n; i += nthr()) {
-      V2 xi(X[i]);
-      float rho_i = fmax_r(m.density[i], 1e-6f);
-      float mu_i = m.mu_eff[i];
-      for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
-        uint32_t j = m.nbrs[k];
-        float rho_j = fmax_r(m.density[j], 1e-6f);
-        V2 delta = xi - V2(X[j]);
-        float r = delta.len();
-        V2 grad = spiky_grad(delta, r, h);
-        float numerator = (mass * (mu_i + m.mu_eff[j]) / (rho_i * rho_j)) * fabsf(delta.dot(grad));
-        m.visc_w[k] = numerator / (delta.len2() + eta2);
-        m.visc_dir[k] = (r > 1e-9f ? delta / r : V2(1.0f, 0.0f)).f2();
-      }
-    }
-    __syncthreads();
-    stage_mark(out.stage, 8);
-    // boundary groups (pbf.rs:2159-2232) on a fresh h-grid, one ball per thread, merged per fluid
-    if (tid() == 0) { S.n_groups = 0; S.n_links = 0; S.links_in_range = 0; }
-    __syncthreads();
-    if (nb > 0 && m.b_r > 0.0f) {
-      grid_build(X, n, h, m.gB, S.hB, err);
-      for (uint32_t j = tid(); j < n; j += nthr())
-        m.f_tmp[j] = BALL_BC_GAIN * (mass * 2.0f * m.mu_eff[j] / (fmax_r(m.density[j], 1e-6f) * rho0));
-      __syncthreads();
-      wide_phase(m, WIDE_GROUPS, &S.hB, [&](uint32_t w0, uint32_t nw) { group_balls(m, U, S.hB, w0, nw); });
-      if (tid() == 0) m.g_off[nb] = 0;
-      __syncthreads();
-      if (*err) return;
-      uint32_t ng = block_exclusive_scan(m.g_off, nb + 1);
-      if (ng > m.cap_groups) { if (tid() == 0) atomicOr(err, ERR_GROUPS); __syncthreads(); return; }
-      for (uint32_t b = tid() >> 5; b < nb; b += nthr() >> 5) {
-        const uint32_t base = b * m.cap_items, o = m.g_off[b], cnt = m.g_off[b + 1] - o;
-        for (uint32_t s = tid() & 31u; s < cnt; s += 32) {
-          m.g_fluid[o + s] = m.item_j[base + s];
-          m.g_ball[o + s] = b;
-          m.g_c[o + s] = m.item_w[base + s];
-          m.g_lc[o + s] = m.item_v[base + s];
-          m.g_l2[o + s] = m.item_w2[base + s];
-        }
-      }
-      if (tid() == 0) S.n_groups = ng;
-      __syncthreads();
-    }
-    stage_mark(out.stage, 9);
-    // ball_v0 (pbf.rs:2237-2239) and squeeze links (pbf.rs:544-625)
-    for (uint32_t b = tid(); b < nb; b += nthr()) {
-      m.ball_v0[b] = (V2(m.bv[b]) + V2(m.imp[b]) / m.b_m).f2();
-      m.ball_w0[b] = m.bom[b] + m.ang[b] / m.b_I;
-    }
-    __syncthreads();
-    if (nb > 0 && m.b_r > 0.0f) {
-      const float r = m.b_r;
-      const double dxd = (double)(0.5f * h);
-      const float reach = (float)(8.0 * dxd);
-      grid_build(m.bx, nb, 2.0f * r + reach, m.gBall, S.hBall, err);
-      uint32_t in_range = 0;
-      // ball i's links go to its slots [i K, i K + K) of the record scratch, then one compaction
-      // copies them to the link list in ball order
-      const uint32_t K = min(nb + 1u, 512u);
-      wide_phase(m, WIDE_LINKS, &S.hBall,
-                 [&](uint32_t w0, uint32_t nw) { in_range += link_balls(m, U, S.hBall, w0, nw); });
-      if (tid() == 0) m.l_off[nb] = 0;
-      __syncthreads();
-      const uint32_t tot_in = block_sum_u(in_range) + wide_counter(m);
-      const uint32_t nl = block_exclusive_scan(m.l_off, nb + 1);
-      if (nl > m.cap_links) { if (tid() == 0) atomicOr(err, ERR_LINKS); __syncthreads(); return; }
-      if (tid() == 0) { S.n_links = nl; S.links_in_range = tot_in; }
-      for (uint32_t i = tid() >> 5; i < nb; i += nthr() >> 5) {
-        const uint32_t o = m.l_off[i], cnt = m.l_off[i + 1] - o, base = i * K;
-        for (uint32_t q = tid() & 31u; q < cnt; q += 32) {
-          m.l_ball[o + q] = i;
-          m.l_other[o + q] = m.rec_i[base + q];
-          m.l_n[o + q] = m.rec_J[base + q];
-          m.l_c[o + q] = m.rec_L[base + q];
-        }
-      }
-      __syncthreads();
-    }
-    if (tid() == 0) {
-      out.ctr.n_groups = S.n_groups;
-      out.ctr.n_links = S.n_links;
-      out.ctr.links_in_range = S.links_in_range;
-    }
-    __syncthreads();
-    stage_mark(out.stage, 10);
-    if (S.n_groups == 0 && S.links_in_range == 0) {
-      // ---- fluid-only CG (pbf.rs:423-480), solution in place in V
-      float2 *r = m.cg_r, *p = m.cg_p, *ap = m.cg_ap;
-      double bn2 = block_dot(V, V, n, fp64, S);
-      double b_norm = fp64 ? sqrt(bn2) : (double)sqrtf((float)bn2);
-      if (b_norm > 0.0 && isfinite(b_norm)) {
-        const float target_f = VISC_CG_TOL * (float)b_norm;
-        const double target_d = (double)VISC_CG_TOL * b_norm;
-        auto apply = [&](const float2* in, float2* o) {
-          for (uint32_t i = tid(); i < n; i += nthr()) o[i] = (V2(in[i]) + dt * laplacian_row(m, in, i)).f2();
-          __syncthreads();
-        };
-        apply(V, m.cg_ap);
-        for (uint32_t i = tid(); i < n; i += nthr()) { r[i] = (V2(V[i]) - V2(ap[i])).f2(); p[i] = r[i]; }
-        __syncthreads();
-        double rs_old = block_dot(r, r, n, fp64, S);
-        bool done = fp64 ? sqrt(rs_old) <= target_d : sqrtf((float)rs_old) <= target_f;
-        if (!done) {
-          visc_iters = VISC_CG_MAX;
-          for (uint32_t it = 1; it <= VISC_CG_MAX; ++it) {
-            apply(p, ap);
-            double p_ap = block_dot(p, ap, n, fp64, S);
-            if (p_ap <= 0.0 || !isfinite(p_ap)) { visc_iters = it; break; }
-            float alpha = fp64 ? (float)(rs_old / p_ap) : (float)rs_old / (float)p_ap;
-            for (uint32_t i = tid(); i < n; i += nthr()) {
-              V[i] = (V2(V[i]) + alpha * V2(p[i])).f2();
-              r[i] = (V2(r[i]) - alpha * V2(ap[i])).f2();
-            }
-            __syncthreads();
-            double rs_new = block_dot(r, r, n, fp64, S);
-            bool conv = fp64 ? sqrt(rs_new) <= target_d : sqrtf((float)rs_new) <= target_f;
-            if (conv) { visc_iters = it; break; }
-            float bt = fp64 ? (float)(rs_new / rs_old) : (float)rs_new / (float)rs_old;
-            for (uint32_t i = tid(); i < n; i += nthr()) p[i] = (V2(r[i]) + bt * V2(p[i])).f2();
-            __syncthreads();
-            rs_old = rs_new;
-          }
-        }
-      }
-    } else {
-      // ---- joint fluid + ball Jacobi-PCG (pbf.rs:641-791)
-      const uint32_t len = n + 2 * nb;
-      // per-fluid group lists and per-ball "other" link lists (stable, in group / link order)
-      for (uint32_t g = tid(); g < S.n_groups; g += nthr()) m.rec_i[g] = m.g_fluid[g];
-      __syncthreads();
-      block_bucket_sort(m.rec_i, S.n_groups, n, m.fg_start, m.bk_start, m.fg_list);
-      for (uint32_t l = tid(); l < S.n_links; l += nthr()) m.rec_b[l] = m.l_other[l] == NONE ? nb : m.l_other[l];
-      __syncthreads();
-      block_bucket_sort(m.rec_b, S.n_links, nb + 1, m.lo_start, m.bk_start, m.lo_list);
-      float2 *x = m.cg_x, *bvec = m.cg_b, *r = m.cg_r, *z = m.cg_z, *p = m.cg_p, *ap = m.cg_ap;
-      float *diag = m.cg_diag, *inv = m.cg_inv;
-      wide_phase(m, WIDE_CG_SETUP, nullptr, [&](uint32_t w0, uint32_t nw) {
-        cg_setup_rows(m, dt, w0 * 32u + (tid() & 31u), nw * 32u);
-      });
-      for (uint32_t e = tid(); e < len; e += nthr()) inv[e] = 1.0f / fmax_r(diag[e], 1e-20f);
-      __syncthreads();
-      joint_apply(m, dt, x, ap);
-      for (uint32_t e = tid(); e < len; e += nthr()) {
-        V2 re = V2(bvec[e]) - V2(ap[e]);
-        r[e] = re.f2();
-        z[e] = (re * inv[e]).f2();
-      }
-      __syncthreads();
-      double b_norm = block_res_norm(bvec, inv, len, fp64, S);
-      double r_norm = block_res_norm(r, inv, len, fp64, S);
-      stage_mark(out.stage, 23);
-      double tol_b = fp64 ? (double)VISC_CG_TOL * b_norm : (double)(VISC_CG_TOL * (float)b_norm);
-      if (b_norm > 0.0 && isfinite(b_norm) && r_norm > tol_b) {
-        for (uint32_t e = tid(); e < len; e += nthr()) p[e] = z[e];
-        __syncthreads();
-        double rz_old = block_dot(r, z, len, fp64, S);
-        for (uint32_t it = 1; it <= 4 * VISC_CG_MAX; ++it) {
-          visc_iters = it;
-          joint_apply(m, dt, p, ap);
-          double p_ap = block_dot(p, ap, len, fp64, S);
-          if (p_ap <= 0.0 || !isfinite(p_ap)) break;
-          float alpha = fp64 ? (float)(rz_old / p_ap) : (float)rz_old / (float)p_ap;
-          for (uint32_t e = tid(); e < len; e += nthr()) {
-            x[e] = (V2(x[e]) + alpha * V2(p[e])).f2();
-            r[e] = (V2(r[e]) - alpha * V2(ap[e])).f2();
-          }
-          __syncthreads();
-          if (block_res_norm(r, inv, len, fp64, S) <= tol_b) break;
-          for (uint32_t e = tid(); e < len; e += nthr()) z[e] = (V2(r[e]) * inv[e]).f2();
-          __syncthreads();
-          double rz_new = block_dot(r, z, len, fp64, S);
-          float bt = fp64 ? (float)(rz_new / rz_old) : (float)rz_new / (float)rz_old;
-          for (uint32_t e = tid(); e < len; e += nthr()) p[e] = (V2(z[e]) + bt * V2(p[e])).f2();
-          __syncthreads();
-          rz_old = rz_new;
-        }
-      }
-      stage_mark(out.stage, 31);
-      for (uint32_t i = tid(); i < n; i += nthr()) {
-        V2 vn(x[i]);
-        V[i] = vn.f2();
-        V2 d = vn - V2(m.dv_tmp[i]);
-        m.fguess[i] = (d.finite() ? d : V2()).f2();
-      }
-      __syncthreads();
-      // ball impulses from the solved velocities (pbf.rs:2237-2298), one thread per ball
-      for (uint32_t b = tid(); b < nb; b += nthr()) {
-        V2 dv = V2(x[n + b]) - V2(m.ball_v0[b]);
-        float dw = x[n + nb + b].x - m.ball_w0[b];
-        if (dv.finite() && finite_f(dw)) {
-          m.imp[b] = (V2(m.imp[b]) + m.b_m * dv).f2();
-          m.ang[b] += m.b_I * dw;
-        }
-      }
-      if (tid() == 0) m.guess_valid_dev[0] = 1u;
-      if (U.want_momentum && tid() < 32) {
-        // the fluid's momentum change loses b_m * dv per ball, in ball order (a - t == a + (-t))
-        auto term = [&](uint32_t b, float& t, int c) {
-          V2 dv = V2(x[n + b]) - V2(m.ball_v0[b]);
-          float dw = x[n + nb + b].x - m.ball_w0[b];
-          if (!(dv.finite() && finite_f(dw))) return false;
-          V2 p = m.b_m * dv;
-          t = -(c ? p.y : p.x);
-          return true;
-        };
-        const float mx = warp_ordered_sum(S.fscal[0], nb, [&](uint32_t b, float& t) { return term(b, t, 0); });
-        const float my = warp_ordered_sum(S.fscal[1], nb, [&](uint32_t b, float& t) { return term(b, t, 1); });
-        if (tid() == 0) {
-          S.fscal[0] = mx;
-          S.fscal[1] = my;
-        }
-      }
-      __syncthreads();
-    }
-  }
+  if (!viscosity_step(m, U, out, err, S, X, V, mu, visc_iters)) return;
   stage_mark(out.stage, 11);
   // ---- mean shear rate (pbf.rs:800-849) on the final velocities
   for (uint32_t i = tid(); i < n; i += nthr()) {

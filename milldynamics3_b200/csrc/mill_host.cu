@@ -360,6 +360,7 @@ int fill_uniform(MgSim* s, const MgDrum& drum, const MgMediaParams& media, const
                                                   SPIN_LIMIT))
                      : SPIN_LIMIT;
   U.skip_done_ball = (s->opt.test_faults & 2u) ? 0u : NONE;
+  U.sweep_order = s->opt.sweep_order;
   // pbf.rs:190-219: boundary points at dx = h / 2 (adhesion and viscosity groups)
   U.boundary_count = 0;
   float br = s->bmat.radius, dx = 0.5f * s->fmat.h;
@@ -758,6 +759,7 @@ int mg_sim_set_options(MgSim* s, const MgOptions* o) {
   if (o->test_wait_limit_us > 10000000u) return fail(s, MG_ERR_ARG, "test_wait_limit_us must be at most 10000000");
   if (o->test_faults & ~3u) return fail(s, MG_ERR_ARG, "test_faults: only bits 1 and 2 are defined");
   if (o->block_regs != 0 && o->block_regs != 64) return fail(s, MG_ERR_ARG, "block_regs must be 0 or 64");
+  if (o->sweep_order > 1) return fail(s, MG_ERR_ARG, "sweep_order must be 0 (by level) or 1 (index order)");
   s->opt = *o;
   return MG_OK;
 }

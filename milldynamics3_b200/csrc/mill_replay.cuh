@@ -127,8 +127,9 @@ __device__ void run_levels(uint32_t nlev, const uint32_t* lev_start, Load load, 
 // ---------------------------------------------------------------- per-ball sweeps over fluid
 // The drag and buoyancy sweeps (pbf.rs:1824-2011, 2042-2121) visit balls in index order; ball b
 // reads and writes the velocities of its items (fluid particles), so it depends on the earlier
-// balls that share an item. Balls are claimed in index order by the warps of the block, and a
-// warp starts ball b once every earlier ball sharing one of b's items is done.
+// balls that share an item. The warps of the block claim balls in index order or by dependency
+// level (ball_level_order), and a warp starts ball b once every earlier ball sharing one of b's
+// items is done.
 
 __shared__ uint32_t g_ticket;
 
@@ -148,21 +149,143 @@ static __device__ uint32_t pack_ball_items(const uint32_t* item_j, const uint32_
   return total;
 }
 
-// rec_pred[r] = the ball of the previous record with the same fluid index (NONE if first).
+// Scratch of the dependency levels of a per-ball sweep (32-bit words in shared memory; LEVEL_PREDS
+// predecessor slots per ball). A ball's predecessors are the balls that hold the previous record of
+// one of its fluid particles; those in the ball's own chunk of 32 balls are kept as a bit mask,
+// the others as a set of up to LEVEL_PREDS balls (more: the ball is marked, its records are read
+// again when its level is computed).
+constexpr uint32_t LEVEL_PREDS = 8;
+struct LevelScratch {
+  uint32_t* plist;   // LEVEL_PREDS per ball, NONE when free
+  uint32_t* over;    // 1: more than LEVEL_PREDS earlier-chunk predecessors
+  uint32_t* pmask;   // same-chunk predecessors, bit (p - chunk start)
+  uint32_t* lvl;
+  uint32_t* order;   // the claim order
+  uint32_t* pos;     // position of each ball in the order
+  uint32_t* lstart;  // nb + 2 counters (levels are below nb + 1)
+};
+__device__ inline uint32_t level_scratch_words(uint32_t nb) { return (LEVEL_PREDS + 7u) * nb + 2u; }
+__device__ inline bool level_scratch(uint32_t nb, uint32_t* scratch, uint32_t words, LevelScratch& L) {
+  if (nb == 0 || scratch == nullptr || words < level_scratch_words(nb)) return false;
+  L.plist = scratch;
+  L.over = L.plist + LEVEL_PREDS * nb;
+  L.pmask = L.over + nb;
+  L.lvl = L.pmask + nb;
+  L.order = L.lvl + nb;
+  L.pos = L.order + nb;
+  L.lstart = L.pos + nb;
+  return true;
+}
+
+// Records ball p as a predecessor of ball b (p < b). Set entries go from NONE to a ball once, so
+// concurrent insertions of the same ball leave it once.
+__device__ __forceinline__ void level_add_pred(const LevelScratch& L, uint32_t b, uint32_t p) {
+  const uint32_t chunk = b & ~31u;
+  if (p >= chunk) {
+    atomicOr(&L.pmask[b], 1u << (p - chunk));
+    return;
+  }
+  uint32_t* S = L.plist + b * LEVEL_PREDS;
+  for (uint32_t i = 0; i < LEVEL_PREDS; ++i) {
+    const uint32_t v = atomicCAS(&S[i], NONE, p);
+    if (v == NONE || v == p) return;
+  }
+  L.over[b] = 1u;
+}
+
+// rec_pred[r] = the ball of the previous record with the same fluid index (NONE if first). With L,
+// also the predecessor sets of the balls (for ball_level_order).
 static __device__ void ball_item_preds(const uint32_t* rec_key, const uint32_t* rec_ball, uint32_t nrec, uint32_t nf,
-                                uint32_t* start, uint32_t* cur, uint32_t* order, uint32_t* rec_pred) {
-  block_bucket_sort(rec_key, nrec, nf, start, cur, order);
+                                       uint32_t nb, uint32_t* start, uint32_t* cur, uint32_t* order, uint32_t* rec_pred,
+                                       const LevelScratch* L = nullptr) {
+  if (L) {
+    for (uint32_t k = tid(); k < LEVEL_PREDS * nb; k += nthr()) L->plist[k] = NONE;
+    for (uint32_t b = tid(); b < nb; b += nthr()) { L->over[b] = 0u; L->pmask[b] = 0u; }
+  }
+  block_bucket_sort(rec_key, nrec, nf, start, cur, order);  // (its barriers order the resets above)
   for (uint32_t j = tid(); j < nf; j += nthr()) {
     uint32_t prev = NONE;
     for (uint32_t q = start[j]; q < start[j + 1]; ++q) {
-      uint32_t r = order[q];
+      const uint32_t r = order[q], b = rec_ball[r];
       rec_pred[r] = prev;
-      prev = rec_ball[r];
+      if (L && prev != NONE) level_add_pred(*L, b, prev);
+      prev = b;
     }
   }
   __syncthreads();
 }
 
+// A claim order for a per-ball sweep from the predecessor sets ball_item_preds left in L: the balls
+// by dependency level (level 0: no predecessor; otherwise one more than the deepest predecessor's
+// level), so that the warps of the sweep take the chain's early links first. Every predecessor of
+// a ball has a lower level and comes earlier, so claims in this order never wait on a ball that is
+// not claimed yet (the order is topological), and the sweep's results do not depend on it.
+//   levels (warp 0, chunk after chunk of 32 balls): from the earlier chunks' levels, then the
+//          chunk's own dependencies in ball order (lane t's level is final when step t reads it);
+//   order: a counting sort by level; pos[] its inverse.
+static __device__ const uint32_t* ball_level_order(uint32_t nb, const uint32_t* rec_off, const uint32_t* rec_pred,
+                                                   const LevelScratch& L) {
+  __shared__ uint32_t s_nlev;
+  if (threadIdx.x < 32) {
+    const uint32_t lane = threadIdx.x;
+    uint32_t maxl = 0;
+    for (uint32_t c = 0; c < nb; c += 32) {
+      const uint32_t k = c + lane;
+      uint32_t base = 0, mk = 0;
+      if (k < nb) {
+        if (!L.over[k]) {
+          const uint32_t* S = L.plist + k * LEVEL_PREDS;
+          for (uint32_t i = 0; i < LEVEL_PREDS && S[i] != NONE; ++i) base = max(base, L.lvl[S[i]] + 1u);
+        } else {
+          for (uint32_t r = rec_off[k]; r < rec_off[k + 1]; ++r) {
+            const uint32_t p = rec_pred[r];
+            if (p != NONE && p < c) base = max(base, L.lvl[p] + 1u);
+          }
+        }
+        mk = L.pmask[k];
+      }
+      uint32_t lv = base;
+      const uint32_t steps = 32u - __clz(__reduce_or_sync(FULL, mk));  // the highest source lane + 1
+      for (uint32_t t = 0; t < steps; ++t) {
+        const uint32_t lt = __shfl_sync(FULL, lv, t);
+        if ((mk >> t) & 1u) lv = max(lv, lt + 1u);
+      }
+      if (k < nb) {
+        L.lvl[k] = lv;
+        maxl = max(maxl, lv + 1u);
+      }
+      __syncwarp();
+    }
+    maxl = __reduce_max_sync(FULL, maxl);
+    if (lane == 0) s_nlev = maxl;
+  }
+  __syncthreads();
+  const uint32_t nlev = s_nlev;
+  for (uint32_t l = tid(); l <= nlev; l += nthr()) L.lstart[l] = 0u;
+  __syncthreads();
+  for (uint32_t b = tid(); b < nb; b += nthr()) atomicAdd(&L.lstart[L.lvl[b]], 1u);
+  __syncthreads();
+  block_exclusive_scan(L.lstart, nlev + 1);
+  for (uint32_t b = tid(); b < nb; b += nthr()) {
+    const uint32_t q = atomicAdd(&L.lstart[L.lvl[b]], 1u);
+    L.order[q] = b;
+    L.pos[b] = q;
+  }
+  __syncthreads();
+  return L.order;
+}
+
+// Whether `order` (positions pos[]) is topological for the records rec_ball / rec_pred: every
+// record's predecessor ball comes before the record's ball.
+static __device__ bool order_respects(const uint32_t* pos, const uint32_t* rec_ball, const uint32_t* rec_pred,
+                                      uint32_t nrec) {
+  bool bad = false;
+  for (uint32_t r = tid(); r < nrec; r += nthr()) {
+    const uint32_t p = rec_pred[r];
+    if (p != NONE && !(pos[p] < pos[rec_ball[r]])) bad = true;
+  }
+  return !__syncthreads_or(bad);
+}
 
 // Runs fn(b, lane) once per ball, one warp per ball, in a dependency-respecting order. done[] is
 // nb words of scratch (shared or global). Waits are bounded: a wait that runs out sets
@@ -192,85 +315,118 @@ __device__ __forceinline__ void wait_ball_done(volatile uint32_t* vdone, uint32_
 
 // Warps from `warps` on sit the sweep out (they wait at the closing barrier). A wait gives up after
 // spin_limit polls. skip_done names a ball whose done flag is never set (tests of the bounded
-// wait only; NONE otherwise).
+// wait only; NONE otherwise). order: the claim order (a topological order such as
+// ball_level_order's), or nullptr for index order.
 template <class Pre, class Run, class Post>
 __device__ void ball_dataflow(uint32_t nb, const uint32_t* rec_off, const uint32_t* rec_pred, uint32_t* done,
-                              uint32_t warps, uint32_t spin_ns, uint32_t spin_limit, uint32_t skip_done, uint32_t* err,
+                              const uint32_t* order, uint32_t warps, uint32_t spin_ns, uint32_t spin_limit, uint32_t skip_done, uint32_t* err,
                               unsigned long long* acct, Pre pre, Run run, Post post) {
   for (uint32_t b = tid(); b < nb; b += nthr()) done[b] = 0u;
   if (tid() == 0) g_ticket = 0;
   __syncthreads();
   volatile uint32_t* vdone = done;
   const int lane = threadIdx.x & 31;
-  unsigned long long t_pre = 0, t_wait = 0, t_run = 0;
+  // 32-bit clock differences (a ball's parts take far fewer than 2^32 cycles), summed per warp
+  uint32_t t_pre = 0, t_wait = 0, t_run = 0;
   for (;;) {
     if ((threadIdx.x >> 5) >= warps) break;
-    uint32_t b = 0;
-    if (lane == 0) b = atomicAdd(&g_ticket, 1u);
-    b = __shfl_sync(FULL, b, 0);
-    if (b >= nb) break;
-    const long long t0 = clock64();
+    uint32_t t = 0;
+    if (lane == 0) t = atomicAdd(&g_ticket, 1u);
+    t = __shfl_sync(FULL, t, 0);
+    if (t >= nb) break;
+    const uint32_t b = order ? order[t] : t;
+    const uint32_t t0 = (uint32_t)clock();
     const uint32_t r0 = rec_off[b], r1 = rec_off[b + 1];
     const uint32_t p0 = r0 + lane < r1 ? rec_pred[r0 + lane] : NONE;
     auto st = pre(b, lane);
-    const long long t1 = clock64();
+    const uint32_t t1 = (uint32_t)clock();
     wait_ball_done(vdone, p0, spin_ns, spin_limit, err);
     for (uint32_t c = r0 + 32; c < r1; c += 32)
       wait_ball_done(vdone, c + lane < r1 ? rec_pred[c + lane] : NONE, spin_ns, spin_limit, err);
     __syncwarp();
     __threadfence_block();
-    const long long t2 = clock64();
+    const uint32_t t2 = (uint32_t)clock();
     run(b, lane, st);
     __threadfence_block();
     __syncwarp();
     if (lane == 0 && b != skip_done) vdone[b] = 1u;
     post(b, lane, st);
-    t_pre += (unsigned long long)(t1 - t0);
-    t_wait += (unsigned long long)(t2 - t1);
-    t_run += (unsigned long long)(clock64() - t2);
+    t_pre += t1 - t0;
+    t_wait += t2 - t1;
+    t_run += (uint32_t)clock() - t2;
   }
   if (acct && lane == 0 && (t_pre | t_wait | t_run)) {
-    atomicAdd(&acct[0], t_pre);
-    atomicAdd(&acct[1], t_wait);
-    atomicAdd(&acct[2], t_run);
+    atomicAdd(&acct[0], (unsigned long long)t_pre);
+    atomicAdd(&acct[1], (unsigned long long)t_wait);
+    atomicAdd(&acct[2], (unsigned long long)t_run);
   }
   __syncthreads();
 }
 
 // Three in-order sums over the lanes' values t = 0..lim-1, added to a, b, c (the same on every
-// lane): the lanes store their values to the warp's shared scratch and lane 0 adds them in lane
-// order (independent loads, three interleaved chains of additions), then broadcasts the sums.
-__shared__ float g_seq_buf[MAX_BLOCK_WARPS][3][32];
+// lane): the lanes store their values to the warp's shared scratch, lanes from lim on store -0.0
+// (x + -0.0 == x for every x, so padding changes no sum), and lane 0 adds them in lane order four
+// at a time from 16-byte loads, the next four's loads in flight during the additions; the sums
+// are then broadcast.
+__shared__ __align__(16) float g_seq_buf[MAX_BLOCK_WARPS][3][32];
 __device__ __forceinline__ void lane_seq_sum3(float& a, float& b, float& c, float va, float vb, float vc,
                                               uint32_t lim) {
   const uint32_t lane = threadIdx.x & 31u;
   float(*B)[32] = g_seq_buf[threadIdx.x >> 5];
-  B[0][lane] = va;
-  B[1][lane] = vb;
-  B[2][lane] = vc;
+  const bool in = lane < lim;
+  B[0][lane] = in ? va : -0.0f;
+  B[1][lane] = in ? vb : -0.0f;
+  B[2][lane] = in ? vc : -0.0f;
   __syncwarp();
   if (lane == 0) {
-    // four terms' loads ahead of their additions
-    uint32_t t = 0;
-    for (; t + 4 <= lim; t += 4) {
-      const float a0 = B[0][t], a1 = B[0][t + 1], a2 = B[0][t + 2], a3 = B[0][t + 3];
-      const float b0 = B[1][t], b1 = B[1][t + 1], b2 = B[1][t + 2], b3 = B[1][t + 3];
-      const float c0 = B[2][t], c1 = B[2][t + 1], c2 = B[2][t + 2], c3 = B[2][t + 3];
-      a += a0; b += b0; c += c0;
-      a += a1; b += b1; c += c1;
-      a += a2; b += b2; c += c2;
-      a += a3; b += b3; c += c3;
-    }
-    for (; t < lim; ++t) {
-      a += B[0][t];
-      b += B[1][t];
-      c += B[2][t];
+    const float4* A4 = reinterpret_cast<const float4*>(B[0]);
+    const float4* B4 = reinterpret_cast<const float4*>(B[1]);
+    const float4* C4 = reinterpret_cast<const float4*>(B[2]);
+    const uint32_t groups = (lim + 3u) >> 2;
+    float4 x = A4[0], y = B4[0], z = C4[0];
+#pragma unroll
+    for (uint32_t g = 0; g < 8; ++g) {
+      if (g >= groups) break;
+      float4 xn, yn, zn;
+      if (g + 1 < 8) { xn = A4[g + 1]; yn = B4[g + 1]; zn = C4[g + 1]; }
+      a += x.x; b += y.x; c += z.x;
+      a += x.y; b += y.y; c += z.y;
+      a += x.z; b += y.z; c += z.z;
+      a += x.w; b += y.w; c += z.w;
+      x = xn; y = yn; z = zn;
     }
   }
   __syncwarp();
   a = __shfl_sync(FULL, a, 0);
   b = __shfl_sync(FULL, b, 0);
   c = __shfl_sync(FULL, c, 0);
+}
+
+// One in-order sum over the lanes' values t = 0..lim-1 added to a (the same on every lane), like
+// lane_seq_sum3.
+__device__ __forceinline__ void lane_seq_sum1(float& a, float va, uint32_t lim) {
+  const uint32_t lane = threadIdx.x & 31u;
+  float* B = g_seq_buf[threadIdx.x >> 5][0];
+  B[lane] = lane < lim ? va : -0.0f;
+  __syncwarp();
+  if (lane == 0) {
+    const float4* A4 = reinterpret_cast<const float4*>(B);
+    const uint32_t groups = (lim + 3u) >> 2;
+    float4 x = A4[0];
+#pragma unroll
+    for (uint32_t g = 0; g < 8; ++g) {
+      if (g >= groups) break;
+      float4 xn;
+      if (g + 1 < 8) xn = A4[g + 1];
+      a += x.x;
+      a += x.y;
+      a += x.z;
+      a += x.w;
+      x = xn;
+    }
+  }
+  __syncwarp();
+  a = __shfl_sync(FULL, a, 0);
 }
 
 // Block-wide in-order f32 sum init + term(0) + term(1) + ... + term(n-1), every term added (the

@@ -149,7 +149,8 @@ class Simulation:
         self._c(self.lib.sim_reset_energy_budget(self.h))
 
     def set_options(self, cg_fp64: int = 0, block_threads: int = 0, sweep_warps: int = 0, spin_ns: int = 0,
-                    mill_blocks: int = 0, test_wait_limit_us: int = 0, test_faults: int = 0, block_regs: int = 0):
+                    mill_blocks: int = 0, test_wait_limit_us: int = 0, test_faults: int = 0, block_regs: int = 0,
+                    sweep_order: int = 0):
         o = capi.Options()
         o.cg_fp64 = cg_fp64
         o.block_threads = block_threads
@@ -159,6 +160,7 @@ class Simulation:
         o.test_wait_limit_us = test_wait_limit_us
         o.test_faults = test_faults
         o.block_regs = block_regs
+        o.sweep_order = sweep_order
         if hasattr(self.lib, "sim_set_options"):
             self._c(self.lib.sim_set_options(self.h, C.byref(o)))
         else:
