@@ -325,7 +325,7 @@ struct MillDev {
   // sweep replay (mill_replay.cuh): predecessors, levels, active contacts of the contact sweeps
   uint32_t *dm_pa, *dm_pb, *dm_lvl, *lev_start, *lev_cur, *lev_items;
   uint32_t *act_i, *act_j, *act_flag;
-  float *act_l, *act_w1, *act_w2;
+  float *act_l, *act_w1, *act_w2, *act_t;
   int32_t* act_bin;
   MgImpactRecord* act_rec;
   uint32_t smem_balls;  // balls whose state fits the launch's dynamic shared memory (0: global)

@@ -150,152 +150,164 @@ static __device__ __noinline__ void project_iterations(const MillDev& m, const S
   }
 }
 
-// Runs body(k, (i, j, lambda_n)) for the active contacts in sweep order: the pair contacts by
-// dependency levels in warp 0 (contacts of one level share no ball), then the wall contacts at once
-// (every wall contact comes after every pair contact and touches one ball); the block waits at the
-// end.
-template <class Body>
-__device__ __forceinline__ void contact_sweep(const MillDev& m, uint32_t nlev_c, uint32_t na_p, uint32_t na, Body body) {
-  run_levels(nlev_c, m.lev_start,
-             [&](uint32_t q) {
-               const uint32_t k = m.lev_items[q];
-               return make_uint4(k, m.act_i[k], m.act_j[k], __float_as_uint(m.act_l[k]));
-             },
-             [&](uint32_t, uint4 d) { body(d.x, make_uint3(d.y, d.z, d.w)); });
-  for (uint32_t k = na_p + tid(); k < na; k += nthr())
-    body(k, make_uint3(m.act_i[k], m.act_j[k], __float_as_uint(m.act_l[k])));
-  __syncthreads();
-}
-
-// Step 5 friction sweep (dem.rs:782-882) over the active contacts; wall contacts leave their work
-// terms in act_w1 / act_w2 (act_bin -2: none). Its own function, like project_iterations.
+// Step 5 friction sweep (dem.rs:782-882) over the active contacts in sweep order: the pair contacts
+// by dependency levels in warp 0 (contacts of one level share no ball), then the wall contacts
+// (every wall contact comes after every pair contact and touches one ball) at once. Wall contacts
+// leave their work terms in act_w1 / act_w2 (act_bin -2: none). Its own function, like
+// project_iterations.
 static __device__ __noinline__ void friction_sweep(const MillDev& m, const StepUniform& U, float2* X, float2* V,
                                                    float* TH, float* OM, uint32_t nlev_c, uint32_t na_p, uint32_t na,
                                                    float w, float w_rot, float r, float dt) {
-  const MgMediaParams& md = U.media;
-  contact_sweep(m, nlev_c, na_p, na, [&](uint32_t k, uint3 d) {
-    // this body's constants and pointers as locals (they stay in registers)
-    float2* const X_l = X;
-    float2* const V_l = V;
-    float* const TH_l = TH;
-    float* const OM_l = OM;
-    const float w_l = w, w_rot_l = w_rot, r_l = r, dt_l = dt;
-    const MgMediaParams md_l = md;
-    const uint32_t i = d.x, j = d.y;
-    const float lambda_n = __uint_as_float(d.z);
-    if (j != NONE) {
-      V2 delta = V2(X_l[i]) - V2(X_l[j]);
-      float dist = delta.len();
-      V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
-      V2 t_hat(-n_hat.y, n_hat.x);
-      float v_t = (V2(V_l[i]) - V2(V_l[j])).dot(t_hat) - r_l * OM_l[i] - r_l * OM_l[j];
-      float w_sum_t = w_l + w_l + r_l * r_l * w_rot_l + r_l * r_l * w_rot_l;
-      if (w_sum_t <= 0.0f) return;
-      float raw = -v_t * dt_l / w_sum_t;
-      float mu = effective_friction(md_l.friction_ball_ball, md_l.friction_ball_ball_static, v_t, md_l.friction_velocity_scale_m_s);
-      float max_mag = mu * lambda_n;
-      float dlt = clamp_r(raw, -max_mag, max_mag);
-      X_l[i] = (V2(X_l[i]) + w_l * dlt * t_hat).f2();
-      X_l[j] = (V2(X_l[j]) - w_l * dlt * t_hat).f2();
-      TH_l[i] -= r_l * w_rot_l * dlt;
-      TH_l[j] -= r_l * w_rot_l * dlt;
-      V2 dv = w_l * dlt * t_hat / dt_l;
-      float domega = -r_l * w_rot_l * dlt / dt_l;
-      V_l[i] = (V2(V_l[i]) + dv).f2();
-      V_l[j] = (V2(V_l[j]) - dv).f2();
-      OM_l[i] += domega;
-      OM_l[j] += domega;
-    } else {
-      m.act_bin[k] = -2;  // no work terms unless the contact completes below
-      float dd;
-      V2 n_hat;
-      drum_sdf_world(U, V2(X_l[i]), U.to_local_next, U.to_world_next, dd, n_hat);
-      V2 t_hat(-n_hat.y, n_hat.x);
-      V2 v_wall = wall_velocity(U.drum_omega, V2(X_l[i]) - r_l * n_hat);
-      float v_t = (V2(V_l[i]) - v_wall).dot(t_hat) - r_l * OM_l[i];
-      float w_sum_t = w_l + r_l * r_l * w_rot_l;
-      if (w_sum_t <= 0.0f) return;
-      float raw = -v_t * dt_l / w_sum_t;
-      float mu = effective_friction(md_l.friction_ball_wall, md_l.friction_ball_wall_static, v_t, md_l.friction_velocity_scale_m_s);
-      float max_mag = mu * lambda_n;
-      float dlt = clamp_r(raw, -max_mag, max_mag);
-      X_l[i] = (V2(X_l[i]) + w_l * dlt * t_hat).f2();
-      TH_l[i] -= r_l * w_rot_l * dlt;
-      V_l[i] = (V2(V_l[i]) + w_l * dlt * t_hat / dt_l).f2();
-      OM_l[i] += -r_l * w_rot_l * dlt / dt_l;
-      m.act_w1[k] = (dlt / dt_l) * t_hat.dot(v_wall);
-      m.act_w2[k] = (lambda_n / dt_l) * n_hat.dot(v_wall);
-      m.act_bin[k] = 0;
-    }
-  });
+  // the sweep's constants, read once (the per-item bodies keep them in registers)
+  const float mu_bb = U.media.friction_ball_ball, mu_bb_s = U.media.friction_ball_ball_static;
+  const float mu_bw = U.media.friction_ball_wall, mu_bw_s = U.media.friction_ball_wall_static;
+  const float vscale = U.media.friction_velocity_scale_m_s;
+  const float w_sum_pair = w + w + r * r * w_rot + r * r * w_rot;
+  const float w_sum_wall = w + r * r * w_rot;
+  float2* const X_l = X;
+  float2* const V_l = V;
+  float* const TH_l = TH;
+  float* const OM_l = OM;
+  // pair contacts by dependency levels in warp 0
+  run_levels(nlev_c, m.lev_start,
+             [&](uint32_t q) {
+               const uint32_t k = m.lev_items[q];
+               return make_uint3(m.act_i[k], m.act_j[k], __float_as_uint(m.act_l[k]));
+             },
+             [&](uint32_t, uint3 d) {
+               const uint32_t i = d.x, j = d.y;
+               const float lambda_n = __uint_as_float(d.z);
+               V2 delta = V2(X_l[i]) - V2(X_l[j]);
+               float dist = delta.len();
+               V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
+               V2 t_hat(-n_hat.y, n_hat.x);
+               float v_t = (V2(V_l[i]) - V2(V_l[j])).dot(t_hat) - r * OM_l[i] - r * OM_l[j];
+               if (w_sum_pair <= 0.0f) return;
+               float raw = -v_t * dt / w_sum_pair;
+               float mu = effective_friction(mu_bb, mu_bb_s, v_t, vscale);
+               float max_mag = mu * lambda_n;
+               float dlt = clamp_r(raw, -max_mag, max_mag);
+               X_l[i] = (V2(X_l[i]) + w * dlt * t_hat).f2();
+               X_l[j] = (V2(X_l[j]) - w * dlt * t_hat).f2();
+               TH_l[i] -= r * w_rot * dlt;
+               TH_l[j] -= r * w_rot * dlt;
+               V2 dv = w * dlt * t_hat / dt;
+               float domega = -r * w_rot * dlt / dt;
+               V_l[i] = (V2(V_l[i]) + dv).f2();
+               V_l[j] = (V2(V_l[j]) - dv).f2();
+               OM_l[i] += domega;
+               OM_l[j] += domega;
+             });
+  // then the wall contacts, each on its own ball, all at once
+  for (uint32_t k = na_p + tid(); k < na; k += nthr()) {
+    const uint32_t i = m.act_i[k];
+    const float lambda_n = m.act_l[k];
+    m.act_bin[k] = -2;  // no work terms unless the contact completes below
+    float dd;
+    V2 n_hat;
+    drum_sdf_world(U, V2(X_l[i]), U.to_local_next, U.to_world_next, dd, n_hat);
+    V2 t_hat(-n_hat.y, n_hat.x);
+    V2 v_wall = wall_velocity(U.drum_omega, V2(X_l[i]) - r * n_hat);
+    float v_t = (V2(V_l[i]) - v_wall).dot(t_hat) - r * OM_l[i];
+    if (w_sum_wall <= 0.0f) continue;
+    float raw = -v_t * dt / w_sum_wall;
+    float mu = effective_friction(mu_bw, mu_bw_s, v_t, vscale);
+    float max_mag = mu * lambda_n;
+    float dlt = clamp_r(raw, -max_mag, max_mag);
+    X_l[i] = (V2(X_l[i]) + w * dlt * t_hat).f2();
+    TH_l[i] -= r * w_rot * dlt;
+    V_l[i] = (V2(V_l[i]) + w * dlt * t_hat / dt).f2();
+    OM_l[i] += -r * w_rot * dlt / dt;
+    m.act_w1[k] = (dlt / dt) * t_hat.dot(v_wall);
+    m.act_w2[k] = (lambda_n / dt) * n_hat.dot(v_wall);
+    m.act_bin[k] = 0;
+  }
+  __syncthreads();
 }
 
 // Step 6 restitution sweep (dem.rs:909-1019) over the active contacts, with the impact accounting
 // (collision count and energy histogram in S, impact records flagged in act_flag / act_rec).
+// Positions do not change in this sweep, so each pair contact's normal, approach speed, impact
+// accounting and target normal speed are computed for all pair contacts at once (act_w1 / act_w2 /
+// act_t); the pair chain then only reads and updates the two velocities. The wall contacts come
+// after every pair contact, each on its own ball, all at once.
 static __device__ __noinline__ void restitution_sweep(const MillDev& m, const StepUniform& U, DemShared& S, float2* X,
                                                       float2* V, uint32_t nlev_c, uint32_t na_p, uint32_t na, float w,
                                                       float r, float impact_threshold) {
-  const MgMediaParams& md = U.media;
-  contact_sweep(m, nlev_c, na_p, na, [&](uint32_t k, uint3 d) {
-    // this body's constants and pointers as locals (they stay in registers)
-    float2* const X_l = X;
-    float2* const V_l = V;
-    const float w_l = w, r_l = r, impact_threshold_l = impact_threshold;
-    const MgMediaParams md_l = md;
-    const uint32_t i = d.x, j = d.y;
+  const float e_bb = U.media.restitution_ball_ball, e_bw = U.media.restitution_ball_wall;
+  for (uint32_t k = tid(); k < na_p; k += nthr()) {
+    const uint32_t i = m.act_i[k], j = m.act_j[k];
     m.act_flag[k] = 0;
-    if (j != NONE) {
-      V2 delta = V2(X_l[i]) - V2(X_l[j]);
-      float dist = delta.len();
-      V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
-      float v_n_pre = (V2(m.bvpre[i]) - V2(m.bvpre[j])).dot(n_hat);
-      bool fresh = v_n_pre < -RESTITUTION_VELOCITY_THRESHOLD;
-      if (fresh) {
-        atomicAdd(&S.collisions, 1u);
-        int bin = impact_energy_bin(0.5f * (m.b_m * 0.5f) * v_n_pre * v_n_pre);
-        if (bin >= 0) atomicAdd(&S.hist[bin], 1u);
-      }
-      float e = fresh ? md_l.restitution_ball_ball : 0.0f;
-      if (-v_n_pre > impact_threshold_l) {
-        V2 t_hat(-n_hat.y, n_hat.x);
-        float slip = (V2(m.bvpre[i]) - V2(m.bvpre[j])).dot(t_hat) - r_l * m.bompre[i] - r_l * m.bompre[j];
-        m.act_rec[k] = MgImpactRecord{MG_IMPACT_BALL_BALL, i, j, -v_n_pre, fabsf(slip), e};
-        m.act_flag[k] = 1;
-      }
-      float target = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
-      float v_n_now = (V2(V_l[i]) - V2(V_l[j])).dot(n_hat);
-      float dvn = target - v_n_now;
-      float w_sum = w_l + w_l;
-      if (w_sum <= 0.0f) return;
-      float impulse = dvn / w_sum;
-      V_l[i] = (V2(V_l[i]) + w_l * impulse * n_hat).f2();
-      V_l[j] = (V2(V_l[j]) - w_l * impulse * n_hat).f2();
-    } else {
-      float dd;
-      V2 n_hat;
-      drum_sdf_world(U, V2(X_l[i]), U.to_local_next, U.to_world_next, dd, n_hat);
-      V2 v_wall = wall_velocity(U.drum_omega, V2(X_l[i]) - r_l * n_hat);
-      float v_n_pre = (V2(m.bvpre[i]) - v_wall).dot(n_hat);
-      bool fresh = v_n_pre < -RESTITUTION_VELOCITY_THRESHOLD;
-      if (fresh) {
-        atomicAdd(&S.collisions, 1u);
-        int bin = impact_energy_bin(0.5f * m.b_m * v_n_pre * v_n_pre);
-        if (bin >= 0) atomicAdd(&S.hist[bin], 1u);
-      }
-      float e = fresh ? md_l.restitution_ball_wall : 0.0f;
-      if (-v_n_pre > impact_threshold_l) {
-        V2 t_hat(-n_hat.y, n_hat.x);
-        float slip = (V2(m.bvpre[i]) - v_wall).dot(t_hat) - r_l * m.bompre[i];
-        m.act_rec[k] = MgImpactRecord{MG_IMPACT_BALL_WALL, i, MG_WALL_PARTNER, -v_n_pre, fabsf(slip), e};
-        m.act_flag[k] = 1;
-      }
-      float target = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
-      float v_n_now = (V2(V_l[i]) - v_wall).dot(n_hat);
-      float dvn = target - v_n_now;
-      if (w_l <= 0.0f) return;
-      V_l[i] = (V2(V_l[i]) + dvn * n_hat).f2();
+    V2 delta = V2(X[i]) - V2(X[j]);
+    float dist = delta.len();
+    V2 n_hat = dist > 1e-9f ? delta / dist : V2(1.0f, 0.0f);
+    float v_n_pre = (V2(m.bvpre[i]) - V2(m.bvpre[j])).dot(n_hat);
+    bool fresh = v_n_pre < -RESTITUTION_VELOCITY_THRESHOLD;
+    if (fresh) {
+      atomicAdd(&S.collisions, 1u);
+      int bin = impact_energy_bin(0.5f * (m.b_m * 0.5f) * v_n_pre * v_n_pre);
+      if (bin >= 0) atomicAdd(&S.hist[bin], 1u);
     }
-  });
+    float e = fresh ? e_bb : 0.0f;
+    if (-v_n_pre > impact_threshold) {
+      V2 t_hat(-n_hat.y, n_hat.x);
+      float slip = (V2(m.bvpre[i]) - V2(m.bvpre[j])).dot(t_hat) - r * m.bompre[i] - r * m.bompre[j];
+      m.act_rec[k] = MgImpactRecord{MG_IMPACT_BALL_BALL, i, j, -v_n_pre, fabsf(slip), e};
+      m.act_flag[k] = 1;
+    }
+    m.act_w1[k] = n_hat.x;
+    m.act_w2[k] = n_hat.y;
+    m.act_t[k] = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
+  }
+  __syncthreads();
+  struct PairDesc {
+    uint32_t i, j;
+    float nx, ny, target;
+  };
+  const float w_l = w, w_sum = w + w;
+  float2* const V_l = V;
+  run_levels(nlev_c, m.lev_start,
+             [&](uint32_t q) {
+               const uint32_t k = m.lev_items[q];
+               return PairDesc{m.act_i[k], m.act_j[k], m.act_w1[k], m.act_w2[k], m.act_t[k]};
+             },
+             [&](uint32_t, PairDesc d) {
+               if (w_sum <= 0.0f) return;
+               const V2 n_hat(d.nx, d.ny);
+               float v_n_now = (V2(V_l[d.i]) - V2(V_l[d.j])).dot(n_hat);
+               float dvn = d.target - v_n_now;
+               float impulse = dvn / w_sum;
+               V_l[d.i] = (V2(V_l[d.i]) + w_l * impulse * n_hat).f2();
+               V_l[d.j] = (V2(V_l[d.j]) - w_l * impulse * n_hat).f2();
+             });
+  for (uint32_t k = na_p + tid(); k < na; k += nthr()) {
+    const uint32_t i = m.act_i[k];
+    m.act_flag[k] = 0;
+    float dd;
+    V2 n_hat;
+    drum_sdf_world(U, V2(X[i]), U.to_local_next, U.to_world_next, dd, n_hat);
+    V2 v_wall = wall_velocity(U.drum_omega, V2(X[i]) - r * n_hat);
+    float v_n_pre = (V2(m.bvpre[i]) - v_wall).dot(n_hat);
+    bool fresh = v_n_pre < -RESTITUTION_VELOCITY_THRESHOLD;
+    if (fresh) {
+      atomicAdd(&S.collisions, 1u);
+      int bin = impact_energy_bin(0.5f * m.b_m * v_n_pre * v_n_pre);
+      if (bin >= 0) atomicAdd(&S.hist[bin], 1u);
+    }
+    float e = fresh ? e_bw : 0.0f;
+    if (-v_n_pre > impact_threshold) {
+      V2 t_hat(-n_hat.y, n_hat.x);
+      float slip = (V2(m.bvpre[i]) - v_wall).dot(t_hat) - r * m.bompre[i];
+      m.act_rec[k] = MgImpactRecord{MG_IMPACT_BALL_WALL, i, MG_WALL_PARTNER, -v_n_pre, fabsf(slip), e};
+      m.act_flag[k] = 1;
+    }
+    float target = fmax_r(fmax_r(-e * v_n_pre, 0.0f), fmax_r(v_n_pre, 0.0f));
+    float v_n_now = (V2(V[i]) - v_wall).dot(n_hat);
+    float dvn = target - v_n_now;
+    if (w <= 0.0f) continue;
+    V[i] = (V2(V[i]) + dvn * n_hat).f2();
+  }
+  __syncthreads();
 }
 
 static __device__ __noinline__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, MgImpactRecord* impacts,

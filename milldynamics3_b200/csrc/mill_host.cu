@@ -218,6 +218,7 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
     m.lev_items = a.take<uint32_t>(nit);
     m.act_i = a.take<uint32_t>(nit); m.act_j = a.take<uint32_t>(nit); m.act_flag = a.take<uint32_t>(nit + 1);
     m.act_l = a.take<float>(nit); m.act_w1 = a.take<float>(nit); m.act_w2 = a.take<float>(nit);
+    m.act_t = a.take<float>(nit);
     m.act_bin = a.take<int32_t>(nit);
     m.act_rec = a.take<MgImpactRecord>(nit);
     m.g_fluid = a.take<uint32_t>(m.cap_groups); m.g_ball = a.take<uint32_t>(m.cap_groups);

@@ -436,30 +436,36 @@ __device__ __forceinline__ void lane_seq_sum1(float& a, float va, uint32_t lim) 
 // With SKIP_NONFINITE, non-finite terms are left out (not added).
 template <bool SKIP_NONFINITE = false, class Term>
 __device__ float block_seq_sum_f32(float init, uint32_t n, Term term) {
-  constexpr uint32_t CHUNK = MAX_BLOCK_WARPS * 3 * 32;
+  constexpr uint32_t CHUNK = MAX_BLOCK_WARPS * 3 * 32;  // a multiple of 4
   float* buf = &g_seq_buf[0][0][0];
   __shared__ float res;
   float acc = init;
+  auto add4 = [&](float4 x) {
+    if (!SKIP_NONFINITE || finite_f(x.x)) acc += x.x;
+    if (!SKIP_NONFINITE || finite_f(x.y)) acc += x.y;
+    if (!SKIP_NONFINITE || finite_f(x.z)) acc += x.z;
+    if (!SKIP_NONFINITE || finite_f(x.w)) acc += x.w;
+  };
   for (uint32_t c0 = 0; c0 < n; c0 += CHUNK) {
-    const uint32_t cnt = min(CHUNK, n - c0);
-    for (uint32_t k = tid(); k < cnt; k += nthr()) buf[k] = term(c0 + k);
+    const uint32_t cnt = min(CHUNK, n - c0), groups = (cnt + 3u) >> 2;
+    // the chunk padded with -0.0 to whole groups of four (x + -0.0 == x for every x)
+    for (uint32_t k = tid(); k < 4u * groups; k += nthr()) buf[k] = k < cnt ? term(c0 + k) : -0.0f;
     __syncthreads();
     if (tid() == 0) {
-      uint32_t k = 0;
-      for (; k + 8 <= cnt; k += 8) {
-        const float x0 = buf[k], x1 = buf[k + 1], x2 = buf[k + 2], x3 = buf[k + 3];
-        const float x4 = buf[k + 4], x5 = buf[k + 5], x6 = buf[k + 6], x7 = buf[k + 7];
-        if (!SKIP_NONFINITE || finite_f(x0)) acc += x0;
-        if (!SKIP_NONFINITE || finite_f(x1)) acc += x1;
-        if (!SKIP_NONFINITE || finite_f(x2)) acc += x2;
-        if (!SKIP_NONFINITE || finite_f(x3)) acc += x3;
-        if (!SKIP_NONFINITE || finite_f(x4)) acc += x4;
-        if (!SKIP_NONFINITE || finite_f(x5)) acc += x5;
-        if (!SKIP_NONFINITE || finite_f(x6)) acc += x6;
-        if (!SKIP_NONFINITE || finite_f(x7)) acc += x7;
+      // 16-byte loads two groups ahead of the additions, so that only the chain of additions
+      // sets the pace
+      const float4* B4 = reinterpret_cast<const float4*>(buf);
+      const float4 zero = make_float4(-0.0f, -0.0f, -0.0f, -0.0f);
+      float4 x0 = groups > 0 ? B4[0] : zero, x1 = groups > 1 ? B4[1] : zero;
+      uint32_t g = 0;
+      for (; g + 2 <= groups; g += 2) {
+        const float4 x2 = g + 2 < groups ? B4[g + 2] : zero, x3 = g + 3 < groups ? B4[g + 3] : zero;
+        add4(x0);
+        add4(x1);
+        x0 = x2;
+        x1 = x3;
       }
-      for (; k < cnt; ++k)
-        if (!SKIP_NONFINITE || finite_f(buf[k])) acc += buf[k];
+      if (g < groups) add4(x0);
     }
     __syncthreads();
   }
