@@ -232,9 +232,11 @@ __device__ __forceinline__ void warp_sort256_u32(uint32_t* a, uint32_t n) {
 }
 
 // Stable bucket sort: start[0..nbk] receives bucket offsets, order[] the record indices grouped by
-// key in ascending record order; cur[0..nbk) is scratch.
+// key in ascending record order; cur[0..nbk) is scratch. Only the first nsorted buckets (all when
+// nsorted >= nbk) are filled: the records of later buckets are counted in start[] but their part of
+// order[] is left unwritten (for a bucket that collects records nobody reads).
 __device__ inline void block_bucket_sort(const uint32_t* keys, uint32_t nrec, uint32_t nbk, uint32_t* start, uint32_t* cur,
-                                  uint32_t* order) {
+                                  uint32_t* order, uint32_t nsorted = 0xFFFFFFFFu) {
   for (uint32_t k = tid(); k <= nbk; k += nthr()) start[k] = 0;
   __syncthreads();
   for (uint32_t r = tid(); r < nrec; r += nthr()) atomicAdd(&start[keys[r]], 1u);
@@ -253,7 +255,9 @@ __device__ inline void block_bucket_sort(const uint32_t* keys, uint32_t nrec, ui
   for (uint32_t k = tid(); k < nbk; k += nthr()) {
     uint32_t c = start[k];
     const uint32_t sz = start[k + 1] - c;
-    if (sz > MID) {
+    if (k >= nsorted) {
+      c = BIG_MARK;  // not filled
+    } else if (sz > MID) {
       const uint32_t q = atomicAdd(&nbig, 1u);
       if (q < NBIG) { big[q] = k; c = BIG_MARK; }
     } else if (sz > SMALL) {

@@ -1213,7 +1213,8 @@ static __device__ __noinline__ bool viscosity_step(const MillDev& m, const StepU
       block_bucket_sort(m.rec_i, S.n_groups, n, m.fg_start, m.bk_start, m.fg_list);
       for (uint32_t l = tid(); l < S.n_links; l += nthr()) m.rec_b[l] = m.l_other[l] == NONE ? nb : m.l_other[l];
       __syncthreads();
-      block_bucket_sort(m.rec_b, S.n_links, nb + 1, m.lo_start, m.bk_start, m.lo_list);
+      // (bucket nb collects the links without a second ball; only the balls' lists are read)
+      block_bucket_sort(m.rec_b, S.n_links, nb + 1, m.lo_start, m.bk_start, m.lo_list, nb);
       float2 *x = m.cg_x, *bvec = m.cg_b, *r = m.cg_r, *z = m.cg_z, *p = m.cg_p, *ap = m.cg_ap;
       float *diag = m.cg_diag, *inv = m.cg_inv;
       wide_phase(m, WIDE_CG_SETUP, nullptr, [&](uint32_t w0, uint32_t nw) {

@@ -26,7 +26,7 @@ template <class ItemOf, class SlotOf>
 __device__ void preds_from_records(const uint32_t* key, uint32_t nrec, uint32_t nbk, uint32_t nballs, uint32_t* start,
                                    uint32_t* cur, uint32_t* order, uint32_t* pred_a, uint32_t* pred_b, ItemOf item_of,
                                    SlotOf slot_of) {
-  block_bucket_sort(key, nrec, nbk, start, cur, order);
+  block_bucket_sort(key, nrec, nbk, start, cur, order, nballs);
   for (uint32_t b = tid(); b < nballs; b += nthr()) {
     uint32_t prev = NONE;
     for (uint32_t q = start[b]; q < start[b + 1]; ++q) {
