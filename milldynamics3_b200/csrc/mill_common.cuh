@@ -254,6 +254,15 @@ struct WideCtl {
   GridHdr hdr;       // the grid the phase searches
   const float2* vin; // the vectors a phase reads and writes (joint operator)
   float2* vout;
+  // the next sub-step's fluid steps 0-3 on helper block 1 (WIDE_FLUID_PREP): its dt, and what the
+  // mill's block takes over from them (their error bits, kept apart from the mill's error word
+  // while the mill's block runs the DEM step; the fluid grid's header, edge count, density
+  // iterations, the helper's cycles of steps 0-2 and of step 3)
+  float prep_dt;
+  uint32_t prep_err;
+  GridHdr prep_hdr;
+  uint32_t prep_edges, prep_iters;
+  unsigned long long prep_cycles[2];
 };
 
 // ---------------------------------------------------------------- per-mill descriptor

@@ -1299,25 +1299,23 @@ static __device__ __noinline__ bool viscosity_step(const MillDev& m, const StepU
   return true;
 }
 
-static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err, FluidShared& S,
-                           unsigned char* dsm) {
-  uint32_t* done = m.ball_done;  // completion flags of the per-ball sweeps (moved to shared below)
-  const uint32_t n = m.nf, nb = m.nb;
-  const float dt = U.dt;
-  for (uint32_t b = tid(); b < nb; b += nthr()) { m.imp[b] = make_float2(0.0f, 0.0f); m.ang[b] = 0.0f; }
-  if (tid() == 0) { memset(&out.fs, 0, sizeof(out.fs)); out.clamp_hits = 0; out.fluid_momentum[0] = out.fluid_momentum[1] = 0.0f; }
-  __syncthreads();
-  if (n == 0 || dt <= 0.0f) return;
+// Steps 0-3 of the fluid sub-step (pbf.rs:1200-1334): sanitize, predict, the fluid grid and its
+// neighbour lists, the density constraint iterations. They read and write only the fluid's arrays,
+// so in a single-mill launch helper block 1 runs them for the next sub-step while the mill's block
+// runs the DEM step (WIDE_FLUID_PREP). The grid header lands in S.hA and the edge count in
+// S.n_edges; iters receives the density iterations and cycles[0..1] (thread 0) the clock cycles of
+// steps 0-2 and of step 3. Returns early, with *err set, when the neighbour lists overflowed.
+static __device__ void fluid_prep(const MillDev& m, uint32_t pbf_iterations, float dt, FluidShared& S,
+                                  uint32_t* err, uint32_t& iters, unsigned long long* cycles) {
+  const uint32_t n = m.nf;
   const float h = m.f_h, rho0 = m.f_rho0, mass = m.f_mass;
   float2* X = m.fx;
   float2* V = m.fv;
+  const long long t0 = clock64();
   // ---- step 0: sanitize (pbf.rs:1200-1205)
   for (uint32_t i = tid(); i < n; i += nthr())
     if (!V2(X[i]).finite() || !V2(V[i]).finite()) { X[i] = make_float2(0.0f, 0.0f); V[i] = make_float2(0.0f, 0.0f); }
   __syncthreads();
-  // ball grid for the overlap push (pbf.rs:1214-1222)
-  const float contact_radius = m.b_r + OVERLAP_PUSH_MARGIN * h;
-  if (nb > 0) grid_build(m.bx, nb, fmax_r(fmax_r(2.0f * m.b_r, contact_radius), 1e-6f), m.gBall, S.hBall, err);
   // ---- step 1: predict (pbf.rs:1225-1235)
   for (uint32_t i = tid(); i < n; i += nthr()) {
     V2 x(X[i]), v(V[i]);
@@ -1331,11 +1329,12 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
   // ---- step 2: grid + neighbour lists (pbf.rs:1238-1239)
   grid_build(X, n, h, m.gA, S.hA, err);
   build_neighbor_lists(X, n, h, S.hA, m.gA, m.nbr_off, m.nbrs, m.cap_edges, err, &S.n_edges);
-  if (tid() == 0) out.ctr.n_fluid_edges = S.n_edges;
-  stage_mark(out.stage, 0);
-  if (*err) return;
+  if (tid() == 0) cycles[0] = (unsigned long long)(clock64() - t0);
+  // (block-uniform: on a helper block the mill's block may set *err at any time)
+  if (__syncthreads_or(*err != 0u)) return;
+  const long long t1 = clock64();
   // ---- step 3: density constraint (pbf.rs:1257-1334)
-  const uint32_t base_it = U.pbf_iterations > 1 ? U.pbf_iterations : 1u;
+  const uint32_t base_it = pbf_iterations > 1 ? pbf_iterations : 1u;
   const float m_rho = mass / rho0;
   const float self_rho = mass * poly6(0.0f, h);
   uint32_t iter_count = 0;
@@ -1381,8 +1380,60 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
     bool converged = max_c <= COMPRESSION_TOL;
     if ((iter_count >= base_it && converged) || iter_count >= base_it + ADAPTIVE_MAX_EXTRA) break;
   }
-  if (tid() == 0) out.ctr.density_iters = iter_count;
-  stage_mark(out.stage, 1);
+  if (tid() == 0) {
+    iters = iter_count;
+    cycles[1] = (unsigned long long)(clock64() - t1);
+  }
+}
+
+static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err, FluidShared& S,
+                           unsigned char* dsm, bool prepped) {
+  if (prepped) wide_finish(m);   // helper block 1 ran steps 0-3 (published with WIDE_FLUID_PREP)
+  uint32_t* done = m.ball_done;  // completion flags of the per-ball sweeps (moved to shared below)
+  const uint32_t n = m.nf, nb = m.nb;
+  const float dt = U.dt;
+  for (uint32_t b = tid(); b < nb; b += nthr()) { m.imp[b] = make_float2(0.0f, 0.0f); m.ang[b] = 0.0f; }
+  if (tid() == 0) { memset(&out.fs, 0, sizeof(out.fs)); out.clamp_hits = 0; out.fluid_momentum[0] = out.fluid_momentum[1] = 0.0f; }
+  __syncthreads();
+  if (n == 0 || dt <= 0.0f) return;
+  const float h = m.f_h, rho0 = m.f_rho0, mass = m.f_mass;
+  float2* X = m.fx;
+  float2* V = m.fv;
+  if (prepped) {
+    // steps 0-3 ran on helper block 1 during the previous sub-step's DEM step: take over the
+    // fluid grid's header and the counts
+    if (tid() == 0) {
+      const WideCtl* c = m.wide;
+      if (c->prep_err) atomicOr(err, c->prep_err);
+      S.hA = c->prep_hdr;
+      S.n_edges = c->prep_edges;
+      out.ctr.n_fluid_edges = c->prep_edges;
+      out.ctr.density_iters = c->prep_iters;
+      out.stage[0] += c->prep_cycles[0];
+      out.stage[1] += c->prep_cycles[1];
+    }
+    __syncthreads();
+    if (*err) return;
+  } else {
+    uint32_t iters = 0;
+    unsigned long long cyc[2] = {0, 0};
+    stage_mark(out.stage, 0);
+    fluid_prep(m, U.pbf_iterations, dt, S, err, iters, cyc);
+    if (tid() == 0) {
+      out.ctr.n_fluid_edges = S.n_edges;
+      out.ctr.density_iters = iters;
+      out.stage[0] += cyc[0];
+      out.stage[1] += cyc[1];
+      g_stage_last = clock64();
+    }
+    __syncthreads();
+    if (*err) return;
+  }
+  // ball grid for the overlap push (pbf.rs:1214-1222); it reads only the balls, so it comes after
+  // steps 0-3 here
+  const float contact_radius = m.b_r + OVERLAP_PUSH_MARGIN * h;
+  if (nb > 0) grid_build(m.bx, nb, fmax_r(fmax_r(2.0f * m.b_r, contact_radius), 1e-6f), m.gBall, S.hBall, err);
+  stage_mark(out.stage, 0);
   // ---- step 3.5: ball overlap push (pbf.rs:1361-1444); two passes (count, fill), then the
   // per-ball reaction sums replayed in the reference's (fluid index, near order) order.
   for (uint32_t i = tid(); i < n; i += nthr()) m.push_ex[i] = make_float2(0.0f, 0.0f);
@@ -1713,6 +1764,7 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
   }
   stage_mark(out.stage, 6);
   // ---- density recompute at final x over the step-2 lists (pbf.rs:2137-2144)
+  const float self_rho = mass * poly6(0.0f, h);
   for (uint32_t i = tid(); i < n; i += nthr()) {
     V2 xi(X[i]);
     float rho = self_rho;

@@ -51,11 +51,26 @@ __global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDe
       else if (phase == WIDE_CG_SETUP) cg_setup_rows(m, U.dt, t0, stride);
       else if (phase == WIDE_JOINT_APPLY) joint_apply_rows(m, U.dt, vin, vout, t0, stride);
       else if (phase == WIDE_DRAG_PRE) drag_pre_balls(m, w0, nw);
+      else if (phase == WIDE_FLUID_PREP && blockIdx.x == 1) {
+        // the next sub-step's fluid steps 0-3, beside the mill block's DEM step
+        WideCtl* c = m.wide;
+        uint32_t iters = 0;
+        unsigned long long cyc[2] = {0, 0};
+        fluid_prep(m, U.pbf_iterations, c->prep_dt, fs, &c->prep_err, iters, cyc);
+        if (threadIdx.x == 0) {
+          c->prep_hdr = fs.hA;
+          c->prep_edges = fs.n_edges;
+          c->prep_iters = iters;
+          c->prep_cycles[0] = cyc[0];
+          c->prep_cycles[1] = cyc[1];
+        }
+      }
       return 0u;
     });
     return;
   }
   const uint32_t my_sub = n_sub_of ? n_sub_of[mill] : n_sub;
+  bool prepped = false;  // this sub-step's fluid steps 0-3 were published to helper block 1
   for (uint32_t s = 0; s < my_sub; ++s) {
     StepUniform& U = uni[mill];
     StepOut& out = m.out[s];
@@ -76,11 +91,25 @@ __global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDe
     __syncthreads();
     if (*m.err) break;
     // Without the fluid half, imp/ang hold the caller's external impulses (DEM-only entry point).
-    if (U.run_fluid) fluid_step(m, U, out, m.err, fs, dsm);
+    if (U.run_fluid) fluid_step(m, U, out, m.err, fs, dsm, prepped);
+    prepped = false;
     __syncthreads();
     if (*m.err) {  // the mill stops; the host reads the error bits from this sub-step's record
       if (threadIdx.x == 0) out.err = *m.err;
       break;
+    }
+    // With helper blocks, the next sub-step's fluid steps 0-3 (they touch only the fluid's arrays,
+    // which the DEM step does not) run on helper block 1 while this block runs the DEM step; the
+    // next fluid step waits for them first.
+    if (helpers && U.run_fluid && s + 1 < my_sub && m.nf > 0) {
+      const float dt_next = angles[(size_t)mill * n_sub + s + 1].dt;
+      if (dt_next > 0.0f) {
+        wide_publish(m, WIDE_FLUID_PREP, nullptr, nullptr, nullptr, [&](WideCtl* c) {
+          c->prep_dt = dt_next;
+          c->prep_err = 0u;
+        });
+        prepped = true;
+      }
     }
     if (U.run_dem) dem_step(m, U, out, m.impacts + (size_t)s * m.cap_impacts, m.err, ds, dsm);
     __syncthreads();

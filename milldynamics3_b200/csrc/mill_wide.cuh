@@ -23,7 +23,8 @@ enum : uint32_t {
   WIDE_BUOYANCY_ITEMS = 5,
   WIDE_CG_SETUP = 6,
   WIDE_JOINT_APPLY = 7,
-  WIDE_DRAG_PRE = 8
+  WIDE_DRAG_PRE = 8,
+  WIDE_FLUID_PREP = 9
 };
 
 
@@ -39,6 +40,44 @@ __device__ inline bool wide_wait(const uint32_t* p, uint32_t target, long long l
   return true;
 }
 
+// Mill block (helpers > 0): publishes a phase after the block's writes that it reads. pre(c), run
+// by thread 0 before the flag, fills the phase's own fields of the control block.
+template <class Pre>
+__device__ void wide_publish(const MillDev& m, uint32_t phase, const GridHdr* hdr, const float2* vin, float2* vout,
+                             Pre pre) {
+  __syncthreads();
+  WideCtl* c = m.wide;
+  if (tid() == 0) {
+    if (hdr) c->hdr = *hdr;
+    c->vin = vin;
+    c->vout = vout;
+    c->phase = phase;
+    c->counter = 0;
+    pre(c);
+    g_wide_seq += 1;
+    __threadfence();
+    *reinterpret_cast<volatile uint32_t*>(&c->seq) = g_wide_seq;
+  }
+}
+
+// Mill block (helpers > 0): waits until every helper block has finished the last published phase;
+// afterwards the block reads what they wrote.
+__device__ inline void wide_finish(const MillDev& m) {
+  __syncthreads();
+  if (tid() == 0) {
+    WideCtl* c = m.wide;
+    const long long lim = m.wide_wait_cycles > 0 ? m.wide_wait_cycles : WIDE_TIMEOUT_CYCLES;
+    if (!wide_wait(&c->done, g_wide_seq * (m.helpers + m.test_extra_helpers), lim)) {
+      atomicOr(m.err, ERR_WIDE);
+      // the helper blocks that did answer finish this phase before the mill's block goes on and
+      // overwrites what they read (bounded too); the launch then ends at the next error check
+      wide_wait(&c->done, g_wide_seq * m.helpers);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
 // Mill block: one phase over all of the mill's warps. share(w0, nw) is called by every thread of
 // the block with w0 = the thread's warp and nw = the warps of all of the mill's blocks.
 template <class F>
@@ -50,31 +89,9 @@ __device__ void wide_phase(const MillDev& m, uint32_t phase, const GridHdr* hdr,
     __syncthreads();
     return;
   }
-  __syncthreads();
-  WideCtl* c = m.wide;
-  if (tid() == 0) {
-    if (hdr) c->hdr = *hdr;
-    c->vin = vin;
-    c->vout = vout;
-    c->phase = phase;
-    c->counter = 0;
-    g_wide_seq += 1;
-    __threadfence();
-    *reinterpret_cast<volatile uint32_t*>(&c->seq) = g_wide_seq;
-  }
+  wide_publish(m, phase, hdr, vin, vout, [](WideCtl*) {});
   share(warp, (1u + m.helpers) * nwarps);
-  __syncthreads();
-  if (tid() == 0) {
-    const long long lim = m.wide_wait_cycles > 0 ? m.wide_wait_cycles : WIDE_TIMEOUT_CYCLES;
-    if (!wide_wait(&c->done, g_wide_seq * (m.helpers + m.test_extra_helpers), lim)) {
-      atomicOr(m.err, ERR_WIDE);
-      // the helper blocks that did answer finish this phase before the mill's block goes on and
-      // overwrites what they read (bounded too); the launch then ends at the next error check
-      wide_wait(&c->done, g_wide_seq * m.helpers);
-    }
-    __threadfence();
-  }
-  __syncthreads();
+  wide_finish(m);
 }
 
 template <class F>
