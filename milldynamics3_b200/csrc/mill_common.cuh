@@ -263,6 +263,12 @@ struct WideCtl {
   GridHdr prep_hdr;
   uint32_t prep_edges, prep_iters;
   unsigned long long prep_cycles[2];
+  // the finished sub-step's fluid tail (mean shear rate, speed clamp and their kinetic-energy
+  // terms), run by helper block 1 before the steps 0-3 above when tail_out is set: that sub-step's
+  // output record, its speed cap and the fluid kinetic energy before the viscosity solve
+  StepOut* tail_out;
+  float tail_vmax;
+  double tail_ke;
 };
 
 // ---------------------------------------------------------------- per-mill descriptor

@@ -1386,8 +1386,70 @@ static __device__ void fluid_prep(const MillDev& m, uint32_t pbf_iterations, flo
   }
 }
 
-static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err, FluidShared& S,
-                           unsigned char* dsm, bool prepped) {
+// The fluid step's tail after the viscosity solve: the mean shear rate on the solved velocities
+// (pbf.rs:800-849), then the speed clamp (pbf.rs:979-996, 2321), with the kinetic-energy terms of
+// both (ke_mark: the fluid's kinetic energy before the solve). It reads and writes only the
+// fluid's arrays and the three stats it sets in fs, and nothing later in the sub-step reads them,
+// so in a single-mill launch helper block 1 runs it (ahead of the next sub-step's steps 0-3) while
+// the mill's block runs the DEM step. Returns the clock cycles it took (thread 0).
+static __device__ unsigned long long fluid_tail(const MillDev& m, float v_max, double ke_mark, MgFluidStepStats& fs,
+                                                FluidShared& S) {
+  const long long t0 = clock64();
+  const uint32_t n = m.nf;
+  const float h = m.f_h, mass = m.f_mass;
+  const float2* X = m.fx;
+  float2* V = m.fv;
+  // ---- mean shear rate (pbf.rs:800-849) on the final velocities
+  for (uint32_t i = tid(); i < n; i += nthr()) {
+    V2 xi(X[i]), vi(V[i]);
+    float gxx = 0.0f, gxy = 0.0f, gyx = 0.0f, gyy = 0.0f;
+    for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
+      uint32_t j = m.nbrs[k];
+      V2 delta = xi - V2(X[j]);
+      float r = delta.len();
+      V2 grad = spiky_grad(delta, r, h);
+      float coeff = mass / fmax_r(m.density[j], 1e-6f);
+      V2 dv = V2(V[j]) - vi;
+      gxx += coeff * dv.x * grad.x;
+      gxy += coeff * dv.x * grad.y;
+      gyx += coeff * dv.y * grad.x;
+      gyy += coeff * dv.y * grad.y;
+    }
+    float dxy = 0.5f * (gxy + gyx);
+    m.f_tmp[i] = sqrtf(2.0f * (gxx * gxx + gyy * gyy + 2.0f * dxy * dxy));
+  }
+  __syncthreads();
+  {
+    const float s = block_seq_sum_f32<true>(0.0f, n, [&](uint32_t i) { return m.f_tmp[i]; });
+    uint32_t c = 0;
+    for (uint32_t i = tid(); i < n; i += nthr()) c += finite_f(m.f_tmp[i]) ? 1u : 0u;
+    c = block_sum_u(c);
+    if (tid() == 0) fs.mean_shear_rate_per_s = c == 0 ? 0.0f : s / (float)c;
+  }
+  __syncthreads();
+  const double ke_after_visc = kinetic_energy_seq(V, n, mass, S);
+  // ---- step 7.5: speed clamp (pbf.rs:979-996, 2321)
+  for (uint32_t i = tid(); i < n; i += nthr()) {
+    V2 v(V[i]);
+    float speed = v.len();
+    if (!finite_f(speed)) v = V2();
+    else if (speed > v_max) v *= v_max / speed;
+    V[i] = v.f2();
+  }
+  __syncthreads();
+  const double ke_after_clamp = kinetic_energy_seq(V, n, mass, S);
+  if (tid() == 0) {
+    fs.ke_delta_viscosity_j = (float)(ke_after_visc - ke_mark);
+    fs.ke_delta_clamp_j = (float)(ke_after_clamp - ke_after_visc);
+  }
+  __syncthreads();
+  return (unsigned long long)(clock64() - t0);
+}
+
+// defer_tail: leave fluid_tail to helper block 1 (the caller publishes it). Returns whether the
+// tail was left out; *ke_tail then receives its ke_mark argument.
+static __device__ bool fluid_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err, FluidShared& S,
+                                  unsigned char* dsm, bool prepped, bool defer_tail, double* ke_tail) {
   if (prepped) wide_finish(m);   // helper block 1 ran steps 0-3 (published with WIDE_FLUID_PREP)
   uint32_t* done = m.ball_done;  // completion flags of the per-ball sweeps (moved to shared below)
   const uint32_t n = m.nf, nb = m.nb;
@@ -1395,7 +1457,7 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
   for (uint32_t b = tid(); b < nb; b += nthr()) { m.imp[b] = make_float2(0.0f, 0.0f); m.ang[b] = 0.0f; }
   if (tid() == 0) { memset(&out.fs, 0, sizeof(out.fs)); out.clamp_hits = 0; out.fluid_momentum[0] = out.fluid_momentum[1] = 0.0f; }
   __syncthreads();
-  if (n == 0 || dt <= 0.0f) return;
+  if (n == 0 || dt <= 0.0f) return false;
   const float h = m.f_h, rho0 = m.f_rho0, mass = m.f_mass;
   float2* X = m.fx;
   float2* V = m.fv;
@@ -1413,7 +1475,7 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
       out.stage[1] += c->prep_cycles[1];
     }
     __syncthreads();
-    if (*err) return;
+    if (*err) return false;
   } else {
     uint32_t iters = 0;
     unsigned long long cyc[2] = {0, 0};
@@ -1427,7 +1489,7 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
       g_stage_last = clock64();
     }
     __syncthreads();
-    if (*err) return;
+    if (*err) return false;
   }
   // ball grid for the overlap push (pbf.rs:1214-1222); it reads only the balls, so it comes after
   // steps 0-3 here
@@ -1485,7 +1547,7 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
         __syncthreads();
         S.n_recs = 0;
         uint32_t tot = block_exclusive_scan(m.rec_cnt, n + 1);
-        if (tot > m.cap_recs) { if (tid() == 0) atomicOr(err, ERR_RECORDS); __syncthreads(); return; }
+        if (tot > m.cap_recs) { if (tid() == 0) atomicOr(err, ERR_RECORDS); __syncthreads(); return false; }
         if (tid() == 0) S.n_recs = tot;
         __syncthreads();
       }
@@ -1545,7 +1607,7 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
     if (h_adh > 0.0f) {
       wide_phase(m, WIDE_ADHESION, &S.hA, [&](uint32_t w0, uint32_t nw) { adhesion_balls(m, U, S.hA, w0, nw); });
       __syncthreads();
-      if (*err) return;
+      if (*err) return false;
       // per-fluid sums of the balls' contributions in ball order (stable bucket sort by fluid)
       uint32_t nrec = pack_ball_items(m.item_j, m.item_n, m.cap_items, nb, m.rec_off, m.rec_i, m.rec_b);
       for (uint32_t b = tid() >> 5; b < nb; b += nthr() >> 5) {
@@ -1746,13 +1808,13 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
   // ---- step 6.5: ball drag, Gauss-Seidel over balls (pbf.rs:1777-2013)
   const float mu = fmax_r(U.slurry.viscosity_pa_s, 0.0f);
   const uint32_t* drag_order = nullptr;  // the drag sweep's claim order, when it ran by level
-  if (!drag_step(m, U, out, err, S, X, V, done, sweep_scratch, sweep_words, &drag_order)) return;
+  if (!drag_step(m, U, out, err, S, X, V, done, sweep_scratch, sweep_words, &drag_order)) return false;
   stage_mark(out.stage, 19);
   double ke_after_drag = kinetic_energy_seq(V, n, mass, S);
   const double ke_delta_drag = ke_after_drag - ke_mark;
   ke_mark = ke_after_drag;
   // ---- step 6.6: buoyancy, Gauss-Seidel over balls on the stale step-2 grid (pbf.rs:2035-2122)
-  if (!buoyancy_step(m, U, out, err, S, X, V, done, sweep_scratch, sweep_words, drag_order)) return;
+  if (!buoyancy_step(m, U, out, err, S, X, V, done, sweep_scratch, sweep_words, drag_order)) return false;
   double ke_after_buoy = kinetic_energy_seq(V, n, mass, S);
   const double ke_delta_buoy = ke_after_buoy - ke_mark;
   ke_mark = ke_after_buoy;
@@ -1775,50 +1837,19 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
   stage_mark(out.stage, 7);
   // ---- step 7: implicit viscosity (pbf.rs:2146-2300)
   uint32_t visc_iters = 0;
-  if (!viscosity_step(m, U, out, err, S, X, V, mu, visc_iters)) return;
+  if (!viscosity_step(m, U, out, err, S, X, V, mu, visc_iters)) return false;
   stage_mark(out.stage, 11);
-  // ---- mean shear rate (pbf.rs:800-849) on the final velocities
-  for (uint32_t i = tid(); i < n; i += nthr()) {
-    V2 xi(X[i]), vi(V[i]);
-    float gxx = 0.0f, gxy = 0.0f, gyx = 0.0f, gyy = 0.0f;
-    for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
-      uint32_t j = m.nbrs[k];
-      V2 delta = xi - V2(X[j]);
-      float r = delta.len();
-      V2 grad = spiky_grad(delta, r, h);
-      float coeff = mass / fmax_r(m.density[j], 1e-6f);
-      V2 dv = V2(V[j]) - vi;
-      gxx += coeff * dv.x * grad.x;
-      gxy += coeff * dv.x * grad.y;
-      gyx += coeff * dv.y * grad.x;
-      gyy += coeff * dv.y * grad.y;
+  // ---- mean shear rate and step 7.5, the speed clamp (fluid_tail); they touch nothing that
+  // step 8 or the DEM step reads
+  if (defer_tail) {
+    *ke_tail = ke_mark;
+  } else {
+    const unsigned long long cyc = fluid_tail(m, fluid_vmax(U), ke_mark, out.fs, S);
+    if (tid() == 0) {
+      out.stage[12] += cyc;
+      g_stage_last = clock64();
     }
-    float dxy = 0.5f * (gxy + gyx);
-    m.f_tmp[i] = sqrtf(2.0f * (gxx * gxx + gyy * gyy + 2.0f * dxy * dxy));
   }
-  __syncthreads();
-  {
-    const float s = block_seq_sum_f32<true>(0.0f, n, [&](uint32_t i) { return m.f_tmp[i]; });
-    uint32_t c = 0;
-    for (uint32_t i = tid(); i < n; i += nthr()) c += finite_f(m.f_tmp[i]) ? 1u : 0u;
-    c = block_sum_u(c);
-    if (tid() == 0) out.fs.mean_shear_rate_per_s = c == 0 ? 0.0f : s / (float)c;
-  }
-  __syncthreads();
-  stage_mark(out.stage, 12);
-  double ke_after_visc = kinetic_energy_seq(V, n, mass, S);
-  const double ke_delta_visc = ke_after_visc - ke_mark;
-  // ---- step 7.5: speed clamp (pbf.rs:979-996, 2321)
-  const float v_max = fluid_vmax(U);
-  for (uint32_t i = tid(); i < n; i += nthr()) {
-    V2 v(V[i]);
-    float speed = v.len();
-    if (!finite_f(speed)) v = V2();
-    else if (speed > v_max) v *= v_max / speed;
-    V[i] = v.f2();
-  }
-  __syncthreads();
-  double ke_after_clamp = kinetic_energy_seq(V, n, mass, S);
   // ---- step 8: impulse clamp (pbf.rs:2330-2345)
   uint32_t hits = 0;
   if (nb > 0) {
@@ -1844,13 +1875,12 @@ static __device__ void fluid_step(const MillDev& m, const StepUniform& U, StepOu
     out.fs.ke_delta_noslip_j = (float)ke_delta_noslip;
     out.fs.ke_delta_drag_j = (float)ke_delta_drag;
     out.fs.ke_delta_buoyancy_j = (float)ke_delta_buoy;
-    out.fs.ke_delta_viscosity_j = (float)ke_delta_visc;
-    out.fs.ke_delta_clamp_j = (float)(ke_after_clamp - ke_after_visc);
     out.fluid_momentum[0] = S.fscal[0];
     out.fluid_momentum[1] = S.fscal[1];
   }
   __syncthreads();
   stage_mark(out.stage, 13);
+  return defer_tail;
 }
 
 }  // namespace mg

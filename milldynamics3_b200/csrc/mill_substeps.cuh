@@ -54,6 +54,12 @@ __global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDe
       else if (phase == WIDE_FLUID_PREP && blockIdx.x == 1) {
         // the next sub-step's fluid steps 0-3, beside the mill block's DEM step
         WideCtl* c = m.wide;
+        if (c->tail_out) {
+          // the finished sub-step's fluid tail first (it reads the velocities the steps 0-3 change)
+          StepOut* to = c->tail_out;
+          const unsigned long long tc = fluid_tail(m, c->tail_vmax, c->tail_ke, to->fs, fs);
+          if (threadIdx.x == 0) to->stage[12] += tc;
+        }
         uint32_t iters = 0;
         unsigned long long cyc[2] = {0, 0};
         fluid_prep(m, U.pbf_iterations, c->prep_dt, fs, &c->prep_err, iters, cyc);
@@ -90,26 +96,31 @@ __global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDe
     }
     __syncthreads();
     if (*m.err) break;
+    // With helper blocks, the next sub-step's fluid steps 0-3 (they touch only the fluid's arrays,
+    // which the DEM step does not) run on helper block 1 while this block runs the DEM step, and
+    // so does this sub-step's fluid tail before them; the next fluid step waits for both first.
+    const float dt_next = helpers && s + 1 < my_sub ? angles[(size_t)mill * n_sub + s + 1].dt : 0.0f;
+    const bool prep_next = helpers && U.run_fluid && s + 1 < my_sub && m.nf > 0 && dt_next > 0.0f;
     // Without the fluid half, imp/ang hold the caller's external impulses (DEM-only entry point).
-    if (U.run_fluid) fluid_step(m, U, out, m.err, fs, dsm, prepped);
+    double ke_tail = 0.0;
+    bool tail_deferred = false;
+    if (U.run_fluid) tail_deferred = fluid_step(m, U, out, m.err, fs, dsm, prepped, prep_next, &ke_tail);
     prepped = false;
     __syncthreads();
     if (*m.err) {  // the mill stops; the host reads the error bits from this sub-step's record
       if (threadIdx.x == 0) out.err = *m.err;
       break;
     }
-    // With helper blocks, the next sub-step's fluid steps 0-3 (they touch only the fluid's arrays,
-    // which the DEM step does not) run on helper block 1 while this block runs the DEM step; the
-    // next fluid step waits for them first.
-    if (helpers && U.run_fluid && s + 1 < my_sub && m.nf > 0) {
-      const float dt_next = angles[(size_t)mill * n_sub + s + 1].dt;
-      if (dt_next > 0.0f) {
-        wide_publish(m, WIDE_FLUID_PREP, nullptr, nullptr, nullptr, [&](WideCtl* c) {
-          c->prep_dt = dt_next;
-          c->prep_err = 0u;
-        });
-        prepped = true;
-      }
+    if (prep_next) {
+      const float v_max = fluid_vmax(U);
+      wide_publish(m, WIDE_FLUID_PREP, nullptr, nullptr, nullptr, [&](WideCtl* c) {
+        c->prep_dt = dt_next;
+        c->prep_err = 0u;
+        c->tail_out = tail_deferred ? &out : nullptr;
+        c->tail_vmax = v_max;
+        c->tail_ke = ke_tail;
+      });
+      prepped = true;
     }
     if (U.run_dem) dem_step(m, U, out, m.impacts + (size_t)s * m.cap_impacts, m.err, ds, dsm);
     __syncthreads();
