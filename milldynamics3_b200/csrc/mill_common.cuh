@@ -269,7 +269,19 @@ struct WideCtl {
   StepOut* tail_out;
   float tail_vmax;
   double tail_ke;
+  // the work the helper blocks do beside the drag sweep (WIDE_BESIDE_DRAG): which parts run
+  // (BESIDE_*), the viscosity the Morris weights use; helper block 1 publishes the group grid's
+  // header (beside_grid_seq = the phase's sequence number once it is built); the other helpers
+  // count their finished buoyancy item shares (beside_buoy_blocks); helper block 1 leaves the
+  // buoyancy records' count and whether it found a claim order
+  uint32_t beside_tasks;
+  float beside_mu;
+  uint32_t beside_grid_seq;
+  uint32_t beside_buoy_blocks;
+  GridHdr beside_hdr;
+  uint32_t beside_nrec, beside_order_ok;
 };
+enum : uint32_t { BESIDE_VISC = 1u, BESIDE_BUOY = 2u };
 
 // ---------------------------------------------------------------- per-mill descriptor
 struct MillDev {
@@ -333,6 +345,19 @@ struct MillDev {
   double* f_cw;  // per-ball coupling work of the predict step
   uint32_t *rec_off, *rec_pred, *ball_done;  // per-ball sweep records (cap_nb + 1, cap_recs, cap_nb)
   uint32_t* slot;  // per-warp fluid -> item maps of the in-order merges (warps of all the mill's blocks x cap_nf, all NONE at rest)
+  // single-mill handles with helper blocks: the item lists the helpers fill beside the drag sweep
+  // (boundary groups in gi_*, buoyancy items in bi_*, cap_items per ball like item_*), the
+  // buoyancy records (b_rec_*: offsets, fluid index, ball, predecessor ball), the helpers'
+  // bucket-sort scratch and the buoyancy sweep's claim order; null otherwise
+  uint32_t* gi_j;
+  float2* gi_v;
+  float *gi_w, *gi_w2;
+  uint32_t *bi_j, *bi_n;
+  float2* bi_v;
+  float* bi_w;
+  uint32_t *b_rec_off, *b_rec_i, *b_rec_b, *b_rec_pred;
+  uint32_t *hb_start, *hb_cur, *hb_order;
+  uint32_t* b_order;
   uint32_t *pair_i, *pair_j;
   float* lam_bb;
   uint32_t* pr_list;  // pairs within reach of touching at the start of the projection

@@ -362,9 +362,20 @@ static __device__ void adhesion_balls(const MillDev& m, const StepUniform& U, co
   }
 }
 
+// Per-ball item lists (cap_items per ball): fluid index, offset / lever, weight, second weight.
+struct ItemLists {
+  uint32_t* j;
+  float2* v;
+  float* w;
+  float* w2;
+};
+__device__ __forceinline__ ItemLists mill_items(const MillDev& m) { return {m.item_j, m.item_v, m.item_w, m.item_w2}; }
+
 // Boundary groups per ball (pbf.rs:2159-2232) on the fresh h-grid: candidates of each boundary
-// point merged per fluid particle in first-seen order; the ball's group count in g_off[b].
-static __device__ void group_balls(const MillDev& m, const StepUniform& U, const GridHdr& hB, uint32_t w0, uint32_t nw) {
+// point merged per fluid particle in first-seen order into the lists I; the ball's group count in
+// g_off[b]. slot_warp: the warp's merge slot map (a warp index of the mill's blocks).
+static __device__ void group_balls(const MillDev& m, const StepUniform& U, const GridHdr& hB, uint32_t w0, uint32_t nw,
+                                   const ItemLists& I, uint32_t slot_warp) {
   const uint32_t nb = m.nb, count_pb = U.boundary_count;
   const float h = m.f_h;
   const float2* X = m.fx;
@@ -372,10 +383,10 @@ static __device__ void group_balls(const MillDev& m, const StepUniform& U, const
   const float eta2 = VISC_ETA * h * h;
   const float spiky_norm = -30.0f / (PI_F * powi5(h));
   const float range2 = h * h * (1.0f + 1e-4f);
-  uint32_t* slot = m.slot + (size_t)w0 * m.cap_nf;
+  uint32_t* slot = m.slot + (size_t)slot_warp * m.cap_nf;
   for (uint32_t b = w0; b < nb; b += nw) {
     const uint32_t lane = tid() & 31u, base = b * m.cap_items;
-    const MergeList L{m.item_j + base, m.item_w + base, m.item_v + base, m.item_w2 + base, m.cap_items};
+    const MergeList L{I.j + base, I.w + base, I.v + base, I.w2 + base, m.cap_items};
     uint32_t cnt = 0;
     bool overflow = false;
     const V2 xb(m.bx[b]);
@@ -545,7 +556,8 @@ static __device__ uint32_t drag_item_balls(const MillDev& m, const GridHdr& hB, 
 // Buoyancy item lists per ball (pbf.rs:2042-2060) on the stale step-2 grid: fluid particles with a
 // positive poly6 weight in for_each_near order, their weights, and the local density (item_v[0]).
 // Returns the thread's part of the item count.
-static __device__ uint32_t buoyancy_item_balls(const MillDev& m, const GridHdr& hA, uint32_t w0, uint32_t nw) {
+static __device__ uint32_t buoyancy_item_balls(const MillDev& m, const GridHdr& hA, uint32_t w0, uint32_t nw,
+                                               const ItemLists& I, uint32_t* item_n) {
   const uint32_t nb = m.nb;
   const float h = m.f_h, mass = m.f_mass;
   const float2* X = m.fx;
@@ -566,7 +578,7 @@ static __device__ uint32_t buoyancy_item_balls(const MillDev& m, const GridHdr& 
         const bool keep = w > 0.0f;
         const uint32_t bal = __ballot_sync(FULL, keep);
         const uint32_t pos = cnt + __popc(bal & ((1u << lane) - 1u));
-        if (keep && pos < m.cap_items) { m.item_j[base + pos] = j; m.item_w[base + pos] = w; }
+        if (keep && pos < m.cap_items) { I.j[base + pos] = j; I.w[base + pos] = w; }
 #pragma unroll
         for (int t = 0; t < 32; ++t) {
           const float wt = __shfl_sync(FULL, w, t);
@@ -577,9 +589,9 @@ static __device__ uint32_t buoyancy_item_balls(const MillDev& m, const GridHdr& 
     }
     if (cnt > m.cap_items) { if (lane == 0) atomicOr(err, ERR_ITEMS); cnt = 0; }
     if (lane == 0) {
-      m.item_n[b] = rho_local > 0.0f ? cnt : 0u;
+      item_n[b] = rho_local > 0.0f ? cnt : 0u;
       if (rho_local > 0.0f) items += cnt;
-      m.item_v[base] = make_float2(rho_local, 0.0f);
+      I.v[base] = make_float2(rho_local, 0.0f);
     }
     __syncwarp();
   }
@@ -806,7 +818,7 @@ static __device__ __noinline__ void drag_sweep(const MillDev& m, const StepUnifo
 static __device__ __noinline__ bool drag_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err,
                                               FluidShared& S, float2* X, float2* V, uint32_t* done,
                                               uint32_t* scratch, uint32_t scratch_words,
-                                              const uint32_t** order_out) {
+                                              const uint32_t** order_out, uint32_t* beside_out) {
   const uint32_t n = m.nf, nb = m.nb;
   const float h = m.f_h, rho0 = m.f_rho0, mass = m.f_mass, dt = U.dt;
   (void)rho0;
@@ -853,6 +865,23 @@ static __device__ __noinline__ bool drag_step(const MillDev& m, const StepUnifor
         K[DK_B_RTRUE] = m.b_rtrue;
       }
       __syncthreads();
+      // With two or more helper blocks, the helpers do what reads only the final positions beside
+      // the sweep (beside_drag): the buoyancy item lists, records and claim order and, without the
+      // Bingham rheology (its viscosity reads the velocities), the density recompute, the
+      // viscosity's Morris weights and its boundary groups.
+      if (m.helpers >= 2 && m.bi_j != nullptr) {
+        const bool bingham = U.slurry.rheology == MG_RHEOLOGY_BINGHAM && U.slurry.yield_stress_pa > 0.0f;
+        const uint32_t tasks = BESIDE_BUOY | (bingham ? 0u : BESIDE_VISC);
+        wide_publish(m, WIDE_BESIDE_DRAG, &S.hA, nullptr, nullptr, [&](WideCtl* c) {
+          c->beside_tasks = tasks;
+          c->beside_mu = mu;
+          c->beside_grid_seq = 0u;
+          c->beside_buoy_blocks = 0u;
+          c->beside_nrec = 0u;
+          c->beside_order_ok = 0u;
+        });
+        *beside_out = tasks;
+      }
       drag_sweep(m, U, out, err, V, done, order);
       if (tid() == 0 && U.want_momentum) {
         V2 mom(S.fscal[0], S.fscal[1]);
@@ -870,11 +899,22 @@ static __device__ __noinline__ bool drag_step(const MillDev& m, const StepUnifor
   return true;
 }
 
-// The buoyancy sweep proper (pbf.rs:2042-2121): balls in dependency order over the item lists,
+// The buoyancy sweep's item lists and records: per-ball item counts, fluid indices, weights and
+// local densities (v[b * cap_items].x), record offsets per ball and predecessor balls.
+struct BuoyLists {
+  const uint32_t* n;
+  const uint32_t* j;
+  const float* w;
+  const float2* v;
+  const uint32_t* rec_off;
+  const uint32_t* rec_pred;
+};
+
+// The buoyancy sweep proper (pbf.rs:2042-2121): balls in dependency order over the item lists BL,
 // on the velocities V at positions X. Its own function, like drag_sweep.
 static __device__ __noinline__ void buoyancy_sweep(const MillDev& m, const StepUniform& U, StepOut& out,
                                                    uint32_t* err, const float2* X, float2* V, uint32_t* done,
-                                                   const uint32_t* order) {
+                                                   const uint32_t* order, const BuoyLists& BL) {
   const uint32_t nb = m.nb;
   const bool want_mom = U.want_momentum != 0;
   if (tid() == 0) {
@@ -895,21 +935,21 @@ static __device__ __noinline__ void buoyancy_sweep(const MillDev& m, const StepU
     bool valid;
   };
   ball_dataflow(
-      nb, m.rec_off, m.rec_pred, done, order, U.sweep_warps, U.spin_ns, U.spin_limit, NONE, err, &out.stage[35],
+      nb, BL.rec_off, BL.rec_pred, done, order, U.sweep_warps, U.spin_ns, U.spin_limit, NONE, err, &out.stage[35],
       // before the wait: item geometry, the weight sum and the weight fractions, which the sweep does
       // not change
       [&](uint32_t b, int lane) {
         BuoyBall q;
-        q.cnt = m.item_n[b];
+        q.cnt = BL.n[b];
         q.j = 0;
         q.w = 0.0f;
         q.valid = false;
         if (q.cnt == 0) return q;
         const uint32_t base = b * m.cap_items, cnt = q.cnt;
-        const float rho_local = m.item_v[base].x;
+        const float rho_local = BL.v[base].x;
         if ((uint32_t)lane < cnt) {
-          q.j = m.item_j[base + lane];
-          q.w = m.item_w[base + lane];
+          q.j = BL.j[base + lane];
+          q.w = BL.w[base + lane];
           q.d = V2(X[q.j]);
           q.d2 = q.d.len2();
           q.valid = !(q.d2 <= 1e-12f);
@@ -923,8 +963,8 @@ static __device__ __noinline__ void buoyancy_sweep(const MillDev& m, const StepU
           if (s < cnt) {
             if (s < 32) {
               if (q.valid) dvw = q.w;
-            } else if (!(V2(X[m.item_j[base + s]]).len2() <= 1e-12f)) {
-              dvw = m.item_w[base + s];
+            } else if (!(V2(X[BL.j[base + s]]).len2() <= 1e-12f)) {
+              dvw = BL.w[base + s];
             }
           }
           lane_seq_sum1(den, dvw, lim);
@@ -955,10 +995,10 @@ static __device__ __noinline__ void buoyancy_sweep(const MillDev& m, const StepU
             if (s < 32) {
               if (q.valid) nv = q.w * cross2(q.d, V2(V_l[q.j])) / q.d2;
             } else {
-              uint32_t j = m.item_j[base + s];
+              uint32_t j = BL.j[base + s];
               V2 d(X[j]);
               float d2 = d.len2();
-              if (!(d2 <= 1e-12f)) nv = m.item_w[base + s] * cross2(d, V2(V_l[j])) / d2;
+              if (!(d2 <= 1e-12f)) nv = BL.w[base + s] * cross2(d, V2(V_l[j])) / d2;
             }
           }
           lane_seq_sum1(num, nv, lim);
@@ -970,12 +1010,12 @@ static __device__ __noinline__ void buoyancy_sweep(const MillDev& m, const StepU
         V2 impulse = -rho_eff * K[BK_AREA] * g_eff * K[BK_DT];
         const float mass_l = K[BK_MASS];
         for (uint32_t s = lane; s < cnt; s += 32) {
-          const uint32_t j = s < 32 ? q.j : m.item_j[base + s];
-          float frac = s < 32 ? q.frac : m.item_w[base + s] / rho_local;
+          const uint32_t j = s < 32 ? q.j : BL.j[base + s];
+          float frac = s < 32 ? q.frac : BL.w[base + s] / rho_local;
           V2 dv = -(impulse * frac) / mass_l;
           V_l[j] = (V2(V_l[j]) + dv).f2();
           if (s < 32) q.dv = dv;
-          else if (want_mom) m.rec_M[m.rec_off[b] + s] = (mass_l * dv).f2();
+          else if (want_mom) m.rec_M[BL.rec_off[b] + s] = (mass_l * dv).f2();
         }
         if (lane == 0) {
           float* slw = g_ball_slot[threadIdx.x >> 5];
@@ -986,7 +1026,7 @@ static __device__ __noinline__ void buoyancy_sweep(const MillDev& m, const StepU
       // after the flag: the ball's impulse, the momentum records
       [&](uint32_t b, int lane, BuoyBall& q) {
         if (q.cnt == 0) return;
-        if (want_mom && (uint32_t)lane < q.cnt) m.rec_M[m.rec_off[b] + lane] = (m.f_mass * q.dv).f2();
+        if (want_mom && (uint32_t)lane < q.cnt) m.rec_M[BL.rec_off[b] + lane] = (m.f_mass * q.dv).f2();
         if (lane == 0) {
           const float* sl = g_ball_slot[threadIdx.x >> 5];
           m.imp[b] = (V2(m.imp[b]) + V2(sl[BS_IMPULSE], sl[BS_IMPULSE + 1])).f2();
@@ -995,15 +1035,41 @@ static __device__ __noinline__ void buoyancy_sweep(const MillDev& m, const StepU
 }
 
 // Step 6.6 (pbf.rs:2035-2122): the buoyancy sweep on the stale step-2 grid, in its own function
-// like the drag sweep. Returns false when the item lists failed (the error is in *err).
+// like the drag sweep. beside: the helper blocks listed the items, records and claim order beside
+// the drag sweep (WIDE_BESIDE_DRAG, still running); they are waited for first. Returns false when
+// the item lists failed (the error is in *err).
 static __device__ __noinline__ bool buoyancy_step(const MillDev& m, const StepUniform& U, StepOut& out,
                                                   uint32_t* err, FluidShared& S, float2* X, float2* V,
                                                   uint32_t* done, uint32_t* scratch, uint32_t scratch_words,
-                                                  const uint32_t* drag_order) {
+                                                  const uint32_t* drag_order, bool beside) {
   const uint32_t n = m.nf, nb = m.nb;
+  if (beside) {
+    wide_finish(m);
+    const uint32_t n_items = wide_counter(m);
+    if (tid() == 0) out.ctr.n_coupling_items += n_items;
+    __syncthreads();
+    if (*err) return false;
+    stage_mark(out.stage, 27);
+    const WideCtl* c = m.wide;
+    const uint32_t nrec = c->beside_nrec;
+    const uint32_t* order = c->beside_order_ok ? m.b_order : nullptr;
+    stage_mark(out.stage, 28);
+    buoyancy_sweep(m, U, out, err, X, V, done, order, BuoyLists{m.bi_n, m.bi_j, m.bi_w, m.bi_v, m.b_rec_off, m.b_rec_pred});
+    if (tid() == 0 && U.want_momentum) {
+      V2 mom(S.fscal[0], S.fscal[1]);
+      for (uint32_t r = 0; r < nrec; ++r) mom += V2(m.rec_M[r]);
+      S.fscal[0] = mom.x;
+      S.fscal[1] = mom.y;
+    }
+    __syncthreads();
+    stage_mark(out.stage, 29);
+    return true;
+  }
   if (nb > 0 && m.b_r > 0.0f) {
     uint32_t n_items = 0;
-    wide_phase(m, WIDE_BUOYANCY_ITEMS, &S.hA, [&](uint32_t w0, uint32_t nw) { n_items += buoyancy_item_balls(m, S.hA, w0, nw); });
+    wide_phase(m, WIDE_BUOYANCY_ITEMS, &S.hA, [&](uint32_t w0, uint32_t nw) {
+      n_items += buoyancy_item_balls(m, S.hA, w0, nw, mill_items(m), m.item_n);
+    });
     n_items = block_sum_u(n_items) + wide_counter(m);
     if (tid() == 0) out.ctr.n_coupling_items += n_items;
     __syncthreads();
@@ -1023,7 +1089,8 @@ static __device__ __noinline__ bool buoyancy_step(const MillDev& m, const StepUn
     if (reuse) order = order_respects(L.pos, m.rec_b, m.rec_pred, nrec) ? drag_order : nullptr;
     else if (by_level) order = ball_level_order(nb, m.rec_off, m.rec_pred, L);
     stage_mark(out.stage, 28);
-    buoyancy_sweep(m, U, out, err, X, V, done, order);
+    buoyancy_sweep(m, U, out, err, X, V, done, order,
+                   BuoyLists{m.item_n, m.item_j, m.item_w, m.item_v, m.rec_off, m.rec_pred});
     if (tid() == 0 && U.want_momentum) {
       V2 mom(S.fscal[0], S.fscal[1]);
       for (uint32_t r = 0; r < nrec; ++r) mom += V2(m.rec_M[r]);
@@ -1036,6 +1103,55 @@ static __device__ __noinline__ bool buoyancy_step(const MillDev& m, const StepUn
   return true;
 }
 
+// Density recompute at the final positions X over the step-2 neighbour lists (pbf.rs:2132-2144).
+static __device__ void density_recompute(const MillDev& m, const float2* X) {
+  const uint32_t n = m.nf;
+  const float h = m.f_h, mass = m.f_mass;
+  const float self_rho = mass * poly6(0.0f, h);
+  for (uint32_t i = tid(); i < n; i += nthr()) {
+    V2 xi(X[i]);
+    float rho = self_rho;
+    for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) rho += mass * poly6((xi - V2(X[m.nbrs[k]])).len2(), h);
+    m.density[i] = rho;
+  }
+  __syncthreads();
+}
+
+// The viscosity's Morris weights and unit directions per edge (morris_weights, pbf.rs:312-345,
+// called at pbf.rs:2154) from mu_eff and the recomputed densities at positions X.
+static __device__ void morris_weights(const MillDev& m, const float2* X) {
+  const uint32_t n = m.nf;
+  const float h = m.f_h, mass = m.f_mass;
+  const float eta2 = VISC_ETA * h * h;
+  for (uint32_t i = tid(); i < n; i += nthr()) {
+    V2 xi(X[i]);
+    float rho_i = fmax_r(m.density[i], 1e-6f);
+    float mu_i = m.mu_eff[i];
+    for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
+      uint32_t j = m.nbrs[k];
+      float rho_j = fmax_r(m.density[j], 1e-6f);
+      V2 delta = xi - V2(X[j]);
+      float r = delta.len();
+      V2 grad = spiky_grad(delta, r, h);
+      float numerator = (mass * (mu_i + m.mu_eff[j]) / (rho_i * rho_j)) * fabsf(delta.dot(grad));
+      m.visc_w[k] = numerator / (delta.len2() + eta2);
+      m.visc_dir[k] = (r > 1e-9f ? delta / r : V2(1.0f, 0.0f)).f2();
+    }
+  }
+  __syncthreads();
+}
+
+// The boundary groups' per-particle factors (fluid_factor, pbf.rs:2172-2178, in f_tmp) and their
+// fresh h-grid on X (pbf.rs:2163, header in hB).
+static __device__ void group_factors_and_grid(const MillDev& m, const float2* X, GridHdr& hB, uint32_t* err) {
+  const uint32_t n = m.nf;
+  const float rho0 = m.f_rho0, mass = m.f_mass;
+  grid_build(X, n, m.f_h, m.gB, hB, err);
+  for (uint32_t j = tid(); j < n; j += nthr())
+    m.f_tmp[j] = BALL_BC_GAIN * (mass * 2.0f * m.mu_eff[j] / (fmax_r(m.density[j], 1e-6f) * rho0));
+  __syncthreads();
+}
+
 // Step 7 (pbf.rs:2146-2300): implicit viscosity on the velocities V at positions X (Morris weights,
 // ball boundary groups, squeeze links, the fluid-only or joint fluid + ball CG and the ball
 // impulses from it), in its own function so that it is register-allocated apart from the rest
@@ -1043,14 +1159,16 @@ static __device__ __noinline__ bool buoyancy_step(const MillDev& m, const StepUn
 // or a grid failed (the error is in *err).
 static __device__ __noinline__ bool viscosity_step(const MillDev& m, const StepUniform& U, StepOut& out,
                                                   uint32_t* err, FluidShared& S, float2* X, float2* V, float mu,
-                                                  uint32_t& visc_iters) {
+                                                  uint32_t& visc_iters, bool beside) {
   const uint32_t n = m.nf, nb = m.nb;
-  const float h = m.f_h, rho0 = m.f_rho0, mass = m.f_mass, dt = U.dt;
+  const float h = m.f_h, mass = m.f_mass, dt = U.dt;
   const bool fp64 = U.cg_fp64 != 0;
   if (mu > 0.0f) {
     const bool bingham = U.slurry.rheology == MG_RHEOLOGY_BINGHAM && U.slurry.yield_stress_pa > 0.0f;
     const float tau_y = U.slurry.yield_stress_pa;
-    for (uint32_t i = tid(); i < n; i += nthr()) {
+    // (beside: the helper blocks computed mu_eff, the Morris weights and the boundary groups'
+    // lists beside the drag sweep)
+    for (uint32_t i = tid(); !beside && i < n; i += nthr()) {
       float mu_i = mu;
       if (bingham) {
         // pbf.rs:821-868 shear rate then Papanastasiou viscosity
@@ -1078,33 +1196,17 @@ static __device__ __noinline__ bool viscosity_step(const MillDev& m, const StepU
       m.mu_eff[i] = mu_i;
     }
     __syncthreads();
-    const float eta2 = VISC_ETA * h * h;
-    for (uint32_t i = tid(); i < n; i += nthr()) {
-      V2 xi(X[i]);
-      float rho_i = fmax_r(m.density[i], 1e-6f);
-      float mu_i = m.mu_eff[i];
-      for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) {
-        uint32_t j = m.nbrs[k];
-        float rho_j = fmax_r(m.density[j], 1e-6f);
-        V2 delta = xi - V2(X[j]);
-        float r = delta.len();
-        V2 grad = spiky_grad(delta, r, h);
-        float numerator = (mass * (mu_i + m.mu_eff[j]) / (rho_i * rho_j)) * fabsf(delta.dot(grad));
-        m.visc_w[k] = numerator / (delta.len2() + eta2);
-        m.visc_dir[k] = (r > 1e-9f ? delta / r : V2(1.0f, 0.0f)).f2();
-      }
-    }
-    __syncthreads();
+    if (!beside) morris_weights(m, X);
     stage_mark(out.stage, 8);
     // boundary groups (pbf.rs:2159-2232) on a fresh h-grid, one ball per thread, merged per fluid
     if (tid() == 0) { S.n_groups = 0; S.n_links = 0; S.links_in_range = 0; }
     __syncthreads();
     if (nb > 0 && m.b_r > 0.0f) {
-      grid_build(X, n, h, m.gB, S.hB, err);
-      for (uint32_t j = tid(); j < n; j += nthr())
-        m.f_tmp[j] = BALL_BC_GAIN * (mass * 2.0f * m.mu_eff[j] / (fmax_r(m.density[j], 1e-6f) * rho0));
-      __syncthreads();
-      wide_phase(m, WIDE_GROUPS, &S.hB, [&](uint32_t w0, uint32_t nw) { group_balls(m, U, S.hB, w0, nw); });
+      const ItemLists I = beside ? ItemLists{m.gi_j, m.gi_v, m.gi_w, m.gi_w2} : mill_items(m);
+      if (!beside) {
+        group_factors_and_grid(m, X, S.hB, err);
+        wide_phase(m, WIDE_GROUPS, &S.hB, [&](uint32_t w0, uint32_t nw) { group_balls(m, U, S.hB, w0, nw, I, w0); });
+      }
       if (tid() == 0) m.g_off[nb] = 0;
       __syncthreads();
       if (*err) return false;
@@ -1113,11 +1215,11 @@ static __device__ __noinline__ bool viscosity_step(const MillDev& m, const StepU
       for (uint32_t b = tid() >> 5; b < nb; b += nthr() >> 5) {
         const uint32_t base = b * m.cap_items, o = m.g_off[b], cnt = m.g_off[b + 1] - o;
         for (uint32_t s = tid() & 31u; s < cnt; s += 32) {
-          m.g_fluid[o + s] = m.item_j[base + s];
+          m.g_fluid[o + s] = I.j[base + s];
           m.g_ball[o + s] = b;
-          m.g_c[o + s] = m.item_w[base + s];
-          m.g_lc[o + s] = m.item_v[base + s];
-          m.g_l2[o + s] = m.item_w2[base + s];
+          m.g_c[o + s] = I.w[base + s];
+          m.g_lc[o + s] = I.v[base + s];
+          m.g_l2[o + s] = I.w2[base + s];
         }
       }
       if (tid() == 0) S.n_groups = ng;
@@ -1444,6 +1546,92 @@ static __device__ unsigned long long fluid_tail(const MillDev& m, float v_max, d
   }
   __syncthreads();
   return (unsigned long long)(clock64() - t0);
+}
+
+// Helper blocks, WIDE_BESIDE_DRAG: the work that reads only the sub-step's final positions (after
+// step 4) and nothing the drag sweep writes, done while the mill's block runs the drag sweep. The
+// tasks the mill's block asked for (BESIDE_*) are split by helper block:
+//   * block 1 (BESIDE_VISC): the density recompute (pbf.rs:2132-2144), mu_eff = mu and the Morris
+//     weights (pbf.rs:2146-2154), the boundary groups' per-particle factors and h-grid, whose
+//     header it publishes for the other helpers right after building it; then (BESIDE_BUOY), once
+//     every other helper has listed its buoyancy items, the buoyancy records, their predecessor
+//     balls and a claim order by dependency level (as buoyancy_step does without a drag order);
+//   * blocks 2..: their shares of the buoyancy item lists (pbf.rs:2042-2060) into bi_*, counted
+//     in the phase's counter, then, once the grid is published, of the boundary groups
+//     (pbf.rs:2159-2232) into gi_* and g_off.
+// The waits between helpers are bounded like the mill's (ERR_WIDE; the waiting block then skips
+// the work that needed the other).
+static __device__ uint32_t beside_drag(const MillDev& m, const StepUniform& U, const GridHdr& hA, FluidShared& S,
+                                       unsigned char* dsm) {
+  __shared__ uint32_t ok;
+  WideCtl* c = m.wide;
+  const uint32_t tasks = c->beside_tasks;
+  const uint32_t n = m.nf, nb = m.nb;
+  const float2* X = m.fx;
+  const long long lim = m.wide_wait_cycles > 0 ? m.wide_wait_cycles : WIDE_TIMEOUT_CYCLES;
+  if (blockIdx.x == 1) {
+    if (tasks & BESIDE_VISC) {
+      density_recompute(m, X);
+      const float mu = c->beside_mu;
+      for (uint32_t i = tid(); i < n; i += nthr()) m.mu_eff[i] = mu;
+      __syncthreads();
+      group_factors_and_grid(m, X, S.hB, m.err);
+      if (tid() == 0) {
+        c->beside_hdr = S.hB;
+        __threadfence();
+        *reinterpret_cast<volatile uint32_t*>(&c->beside_grid_seq) = 1u;
+      }
+      morris_weights(m, X);
+    }
+    if (tasks & BESIDE_BUOY) {
+      if (tid() == 0) {
+        ok = wide_wait(&c->beside_buoy_blocks, m.helpers - 1u, lim) ? 1u : 0u;
+        if (!ok) atomicOr(m.err, ERR_WIDE);
+        __threadfence();
+      }
+      __syncthreads();
+      if (ok) {
+        const uint32_t nrec = pack_ball_items(m.bi_j, m.bi_n, m.cap_items, nb, m.b_rec_off, m.b_rec_i, m.b_rec_b);
+        LevelScratch L;
+        const bool by_level = U.sweep_order == 0 &&
+                              level_scratch(nb, reinterpret_cast<uint32_t*>(dsm), m.smem_bytes / 4u, L);
+        ball_item_preds(m.b_rec_i, m.b_rec_b, nrec, n, nb, m.hb_start, m.hb_cur, m.hb_order, m.b_rec_pred,
+                        by_level ? &L : nullptr);
+        if (by_level) {
+          const uint32_t* order = ball_level_order(nb, m.b_rec_off, m.b_rec_pred, L);
+          for (uint32_t b = tid(); b < nb; b += nthr()) m.b_order[b] = order[b];
+        }
+        if (tid() == 0) {
+          c->beside_nrec = nrec;
+          c->beside_order_ok = by_level ? 1u : 0u;
+        }
+        __syncthreads();
+      }
+    }
+    return 0u;
+  }
+  const uint32_t nwarps = nthr() >> 5, warp = tid() >> 5;
+  const uint32_t w0 = (blockIdx.x - 2u) * nwarps + warp, nw = (m.helpers - 1u) * nwarps;
+  uint32_t items = 0;
+  if (tasks & BESIDE_BUOY) {
+    items = buoyancy_item_balls(m, hA, w0, nw, ItemLists{m.bi_j, m.bi_v, m.bi_w, nullptr}, m.bi_n);
+    __syncthreads();
+    if (tid() == 0) {
+      __threadfence();
+      atomicAdd(&c->beside_buoy_blocks, 1u);
+    }
+  }
+  if (tasks & BESIDE_VISC) {
+    if (tid() == 0) {
+      ok = wide_wait(&c->beside_grid_seq, 1u, lim) ? 1u : 0u;
+      if (!ok) atomicOr(m.err, ERR_WIDE);
+      __threadfence();
+      S.hB = c->beside_hdr;
+    }
+    __syncthreads();
+    if (ok) group_balls(m, U, S.hB, w0, nw, ItemLists{m.gi_j, m.gi_v, m.gi_w, m.gi_w2}, blockIdx.x * nwarps + warp);
+  }
+  return items;
 }
 
 // defer_tail: leave fluid_tail to helper block 1 (the caller publishes it). Returns whether the
@@ -1808,13 +1996,16 @@ static __device__ bool fluid_step(const MillDev& m, const StepUniform& U, StepOu
   // ---- step 6.5: ball drag, Gauss-Seidel over balls (pbf.rs:1777-2013)
   const float mu = fmax_r(U.slurry.viscosity_pa_s, 0.0f);
   const uint32_t* drag_order = nullptr;  // the drag sweep's claim order, when it ran by level
-  if (!drag_step(m, U, out, err, S, X, V, done, sweep_scratch, sweep_words, &drag_order)) return false;
+  uint32_t beside = 0;  // BESIDE_* parts the helper blocks do beside the drag sweep
+  if (!drag_step(m, U, out, err, S, X, V, done, sweep_scratch, sweep_words, &drag_order, &beside)) return false;
   stage_mark(out.stage, 19);
   double ke_after_drag = kinetic_energy_seq(V, n, mass, S);
   const double ke_delta_drag = ke_after_drag - ke_mark;
   ke_mark = ke_after_drag;
   // ---- step 6.6: buoyancy, Gauss-Seidel over balls on the stale step-2 grid (pbf.rs:2035-2122)
-  if (!buoyancy_step(m, U, out, err, S, X, V, done, sweep_scratch, sweep_words, drag_order)) return false;
+  if (!buoyancy_step(m, U, out, err, S, X, V, done, sweep_scratch, sweep_words, drag_order,
+                     (beside & BESIDE_BUOY) != 0u))
+    return false;
   double ke_after_buoy = kinetic_energy_seq(V, n, mass, S);
   const double ke_delta_buoy = ke_after_buoy - ke_mark;
   ke_mark = ke_after_buoy;
@@ -1825,19 +2016,13 @@ static __device__ bool fluid_step(const MillDev& m, const StepUniform& U, StepOu
     __syncthreads();
   }
   stage_mark(out.stage, 6);
-  // ---- density recompute at final x over the step-2 lists (pbf.rs:2137-2144)
-  const float self_rho = mass * poly6(0.0f, h);
-  for (uint32_t i = tid(); i < n; i += nthr()) {
-    V2 xi(X[i]);
-    float rho = self_rho;
-    for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) rho += mass * poly6((xi - V2(X[m.nbrs[k]])).len2(), h);
-    m.density[i] = rho;
-  }
-  __syncthreads();
+  // ---- density recompute at final x over the step-2 lists (the helper blocks did it beside the
+  // drag sweep with BESIDE_VISC)
+  if (!(beside & BESIDE_VISC)) density_recompute(m, X);
   stage_mark(out.stage, 7);
   // ---- step 7: implicit viscosity (pbf.rs:2146-2300)
   uint32_t visc_iters = 0;
-  if (!viscosity_step(m, U, out, err, S, X, V, mu, visc_iters)) return false;
+  if (!viscosity_step(m, U, out, err, S, X, V, mu, visc_iters, (beside & BESIDE_VISC) != 0u)) return false;
   stage_mark(out.stage, 11);
   // ---- mean shear rate and step 7.5, the speed clamp (fluid_tail); they touch nothing that
   // step 8 or the DEM step reads

@@ -241,6 +241,22 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
     m.rec_off = a.take<uint32_t>(cb + 1); m.rec_pred = a.take<uint32_t>(m.cap_recs);
     m.ball_done = a.take<uint32_t>(cb);
     m.slot = a.take<uint32_t>((size_t)MAX_BLOCK_WARPS * s->mill_blocks_cap * cf);
+    if (s->mill_blocks_cap > 1) {
+      // the lists and records the helper blocks fill beside the drag sweep
+      m.gi_j = a.take<uint32_t>(items); m.gi_v = a.take<float2>(items);
+      m.gi_w = a.take<float>(items); m.gi_w2 = a.take<float>(items);
+      m.bi_j = a.take<uint32_t>(items); m.bi_v = a.take<float2>(items); m.bi_w = a.take<float>(items);
+      m.bi_n = a.take<uint32_t>(cb + 1);
+      m.b_rec_off = a.take<uint32_t>(cb + 1); m.b_rec_i = a.take<uint32_t>(items);
+      m.b_rec_b = a.take<uint32_t>(items); m.b_rec_pred = a.take<uint32_t>(items);
+      m.hb_start = a.take<uint32_t>(nbig); m.hb_cur = a.take<uint32_t>(nbig); m.hb_order = a.take<uint32_t>(items);
+      m.b_order = a.take<uint32_t>(cb);
+    } else {
+      m.gi_j = m.bi_j = m.bi_n = m.b_rec_off = m.b_rec_i = m.b_rec_b = m.b_rec_pred = nullptr;
+      m.hb_start = m.hb_cur = m.hb_order = m.b_order = nullptr;
+      m.gi_v = m.bi_v = nullptr;
+      m.gi_w = m.gi_w2 = m.bi_w = nullptr;
+    }
     m.wide = a.take<WideCtl>(1);
     s->d_metrics = a.take<MgMetrics>(1);
     m.pair_i = a.take<uint32_t>(m.cap_pairs); m.pair_j = a.take<uint32_t>(m.cap_pairs);

@@ -24,7 +24,8 @@ enum : uint32_t {
   WIDE_CG_SETUP = 6,
   WIDE_JOINT_APPLY = 7,
   WIDE_DRAG_PRE = 8,
-  WIDE_FLUID_PREP = 9
+  WIDE_FLUID_PREP = 9,
+  WIDE_BESIDE_DRAG = 10
 };
 
 
