@@ -280,6 +280,15 @@ struct WideCtl {
   uint32_t beside_buoy_blocks;
   GridHdr beside_hdr;
   uint32_t beside_nrec, beside_order_ok;
+  GridHdr beside_link_hdr;      // the squeeze links' ball grid (cell 2 r + reach)
+  uint32_t beside_link_over;    // balls whose squeeze-link candidates did not fit their slots
+  // the drag sweep's item lists, records and claim order, listed by the helper blocks while the
+  // mill's block runs steps 5-6 (WIDE_DRAG_LISTS): helper block 1 publishes the drag grid's header
+  // (drag_grid_seq = 1 once built), the other helpers count their finished shares of the item
+  // lists and the per-ball pre-sums (drag_blocks), helper block 1 then leaves whether it found a
+  // claim order
+  uint32_t drag_grid_seq, drag_blocks, drag_order_ok;
+  GridHdr drag_hdr;
 };
 enum : uint32_t { BESIDE_VISC = 1u, BESIDE_BUOY = 2u };
 
@@ -358,6 +367,17 @@ struct MillDev {
   uint32_t *b_rec_off, *b_rec_i, *b_rec_b, *b_rec_pred;
   uint32_t *hb_start, *hb_cur, *hb_order;
   uint32_t* b_order;
+  uint32_t* d_order;  // the drag sweep's claim order when the helper blocks listed its items
+  // squeeze-link candidates the helpers list beside the drag sweep (geometry only; which of them
+  // are links depends on the balls' velocities after the sweeps): per ball i, its partners j > i
+  // within reach in slots [i K, i K + K) (K = min(nb + 1, 512)) with their normals and film
+  // coefficients, their count, and the wall candidate (in range, normal, coefficient)
+  uint32_t* lk_j;
+  float2* lk_n;
+  float* lk_c;
+  uint32_t *lk_cnt, *lk_winr;
+  float2* lk_wn;
+  float* lk_wc;
   uint32_t *pair_i, *pair_j;
   float* lam_bb;
   uint32_t* pr_list;  // pairs within reach of touching at the start of the projection

@@ -505,6 +505,133 @@ static __device__ uint32_t link_balls(const MillDev& m, const StepUniform& U, co
   return in_range;
 }
 
+// Squeeze-link candidates per ball (the geometry of link_balls, before the velocity test): for
+// the balls w0, w0 + nw, ..., the partners j > i in for_each_near order that are within reach, with
+// the normal and film coefficient link_pair gives them, into lk_* (count lk_cnt[i]; a ball with
+// more candidates than its K slots counts into *over and is left for the full path), and the wall
+// candidate in lk_winr / lk_wn / lk_wc. link_pair and link_wall evaluate the same expressions;
+// only the test n . (v0_i - v0_j) > 0 (n . v0_i > 0 for the wall) is left to links_from_candidates.
+static __device__ void link_candidate_balls(const MillDev& m, const StepUniform& U, const GridHdr& hBall, uint32_t w0,
+                                            uint32_t nw, uint32_t* over) {
+  const uint32_t nb = m.nb;
+  const float h = m.f_h, dt = U.dt;
+  const float r = m.b_r;
+  const double dxd = (double)(0.5f * h);
+  const float reach = (float)(8.0 * dxd);
+  const float c_max = 8.0f * m.b_m / fmax_r(dt, 1e-12f);
+  const float range2 = (2.0f * r + reach) * (2.0f * r + reach) * (1.0f + 1e-4f);
+  const uint32_t K = min(nb + 1u, 512u);
+  for (uint32_t i = w0; i < nb; i += nw) {
+    const uint32_t lane = tid() & 31u;
+    const V2 xi(m.bx[i]);
+    const uint32_t base = i * K;
+    uint32_t c = 0;
+    if (xi.finite()) {
+      warp_near_multi(
+          hBall, m.gBall, 1u, [&](uint32_t) { return xi; },
+          [&](uint32_t j, bool valid) { return valid && j > i ? V2(m.bx[j]) : V2(); },
+          [&](uint32_t j, uint32_t, V2 xj, bool valid) {
+            bool keep = false;
+            V2 nrm;
+            float cf = 0.0f;
+            if (valid && j > i) {
+              V2 e = xj - xi;
+              if (!(e.len2() >= range2 || !e.finite())) {
+                float dist = e.len();
+                float gap = dist - 2.0f * r;
+                if (!(gap >= reach || dist < 1e-9f)) {
+                  keep = true;
+                  nrm = e / dist;
+                  double weight = 1.0 - resolved_ratio((double)gap / dxd);
+                  double hh = (double)gap > 0.02 * (double)r ? (double)gap : 0.02 * (double)r;
+                  double cc = weight * film_coefficient(U.pair_film, hh);
+                  cf = fmin_r(1.0f * (float)cc, c_max);
+                }
+              }
+            }
+            const uint32_t bal = __ballot_sync(FULL, keep);
+            const uint32_t q = c + __popc(bal & ((1u << lane) - 1u));
+            if (keep && q < K) {
+              m.lk_j[base + q] = j;
+              m.lk_n[base + q] = nrm.f2();
+              m.lk_c[base + q] = cf;
+            }
+            c += __popc(bal);
+          });
+    }
+    if (lane == 0) {
+      uint32_t winr = 0;
+      V2 wn;
+      float wc = 0.0f;
+      const float dist = xi.len();
+      const float gap = U.drum_radius - r - dist;
+      if (gap < reach && dist > 1e-9f) {
+        winr = 1u;
+        wn = xi / dist;
+        double weight = 1.0 - resolved_ratio((double)gap / dxd);
+        double hh = (double)gap > 0.02 * (double)r ? (double)gap : 0.02 * (double)r;
+        double cc = weight * film_coefficient(U.wall_film, hh);
+        wc = fmin_r(1.0f * (float)cc, c_max);
+      }
+      m.lk_winr[i] = winr;
+      m.lk_wn[i] = wn.f2();
+      m.lk_wc[i] = wc;
+      if (c > K) { atomicAdd(over, 1u); c = K; }
+      m.lk_cnt[i] = c;
+    }
+    __syncwarp();
+  }
+}
+
+// Squeeze links per ball from the candidates link_candidate_balls listed, once ball_v0 is known:
+// candidate j is a link when n . (v0_i - v0_j) > 0 (the wall when n . v0_i > 0), kept in candidate
+// order, then the wall, into the record scratch slots [i K, i K + K) and the count into l_off[i]
+// as link_balls leaves them. Returns the thread's part of the count of candidates in range.
+static __device__ uint32_t links_from_candidates(const MillDev& m, uint32_t w0, uint32_t nw) {
+  const uint32_t nb = m.nb;
+  const uint32_t K = min(nb + 1u, 512u);
+  uint32_t in_range = 0;
+  for (uint32_t i = w0; i < nb; i += nw) {
+    const uint32_t lane = tid() & 31u, base = i * K, cnt = m.lk_cnt[i];
+    const V2 v0i(m.ball_v0[i]);
+    uint32_t c = 0;
+    for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+      const uint32_t q = c0 + lane;
+      bool emit = false;
+      uint32_t j = 0;
+      V2 nrm;
+      if (q < cnt) {
+        j = m.lk_j[base + q];
+        nrm = V2(m.lk_n[base + q]);
+        emit = !(nrm.dot(v0i - V2(m.ball_v0[j])) <= 0.0f);
+      }
+      const uint32_t bal = __ballot_sync(FULL, emit);
+      const uint32_t pos = c + __popc(bal & ((1u << lane) - 1u));
+      if (emit && pos < K) {
+        m.rec_i[base + pos] = j;
+        m.rec_J[base + pos] = nrm.f2();
+        m.rec_L[base + pos] = m.lk_c[base + q];
+      }
+      c += __popc(bal);
+    }
+    if (lane == 0) {
+      const uint32_t winr = m.lk_winr[i];
+      if (winr) {
+        const V2 wn(m.lk_wn[i]);
+        if (!(wn.dot(v0i) <= 0.0f)) {
+          if (c < K) { m.rec_i[base + c] = NONE; m.rec_J[base + c] = wn.f2(); m.rec_L[base + c] = m.lk_wc[i]; }
+          ++c;
+        }
+      }
+      if (c > K) { atomicOr(m.err, ERR_LINKS); c = K; }
+      m.l_off[i] = c;
+      in_range += cnt + winr;
+    }
+    __syncwarp();
+  }
+  return in_range;
+}
+
 // Drag item lists per ball (pbf.rs:1794-1822): fluid particles within r + h of the ball centre in
 // for_each_near order, with their offsets and weights (item_j / item_v / item_w, count item_n).
 // Returns the thread's part of the item count.
@@ -818,7 +945,7 @@ static __device__ __noinline__ void drag_sweep(const MillDev& m, const StepUnifo
 static __device__ __noinline__ bool drag_step(const MillDev& m, const StepUniform& U, StepOut& out, uint32_t* err,
                                               FluidShared& S, float2* X, float2* V, uint32_t* done,
                                               uint32_t* scratch, uint32_t scratch_words,
-                                              const uint32_t** order_out, uint32_t* beside_out) {
+                                              const uint32_t** order_out, uint32_t* beside_out, bool listed) {
   const uint32_t n = m.nf, nb = m.nb;
   const float h = m.f_h, rho0 = m.f_rho0, mass = m.f_mass, dt = U.dt;
   (void)rho0;
@@ -830,26 +957,41 @@ static __device__ __noinline__ bool drag_step(const MillDev& m, const StepUnifor
     const float mass_true = rho_ball * PI_F * m.b_rtrue * m.b_rtrue;
     if (beta_b > 0.0f) {
       const float h_c = m.b_r + h;
-      const float w_hc0 = fmax_r(poly6(0.0f, h_c), 1e-12f);
-      grid_build(X, n, fmax_r(h_c, 1e-6f), m.gB, S.hB, err);
-      // item lists per ball in for_each_near order (positions do not change during the sweep):
-      // one warp per ball, an ordered compaction of each 32-candidate chunk
-      uint32_t n_items = 0;
-      wide_phase(m, WIDE_DRAG_ITEMS, &S.hB, [&](uint32_t w0, uint32_t nw) { n_items += drag_item_balls(m, S.hB, w0, nw); });
-      n_items = block_sum_u(n_items) + wide_counter(m);
-      if (tid() == 0) out.ctr.n_coupling_items += n_items;
-      __syncthreads();
-      if (*err) return false;
-      stage_mark(out.stage, 24);
-      const uint32_t nrec = pack_ball_items(m.item_j, m.item_n, m.cap_items, nb, m.rec_off, m.rec_i, m.rec_b);
-      LevelScratch L;
-      const bool by_level = U.sweep_order == 0 && level_scratch(nb, scratch, scratch_words, L);
-      ball_item_preds(m.rec_i, m.rec_b, nrec, n, nb, m.bk_start, m.bk_cur, m.bk_order, m.rec_pred,
-                      by_level ? &L : nullptr);
-      const uint32_t* order = by_level ? ball_level_order(nb, m.rec_off, m.rec_pred, L) : nullptr;
-      *order_out = order;
-      stage_mark(out.stage, 25);
-      wide_phase(m, WIDE_DRAG_PRE, nullptr, [&](uint32_t w0, uint32_t nw) { drag_pre_balls(m, w0, nw); });
+      const uint32_t* order = nullptr;
+      if (listed) {
+        // the helper blocks listed the items, records, claim order and pre-sums during steps 5-6
+        // (WIDE_DRAG_LISTS); the claim order lives in d_order, not in this block's scratch, so
+        // the buoyancy sweep does not reuse it
+        wide_finish(m);
+        const uint32_t n_items = wide_counter(m);
+        if (tid() == 0) out.ctr.n_coupling_items += n_items;
+        __syncthreads();
+        if (*err) return false;
+        stage_mark(out.stage, 24);
+        order = m.wide->drag_order_ok ? m.d_order : nullptr;
+        stage_mark(out.stage, 25);
+      } else {
+        grid_build(X, n, fmax_r(h_c, 1e-6f), m.gB, S.hB, err);
+        // item lists per ball in for_each_near order (positions do not change during the sweep):
+        // one warp per ball, an ordered compaction of each 32-candidate chunk
+        uint32_t n_items = 0;
+        wide_phase(m, WIDE_DRAG_ITEMS, &S.hB,
+                   [&](uint32_t w0, uint32_t nw) { n_items += drag_item_balls(m, S.hB, w0, nw); });
+        n_items = block_sum_u(n_items) + wide_counter(m);
+        if (tid() == 0) out.ctr.n_coupling_items += n_items;
+        __syncthreads();
+        if (*err) return false;
+        stage_mark(out.stage, 24);
+        const uint32_t nrec = pack_ball_items(m.item_j, m.item_n, m.cap_items, nb, m.rec_off, m.rec_i, m.rec_b);
+        LevelScratch L;
+        const bool by_level = U.sweep_order == 0 && level_scratch(nb, scratch, scratch_words, L);
+        ball_item_preds(m.rec_i, m.rec_b, nrec, n, nb, m.bk_start, m.bk_cur, m.bk_order, m.rec_pred,
+                        by_level ? &L : nullptr);
+        order = by_level ? ball_level_order(nb, m.rec_off, m.rec_pred, L) : nullptr;
+        *order_out = order;
+        stage_mark(out.stage, 25);
+        wide_phase(m, WIDE_DRAG_PRE, nullptr, [&](uint32_t w0, uint32_t nw) { drag_pre_balls(m, w0, nw); });
+      }
       // the sweep's constants, read from shared memory by the per-ball bodies
       if (tid() == 0) {
         float* K = g_sweep_const;
@@ -879,6 +1021,7 @@ static __device__ __noinline__ bool drag_step(const MillDev& m, const StepUnifor
           c->beside_buoy_blocks = 0u;
           c->beside_nrec = 0u;
           c->beside_order_ok = 0u;
+          c->beside_link_over = 0u;
         });
         *beside_out = tasks;
       }
@@ -1236,16 +1379,23 @@ static __device__ __noinline__ bool viscosity_step(const MillDev& m, const StepU
       const float r = m.b_r;
       const double dxd = (double)(0.5f * h);
       const float reach = (float)(8.0 * dxd);
-      grid_build(m.bx, nb, 2.0f * r + reach, m.gBall, S.hBall, err);
-      uint32_t in_range = 0;
+      uint32_t tot_in = 0;
       // ball i's links go to its slots [i K, i K + K) of the record scratch, then one compaction
-      // copies them to the link list in ball order
+      // copies them to the link list in ball order. beside: the helper blocks listed the
+      // candidates beside the drag sweep (unless a ball had more than its slots hold), so only the
+      // velocity test is left.
       const uint32_t K = min(nb + 1u, 512u);
-      wide_phase(m, WIDE_LINKS, &S.hBall,
-                 [&](uint32_t w0, uint32_t nw) { in_range += link_balls(m, U, S.hBall, w0, nw); });
+      if (beside && m.wide->beside_link_over == 0u) {
+        tot_in = block_sum_u(links_from_candidates(m, tid() >> 5, nthr() >> 5));
+      } else {
+        uint32_t in_range = 0;
+        grid_build(m.bx, nb, 2.0f * r + reach, m.gBall, S.hBall, err);
+        wide_phase(m, WIDE_LINKS, &S.hBall,
+                   [&](uint32_t w0, uint32_t nw) { in_range += link_balls(m, U, S.hBall, w0, nw); });
+        tot_in = block_sum_u(in_range) + wide_counter(m);
+      }
       if (tid() == 0) m.l_off[nb] = 0;
       __syncthreads();
-      const uint32_t tot_in = block_sum_u(in_range) + wide_counter(m);
       const uint32_t nl = block_exclusive_scan(m.l_off, nb + 1);
       if (nl > m.cap_links) { if (tid() == 0) atomicOr(err, ERR_LINKS); __syncthreads(); return false; }
       if (tid() == 0) { S.n_links = nl; S.links_in_range = tot_in; }
@@ -1576,8 +1726,11 @@ static __device__ uint32_t beside_drag(const MillDev& m, const StepUniform& U, c
       for (uint32_t i = tid(); i < n; i += nthr()) m.mu_eff[i] = mu;
       __syncthreads();
       group_factors_and_grid(m, X, S.hB, m.err);
+      if (nb > 0 && m.b_r > 0.0f)  // the squeeze links' ball grid (pbf.rs:544-560)
+        grid_build(m.bx, nb, 2.0f * m.b_r + (float)(8.0 * (double)(0.5f * m.f_h)), m.gBall, S.hBall, m.err);
       if (tid() == 0) {
         c->beside_hdr = S.hB;
+        c->beside_link_hdr = S.hBall;
         __threadfence();
         *reinterpret_cast<volatile uint32_t*>(&c->beside_grid_seq) = 1u;
       }
@@ -1627,9 +1780,77 @@ static __device__ uint32_t beside_drag(const MillDev& m, const StepUniform& U, c
       if (!ok) atomicOr(m.err, ERR_WIDE);
       __threadfence();
       S.hB = c->beside_hdr;
+      S.hBall = c->beside_link_hdr;
     }
     __syncthreads();
-    if (ok) group_balls(m, U, S.hB, w0, nw, ItemLists{m.gi_j, m.gi_v, m.gi_w, m.gi_w2}, blockIdx.x * nwarps + warp);
+    if (ok) {
+      group_balls(m, U, S.hB, w0, nw, ItemLists{m.gi_j, m.gi_v, m.gi_w, m.gi_w2}, blockIdx.x * nwarps + warp);
+      if (nb > 0 && m.b_r > 0.0f) link_candidate_balls(m, U, S.hBall, w0, nw, &c->beside_link_over);
+    }
+  }
+  return items;
+}
+
+// Helper blocks, WIDE_DRAG_LISTS: the drag sweep's inputs, which read only the final positions,
+// listed while the mill's block runs steps 5-6 (velocity reconstruction and wall no-slip, which
+// write only velocities). Helper block 1 builds the drag grid (cell r + h, pbf.rs:1794-1796) and
+// publishes its header; helper blocks 2.. then list their shares of the item lists
+// (drag_item_balls) and the per-ball pre-sums (drag_pre_balls) and count themselves done; helper
+// block 1 then packs the records, their predecessor balls and, by dependency level, the claim order
+// into d_order. The phase's counter receives the item count. Waits between helpers are bounded
+// (ERR_WIDE).
+static __device__ uint32_t drag_lists(const MillDev& m, const StepUniform& U, FluidShared& S, unsigned char* dsm) {
+  __shared__ uint32_t ok;
+  WideCtl* c = m.wide;
+  const uint32_t n = m.nf, nb = m.nb;
+  const long long lim = m.wide_wait_cycles > 0 ? m.wide_wait_cycles : WIDE_TIMEOUT_CYCLES;
+  if (blockIdx.x == 1) {
+    const float h_c = m.b_r + m.f_h;
+    grid_build(m.fx, n, fmax_r(h_c, 1e-6f), m.gB, S.hB, m.err);
+    if (tid() == 0) {
+      c->drag_hdr = S.hB;
+      __threadfence();
+      *reinterpret_cast<volatile uint32_t*>(&c->drag_grid_seq) = 1u;
+      ok = wide_wait(&c->drag_blocks, m.helpers - 1u, lim) ? 1u : 0u;
+      if (!ok) atomicOr(m.err, ERR_WIDE);
+      __threadfence();
+    }
+    __syncthreads();
+    if (ok) {
+      const uint32_t nrec = pack_ball_items(m.item_j, m.item_n, m.cap_items, nb, m.rec_off, m.rec_i, m.rec_b);
+      LevelScratch L;
+      const bool by_level =
+          U.sweep_order == 0 && level_scratch(nb, reinterpret_cast<uint32_t*>(dsm), m.smem_bytes / 4u, L);
+      ball_item_preds(m.rec_i, m.rec_b, nrec, n, nb, m.bk_start, m.bk_cur, m.bk_order, m.rec_pred,
+                      by_level ? &L : nullptr);
+      if (by_level) {
+        const uint32_t* order = ball_level_order(nb, m.rec_off, m.rec_pred, L);
+        for (uint32_t b = tid(); b < nb; b += nthr()) m.d_order[b] = order[b];
+      }
+      if (tid() == 0) c->drag_order_ok = by_level ? 1u : 0u;
+      __syncthreads();
+    }
+    return 0u;
+  }
+  if (tid() == 0) {
+    ok = wide_wait(&c->drag_grid_seq, 1u, lim) ? 1u : 0u;
+    if (!ok) atomicOr(m.err, ERR_WIDE);
+    __threadfence();
+    S.hB = c->drag_hdr;
+  }
+  __syncthreads();
+  uint32_t items = 0;
+  if (ok) {
+    const uint32_t nwarps = nthr() >> 5;
+    const uint32_t w0 = (blockIdx.x - 2u) * nwarps + (tid() >> 5), nw = (m.helpers - 1u) * nwarps;
+    items = drag_item_balls(m, S.hB, w0, nw);
+    __syncwarp();
+    drag_pre_balls(m, w0, nw);  // the same balls, from the lists this warp just wrote
+  }
+  __syncthreads();
+  if (tid() == 0) {
+    __threadfence();
+    atomicAdd(&c->drag_blocks, 1u);
   }
   return items;
 }
@@ -1841,6 +2062,22 @@ static __device__ bool fluid_step(const MillDev& m, const StepUniform& U, StepOu
     }
   }
   __syncthreads();
+  // The positions are final from here on: with two or more helper blocks and a drag sweep to run,
+  // the helpers list the drag sweep's items, records and claim order (drag_lists) while this
+  // block runs steps 5-6.
+  bool drag_listed = false;
+  {
+    const float mu_d = fmax_r(U.slurry.viscosity_pa_s, 0.0f);
+    if (m.helpers >= 2 && m.d_order != nullptr && nb > 0 && m.b_r > 0.0f && m.b_rtrue > 0.0f && mu_d > 1e-6f &&
+        clamp_r(U.slurry.ball_no_slip, 0.0f, 1.0f) > 0.0f) {
+      wide_publish(m, WIDE_DRAG_LISTS, nullptr, nullptr, nullptr, [&](WideCtl* c) {
+        c->drag_grid_seq = 0u;
+        c->drag_blocks = 0u;
+        c->drag_order_ok = 0u;
+      });
+      drag_listed = true;
+    }
+  }
   // accumulations in particle order by warp 0: each lane keeps one angle bin; every lane carries
   // the three f64 sums (identical chains)
   if (tid() < 32) {
@@ -1997,7 +2234,8 @@ static __device__ bool fluid_step(const MillDev& m, const StepUniform& U, StepOu
   const float mu = fmax_r(U.slurry.viscosity_pa_s, 0.0f);
   const uint32_t* drag_order = nullptr;  // the drag sweep's claim order, when it ran by level
   uint32_t beside = 0;  // BESIDE_* parts the helper blocks do beside the drag sweep
-  if (!drag_step(m, U, out, err, S, X, V, done, sweep_scratch, sweep_words, &drag_order, &beside)) return false;
+  if (!drag_step(m, U, out, err, S, X, V, done, sweep_scratch, sweep_words, &drag_order, &beside, drag_listed))
+    return false;
   stage_mark(out.stage, 19);
   double ke_after_drag = kinetic_energy_seq(V, n, mass, S);
   const double ke_delta_drag = ke_after_drag - ke_mark;

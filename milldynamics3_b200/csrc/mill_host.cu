@@ -250,10 +250,16 @@ int alloc_state(MgSim* s, uint32_t nf, uint32_t nb) {
       m.b_rec_off = a.take<uint32_t>(cb + 1); m.b_rec_i = a.take<uint32_t>(items);
       m.b_rec_b = a.take<uint32_t>(items); m.b_rec_pred = a.take<uint32_t>(items);
       m.hb_start = a.take<uint32_t>(nbig); m.hb_cur = a.take<uint32_t>(nbig); m.hb_order = a.take<uint32_t>(items);
-      m.b_order = a.take<uint32_t>(cb);
+      m.b_order = a.take<uint32_t>(cb); m.d_order = a.take<uint32_t>(cb);
+      m.lk_j = a.take<uint32_t>(m.cap_links); m.lk_n = a.take<float2>(m.cap_links); m.lk_c = a.take<float>(m.cap_links);
+      m.lk_cnt = a.take<uint32_t>(cb); m.lk_winr = a.take<uint32_t>(cb);
+      m.lk_wn = a.take<float2>(cb); m.lk_wc = a.take<float>(cb);
     } else {
       m.gi_j = m.bi_j = m.bi_n = m.b_rec_off = m.b_rec_i = m.b_rec_b = m.b_rec_pred = nullptr;
-      m.hb_start = m.hb_cur = m.hb_order = m.b_order = nullptr;
+      m.hb_start = m.hb_cur = m.hb_order = m.b_order = m.d_order = nullptr;
+      m.lk_j = m.lk_cnt = m.lk_winr = nullptr;
+      m.lk_n = m.lk_wn = nullptr;
+      m.lk_c = m.lk_wc = nullptr;
       m.gi_v = m.bi_v = nullptr;
       m.gi_w = m.gi_w2 = m.bi_w = nullptr;
     }

@@ -49,6 +49,7 @@ __global__ void __launch_bounds__(MAX_THREADS) mill_substeps_kernel(const MillDe
       else if (phase == WIDE_DRAG_ITEMS) return drag_item_balls(m, hdr, w0, nw);
       else if (phase == WIDE_BUOYANCY_ITEMS) return buoyancy_item_balls(m, hdr, w0, nw, mill_items(m), m.item_n);
       else if (phase == WIDE_BESIDE_DRAG) return beside_drag(m, U, hdr, fs, dsm);
+      else if (phase == WIDE_DRAG_LISTS) return drag_lists(m, U, fs, dsm);
       else if (phase == WIDE_CG_SETUP) cg_setup_rows(m, U.dt, t0, stride);
       else if (phase == WIDE_JOINT_APPLY) joint_apply_rows(m, U.dt, vin, vout, t0, stride);
       else if (phase == WIDE_DRAG_PRE) drag_pre_balls(m, w0, nw);

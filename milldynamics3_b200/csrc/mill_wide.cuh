@@ -25,7 +25,8 @@ enum : uint32_t {
   WIDE_JOINT_APPLY = 7,
   WIDE_DRAG_PRE = 8,
   WIDE_FLUID_PREP = 9,
-  WIDE_BESIDE_DRAG = 10
+  WIDE_BESIDE_DRAG = 10,
+  WIDE_DRAG_LISTS = 11
 };
 
 
