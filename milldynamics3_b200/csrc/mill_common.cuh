@@ -20,6 +20,9 @@ constexpr uint32_t NONE = 0xFFFFFFFFu;
 constexpr int MAX_LIFTERS = 64;
 // Per-ball sweeps (drag, buoyancy): warps taking balls and the poll interval of a waiting ball.
 constexpr uint32_t DEFAULT_SWEEP_WARPS = 32;
+// ... for single-mill handles, whose helper blocks take the sweeps' other work meanwhile (fewer
+// waiting warps keep more issue slots for the ball on the dependency chain; measured fastest)
+constexpr uint32_t DEFAULT_SWEEP_WARPS_SINGLE = 20;
 // Largest block of the frame kernel (32 warps); per-warp scratch (the merge slot maps) is sized for it.
 constexpr uint32_t MAX_BLOCK_THREADS = 1024;
 constexpr uint32_t MAX_BLOCK_WARPS = MAX_BLOCK_THREADS / 32;
@@ -282,6 +285,10 @@ struct WideCtl {
   uint32_t beside_nrec, beside_order_ok;
   GridHdr beside_link_hdr;      // the squeeze links' ball grid (cell 2 r + reach)
   uint32_t beside_link_over;    // balls whose squeeze-link candidates did not fit their slots
+  // helpers done with their boundary-group shares (beside_group_blocks); helper block 1 then
+  // compacts the groups and sorts them by fluid particle, leaving the count (beside_ngroups) and
+  // whether it did (beside_groups_ok)
+  uint32_t beside_group_blocks, beside_ngroups, beside_groups_ok;
   // the drag sweep's item lists, records and claim order, listed by the helper blocks while the
   // mill's block runs steps 5-6 (WIDE_DRAG_LISTS): helper block 1 publishes the drag grid's header
   // (drag_grid_seq = 1 once built), the other helpers count their finished shares of the item

@@ -56,7 +56,7 @@ __device__ __forceinline__ int impact_energy_bin(float e) {
 
 // dem.rs:253-261 f32 mechanical energy, summed in ball order (three adds per ball); called by
 // warp 0, result in every lane
-static __device__ float mech_energy_seq(const MillDev& m, const float2* X, const float2* V, const float* OM) {
+static __device__ __noinline__ float mech_energy_seq(const MillDev& m, const float2* X, const float2* V, const float* OM) {
   const uint32_t lane = threadIdx.x & 31u;
   float e = 0.0f;
   for (uint32_t c = 0; c < m.nb; c += 32) {
@@ -308,6 +308,40 @@ static __device__ __noinline__ void restitution_sweep(const MillDev& m, const St
     V[i] = (V2(V[i]) + dvn * n_hat).f2();
   }
   __syncthreads();
+}
+
+// After the friction sweep, by warp 0: the wall work summed in wall-contact order, two adds per
+// contact (dem.rs:870, 881), into S.fscal[1]; the active pair contacts counted; the restitution
+// sweep's collision count and histogram cleared. Its own function, so that the unrolled shuffle
+// loop is register-allocated apart from the DEM step around it.
+static __device__ __noinline__ void friction_wall_work(const MillDev& m, uint32_t na, DemShared& S, StepOut& out) {
+  if (tid() < 32) {
+    const uint32_t lane = tid();
+    float wall_work = 0.0f;
+    uint32_t act = 0;
+    for (uint32_t c = 0; c < na; c += 32) {
+      uint32_t k = c + lane;
+      bool wall = k < na && m.act_j[k] == NONE && m.act_bin[k] != -2;
+      act += (k < na && m.act_j[k] != NONE) ? 1u : 0u;
+      float a = wall ? m.act_w1[k] : 0.0f, b = wall ? m.act_w2[k] : 0.0f;
+      const uint32_t mask = __ballot_sync(FULL, wall);
+#pragma unroll
+      for (int t = 0; t < 32; ++t) {
+        const float at = __shfl_sync(FULL, a, t), bt = __shfl_sync(FULL, b, t);
+        if ((mask >> t) & 1u) {
+          wall_work += at;
+          wall_work += bt;
+        }
+      }
+    }
+    act = warp_sum(act);
+    if (lane == 0) {
+      S.fscal[1] = wall_work;
+      out.ctr.n_active_contacts = act;
+      S.collisions = 0;
+      for (int q = 0; q < MG_IMPACT_BINS; ++q) S.hist[q] = 0;
+    }
+  }
 }
 
 static __device__ __noinline__ void dem_step(const MillDev& m, const StepUniform& U, StepOut& out, MgImpactRecord* impacts,
@@ -579,34 +613,7 @@ static __device__ __noinline__ void dem_step(const MillDev& m, const StepUniform
   bucket_levels(na_p, m.dm_lvl, nlev_c, m.lev_start, m.lev_cur, m.lev_items);
   stage_mark(out.stage, 38);
   friction_sweep(m, U, X, V, TH, OM, nlev_c, na_p, na, w, w_rot, r, dt);
-  if (tid() < 32) {
-    // wall work summed in wall-contact order, two adds per contact (dem.rs:870, 881)
-    const uint32_t lane = tid();
-    float wall_work = 0.0f;
-    uint32_t act = 0;
-    for (uint32_t c = 0; c < na; c += 32) {
-      uint32_t k = c + lane;
-      bool wall = k < na && m.act_j[k] == NONE && m.act_bin[k] != -2;
-      act += (k < na && m.act_j[k] != NONE) ? 1u : 0u;
-      float a = wall ? m.act_w1[k] : 0.0f, b = wall ? m.act_w2[k] : 0.0f;
-      const uint32_t mask = __ballot_sync(FULL, wall);
-#pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const float at = __shfl_sync(FULL, a, t), bt = __shfl_sync(FULL, b, t);
-        if ((mask >> t) & 1u) {
-          wall_work += at;
-          wall_work += bt;
-        }
-      }
-    }
-    act = warp_sum(act);
-    if (lane == 0) {
-      S.fscal[1] = wall_work;
-      out.ctr.n_active_contacts = act;
-      S.collisions = 0;
-      for (int q = 0; q < MG_IMPACT_BINS; ++q) S.hist[q] = 0;
-    }
-  }
+  friction_wall_work(m, na, S, out);
   __syncthreads();
   stage_mark(out.stage, 17);
   // resync (dem.rs:887-890)

@@ -35,7 +35,7 @@ __device__ __forceinline__ float fluid_vmax(const StepUniform& U) {
 }
 
 // pbf.rs:924-926: 0.5 m sum |v|^2 in f64, summed in particle order.
-static __device__ double kinetic_energy_seq(const float2* v, uint32_t n, float mass, FluidShared& S) {
+static __device__ __noinline__ double kinetic_energy_seq(const float2* v, uint32_t n, float mass, FluidShared& S) {
   if (tid() < 32) {
     double s = warp_ordered_sum(0.0, n, [&](uint32_t i, double& t) { t = (double)V2(v[i]).len2(); return true; });
     if (tid() == 0) S.dscal[7] = 0.5 * (double)mass * s;
@@ -47,7 +47,7 @@ static __device__ double kinetic_energy_seq(const float2* v, uint32_t n, float m
 }
 
 // pbf.rs:292-294 dot in the reference's sequential f32 order, or in f64 (deterministic tree).
-static __device__ double block_dot(const float2* a, const float2* b, uint32_t len, bool fp64, FluidShared& S) {
+static __device__ __noinline__ double block_dot(const float2* a, const float2* b, uint32_t len, bool fp64, FluidShared& S) {
   if (fp64) {
     double acc = 0.0;
     for (uint32_t e = tid(); e < len; e += nthr())
@@ -58,7 +58,7 @@ static __device__ double block_dot(const float2* a, const float2* b, uint32_t le
 }
 
 // pbf.rs:738-744 residual norm sqrt(sum inv_diag |r|^2), sequential f32 or f64.
-static __device__ double block_res_norm(const float2* r, const float* inv, uint32_t len, bool fp64, FluidShared& S) {
+static __device__ __noinline__ double block_res_norm(const float2* r, const float* inv, uint32_t len, bool fp64, FluidShared& S) {
   if (fp64) {
     double acc = 0.0;
     for (uint32_t e = tid(); e < len; e += nthr())
@@ -1022,6 +1022,9 @@ static __device__ __noinline__ bool drag_step(const MillDev& m, const StepUnifor
           c->beside_nrec = 0u;
           c->beside_order_ok = 0u;
           c->beside_link_over = 0u;
+          c->beside_group_blocks = 0u;
+          c->beside_ngroups = 0u;
+          c->beside_groups_ok = 0u;
         });
         *beside_out = tasks;
       }
@@ -1295,6 +1298,21 @@ static __device__ void group_factors_and_grid(const MillDev& m, const float2* X,
   __syncthreads();
 }
 
+// The boundary groups in ball order from the per-ball lists I and the offsets g_off (scanned):
+// fluid index, ball, coefficient, lever and squared lever per group (pbf.rs:2159-2232).
+static __device__ void compact_groups(const MillDev& m, const ItemLists& I) {
+  for (uint32_t b = tid() >> 5; b < m.nb; b += nthr() >> 5) {
+    const uint32_t base = b * m.cap_items, o = m.g_off[b], cnt = m.g_off[b + 1] - o;
+    for (uint32_t s = tid() & 31u; s < cnt; s += 32) {
+      m.g_fluid[o + s] = I.j[base + s];
+      m.g_ball[o + s] = b;
+      m.g_c[o + s] = I.w[base + s];
+      m.g_lc[o + s] = I.v[base + s];
+      m.g_l2[o + s] = I.w2[base + s];
+    }
+  }
+}
+
 // Step 7 (pbf.rs:2146-2300): implicit viscosity on the velocities V at positions X (Morris weights,
 // ball boundary groups, squeeze links, the fluid-only or joint fluid + ball CG and the ball
 // impulses from it), in its own function so that it is register-allocated apart from the rest
@@ -1350,22 +1368,19 @@ static __device__ __noinline__ bool viscosity_step(const MillDev& m, const StepU
         group_factors_and_grid(m, X, S.hB, err);
         wide_phase(m, WIDE_GROUPS, &S.hB, [&](uint32_t w0, uint32_t nw) { group_balls(m, U, S.hB, w0, nw, I, w0); });
       }
-      if (tid() == 0) m.g_off[nb] = 0;
+      // (beside: helper block 1 compacted and sorted the groups unless something failed)
+      const bool groups_sorted = beside && m.wide->beside_groups_ok != 0u;
+      if (!groups_sorted && tid() == 0) m.g_off[nb] = 0;
       __syncthreads();
       if (*err) return false;
-      uint32_t ng = block_exclusive_scan(m.g_off, nb + 1);
-      if (ng > m.cap_groups) { if (tid() == 0) atomicOr(err, ERR_GROUPS); __syncthreads(); return false; }
-      for (uint32_t b = tid() >> 5; b < nb; b += nthr() >> 5) {
-        const uint32_t base = b * m.cap_items, o = m.g_off[b], cnt = m.g_off[b + 1] - o;
-        for (uint32_t s = tid() & 31u; s < cnt; s += 32) {
-          m.g_fluid[o + s] = I.j[base + s];
-          m.g_ball[o + s] = b;
-          m.g_c[o + s] = I.w[base + s];
-          m.g_lc[o + s] = I.v[base + s];
-          m.g_l2[o + s] = I.w2[base + s];
-        }
+      if (groups_sorted) {
+        if (tid() == 0) S.n_groups = m.wide->beside_ngroups;
+      } else {
+        uint32_t ng = block_exclusive_scan(m.g_off, nb + 1);
+        if (ng > m.cap_groups) { if (tid() == 0) atomicOr(err, ERR_GROUPS); __syncthreads(); return false; }
+        compact_groups(m, I);
+        if (tid() == 0) S.n_groups = ng;
       }
-      if (tid() == 0) S.n_groups = ng;
       __syncthreads();
     }
     stage_mark(out.stage, 9);
@@ -1460,9 +1475,7 @@ static __device__ __noinline__ bool viscosity_step(const MillDev& m, const StepU
       // ---- joint fluid + ball Jacobi-PCG (pbf.rs:641-791)
       const uint32_t len = n + 2 * nb;
       // per-fluid group lists and per-ball "other" link lists (stable, in group / link order)
-      for (uint32_t g = tid(); g < S.n_groups; g += nthr()) m.rec_i[g] = m.g_fluid[g];
-      __syncthreads();
-      block_bucket_sort(m.rec_i, S.n_groups, n, m.fg_start, m.bk_start, m.fg_list);
+      if (!(beside && m.wide->beside_groups_ok)) block_bucket_sort(m.g_fluid, S.n_groups, n, m.fg_start, m.bk_start, m.fg_list);
       for (uint32_t l = tid(); l < S.n_links; l += nthr()) m.rec_b[l] = m.l_other[l] == NONE ? nb : m.l_other[l];
       __syncthreads();
       // (bucket nb collects the links without a second ball; only the balls' lists are read)
@@ -1761,6 +1774,33 @@ static __device__ uint32_t beside_drag(const MillDev& m, const StepUniform& U, c
         __syncthreads();
       }
     }
+    if (tasks & BESIDE_VISC) {
+      // the boundary groups in ball order (their lists compacted from gi_*) and their per-fluid
+      // lists (a stable bucket sort by fluid particle), once every helper has listed its share
+      if (tid() == 0) {
+        ok = wide_wait(&c->beside_group_blocks, m.helpers - 1u, lim) ? 1u : 0u;
+        if (!ok) atomicOr(m.err, ERR_WIDE);
+        __threadfence();
+        if (*reinterpret_cast<volatile uint32_t*>(m.err) != 0u) ok = 0u;
+        m.g_off[nb] = 0;
+      }
+      __syncthreads();
+      if (ok) {
+        const uint32_t ng = block_exclusive_scan(m.g_off, nb + 1);
+        if (ng > m.cap_groups) {
+          if (tid() == 0) atomicOr(m.err, ERR_GROUPS);
+        } else {
+          compact_groups(m, ItemLists{m.gi_j, m.gi_v, m.gi_w, m.gi_w2});
+          __syncthreads();
+          block_bucket_sort(m.g_fluid, ng, n, m.fg_start, m.hb_cur, m.fg_list);
+          if (tid() == 0) {
+            c->beside_ngroups = ng;
+            c->beside_groups_ok = 1u;
+          }
+        }
+        __syncthreads();
+      }
+    }
     return 0u;
   }
   const uint32_t nwarps = nthr() >> 5, warp = tid() >> 5;
@@ -1783,10 +1823,13 @@ static __device__ uint32_t beside_drag(const MillDev& m, const StepUniform& U, c
       S.hBall = c->beside_link_hdr;
     }
     __syncthreads();
-    if (ok) {
-      group_balls(m, U, S.hB, w0, nw, ItemLists{m.gi_j, m.gi_v, m.gi_w, m.gi_w2}, blockIdx.x * nwarps + warp);
-      if (nb > 0 && m.b_r > 0.0f) link_candidate_balls(m, U, S.hBall, w0, nw, &c->beside_link_over);
+    if (ok) group_balls(m, U, S.hB, w0, nw, ItemLists{m.gi_j, m.gi_v, m.gi_w, m.gi_w2}, blockIdx.x * nwarps + warp);
+    __syncthreads();
+    if (tid() == 0) {
+      __threadfence();
+      atomicAdd(&c->beside_group_blocks, 1u);
     }
+    if (ok && nb > 0 && m.b_r > 0.0f) link_candidate_balls(m, U, S.hBall, w0, nw, &c->beside_link_over);
   }
   return items;
 }
@@ -1853,6 +1896,120 @@ static __device__ uint32_t drag_lists(const MillDev& m, const StepUniform& U, Fl
     atomicAdd(&c->drag_blocks, 1u);
   }
   return items;
+}
+
+// Step 4's wall accumulations in particle order (pbf.rs:1635-1653), by warp 0: each lane keeps one
+// angle bin of the normal impulse; every lane carries the three f64 impulse sums (identical
+// chains), left in S.dscal[0..2]. Its own function, so that the unrolled shuffle loops are
+// register-allocated apart from the fluid step around them (inlined there they spilled).
+static __device__ __noinline__ void wall_sums_step4(const MillDev& m, uint32_t n, StepOut& out, FluidShared& S) {
+  if (tid() < 32) {
+    const int lane = tid();
+    float bin_acc = 0.0f;
+    double ix = 0.0, iy = 0.0, ia = 0.0;
+    // the three f64 sums by the order-free exact path when it applies (same bits), else below
+    const bool exact = warp_exact_sum_f64(0.0, n, [&](uint32_t i, double& t) {
+                         if (m.wall_bin[i] < 0) return false; t = (double)m.dv_tmp[i].x; return true; }, ix) &&
+                       warp_exact_sum_f64(0.0, n, [&](uint32_t i, double& t) {
+                         if (m.wall_bin[i] < 0) return false; t = (double)m.dv_tmp[i].y; return true; }, iy) &&
+                       warp_exact_sum_f64(0.0, n, [&](uint32_t i, double& t) {
+                         if (m.wall_bin[i] < 0) return false; t = (double)m.f_tmp[i]; return true; }, ia);
+    if (!exact) ix = iy = ia = 0.0;
+    for (uint32_t c = 0; c < n; c += 32) {
+      int32_t bin = -1;
+      float val = 0.0f, px = 0.0f, py = 0.0f, pa = 0.0f;
+      if (c + lane < n) {
+        bin = m.wall_bin[c + lane];
+        if (bin >= 0) { val = m.wall_val[c + lane]; px = m.dv_tmp[c + lane].x; py = m.dv_tmp[c + lane].y; pa = m.f_tmp[c + lane]; }
+      }
+      const uint32_t mask = __ballot_sync(FULL, bin >= 0);
+      if (mask == 0u) continue;  // no particle of the chunk touched the wall
+      if (exact) {
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+          const int bt = __shfl_sync(FULL, bin, t);
+          const float vt = __shfl_sync(FULL, val, t);
+          if (((mask >> t) & 1u) && bt == lane) bin_acc += vt;
+        }
+        continue;
+      }
+#pragma unroll
+      for (int t = 0; t < 32; ++t) {
+        const int bt = __shfl_sync(FULL, bin, t);
+        const float vt = __shfl_sync(FULL, val, t), xt = __shfl_sync(FULL, px, t), yt = __shfl_sync(FULL, py, t);
+        const float at = __shfl_sync(FULL, pa, t);
+        if ((mask >> t) & 1u) {
+          ix += (double)xt;
+          iy += (double)yt;
+          ia += (double)at;
+          if (bt == lane) bin_acc += vt;
+        }
+      }
+    }
+    out.fs.wall_normal_impulse_by_angle[lane] = bin_acc;
+    if (lane == 0) { S.dscal[0] = ix; S.dscal[1] = iy; S.dscal[2] = ia; }
+  }
+}
+
+// Step 6's accumulations in particle order (pbf.rs:1677-1700), continuing the step-4 impulse sums in
+// S.dscal[0..2], and the wall work into out.fs.wall_work_j, by warp 0. Its own function, like
+// wall_sums_step4.
+static __device__ __noinline__ void wall_sums_step6(const MillDev& m, const StepUniform& U, const float2* X,
+                                                    uint32_t n, float mass, StepOut& out, FluidShared& S) {
+  if (tid() < 32) {
+    const int lane = tid();
+    float work = 0.0f;
+    double ix = S.dscal[0], iy = S.dscal[1], ia = S.dscal[2];
+    // the three f64 sums by the order-free exact path when it applies (same bits), else below
+    double ex_ix, ex_iy, ex_ia;
+    const bool exact =
+        warp_exact_sum_f64(ix, n, [&](uint32_t i, double& t) {
+          if (m.wall_bin[i] < 0) return false; t = (double)(mass * V2(m.dv_tmp[i]).x); return true; }, ex_ix) &&
+        warp_exact_sum_f64(iy, n, [&](uint32_t i, double& t) {
+          if (m.wall_bin[i] < 0) return false; t = (double)(mass * V2(m.dv_tmp[i]).y); return true; }, ex_iy) &&
+        warp_exact_sum_f64(ia, n, [&](uint32_t i, double& t) {
+          if (m.wall_bin[i] < 0) return false; t = (double)cross2(V2(X[i]), mass * V2(m.dv_tmp[i])); return true; }, ex_ia);
+    for (uint32_t c = 0; c < n; c += 32) {
+      bool touched = c + lane < n && m.wall_bin[c + lane] >= 0;
+      float wk = 0.0f, jx = 0.0f, jy = 0.0f, ja = 0.0f;
+      if (touched) {
+        V2 x(X[c + lane]);
+        V2 dv(m.dv_tmp[c + lane]);
+        wk = mass * dv.dot(wall_velocity(U.drum_omega, x));
+        jx = mass * dv.x;
+        jy = mass * dv.y;
+        ja = cross2(x, mass * dv);
+      }
+      const uint32_t mask = __ballot_sync(FULL, touched);
+      if (mask == 0u) continue;
+      if (exact) {
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+          const float wt = __shfl_sync(FULL, wk, t);
+          if ((mask >> t) & 1u) work += wt;
+        }
+        continue;
+      }
+#pragma unroll
+      for (int t = 0; t < 32; ++t) {
+        const float wt = __shfl_sync(FULL, wk, t), xt = __shfl_sync(FULL, jx, t), yt = __shfl_sync(FULL, jy, t);
+        const float at = __shfl_sync(FULL, ja, t);
+        if ((mask >> t) & 1u) {
+          work += wt;
+          ix += (double)xt;
+          iy += (double)yt;
+          ia += (double)at;
+        }
+      }
+    }
+    __syncwarp();
+    if (exact) {
+      ix = ex_ix;
+      iy = ex_iy;
+      ia = ex_ia;
+    }
+    if (lane == 0) { S.dscal[0] = ix; S.dscal[1] = iy; S.dscal[2] = ia; out.fs.wall_work_j = work; }
+  }
 }
 
 // defer_tail: leave fluid_tail to helper block 1 (the caller publishes it). Returns whether the
@@ -2078,54 +2235,8 @@ static __device__ bool fluid_step(const MillDev& m, const StepUniform& U, StepOu
       drag_listed = true;
     }
   }
-  // accumulations in particle order by warp 0: each lane keeps one angle bin; every lane carries
-  // the three f64 sums (identical chains)
-  if (tid() < 32) {
-    const int lane = tid();
-    float bin_acc = 0.0f;
-    double ix = 0.0, iy = 0.0, ia = 0.0;
-    // the three f64 sums by the order-free exact path when it applies (same bits), else below
-    const bool exact = warp_exact_sum_f64(0.0, n, [&](uint32_t i, double& t) {
-                         if (m.wall_bin[i] < 0) return false; t = (double)m.dv_tmp[i].x; return true; }, ix) &&
-                       warp_exact_sum_f64(0.0, n, [&](uint32_t i, double& t) {
-                         if (m.wall_bin[i] < 0) return false; t = (double)m.dv_tmp[i].y; return true; }, iy) &&
-                       warp_exact_sum_f64(0.0, n, [&](uint32_t i, double& t) {
-                         if (m.wall_bin[i] < 0) return false; t = (double)m.f_tmp[i]; return true; }, ia);
-    if (!exact) ix = iy = ia = 0.0;
-    for (uint32_t c = 0; c < n; c += 32) {
-      int32_t bin = -1;
-      float val = 0.0f, px = 0.0f, py = 0.0f, pa = 0.0f;
-      if (c + lane < n) {
-        bin = m.wall_bin[c + lane];
-        if (bin >= 0) { val = m.wall_val[c + lane]; px = m.dv_tmp[c + lane].x; py = m.dv_tmp[c + lane].y; pa = m.f_tmp[c + lane]; }
-      }
-      const uint32_t mask = __ballot_sync(FULL, bin >= 0);
-      if (mask == 0u) continue;  // no particle of the chunk touched the wall
-      if (exact) {
-#pragma unroll
-        for (int t = 0; t < 32; ++t) {
-          const int bt = __shfl_sync(FULL, bin, t);
-          const float vt = __shfl_sync(FULL, val, t);
-          if (((mask >> t) & 1u) && bt == lane) bin_acc += vt;
-        }
-        continue;
-      }
-#pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int bt = __shfl_sync(FULL, bin, t);
-        const float vt = __shfl_sync(FULL, val, t), xt = __shfl_sync(FULL, px, t), yt = __shfl_sync(FULL, py, t);
-        const float at = __shfl_sync(FULL, pa, t);
-        if ((mask >> t) & 1u) {
-          ix += (double)xt;
-          iy += (double)yt;
-          ia += (double)at;
-          if (bt == lane) bin_acc += vt;
-        }
-      }
-    }
-    out.fs.wall_normal_impulse_by_angle[lane] = bin_acc;
-    if (lane == 0) { S.dscal[0] = ix; S.dscal[1] = iy; S.dscal[2] = ia; }
-  }
+  // accumulations in particle order by warp 0 (wall_sums_step4)
+  wall_sums_step4(m, n, out, S);
   __syncthreads();
   // ---- step 5: velocity reconstruction (pbf.rs:1656-1674)
   for (uint32_t i = tid(); i < n; i += nthr()) {
@@ -2150,61 +2261,8 @@ static __device__ bool fluid_step(const MillDev& m, const StepUniform& U, StepOu
       m.dv_tmp[i] = (v - v_old).f2();
     }
     __syncthreads();
-    // accumulations in particle order, continuing the step-4 sums (warp 0, identical chains)
-    if (tid() < 32) {
-      const int lane = tid();
-      float work = 0.0f;
-      double ix = S.dscal[0], iy = S.dscal[1], ia = S.dscal[2];
-      // the three f64 sums by the order-free exact path when it applies (same bits), else below
-      double ex_ix, ex_iy, ex_ia;
-      const bool exact =
-          warp_exact_sum_f64(ix, n, [&](uint32_t i, double& t) {
-            if (m.wall_bin[i] < 0) return false; t = (double)(mass * V2(m.dv_tmp[i]).x); return true; }, ex_ix) &&
-          warp_exact_sum_f64(iy, n, [&](uint32_t i, double& t) {
-            if (m.wall_bin[i] < 0) return false; t = (double)(mass * V2(m.dv_tmp[i]).y); return true; }, ex_iy) &&
-          warp_exact_sum_f64(ia, n, [&](uint32_t i, double& t) {
-            if (m.wall_bin[i] < 0) return false; t = (double)cross2(V2(X[i]), mass * V2(m.dv_tmp[i])); return true; }, ex_ia);
-      for (uint32_t c = 0; c < n; c += 32) {
-        bool touched = c + lane < n && m.wall_bin[c + lane] >= 0;
-        float wk = 0.0f, jx = 0.0f, jy = 0.0f, ja = 0.0f;
-        if (touched) {
-          V2 x(X[c + lane]);
-          V2 dv(m.dv_tmp[c + lane]);
-          wk = mass * dv.dot(wall_velocity(U.drum_omega, x));
-          jx = mass * dv.x;
-          jy = mass * dv.y;
-          ja = cross2(x, mass * dv);
-        }
-        const uint32_t mask = __ballot_sync(FULL, touched);
-        if (mask == 0u) continue;
-        if (exact) {
-#pragma unroll
-          for (int t = 0; t < 32; ++t) {
-            const float wt = __shfl_sync(FULL, wk, t);
-            if ((mask >> t) & 1u) work += wt;
-          }
-          continue;
-        }
-#pragma unroll
-        for (int t = 0; t < 32; ++t) {
-          const float wt = __shfl_sync(FULL, wk, t), xt = __shfl_sync(FULL, jx, t), yt = __shfl_sync(FULL, jy, t);
-          const float at = __shfl_sync(FULL, ja, t);
-          if ((mask >> t) & 1u) {
-            work += wt;
-            ix += (double)xt;
-            iy += (double)yt;
-            ia += (double)at;
-          }
-        }
-      }
-      __syncwarp();
-      if (exact) {
-        ix = ex_ix;
-        iy = ex_iy;
-        ia = ex_ia;
-      }
-      if (lane == 0) { S.dscal[0] = ix; S.dscal[1] = iy; S.dscal[2] = ia; out.fs.wall_work_j = work; }
-    }
+    // accumulations in particle order, continuing the step-4 sums (warp 0: wall_sums_step6)
+    wall_sums_step6(m, U, X, n, mass, out, S);
     __syncthreads();
   }
   double ke_mark = kinetic_energy_seq(V, n, mass, S);

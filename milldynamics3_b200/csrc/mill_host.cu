@@ -374,7 +374,8 @@ int fill_uniform(MgSim* s, const MgDrum& drum, const MgMediaParams& media, const
   U.media = media;
   U.slurry = slurry;
   U.cg_fp64 = s->opt.cg_fp64;
-  U.sweep_warps = s->opt.sweep_warps ? s->opt.sweep_warps : DEFAULT_SWEEP_WARPS;
+  U.sweep_warps = s->opt.sweep_warps ? s->opt.sweep_warps
+                 : s->mill_blocks_cap > 1 ? DEFAULT_SWEEP_WARPS_SINGLE : DEFAULT_SWEEP_WARPS;
   U.spin_ns = s->opt.spin_ns ? s->opt.spin_ns : DEFAULT_SPIN_NS;
   // polls of a waiting ball before it gives up: about a second, or the tests' short limit
   U.spin_limit = s->opt.test_wait_limit_us
