@@ -801,14 +801,15 @@ static __device__ void drag_pre_balls(const MillDev& m, uint32_t w0, uint32_t nw
 // memory so that the per-ball bodies keep few values in registers across the dependency wait.
 enum : uint32_t {
   DS_M_ENT = 0, DS_I_ENT = 1, DS_R_BAR = 2, DS_S_ACC = 4, DS_S_SCALE = 5, DS_PRE = 6,  // drag_pre[0..5]
-  DS_VB = 6, DS_OMB = 8, DS_DV_B = 9, DS_DW_B = 11, DS_SLOT = 12
+  DS_VB = 6, DS_OMB = 8, DS_DV_B = 9, DS_DW_B = 11, DS_LIN_DEN = 12, DS_ROT_DEN = 13, DS_NEG_BM_MENT = 14,
+  DS_SLOT = 15
 };
 enum : uint32_t { BS_RHO_LOCAL = 0, BS_DEN = 1, BS_XB = 2, BS_IMPULSE = 4 };
 enum : uint32_t {
-  DK_MASS, DK_RHO0, DK_MASS_TRUE, DK_BETA, DK_DT, DK_I_B, DK_H_C, DK_ROT_CAP, DK_B_M, DK_B_RTRUE
+  DK_MASS, DK_RHO0, DK_MASS_TRUE, DK_BETA, DK_DT, DK_I_B, DK_H_C, DK_ROT_CAP, DK_B_M, DK_B_RTRUE, DK_FORM, DK_CAP
 };
 enum : uint32_t { BK_RHO0, BK_OM_ABS, BK_AREA, BK_DT, BK_MASS };
-constexpr uint32_t SWEEP_CONSTS = 10;  // DK_* and BK_* indices are below it
+constexpr uint32_t SWEEP_CONSTS = 12;  // DK_* and BK_* indices are below it
 constexpr uint32_t DRAG_LIVE = 0x80000000u;
 __shared__ float g_ball_slot[MAX_BLOCK_WARPS][DS_SLOT];
 __shared__ float g_sweep_const[SWEEP_CONSTS];
@@ -853,6 +854,11 @@ static __device__ __noinline__ void drag_sweep(const MillDev& m, const StepUnifo
         if (lane < DS_PRE) sl[lane] = m.drag_pre[8u * b + lane];
         else if (lane < DS_OMB) sl[lane] = reinterpret_cast<const float*>(m.bv + b)[lane - DS_VB];
         else if (lane == DS_OMB) sl[lane] = m.bom[b];
+        // the relaxation's terms that do not read the swept velocities (the same operations as on
+        // the chain, done ahead): b_m + m_ent, i_b + i_ent, -(b_m / m_ent)
+        else if (lane == DS_LIN_DEN) sl[lane] = g_sweep_const[DK_B_M] + m.drag_pre[8u * b + DS_M_ENT];
+        else if (lane == DS_ROT_DEN) sl[lane] = g_sweep_const[DK_I_B] + m.drag_pre[8u * b + DS_I_ENT];
+        else if (lane == DS_NEG_BM_MENT) sl[lane] = -(g_sweep_const[DK_B_M] / m.drag_pre[8u * b + DS_M_ENT]);
         if (!(m.drag_pre[8u * b] <= 1e-12f)) q.cnt |= DRAG_LIVE;  // (a NaN mass takes part too)
         return q;
       },
@@ -878,27 +884,25 @@ static __device__ __noinline__ void drag_sweep(const MillDev& m, const StepUnifo
           }
           lane_seq_sum3(vsx, vsy, l_sum, vw.x, vw.y, lw, lim);
         }
-        const float m_ent = sl[DS_M_ENT], i_ent = sl[DS_I_ENT], b_m = K[DK_B_M], i_b = K[DK_I_B];
+        const float m_ent = sl[DS_M_ENT], i_ent = sl[DS_I_ENT], i_b = K[DK_I_B];
         V2 v_bar = V2(vsx, vsy) / m_ent;
         V2 v_rel = v_bar - V2(sl[DS_VB], sl[DS_VB + 1]);
         float speed_rel = v_rel.len();
         const float rho0_l = K[DK_RHO0];
-        float inv_tau_form = (speed_rel > 1e-6f && rho0_l > 0.0f)
-                                 ? 0.5f * rho0_l * 1.0f * (2.0f * K[DK_B_RTRUE]) * speed_rel / K[DK_MASS_TRUE]
-                                 : 0.0f;
+        // (K[DK_FORM] = 0.5 rho0 1 (2 r_true), the left part of the product, formed ahead)
+        float inv_tau_form = (speed_rel > 1e-6f && rho0_l > 0.0f) ? K[DK_FORM] * speed_rel / K[DK_MASS_TRUE] : 0.0f;
         float bt = K[DK_BETA] * (1.0f - expf_r(-K[DK_DT] * (0.0f + inv_tau_form)));
-        float a_lin = bt * m_ent / (b_m + m_ent);
+        float a_lin = bt * m_ent / sl[DS_LIN_DEN];
         V2 dv_b = a_lin * v_rel;
         float dw_b = 0.0f, c_rot = 0.0f;
         if (i_ent > 1e-12f) {
           float omega_bar = l_sum / i_ent;
-          float a_rot = bt * i_ent / (i_b + i_ent);
+          float a_rot = bt * i_ent / sl[DS_ROT_DEN];
           float candidate_dw = a_rot * (omega_bar - sl[DS_OMB]);
           const float s_acc = sl[DS_S_ACC];
           if (fabsf(s_acc) > 0.1f * sl[DS_S_SCALE]) {
             float raw_c_rot = -i_b * candidate_dw / s_acc;
-            float max_lever = 2.0f * K[DK_H_C];
-            float cap = max_lever > 1e-9f ? K[DK_ROT_CAP] / max_lever : 0.0f;
+            const float cap = K[DK_CAP];  // rot_cap / (2 h_c), formed ahead
             c_rot = clamp_r(raw_c_rot, -cap, cap);
             dw_b = -c_rot * s_acc / i_b;
           }
@@ -908,7 +912,7 @@ static __device__ __noinline__ void drag_sweep(const MillDev& m, const StepUnifo
           const uint32_t j = s < 32 ? q.j : m.item_j[base + s];
           const V2 r_i = s < 32 ? q.r_i : V2(m.item_v[base + s]);
           const float phi = s < 32 ? q.phi : m.item_w[base + s];
-          V2 dv_i = -(b_m / m_ent) * dv_b * phi;
+          V2 dv_i = sl[DS_NEG_BM_MENT] * dv_b * phi;  // -(b_m / m_ent), formed ahead
           if (c_rot != 0.0f) {
             V2 perp_i(-r_i.y, r_i.x);
             dv_i += c_rot * phi * (perp_i - p_bar);
@@ -1005,6 +1009,9 @@ static __device__ __noinline__ bool drag_step(const MillDev& m, const StepUnifor
         K[DK_ROT_CAP] = rot_cap;
         K[DK_B_M] = m.b_m;
         K[DK_B_RTRUE] = m.b_rtrue;
+        K[DK_FORM] = 0.5f * rho0 * 1.0f * (2.0f * m.b_rtrue);
+        const float max_lever = 2.0f * h_c;
+        K[DK_CAP] = max_lever > 1e-9f ? rot_cap / max_lever : 0.0f;
       }
       __syncthreads();
       // With two or more helper blocks, the helpers do what reads only the final positions beside
