@@ -365,9 +365,9 @@ __device__ void ball_dataflow(uint32_t nb, const uint32_t* rec_off, const uint32
 
 // Three in-order sums over the lanes' values t = 0..lim-1, added to a, b, c (the same on every
 // lane): the lanes store their values to the warp's shared scratch, lanes from lim on store -0.0
-// (x + -0.0 == x for every x, so padding changes no sum), and lane 0 adds them in lane order four
-// at a time from 16-byte loads, the next four's loads in flight during the additions; the sums
-// are then broadcast.
+// (x + -0.0 == x for every x, so padding changes no sum), and lanes 0, 1 and 2 each add one of
+// the three in lane order, four at a time from 16-byte loads, the next four's loads in flight
+// during the additions; the sums are then broadcast.
 __shared__ __align__(16) float g_seq_buf[MAX_BLOCK_WARPS][3][32];
 __device__ __forceinline__ void lane_seq_sum3(float& a, float& b, float& c, float va, float vb, float vc,
                                               uint32_t lim) {
@@ -378,28 +378,31 @@ __device__ __forceinline__ void lane_seq_sum3(float& a, float& b, float& c, floa
   B[1][lane] = in ? vb : -0.0f;
   B[2][lane] = in ? vc : -0.0f;
   __syncwarp();
-  if (lane == 0) {
-    const float4* A4 = reinterpret_cast<const float4*>(B[0]);
-    const float4* B4 = reinterpret_cast<const float4*>(B[1]);
-    const float4* C4 = reinterpret_cast<const float4*>(B[2]);
+  // lanes 0, 1 and 2 each add one of the three sums (one instruction stream for all three)
+  if (lane < 3u) {
+    const float4* P4 = reinterpret_cast<const float4*>(B[lane]);
+    float acc = lane == 0u ? a : (lane == 1u ? b : c);
     const uint32_t groups = (lim + 3u) >> 2;
-    float4 x = A4[0], y = B4[0], z = C4[0];
+    float4 x = P4[0];
 #pragma unroll
     for (uint32_t g = 0; g < 8; ++g) {
       if (g >= groups) break;
-      float4 xn, yn, zn;
-      if (g + 1 < 8) { xn = A4[g + 1]; yn = B4[g + 1]; zn = C4[g + 1]; }
-      a += x.x; b += y.x; c += z.x;
-      a += x.y; b += y.y; c += z.y;
-      a += x.z; b += y.z; c += z.z;
-      a += x.w; b += y.w; c += z.w;
-      x = xn; y = yn; z = zn;
+      float4 xn;
+      if (g + 1 < 8) xn = P4[g + 1];
+      acc += x.x;
+      acc += x.y;
+      acc += x.z;
+      acc += x.w;
+      x = xn;
     }
+    if (lane == 0u) a = acc;
+    else if (lane == 1u) b = acc;
+    else c = acc;
   }
   __syncwarp();
   a = __shfl_sync(FULL, a, 0);
-  b = __shfl_sync(FULL, b, 0);
-  c = __shfl_sync(FULL, c, 0);
+  b = __shfl_sync(FULL, b, 1);
+  c = __shfl_sync(FULL, c, 2);
 }
 
 // One in-order sum over the lanes' values t = 0..lim-1 added to a (the same on every lane), like
