@@ -154,10 +154,10 @@ static __device__ void joint_apply_rows(const MillDev& m, float dt, const float2
   const uint32_t n = m.nf, nb = m.nb;
   const float mass = m.f_mass;
   const float k = dt * mass;
-  // (the loops are unrolled so that the independent loads of consecutive terms overlap; the
-  // additions keep their order)
-  for (uint32_t t = t0; t < n + nb; t += stride) {
-    if (t < n) {
+  // fluid rows 0..n-1, one thread per row (the loops are unrolled so that the independent loads
+  // of consecutive terms overlap; the additions keep their order)
+  for (uint32_t t = t0; t < n; t += stride) {
+    {
       const uint32_t i = t;
       const V2 lv(laplacian_row(m, xx, i).f2());
       V2 o = mass * (V2(xx[i]) + dt * lv);
@@ -174,44 +174,62 @@ static __device__ void joint_apply_rows(const MillDev& m, float dt, const float2
         o += d;
       }
       out[i] = o.f2();
-      continue;
     }
-    const uint32_t bi = t - n;
-    V2 vb(xx[n + bi]);
-    float w = xx[n + nb + bi].x;
-    V2 o = m.b_m * vb;
-    float oa = m.b_I * w;
-    const uint32_t g0 = m.g_off[bi], g1 = m.g_off[bi + 1];
-#pragma unroll 4
-    for (uint32_t g = g0; g < g1; ++g) {
-      uint32_t i = m.g_fluid[g];
-      V2 rel = V2(xx[i]) - vb;
-      V2 lc(m.g_lc[g]);
-      V2 d = k * (m.g_c[g] * rel - w * V2(-lc.y, lc.x));
-      o -= d;
-      oa -= k * (cross2(lc, rel) - w * m.g_l2[g]);
+  }
+  // ball rows n..n+nb-1, one warp per row: the lanes form the terms of 32 consecutive entries of
+  // the row (its groups, then the links naming it as the other ball, then its own links) in
+  // parallel, and the three running sums add them in entry order (lane_seq_sum3; o -= d as
+  // o + (-d), the same f32 result; entries without an angular term add -0.0, which changes nothing)
+  const uint32_t lane = tid() & 31u;
+  for (uint32_t bi = t0 >> 5; bi < nb; bi += stride >> 5) {
+    const V2 vb(xx[n + bi]);
+    const float w = xx[n + nb + bi].x;
+    float ox = 0.0f, oy = 0.0f, oa = 0.0f;
+    {
+      const V2 o0 = m.b_m * vb;
+      ox = o0.x;
+      oy = o0.y;
+      oa = m.b_I * w;
     }
-    const uint32_t lq0 = m.lo_start[bi], lq1 = m.lo_start[bi + 1];
-#pragma unroll 4
-    for (uint32_t q = lq0; q < lq1; ++q) {
-      uint32_t l = m.lo_list[q];
-      V2 rel = V2(xx[n + m.l_ball[l]]) - vb;
-      V2 ln(m.l_n[l]);
-      V2 d = (dt * m.l_c[l] * ln.dot(rel)) * ln;
-      o -= d;
+    const uint32_t g0 = m.g_off[bi], ng = m.g_off[bi + 1] - g0;
+    const uint32_t lq0 = m.lo_start[bi], nlo = m.lo_start[bi + 1] - lq0;
+    const uint32_t l0 = m.l_off[bi], nown = m.l_off[bi + 1] - l0;
+    const uint32_t cnt = ng + nlo + nown;
+    for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+      const uint32_t e = c0 + lane;
+      float tx = -0.0f, ty = -0.0f, ta = -0.0f;
+      if (e < ng) {
+        const uint32_t g = g0 + e;
+        const uint32_t i = m.g_fluid[g];
+        const V2 rel = V2(xx[i]) - vb;
+        const V2 lc(m.g_lc[g]);
+        const V2 d = k * (m.g_c[g] * rel - w * V2(-lc.y, lc.x));
+        tx = -d.x;
+        ty = -d.y;
+        ta = -(k * (cross2(lc, rel) - w * m.g_l2[g]));
+      } else if (e < ng + nlo) {
+        const uint32_t l = m.lo_list[lq0 + (e - ng)];
+        const V2 rel = V2(xx[n + m.l_ball[l]]) - vb;
+        const V2 ln(m.l_n[l]);
+        const V2 d = (dt * m.l_c[l] * ln.dot(rel)) * ln;
+        tx = -d.x;
+        ty = -d.y;
+      } else if (e < cnt) {
+        const uint32_t l = l0 + (e - ng - nlo);
+        const uint32_t other = m.l_other[l];
+        V2 rel = vb;
+        if (other != NONE) rel = rel - V2(xx[n + other]);
+        const V2 ln(m.l_n[l]);
+        const V2 d = (dt * m.l_c[l] * ln.dot(rel)) * ln;
+        tx = d.x;
+        ty = d.y;
+      }
+      lane_seq_sum3(ox, oy, oa, tx, ty, ta, min(32u, cnt - c0));
     }
-    const uint32_t l0 = m.l_off[bi], l1 = m.l_off[bi + 1];
-#pragma unroll 4
-    for (uint32_t l = l0; l < l1; ++l) {
-      uint32_t other = m.l_other[l];
-      V2 rel = vb;
-      if (other != NONE) rel = rel - V2(xx[n + other]);
-      V2 ln(m.l_n[l]);
-      V2 d = (dt * m.l_c[l] * ln.dot(rel)) * ln;
-      o += d;
+    if (lane == 0) {
+      out[n + bi] = make_float2(ox, oy);
+      out[n + nb + bi] = make_float2(oa, 0.0f);
     }
-    out[n + bi] = o.f2();
-    out[n + nb + bi] = make_float2(oa, 0.0f);
   }
 }
 
