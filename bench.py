@@ -36,7 +36,7 @@ sys.path.insert(0, ROOT)
 METRIC = "sub-steps/s (1 mill) & batched mill-frames/s on 1 B200; p50/p99 frame latency"
 UNIT = "sub-steps/s"
 # DRAM bytes (read + write) of one realtime frame launch, from an ncu capture (see profiles/)
-REALTIME_LAUNCH_DRAM_BYTES = 2.519e6 + 0.440e6
+REALTIME_LAUNCH_DRAM_BYTES = 2.435e6 + 0.377e6
 # The headline workload's description, the same in both arms' lines.
 CONFIG = {"workload": "realtime preset, 1 mill per GPU (63 mm drum, 407 ZrO2 discs of 2 mm, 794 fluid particles at "
                       "resolution 25, 24 sub-steps per 1/60 s frame)",
