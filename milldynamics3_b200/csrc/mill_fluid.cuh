@@ -249,36 +249,54 @@ static __device__ void cg_setup_rows(const MillDev& m, float dt, uint32_t t0, ui
   float2 *x = m.cg_x, *bvec = m.cg_b;
   float* diag = m.cg_diag;
   const bool use_guess = *m.guess_valid_dev != 0;
-  for (uint32_t t = t0; t < n + nb; t += stride) {
-    if (t < n) {
-      const uint32_t i = t;
-      V2 v(V[i]);
-      x[i] = (use_guess ? v + V2(m.fguess[i]) : v).f2();
-      bvec[i] = (mass * v).f2();
-      float sw = 0.0f;
-      for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) sw += m.visc_w[k];
-      float d = mass * (1.0f + dt * (0.5f * CENTRAL_VISC * sw));
-      for (uint32_t q = m.fg_start[i]; q < m.fg_start[i + 1]; ++q) d += dt * mass * m.g_c[m.fg_list[q]];
-      diag[i] = d;
-      m.dv_tmp[i] = V[i];  // v_in for the warm start of the next sub-step
-      continue;
-    }
-    const uint32_t b = t - n;
+  // fluid rows 0..n-1, one thread per row
+  for (uint32_t t = t0; t < n; t += stride) {
+    const uint32_t i = t;
+    V2 v(V[i]);
+    x[i] = (use_guess ? v + V2(m.fguess[i]) : v).f2();
+    bvec[i] = (mass * v).f2();
+    float sw = 0.0f;
+    for (uint32_t k = m.nbr_off[i]; k < m.nbr_off[i + 1]; ++k) sw += m.visc_w[k];
+    float d = mass * (1.0f + dt * (0.5f * CENTRAL_VISC * sw));
+    for (uint32_t q = m.fg_start[i]; q < m.fg_start[i + 1]; ++q) d += dt * mass * m.g_c[m.fg_list[q]];
+    diag[i] = d;
+    m.dv_tmp[i] = V[i];  // v_in for the warm start of the next sub-step
+  }
+  // ball rows, one warp per ball: the diagonal's terms (groups, then the links naming the ball as
+  // the other ball, then its own links) formed by the lanes in parallel and added in entry order
+  // by the three-way lane sum (link entries add -0.0 to the angular diagonal: no change)
+  const uint32_t lane = tid() & 31u;
+  for (uint32_t b = t0 >> 5; b < nb; b += stride >> 5) {
     V2 v0(m.ball_v0[b]);
     float w0 = m.ball_w0[b];
-    x[n + b] = v0.f2();
-    x[n + nb + b] = make_float2(w0, 0.0f);
-    bvec[n + b] = (m.b_m * v0).f2();
-    bvec[n + nb + b] = make_float2(m.b_I * w0, 0.0f);
-    float dl = m.b_m, da = m.b_I;
-    for (uint32_t g = m.g_off[b]; g < m.g_off[b + 1]; ++g) {
-      dl += dt * mass * m.g_c[g];
-      da += dt * mass * m.g_l2[g];
+    if (lane == 0) {
+      x[n + b] = v0.f2();
+      x[n + nb + b] = make_float2(w0, 0.0f);
+      bvec[n + b] = (m.b_m * v0).f2();
+      bvec[n + nb + b] = make_float2(m.b_I * w0, 0.0f);
     }
-    for (uint32_t q = m.lo_start[b]; q < m.lo_start[b + 1]; ++q) dl += dt * m.l_c[m.lo_list[q]];
-    for (uint32_t l = m.l_off[b]; l < m.l_off[b + 1]; ++l) dl += dt * m.l_c[l];
-    diag[n + b] = dl;
-    diag[n + nb + b] = da;
+    float dl = m.b_m, da = m.b_I, unused = 0.0f;
+    const uint32_t g0 = m.g_off[b], ng = m.g_off[b + 1] - g0;
+    const uint32_t lq0 = m.lo_start[b], nlo = m.lo_start[b + 1] - lq0;
+    const uint32_t l0 = m.l_off[b], nown = m.l_off[b + 1] - l0;
+    const uint32_t cnt = ng + nlo + nown;
+    for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+      const uint32_t e = c0 + lane;
+      float tl = -0.0f, ta = -0.0f;
+      if (e < ng) {
+        tl = dt * mass * m.g_c[g0 + e];
+        ta = dt * mass * m.g_l2[g0 + e];
+      } else if (e < ng + nlo) {
+        tl = dt * m.l_c[m.lo_list[lq0 + (e - ng)]];
+      } else if (e < cnt) {
+        tl = dt * m.l_c[l0 + (e - ng - nlo)];
+      }
+      lane_seq_sum3(dl, da, unused, tl, ta, -0.0f, min(32u, cnt - c0));
+    }
+    if (lane == 0) {
+      diag[n + b] = dl;
+      diag[n + nb + b] = da;
+    }
   }
 }
 
