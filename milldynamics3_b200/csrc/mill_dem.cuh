@@ -81,6 +81,12 @@ static __device__ __noinline__ float mech_energy_seq(const MillDev& m, const flo
   return e;
 }
 
+// The predict step's coupling work summed in ball order in f64 (dem.rs:577-586), by warp 0 (result
+// in every lane). Its own function, so that the unrolled shuffle loop does not spill.
+static __device__ __noinline__ double coupling_work_seq(const MillDev& m) {
+  return warp_ordered_sum(0.0, m.nb, [&](uint32_t i, double& t) { t = m.f_cw[i]; return true; });
+}
+
 // `iters` iterations of the projection (dem.rs:711-750): the pair items by dependency levels in
 // warp 0 (level-ordered descriptors di/dj, multipliers dl), then every wall at once. With track,
 // bm[i] keeps ball i's largest squared excursion from its start position m.bxs[i]. Its own
@@ -397,7 +403,7 @@ static __device__ __noinline__ void dem_step(const MillDev& m, const StepUniform
   max_disp = block_max_f(max_disp);
   max_speed = block_max_f(max_speed);
   if (tid() < 32) {
-    double cw = warp_ordered_sum(0.0, n, [&](uint32_t i, double& t) { t = m.f_cw[i]; return true; });
+    double cw = coupling_work_seq(m);
     float e = mech_energy_seq(m, X, V, OM);
     if (tid() == 0) { S.dscal[0] = cw; S.fscal[0] = e; }
   }
