@@ -574,6 +574,31 @@ static __device__ __noinline__ void dem_step(const MillDev& m, const StepUniform
   block_bucket_sort(m.dm_lvl, na_p, n, m.bk_start, m.bk_cur, m.bk_order);
   for (uint32_t b = tid(); b < n; b += nthr()) {
     const uint32_t s = m.bk_start[b], e = m.bk_start[b + 1];
+    if (e - s < 2u) continue;
+    if (e - s <= 8u) {
+      // up to 8 contacts: their keys (j) loaded once, a sorting network in registers (the keys
+      // of one bucket are distinct, so any correct sort gives the insertion sort's order)
+      const uint32_t c = e - s;
+      uint32_t kv[8], vv[8];
+#pragma unroll
+      for (uint32_t t = 0; t < 8; ++t) {
+        vv[t] = t < c ? m.bk_order[s + t] : 0u;
+        kv[t] = t < c ? m.pair_j[m.pr_list[vv[t]]] : 0xFFFFFFFFu;
+      }
+      auto ce = [&](int i, int j) {
+        if (kv[i] > kv[j]) {
+          const uint32_t tk = kv[i], tv = vv[i];
+          kv[i] = kv[j]; vv[i] = vv[j];
+          kv[j] = tk; vv[j] = tv;
+        }
+      };
+      ce(0, 1); ce(2, 3); ce(4, 5); ce(6, 7); ce(0, 2); ce(1, 3); ce(4, 6); ce(5, 7); ce(1, 2); ce(5, 6);
+      ce(0, 4); ce(3, 7); ce(1, 5); ce(2, 6); ce(1, 4); ce(3, 6); ce(2, 4); ce(3, 5); ce(3, 4);
+#pragma unroll
+      for (uint32_t t = 0; t < 8; ++t)
+        if (t < c) m.bk_order[s + t] = vv[t];
+      continue;
+    }
     for (uint32_t a = s + 1; a < e; ++a) {
       const uint32_t v = m.bk_order[a], vj = m.pair_j[m.pr_list[v]];
       uint32_t q = a;
